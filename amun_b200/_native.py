@@ -1,0 +1,107 @@
+"""ctypes binding of libamun_gpu.so (the C ABI declared in include/amun_gpu.h).
+
+The library is the only compute path: when it is missing or no CUDA device is
+present, calls raise AmunError; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libamun_gpu.so")
+
+AMUN_EQ_HD, AMUN_EQ_MHD = 0, 1
+AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
+AMUN_FP64, AMUN_FP32_BULK = 0, 1
+
+
+class AmunError(RuntimeError):
+    """Error reported by the C ABI (code is the returned iret)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"amun_gpu error {code}: {msg}")
+        self.code = code
+
+
+class amun_params(C.Structure):
+    _fields_ = [
+        ("ndims", C.c_int), ("eqsys", C.c_int), ("reconstruction", C.c_int), ("limiter", C.c_int),
+        ("extrema_limiter", C.c_int), ("riemann", C.c_int), ("time_advance", C.c_int), ("stages", C.c_int),
+        ("fix_positivity", C.c_int), ("clip_extrema", C.c_int), ("precision", C.c_int), ("ncells", C.c_int),
+        ("nghosts", C.c_int), ("gamma", C.c_double), ("cfl", C.c_double), ("alpha", C.c_double),
+        ("eps", C.c_double),
+    ]
+
+
+class amun_block_desc(C.Structure):
+    _fields_ = [("level", C.c_int), ("dx", C.c_double * 3), ("neighbor", C.c_int * 27)]
+
+
+class amun_status(C.Structure):
+    _fields_ = [("time", C.c_double), ("dt", C.c_double), ("dtn", C.c_double), ("cmax", C.c_double),
+                ("step", C.c_longlong), ("nonpositive", C.c_longlong), ("device_bytes", C.c_longlong)]
+
+
+_lib = None
+_D = C.POINTER(C.c_double)
+
+
+def lib():
+    """Load libamun_gpu.so (built by amun_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise AmunError(-1, f"{LIB_PATH} is missing; build it with `python -m amun_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    i, d, vp = C.c_int, C.c_double, C.c_void_p
+    sig = {
+        "amun_gpu_default_params": (None, [C.POINTER(amun_params)]),
+        "amun_gpu_set_param": (i, [C.POINTER(amun_params), C.c_char_p, C.c_char_p]),
+        "amun_gpu_init": (i, [C.POINTER(amun_params)]),
+        "amun_gpu_set_blocks": (i, [i, C.POINTER(amun_block_desc)]),
+        "amun_gpu_upload": (i, [i, _D, _D, _D]),
+        "amun_gpu_upload_blocks": (i, [i, i, _D, _D]),
+        "amun_gpu_download": (i, [i, _D, _D, _D]),
+        "amun_gpu_download_blocks": (i, [i, i, _D, _D]),
+        "amun_gpu_boundary_variables": (i, []),
+        "amun_gpu_new_time_step": (i, [d, _D, _D]),
+        "amun_gpu_evolve": (i, []),
+        "amun_gpu_advance": (i, [d, _D, _D]),
+        "amun_gpu_run": (i, [i, d, i]),
+        "amun_gpu_status": (i, [C.POINTER(amun_status)]),
+        "amun_gpu_set_time": (i, [d, d]),
+        "amun_gpu_update_flux_block": (i, [_D, _D, _D]),
+        "amun_gpu_riemann": (i, [i, _D, _D, _D]),
+        "amun_gpu_prim2cons": (i, [i, _D, _D]),
+        "amun_gpu_cons2prim": (i, [i, _D, _D]),
+        "amun_gpu_fluxspeed": (i, [i, _D, _D, _D, _D, _D]),
+        "amun_gpu_maxspeed": (i, [_D, _D]),
+        "amun_gpu_set_cmax": (i, [d]),
+        "amun_gpu_set_stream": (i, [vp]),
+        "amun_gpu_profile": (i, [i, i]),
+        "amun_gpu_profile_read": (i, [i, _D, C.POINTER(C.c_longlong)]),
+        "amun_gpu_finalize": (None, []),
+        "amun_gpu_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(code: int):
+    if code != 0:
+        msg = lib().amun_gpu_last_error()
+        raise AmunError(code, msg.decode() if msg else "")
+
+
+def dptr(a):
+    """double* of a C-contiguous float64 numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.dtype.name == "float64" and a.flags["C_CONTIGUOUS"], "expected C-contiguous float64"
+    return a.ctypes.data_as(_D)

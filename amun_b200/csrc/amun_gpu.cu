@@ -1,0 +1,864 @@
+// amun_gpu.cu -- host side of libamun_gpu.so: the C ABI of include/amun_gpu.h.
+//
+// Owns the HBM block pool, builds the stage schedule of the selected SSPRK
+// integrator (src/evolution.F90:517-1793), launches the per-direction sweep
+// kernels, ghost fill and CFL kernels on one stream, and optionally replays
+// whole steps from captured CUDA graphs.  No CPU fallback: every compute
+// entry point fails with AMUN_E_CUDA when no device is usable.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/amun_gpu.h"
+#include "launch.cuh"
+#include "unit.h"
+
+using namespace amun;
+
+namespace {
+
+enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
+
+struct Ctx {
+  bool inited = false;
+  amun_params p{};
+  int nv = 5;
+  double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5;
+  double cfl = 0.5, decay = 1.0;
+  double host_cmax = 0.0;  // module cmax for the unit entry points
+  // mesh
+  int nblocks = 0;
+  Geo g{};
+  std::vector<amun_block_desc> blocks;
+  double dx_min = 1.0;
+  // device pool
+  void* q[2] = {nullptr, nullptr};
+  double* u0 = nullptr;
+  void* u1 = nullptr;
+  void* du = nullptr;
+  int* nbr = nullptr;
+  double* binv = nullptr;
+  DevScalars* sc = nullptr;
+  double* staging = nullptr;
+  size_t staging_bytes = 0;
+  long long pool_bytes = 0;
+  int cur = 0;            // q buffer holding the current primitives
+  bool ms_valid = false;  // max-speed accumulator holds the current state
+  cudaStream_t stream = nullptr;      // the stream every launch goes to
+  cudaStream_t own_stream = nullptr;  // the library's stream
+  // captured step graphs, one per parity of the q ping-pong
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dtnext[2] = {0, 0};
+  bool capturing = false;
+  // per-kernel timers
+  bool prof_on = false;
+  struct Mark { int kind; cudaEvent_t a, b; };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  long long prof_n[5] = {0, 0, 0, 0, 0};
+  std::string err;
+};
+
+Ctx C;
+
+cudaEvent_t pool_event() {
+  if (!C.event_pool.empty()) {
+    cudaEvent_t e = C.event_pool.back();
+    C.event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// RAII timer around one launch when profiling eagerly
+struct ProfScope {
+  int kind;
+  bool on;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit ProfScope(int k) : kind(k), on(C.prof_on && !C.capturing) {
+    if (on) { a = pool_event(); b = pool_event(); cudaEventRecord(a, C.stream); }
+  }
+  ~ProfScope() {
+    if (on) { cudaEventRecord(b, C.stream); C.marks.push_back({kind, a, b}); }
+  }
+};
+
+void prof_collect() {
+  if (C.marks.empty()) return;
+  cudaStreamSynchronize(C.stream);
+  for (auto& m : C.marks) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) {
+      C.prof_ms[m.kind] += ms;
+      C.prof_n[m.kind] += 1;
+    }
+    C.event_pool.push_back(m.a);
+    C.event_pool.push_back(m.b);
+  }
+  C.marks.clear();
+}
+
+int fail(int code, const std::string& msg) {
+  C.err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+  C.err = std::string(where) + ": " + cudaGetErrorString(e);
+  return AMUN_E_CUDA;
+}
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);       \
+  } while (0)
+
+bool bulk() { return C.p.precision == AMUN_FP32_BULK; }
+size_t rsize() { return bulk() ? sizeof(float) : sizeof(double); }
+
+bool is_one_of(const char* s, std::initializer_list<const char*> l) {
+  for (auto* x : l)
+    if (!strcmp(s, x)) return true;
+  return false;
+}
+bool is_on(const char* s) { return is_one_of(s, {"on", "ON", "t", "T", "y", "Y", "true", "TRUE", "yes", "YES"}); }
+
+std::string strip(const char* v) {
+  std::string s(v ? v : "");
+  size_t a = s.find_first_not_of(" \t\"'"), b = s.find_last_not_of(" \t\"'");
+  return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+void free_pool() {
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  for (auto& x : C.q)
+    if (x) { cudaFree(x); x = nullptr; }
+  if (C.u0) cudaFree(C.u0);
+  if (C.u1) cudaFree(C.u1);
+  if (C.du) cudaFree(C.du);
+  if (C.nbr) cudaFree(C.nbr);
+  if (C.binv) cudaFree(C.binv);
+  if (C.staging) cudaFree(C.staging);
+  C.u0 = nullptr; C.u1 = nullptr; C.du = nullptr; C.nbr = nullptr; C.binv = nullptr; C.staging = nullptr;
+  C.staging_bytes = 0;
+  C.pool_bytes = 0;
+  C.nblocks = 0;
+}
+
+int ensure_staging(size_t bytes) {
+  if (C.staging_bytes >= bytes) return 0;
+  if (C.staging) cudaFree(C.staging);
+  C.staging = nullptr;
+  C.staging_bytes = 0;
+  CK(cudaMalloc(&C.staging, bytes));
+  C.staging_bytes = bytes;
+  return 0;
+}
+
+// --- stage schedule ------------------------------------------------------------
+// Each integrator of src/evolution.F90 as a list of stage combinations.
+struct Schedule {
+  bool copy_first = false;  // evolve_ssprk2: U1 = U0 before the stages
+  std::vector<StageDesc> stages;
+};
+
+StageDesc sd(int form, int a, int b, int out, double ca, double cb, double dscoef, int fin = 0) {
+  StageDesc s;
+  s.form = form; s.a_src = a; s.b_src = b; s.out_dst = out; s.final_stage = fin;
+  s.ca = ca; s.cb = cb; s.dscoef = dscoef;
+  return s;
+}
+
+Schedule schedule() {
+  Schedule S;
+  switch (C.p.time_advance) {
+    case TA_EULER:  // evolve_euler 517-611
+      S.stages = {sd(0, 0, 0, 0, 0, 0, 1.0, 1)};
+      break;
+    case TA_SSPRK2: {  // evolve_ssprk2 791-986
+      int m = C.p.stages;
+      double ft = 1.0 / (m - 1), fl = 1.0 / m, fr = 1.0 - fl;
+      S.copy_first = true;
+      for (int n = 1; n <= m - 1; ++n) S.stages.push_back(sd(0, 1, 1, 1, 0, 0, ft));
+      S.stages.push_back(sd(3, 0, 1, 0, fl, fr, ft, 1));
+      break;
+    }
+    case TA_RK3: {  // evolve_rk3 1005-1208
+      const double f21 = 3.0 / 4.0, f22 = 1.0 / 4.0, f31 = 1.0 / 3.0, f32 = 2.0 / 3.0;
+      S.stages = {sd(0, 0, 0, 1, 0, 0, 1.0), sd(1, 0, 1, 1, f21, f22, f22), sd(1, 0, 1, 0, f31, f32, f32, 1)};
+      break;
+    }
+    case TA_SSPRK34: {  // evolve_ssprk34 1228-1472
+      const double b1 = 1.0 / 2.0, b3 = 1.0 / 6.0, a31 = 2.0 / 3.0, a33 = 1.0 / 3.0;
+      S.stages = {sd(0, 0, 0, 1, 0, 0, b1), sd(0, 1, 1, 1, 0, 0, b1), sd(1, 0, 1, 1, a31, a33, b3),
+                  sd(0, 1, 1, 0, 0, 0, b1, 1)};
+      break;
+    }
+    case TA_SSPRK35: {  // evolve_ssprk35 1492-1793
+      const double b1 = 3.77268915331368e-01, b3 = 2.42995220537396e-01;
+      const double b4 = 2.38458932846290e-01, b5 = 2.87632146308408e-01;
+      const double a31 = 3.55909775063327e-01, a33 = 6.44090224936673e-01;
+      const double a41 = 3.67933791638137e-01, a44 = 6.32066208361863e-01;
+      const double a53 = 2.37593836598569e-01, a55 = 7.62406163401431e-01;
+      S.stages = {sd(0, 0, 0, 1, 0, 0, b1), sd(0, 1, 1, 1, 0, 0, b1), sd(1, 0, 1, 1, a31, a33, b3),
+                  sd(1, 0, 1, 0, a41, a44, b4), sd(1, 1, 0, 0, a53, a55, b5, 1)};
+      break;
+    }
+    default:  // evolve_rk2 628-770
+      S.stages = {sd(0, 0, 0, 1, 0, 0, 1.0), sd(2, 0, 1, 0, 0, 0, 1.0, 1)};
+      break;
+  }
+  return S;
+}
+
+// tile shape of the sweep kernels: LP cells along the sweep, LW lanes
+void tile_shape(int& LP, int& LW) {
+  int nc = C.g.nc;
+  LP = 1;
+  for (int d = 32; d >= 1; --d)
+    if (nc % d == 0) { LP = d; break; }
+  LW = 1;
+  for (int d = 256 / LP; d >= 1; --d)
+    if (nc % d == 0 && (LP + 2) * d <= 288) { LW = d; break; }
+}
+
+MethodConst method_const() {
+  MethodConst m;
+  m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.eps = C.p.eps; m.decay = C.decay;
+  m.lim = C.p.limiter; m.clim = C.p.extrema_limiter; m.positivity = C.p.fix_positivity; m.clip = C.p.clip_extrema;
+  return m;
+}
+
+template <typename R>
+int launch_stage(const StageDesc& st) {
+  int LP, LW;
+  tile_shape(LP, LW);
+  const int RR = C.p.reconstruction == AMUN_REC_WENO5Z ? 2 : 1;
+  const int threads = (((LP + 2) * LW + 31) / 32) * 32;
+  const size_t smem = (size_t)C.nv * ((LP + 2 * RR + 2) + 2 * (LP + 2)) * LW * sizeof(R);
+  const int nthird = C.g.ndims == 3 ? C.g.nc : 1;
+  dim3 grid((C.g.nc / LP) * (C.g.nc / LW) * nthird, C.nblocks);
+  SweepArgs<R, R> a;
+  a.q = (const R*)C.q[C.cur];
+  a.du = (R*)C.du;
+  a.u0 = C.u0;
+  a.u1 = (R*)C.u1;
+  a.qout = (R*)C.q[1 - C.cur];
+  a.sc = C.sc;
+  a.binv = C.binv;
+  a.g = C.g;
+  a.m = method_const();
+  a.st = st;
+  a.LP = LP; a.LW = LW;
+  int rs = C.p.riemann;
+  if (C.nv == 5 && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
+  for (int d = 0; d < C.g.ndims; ++d) {
+    a.first = d == 0;
+    a.last = d == C.g.ndims - 1;
+    ProfScope ps(d);
+    cudaError_t e = Launch<R, R>::sweep(C.nv, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+  }
+  C.cur = 1 - C.cur;
+  ProfScope ps(3);
+  cudaError_t e = Launch<R, R>::ghost((R*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  return 0;
+}
+
+template <typename R>
+int launch_evolve() {
+  Schedule S = schedule();
+  if (S.copy_first) {
+    long long n = (long long)C.nblocks * C.g.ubs;
+    cudaError_t e = Launch<R, R>::copy_u0_u1(C.u0, (R*)C.u1, n, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "copy u0->u1");
+  }
+  for (const auto& st : S.stages) {
+    int r = launch_stage<R>(st);
+    if (r) return r;
+  }
+  return 0;
+}
+
+int evolve_launches() { return bulk() ? launch_evolve<float>() : launch_evolve<double>(); }
+
+int ensure_maxspeed() {
+  if (C.ms_valid) return 0;
+  CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
+  cudaError_t e = bulk() ? Launch<float, float>::maxspeed(C.nv, (const float*)C.q[C.cur], C.g, C.gamma, C.sc,
+                                                          C.nblocks, C.stream)
+                         : Launch<double, double>::maxspeed(C.nv, (const double*)C.q[C.cur], C.g, C.gamma, C.sc,
+                                                            C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
+  C.ms_valid = true;
+  return 0;
+}
+
+// one advance: new_time_step, evolve, time update (device only)
+int step_launches(double dtnext) {
+  {
+    ProfScope ps(4);
+    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+    CK(cudaGetLastError());
+  }
+  int r = evolve_launches();
+  if (r) return r;
+  ProfScope ps(4);
+  end_step_kernel<<<1, 32, 0, C.stream>>>(C.sc);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int check_ready() {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (C.nblocks <= 0) return fail(AMUN_E_NO_BLOCKS, "amun_gpu_set_blocks has not been called");
+  return 0;
+}
+
+UnitArgs unit_args(int im, int jm, int km) {
+  UnitArgs u;
+  u.nv = C.nv; u.ndims = C.p.ndims; u.im = im; u.jm = jm; u.km = km; u.ng = C.p.nghosts;
+  u.rec = C.p.reconstruction; u.lim = C.p.limiter; u.clim = C.p.extrema_limiter;
+  u.rs = (C.nv == 5 && C.p.riemann == AMUN_RS_HLLD) ? AMUN_RS_HLL : C.p.riemann;
+  u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
+  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax;
+  return u;
+}
+
+// scratch device buffers for the unit entry points
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+}  // namespace
+
+extern "C" {
+
+void amun_gpu_default_params(amun_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->ndims = 2;
+  p->eqsys = AMUN_EQ_HD;
+  p->reconstruction = AMUN_REC_TVD;
+  p->limiter = AMUN_LIM_MM;
+  p->extrema_limiter = AMUN_LIM_MM;
+  p->riemann = AMUN_RS_HLL;
+  p->time_advance = AMUN_TA_RK2;
+  p->stages = 2;
+  p->fix_positivity = 0;
+  p->clip_extrema = 0;
+  p->precision = AMUN_FP64;
+  p->ncells = 8;
+  p->nghosts = 2;
+  p->gamma = 5.0 / 3.0;
+  p->cfl = 0.5;
+  p->alpha = 2.0;
+  p->eps = 2.220446049250313e-16;  // epsilon(1d0)
+}
+
+int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
+  if (!p || !key) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  std::string vs = strip(value);
+  const char* v = vs.c_str();
+  std::string k(key);
+  if (k == "ndims") p->ndims = atoi(v);
+  else if (k == "equation_system") {
+    if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p->eqsys = AMUN_EQ_HD;
+    else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p->eqsys = AMUN_EQ_MHD;
+    else return fail(100, std::string("equation system not implemented: ") + v);
+  } else if (k == "equation_of_state") {
+    if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"}))
+      return fail(110, std::string("equation of state not implemented: ") + v);
+  } else if (k == "reconstruction") {
+    if (is_one_of(v, {"tvd", "TVD"})) p->reconstruction = AMUN_REC_TVD;
+    else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p->reconstruction = AMUN_REC_WENO5Z;
+    else return fail(200, std::string("reconstruction not implemented: ") + v);
+  } else if (k == "limiter" || k == "extrema_limiter") {
+    int l = AMUN_LIM_ZERO;
+    if (is_one_of(v, {"mm", "minmod"})) l = AMUN_LIM_MM;
+    else if (is_one_of(v, {"mc", "monotonized_central"})) l = AMUN_LIM_MC;
+    else if (is_one_of(v, {"sb", "superbee"})) l = AMUN_LIM_SB;
+    else if (is_one_of(v, {"vl", "vanleer"})) l = AMUN_LIM_VL;
+    else if (k == "limiter" && is_one_of(v, {"va", "vanalbada"})) l = AMUN_LIM_VA;
+    if (k == "limiter") p->limiter = l; else p->extrema_limiter = l;
+  } else if (k == "riemann_solver") {
+    if (is_one_of(v, {"hllc", "HLLC"})) p->riemann = AMUN_RS_HLLC;
+    else if (is_one_of(v, {"hlld", "HLLD"})) p->riemann = AMUN_RS_HLLD;
+    else if (is_one_of(v, {"roe", "ROE"})) p->riemann = AMUN_RS_ROE;
+    else p->riemann = AMUN_RS_HLL;
+  } else if (k == "time_advance") {
+    if (is_one_of(v, {"euler", "EULER"})) p->time_advance = AMUN_TA_EULER;
+    else if (is_one_of(v, {"rk2", "RK2"})) p->time_advance = AMUN_TA_RK2;
+    else if (is_one_of(v, {"ssprk(m,2)", "SSPRK(m,2)"})) p->time_advance = AMUN_TA_SSPRK2;
+    else if (is_one_of(v, {"rk3", "RK3"})) p->time_advance = AMUN_TA_RK3;
+    else if (is_one_of(v, {"rk3.4", "RK3.4", "ssprk(4,3)", "SSPRK(4,3)"})) p->time_advance = AMUN_TA_SSPRK34;
+    else if (is_one_of(v, {"rk3.5", "RK3.5", "ssprk(5,3)", "SSPRK(5,3)"})) p->time_advance = AMUN_TA_SSPRK35;
+    else p->time_advance = AMUN_TA_RK2;
+  } else if (k == "stages") p->stages = atoi(v);
+  else if (k == "fix_positivity") p->fix_positivity = is_on(v);
+  else if (k == "clip_extrema") p->clip_extrema = is_on(v);
+  else if (k == "precision") {
+    if (is_one_of(v, {"fp32", "FP32", "fp32_bulk", "bulk"})) p->precision = AMUN_FP32_BULK;
+    else p->precision = AMUN_FP64;
+  } else if (k == "ncells") p->ncells = atoi(v);
+  else if (k == "nghosts") p->nghosts = atoi(v);
+  else if (k == "gamma") p->gamma = atof(v);
+  else if (k == "cfl") p->cfl = atof(v);
+  else if (k == "alpha") p->alpha = atof(v);
+  else if (k == "eps") p->eps = atof(v);
+  return 0;
+}
+
+int amun_gpu_init(const amun_params* p) {
+  if (!p) return fail(AMUN_E_BAD_ARGUMENT, "null params");
+  if (p->ndims != 2 && p->ndims != 3) return fail(AMUN_E_BAD_ARGUMENT, "ndims must be 2 or 3");
+  if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD) return fail(100, "equation system not implemented");
+  if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
+    return fail(200, "reconstruction not implemented");
+  int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;
+  if (p->nghosts < need || p->ncells < p->nghosts)
+    return fail(AMUN_E_BAD_ARGUMENT, "nghosts too small for the reconstruction stencil (or ncells < nghosts)");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(AMUN_E_CUDA, "no CUDA device available");
+  free_pool();
+  if (!C.own_stream) CK(cudaStreamCreateWithFlags(&C.own_stream, cudaStreamNonBlocking));
+  if (!C.stream) C.stream = C.own_stream;
+  if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
+  CK(cudaMemset(C.sc, 0, sizeof(DevScalars)));
+  C.p = *p;
+  C.nv = p->eqsys == AMUN_EQ_MHD ? 9 : 5;
+  C.gamma = p->gamma;
+  C.gammam1 = C.gamma - 1.0;
+  C.gammam1i = 1.0 / C.gammam1;
+  // CFL rescale of the SSPRK variants and the GLM decay factor
+  // (src/evolution.F90:164-213)
+  C.cfl = p->cfl;
+  if (p->time_advance == AMUN_TA_SSPRK2) {
+    C.p.stages = p->stages < 2 ? 2 : (p->stages > 9 ? 9 : p->stages);
+    C.cfl = (C.p.stages - 1) * C.cfl;
+  }
+  if (p->time_advance == AMUN_TA_SSPRK34) C.cfl = 2.0 * C.cfl;
+  if (p->time_advance == AMUN_TA_SSPRK35) C.cfl = 2.65062919143939 * C.cfl;
+  C.decay = std::exp(-p->alpha * C.cfl);
+  C.inited = true;
+  C.err.clear();
+  return 0;
+}
+
+int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (nblocks <= 0 || !blocks) return fail(AMUN_E_BAD_ARGUMENT, "empty block list");
+  for (int b = 0; b < nblocks; ++b) {
+    for (int n = 0; n < 27; ++n) {
+      int nb = blocks[b].neighbor[n];
+      if (nb >= nblocks) return fail(AMUN_E_BAD_ARGUMENT, "neighbour index out of range");
+      if (nb >= 0 && blocks[nb].level != blocks[b].level)
+        return fail(AMUN_E_UNSUPPORTED, "neighbours at a different level are not supported");
+      if (nb < 0 && n != 13) return fail(AMUN_E_UNSUPPORTED, "non-periodic domain boundaries are not supported");
+    }
+  }
+  free_pool();
+  const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
+  Geo& g = C.g;
+  g.nc = nc; g.ng = ng; g.ndims = nd;
+  g.IM = nc + 2 * ng; g.JM = nc + 2 * ng; g.KM = nd == 3 ? nc + 2 * ng : 1;
+  g.qvs = (long long)g.IM * g.JM * g.KM;
+  g.qbs = g.qvs * C.nv;
+  g.uvs = (long long)nc * nc * (nd == 3 ? nc : 1);
+  g.ubs = g.uvs * C.nv;
+  C.nblocks = nblocks;
+  C.blocks.assign(blocks, blocks + nblocks);
+  const size_t rs = rsize();
+  size_t qbytes = (size_t)g.qbs * nblocks * rs, ubytes = (size_t)g.ubs * nblocks;
+  CK(cudaMalloc(&C.q[0], qbytes));
+  CK(cudaMalloc(&C.q[1], qbytes));
+  CK(cudaMalloc(&C.u0, ubytes * sizeof(double)));
+  CK(cudaMalloc(&C.u1, ubytes * rs));
+  CK(cudaMalloc(&C.du, ubytes * rs));
+  CK(cudaMemset(C.q[0], 0, qbytes));
+  CK(cudaMemset(C.q[1], 0, qbytes));
+  CK(cudaMemset(C.u0, 0, ubytes * sizeof(double)));
+  CK(cudaMemset(C.u1, 0, ubytes * rs));
+  C.pool_bytes = (long long)(2 * qbytes + ubytes * (sizeof(double) + 2 * rs));
+  std::vector<int> nbr(27 * (size_t)nblocks);
+  std::vector<double> binv(3 * (size_t)nblocks);
+  C.dx_min = 1e300;
+  for (int b = 0; b < nblocks; ++b) {
+    for (int n = 0; n < 27; ++n) nbr[27 * b + n] = blocks[b].neighbor[n];
+    nbr[27 * b + 13] = b;
+    for (int d = 0; d < 3; ++d) binv[3 * b + d] = 1.0 / blocks[b].dx[d];
+    // dx_min of the finest level (src/evolution.F90:465-475)
+    double m = blocks[b].dx[0] < blocks[b].dx[1] ? blocks[b].dx[0] : blocks[b].dx[1];
+    if (nd == 3) m = m < blocks[b].dx[2] ? m : blocks[b].dx[2];
+    if (m < C.dx_min) C.dx_min = m;
+  }
+  CK(cudaMalloc(&C.nbr, nbr.size() * sizeof(int)));
+  CK(cudaMalloc(&C.binv, binv.size() * sizeof(double)));
+  CK(cudaMemcpy(C.nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(C.binv, binv.data(), binv.size() * sizeof(double), cudaMemcpyHostToDevice));
+  C.cur = 0;
+  C.ms_valid = false;
+  return 0;
+}
+
+static int upload_range(int first, int count, const double* u0, const double* u1, const double* q) {
+  int r = check_ready();
+  if (r) return r;
+  if (first < 0 || count <= 0 || first + count > C.nblocks) return fail(AMUN_E_BAD_ARGUMENT, "block range");
+  const Geo& g = C.g;
+  size_t per = (size_t)g.qbs * sizeof(double);  // one Fortran block array
+  if ((r = ensure_staging(per * count))) return r;
+  cudaError_t e;
+  if (q) {
+    CK(cudaMemcpyAsync(C.staging, q, per * count, cudaMemcpyHostToDevice, C.stream));
+    e = bulk() ? Launch<float, float>::upload_q(C.staging, (float*)C.q[C.cur], g, C.nv, first, count, C.stream)
+               : Launch<double, double>::upload_q(C.staging, (double*)C.q[C.cur], g, C.nv, first, count, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "upload q");
+  }
+  if (u0) {
+    CK(cudaMemcpyAsync(C.staging, u0, per * count, cudaMemcpyHostToDevice, C.stream));
+    e = Launch<double, double>::upload_u0(C.staging, C.u0, g, C.nv, first, count, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "upload u0");
+  }
+  if (u1) {
+    CK(cudaMemcpyAsync(C.staging, u1, per * count, cudaMemcpyHostToDevice, C.stream));
+    e = bulk() ? Launch<float, float>::upload_u1(C.staging, (float*)C.u1, g, C.nv, first, count, C.stream)
+               : Launch<double, double>::upload_u1(C.staging, (double*)C.u1, g, C.nv, first, count, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "upload u1");
+  }
+  C.ms_valid = false;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_upload(int block, const double* u0, const double* u1, const double* q) {
+  return upload_range(block, 1, u0, u1, q);
+}
+int amun_gpu_upload_blocks(int first, int count, const double* u0, const double* q) {
+  return upload_range(first, count, u0, nullptr, q);
+}
+
+static int download_range(int first, int count, double* u0, double* u1, double* q) {
+  int r = check_ready();
+  if (r) return r;
+  if (first < 0 || count <= 0 || first + count > C.nblocks) return fail(AMUN_E_BAD_ARGUMENT, "block range");
+  const Geo& g = C.g;
+  size_t per = (size_t)g.qbs * sizeof(double);
+  if ((r = ensure_staging(per * count))) return r;
+  cudaError_t e;
+  if (q) {
+    e = bulk() ? Launch<float, float>::download_q((const float*)C.q[C.cur], C.staging, g, C.nv, first, count, C.stream)
+               : Launch<double, double>::download_q((const double*)C.q[C.cur], C.staging, g, C.nv, first, count,
+                                                    C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "download q");
+    CK(cudaMemcpyAsync(q, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  if (u0) {
+    e = bulk() ? Launch<float, float>::download_u0(C.nv, C.u0, (const float*)C.q[C.cur], C.staging, g, C.gammam1i,
+                                                   first, count, C.stream)
+               : Launch<double, double>::download_u0(C.nv, C.u0, (const double*)C.q[C.cur], C.staging, g,
+                                                     C.gammam1i, first, count, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "download u0");
+    CK(cudaMemcpyAsync(u0, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  if (u1) {
+    e = bulk() ? Launch<float, float>::download_u1(C.nv, (const float*)C.u1, (const float*)C.q[C.cur], C.staging, g,
+                                                   C.gammam1i, first, count, C.stream)
+               : Launch<double, double>::download_u1(C.nv, (const double*)C.u1, (const double*)C.q[C.cur],
+                                                     C.staging, g, C.gammam1i, first, count, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "download u1");
+    CK(cudaMemcpyAsync(u1, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  return 0;
+}
+
+int amun_gpu_download(int block, double* u0, double* u1, double* q) { return download_range(block, 1, u0, u1, q); }
+int amun_gpu_download_blocks(int first, int count, double* u0, double* q) {
+  return download_range(first, count, u0, nullptr, q);
+}
+
+int amun_gpu_boundary_variables(void) {
+  int r = check_ready();
+  if (r) return r;
+  cudaError_t e = bulk() ? Launch<float, float>::ghost((float*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream)
+                         : Launch<double, double>::ghost((double*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt) {
+  int r = check_ready();
+  if (r) return r;
+  if ((r = ensure_maxspeed())) return r;
+  new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+  CK(cudaGetLastError());
+  DevScalars h;
+  CK(cudaMemcpyAsync(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+  CK(cudaStreamSynchronize(C.stream));
+  // the accumulator was consumed; the current state's max speed is still the
+  // one just used, so restore it for a following advance
+  unsigned long long bits;
+  double cm = h.cmax;
+  memcpy(&bits, &cm, sizeof(bits));
+  CK(cudaMemcpy(&C.sc->ms_bits, &bits, sizeof(bits), cudaMemcpyHostToDevice));
+  if (cmax) *cmax = h.cmax;
+  if (dt) *dt = h.dt;
+  C.host_cmax = h.cmax;
+  return 0;
+}
+
+int amun_gpu_evolve(void) {
+  int r = check_ready();
+  if (r) return r;
+  // evolve uses the module dt/cmax of the last new_time_step; the max-speed
+  // accumulator is re-armed by the final stage
+  CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
+  if ((r = evolve_launches())) return r;
+  C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_advance(double dtnext, double* time, double* dt) {
+  int r = check_ready();
+  if (r) return r;
+  if ((r = ensure_maxspeed())) return r;
+  if ((r = step_launches(dtnext))) return r;
+  C.ms_valid = true;
+  if (time || dt) {
+    DevScalars h;
+    CK(cudaMemcpyAsync(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+    if (time) *time = h.time;
+    if (dt) *dt = h.dt;
+  } else {
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  return 0;
+}
+
+int amun_gpu_run(int nsteps, double dtnext, int use_graph) {
+  int r = check_ready();
+  if (r) return r;
+  if (nsteps <= 0) return 0;
+  if ((r = ensure_maxspeed())) return r;
+  if (!use_graph) {
+    for (int n = 0; n < nsteps; ++n)
+      if ((r = step_launches(dtnext))) return r;
+  } else {
+    for (int n = 0; n < nsteps; ++n) {
+      int par = C.cur;
+      if (!C.graph[par] || C.graph_dtnext[par] != dtnext) {
+        // run this step eagerly (first launches configure the kernels), then
+        // capture the step graph of this q-buffer parity for later steps
+        if ((r = step_launches(dtnext))) return r;
+        int after = C.cur;
+        C.cur = par;
+        if (C.graph[par]) { cudaGraphExecDestroy(C.graph[par]); C.graph[par] = nullptr; }
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
+        int cur0 = C.cur;
+        C.capturing = true;
+        r = step_launches(dtnext);
+        C.capturing = false;
+        cudaError_t e = cudaStreamEndCapture(C.stream, &gr);
+        C.cur = cur0;  // the capture did not execute anything
+        if (r) return r;
+        if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+        e = cudaGraphInstantiate(&C.graph[par], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+        C.graph_dtnext[par] = dtnext;
+        C.cur = after;
+        continue;
+      }
+      CK(cudaGraphLaunch(C.graph[par], C.stream));
+      // a step flips the q buffer once per stage
+      if (schedule().stages.size() % 2) C.cur = 1 - C.cur;
+    }
+  }
+  C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_status(amun_status* s) {
+  if (!s) return fail(AMUN_E_BAD_ARGUMENT, "null status");
+  memset(s, 0, sizeof(*s));
+  if (!C.inited || !C.sc) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  DevScalars h;
+  CK(cudaStreamSynchronize(C.stream));
+  CK(cudaMemcpy(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost));
+  s->time = h.time; s->dt = h.dt; s->dtn = h.dtn; s->cmax = h.cmax; s->step = h.step;
+  s->nonpositive = (long long)h.nonpositive;
+  s->device_bytes = C.pool_bytes;
+  return 0;
+}
+
+int amun_gpu_set_time(double time, double dt) {
+  if (!C.inited || !C.sc) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  CK(cudaStreamSynchronize(C.stream));
+  DevScalars h;
+  CK(cudaMemcpy(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost));
+  h.time = time; h.dt = dt;
+  CK(cudaMemcpy(C.sc, &h, sizeof(h), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int amun_gpu_update_flux_block(const double* dx, const double* q, double* f) {
+  (void)dx;  // the adiabatic HD/MHD flux of the reference does not use dx
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (!q || !f) return fail(AMUN_E_BAD_ARGUMENT, "null array");
+  const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
+  const int im = nc + 2 * ng, jm = im, km = nd == 3 ? im : 1;
+  UnitArgs u = unit_args(im, jm, km);
+  size_t cells = (size_t)im * jm * km;
+  DevBuf dq, dqs, df, dsc, dnp;
+  CK(cudaMalloc(&dq.p, cells * C.nv * sizeof(double)));
+  CK(cudaMalloc(&dqs.p, cells * C.nv * 2 * nd * sizeof(double)));
+  CK(cudaMalloc(&df.p, cells * C.nv * nd * sizeof(double)));
+  CK(cudaMalloc(&dsc.p, unit_block_flux_scratch(u)));
+  CK(cudaMalloc(&dnp.p, sizeof(unsigned long long)));
+  CK(cudaMemcpy(dq.p, q, cells * C.nv * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemset(df.p, 0, cells * C.nv * nd * sizeof(double)));
+  CK(cudaMemset(dqs.p, 0, cells * C.nv * 2 * nd * sizeof(double)));
+  CK(cudaMemset(dnp.p, 0, sizeof(unsigned long long)));
+  cudaError_t e = unit_block_flux(u, (const double*)dq.p, (double*)dqs.p, (double*)df.p, (double*)dsc.p,
+                                  (unsigned long long*)dnp.p, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "update_flux_block");
+  CK(cudaStreamSynchronize(C.stream));
+  CK(cudaMemcpy(f, df.p, cells * C.nv * nd * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int amun_gpu_riemann(int n, const double* ql, const double* qr, double* f) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (n <= 0 || !ql || !qr || !f) return fail(AMUN_E_BAD_ARGUMENT, "bad arguments");
+  UnitArgs u = unit_args(0, 0, 0);
+  size_t bytes = (size_t)n * C.nv * sizeof(double);
+  DevBuf a, b, o;
+  CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&b.p, bytes)); CK(cudaMalloc(&o.p, bytes));
+  CK(cudaMemcpy(a.p, ql, bytes, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.p, qr, bytes, cudaMemcpyHostToDevice));
+  cudaError_t e = unit_riemann(u, n, (const double*)a.p, (const double*)b.p, (double*)o.p, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "riemann");
+  CK(cudaStreamSynchronize(C.stream));
+  CK(cudaMemcpy(f, o.p, bytes, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+static int pointwise(int op, int n, const double* x, const double* y, double* out, double* cm, double* cp) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (n <= 0 || !x || !out) return fail(AMUN_E_BAD_ARGUMENT, "bad arguments");
+  UnitArgs u = unit_args(0, 0, 0);
+  size_t bytes = (size_t)n * C.nv * sizeof(double);
+  DevBuf a, b, o, m, p;
+  CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&o.p, bytes));
+  CK(cudaMemcpy(a.p, x, bytes, cudaMemcpyHostToDevice));
+  if (y) { CK(cudaMalloc(&b.p, bytes)); CK(cudaMemcpy(b.p, y, bytes, cudaMemcpyHostToDevice)); }
+  if (op == 2) { CK(cudaMalloc(&m.p, n * sizeof(double))); CK(cudaMalloc(&p.p, n * sizeof(double))); }
+  cudaError_t e = unit_pointwise(u, op, n, (const double*)a.p, (const double*)b.p, (double*)o.p, (double*)m.p,
+                                 (double*)p.p, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "pointwise");
+  CK(cudaStreamSynchronize(C.stream));
+  CK(cudaMemcpy(out, o.p, bytes, cudaMemcpyDeviceToHost));
+  if (op == 2 && cm) CK(cudaMemcpy(cm, m.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (op == 2 && cp) CK(cudaMemcpy(cp, p.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int amun_gpu_prim2cons(int n, const double* q, double* u) { return pointwise(0, n, q, nullptr, u, nullptr, nullptr); }
+int amun_gpu_cons2prim(int n, const double* u, double* q) { return pointwise(1, n, u, nullptr, q, nullptr, nullptr); }
+int amun_gpu_fluxspeed(int n, const double* q, const double* u, double* f, double* cm, double* cp) {
+  if (!u) return fail(AMUN_E_BAD_ARGUMENT, "null u");
+  return pointwise(2, n, q, u, f, cm, cp);
+}
+
+int amun_gpu_maxspeed(const double* q, double* maxspeed) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (!q || !maxspeed) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
+  const int im = nc + 2 * ng, jm = im, km = nd == 3 ? im : 1;
+  UnitArgs u = unit_args(im, jm, km);
+  size_t bytes = (size_t)im * jm * km * C.nv * sizeof(double);
+  DevBuf a, o;
+  CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&o.p, sizeof(unsigned long long)));
+  CK(cudaMemcpy(a.p, q, bytes, cudaMemcpyHostToDevice));
+  CK(cudaMemset(o.p, 0, sizeof(unsigned long long)));
+  cudaError_t e = unit_maxspeed(u, (const double*)a.p, (unsigned long long*)o.p, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
+  CK(cudaStreamSynchronize(C.stream));
+  unsigned long long bits;
+  CK(cudaMemcpy(&bits, o.p, sizeof(bits), cudaMemcpyDeviceToHost));
+  double v;
+  memcpy(&v, &bits, sizeof(v));
+  *maxspeed = v;
+  return 0;
+}
+
+int amun_gpu_set_cmax(double cmax) {
+  C.host_cmax = cmax;
+  if (C.inited && C.sc) {
+    CK(cudaStreamSynchronize(C.stream));
+    double v[2] = {cmax, cmax * cmax};
+    CK(cudaMemcpy(C.sc, v, sizeof(v), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+int amun_gpu_set_stream(void* stream) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  CK(cudaStreamSynchronize(C.stream));
+  prof_collect();
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  C.stream = stream ? (cudaStream_t)stream : C.own_stream;
+  return 0;
+}
+
+int amun_gpu_profile(int enable, int reset) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  prof_collect();
+  if (reset)
+    for (int k = 0; k < 5; ++k) { C.prof_ms[k] = 0.0; C.prof_n[k] = 0; }
+  C.prof_on = enable != 0;
+  return 0;
+}
+
+int amun_gpu_profile_read(int kind, double* total_ms, long long* launches) {
+  if (kind < 0 || kind > 4) return fail(AMUN_E_BAD_ARGUMENT, "kind must be 0..4");
+  prof_collect();
+  if (total_ms) *total_ms = C.prof_ms[kind];
+  if (launches) *launches = C.prof_n[kind];
+  return 0;
+}
+
+void amun_gpu_finalize(void) {
+  if (C.stream) cudaStreamSynchronize(C.stream);
+  C.marks.clear();
+  for (auto e : C.event_pool) cudaEventDestroy(e);
+  C.event_pool.clear();
+  C.prof_on = false;
+  free_pool();
+  if (C.sc) { cudaFree(C.sc); C.sc = nullptr; }
+  if (C.own_stream) { cudaStreamDestroy(C.own_stream); C.own_stream = nullptr; }
+  C.stream = nullptr;
+  C.inited = false;
+}
+
+const char* amun_gpu_last_error(void) { return C.err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,7 @@
+// Sweep kernels of the fp32 mode for the HD system (NV=5).
+#define AMUN_SWEEP_IMPL
+#include "launch.cuh"
+namespace amun {
+template cudaError_t sweep_nv<float, float, 5>(int, int, int, const SweepArgs<float, float>&, dim3, int, size_t,
+                                              cudaStream_t);
+}

@@ -1,0 +1,170 @@
+// launch.cuh -- host-side launchers of the stage kernels, one explicit
+// instantiation per precision mode (see kernels_*.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "sweep.cuh"
+
+namespace amun {
+
+template <typename R, typename U1T> struct Launch {
+  static cudaError_t sweep(int nv, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
+                           size_t smem, cudaStream_t s);
+  static cudaError_t ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s);
+  static cudaError_t maxspeed(int nv, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
+                              cudaStream_t s);
+  static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
+  static cudaError_t upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
+  static cudaError_t upload_u0(const double* fu, double* u0, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
+  static cudaError_t upload_u1(const double* fu, U1T* u1, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
+  static cudaError_t download_q(const R* q, double* fq, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
+  static cudaError_t download_u0(int nv, const double* u0, const R* q, double* fu, const Geo& g, double gammam1i,
+                                 int b0, int nb, cudaStream_t s);
+  static cudaError_t download_u1(int nv, const U1T* u1, const R* q, double* fu, const Geo& g, double gammam1i,
+                                 int b0, int nb, cudaStream_t s);
+};
+
+inline int grid_for(long long n, int threads, int max_blocks = 148 * 16) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+// sweep dispatch per variable count; instantiated in kernels_<prec>_<eq>.cu so
+// the large solver kernels compile in parallel
+template <typename R, typename U1T, int NV>
+cudaError_t sweep_nv(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
+                     cudaStream_t s);
+
+#ifdef AMUN_SWEEP_IMPL
+template <typename R, typename U1T, int NV, int REC, int RS, int DIR>
+static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
+  auto k = sweep_kernel<NV, REC, RS, DIR, R, U1T>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  k<<<grid, threads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T, int NV, int REC, int RS>
+static cudaError_t go_dir(int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
+  switch (dir) {
+    case 0: return go_sweep<R, U1T, NV, REC, RS, 0>(a, grid, threads, smem, s);
+    case 1: return go_sweep<R, U1T, NV, REC, RS, 1>(a, grid, threads, smem, s);
+    default: return go_sweep<R, U1T, NV, REC, RS, 2>(a, grid, threads, smem, s);
+  }
+}
+
+template <typename R, typename U1T, int NV, int REC>
+static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
+                         cudaStream_t s) {
+  if constexpr (NV == 5) {
+    switch (rs) {
+      case RS_HLLC: return go_dir<R, U1T, NV, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, NV, REC, RS_ROE>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, NV, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+    }
+  } else {
+    switch (rs) {
+      case RS_HLLC: return go_dir<R, U1T, NV, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
+      case RS_HLLD: return go_dir<R, U1T, NV, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, NV, REC, RS_ROE>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, NV, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+    }
+  }
+}
+
+template <typename R, typename U1T, int NV>
+cudaError_t sweep_nv(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
+                     cudaStream_t s) {
+  if (rec == REC_WENO5Z) return go_rs<R, U1T, NV, REC_WENO5Z>(rs, dir, a, grid, threads, smem, s);
+  return go_rs<R, U1T, NV, REC_TVD>(rs, dir, a, grid, threads, smem, s);
+}
+#endif  // AMUN_SWEEP_IMPL
+
+#ifdef AMUN_LAUNCH_IMPL
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::sweep(int nv, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
+                                  int threads, size_t smem, cudaStream_t s) {
+  if (nv == 5) return sweep_nv<R, U1T, 5>(rec, rs, dir, a, grid, threads, smem, s);
+  return sweep_nv<R, U1T, 9>(rec, rs, dir, a, grid, threads, smem, s);
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s) {
+  long long per = g.ndims == 3
+                      ? 2LL * g.ng * g.IM * g.JM + 2LL * g.ng * g.IM * g.nc + 2LL * g.ng * g.nc * g.nc
+                      : 2LL * g.ng * g.IM + 2LL * g.ng * g.nc;
+  int threads = 256;
+  dim3 grid(grid_for(per, threads, 4096), nblocks);
+  ghost_copy_kernel<R><<<grid, threads, 0, s>>>(q, nbr, g, nv, per);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::maxspeed(int nv, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
+                                     cudaStream_t s) {
+  long long n = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1) * nblocks;
+  int threads = 256;
+  int grid = grid_for(n, threads);
+  if (nv == 5) maxspeed_kernel<5, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  else maxspeed_kernel<9, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s) {
+  copy_u0_to_u1_kernel<U1T><<<grid_for(n, 256), 256, 0, s>>>(u0, u1, n);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s) {
+  long long n = (long long)g.IM * g.JM * g.KM * nb;
+  upload_q_kernel<R><<<grid_for(n, 256), 256, 0, s>>>(fq, q, g, nv, b0, nb);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::upload_u0(const double* fu, double* u0, const Geo& g, int nv, int b0, int nb,
+                                      cudaStream_t s) {
+  long long n = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1) * nb;
+  upload_u_kernel<double><<<grid_for(n, 256), 256, 0, s>>>(fu, u0, g, nv, b0, nb);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::upload_u1(const double* fu, U1T* u1, const Geo& g, int nv, int b0, int nb,
+                                      cudaStream_t s) {
+  long long n = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1) * nb;
+  upload_u_kernel<U1T><<<grid_for(n, 256), 256, 0, s>>>(fu, u1, g, nv, b0, nb);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::download_q(const R* q, double* fq, const Geo& g, int nv, int b0, int nb,
+                                       cudaStream_t s) {
+  long long n = (long long)g.IM * g.JM * g.KM * nb;
+  download_q_kernel<R><<<grid_for(n, 256), 256, 0, s>>>(q, fq, g, nv, b0, nb);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::download_u0(int nv, const double* u0, const R* q, double* fu, const Geo& g,
+                                        double gammam1i, int b0, int nb, cudaStream_t s) {
+  long long n = (long long)g.IM * g.JM * g.KM * nb;
+  if (nv == 5) download_u_kernel<5, R, double><<<grid_for(n, 256), 256, 0, s>>>(u0, q, fu, g, gammam1i, b0, nb);
+  else download_u_kernel<9, R, double><<<grid_for(n, 256), 256, 0, s>>>(u0, q, fu, g, gammam1i, b0, nb);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::download_u1(int nv, const U1T* u1, const R* q, double* fu, const Geo& g,
+                                        double gammam1i, int b0, int nb, cudaStream_t s) {
+  long long n = (long long)g.IM * g.JM * g.KM * nb;
+  if (nv == 5) download_u_kernel<5, R, U1T><<<grid_for(n, 256), 256, 0, s>>>(u1, q, fu, g, gammam1i, b0, nb);
+  else download_u_kernel<9, R, U1T><<<grid_for(n, 256), 256, 0, s>>>(u1, q, fu, g, gammam1i, b0, nb);
+  return cudaGetLastError();
+}
+#endif  // AMUN_LAUNCH_IMPL
+
+}  // namespace amun

@@ -1,0 +1,863 @@
+// physics.cuh -- device-side equations, limiters, reconstruction and Riemann
+// solvers of AMUN's adiabatic HD and GLM-MHD systems, written as
+// straight-line register code.  Every function restates the cited Fortran
+// procedure with the same operation order, so the FP64 build (compiled with
+// -fmad=false) reproduces the reference arithmetic bit for bit.
+//
+// Variable order (src/equations.F90:335-485), 0-based here:
+//   HD  (NV=5): dens, velx, vely, velz, pres
+//   MHD (NV=9): dens, velx, vely, velz, magx, magy, magz, bpsi, pres
+// Conserved variables use the same slots (momenta, energy in the pres slot).
+#pragma once
+#include <cstdint>
+
+namespace amun {
+
+enum { LIM_ZERO = 0, LIM_MM = 1, LIM_MC = 2, LIM_SB = 3, LIM_VL = 4, LIM_VA = 5 };
+enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_ROE = 3 };
+enum { REC_TVD = 0, REC_WENO5Z = 1 };
+
+template <int NV> struct Var;
+template <> struct Var<5> {
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, PR = 4, EN = 4;
+  static constexpr int BX = -1, BY = -1, BZ = -1, BP = -1;
+  static constexpr bool MHD = false;
+};
+template <> struct Var<9> {
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
+  static constexpr bool MHD = true;
+};
+
+// Equation and method constants in the working precision R.
+template <typename R> struct Phys {
+  R gamma, gammam1, gammam1i;
+  R eps;      // reconstruction epsilon (WENO-Z, van Albada)
+  R cmax, cmax2;
+  int lim, clim;
+};
+
+template <typename R> __device__ __forceinline__ R d_abs(R x) { return x < R(0) ? -x : (x == R(0) ? R(0) : x); }
+__device__ __forceinline__ double d_fabs(double x) { return fabs(x); }
+__device__ __forceinline__ float d_fabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double d_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double d_copysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float d_copysign(float a, float b) { return copysignf(a, b); }
+template <typename R> __device__ __forceinline__ R d_min(R a, R b) { return a < b ? a : b; }
+template <typename R> __device__ __forceinline__ R d_max(R a, R b) { return a > b ? a : b; }
+
+// Fortran SIGN(x, a) = |x| with the sign of a.
+template <typename R> __device__ __forceinline__ R fsign(R x, R a) { return d_copysign(d_fabs(x), a); }
+
+// TVD limiters, src/interpolations.F90:4684-4877
+template <typename R>
+__device__ __forceinline__ R limiter(int which, R x, R a, R b, R eps) {
+  switch (which) {
+    case LIM_MM:
+      return R(0.5) * (fsign(x, a) + fsign(x, b)) * d_min(d_fabs(a), d_fabs(b));
+    case LIM_MC:
+      return (fsign(x, a) + fsign(x, b)) * d_min(d_min(d_fabs(a), d_fabs(b)), R(0.25) * d_fabs(a + b));
+    case LIM_SB:
+      return R(0.5) * (fsign(x, a) + fsign(x, b)) *
+             d_max(d_min(R(2) * d_fabs(a), d_fabs(b)), d_min(d_fabs(a), R(2) * d_fabs(b)));
+    case LIM_VL: {
+      R c = a * b;
+      if (c > R(0)) c = R(2) * x * c / (a + b); else c = R(0);
+      return c;
+    }
+    case LIM_VA:
+      return x * a * b * (a + b) / d_max(eps, a * a + b * b);
+    default:
+      return R(0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Conversions and physical fluxes
+// ---------------------------------------------------------------------------
+// prim2cons_hd_adi src/equations.F90:1762-1810; prim2cons_mhd_adi 2815-2868
+template <int NV, typename R>
+__device__ __forceinline__ void prim2cons(const R* q, R* u, const Phys<R>& P) {
+  using V = Var<NV>;
+  u[V::DN] = q[V::DN];
+  u[V::VX] = q[V::DN] * q[V::VX];
+  u[V::VY] = q[V::DN] * q[V::VY];
+  u[V::VZ] = q[V::DN] * q[V::VZ];
+  if constexpr (!V::MHD) {
+    R ek = R(0.5) * (u[V::VX] * q[V::VX] + u[V::VY] * q[V::VY] + u[V::VZ] * q[V::VZ]);
+    R ei = P.gammam1i * q[V::PR];
+    u[V::EN] = ei + ek;
+  } else {
+    u[V::BX] = q[V::BX]; u[V::BY] = q[V::BY]; u[V::BZ] = q[V::BZ]; u[V::BP] = q[V::BP];
+    R ei = P.gammam1i * q[V::PR];
+    R ek = R(0.5) * (u[V::VX] * q[V::VX] + u[V::VY] * q[V::VY] + u[V::VZ] * q[V::VZ]);
+    R em = R(0.5) * (q[V::BX] * q[V::BX] + q[V::BY] * q[V::BY] + q[V::BZ] * q[V::BZ]);
+    u[V::EN] = ei + ek + em;
+  }
+}
+
+// cons2prim_hd_adi src/equations.F90:1828-1876; cons2prim_mhd_adi 2886-2939
+template <int NV, typename R>
+__device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
+  using V = Var<NV>;
+  q[V::DN] = u[V::DN];
+  q[V::VX] = u[V::VX] / u[V::DN];
+  q[V::VY] = u[V::VY] / u[V::DN];
+  q[V::VZ] = u[V::VZ] / u[V::DN];
+  if constexpr (!V::MHD) {
+    R ek = R(0.5) * (u[V::VX] * q[V::VX] + u[V::VY] * q[V::VY] + u[V::VZ] * q[V::VZ]);
+    R ei = u[V::EN] - ek;
+    q[V::PR] = P.gammam1 * ei;
+  } else {
+    q[V::BX] = u[V::BX]; q[V::BY] = u[V::BY]; q[V::BZ] = u[V::BZ]; q[V::BP] = u[V::BP];
+    R ek = R(0.5) * (u[V::VX] * q[V::VX] + u[V::VY] * q[V::VY] + u[V::VZ] * q[V::VZ]);
+    R em = R(0.5) * (q[V::BX] * q[V::BX] + q[V::BY] * q[V::BY] + q[V::BZ] * q[V::BZ]);
+    R ei = u[V::EN] - (ek + em);
+    q[V::PR] = P.gammam1 * ei;
+  }
+}
+
+// fluxspeed_hd_adi src/equations.F90:1896-1958;
+// fluxspeed_mhd_adi src/equations.F90:2959-3045
+template <int NV, bool SPEEDS, typename R>
+__device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R& cp, const Phys<R>& P) {
+  using V = Var<NV>;
+  if constexpr (!V::MHD) {
+    f[V::DN] = u[V::VX];
+    f[V::VX] = q[V::VX] * u[V::VX];
+    f[V::VY] = q[V::VX] * u[V::VY];
+    f[V::VZ] = q[V::VX] * u[V::VZ];
+    f[V::VX] = f[V::VX] + q[V::PR];
+    f[V::EN] = q[V::VX] * (u[V::EN] + q[V::PR]);
+    if constexpr (SPEEDS) {
+      R cs = d_sqrt(P.gamma * q[V::PR] / q[V::DN]);
+      cm = q[V::VX] - cs;
+      cp = q[V::VX] + cs;
+    }
+  } else {
+    R bx2 = q[V::BX] * q[V::BX];
+    R by2 = q[V::BY] * q[V::BY];
+    R bz2 = q[V::BZ] * q[V::BZ];
+    R bb = bx2 + by2 + bz2;
+    R vb = q[V::VX] * q[V::BX] + q[V::VY] * q[V::BY] + q[V::VZ] * q[V::BZ];
+    R pt = q[V::PR] + R(0.5) * bb;
+    f[V::DN] = u[V::VX];
+    f[V::VX] = q[V::VX] * u[V::VX] - bx2;
+    f[V::VY] = q[V::VX] * u[V::VY] - q[V::BX] * q[V::BY];
+    f[V::VZ] = q[V::VX] * u[V::VZ] - q[V::BX] * q[V::BZ];
+    f[V::VX] = f[V::VX] + pt;
+    f[V::BX] = q[V::BP];
+    f[V::BY] = q[V::VX] * q[V::BY] - q[V::BX] * q[V::VY];
+    f[V::BZ] = q[V::VX] * q[V::BZ] - q[V::BX] * q[V::VZ];
+    f[V::BP] = P.cmax2 * q[V::BX];
+    f[V::EN] = q[V::VX] * (u[V::EN] + pt) - q[V::BX] * vb;
+    if constexpr (SPEEDS) {
+      R fa = P.gamma * q[V::PR];
+      R fb = fa + bb;
+      R fc = fb * fb - R(4) * fa * bx2;
+      R cf;
+      if (fc > R(0)) cf = d_sqrt(R(0.5) * (fb + d_sqrt(fc)) / q[V::DN]);
+      else cf = d_sqrt(R(0.5) * fb / q[V::DN]);
+      cm = q[V::VX] - cf;
+      cp = q[V::VX] + cf;
+    }
+  }
+}
+
+// maxspeed_hd_adi src/equations.F90:1974-2044 / maxspeed_mhd_adi 3060-3131,
+// the per-cell term |v| + c
+template <int NV, typename R>
+__device__ __forceinline__ double cell_speed(const R* q, double gamma) {
+  using V = Var<NV>;
+  double vx = q[V::VX], vy = q[V::VY], vz = q[V::VZ];
+  double vv = vx * vx + vy * vy + vz * vz;
+  double v = sqrt(vv);
+  double c;
+  if constexpr (!V::MHD) {
+    c = sqrt(gamma * (double)q[V::PR] / (double)q[V::DN]);
+  } else {
+    double bx = q[V::BX], by = q[V::BY], bz = q[V::BZ];
+    double bb = bx * bx + by * by + bz * bz;
+    c = sqrt((gamma * (double)q[V::PR] + bb) / (double)q[V::DN]);
+  }
+  return v + c;
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction of one cell's two faces along one direction.
+// fR = state at the cell's right face (the reference's fl(i), left state of
+// interface i+1/2), fL = state at the cell's left face (fr(i-1), right state
+// of interface i-1/2).
+// ---------------------------------------------------------------------------
+// reconstruct_weno5z src/interpolations.F90:1937-2083, main-loop body for
+// cell i with stencil f(i-2..i+2) given as a,b,c,d,e.
+template <typename R>
+__device__ __forceinline__ void weno5z_faces(R fm2, R fm1, R f0, R fp1, R fp2, R eps, R& fR, R& fL) {
+  const R c1 = R(13.0 / 12.0), c2 = R(0.25);
+  const R dl = R(0.1), dc = R(0.6), dr = R(0.3);
+  const R a11 = R(2.0 / 6.0), a12 = R(-7.0 / 6.0), a13 = R(11.0 / 6.0);
+  const R a21 = R(-1.0 / 6.0), a22 = R(5.0 / 6.0), a23 = R(2.0 / 6.0);
+  const R a31 = R(2.0 / 6.0), a32 = R(5.0 / 6.0), a33 = R(-1.0 / 6.0);
+  // dfm(i-1), dfm(i) = dfp(i-1), dfp(i), dfp(i+1)
+  R dm1 = fm1 - fm2;
+  R d0m = f0 - fm1;
+  R d0p = fp1 - f0;
+  R dp1 = fp2 - fp1;
+  R t;
+  t = d0m - dm1; R df2m = c1 * (t * t);   // df2(i-1): dfp(i-1) - dfm(i-1)
+  t = d0p - d0m; R df20 = c1 * (t * t);   // df2(i)
+  t = dp1 - d0p; R df2p = c1 * (t * t);   // df2(i+1)
+  t = R(3) * d0m - dm1; R bl = df2m + c2 * (t * t);
+  t = d0p + d0m;        R bc = df20 + c2 * (t * t);
+  t = R(3) * d0p - dp1; R br = df2p + c2 * (t * t);
+  R tt = d_fabs(br - bl);
+  R al = R(1) + tt / (bl + eps);
+  R ac = R(1) + tt / (bc + eps);
+  R ar = R(1) + tt / (br + eps);
+  R wl = dl * al, wc = dc * ac, wr = dr * ar;
+  R ww = (wl + wr) + wc;
+  wl = wl / ww; wr = wr / ww; wc = R(1) - (wl + wr);
+  R ql = a11 * fm2 + a12 * fm1 + a13 * f0;
+  R qc = a21 * fm1 + a22 * f0 + a23 * fp1;
+  R qr = a31 * f0 + a32 * fp1 + a33 * fp2;
+  fR = (wl * ql + wr * qr) + wc * qc;
+  wl = dl * ar; wc = dc * ac; wr = dr * al;
+  ww = (wl + wr) + wc;
+  wl = wl / ww; wr = wr / ww; wc = R(1) - (wl + wr);
+  ql = a11 * fp2 + a12 * fp1 + a13 * f0;
+  qc = a21 * fp1 + a22 * f0 + a23 * fm1;
+  qr = a31 * f0 + a32 * fm1 + a33 * fm2;
+  fL = (wl * ql + wr * qr) + wc * qc;
+}
+
+// clip_extrema src/interpolations.F90:5081-5175 restated per cell: the cell's
+// faces fall back to the limited linear states when its left face leaves
+// [min,max](f(i-1),f(i)) or its right face leaves [min,max](f(i),f(i+1)).
+template <typename R>
+__device__ __forceinline__ void clip_cell(R fm1, R f0, R fp1, int clim, R eps, R& fR, R& fL) {
+  R mnL = d_min(fm1, f0), mxL = d_max(fm1, f0);
+  R mnR = d_min(f0, fp1), mxR = d_max(f0, fp1);
+  if (fL < mnL || fL > mxL || fR < mnR || fR > mxR) {
+    R df = limiter<R>(clim, R(0.5), f0 - fm1, fp1 - f0, eps);
+    fR = f0 + df;
+    fL = f0 - df;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers on rotated primitive states (normal component first).
+// ---------------------------------------------------------------------------
+// GLM averaging of Bx and psi (e.g. src/schemes.F90:3196-3215)
+template <int NV, typename R>
+__device__ __forceinline__ void glm_average(R* ql, R* qr, const Phys<R>& P) {
+  using V = Var<NV>;
+  R bx = R(0.5) * ((qr[V::BX] + ql[V::BX]) - (qr[V::BP] - ql[V::BP]) / P.cmax);
+  R bp = R(0.5) * ((qr[V::BP] + ql[V::BP]) - (qr[V::BX] - ql[V::BX]) * P.cmax);
+  ql[V::BX] = bx; qr[V::BX] = bx; ql[V::BP] = bp; qr[V::BP] = bp;
+}
+
+// esystem_roe_hd_adi src/equations.F90:2075-2180 (l[var*5+wave], r[wave*5+var])
+template <typename R>
+__device__ void esystem_roe_hd(const R* q, R* c, R* l, R* r, const Phys<R>& P) {
+  using V = Var<5>;
+#pragma unroll
+  for (int m = 0; m < 25; ++m) { l[m] = R(0); r[m] = R(0); }
+  auto L = [&](int var, int wave) -> R& { return l[var * 5 + wave]; };
+  auto Rm = [&](int wave, int var) -> R& { return r[wave * 5 + var]; };
+  L(V::VY, 1) = R(1); L(V::VZ, 2) = R(1);
+  Rm(0, V::DN) = R(1); Rm(1, V::VY) = R(1); Rm(2, V::VZ) = R(1); Rm(3, V::DN) = R(1); Rm(4, V::DN) = R(1);
+  R vv = q[V::VX] * q[V::VX] + q[V::VY] * q[V::VY] + q[V::VZ] * q[V::VZ];
+  R vh = R(0.5) * vv;
+  R c2 = P.gammam1 * (q[V::EN] - vh);
+  R na = R(0.5) / c2;
+  R cc = d_sqrt(c2);
+  R vc = q[V::VX] * cc;
+  R ng = na * P.gammam1;
+  R nd = R(2) * ng;
+  R nw = na * vc;
+  R nh = na * P.gammam1 * vh;
+  R nc = na * cc;
+  c[0] = q[V::VX] - cc; c[1] = q[V::VX]; c[2] = q[V::VX]; c[3] = q[V::VX]; c[4] = q[V::VX] + cc;
+  L(V::DN, 0) = nh + nw;
+  L(V::VX, 0) = -ng * q[V::VX] - nc;
+  L(V::VY, 0) = -ng * q[V::VY];
+  L(V::VZ, 0) = -ng * q[V::VZ];
+  L(V::EN, 0) = ng;
+  L(V::DN, 1) = -q[V::VY];
+  L(V::DN, 2) = -q[V::VZ];
+  L(V::DN, 3) = R(1) - ng * vv;
+  L(V::VX, 3) = nd * q[V::VX];
+  L(V::VY, 3) = nd * q[V::VY];
+  L(V::VZ, 3) = nd * q[V::VZ];
+  L(V::EN, 3) = -nd;
+  L(V::DN, 4) = nh - nw;
+  L(V::VX, 4) = -ng * q[V::VX] + nc;
+  L(V::VY, 4) = -ng * q[V::VY];
+  L(V::VZ, 4) = -ng * q[V::VZ];
+  L(V::EN, 4) = ng;
+  Rm(0, V::VX) = q[V::VX] - cc; Rm(0, V::VY) = q[V::VY]; Rm(0, V::VZ) = q[V::VZ]; Rm(0, V::EN) = q[V::EN] - vc;
+  Rm(1, V::EN) = q[V::VY];
+  Rm(2, V::EN) = q[V::VZ];
+  Rm(3, V::VX) = q[V::VX]; Rm(3, V::VY) = q[V::VY]; Rm(3, V::VZ) = q[V::VZ]; Rm(3, V::EN) = vh;
+  Rm(4, V::VX) = q[V::VX] + cc; Rm(4, V::VY) = q[V::VY]; Rm(4, V::VZ) = q[V::VZ]; Rm(4, V::EN) = q[V::EN] + vc;
+}
+
+// esystem_roe_mhd_adi src/equations.F90:3162-3468 (l[var*9+wave], r[wave*9+var]).
+// Returns false when the eigenvectors are not needed (3237-3238).
+template <typename R>
+__device__ bool esystem_roe_mhd(R x, R y, const R* q, R* c, R* l, R* r, const Phys<R>& P) {
+  using V = Var<9>;
+  for (int m = 0; m < 81; ++m) { l[m] = R(0); r[m] = R(0); }
+  auto L = [&](int var, int wave) -> R& { return l[var * 9 + wave]; };
+  auto Rm = [&](int wave, int var) -> R& { return r[wave * 9 + var]; };
+  const R eps = sizeof(R) == 8 ? R(2.220446049250313e-16) : R(1.1920929e-07f);
+  const R gammam1 = P.gammam1, gammam2 = P.gamma - R(2);
+  Rm(3, V::DN) = R(1);
+  R di = R(1) / q[V::DN];
+  R casq = q[V::BX] * q[V::BX] * di;
+  R ca = d_sqrt(casq);
+  R vsq = q[V::VX] * q[V::VX] + q[V::VY] * q[V::VY] + q[V::VZ] * q[V::VZ];
+  R btsq = q[V::BY] * q[V::BY] + q[V::BZ] * q[V::BZ];
+  R bt_starsq = (gammam1 - gammam2 * y) * btsq;
+  R hp = q[V::EN] - (casq + btsq * di);
+  R twid_asq = d_max(eps, (gammam1 * (hp - R(0.5) * vsq) - gammam2 * x));
+  R ct2 = bt_starsq * di;
+  R tsum = casq + ct2 + twid_asq;
+  R tdif = casq + ct2 - twid_asq;
+  R cf2_cs2 = d_sqrt((tdif * tdif + R(4) * twid_asq * ct2));
+  R cfsq = R(0.5) * (tsum + cf2_cs2);
+  R cf = d_sqrt(cfsq);
+  R cssq = twid_asq * casq / cfsq;
+  R cs = d_sqrt(cssq);
+  c[0] = q[V::VX] - cf; c[1] = q[V::VX] - ca; c[2] = q[V::VX] - cs; c[3] = q[V::VX];
+  c[4] = q[V::VX]; c[5] = q[V::VX] + cs; c[6] = q[V::VX] + ca; c[7] = q[V::VX] + cf; c[8] = c[7];
+  if (c[0] >= R(0)) return false;
+  if (c[7] <= R(0)) return false;
+  R bt = d_sqrt(btsq);
+  R bt_star = d_sqrt(bt_starsq);
+  R bet2, bet3;
+  if (bt == R(0)) { bet2 = R(1); bet3 = R(0); }
+  else { bet2 = q[V::BY] / bt; bet3 = q[V::BZ] / bt; }
+  R bet2_star = bet2 / d_sqrt(gammam1 - gammam2 * y);
+  R bet3_star = bet3 / d_sqrt(gammam1 - gammam2 * y);
+  R bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+  R vbet = q[V::VY] * bet2_star + q[V::VZ] * bet3_star;
+  R alpha_f, alpha_s;
+  if ((cfsq - cssq) == R(0)) { alpha_f = R(1); alpha_s = R(0); }
+  else if ((twid_asq - cssq) <= R(0)) { alpha_f = R(0); alpha_s = R(1); }
+  else if ((cfsq - twid_asq) <= R(0)) { alpha_f = R(1); alpha_s = R(0); }
+  else {
+    alpha_f = d_sqrt((twid_asq - cssq) / (cfsq - cssq));
+    alpha_s = d_sqrt((cfsq - twid_asq) / (cfsq - cssq));
+  }
+  R sqrtd = d_sqrt(q[V::DN]);
+  R isqrtd = R(1) / sqrtd;
+  R s = fsign(R(1), q[V::BX]);
+  R twid_a = d_sqrt(twid_asq);
+  R qf = cf * alpha_f * s;
+  R qs = cs * alpha_s * s;
+  R af_prime = twid_a * alpha_f * isqrtd;
+  R as_prime = twid_a * alpha_s * isqrtd;
+  R afpbb = af_prime * bt_star * bet_starsq;
+  R aspbb = as_prime * bt_star * bet_starsq;
+  Rm(0, V::DN) = alpha_f; Rm(2, V::DN) = alpha_s; Rm(5, V::DN) = alpha_s; Rm(7, V::DN) = alpha_f;
+  Rm(0, V::VX) = alpha_f * c[0]; Rm(2, V::VX) = alpha_s * c[2]; Rm(3, V::VX) = q[V::VX];
+  Rm(5, V::VX) = alpha_s * c[5]; Rm(7, V::VX) = alpha_f * c[7];
+  R qa = alpha_f * q[V::VY], qb = alpha_s * q[V::VY], qc = qs * bet2_star, qd = qf * bet2_star;
+  Rm(0, V::VY) = qa + qc; Rm(1, V::VY) = -bet3; Rm(2, V::VY) = qb - qd; Rm(3, V::VY) = q[V::VY];
+  Rm(5, V::VY) = qb + qd; Rm(6, V::VY) = bet3; Rm(7, V::VY) = qa - qc;
+  qa = alpha_f * q[V::VZ]; qb = alpha_s * q[V::VZ]; qc = qs * bet3_star; qd = qf * bet3_star;
+  Rm(0, V::VZ) = qa + qc; Rm(1, V::VZ) = bet2; Rm(2, V::VZ) = qb - qd; Rm(3, V::VZ) = q[V::VZ];
+  Rm(5, V::VZ) = qb + qd; Rm(6, V::VZ) = -bet2; Rm(7, V::VZ) = qa - qc;
+  Rm(0, V::PR) = alpha_f * (hp - q[V::VX] * cf) + qs * vbet + aspbb;
+  Rm(1, V::PR) = -(q[V::VY] * bet3 - q[V::VZ] * bet2);
+  Rm(2, V::PR) = alpha_s * (hp - q[V::VX] * cs) - qf * vbet - afpbb;
+  Rm(3, V::PR) = R(0.5) * vsq + gammam2 * x / gammam1;
+  Rm(5, V::PR) = alpha_s * (hp + q[V::VX] * cs) + qf * vbet - afpbb;
+  Rm(6, V::PR) = -Rm(1, V::PR);
+  Rm(7, V::PR) = alpha_f * (hp + q[V::VX] * cf) - qs * vbet + aspbb;
+  Rm(0, V::BY) = as_prime * bet2_star;
+  Rm(1, V::BY) = -bet3 * s * isqrtd;
+  Rm(2, V::BY) = -af_prime * bet2_star;
+  Rm(5, V::BY) = Rm(2, V::BY); Rm(6, V::BY) = Rm(1, V::BY); Rm(7, V::BY) = Rm(0, V::BY);
+  Rm(0, V::BZ) = as_prime * bet3_star;
+  Rm(1, V::BZ) = bet2 * s * isqrtd;
+  Rm(2, V::BZ) = -af_prime * bet3_star;
+  Rm(5, V::BZ) = Rm(2, V::BZ); Rm(6, V::BZ) = Rm(1, V::BZ); Rm(7, V::BZ) = Rm(0, V::BZ);
+  R norm = R(0.5) / twid_asq;
+  R cff = norm * alpha_f * cf;
+  R css = norm * alpha_s * cs;
+  qf = qf * norm;
+  qs = qs * norm;
+  R af = norm * af_prime * q[V::DN];
+  R as = norm * as_prime * q[V::DN];
+  R afpb = norm * af_prime * bt_star;
+  R aspb = norm * as_prime * bt_star;
+  norm = norm * gammam1;
+  alpha_f = alpha_f * norm;
+  alpha_s = alpha_s * norm;
+  R q2_star = bet2_star / bet_starsq;
+  R q3_star = bet3_star / bet_starsq;
+  R vqstr = (q[V::VY] * q2_star + q[V::VZ] * q3_star);
+  norm = R(2) * norm;
+  L(V::DN, 0) = alpha_f * (vsq - hp) + cff * (cf + q[V::VX]) - qs * vqstr - aspb;
+  L(V::VX, 0) = -alpha_f * q[V::VX] - cff;
+  L(V::VY, 0) = -alpha_f * q[V::VY] + qs * q2_star;
+  L(V::VZ, 0) = -alpha_f * q[V::VZ] + qs * q3_star;
+  L(V::PR, 0) = alpha_f;
+  L(V::BY, 0) = as * q2_star - alpha_f * q[V::BY];
+  L(V::BZ, 0) = as * q3_star - alpha_f * q[V::BZ];
+  L(V::DN, 1) = R(0.5) * (q[V::VY] * bet3 - q[V::VZ] * bet2);
+  L(V::VY, 1) = -R(0.5) * bet3;
+  L(V::VZ, 1) = R(0.5) * bet2;
+  L(V::BY, 1) = -R(0.5) * sqrtd * bet3 * s;
+  L(V::BZ, 1) = R(0.5) * sqrtd * bet2 * s;
+  L(V::DN, 2) = alpha_s * (vsq - hp) + css * (cs + q[V::VX]) + qf * vqstr + afpb;
+  L(V::VX, 2) = -alpha_s * q[V::VX] - css;
+  L(V::VY, 2) = -alpha_s * q[V::VY] - qf * q2_star;
+  L(V::VZ, 2) = -alpha_s * q[V::VZ] - qf * q3_star;
+  L(V::PR, 2) = alpha_s;
+  L(V::BY, 2) = -af * q2_star - alpha_s * q[V::BY];
+  L(V::BZ, 2) = -af * q3_star - alpha_s * q[V::BZ];
+  L(V::DN, 3) = R(1) - norm * (R(0.5) * vsq - gammam2 * x / gammam1);
+  L(V::VX, 3) = norm * q[V::VX];
+  L(V::VY, 3) = norm * q[V::VY];
+  L(V::VZ, 3) = norm * q[V::VZ];
+  L(V::PR, 3) = -norm;
+  L(V::BY, 3) = norm * q[V::BY];
+  L(V::BZ, 3) = norm * q[V::BZ];
+  L(V::DN, 5) = alpha_s * (vsq - hp) + css * (cs - q[V::VX]) - qf * vqstr + afpb;
+  L(V::VX, 5) = -alpha_s * q[V::VX] + css;
+  L(V::VY, 5) = -alpha_s * q[V::VY] + qf * q2_star;
+  L(V::VZ, 5) = -alpha_s * q[V::VZ] + qf * q3_star;
+  L(V::PR, 5) = alpha_s;
+  L(V::BY, 5) = L(V::BY, 2);
+  L(V::BZ, 5) = L(V::BZ, 2);
+  L(V::DN, 6) = -L(V::DN, 1);
+  L(V::VY, 6) = -L(V::VY, 1);
+  L(V::VZ, 6) = -L(V::VZ, 1);
+  L(V::BY, 6) = L(V::BY, 1);
+  L(V::BZ, 6) = L(V::BZ, 1);
+  L(V::DN, 7) = alpha_f * (vsq - hp) + cff * (cf - q[V::VX]) + qs * vqstr - aspb;
+  L(V::VX, 7) = -alpha_f * q[V::VX] + cff;
+  L(V::VY, 7) = -alpha_f * q[V::VY] - qs * q2_star;
+  L(V::VZ, 7) = -alpha_f * q[V::VZ] - qs * q3_star;
+  L(V::PR, 7) = alpha_f;
+  L(V::BY, 7) = L(V::BY, 0);
+  L(V::BZ, 7) = L(V::BZ, 0);
+  return true;
+}
+
+// One interface of the selected solver.  ql/qr are rotated primitive states
+// and are modified (GLM averaging) like the Fortran intent(inout) arrays.
+// riemann_hd_adi_hll  src/schemes.F90:1248-1341
+// riemann_hd_adi_hllc src/schemes.F90:1366-1513
+// riemann_hd_adi_roe  src/schemes.F90:1541-1661
+// riemann_mhd_adi_hll  src/schemes.F90:3163-3274
+// riemann_mhd_adi_hllc src/schemes.F90:3305-3571
+// riemann_mhd_adi_hlld src/schemes.F90:3596-4203
+// riemann_mhd_adi_roe  src/schemes.F90:4230-4410
+template <int NV, int RS, typename R>
+__device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
+  using V = Var<NV>;
+  constexpr int Dn = V::DN, Mx = V::VX, My = V::VY, Mz = V::VZ, En = V::EN;
+  R ul[NV], ur[NV], fl[NV], fr[NV];
+  R clm, clp, crm, crp;
+  if constexpr (V::MHD) glm_average<NV>(ql, qr, P);
+  prim2cons<NV>(ql, ul, P);
+  prim2cons<NV>(qr, ur, P);
+  if constexpr (RS == RS_ROE) {
+    fluxspeed<NV, false>(ql, ul, fl, clm, clp, P);
+    fluxspeed<NV, false>(qr, ur, fr, crm, crp, P);
+    R qi[NV], ci[NV], al[NV], li[NV * NV], ri[NV * NV];
+    R sdl = d_sqrt(ql[Dn]), sdr = d_sqrt(qr[Dn]), sds = sdl + sdr;
+    bool full;
+    if constexpr (!V::MHD) {
+      qi[Dn] = sdl * sdr;
+      qi[Mx] = (sdl * ql[Mx] + sdr * qr[Mx]) / sds;
+      qi[My] = (sdl * ql[My] + sdr * qr[My]) / sds;
+      qi[Mz] = (sdl * ql[Mz] + sdr * qr[Mz]) / sds;
+      qi[En] = ((ul[En] + ql[V::PR]) / sdl + (ur[En] + qr[V::PR]) / sdr) / sds;
+      esystem_roe_hd(qi, ci, li, ri, P);
+      full = true;
+    } else {
+      R pml = R(0.5) * (ql[V::BX] * ql[V::BX] + ql[V::BY] * ql[V::BY] + ql[V::BZ] * ql[V::BZ]);
+      R pmr = R(0.5) * (qr[V::BX] * qr[V::BX] + qr[V::BY] * qr[V::BY] + qr[V::BZ] * qr[V::BZ]);
+      qi[Dn] = sdl * sdr;
+      qi[Mx] = (sdl * ql[Mx] + sdr * qr[Mx]) / sds;
+      qi[My] = (sdl * ql[My] + sdr * qr[My]) / sds;
+      qi[Mz] = (sdl * ql[Mz] + sdr * qr[Mz]) / sds;
+      qi[En] = ((ul[En] + ql[V::PR] + pml) / sdl + (ur[En] + qr[V::PR] + pmr) / sdr) / sds;
+      qi[V::BX] = ql[V::BX];
+      qi[V::BY] = (sdr * ql[V::BY] + sdl * qr[V::BY]) / sds;
+      qi[V::BZ] = (sdr * ql[V::BZ] + sdl * qr[V::BZ]) / sds;
+      qi[V::BP] = ql[V::BP];
+      R t1 = ql[V::BY] - qr[V::BY], t2 = ql[V::BZ] - qr[V::BZ];
+      R xx = R(0.5) * ((t1 * t1) + (t2 * t2)) / (sds * sds);
+      R yy = R(0.5) * (ql[Dn] + qr[Dn]) / qi[Dn];
+      full = esystem_roe_mhd(xx, yy, qi, ci, li, ri, P);
+    }
+    (void)full;
+    if (ci[0] >= R(0)) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = fl[v];
+      return;
+    }
+    if (ci[NV - 1] <= R(0)) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = fr[v];
+      return;
+    }
+    if constexpr (V::MHD) { f[V::BX] = fl[V::BX]; f[V::BP] = fl[V::BP]; }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) al[v] = R(0);
+    for (int p = 0; p < NV; ++p) {
+      R d = ur[p] - ul[p];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) al[v] = al[v] + li[p * NV + v] * d;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if constexpr (V::MHD) { if (v == V::BX || v == V::BP) continue; }
+      f[v] = R(0.5) * (fl[v] + fr[v]);
+    }
+    if (qi[Mx] >= R(0)) {
+      for (int p = 0; p < NV; ++p) {
+        R xx = -R(0.5) * al[p] * d_fabs(ci[p]);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          if constexpr (V::MHD) { if (v == V::BX || v == V::BP) continue; }
+          f[v] = f[v] + xx * ri[p * NV + v];
+        }
+      }
+    } else {
+      for (int p = NV - 1; p >= 0; --p) {
+        R xx = -R(0.5) * al[p] * d_fabs(ci[p]);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          if constexpr (V::MHD) { if (v == V::BX || v == V::BP) continue; }
+          f[v] = f[v] + xx * ri[p * NV + v];
+        }
+      }
+    }
+    return;
+  } else {
+    fluxspeed<NV, true>(ql, ul, fl, clm, clp, P);
+    fluxspeed<NV, true>(qr, ur, fr, crm, crp, P);
+    R sl = d_min(clm, crm), sr = d_max(clp, crp);
+    if (sl >= R(0)) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = fl[v];
+      return;
+    }
+    if (sr <= R(0)) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = fr[v];
+      return;
+    }
+    R srml = sr - sl;
+    R wl[NV], wr[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { wl[v] = sl * ul[v] - fl[v]; wr[v] = sr * ur[v] - fr[v]; }
+    if constexpr (RS == RS_HLL) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+      return;
+    } else if constexpr (!V::MHD) {
+      // HD HLLC
+      R ui[NV];
+      R dn = wr[Dn] - wl[Dn];
+      R sm = (wr[Mx] - wl[Mx]) / dn;
+      R pr = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn;
+      if (sm > R(0)) {
+        R slmm = sl - sm;
+        ui[Dn] = wl[Dn] / slmm;
+        ui[Mx] = ui[Dn] * sm;
+        ui[My] = ui[Dn] * ql[My];
+        ui[Mz] = ui[Dn] * ql[Mz];
+        ui[En] = (wl[En] + sm * pr) / slmm;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+      } else if (sm < R(0)) {
+        R srmm = sr - sm;
+        ui[Dn] = wr[Dn] / srmm;
+        ui[Mx] = ui[Dn] * sm;
+        ui[My] = ui[Dn] * qr[My];
+        ui[Mz] = ui[Dn] * qr[Mz];
+        ui[En] = (wr[En] + sm * pr) / srmm;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        f[Dn] = R(0); f[Mx] = -wl[Mx]; f[My] = R(0); f[Mz] = R(0); f[En] = R(0);
+      }
+      return;
+    } else {
+      constexpr int Bx = V::BX, By = V::BY, Bz = V::BZ, Bp = V::BP;
+      R ui[NV];
+      R dn = wr[Dn] - wl[Dn];
+      R sm = (wr[Mx] - wl[Mx]) / dn;
+      if constexpr (RS == RS_HLLC) {
+        R bx = ql[Bx];
+        R b2 = ql[Bx] * qr[Bx];
+        if (b2 > R(0)) {
+          R pt = R(0.5) * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx])) + b2;
+          R vy = (wr[My] - wl[My]) / dn;
+          R vz = (wr[Mz] - wl[Mz]) / dn;
+          R by = (wr[By] - wl[By]) / srml;
+          R bz = (wr[Bz] - wl[Bz]) / srml;
+          R vb = sm * bx + vy * by + vz * bz;
+          if (sm > R(0)) {
+            R slmm = sl - sm;
+            ui[Dn] = wl[Dn] / slmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * vy; ui[Mz] = ui[Dn] * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ql[Bp];
+            ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+          } else if (sm < R(0)) {
+            R srmm = sr - sm;
+            ui[Dn] = wr[Dn] / srmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * vy; ui[Mz] = ui[Dn] * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = qr[Bp];
+            ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+          }
+        } else {
+          R pt = R(0.5) * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx]));
+          if (sm > R(0)) {
+            R slmm = sl - sm;
+            ui[Dn] = wl[Dn] / slmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * ql[My]; ui[Mz] = ui[Dn] * ql[Mz];
+            ui[Bx] = R(0); ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm; ui[Bp] = ql[Bp];
+            ui[En] = (wl[En] + sm * pt) / slmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+          } else if (sm < R(0)) {
+            R srmm = sr - sm;
+            ui[Dn] = wr[Dn] / srmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * qr[My]; ui[Mz] = ui[Dn] * qr[Mz];
+            ui[Bx] = R(0); ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm; ui[Bp] = qr[Bp];
+            ui[En] = (wr[En] + sm * pt) / srmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+          } else {
+            f[Dn] = R(0); f[Mx] = -R(0.5) * (wl[Mx] + wr[Mx]); f[My] = R(0); f[Mz] = R(0);
+            f[Bx] = fl[Bx]; f[By] = R(0); f[Bz] = R(0); f[Bp] = fl[Bp]; f[En] = R(0);
+          }
+        }
+        return;
+      } else {
+        // MHD HLLD
+        R slmm = sl - sm, srmm = sr - sm;
+        R dnl = wl[Dn] / slmm, dnr = wr[Dn] / srmm;
+        R bx = ql[Bx];
+        R b2 = ql[Bx] * qr[Bx];
+        R pt = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn + b2;
+        R vy, vz, by, bz, vb, dvl = R(0), dvr = R(0);
+        auto outer_left = [&]() {
+          vy = (slmm * wl[My] - bx * wl[By]) / dvl;
+          vz = (slmm * wl[Mz] - bx * wl[Bz]) / dvl;
+          by = (wl[Dn] * wl[By] - bx * wl[My]) / dvl;
+          bz = (wl[Dn] * wl[Bz] - bx * wl[Mz]) / dvl;
+          vb = sm * bx + vy * by + vz * bz;
+          ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+          ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+          ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+        };
+        auto outer_right = [&]() {
+          vy = (srmm * wr[My] - bx * wr[By]) / dvr;
+          vz = (srmm * wr[Mz] - bx * wr[Bz]) / dvr;
+          by = (wr[Dn] * wr[By] - bx * wr[My]) / dvr;
+          bz = (wr[Dn] * wr[Bz] - bx * wr[Mz]) / dvr;
+          vb = sm * bx + vy * by + vz * bz;
+          ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+          ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+          ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+        };
+        if (b2 > R(1.0e-08) * d_max(dnl * (sl * sl), dnr * (sr * sr))) {
+          R cal = d_sqrt(b2 / dnl), car = d_sqrt(b2 / dnr);
+          R sml = sm - cal, smr = sm + car;
+          dvl = slmm * wl[Dn] - b2;
+          dvr = srmm * wr[Dn] - b2;
+          if (dvl > R(0) && dvr > R(0)) {
+            if (sml >= R(0)) {
+              outer_left();
+#pragma unroll
+              for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+            } else if (smr <= R(0)) {
+              outer_right();
+#pragma unroll
+              for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+            } else {
+              R wcl[NV], wcr[NV];
+              outer_left();
+#pragma unroll
+              for (int v = 0; v < NV; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+              outer_right();
+#pragma unroll
+              for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+              R dv = car * dnr + cal * dnl;
+              vy = (wcr[My] - wcl[My]) / dv;
+              vz = (wcr[Mz] - wcl[Mz]) / dv;
+              dv = car + cal;
+              by = (wcr[By] - wcl[By]) / dv;
+              bz = (wcr[Bz] - wcl[Bz]) / dv;
+              vb = sm * bx + vy * by + vz * bz;
+              if (sm > R(0)) {
+                ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+                ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+                ui[En] = -(wcl[En] + sm * pt - bx * vb) / cal;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) f[v] = sml * ui[v] - wcl[v];
+              } else if (sm < R(0)) {
+                ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+                ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+                ui[En] = (wcr[En] + sm * pt - bx * vb) / car;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) f[v] = smr * ui[v] - wcr[v];
+              } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) f[v] = (sml * wcr[v] - smr * wcl[v]) / (smr - sml);
+              }
+            }
+          } else {
+            if (dvl > R(0)) {
+              outer_left();
+              if (sml >= R(0)) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+              } else {
+                R wcl[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+                R dv = srmm * dnr + cal * dnl;
+                vy = (wr[My] - wcl[My]) / dv;
+                vz = (wr[Mz] - wcl[Mz]) / dv;
+                dv = sr - sml;
+                by = (wr[By] - wcl[By]) / dv;
+                bz = (wr[Bz] - wcl[Bz]) / dv;
+                vb = sm * bx + vy * by + vz * bz;
+                ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+                ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+                ui[En] = -(wcl[En] + sm * pt - bx * vb) / cal;
+                if (sm >= R(0)) {
+#pragma unroll
+                  for (int v = 0; v < NV; ++v) f[v] = sml * ui[v] - wcl[v];
+                } else {
+#pragma unroll
+                  for (int v = 0; v < NV; ++v) {
+                    R wcr = (sm - sml) * ui[v] + wcl[v];
+                    f[v] = (sm * wr[v] - sr * wcr) / srmm;
+                  }
+                }
+              }
+            } else if (dvr > R(0)) {
+              outer_right();
+              if (smr <= R(0)) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+              } else {
+                R wcr[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+                R dv = slmm * dnl - car * dnr;
+                vy = (wl[My] - wcr[My]) / dv;
+                vz = (wl[Mz] - wcr[Mz]) / dv;
+                dv = sl - smr;
+                by = (wl[By] - wcr[By]) / dv;
+                bz = (wl[Bz] - wcr[Bz]) / dv;
+                vb = sm * bx + vy * by + vz * bz;
+                ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+                ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+                ui[En] = (wcr[En] + sm * pt - bx * vb) / car;
+                if (sm <= R(0)) {
+#pragma unroll
+                  for (int v = 0; v < NV; ++v) f[v] = smr * ui[v] - wcr[v];
+                } else {
+#pragma unroll
+                  for (int v = 0; v < NV; ++v) {
+                    R wcl = (sm - smr) * ui[v] + wcr[v];
+                    f[v] = (sm * wl[v] - sl * wcl) / slmm;
+                  }
+                }
+              }
+            } else {
+#pragma unroll
+              for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+            }
+          }
+        } else if (b2 > R(0)) {
+          vy = (wr[My] - wl[My]) / dn;
+          vz = (wr[Mz] - wl[Mz]) / dn;
+          by = (wr[By] - wl[By]) / srml;
+          bz = (wr[Bz] - wl[Bz]) / srml;
+          vb = sm * bx + vy * by + vz * bz;
+          if (sm > R(0)) {
+            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+            ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+          } else if (sm < R(0)) {
+            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+            ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+          }
+        } else {
+          if (sm > R(0)) {
+            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = wl[My] / slmm; ui[Mz] = wl[Mz] / slmm;
+            ui[Bx] = R(0); ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm; ui[Bp] = ul[Bp];
+            ui[En] = (wl[En] + sm * pt) / slmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+          } else if (sm < R(0)) {
+            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = wr[My] / srmm; ui[Mz] = wr[Mz] / srmm;
+            ui[Bx] = R(0); ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm; ui[Bp] = ur[Bp];
+            ui[En] = (wr[En] + sm * pt) / srmm;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+          }
+        }
+        return;
+      }
+    }
+  }
+}
+
+// Component rotation for direction DIR (src/schemes.F90:1147-1211): the
+// solver sees (normal, t1, t2) = x:(x,y,z) y:(y,z,x) z:(z,x,y).
+template <int DIR> struct Rot;
+template <> struct Rot<0> { static constexpr int p0 = 0, p1 = 1, p2 = 2; };
+template <> struct Rot<1> { static constexpr int p0 = 1, p1 = 2, p2 = 0; };
+template <> struct Rot<2> { static constexpr int p0 = 2, p1 = 0, p2 = 1; };
+
+template <int NV, int DIR, typename R>
+__device__ __forceinline__ void rotate(const R* in, R* out) {
+  using V = Var<NV>; using T = Rot<DIR>;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] = in[v];
+  out[V::VX + 0] = in[V::VX + T::p0]; out[V::VX + 1] = in[V::VX + T::p1]; out[V::VX + 2] = in[V::VX + T::p2];
+  if constexpr (V::MHD) {
+    out[V::BX + 0] = in[V::BX + T::p0]; out[V::BX + 1] = in[V::BX + T::p1]; out[V::BX + 2] = in[V::BX + T::p2];
+  }
+}
+template <int NV, int DIR, typename R>
+__device__ __forceinline__ void unrotate(const R* in, R* out) {
+  using V = Var<NV>; using T = Rot<DIR>;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] = in[v];
+  out[V::VX + T::p0] = in[V::VX + 0]; out[V::VX + T::p1] = in[V::VX + 1]; out[V::VX + T::p2] = in[V::VX + 2];
+  if constexpr (V::MHD) {
+    out[V::BX + T::p0] = in[V::BX + 0]; out[V::BX + T::p1] = in[V::BX + 1]; out[V::BX + T::p2] = in[V::BX + 2];
+  }
+}
+
+}  // namespace amun

@@ -1,0 +1,464 @@
+// sweep.cuh -- the fused per-direction stage kernel and the small kernels
+// around it (ghost fill, CFL reduction and time step, layout transposes).
+//
+// One sweep kernel per direction d stages a tile of primitive states plus its
+// stencil halo in shared memory and runs, per tile:
+//   load  -> per-cell face reconstruction (TVD / WENO-Z) -> per-interface
+//   Riemann solve -> flux difference accumulated into the increment du.
+// The sweep of the last direction also applies the SSPRK stage combination
+// of the conserved state, the GLM psi decay of the final stage, cons2prim of
+// the new state and the per-cell max speed of the CFL condition.
+//
+// Reference path (per stage): update_fluxes src/evolution.F90:1807-1881 ->
+// update_flux_{hd,mhd}_adi src/schemes.F90:1080-1223, 2970-3138 ->
+// update_increment src/evolution.F90:1898-1977 -> stage combination e.g.
+// src/evolution.F90:681-704, 729-753 -> update_variables 1994-2094.
+//
+// HBM layout (per block b, variable v, padded cell (i,j,k)):
+//   Q  [b][v][k][j][i]   primitive with ng ghost layers (IM = nc + 2 ng)
+//   U0 [b][v][k][j][i]   interior only, FP64 (U^n / U^{n+1})
+//   U1 [b][v][k][j][i]   interior only, stage state (FP64, or FP32 in bulk)
+//   du [b][v][k][j][i]   interior only, increment in the working precision
+#pragma once
+#include "physics.cuh"
+
+namespace amun {
+
+struct Geo {
+  int nc, ng, ndims;
+  int IM, JM, KM;             // padded extents (KM == 1 in 2D)
+  long long qvs, qbs;         // padded variable / block strides
+  long long uvs, ubs;         // interior variable / block strides
+};
+
+// Device-resident scalars of the time step (new_time_step state).
+struct DevScalars {
+  double cmax, cmax2, dt, dtn, time;
+  unsigned long long ms_bits;      // max |v|+c of the current state, as bits
+  unsigned long long nonpositive;  // positive variable not positive (TVD)
+  long long step;
+};
+
+// One SSPRK stage combination.  ds = dscoef * dt.
+//   form 0: out = A + ds du
+//   form 1: out = (ca A + cb B) + ds du
+//   form 2: out = 0.5 ((A + B) + ds du)
+//   form 3: out = ca A + cb (B + ds du)
+// A/B/out select the state arrays: 0 = U0, 1 = U1.
+struct StageDesc {
+  int form, a_src, b_src, out_dst, final_stage;
+  double ca, cb, dscoef;
+};
+
+struct MethodConst {
+  double gamma, gammam1, gammam1i, eps, decay;
+  int lim, clim, positivity, clip;
+};
+
+template <typename R, typename U1T> struct SweepArgs {
+  const R* q;          // stage input primitives (padded)
+  R* du;               // increment (interior)
+  double* u0;          // U0 (interior, FP64)
+  U1T* u1;             // U1 (interior)
+  R* qout;             // stage output primitives (padded)
+  DevScalars* sc;
+  const double* binv;  // per block 1/dx, 1/dy, 1/dz
+  Geo g;
+  MethodConst m;
+  StageDesc st;
+  int LP, LW;          // tile: cells along the sweep, lanes across it
+  int first, last;
+};
+
+template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
+
+// block-wide max of non-negative doubles, then one atomicMax per CTA on the
+// ordered bit image (non-negative IEEE doubles order like their bits)
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long* target) {
+  __shared__ double red[32];
+  unsigned mask = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
+    if (lane == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+template <int NV, int REC, int RS, int DIR, typename R, typename U1T>
+__global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  using V = Var<NV>;
+  constexpr int RR = (REC == REC_WENO5Z) ? 2 : 1;
+  const Geo& g = a.g;
+  const int LP = a.LP, LW = a.LW;
+  const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
+  R* Qs = sm;
+  R* FLs = Qs + (size_t)NV * NPQ * LW;
+  R* FRs = FLs + (size_t)NV * NPF * LW;
+  R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
+
+  const int nc = g.nc, ng = g.ng;
+  const int b = blockIdx.y;
+  int tile = blockIdx.x;
+  const int ntp = nc / LP, ntl = nc / LW;
+  const int tp = tile % ntp; tile /= ntp;
+  const int tl = tile % ntl; tile /= ntl;
+  const int th = tile;
+  const int p0 = ng + tp * LP, l0 = ng + tl * LW;
+  const int t0 = (g.ndims == 3) ? ng + th : 0;
+  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
+  const long long sP = DIR == 0 ? sX : (DIR == 1 ? sY : sZ);
+  const long long sL = DIR == 0 ? sY : sX;
+  const long long sT = DIR == 2 ? sY : sZ;
+  const long long iP = DIR == 0 ? 1 : (DIR == 1 ? nc : (long long)nc * nc);
+  const long long iL = DIR == 0 ? nc : 1;
+  const long long iT = DIR == 2 ? nc : (long long)nc * nc;
+  const R* qb = a.q + (long long)b * g.qbs;
+
+  auto sidx = [&](int v, int pp, int ll, int NP) -> int {
+    return DIR == 0 ? (v * LW + ll) * NP + pp : (v * NP + pp) * LW + ll;
+  };
+  auto decode = [&](int t, int NP, int& pp, int& ll) {
+    if (DIR == 0) { ll = t / NP; pp = t - ll * NP; }
+    else { pp = t / LW; ll = t - pp * LW; }
+  };
+
+  // ---- load the tile and its halo --------------------------------------------
+  for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
+    int pp, ll; decode(t, NPQ, pp, ll);
+    long long c = (long long)(p0 - RR - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Qs[sidx(v, pp, ll, NPQ)] = ld_ro(qb + c + v * g.qvs);
+  }
+  __syncthreads();
+
+  // ---- reconstruct both faces of cells p0-1 .. p0+LP ---------------------------
+  {
+    const R eps = R(a.m.eps);
+    for (int t = threadIdx.x; t < NPF * LW; t += blockDim.x) {
+      int pp, ll; decode(t, NPF, pp, ll);
+      const int cq = pp + RR;  // index of this cell in Qs
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        R fR, fL;
+        const R f0 = Qs[sidx(v, cq, ll, NPQ)];
+        const bool positive = (v == V::DN || v == V::PR);
+        if constexpr (REC == REC_WENO5Z) {
+          // interfaces_dir src/interpolations.F90:867-959 -> reconstruct
+          // 1343-1381 -> reconstruct_weno5z (main loop, 1997-2066)
+          const R fm2 = Qs[sidx(v, cq - 2, ll, NPQ)], fm1 = Qs[sidx(v, cq - 1, ll, NPQ)];
+          const R fp1 = Qs[sidx(v, cq + 1, ll, NPQ)], fp2 = Qs[sidx(v, cq + 2, ll, NPQ)];
+          weno5z_faces(fm2, fm1, f0, fp1, fp2, eps, fR, fL);
+          if (a.m.clip) clip_cell(fm1, f0, fp1, a.m.clim, eps, fR, fL);
+          // fix_positivity src/interpolations.F90:4987-5062 per cell
+          if (positive && a.m.positivity && (fR <= R(0) || fL <= R(0))) { fR = f0; fL = f0; }
+        } else {
+          // interfaces_tvd src/interpolations.F90:729-848
+          const R fm1 = Qs[sidx(v, cq - 1, ll, NPQ)], fp1 = Qs[sidx(v, cq + 1, ll, NPQ)];
+          R dqd;
+          if (!positive) {
+            dqd = limiter<R>(a.m.lim, R(0.5), f0 - fm1, fp1 - f0, eps);
+          } else {
+            // multi-dimensional slopes, halved together while q <= sum|dq|
+            const long long c = (long long)(p0 - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+            const R* qv = qb + (long long)v * g.qvs + c;
+            R dq[3];
+            dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sX), ld_ro(qv + sX) - f0, eps);
+            dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sY), ld_ro(qv + sY) - f0, eps);
+            dq[2] = R(0);
+            if (g.ndims == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sZ), ld_ro(qv + sZ) - f0, eps);
+            if (f0 > R(0)) {
+              for (int it = 0; it < 4096; ++it) {
+                R s = d_fabs(dq[0]) + d_fabs(dq[1]);
+                if (g.ndims == 3) s = s + d_fabs(dq[2]);
+                if (!(f0 <= s)) break;
+                dq[0] = R(0.5) * dq[0]; dq[1] = R(0.5) * dq[1]; dq[2] = R(0.5) * dq[2];
+              }
+            } else {
+              dq[0] = dq[1] = dq[2] = R(0);
+              // counted once per cell and stage: in the x sweep, tile cells only
+              if (DIR == 0 && pp >= 1 && pp <= LP) atomicAdd(&a.sc->nonpositive, 1ull);
+            }
+            dqd = dq[DIR];
+          }
+          fR = f0 + dqd;
+          fL = f0 - dqd;
+        }
+        FLs[sidx(v, pp, ll, NPF)] = fR;
+        FRs[sidx(v, pp, ll, NPF)] = fL;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- Riemann problems at interfaces (p0-1)+1/2 .. (p0+LP-1)+1/2 -------------
+  {
+    Phys<R> P;
+    P.gamma = R(a.m.gamma); P.gammam1 = R(a.m.gammam1); P.gammam1i = R(a.m.gammam1i);
+    P.eps = R(a.m.eps); P.cmax = R(a.sc->cmax); P.cmax2 = R(a.sc->cmax2);
+    P.lim = a.m.lim; P.clim = a.m.clim;
+    for (int t = threadIdx.x; t < NPI * LW; t += blockDim.x) {
+      int pp, ll; decode(t, NPI, pp, ll);
+      R ql[NV], qr[NV], tl[NV], tr[NV], f[NV], fo[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) { tl[v] = FLs[sidx(v, pp, ll, NPF)]; tr[v] = FRs[sidx(v, pp + 1, ll, NPF)]; }
+      rotate<NV, DIR>(tl, ql);
+      rotate<NV, DIR>(tr, qr);
+      riemann<NV, RS>(ql, qr, f, P);
+      unrotate<NV, DIR>(f, fo);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Fs[sidx(v, pp, ll, NPI)] = fo[v];
+    }
+  }
+  __syncthreads();
+
+  // ---- flux difference, stage combination -------------------------------------
+  const double* bi = a.binv + 3 * b;
+  const R dsi = R(bi[DIR]);
+  const bool final_stage = a.last && a.st.final_stage;
+  double vmax = 0.0;
+  for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
+    int pp, ll;
+    if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
+    const long long ci = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP + (long long)(l0 - ng + ll) * iL +
+                         (long long)(g.ndims == 3 ? th : 0) * iT;
+    R dloc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      R d = Fs[sidx(v, pp + 1, ll, NPI)] - Fs[sidx(v, pp, ll, NPI)];
+      if (a.first) dloc[v] = -(dsi * d);
+      else dloc[v] = a.du[ci + v * g.uvs] - dsi * d;
+    }
+    if (!a.last) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a.du[ci + v * g.uvs] = dloc[v];
+      continue;
+    }
+    // stage combination (all cells updated by this stage are interior)
+    const double dt = a.sc->dt;
+    const double ds = a.st.dscoef * dt;
+    double un[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const long long o = ci + v * g.uvs;
+      double A = a.st.a_src == 0 ? a.u0[o] : (double)a.u1[o];
+      double dd = (double)dloc[v];
+      double r;
+      switch (a.st.form) {
+        case 0: r = A + ds * dd; break;
+        case 1: {
+          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
+          r = (a.st.ca * A + a.st.cb * B) + ds * dd;
+          break;
+        }
+        case 2: {
+          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
+          r = 0.5 * ((A + B) + ds * dd);
+          break;
+        }
+        default: {
+          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
+          r = a.st.ca * A + a.st.cb * (B + ds * dd);
+          break;
+        }
+      }
+      if constexpr (V::MHD) {
+        if (a.st.final_stage && v == V::BP) r = a.m.decay * r;
+      }
+      if (a.st.out_dst == 0) { a.u0[o] = r; un[v] = r; }
+      else { U1T s = (U1T)r; a.u1[o] = s; un[v] = (double)s; }
+    }
+    // cons2prim of the new state (update_primitive_variables,
+    // src/equations.F90:1088-1148)
+    Phys<double> Pd;
+    Pd.gamma = a.m.gamma; Pd.gammam1 = a.m.gammam1; Pd.gammam1i = a.m.gammam1i;
+    double qn[NV];
+    cons2prim<NV>(un, qn, Pd);
+    const long long co = (long long)b * g.qbs + (long long)(p0 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+    R qs[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { qs[v] = (R)qn[v]; a.qout[co + v * g.qvs] = qs[v]; }
+    if (final_stage) vmax = fmax(vmax, cell_speed<NV>(qs, a.m.gamma));
+  }
+  if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
+}
+
+// ---------------------------------------------------------------------------
+// Ghost fill from same-level neighbours (face / edge / corner copy of
+// boundaries_{face,edge,corner}_copy, src/boundaries.F90:1273, 2447, 3867).
+// nbr[27*b + (ox+1) + 3 (oy+1) + 9 (oz+1)] is the neighbour block in that
+// direction.  Ghost cells are enumerated as z-slabs, then y-slabs, then x.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void ghost_copy_kernel(R* q, const int* nbr, Geo g, int nv, long long nghost_per_block) {
+  const int b = blockIdx.y;
+  const int nc = g.nc, ng = g.ng, IM = g.IM, JM = g.JM;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nghost_per_block;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    long long r = t;
+    if (g.ndims == 3) {
+      long long zs = 2LL * ng * IM * JM;
+      if (r < zs) {
+        int kk = (int)(r / ((long long)IM * JM)); long long rem = r - (long long)kk * IM * JM;
+        k = kk < ng ? kk : kk - ng + ng + nc;
+        j = (int)(rem / IM); i = (int)(rem - (long long)j * IM);
+      } else {
+        r -= zs;
+        long long ys = 2LL * ng * IM * nc;
+        if (r < ys) {
+          int kk = (int)(r / (2LL * ng * IM)); long long rem = r - (long long)kk * 2 * ng * IM;
+          k = ng + kk;
+          int jj = (int)(rem / IM); i = (int)(rem - (long long)jj * IM);
+          j = jj < ng ? jj : jj - ng + ng + nc;
+        } else {
+          r -= ys;
+          int row = (int)(r / (2 * ng)); int ii = (int)(r - (long long)row * 2 * ng);
+          k = ng + row / nc; j = ng + row % nc;
+          i = ii < ng ? ii : ii - ng + ng + nc;
+        }
+      }
+    } else {
+      k = 0;
+      long long ys = 2LL * ng * IM;
+      if (r < ys) {
+        int jj = (int)(r / IM); i = (int)(r - (long long)jj * IM);
+        j = jj < ng ? jj : jj - ng + ng + nc;
+      } else {
+        r -= ys;
+        int row = (int)(r / (2 * ng)); int ii = (int)(r - (long long)row * 2 * ng);
+        j = ng + row;
+        i = ii < ng ? ii : ii - ng + ng + nc;
+      }
+    }
+    int ox = i < ng ? -1 : (i >= ng + nc ? 1 : 0);
+    int oy = j < ng ? -1 : (j >= ng + nc ? 1 : 0);
+    int oz = g.ndims == 3 ? (k < ng ? -1 : (k >= ng + nc ? 1 : 0)) : 0;
+    int nb = nbr[27 * b + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+    if (nb < 0) continue;
+    long long dst = (long long)b * g.qbs + ((long long)k * JM + j) * IM + i;
+    long long src = (long long)nb * g.qbs + ((long long)(k - oz * nc) * JM + (j - oy * nc)) * IM + (i - ox * nc);
+    for (int v = 0; v < nv; ++v) q[dst + v * g.qvs] = q[src + v * g.qvs];
+  }
+}
+
+// max over interior cells of |v|+c (maxspeed_*, src/equations.F90:1974,
+// 3060), accumulated into sc->ms_bits
+template <int NV, typename R>
+__global__ void maxspeed_kernel(const R* q, Geo g, double gamma, DevScalars* sc, int nblocks) {
+  const long long ncell = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1);
+  const long long total = ncell * nblocks;
+  double vmax = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long b = t / ncell, c = t - b * ncell;
+    int i = (int)(c % g.nc), j = (int)((c / g.nc) % g.nc), k = (int)(c / ((long long)g.nc * g.nc));
+    long long o = b * g.qbs + ((long long)(g.ndims == 3 ? k + g.ng : 0) * g.JM + (j + g.ng)) * g.IM + (i + g.ng);
+    R qc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = q[o + v * g.qvs];
+    vmax = fmax(vmax, cell_speed<NV>(qc, gamma));
+  }
+  block_max_atomic(vmax, &sc->ms_bits);
+}
+
+// new_time_step src/evolution.F90:379-493 on device: cmax from the max-speed
+// accumulator (then reset for the next reduction), dt from the CFL condition.
+static __global__ void new_time_step_kernel(DevScalars* sc, double cfl, double dx_min, double dtnext, double visc_res) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double eps = 2.2250738585072014e-308;  // tiny(1d0)
+  double ms = __longlong_as_double((long long)sc->ms_bits);
+  double cmax = eps > ms ? eps : ms;
+  sc->cmax = cmax;
+  sc->cmax2 = cmax * cmax;
+  double den = cmax + 2.0 * visc_res / dx_min;
+  sc->dtn = cfl * dx_min / (den > eps ? den : eps);
+  if (dtnext > 0.0) sc->dt = sc->dtn < dtnext ? sc->dtn : dtnext;
+  sc->ms_bits = 0ull;
+}
+
+// the driver's time/step update after advance (src/driver.F90:582-585)
+static __global__ void end_step_kernel(DevScalars* sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) { sc->time = sc->time + sc->dt; sc->step += 1; }
+}
+
+// U1 = U0 (first step of evolve_ssprk2, src/evolution.F90:854-874)
+template <typename U1T>
+__global__ void copy_u0_to_u1_kernel(const double* u0, U1T* u1, long long n) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    u1[t] = (U1T)u0[t];
+}
+
+// Fortran block arrays (nv,im,jm,km) <-> SoA pool.  `fq`/`fu` hold nb
+// consecutive blocks starting at block b0.
+template <typename R>
+__global__ void upload_q_kernel(const double* fq, R* q, Geo g, int nv, int b0, int nb) {
+  const long long cells = (long long)g.IM * g.JM * g.KM;
+  const long long total = cells * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long bb = t / cells, c = t - bb * cells;
+    const double* src = fq + t * nv;
+    R* dst = q + (b0 + bb) * g.qbs + c;
+    for (int v = 0; v < nv; ++v) dst[v * g.qvs] = (R)src[v];
+  }
+}
+template <typename UT>
+__global__ void upload_u_kernel(const double* fu, UT* u, Geo g, int nv, int b0, int nb) {
+  const long long icell = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1);
+  const long long total = icell * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long bb = t / icell, c = t - bb * icell;
+    int i = (int)(c % g.nc), j = (int)((c / g.nc) % g.nc), k = (int)(c / ((long long)g.nc * g.nc));
+    long long pc = ((long long)(g.ndims == 3 ? k + g.ng : 0) * g.JM + (j + g.ng)) * g.IM + (i + g.ng);
+    const double* src = fu + (bb * (long long)g.IM * g.JM * g.KM + pc) * nv;
+    UT* dst = u + (b0 + bb) * g.ubs + c;
+    for (int v = 0; v < nv; ++v) dst[v * g.uvs] = (UT)src[v];
+  }
+}
+template <typename R>
+__global__ void download_q_kernel(const R* q, double* fq, Geo g, int nv, int b0, int nb) {
+  const long long cells = (long long)g.IM * g.JM * g.KM;
+  const long long total = cells * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long bb = t / cells, c = t - bb * cells;
+    const R* src = q + (b0 + bb) * g.qbs + c;
+    double* dst = fq + t * nv;
+    for (int v = 0; v < nv; ++v) dst[v] = (double)src[v * g.qvs];
+  }
+}
+// u (Fortran layout, all cells): interior from the state array, ghosts from
+// prim2cons of the ghost primitives (update_ghost_cells,
+// src/boundaries.F90:6633-6736)
+template <int NV, typename R, typename UT>
+__global__ void download_u_kernel(const UT* u, const R* q, double* fu, Geo g, double gammam1i, int b0, int nb) {
+  const long long cells = (long long)g.IM * g.JM * g.KM;
+  const long long total = cells * nb;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    long long bb = t / cells, c = t - bb * cells;
+    int i = (int)(c % g.IM), j = (int)((c / g.IM) % g.JM), k = (int)(c / ((long long)g.IM * g.JM));
+    bool interior = i >= g.ng && i < g.ng + g.nc && j >= g.ng && j < g.ng + g.nc &&
+                    (g.ndims == 2 || (k >= g.ng && k < g.ng + g.nc));
+    double* dst = fu + t * NV;
+    if (interior) {
+      long long ic = (long long)(i - g.ng) + (long long)g.nc * ((j - g.ng) + (long long)g.nc * (g.ndims == 3 ? k - g.ng : 0));
+      const UT* src = u + (b0 + bb) * g.ubs + ic;
+      for (int v = 0; v < NV; ++v) dst[v] = (double)src[v * g.uvs];
+    } else {
+      double qc[NV], uc[NV];
+      const R* src = q + (b0 + bb) * g.qbs + c;
+      for (int v = 0; v < NV; ++v) qc[v] = (double)src[v * g.qvs];
+      Phys<double> P; P.gammam1i = gammam1i;
+      prim2cons<NV>(qc, uc, P);
+      for (int v = 0; v < NV; ++v) dst[v] = uc[v];
+    }
+  }
+}
+
+}  // namespace amun

@@ -1,0 +1,338 @@
+// unit_fp64.cu -- FP64 stand-ins for the reference's per-procedure
+// interfaces on Fortran-layout arrays: update_flux (one block, including the
+// line-end fallbacks of the reconstruction), riemann, prim2cons, cons2prim,
+// fluxspeed and maxspeed.  Used for per-procedure parity and by callers that
+// keep the reference's own stage loop.  Compiled with -fmad=false.
+#include <cuda_runtime.h>
+#include "physics.cuh"
+#include "unit.h"
+
+namespace amun {
+
+// Layout helpers: q(nv,im,jm,km) and qs(nv, cells, 2, NDIMS) as in
+// reconstruct_interfaces (src/schemes.F90:591-633) but variable fastest.
+struct BlockDims { int nv, ndims, im, jm, km, ng; };
+
+// ---- interfaces_tvd (src/interpolations.F90:729-848) -------------------------
+// pass 1: ghost copy of every variable and direction (758-771)
+__global__ void tvd_ghost_copy(const double* q, double* qs, BlockDims d) {
+  const int ib = d.ng, ie = d.ng + (d.im - 2 * d.ng) - 1;   // 0-based ib..ie
+  const int jb = d.ng, je = d.ng + (d.jm - 2 * d.ng) - 1;
+  const int kb = d.ndims == 3 ? d.ng : 0, ke = d.ndims == 3 ? d.ng + (d.km - 2 * d.ng) - 1 : 0;
+  long long cells = (long long)d.im * d.jm * d.km;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells; c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c % d.im), j = (int)((c / d.im) % d.jm), k = (int)(c / ((long long)d.im * d.jm));
+    bool gh = i <= ib || i >= ie || j <= jb || j >= je;
+    if (d.ndims == 3) gh = gh || k <= kb || k >= ke;
+    if (!gh) continue;
+    for (int s = 0; s < 2 * d.ndims; ++s)
+      for (int v = 0; v < d.nv; ++v) qs[((long long)s * cells + c) * d.nv + v] = q[c * d.nv + v];
+  }
+}
+
+template <int NV>
+__global__ void tvd_box(const double* q, double* qs, BlockDims d, int lim, double eps, unsigned long long* nonpos) {
+  using V = Var<NV>;
+  const int nx = d.im - 2 * d.ng + 2, ny = d.jm - 2 * d.ng + 2, nz = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
+  const long long cells = (long long)d.im * d.jm * d.km;
+  const long long n = (long long)nx * ny * nz;
+  const long long sx = 1, sy = d.im, sz = (long long)d.im * d.jm;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = d.ng - 1 + (int)(t % nx), j = d.ng - 1 + (int)((t / nx) % ny);
+    int k = d.ndims == 3 ? d.ng - 1 + (int)(t / ((long long)nx * ny)) : 0;
+    long long c = i * sx + j * sy + k * sz;
+    for (int v = 0; v < NV; ++v) {
+      const double* qv = q + v;
+      auto Q = [&](long long cc) { return qv[cc * NV]; };
+      double f0 = Q(c);
+      double dq[3] = {0.0, 0.0, 0.0};
+      dq[0] = limiter<double>(lim, 0.5, f0 - Q(c - sx), Q(c + sx) - f0, eps);
+      dq[1] = limiter<double>(lim, 0.5, f0 - Q(c - sy), Q(c + sy) - f0, eps);
+      if (d.ndims == 3) dq[2] = limiter<double>(lim, 0.5, f0 - Q(c - sz), Q(c + sz) - f0, eps);
+      if (v == V::DN || v == V::PR) {
+        if (f0 > 0.0) {
+          for (int it = 0; it < 4096; ++it) {
+            double s = fabs(dq[0]) + fabs(dq[1]);
+            if (d.ndims == 3) s = s + fabs(dq[2]);
+            if (!(f0 <= s)) break;
+            dq[0] = 0.5 * dq[0]; dq[1] = 0.5 * dq[1]; dq[2] = 0.5 * dq[2];
+          }
+        } else {
+          dq[0] = dq[1] = dq[2] = 0.0;
+          atomicAdd(nonpos, 1ull);
+        }
+      }
+      const long long st[3] = {sx, sy, sz};
+      for (int dd = 0; dd < d.ndims; ++dd) {
+        qs[((long long)(2 * dd + 0) * cells + c) * NV + v] = f0 + dq[dd];
+        qs[((long long)(2 * dd + 1) * cells + (c - st[dd])) * NV + v] = f0 - dq[dd];
+      }
+    }
+  }
+}
+
+// ---- interfaces_dir + reconstruct (src/interpolations.F90:867-959,
+// 1343-1381): one thread per (variable, line); the line is reconstructed
+// with reconstruct_weno5z (1937-2083) including its line-end fallbacks, then
+// clip_extrema (5081-5175) and fix_positivity (4987-5062) run sequentially.
+template <int NV>
+__global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int lim, int clim, double eps,
+                          int clip, int positivity, double* scratch) {
+  using V = Var<NV>;
+  const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
+  int a0, a1, n;  // line counts
+  long long stride, s0, s1;
+  const long long sx = 1, sy = d.im, sz = (long long)d.im * d.jm;
+  if (dir == 0) { a0 = nj; a1 = nk; n = d.im; stride = sx; s0 = sy; s1 = sz; }
+  else if (dir == 1) { a0 = ni; a1 = nk; n = d.jm; stride = sy; s0 = sx; s1 = sz; }
+  else { a0 = ni; a1 = nj; n = d.km; stride = sz; s0 = sx; s1 = sy; }
+  const long long cells = (long long)d.im * d.jm * d.km;
+  const long long lines = (long long)a0 * a1 * NV;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < lines; t += (long long)gridDim.x * blockDim.x) {
+    int v = (int)(t % NV);
+    long long l = t / NV;
+    int c0 = (int)(l % a0) + d.ng - 1, c1 = (int)(l / a0) + (d.ndims == 3 || dir == 2 ? d.ng - 1 : 0);
+    if (d.ndims == 2 && dir != 2) c1 = 0;
+    long long base = c0 * s0 + c1 * s1;
+    double* f = scratch + t * 3LL * n;
+    double* fl = f + n;
+    double* fr = fl + n;
+    for (int p = 0; p < n; ++p) f[p] = q[(base + p * stride) * NV + v];
+    // main loop, i = 3 .. n-2 (1-based)
+    for (int i = 2; i <= n - 3; ++i) {
+      double a, b;
+      weno5z_faces<double>(f[i - 2], f[i - 1], f[i], f[i + 1], f[i + 2], eps, a, b);
+      fl[i] = a;
+      fr[i - 1] = b;
+    }
+    // line ends (2069-2079)
+    fl[0] = 0.5 * (f[0] + f[1]);
+    double df = limiter<double>(lim, 0.5, f[1] - f[0], f[2] - f[1], eps);
+    fr[0] = f[1] - df;
+    fl[1] = f[1] + df;
+    int i = n - 2;  // 0-based of Fortran n-1
+    df = limiter<double>(lim, 0.5, f[i] - f[i - 1], f[i + 1] - f[i], eps);
+    fr[i - 1] = f[i] - df;
+    fl[i] = f[i] + df;
+    fr[i] = 0.5 * (f[i] + f[n - 1]);
+    fl[n - 1] = f[n - 1];
+    fr[n - 1] = f[n - 1];
+    if (clip) {
+      for (int ii = 0; ii < n; ++ii) {
+        int im1 = ii > 0 ? ii - 1 : 0, ip1 = ii < n - 1 ? ii + 1 : n - 1;
+        double fmn = d_min(f[ii], f[ip1]), fmx = d_max(f[ii], f[ip1]);
+        if (fl[ii] < fmn || fl[ii] > fmx) {
+          double dd = limiter<double>(clim, 0.5, f[ii] - f[im1], f[ip1] - f[ii], eps);
+          fl[ii] = f[ii] + dd;
+          fr[im1] = f[ii] - dd;
+        }
+        if (fr[ii] < fmn || fr[ii] > fmx) {
+          int ip2 = ii + 2 < n ? ii + 2 : n - 1;
+          double dd = limiter<double>(clim, 0.5, f[ip1] - f[ii], f[ip2] - f[ip1], eps);
+          fl[ip1] = f[ip1] + dd;
+          fr[ii] = f[ip1] - dd;
+        }
+      }
+    }
+    if (positivity && (v == V::DN || v == V::PR)) {
+      for (int ii = 0; ii < n; ++ii) {
+        if (fl[ii] <= 0.0) { int im1 = ii > 0 ? ii - 1 : 0; fl[ii] = f[ii]; fr[im1] = f[ii]; }
+        if (fr[ii] <= 0.0) { int ip1 = ii < n - 1 ? ii + 1 : n - 1; fl[ip1] = f[ip1]; fr[ii] = f[ip1]; }
+      }
+    }
+    for (int p = 0; p < n; ++p) {
+      long long cc = base + p * stride;
+      qs[((long long)(2 * dir + 0) * cells + cc) * NV + v] = fl[p];
+      qs[((long long)(2 * dir + 1) * cells + cc) * NV + v] = fr[p];
+    }
+  }
+}
+
+// Riemann along every flux line of direction dir; f(NDIMS,nv,im,jm,km).
+template <int NV, int RS, int DIR>
+__global__ void block_riemann(const double* qs, double* f, BlockDims d, Phys<double> P) {
+  const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
+  const long long sx = 1, sy = d.im, sz = (long long)d.im * d.jm;
+  const long long cells = (long long)d.im * d.jm * d.km;
+  int n, a0, a1;
+  long long stride, s0, s1;
+  if (DIR == 0) { a0 = nj; a1 = nk; n = d.im; stride = sx; s0 = sy; s1 = sz; }
+  else if (DIR == 1) { a0 = ni; a1 = nk; n = d.jm; stride = sy; s0 = sx; s1 = sz; }
+  else { a0 = ni; a1 = nj; n = d.km; stride = sz; s0 = sx; s1 = sy; }
+  const long long total = (long long)a0 * a1 * n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    int p = (int)(t % n);
+    long long l = t / n;
+    int c0 = (int)(l % a0) + d.ng - 1;
+    int c1 = (int)(l / a0) + d.ng - 1;
+    if (d.ndims == 2 && DIR != 2) c1 = 0;
+    long long cc = c0 * s0 + c1 * s1 + p * stride;
+    double tl[NV], tr[NV], ql[NV], qr[NV], fx[NV], fo[NV];
+    for (int v = 0; v < NV; ++v) {
+      tl[v] = qs[((long long)(2 * DIR + 0) * cells + cc) * NV + v];
+      tr[v] = qs[((long long)(2 * DIR + 1) * cells + cc) * NV + v];
+    }
+    rotate<NV, DIR>(tl, ql);
+    rotate<NV, DIR>(tr, qr);
+    riemann<NV, RS>(ql, qr, fx, P);
+    unrotate<NV, DIR>(fx, fo);
+    for (int v = 0; v < NV; ++v) f[(cc * NV + v) * d.ndims + DIR] = fo[v];
+  }
+}
+
+template <int NV, int RS>
+__global__ void line_riemann(int n, const double* ql_, const double* qr_, double* f_, Phys<double> P) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double ql[NV], qr[NV], f[NV];
+    for (int v = 0; v < NV; ++v) { ql[v] = ql_[t * NV + v]; qr[v] = qr_[t * NV + v]; }
+    riemann<NV, RS>(ql, qr, f, P);
+    for (int v = 0; v < NV; ++v) f_[t * NV + v] = f[v];
+  }
+}
+
+template <int NV>
+__global__ void pointwise(int op, int n, const double* a, const double* b, double* o, double* cm, double* cp,
+                          Phys<double> P) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double x[NV], y[NV], z[NV];
+    for (int v = 0; v < NV; ++v) x[v] = a[t * NV + v];
+    if (op == 0) prim2cons<NV>(x, z, P);
+    else if (op == 1) cons2prim<NV>(x, z, P);
+    else {
+      for (int v = 0; v < NV; ++v) y[v] = b[t * NV + v];
+      double m, p;
+      fluxspeed<NV, true>(x, y, z, m, p, P);
+      if (cm) cm[t] = m;
+      if (cp) cp[t] = p;
+    }
+    for (int v = 0; v < NV; ++v) o[t * NV + v] = z[v];
+  }
+}
+
+template <int NV>
+__global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsigned long long* out) {
+  const int nx = d.im - 2 * d.ng, ny = d.jm - 2 * d.ng, nz = d.ndims == 3 ? d.km - 2 * d.ng : 1;
+  const long long n = (long long)nx * ny * nz;
+  double vmax = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = d.ng + (int)(t % nx), j = d.ng + (int)((t / nx) % ny);
+    int k = d.ndims == 3 ? d.ng + (int)(t / ((long long)nx * ny)) : 0;
+    long long c = i + (long long)d.im * (j + (long long)d.jm * k);
+    double qc[NV];
+    for (int v = 0; v < NV; ++v) qc[v] = q[c * NV + v];
+    vmax = fmax(vmax, cell_speed<NV>(qc, gamma));
+  }
+  unsigned mask = 0xffffffffu;
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(mask, vmax, o));
+  if ((threadIdx.x & 31) == 0 && vmax > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(vmax));
+}
+
+// ---------------------------------------------------------------------------
+template <int NV, int RS>
+static cudaError_t riemann_dirs(const double* qs, double* f, BlockDims d, const Phys<double>& P, cudaStream_t s) {
+  for (int dir = 0; dir < d.ndims; ++dir) {
+    const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
+    long long total = dir == 0 ? (long long)nj * nk * d.im : (dir == 1 ? (long long)ni * nk * d.jm : (long long)ni * nj * d.km);
+    int grid = (int)((total + 255) / 256);
+    if (dir == 0) block_riemann<NV, RS, 0><<<grid, 256, 0, s>>>(qs, f, d, P);
+    else if (dir == 1) block_riemann<NV, RS, 1><<<grid, 256, 0, s>>>(qs, f, d, P);
+    else block_riemann<NV, RS, 2><<<grid, 256, 0, s>>>(qs, f, d, P);
+  }
+  return cudaGetLastError();
+}
+
+template <int NV>
+static cudaError_t block_flux_nv(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,
+                                 unsigned long long* nonpos, cudaStream_t s) {
+  BlockDims d{NV, u.ndims, u.im, u.jm, u.km, u.ng};
+  long long cells = (long long)u.im * u.jm * u.km;
+  if (u.rec == REC_TVD) {
+    tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(q, qs, d);
+    const long long nbox = (long long)(u.im - 2 * u.ng + 2) * (u.jm - 2 * u.ng + 2) * (u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1);
+    tvd_box<NV><<<(int)((nbox + 255) / 256), 256, 0, s>>>(q, qs, d, u.lim, u.eps, nonpos);
+  } else {
+    tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(q, qs, d);
+    for (int dir = 0; dir < u.ndims; ++dir) {
+      const int ni = u.im - 2 * u.ng + 2, nj = u.jm - 2 * u.ng + 2, nk = u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1;
+      long long lines = (dir == 0 ? (long long)nj * nk : (dir == 1 ? (long long)ni * nk : (long long)ni * nj)) * NV;
+      dir_lines<NV><<<(int)((lines + 127) / 128), 128, 0, s>>>(q, qs, d, dir, u.lim, u.clim, u.eps, u.clip,
+                                                               u.positivity, scratch);
+    }
+  }
+  Phys<double> P{};
+  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
+  P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax; P.lim = u.lim; P.clim = u.clim;
+  if (NV == 5) {
+    switch (u.rs) {
+      case RS_HLLC: return riemann_dirs<NV, RS_HLLC>(qs, f, d, P, s);
+      case RS_ROE: return riemann_dirs<NV, RS_ROE>(qs, f, d, P, s);
+      default: return riemann_dirs<NV, RS_HLL>(qs, f, d, P, s);
+    }
+  }
+  switch (u.rs) {
+    case RS_HLLC: return riemann_dirs<NV, RS_HLLC>(qs, f, d, P, s);
+    case RS_HLLD: return riemann_dirs<NV, RS_HLLD>(qs, f, d, P, s);
+    case RS_ROE: return riemann_dirs<NV, RS_ROE>(qs, f, d, P, s);
+    default: return riemann_dirs<NV, RS_HLL>(qs, f, d, P, s);
+  }
+}
+
+cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,
+                            unsigned long long* nonpos, cudaStream_t s) {
+  if (u.nv == 5) return block_flux_nv<5>(u, q, qs, f, scratch, nonpos, s);
+  return block_flux_nv<9>(u, q, qs, f, scratch, nonpos, s);
+}
+
+size_t unit_block_flux_scratch(const UnitArgs& u) {
+  int n = u.im > u.jm ? u.im : u.jm;
+  if (u.km > n) n = u.km;
+  long long lines = (long long)(n + 2) * (n + 2) * u.nv;
+  return (size_t)lines * 3 * n * sizeof(double);
+}
+
+cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const double* qr, double* f, cudaStream_t s) {
+  Phys<double> P{};
+  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
+  P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax;
+  int grid = (n + 127) / 128;
+  if (grid < 1) grid = 1;
+  if (u.nv == 5) {
+    switch (u.rs) {
+      case RS_HLLC: line_riemann<5, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_ROE: line_riemann<5, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      default: line_riemann<5, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+    }
+  } else {
+    switch (u.rs) {
+      case RS_HLLC: line_riemann<9, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_HLLD: line_riemann<9, RS_HLLD><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_ROE: line_riemann<9, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      default: line_riemann<9, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t unit_pointwise(const UnitArgs& u, int op, int n, const double* a, const double* b, double* o, double* cm,
+                           double* cp, cudaStream_t s) {
+  Phys<double> P{};
+  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
+  P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax;
+  int grid = (n + 127) / 128;
+  if (grid < 1) grid = 1;
+  if (u.nv == 5) pointwise<5><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else pointwise<9><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  return cudaGetLastError();
+}
+
+cudaError_t unit_maxspeed(const UnitArgs& u, const double* q, unsigned long long* out, cudaStream_t s) {
+  BlockDims d{u.nv, u.ndims, u.im, u.jm, u.km, u.ng};
+  long long n = (long long)(u.im - 2 * u.ng) * (u.jm - 2 * u.ng) * (u.ndims == 3 ? u.km - 2 * u.ng : 1);
+  int grid = (int)((n + 255) / 256);
+  if (grid > 4096) grid = 4096;
+  if (u.nv == 5) block_maxspeed<5><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  else block_maxspeed<9><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  return cudaGetLastError();
+}
+
+}  // namespace amun

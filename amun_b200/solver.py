@@ -1,0 +1,141 @@
+"""Host-side mirror of the reference's evolution interface over the C ABI.
+
+``Simulation`` holds one configured device context and a uniform block mesh
+and exposes the reference's operations by their names: ``new_time_step``
+(src/evolution.F90:379), ``evolve`` (the selected evolve_* procedure),
+``advance`` (src/evolution.F90:292 plus the driver's time update,
+src/driver.F90:579-585) and ``boundary_variables``
+(src/boundaries.F90:372).  Errors raise AmunError carrying the reference's
+iret codes; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .mesh import UniformMesh
+from .params import geometry, to_native
+
+
+class Simulation:
+    def __init__(self, params: dict, precision: str = "fp64"):
+        self.params = dict(params)
+        self.params["precision"] = precision
+        self.L = N.lib()
+        self.native = to_native(self.params)
+        self.geo = geometry(self.params)
+        self.mesh = UniformMesh(self.geo)
+        self.nv = 9 if self.native.eqsys == N.AMUN_EQ_MHD else 5
+        N.check(self.L.amun_gpu_init(C.byref(self.native)))
+        self._desc = self.mesh.descriptors()
+        N.check(self.L.amun_gpu_set_blocks(self.mesh.nblocks, self._desc))
+
+    # ---- state ---------------------------------------------------------------
+    def set_primitive(self, q: np.ndarray):
+        """Set the state from a global primitive field (NZ,NY,NX,nv): the
+        block arrays get periodic ghosts, u0 = prim2cons(q) (as
+        setup_problem does), both are uploaded and ghosts refreshed."""
+        qb = np.ascontiguousarray(self.mesh.to_blocks(np.asarray(q, dtype=np.float64)))
+        ub = self.prim2cons(qb)
+        self.upload_blocks(ub, qb)
+        N.check(self.L.amun_gpu_boundary_variables())
+        N.check(self.L.amun_gpu_set_time(0.0, 0.0))
+
+    def upload_blocks(self, u0: np.ndarray, q: np.ndarray):
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        N.check(self.L.amun_gpu_upload_blocks(0, self.mesh.nblocks, N.dptr(u0), N.dptr(q)))
+
+    def download_blocks(self, u0: np.ndarray | None = None, q: np.ndarray | None = None):
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
+        if u0 is None:
+            u0 = np.empty(shp)
+        if q is None:
+            q = np.empty(shp)
+        N.check(self.L.amun_gpu_download_blocks(0, self.mesh.nblocks, N.dptr(u0), N.dptr(q)))
+        return u0, q
+
+    def primitive(self) -> np.ndarray:
+        _, q = self.download_blocks()
+        return self.mesh.from_blocks(q)
+
+    def conserved(self) -> np.ndarray:
+        u, _ = self.download_blocks()
+        return self.mesh.from_blocks(u)
+
+    # ---- evolution -------------------------------------------------------------
+    def new_time_step(self, dtnext: float):
+        cm, dt = C.c_double(), C.c_double()
+        N.check(self.L.amun_gpu_new_time_step(dtnext, C.byref(cm), C.byref(dt)))
+        return cm.value, dt.value
+
+    def evolve(self):
+        N.check(self.L.amun_gpu_evolve())
+
+    def advance(self, dtnext: float):
+        t, dt = C.c_double(), C.c_double()
+        N.check(self.L.amun_gpu_advance(dtnext, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
+
+    def run(self, nsteps: int, dtnext: float, graph: bool = True):
+        N.check(self.L.amun_gpu_run(int(nsteps), dtnext, 1 if graph else 0))
+
+    def boundary_variables(self):
+        N.check(self.L.amun_gpu_boundary_variables())
+
+    def status(self) -> dict:
+        s = N.amun_status()
+        N.check(self.L.amun_gpu_status(C.byref(s)))
+        return dict(time=s.time, dt=s.dt, dtn=s.dtn, cmax=s.cmax, step=s.step,
+                    nonpositive=s.nonpositive, device_bytes=s.device_bytes)
+
+    # ---- per-procedure entry points (FP64) -------------------------------------
+    def prim2cons(self, q: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        u = np.empty_like(q)
+        N.check(self.L.amun_gpu_prim2cons(q.size // self.nv, N.dptr(q), N.dptr(u)))
+        return u
+
+    def cons2prim(self, u: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        q = np.empty_like(u)
+        N.check(self.L.amun_gpu_cons2prim(u.size // self.nv, N.dptr(u), N.dptr(q)))
+        return q
+
+    def fluxspeed(self, q: np.ndarray, u: np.ndarray):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        n = q.size // self.nv
+        f, cm, cp = np.empty_like(q), np.empty(n), np.empty(n)
+        N.check(self.L.amun_gpu_fluxspeed(n, N.dptr(q), N.dptr(u), N.dptr(f), N.dptr(cm), N.dptr(cp)))
+        return f, cm, cp
+
+    def riemann(self, ql: np.ndarray, qr: np.ndarray) -> np.ndarray:
+        ql = np.ascontiguousarray(ql, dtype=np.float64)
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        f = np.empty_like(ql)
+        N.check(self.L.amun_gpu_riemann(ql.size // self.nv, N.dptr(ql), N.dptr(qr), N.dptr(f)))
+        return f
+
+    def set_cmax(self, cmax: float):
+        N.check(self.L.amun_gpu_set_cmax(cmax))
+
+    def update_flux_block(self, qblock: np.ndarray) -> np.ndarray:
+        """update_flux on one block array (km,jm,im,nv) -> f (km,jm,im,nv,NDIMS)."""
+        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        nd = self.mesh.ndims
+        f = np.zeros(qblock.shape + (nd,))
+        dx = np.array([self.mesh.dx, self.mesh.dy, self.mesh.dz][:nd])
+        N.check(self.L.amun_gpu_update_flux_block(N.dptr(dx), N.dptr(qblock), N.dptr(f)))
+        return f
+
+    def maxspeed_block(self, qblock: np.ndarray) -> float:
+        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        out = C.c_double()
+        N.check(self.L.amun_gpu_maxspeed(N.dptr(qblock), C.byref(out)))
+        return out.value
+
+    def close(self):
+        self.L.amun_gpu_finalize()

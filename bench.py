@@ -1,0 +1,377 @@
+"""Benchmark: zone-updates/s of the per-stage finite-volume update.
+
+Workload (the single-GPU configuration the metric is quoted on): 3D ideal
+adiabatic GLM-MHD on a uniform 128^3 periodic box, gamma 5/3, rho=1, p=1,
+B=(1,0,0)/sqrt(4 pi), velocity a seeded random-phase field with |k|^-2
+spectrum on 1<=|k|<=4 at rms Mach 1; WENO-Z, HLLD, SSPRK(3,3), CFL 0.4.
+One step = one full SSPRK(3,3) time step (3 stages) over all 128^3 cells.
+
+`value` is the FP32-bulk path (FP32 reconstruction/fluxes/increments, FP64
+U^n and stage combination); the FP64 plain path, the L1 density error of the
+FP32-bulk state against FP64 after the same steps, the energy drift, the
+e2e number through the C ABI with host arrays, the roofline and a CPU
+baseline (the oracle restatement on the host cores) are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GAMMA = 5.0 / 3.0
+NV = 9
+WORKLOAD = dict(ndims=3, equation_system="mhd", equation_of_state="adi", reconstruction="weno5z", limiter="mc",
+                riemann_solver="hlld", time_advance="rk3", cfl=0.4, gamma=GAMMA, nghosts=4, ncells=128,
+                xblocks=1, yblocks=1, zblocks=1, maxlev=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0,
+                zmax=1.0)
+NCELL = 128 ** 3
+# Algorithmic conserved-state bytes per zone-update of SSPRK(3,3), nv = 9
+# (primitives, fluxes, ghosts and halo re-reads are not credited): the three
+# stages touch 8 state arrays (stage inputs, U^n where the combination reads
+# it, stage outputs).  FP64 plain: 8 x 9 x 8 B = 576 B.  FP32 bulk: U^n and
+# U^{n+1} stay FP64, intermediate stage states are FP32: 48 x 9 = 432 B.
+B_ZU = {"fp64": 8 * NV * 8, "fp32": 48 * NV}
+METRIC = "zone-updates/s FP32 vs FP64 at stated L1 error vs FP64; adjoint/forward time"
+LAUNCHES_PER_STEP = 2 + 3 * (3 + 1)  # dt + end-of-step + 3 stages x (3 sweeps + ghost fill)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def initial_state(mesh):
+    from amun_b200 import problems
+    return problems.turbulence(mesh, GAMMA, seed=0, mach=1.0)
+
+
+def timed_run(sim, torch, steps, warmup, dtnext):
+    """W untimed steps, then K steps bracketed by synchronize and CUDA events
+    recorded on the stream the library launches on."""
+    stream = torch.cuda.current_stream()
+    sim.run(warmup, dtnext, graph=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    sim.run(steps, dtnext, graph=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def kernel_profile(sim, steps, dtnext):
+    """Per-kernel-class device times of eager steps (events around every
+    launch on the launching stream)."""
+    L = sim.L
+    import ctypes as C
+    L.amun_gpu_profile(1, 1)
+    for _ in range(steps):
+        sim.advance(dtnext)
+    L.amun_gpu_profile(0, 0)
+    out = {}
+    for k, name in enumerate(["sweep_x", "sweep_y", "sweep_z", "ghost_fill", "time_step"]):
+        ms, n = C.c_double(), C.c_longlong()
+        L.amun_gpu_profile_read(k, C.byref(ms), C.byref(n))
+        out[name] = {"total_ms": ms.value, "launches": n.value,
+                     "avg_ms": (ms.value / n.value) if n.value else None}
+    return out
+
+
+def cpu_baseline(threads: int, steps: int = 1):
+    """The oracle (FP64 C++ restatement of the reference) on the host cores:
+    a 64^3 sample of the same scheme (64 blocks of 16^3, block-parallel
+    threads like the reference's MPI block decomposition)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from amun_b200.mesh import UniformMesh
+    from amun_b200.params import geometry
+    p = dict(WORKLOAD, ncells=16, xblocks=4, yblocks=4, zblocks=4)
+    o = oracle.Oracle(p, threads=threads)
+    mesh = UniformMesh(geometry(p))
+    o.set_prim(initial_state(mesh))
+    o.advance(1.0)  # warm-up step
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.advance(1.0)
+    dt = time.perf_counter() - t0
+    zu = mesh.ncells_total * steps / dt
+    return {"value": zu, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": f"64^3 periodic box, 64 blocks of 16^3, {steps} SSPRK(3,3) step(s) of the same scheme, "
+                      f"{threads} threads"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from amun_b200.mesh import UniformMesh
+    from amun_b200.params import geometry
+    p = dict(WORKLOAD, ncells=16, xblocks=4, yblocks=4, zblocks=4)
+    o = oracle.Oracle(p, threads=threads)
+    mesh = UniformMesh(geometry(p))
+    o.set_prim(initial_state(mesh))
+    for _ in range(args.warmup):
+        o.advance(1.0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.advance(1.0)
+    dt = time.perf_counter() - t0
+    zu = mesh.ncells_total * args.steps / dt
+    sample = (f"64^3 periodic sample of the 128^3 workload (64 blocks of 16^3), block-parallel over {threads} "
+              f"host threads; FP64 C++ restatement of the reference (the Fortran reference cannot be built here)")
+    line = {"impl": "reference", "metric": METRIC, "value": zu, "unit": "zone-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "mhd3d-128-wenoz-hlld-ssprk33", "sample": "64^3", "parallelism": "host threads"},
+            "cpu_baseline": {"value": zu, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": zu, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    from amun_b200.solver import Simulation
+    dtnext = 1.0e30
+    results = {}
+    q0 = None
+    for prec in ("fp64", "fp32"):
+        sim = Simulation(WORKLOAD, precision=prec)
+        if q0 is None:
+            q0 = initial_state(sim.mesh)
+        sim.L.amun_gpu_set_stream(torch.cuda.current_stream().cuda_stream)
+        sim.set_primitive(q0)
+        barrier()
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            ms = timed_run(sim, torch, args.steps, args.warmup, dtnext)
+        barrier()
+        ms = max_over_ranks(ms)
+        prof = kernel_profile(sim, 3, dtnext)
+        results[prec] = {"ms": ms, "clocks": clk.summary(), "profile": prof,
+                         "zu_per_s": ws * NCELL * args.steps / (ms * 1e-3)}
+        sim.close()
+
+    # accuracy of the FP32-bulk path against FP64 after the same steps
+    acc_steps = 20
+    states = {}
+    for prec in ("fp64", "fp32"):
+        sim = Simulation(WORKLOAD, precision=prec)
+        sim.set_primitive(q0)
+        e0 = None
+        sim.run(acc_steps, dtnext, graph=True)
+        states[prec] = sim.conserved()
+        sim.close()
+    u64, u32 = states["fp64"], states["fp32"]
+    l1 = float(np.sum(np.abs(u32[..., 0] - u64[..., 0])) / np.sum(np.abs(u64[..., 0])))
+    linf = float(np.max(np.abs(u32[..., 0] - u64[..., 0])) / np.max(np.abs(u64[..., 0])))
+    en64, en32 = float(u64[..., 8].sum()), float(u32[..., 8].sum())
+    mass64, mass32 = float(u64[..., 0].sum()), float(u32[..., 0].sum())
+    accuracy = {"steps": acc_steps, "l1_density_rel": l1, "linf_density_rel": linf,
+                "energy_drift_rel": (en32 - en64) / en64, "mass_drift_rel": (mass32 - mass64) / mass64}
+
+    # e2e through the C ABI with host arrays: each step uploads u0 and q of
+    # every block (Fortran layout, pinned host memory), advances one step and
+    # downloads u0 and q, as a caller that owns the arrays does.
+    sim = Simulation(WORKLOAD, precision="fp32")
+    stream = torch.cuda.current_stream()
+    sim.L.amun_gpu_set_stream(stream.cuda_stream)
+    m = sim.mesh
+    shp = (m.nblocks, m.km, m.jm, m.im, NV)
+    qh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+    uh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+    qh[...] = m.to_blocks(q0)
+    uh[...] = sim.prim2cons(qh)
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        sim.upload_blocks(uh, qh)
+        sim.advance(dtnext)
+        sim.download_blocks(uh, qh)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        sim.upload_blocks(uh, qh)
+        sim.advance(dtnext)
+        sim.download_blocks(uh, qh)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(a.elapsed_time(b)) / e2e_steps
+    sim.close()
+    bytes_per_array = int(np.prod(shp)) * 8
+    e2e = {"value": ws * NCELL / (e2e_ms * 1e-3), "unit": "zone-updates/s",
+           "h2d_bytes_per_step": 2 * bytes_per_array, "d2h_bytes_per_step": 2 * bytes_per_array,
+           "ms_per_step": e2e_ms}
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        r32, r64 = results["fp32"], results["fp64"]
+        zu = r32["zu_per_s"]
+        per_gpu = zu / ws
+        achieved = per_gpu * B_ZU["fp32"] / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get("fp32_stage_bytes_per_cell")
+            except Exception:
+                traffic = None
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_kind": peak_kind,
+                    "kernel": "stage sweeps x/y/z + ghost fill (whole SSPRK step, 432 B/zone-update)",
+                    "traffic": traffic,
+                    "fp64": {"achieved": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9,
+                             "frac": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9 / peak}}
+        cpu = None
+        if not args.no_cpu:
+            try:
+                cpu = cpu_baseline(os.cpu_count() or 1)
+            except Exception as exc:  # pragma: no cover
+                cpu = {"error": str(exc)}
+        clocks = r32["clocks"] or {}
+        line = {
+            "metric": METRIC, "value": zu, "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r32["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-phase velocity, PCG64 seed 0)",
+            "config": {"workload": "mhd3d-128^3-periodic weno5z hlld ssprk(3,3) cfl0.4",
+                       "cells_per_gpu": NCELL, "blocks": "1 block of 128^3, 4 ghost layers",
+                       "parallelism": f"{ws} independent replicas" if ws > 1 else "1 GPU",
+                       "l2": "state arrays larger than L2 (>= 0.5 GB resident)",
+                       "precision": "FP32 reconstruction/fluxes/increments, FP64 U^n and stage combination"},
+            "fp64": {"value": r64["zu_per_s"], "ms_per_step": r64["ms"] / args.steps,
+                     "clocks": r64["clocks"]},
+            "speedup_fp32_over_fp64": r32["zu_per_s"] / r64["zu_per_s"],
+            "accuracy_vs_fp64": accuracy,
+            "kernel_profile_fp32": r32["profile"], "kernel_profile_fp64": r64["profile"],
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

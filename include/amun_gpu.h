@@ -1,0 +1,188 @@
+/*
+ * amun_gpu.h -- C ABI of the B200 stage library (libamun_gpu.so).
+ *
+ * Drop-in for AMUN's per-stage finite-volume update: the Fortran driver, the
+ * parameter keys and the block tree stay in the reference; this library
+ * replaces the procedures bound through the reference's procedure pointers
+ * and the per-stage loops of module evolution.  Plain C types only: every
+ * array argument is a HOST pointer in the reference's Fortran layout
+ * (column-major, variable index fastest):
+ *     q, u0, u1 : (nv, im, jm, km)          src/blocks.F90:1153-1161
+ *     f         : (NDIMS, nv, im, jm, km)    src/blocks.F90:1161
+ * with im = ncells + 2 nghosts (km = 1 in 2D), src/coordinates.F90:211-215.
+ *
+ * Conventions (reference error codes, src/driver.F90:847-874):
+ *   return 0 = success; a positive value is a Fortran-compatible iret
+ *   (100 unsupported equation system, 110 unsupported equation of state,
+ *   200 unsupported reconstruction); AMUN_E_* below are library errors.
+ *   The library never traps or aborts; calls are ordered on one CUDA stream.
+ *   State is per process, like the reference's module-level save variables.
+ */
+#ifndef AMUN_GPU_H
+#define AMUN_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* library error codes (above the reference's iret ranges) */
+#define AMUN_E_NOT_INITIALIZED 901
+#define AMUN_E_BAD_ARGUMENT    902
+#define AMUN_E_CUDA            903
+#define AMUN_E_UNSUPPORTED     904
+#define AMUN_E_NO_BLOCKS       905
+
+/* equation_system / equation_of_state (src/equations.F90:322-833) */
+enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1 };
+/* reconstruction (src/interpolations.F90:226-382) */
+enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
+/* limiter / extrema_limiter (src/interpolations.F90:389-445) */
+enum { AMUN_LIM_ZERO = 0, AMUN_LIM_MM = 1, AMUN_LIM_MC = 2, AMUN_LIM_SB = 3,
+       AMUN_LIM_VL = 4, AMUN_LIM_VA = 5 };
+/* riemann_solver (src/schemes.F90:159-503) */
+enum { AMUN_RS_HLL = 0, AMUN_RS_HLLC = 1, AMUN_RS_HLLD = 2, AMUN_RS_ROE = 3 };
+/* time_advance (src/evolution.F90:164-209) */
+enum { AMUN_TA_EULER = 0, AMUN_TA_RK2 = 1, AMUN_TA_SSPRK2 = 2, AMUN_TA_RK3 = 3,
+       AMUN_TA_SSPRK34 = 4, AMUN_TA_SSPRK35 = 5 };
+/* precision modes: FP64 plain (bit-for-bit with the reference arithmetic) and
+ * FP32 bulk (FP32 reconstruction, fluxes and increments; FP64 U^n and stage
+ * combination) */
+enum { AMUN_FP64 = 0, AMUN_FP32_BULK = 1 };
+
+/* The hot-path parameter keys, already parsed.  Field meaning and defaults
+ * are those of the reference's initialize_* routines. */
+typedef struct amun_params {
+  int ndims;            /* NDIMS (compile-time in the reference): 2 or 3       */
+  int eqsys;            /* AMUN_EQ_*              "equation_system"           */
+  int reconstruction;   /* AMUN_REC_*             "reconstruction"            */
+  int limiter;          /* AMUN_LIM_*             "limiter"                   */
+  int extrema_limiter;  /* AMUN_LIM_*             "extrema_limiter"           */
+  int riemann;          /* AMUN_RS_*              "riemann_solver"            */
+  int time_advance;     /* AMUN_TA_*              "time_advance"              */
+  int stages;           /*                        "stages" (ssprk(m,2))       */
+  int fix_positivity;   /* 0/1                    "fix_positivity"            */
+  int clip_extrema;     /* 0/1                    "clip_extrema"              */
+  int precision;        /* AMUN_FP64 / AMUN_FP32_BULK                         */
+  int ncells;           /*                        "ncells"                    */
+  int nghosts;          /*                        "nghosts"                   */
+  double gamma;         /*                        "gamma"                     */
+  double cfl;           /*                        "cfl"                       */
+  double alpha;         /*                        "alpha" (GLM psi decay)     */
+  double eps;           /*                        "eps" (WENO-Z, van Albada)  */
+} amun_params;
+
+/* One leaf block of the mesh, built from the reference's meta block
+ * (src/blocks.F90:109-228) after every regrid. */
+typedef struct amun_block_desc {
+  int level;            /* refinement level, 1-based                          */
+  double dx[3];         /* adx/ady/adz of the level (src/coordinates.F90:339) */
+  int neighbor[27];     /* index of the same-level neighbour block in direction
+                           (ox,oy,oz) at [(ox+1) + 3(oy+1) + 9(oz+1)], -1 when
+                           there is none (non-periodic domain edge)           */
+} amun_block_desc;
+
+typedef struct amun_status {
+  double time, dt, dtn, cmax;
+  long long step;
+  long long nonpositive;  /* "Positive variable is not positive" events of
+                             interfaces_tvd (src/interpolations.F90:813-823) */
+  long long device_bytes; /* bytes of device memory held by the block pool    */
+} amun_status;
+
+/* Fill *p with the reference defaults (hd/adi, tvd/mm, hll, rk2, cfl 0.5 ...). */
+void amun_gpu_default_params(amun_params* p);
+
+/* Apply one parameter-file key the way the reference's initialize_* routines
+ * interpret it, including the accepted spellings (e.g. "hllc"/"HLLC",
+ * "weno5z"/"WENO5-Z").  Unknown keys are ignored (src/parameters.F90:545-551).
+ * Returns the reference iret for unsupported choices (100/110/200). */
+int amun_gpu_set_param(amun_params* p, const char* key, const char* value);
+
+/* initialize_equations/schemes/interpolations/evolution
+ * (src/equations.F90:257, src/schemes.F90:114, src/interpolations.F90:144,
+ *  src/evolution.F90:115): select the kernels for the parameters. */
+int amun_gpu_init(const amun_params* p);
+
+/* Replace the device block list (after generate_mesh / update_mesh,
+ * src/mesh.F90:436, 756; leaf list src/blocks.F90:3756).  Allocates the HBM
+ * block pool and invalidates captured CUDA graphs. */
+int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks);
+
+/* Copy one block's arrays host -> device (u1 may be NULL).  Device state
+ * stays resident between calls. */
+int amun_gpu_upload(int block, const double* u0, const double* u1, const double* q);
+/* Same for `count` consecutive blocks stored back to back. */
+int amun_gpu_upload_blocks(int first, int count, const double* u0, const double* q);
+/* Copy one block's arrays device -> host (any pointer may be NULL).  Ghost
+ * cells of u0 and u1 are prim2cons of the ghost primitives
+ * (update_ghost_cells, src/boundaries.F90:6633). */
+int amun_gpu_download(int block, double* u0, double* u1, double* q);
+int amun_gpu_download_blocks(int first, int count, double* u0, double* q);
+
+/* boundary_variables (src/boundaries.F90:372-479): ghost fill of the
+ * primitive variables from the neighbour blocks. */
+int amun_gpu_boundary_variables(void);
+
+/* new_time_step (src/evolution.F90:379-493): global max speed and dt. */
+int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt);
+
+/* evolve => evolve_{euler,rk2,ssprk2,rk3,ssprk34,ssprk35}
+ * (src/evolution.F90:517-1793): all stages of one step with the current dt,
+ * including ghost fill and primitive update after each stage. */
+int amun_gpu_evolve(void);
+
+/* advance (src/evolution.F90:292-372, single-level mesh) followed by the
+ * driver's time/step update (src/driver.F90:579-585). */
+int amun_gpu_advance(double dtnext, double* time, double* dt);
+
+/* `nsteps` consecutive advance calls without host synchronisation; dt and
+ * time stay on the device.  use_graph != 0 replays one captured CUDA graph
+ * per step. */
+int amun_gpu_run(int nsteps, double dtnext, int use_graph);
+
+/* time, dt, cmax, step and error counters. */
+int amun_gpu_status(amun_status* s);
+/* set the simulation time and dt (restart). */
+int amun_gpu_set_time(double time, double dt);
+
+/* update_flux_iface (src/schemes.F90:58-65) for one block: the exact
+ * stand-in of update_flux_{hd,mhd}_adi (src/schemes.F90:1080, 2970) on the
+ * Fortran arrays, FP64.  dx has NDIMS entries. */
+int amun_gpu_update_flux_block(const double* dx, const double* q, double* f);
+
+/* riemann_iface (src/schemes.F90:66-71): n interfaces, FP64; ql/qr are not
+ * modified (the reference modifies its copies for GLM-MHD). */
+int amun_gpu_riemann(int n, const double* ql, const double* qr, double* f);
+
+/* prim2cons_iface / cons2prim_iface / fluxspeed_iface / maxspeed_iface
+ * (src/equations.F90:70-93), FP64. cm/cp may be NULL. */
+int amun_gpu_prim2cons(int n, const double* q, double* u);
+int amun_gpu_cons2prim(int n, const double* u, double* q);
+int amun_gpu_fluxspeed(int n, const double* q, const double* u, double* f, double* cm, double* cp);
+int amun_gpu_maxspeed(const double* q, double* maxspeed);
+/* module variable cmax of src/equations.F90 (GLM speed), also sets cmax2 */
+int amun_gpu_set_cmax(double cmax);
+
+/* Run all device work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*); NULL returns to the library's own stream.  Invalidates graphs. */
+int amun_gpu_set_stream(void* stream);
+
+/* Per-kernel timers, the device analogue of the reference's PROFILE timers
+ * (src/timers.F90:154-299, e.g. src/evolution.F90:141-147).  While enabled,
+ * every eagerly launched kernel is bracketed by CUDA events on the launching
+ * stream (graph replays are not).  Kinds: 0/1/2 sweep along x/y/z, 3 ghost
+ * fill, 4 time step and reductions.  enable=0 stops recording; reset != 0
+ * clears the accumulated times. */
+int amun_gpu_profile(int enable, int reset);
+int amun_gpu_profile_read(int kind, double* total_ms, long long* launches);
+
+/* finalize_*: release the device pool, graphs and stream. */
+void amun_gpu_finalize(void);
+
+/* Text of the last error (empty when none). */
+const char* amun_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMUN_GPU_H */

@@ -1,0 +1,1534 @@
+// amun_oracle.cpp -- CPU FP64 restatement of AMUN's per-stage finite-volume
+// update, used ONLY as the checker for the GPU library (tests, smoke, and the
+// CPU-baseline leg of bench.py).  It is never linked into, loaded by or called
+// from the product path.
+//
+// Parity status: unpinned by the reference.  AMUN ships no tests, golden
+// vectors or recorded outputs, and the reference (Fortran 2003) cannot be
+// compiled in this environment (no Fortran compiler).  The restatement is
+// therefore pinned by analytic invariants checked in tests/ (exact
+// preservation of uniform states, mirror symmetry, conservation to round-off,
+// Rankine-Hugoniot flux identities and convergence order).
+//
+// Every routine follows the cited Fortran procedure statement by statement,
+// with the same evaluation order and parenthesisation.  Build with
+// -ffp-contract=off so no multiply-add is fused (the GPU FP64 parity build
+// uses -fmad=false for the same reason).  Fortran SIGN(a,b) is copysign.
+//
+// Array layouts are the reference's Fortran layouts (column-major, variable
+// index fastest):  q,u0,u1(nv,im,jm,km), f(NDIMS,nv,im,jm,km)
+// (src/blocks.F90:1153-1161).  Indices below are 1-based like the Fortran.
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cfloat>
+#include <string>
+#include <vector>
+#include <thread>
+#include <algorithm>
+#include <atomic>
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Parameters (src/equations.F90:257-952, src/schemes.F90:114-522,
+// src/interpolations.F90:144-495, src/evolution.F90:115-230,
+// src/coordinates.F90:160-357).  Defaults are the reference defaults.
+// ---------------------------------------------------------------------------
+enum { EQ_HD = 0, EQ_MHD = 1 };
+enum { REC_TVD = 0, REC_WENO5Z = 1 };
+enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
+enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE };
+enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
+
+struct Params {
+  int ndims = 2;
+  int eqsys = EQ_HD;
+  int rec = REC_TVD;
+  int lim = LIM_MM, clim = LIM_MM, plim = LIM_MM;
+  int rs = RS_HLL;
+  int ta = TA_RK2;
+  int stages = 2;
+  bool positivity = false, clip = false, mlp = false;
+  double gamma = 5.0 / 3.0;
+  double cfl = 0.5, alpha = 2.0;
+  double eps = DBL_EPSILON;
+  int ncells = 8, nghosts = 2;
+  int xblocks = 1, yblocks = 1, zblocks = 1;
+  int minlev = 1, maxlev = 1;
+  double xmin = 0, xmax = 1, ymin = 0, ymax = 1, zmin = 0, zmax = 1;
+  double viscosity = 0, resistivity = 0;
+};
+
+bool is_one_of(const std::string& s, std::initializer_list<const char*> l) {
+  for (auto* x : l) if (s == x) return true;
+  return false;
+}
+bool is_on(const std::string& s) {
+  return is_one_of(s, {"on", "ON", "t", "T", "y", "Y", "true", "TRUE", "yes", "YES"});
+}
+std::string strip(const std::string& v) {
+  size_t a = v.find_first_not_of(" \t\"'"), b = v.find_last_not_of(" \t\"'");
+  return a == std::string::npos ? std::string() : v.substr(a, b - a + 1);
+}
+
+// Restates the string selections of the initialize_* routines cited above.
+int apply_key(Params& p, const std::string& key, const std::string& raw) {
+  std::string v = strip(raw);
+  if (key == "ndims") p.ndims = atoi(v.c_str());
+  else if (key == "equation_system") {
+    if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p.eqsys = EQ_HD;
+    else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p.eqsys = EQ_MHD;
+    else return 100;  // src/equations.F90:830
+  } else if (key == "equation_of_state") {
+    if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) return 110;
+  } else if (key == "reconstruction") {
+    if (is_one_of(v, {"tvd", "TVD"})) p.rec = REC_TVD;
+    else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p.rec = REC_WENO5Z;
+    else return 200;  // src/interpolations.F90:382
+  } else if (key == "limiter" || key == "extrema_limiter" || key == "prolongation_limiter") {
+    int l = LIM_ZERO;
+    if (is_one_of(v, {"mm", "minmod"})) l = LIM_MM;
+    else if (is_one_of(v, {"mc", "monotonized_central"})) l = LIM_MC;
+    else if (is_one_of(v, {"sb", "superbee"})) l = LIM_SB;
+    else if (is_one_of(v, {"vl", "vanleer"})) l = LIM_VL;
+    else if (key == "limiter" && is_one_of(v, {"va", "vanalbada"})) l = LIM_VA;
+    if (key == "limiter") p.lim = l; else if (key == "extrema_limiter") p.clim = l; else p.plim = l;
+  } else if (key == "riemann_solver") {
+    // src/schemes.F90:159-503: unknown names revert to HLL; HLLD is MHD only.
+    if (is_one_of(v, {"hllc", "HLLC"})) p.rs = RS_HLLC;
+    else if (is_one_of(v, {"hlld", "HLLD"})) p.rs = RS_HLLD;
+    else if (is_one_of(v, {"roe", "ROE"})) p.rs = RS_ROE;
+    else p.rs = RS_HLL;
+  } else if (key == "time_advance") {
+    if (is_one_of(v, {"euler", "EULER"})) p.ta = TA_EULER;
+    else if (is_one_of(v, {"rk2", "RK2"})) p.ta = TA_RK2;
+    else if (is_one_of(v, {"ssprk(m,2)", "SSPRK(m,2)"})) p.ta = TA_SSPRK2;
+    else if (is_one_of(v, {"rk3", "RK3"})) p.ta = TA_RK3;
+    else if (is_one_of(v, {"rk3.4", "RK3.4", "ssprk(4,3)", "SSPRK(4,3)"})) p.ta = TA_SSPRK34;
+    else if (is_one_of(v, {"rk3.5", "RK3.5", "ssprk(5,3)", "SSPRK(5,3)"})) p.ta = TA_SSPRK35;
+    else p.ta = TA_RK2;
+  } else if (key == "stages") p.stages = atoi(v.c_str());
+  else if (key == "fix_positivity") p.positivity = is_on(v);
+  else if (key == "clip_extrema") p.clip = is_on(v);
+  else if (key == "mlp_limiting") p.mlp = is_on(v);
+  else if (key == "gamma") p.gamma = atof(v.c_str());
+  else if (key == "cfl") p.cfl = atof(v.c_str());
+  else if (key == "alpha") p.alpha = atof(v.c_str());
+  else if (key == "eps") p.eps = atof(v.c_str());
+  else if (key == "ncells") p.ncells = atoi(v.c_str());
+  else if (key == "nghosts") p.nghosts = atoi(v.c_str());
+  else if (key == "xblocks") p.xblocks = atoi(v.c_str());
+  else if (key == "yblocks") p.yblocks = atoi(v.c_str());
+  else if (key == "zblocks") p.zblocks = atoi(v.c_str());
+  else if (key == "minlev") p.minlev = atoi(v.c_str());
+  else if (key == "maxlev") p.maxlev = atoi(v.c_str());
+  else if (key == "xmin") p.xmin = atof(v.c_str());
+  else if (key == "xmax") p.xmax = atof(v.c_str());
+  else if (key == "ymin") p.ymin = atof(v.c_str());
+  else if (key == "ymax") p.ymax = atof(v.c_str());
+  else if (key == "zmin") p.zmin = atof(v.c_str());
+  else if (key == "zmax") p.zmax = atof(v.c_str());
+  return 0;  // unknown keys are ignored, like get_parameter_* (src/parameters.F90:545-551)
+}
+
+inline double fsign(double a, double b) { return std::copysign(std::fabs(a), b); }
+inline double fmin2(double a, double b) { return a < b ? a : b; }
+inline double fmax2(double a, double b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// The oracle state: equation constants, coordinates and the block data.
+// ---------------------------------------------------------------------------
+struct Oracle {
+  Params p;
+  // equation indices (src/equations.F90:335-485), 1-based
+  int nv = 5, idn = 1, ivx = 2, ivy = 3, ivz = 4, imx = 2, imy = 3, imz = 4;
+  int ibx = -1, iby = -1, ibz = -1, ibp = -1, ipr = 5, ien = 5;
+  double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5;
+  double cmax = 0.0, cmax2 = 0.0;
+  // evolution (src/evolution.F90:60-90)
+  double cfl = 0.5, decay = 1.0, time = 0.0, dt = 0.0, dtn = 1.0;
+  long step = 0;
+  // coordinates (src/coordinates.F90:42-72, 198-249)
+  int nc = 8, ng = 2, in = 8, jn = 8, kn = 1, im = 12, jm = 12, km = 1;
+  int ib, ie, ibl, ieu, jb, je, jbl, jeu, kb = 1, ke = 1, kbl = 1, keu = 1;
+  double dx = 1, dy = 1, dz = 1;
+  // uniform block grid at one level
+  int nbx = 1, nby = 1, nbz = 1;
+  struct Block { std::vector<double> u0, u1, q, f; double* u; };
+  std::vector<Block> blocks;
+  int nthreads = 1;
+  std::atomic<long> nonpositive{0};  // "Positive variable is not positive" events
+
+  // --- helpers for Fortran layout ------------------------------------------
+  inline size_t qi(int p_, int i, int j, int k) const {
+    return (size_t)(p_ - 1) + (size_t)nv * ((size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (size_t)(k - 1)));
+  }
+  inline size_t fi(int d, int p_, int i, int j, int k) const {
+    return (size_t)(d - 1) + (size_t)p.ndims * qi(p_, i, j, k);
+  }
+  size_t cells() const { return (size_t)im * jm * km; }
+
+  int setup() {
+    // equations (src/equations.F90:322-485)
+    if (p.eqsys == EQ_HD) {
+      nv = 5; idn = 1; ivx = 2; ivy = 3; ivz = 4; imx = 2; imy = 3; imz = 4;
+      ibx = iby = ibz = ibp = -1; ipr = ien = 5;
+    } else {
+      nv = 9; idn = 1; ivx = 2; ivy = 3; ivz = 4; imx = 2; imy = 3; imz = 4;
+      ibx = 5; iby = 6; ibz = 7; ibp = 8; ipr = ien = 9;
+    }
+    if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
+    gamma = p.gamma; gammam1 = gamma - 1.0; gammam1i = 1.0 / gammam1;
+    // evolution: CFL rescale and decay (src/evolution.F90:164-213)
+    cfl = p.cfl;
+    if (p.ta == TA_SSPRK2) { p.stages = std::max(2, std::min(9, p.stages)); cfl = (p.stages - 1) * cfl; }
+    if (p.ta == TA_SSPRK34) cfl = 2.0 * cfl;
+    if (p.ta == TA_SSPRK35) cfl = 2.65062919143939 * cfl;
+    decay = std::exp(-p.alpha * cfl);
+    // coordinates (src/coordinates.F90:180-249)
+    nc = p.ncells; ng = p.nghosts;
+    in = jn = nc; kn = (p.ndims == 3) ? nc : 1;
+    im = in + 2 * ng; jm = jn + 2 * ng; km = (p.ndims == 3) ? kn + 2 * ng : 1;
+    ib = ng + 1; ie = ng + in; ibl = ib - 1; ieu = ie + 1;
+    jb = ng + 1; je = ng + jn; jbl = jb - 1; jeu = je + 1;
+    if (p.ndims == 3) { kb = ng + 1; ke = ng + kn; kbl = kb - 1; keu = ke + 1; }
+    else { kb = ke = kbl = keu = 1; }
+    int lev = p.maxlev, ff = 1 << (lev - 1);
+    dx = (p.xmax - p.xmin) / (p.xblocks * (in * ff));
+    dy = (p.ymax - p.ymin) / (p.yblocks * (jn * ff));
+    dz = (p.ndims == 3) ? (p.zmax - p.zmin) / (p.zblocks * (kn * ff)) : 1.0;
+    nbx = p.xblocks * ff; nby = p.yblocks * ff; nbz = (p.ndims == 3) ? p.zblocks * ff : 1;
+    blocks.assign((size_t)nbx * nby * nbz, Block());
+    for (auto& b : blocks) {
+      b.u0.assign(nv * cells(), 0.0); b.u1.assign(nv * cells(), 0.0);
+      b.q.assign(nv * cells(), 0.0);
+      b.f.assign((size_t)p.ndims * nv * cells(), 0.0);
+      b.u = b.u0.data();
+    }
+    return 0;
+  }
+
+  // =========================================================================
+  // EQUATIONS
+  // =========================================================================
+  // prim2cons_hd_adi src/equations.F90:1762-1810, prim2cons_mhd_adi 2815-2868
+  void prim2cons(int n, const double* q, double* u) const {
+    for (int i = 0; i < n; ++i) {
+      const double* Q = q + (size_t)nv * i; double* U = u + (size_t)nv * i;
+      U[idn - 1] = Q[idn - 1];
+      U[imx - 1] = Q[idn - 1] * Q[ivx - 1];
+      U[imy - 1] = Q[idn - 1] * Q[ivy - 1];
+      U[imz - 1] = Q[idn - 1] * Q[ivz - 1];
+      if (p.eqsys == EQ_HD) {
+        double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
+        double ei = gammam1i * Q[ipr - 1];
+        U[ien - 1] = ei + ek;
+      } else {
+        U[ibx - 1] = Q[ibx - 1]; U[iby - 1] = Q[iby - 1]; U[ibz - 1] = Q[ibz - 1]; U[ibp - 1] = Q[ibp - 1];
+        double ei = gammam1i * Q[ipr - 1];
+        double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
+        double em = 0.5 * (Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1]);
+        U[ien - 1] = ei + ek + em;
+      }
+    }
+  }
+
+  // cons2prim_hd_adi src/equations.F90:1828-1876, cons2prim_mhd_adi 2886-2939
+  void cons2prim(int n, const double* u, double* q) const {
+    for (int i = 0; i < n; ++i) {
+      const double* U = u + (size_t)nv * i; double* Q = q + (size_t)nv * i;
+      Q[idn - 1] = U[idn - 1];
+      Q[ivx - 1] = U[imx - 1] / U[idn - 1];
+      Q[ivy - 1] = U[imy - 1] / U[idn - 1];
+      Q[ivz - 1] = U[imz - 1] / U[idn - 1];
+      if (p.eqsys == EQ_HD) {
+        double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
+        double ei = U[ien - 1] - ek;
+        Q[ipr - 1] = gammam1 * ei;
+      } else {
+        Q[ibx - 1] = U[ibx - 1]; Q[iby - 1] = U[iby - 1]; Q[ibz - 1] = U[ibz - 1]; Q[ibp - 1] = U[ibp - 1];
+        double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
+        double em = 0.5 * (Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1]);
+        double ei = U[ien - 1] - (ek + em);
+        Q[ipr - 1] = gammam1 * ei;
+      }
+    }
+  }
+
+  // fluxspeed_hd_adi src/equations.F90:1896-1958,
+  // fluxspeed_mhd_adi src/equations.F90:2959-3045
+  void fluxspeed(int n, const double* q, const double* u, double* f, double* cm, double* cp) const {
+    for (int i = 0; i < n; ++i) {
+      const double* Q = q + (size_t)nv * i; const double* U = u + (size_t)nv * i; double* F = f + (size_t)nv * i;
+      if (p.eqsys == EQ_HD) {
+        F[idn - 1] = U[imx - 1];
+        F[imx - 1] = Q[ivx - 1] * U[imx - 1];
+        F[imy - 1] = Q[ivx - 1] * U[imy - 1];
+        F[imz - 1] = Q[ivx - 1] * U[imz - 1];
+        F[imx - 1] = F[imx - 1] + Q[ipr - 1];
+        F[ien - 1] = Q[ivx - 1] * (U[ien - 1] + Q[ipr - 1]);
+        if (cm && cp) {
+          double cs = std::sqrt(gamma * Q[ipr - 1] / Q[idn - 1]);
+          cm[i] = Q[ivx - 1] - cs;
+          cp[i] = Q[ivx - 1] + cs;
+        }
+      } else {
+        double bx2 = Q[ibx - 1] * Q[ibx - 1];
+        double by2 = Q[iby - 1] * Q[iby - 1];
+        double bz2 = Q[ibz - 1] * Q[ibz - 1];
+        double bb = bx2 + by2 + bz2;
+        double vb = Q[ivx - 1] * Q[ibx - 1] + Q[ivy - 1] * Q[iby - 1] + Q[ivz - 1] * Q[ibz - 1];
+        double pt = Q[ipr - 1] + 0.5 * bb;
+        F[idn - 1] = U[imx - 1];
+        F[imx - 1] = Q[ivx - 1] * U[imx - 1] - bx2;
+        F[imy - 1] = Q[ivx - 1] * U[imy - 1] - Q[ibx - 1] * Q[iby - 1];
+        F[imz - 1] = Q[ivx - 1] * U[imz - 1] - Q[ibx - 1] * Q[ibz - 1];
+        F[imx - 1] = F[imx - 1] + pt;
+        F[ibx - 1] = Q[ibp - 1];
+        F[iby - 1] = Q[ivx - 1] * Q[iby - 1] - Q[ibx - 1] * Q[ivy - 1];
+        F[ibz - 1] = Q[ivx - 1] * Q[ibz - 1] - Q[ibx - 1] * Q[ivz - 1];
+        F[ibp - 1] = cmax2 * Q[ibx - 1];
+        F[ien - 1] = Q[ivx - 1] * (U[ien - 1] + pt) - Q[ibx - 1] * vb;
+        if (cm && cp) {
+          double fa = gamma * Q[ipr - 1];
+          double fb = fa + bb;
+          double fc = fb * fb - 4.0 * fa * bx2;
+          double cf;
+          if (fc > 0.0) cf = std::sqrt(0.5 * (fb + std::sqrt(fc)) / Q[idn - 1]);
+          else cf = std::sqrt(0.5 * fb / Q[idn - 1]);
+          cm[i] = Q[ivx - 1] - cf;
+          cp[i] = Q[ivx - 1] + cf;
+        }
+      }
+    }
+  }
+
+  // maxspeed_hd_adi src/equations.F90:1974-2044, maxspeed_mhd_adi 3060-3131
+  double maxspeed(const double* qq) const {
+    double ms = 0.0;
+    for (int k = kb; k <= ke; ++k)
+      for (int j = jb; j <= je; ++j)
+        for (int i = ib; i <= ie; ++i) {
+          const double* Q = qq + qi(1, i, j, k);
+          double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+          double v = std::sqrt(vv);
+          double c;
+          if (p.eqsys == EQ_HD) {
+            c = std::sqrt(gamma * Q[ipr - 1] / Q[idn - 1]);
+          } else {
+            double bb = Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1];
+            c = std::sqrt((gamma * Q[ipr - 1] + bb) / Q[idn - 1]);
+          }
+          ms = fmax2(ms, v + c);
+        }
+    return ms;
+  }
+
+  // esystem_roe_hd_adi src/equations.F90:2075-2180.  l(var,wave), r(wave,var)
+  // are returned as l[(var-1)+nv*(wave-1)], r[(wave-1)+nv*(var-1)].
+  void esystem_roe_hd(const double* q, double* c, double* l, double* r) const {
+    const int N = nv;
+    std::fill(l, l + N * N, 0.0); std::fill(r, r + N * N, 0.0);
+    auto L = [&](int var, int wave) -> double& { return l[(var - 1) + N * (wave - 1)]; };
+    auto R = [&](int wave, int var) -> double& { return r[(wave - 1) + N * (var - 1)]; };
+    L(ivy, 2) = 1.0; L(ivz, 3) = 1.0;
+    R(1, idn) = 1.0; R(2, ivy) = 1.0; R(3, ivz) = 1.0; R(4, idn) = 1.0; R(5, idn) = 1.0;
+    double vv = q[ivx - 1] * q[ivx - 1] + q[ivy - 1] * q[ivy - 1] + q[ivz - 1] * q[ivz - 1];
+    double vh = 0.5 * vv;
+    double c2 = gammam1 * (q[ien - 1] - vh);
+    double na = 0.5 / c2;
+    double cc = std::sqrt(c2);
+    double vc = q[ivx - 1] * cc;
+    double ng_ = na * gammam1;
+    double nd = 2.0 * ng_;
+    double nw = na * vc;
+    double nh = na * gammam1 * vh;
+    double ncc = na * cc;
+    c[0] = q[ivx - 1] - cc; c[1] = q[ivx - 1]; c[2] = q[ivx - 1]; c[3] = q[ivx - 1]; c[4] = q[ivx - 1] + cc;
+    L(idn, 1) = nh + nw;
+    L(ivx, 1) = -ng_ * q[ivx - 1] - ncc;
+    L(ivy, 1) = -ng_ * q[ivy - 1];
+    L(ivz, 1) = -ng_ * q[ivz - 1];
+    L(ien, 1) = ng_;
+    L(idn, 2) = -q[ivy - 1];
+    L(idn, 3) = -q[ivz - 1];
+    L(idn, 4) = 1.0 - ng_ * vv;
+    L(ivx, 4) = nd * q[ivx - 1];
+    L(ivy, 4) = nd * q[ivy - 1];
+    L(ivz, 4) = nd * q[ivz - 1];
+    L(ien, 4) = -nd;
+    L(idn, 5) = nh - nw;
+    L(ivx, 5) = -ng_ * q[ivx - 1] + ncc;
+    L(ivy, 5) = -ng_ * q[ivy - 1];
+    L(ivz, 5) = -ng_ * q[ivz - 1];
+    L(ien, 5) = ng_;
+    R(1, ivx) = q[ivx - 1] - cc;
+    R(1, ivy) = q[ivy - 1];
+    R(1, ivz) = q[ivz - 1];
+    R(1, ien) = q[ien - 1] - vc;
+    R(2, ien) = q[ivy - 1];
+    R(3, ien) = q[ivz - 1];
+    R(4, ivx) = q[ivx - 1];
+    R(4, ivy) = q[ivy - 1];
+    R(4, ivz) = q[ivz - 1];
+    R(4, ien) = vh;
+    R(5, ivx) = q[ivx - 1] + cc;
+    R(5, ivy) = q[ivy - 1];
+    R(5, ivz) = q[ivz - 1];
+    R(5, ien) = q[ien - 1] + vc;
+  }
+
+  // esystem_roe_mhd_adi src/equations.F90:3162-3468.  Returns false when the
+  // eigenvectors are not computed (all waves in one direction, 3237-3238).
+  bool esystem_roe_mhd(double x, double y, const double* q, double* c, double* l, double* r) const {
+    const int N = nv;
+    std::fill(l, l + N * N, 0.0); std::fill(r, r + N * N, 0.0);
+    auto L = [&](int var, int wave) -> double& { return l[(var - 1) + N * (wave - 1)]; };
+    auto R = [&](int wave, int var) -> double& { return r[(wave - 1) + N * (var - 1)]; };
+    const double eps = DBL_EPSILON;
+    const double gammam2 = gamma - 2.0;
+    R(4, idn) = 1.0;
+    double di = 1.0 / q[idn - 1];
+    double casq = q[ibx - 1] * q[ibx - 1] * di;
+    double ca = std::sqrt(casq);
+    double vsq = q[ivx - 1] * q[ivx - 1] + q[ivy - 1] * q[ivy - 1] + q[ivz - 1] * q[ivz - 1];
+    double btsq = q[iby - 1] * q[iby - 1] + q[ibz - 1] * q[ibz - 1];
+    double bt_starsq = (gammam1 - gammam2 * y) * btsq;
+    double hp = q[ien - 1] - (casq + btsq * di);
+    double twid_asq = fmax2(eps, (gammam1 * (hp - 0.5 * vsq) - gammam2 * x));
+    double ct2 = bt_starsq * di;
+    double tsum = casq + ct2 + twid_asq;
+    double tdif = casq + ct2 - twid_asq;
+    double cf2_cs2 = std::sqrt((tdif * tdif + 4.0 * twid_asq * ct2));
+    double cfsq = 0.5 * (tsum + cf2_cs2);
+    double cf = std::sqrt(cfsq);
+    double cssq = twid_asq * casq / cfsq;
+    double cs = std::sqrt(cssq);
+    c[0] = q[ivx - 1] - cf; c[1] = q[ivx - 1] - ca; c[2] = q[ivx - 1] - cs; c[3] = q[ivx - 1];
+    c[4] = q[ivx - 1]; c[5] = q[ivx - 1] + cs; c[6] = q[ivx - 1] + ca; c[7] = q[ivx - 1] + cf; c[8] = c[7];
+    if (c[0] >= 0.0) return false;
+    if (c[7] <= 0.0) return false;
+    double bt = std::sqrt(btsq);
+    double bt_star = std::sqrt(bt_starsq);
+    double bet2, bet3;
+    if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; }
+    else { bet2 = q[iby - 1] / bt; bet3 = q[ibz - 1] / bt; }
+    double bet2_star = bet2 / std::sqrt(gammam1 - gammam2 * y);
+    double bet3_star = bet3 / std::sqrt(gammam1 - gammam2 * y);
+    double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+    double vbet = q[ivy - 1] * bet2_star + q[ivz - 1] * bet3_star;
+    double alpha_f, alpha_s;
+    if ((cfsq - cssq) == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+    else if ((twid_asq - cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
+    else if ((cfsq - twid_asq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+    else {
+      alpha_f = std::sqrt((twid_asq - cssq) / (cfsq - cssq));
+      alpha_s = std::sqrt((cfsq - twid_asq) / (cfsq - cssq));
+    }
+    double sqrtd = std::sqrt(q[idn - 1]);
+    double isqrtd = 1.0 / sqrtd;
+    double s = fsign(1.0, q[ibx - 1]);
+    double twid_a = std::sqrt(twid_asq);
+    double qf = cf * alpha_f * s;
+    double qs = cs * alpha_s * s;
+    double af_prime = twid_a * alpha_f * isqrtd;
+    double as_prime = twid_a * alpha_s * isqrtd;
+    double afpbb = af_prime * bt_star * bet_starsq;
+    double aspbb = as_prime * bt_star * bet_starsq;
+    R(1, idn) = alpha_f; R(3, idn) = alpha_s; R(6, idn) = alpha_s; R(8, idn) = alpha_f;
+    R(1, ivx) = alpha_f * c[0]; R(3, ivx) = alpha_s * c[2]; R(4, ivx) = q[ivx - 1];
+    R(6, ivx) = alpha_s * c[5]; R(8, ivx) = alpha_f * c[7];
+    double qa = alpha_f * q[ivy - 1], qb = alpha_s * q[ivy - 1], qc = qs * bet2_star, qd = qf * bet2_star;
+    R(1, ivy) = qa + qc; R(2, ivy) = -bet3; R(3, ivy) = qb - qd; R(4, ivy) = q[ivy - 1];
+    R(6, ivy) = qb + qd; R(7, ivy) = bet3; R(8, ivy) = qa - qc;
+    qa = alpha_f * q[ivz - 1]; qb = alpha_s * q[ivz - 1]; qc = qs * bet3_star; qd = qf * bet3_star;
+    R(1, ivz) = qa + qc; R(2, ivz) = bet2; R(3, ivz) = qb - qd; R(4, ivz) = q[ivz - 1];
+    R(6, ivz) = qb + qd; R(7, ivz) = -bet2; R(8, ivz) = qa - qc;
+    R(1, ipr) = alpha_f * (hp - q[ivx - 1] * cf) + qs * vbet + aspbb;
+    R(2, ipr) = -(q[ivy - 1] * bet3 - q[ivz - 1] * bet2);
+    R(3, ipr) = alpha_s * (hp - q[ivx - 1] * cs) - qf * vbet - afpbb;
+    R(4, ipr) = 0.5 * vsq + gammam2 * x / gammam1;
+    R(6, ipr) = alpha_s * (hp + q[ivx - 1] * cs) + qf * vbet - afpbb;
+    R(7, ipr) = -R(2, ipr);
+    R(8, ipr) = alpha_f * (hp + q[ivx - 1] * cf) - qs * vbet + aspbb;
+    R(1, iby) = as_prime * bet2_star;
+    R(2, iby) = -bet3 * s * isqrtd;
+    R(3, iby) = -af_prime * bet2_star;
+    R(6, iby) = R(3, iby); R(7, iby) = R(2, iby); R(8, iby) = R(1, iby);
+    R(1, ibz) = as_prime * bet3_star;
+    R(2, ibz) = bet2 * s * isqrtd;
+    R(3, ibz) = -af_prime * bet3_star;
+    R(6, ibz) = R(3, ibz); R(7, ibz) = R(2, ibz); R(8, ibz) = R(1, ibz);
+    double norm = 0.5 / twid_asq;
+    double cff = norm * alpha_f * cf;
+    double css = norm * alpha_s * cs;
+    qf = qf * norm;
+    qs = qs * norm;
+    double af = norm * af_prime * q[idn - 1];
+    double as = norm * as_prime * q[idn - 1];
+    double afpb = norm * af_prime * bt_star;
+    double aspb = norm * as_prime * bt_star;
+    norm = norm * gammam1;
+    alpha_f = alpha_f * norm;
+    alpha_s = alpha_s * norm;
+    double q2_star = bet2_star / bet_starsq;
+    double q3_star = bet3_star / bet_starsq;
+    double vqstr = (q[ivy - 1] * q2_star + q[ivz - 1] * q3_star);
+    norm = 2.0 * norm;
+    L(idn, 1) = alpha_f * (vsq - hp) + cff * (cf + q[ivx - 1]) - qs * vqstr - aspb;
+    L(ivx, 1) = -alpha_f * q[ivx - 1] - cff;
+    L(ivy, 1) = -alpha_f * q[ivy - 1] + qs * q2_star;
+    L(ivz, 1) = -alpha_f * q[ivz - 1] + qs * q3_star;
+    L(ipr, 1) = alpha_f;
+    L(iby, 1) = as * q2_star - alpha_f * q[iby - 1];
+    L(ibz, 1) = as * q3_star - alpha_f * q[ibz - 1];
+    L(idn, 2) = 0.5 * (q[ivy - 1] * bet3 - q[ivz - 1] * bet2);
+    L(ivy, 2) = -0.5 * bet3;
+    L(ivz, 2) = 0.5 * bet2;
+    L(iby, 2) = -0.5 * sqrtd * bet3 * s;
+    L(ibz, 2) = 0.5 * sqrtd * bet2 * s;
+    L(idn, 3) = alpha_s * (vsq - hp) + css * (cs + q[ivx - 1]) + qf * vqstr + afpb;
+    L(ivx, 3) = -alpha_s * q[ivx - 1] - css;
+    L(ivy, 3) = -alpha_s * q[ivy - 1] - qf * q2_star;
+    L(ivz, 3) = -alpha_s * q[ivz - 1] - qf * q3_star;
+    L(ipr, 3) = alpha_s;
+    L(iby, 3) = -af * q2_star - alpha_s * q[iby - 1];
+    L(ibz, 3) = -af * q3_star - alpha_s * q[ibz - 1];
+    L(idn, 4) = 1.0 - norm * (0.5 * vsq - gammam2 * x / gammam1);
+    L(ivx, 4) = norm * q[ivx - 1];
+    L(ivy, 4) = norm * q[ivy - 1];
+    L(ivz, 4) = norm * q[ivz - 1];
+    L(ipr, 4) = -norm;
+    L(iby, 4) = norm * q[iby - 1];
+    L(ibz, 4) = norm * q[ibz - 1];
+    L(idn, 6) = alpha_s * (vsq - hp) + css * (cs - q[ivx - 1]) - qf * vqstr + afpb;
+    L(ivx, 6) = -alpha_s * q[ivx - 1] + css;
+    L(ivy, 6) = -alpha_s * q[ivy - 1] + qf * q2_star;
+    L(ivz, 6) = -alpha_s * q[ivz - 1] + qf * q3_star;
+    L(ipr, 6) = alpha_s;
+    L(iby, 6) = L(iby, 3);
+    L(ibz, 6) = L(ibz, 3);
+    L(idn, 7) = -L(idn, 2);
+    L(ivy, 7) = -L(ivy, 2);
+    L(ivz, 7) = -L(ivz, 2);
+    L(iby, 7) = L(iby, 2);
+    L(ibz, 7) = L(ibz, 2);
+    L(idn, 8) = alpha_f * (vsq - hp) + cff * (cf - q[ivx - 1]) + qs * vqstr - aspb;
+    L(ivx, 8) = -alpha_f * q[ivx - 1] + cff;
+    L(ivy, 8) = -alpha_f * q[ivy - 1] - qs * q2_star;
+    L(ivz, 8) = -alpha_f * q[ivz - 1] - qs * q3_star;
+    L(ipr, 8) = alpha_f;
+    L(iby, 8) = L(iby, 1);
+    L(ibz, 8) = L(ibz, 1);
+    return true;
+  }
+
+  // =========================================================================
+  // INTERPOLATIONS
+  // =========================================================================
+  // limiters src/interpolations.F90:4684-4877
+  double limiter(int which, double x, double a, double b) const {
+    switch (which) {
+      case LIM_MM: return 0.5 * (fsign(x, a) + fsign(x, b)) * fmin2(std::fabs(a), std::fabs(b));
+      case LIM_MC: return (fsign(x, a) + fsign(x, b)) * fmin2(fmin2(std::fabs(a), std::fabs(b)), 0.25 * std::fabs(a + b));
+      case LIM_SB: return 0.5 * (fsign(x, a) + fsign(x, b)) *
+                          fmax2(fmin2(2.0 * std::fabs(a), std::fabs(b)), fmin2(std::fabs(a), 2.0 * std::fabs(b)));
+      case LIM_VL: {
+        double c = a * b;
+        if (c > 0.0) c = 2.0 * x * c / (a + b); else c = 0.0;
+        return c;
+      }
+      case LIM_VA: return x * a * b * (a + b) / fmax2(p.eps, a * a + b * b);
+      default: return 0.0;
+    }
+  }
+
+  // interfaces_tvd src/interpolations.F90:729-848.  qv(im,jm,km) one variable;
+  // out qs(im,jm,km,2,NDIMS).
+  void interfaces_tvd(bool positive, const double* qv, double* qs) {
+    const size_t N = cells();
+    auto Q = [&](int i, int j, int k) { return qv[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1))]; };
+    auto QS = [&](int i, int j, int k, int s, int d) -> double& {
+      return qs[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)) + N * ((size_t)(s - 1) + 2 * (size_t)(d - 1))];
+    };
+    ghost_copy(qv, qs);
+    const int nd = p.ndims;
+    for (int k = kbl; k <= keu; ++k)
+      for (int j = jbl; j <= jeu; ++j)
+        for (int i = ibl; i <= ieu; ++i) {
+          double dql[3], dqr[3], dq[3] = {0, 0, 0};
+          dql[0] = Q(i, j, k) - Q(i - 1, j, k); dqr[0] = Q(i + 1, j, k) - Q(i, j, k);
+          dq[0] = limiter(p.lim, 0.5, dql[0], dqr[0]);
+          dql[1] = Q(i, j, k) - Q(i, j - 1, k); dqr[1] = Q(i, j + 1, k) - Q(i, j, k);
+          dq[1] = limiter(p.lim, 0.5, dql[1], dqr[1]);
+          if (nd == 3) {
+            dql[2] = Q(i, j, k) - Q(i, j, k - 1); dqr[2] = Q(i, j, k + 1) - Q(i, j, k);
+            dq[2] = limiter(p.lim, 0.5, dql[2], dqr[2]);
+          }
+          if (positive) {
+            if (Q(i, j, k) > 0.0) {
+              for (;;) {
+                double s = std::fabs(dq[0]) + std::fabs(dq[1]);
+                if (nd == 3) s = s + std::fabs(dq[2]);
+                if (!(Q(i, j, k) <= s)) break;
+                for (int d = 0; d < nd; ++d) dq[d] = 0.5 * dq[d];
+              }
+            } else {
+              ++nonpositive;
+              for (int d = 0; d < nd; ++d) dq[d] = 0.0;
+            }
+          }
+          QS(i, j, k, 1, 1) = Q(i, j, k) + dq[0];
+          QS(i - 1, j, k, 2, 1) = Q(i, j, k) - dq[0];
+          QS(i, j, k, 1, 2) = Q(i, j, k) + dq[1];
+          QS(i, j - 1, k, 2, 2) = Q(i, j, k) - dq[1];
+          if (nd == 3) {
+            QS(i, j, k, 1, 3) = Q(i, j, k) + dq[2];
+            QS(i, j, k - 1, 2, 3) = Q(i, j, k) - dq[2];
+          }
+        }
+  }
+
+  // the "copy ghost zones" block shared by interfaces_tvd / interfaces_dir
+  // (src/interpolations.F90:758-771, 893-906)
+  void ghost_copy(const double* qv, double* qs) const {
+    const size_t N = cells();
+    for (int d = 1; d <= p.ndims; ++d)
+      for (int s = 1; s <= 2; ++s) {
+        double* out = qs + N * ((size_t)(s - 1) + 2 * (size_t)(d - 1));
+        for (int k = 1; k <= km; ++k)
+          for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) {
+              bool g = (i <= ib) || (i >= ie) || (j <= jb) || (j >= je);
+              if (p.ndims == 3) g = g || (k <= kb) || (k >= ke);
+              if (g) {
+                size_t o = (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1));
+                out[o] = qv[o];
+              }
+            }
+      }
+  }
+
+  // reconstruct_tvd src/interpolations.F90:1396-1451 (line form)
+  void reconstruct_tvd(int n, const double* f, double* fl, double* fr) const {
+    for (int i = 2; i <= n - 1; ++i) {
+      double dfl = f[i - 1] - f[i - 2];
+      double dfr = f[i] - f[i - 1];
+      double df = limiter(p.lim, 0.5, dfl, dfr);
+      fl[i - 1] = f[i - 1] + df;
+      fr[i - 2] = f[i - 1] - df;
+    }
+    int i = n - 1;
+    fl[0] = 0.5 * (f[0] + f[1]);
+    fr[i - 1] = 0.5 * (f[i - 1] + f[n - 1]);
+    fl[n - 1] = f[n - 1];
+    fr[n - 1] = f[n - 1];
+  }
+
+  // reconstruct_weno5z src/interpolations.F90:1937-2083
+  void reconstruct_weno5z(int n, const double* fv, double* flv, double* frv) const {
+    std::vector<double> dfm(n + 1), dfp(n + 1), df2(n + 1);
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto fl = [&](int i) -> double& { return flv[i - 1]; };
+    auto fr = [&](int i) -> double& { return frv[i - 1]; };
+    const double c1 = 13.0 / 12.0, c2 = 0.25;
+    const double dl = 0.1, dc = 0.6, dr = 0.3;
+    const double a11 = 2.0 / 6.0, a12 = -7.0 / 6.0, a13 = 11.0 / 6.0;
+    const double a21 = -1.0 / 6.0, a22 = 5.0 / 6.0, a23 = 2.0 / 6.0;
+    const double a31 = 2.0 / 6.0, a32 = 5.0 / 6.0, a33 = -1.0 / 6.0;
+    const double eps = p.eps;
+    for (int i = 1; i <= n - 1; ++i) { dfp[i] = f(i + 1) - f(i); dfm[i + 1] = dfp[i]; }
+    dfm[1] = dfp[1];
+    dfp[n] = dfm[n];
+    for (int i = 1; i <= n; ++i) { double t = dfp[i] - dfm[i]; df2[i] = c1 * (t * t); }
+    for (int i = 3; i <= n - 2; ++i) {
+      int im2 = i - 2, im1 = i - 1, ip1 = i + 1, ip2 = i + 2;
+      double t;
+      t = 3.0 * dfm[i] - dfm[im1]; double bl = df2[im1] + c2 * (t * t);
+      t = dfp[i] + dfm[i];         double bc = df2[i] + c2 * (t * t);
+      t = 3.0 * dfp[i] - dfp[ip1]; double br = df2[ip1] + c2 * (t * t);
+      double tt = std::fabs(br - bl);
+      double al = 1.0 + tt / (bl + eps);
+      double ac = 1.0 + tt / (bc + eps);
+      double ar = 1.0 + tt / (br + eps);
+      double wl = dl * al, wc = dc * ac, wr = dr * ar;
+      double ww = (wl + wr) + wc;
+      wl = wl / ww; wr = wr / ww; wc = 1.0 - (wl + wr);
+      double ql = a11 * f(im2) + a12 * f(im1) + a13 * f(i);
+      double qc = a21 * f(im1) + a22 * f(i) + a23 * f(ip1);
+      double qr = a31 * f(i) + a32 * f(ip1) + a33 * f(ip2);
+      fl(i) = (wl * ql + wr * qr) + wc * qc;
+      wl = dl * ar; wc = dc * ac; wr = dr * al;
+      ww = (wl + wr) + wc;
+      wl = wl / ww; wr = wr / ww; wc = 1.0 - (wl + wr);
+      ql = a11 * f(ip2) + a12 * f(ip1) + a13 * f(i);
+      qc = a21 * f(ip1) + a22 * f(i) + a23 * f(im1);
+      qr = a31 * f(i) + a32 * f(im1) + a33 * f(im2);
+      fr(im1) = (wl * ql + wr * qr) + wc * qc;
+    }
+    fl(1) = 0.5 * (f(1) + f(2));
+    double df = limiter(p.lim, 0.5, dfm[2], dfp[2]);
+    fr(1) = f(2) - df;
+    fl(2) = f(2) + df;
+    int i = n - 1;
+    df = limiter(p.lim, 0.5, dfm[i], dfp[i]);
+    fr(i - 1) = f(i) - df;
+    fl(i) = f(i) + df;
+    fr(i) = 0.5 * (f(i) + f(n));
+    fl(n) = f(n);
+    fr(n) = f(n);
+  }
+
+  // clip_extrema src/interpolations.F90:5081-5175
+  void clip_extrema(int n, const double* f, double* fl, double* fr) const {
+    for (int i = 1; i <= n; ++i) {
+      int im1 = std::max(1, i - 1), ip1 = std::min(n, i + 1);
+      double fmn = fmin2(f[i - 1], f[ip1 - 1]);
+      double fmx = fmax2(f[i - 1], f[ip1 - 1]);
+      if (fl[i - 1] < fmn || fl[i - 1] > fmx) {
+        double dfl = f[i - 1] - f[im1 - 1];
+        double dfr = f[ip1 - 1] - f[i - 1];
+        double df = limiter(p.clim, 0.5, dfl, dfr);
+        fl[i - 1] = f[i - 1] + df;
+        fr[im1 - 1] = f[i - 1] - df;
+      }
+      if (fr[i - 1] < fmn || fr[i - 1] > fmx) {
+        int ip2 = std::min(n, i + 2);
+        double dfl = f[ip1 - 1] - f[i - 1];
+        double dfr = f[ip2 - 1] - f[ip1 - 1];
+        double df = limiter(p.clim, 0.5, dfl, dfr);
+        fl[ip1 - 1] = f[ip1 - 1] + df;
+        fr[i - 1] = f[ip1 - 1] - df;
+      }
+    }
+  }
+
+  // fix_positivity src/interpolations.F90:4987-5062
+  void fix_positivity(int n, const double* f, double* fl, double* fr) const {
+    if (!p.positivity) return;
+    for (int i = 1; i <= n; ++i) {
+      if (fl[i - 1] <= 0.0) {
+        int im1 = std::max(1, i - 1);
+        fl[i - 1] = f[i - 1];
+        fr[im1 - 1] = f[i - 1];
+      }
+      if (fr[i - 1] <= 0.0) {
+        int ip1 = std::min(n, i + 1);
+        fl[ip1 - 1] = f[ip1 - 1];
+        fr[i - 1] = f[ip1 - 1];
+      }
+    }
+  }
+
+  // reconstruct src/interpolations.F90:1343-1381
+  void reconstruct(int n, const double* f, double* fl, double* fr) const {
+    if (p.rec == REC_WENO5Z) reconstruct_weno5z(n, f, fl, fr);
+    else reconstruct_tvd(n, f, fl, fr);
+    if (p.clip) clip_extrema(n, f, fl, fr);
+  }
+
+  // interfaces_dir src/interpolations.F90:867-959
+  void interfaces_dir(bool positive, const double* qv, double* qs) {
+    const size_t N = cells();
+    ghost_copy(qv, qs);
+    std::vector<double> f(std::max(im, std::max(jm, km))), fl(f.size()), fr(f.size());
+    auto line = [&](int d, int i0, int j0, int k0, bool pos_pass) {
+      int n = d == 1 ? im : (d == 2 ? jm : km);
+      size_t stride = d == 1 ? 1 : (d == 2 ? (size_t)im : (size_t)im * jm);
+      size_t base = (size_t)(i0 - 1) + (size_t)im * ((size_t)(j0 - 1) + (size_t)jm * (k0 - 1));
+      double* ql = qs + N * (0 + 2 * (size_t)(d - 1));
+      double* qr = qs + N * (1 + 2 * (size_t)(d - 1));
+      for (int t = 0; t < n; ++t) f[t] = qv[base + t * stride];
+      if (!pos_pass) {
+        reconstruct(n, f.data(), fl.data(), fr.data());
+      } else {
+        for (int t = 0; t < n; ++t) { fl[t] = ql[base + t * stride]; fr[t] = qr[base + t * stride]; }
+        fix_positivity(n, f.data(), fl.data(), fr.data());
+      }
+      for (int t = 0; t < n; ++t) { ql[base + t * stride] = fl[t]; qr[base + t * stride] = fr[t]; }
+    };
+    for (int pass = 0; pass < (positive ? 2 : 1); ++pass) {
+      bool pp = pass == 1;
+      for (int k = kbl; k <= keu; ++k) {
+        for (int j = jbl; j <= jeu; ++j) line(1, 1, j, k, pp);
+        for (int i = ibl; i <= ieu; ++i) line(2, i, 1, k, pp);
+      }
+      if (p.ndims == 3)
+        for (int j = jbl; j <= jeu; ++j)
+          for (int i = ibl; i <= ieu; ++i) line(3, i, j, 1, pp);
+    }
+  }
+
+  // =========================================================================
+  // SCHEMES
+  // =========================================================================
+  // GLM averaging of Bx and psi (src/schemes.F90:3196-3215 and the same
+  // block in every MHD solver)
+  void glm(double* ql, double* qr) const {
+    double bx = 0.5 * ((qr[ibx - 1] + ql[ibx - 1]) - (qr[ibp - 1] - ql[ibp - 1]) / cmax);
+    double bp = 0.5 * ((qr[ibp - 1] + ql[ibp - 1]) - (qr[ibx - 1] - ql[ibx - 1]) * cmax);
+    ql[ibx - 1] = bx; qr[ibx - 1] = bx; ql[ibp - 1] = bp; qr[ibp - 1] = bp;
+  }
+
+  // One interface of the selected Riemann solver.  ql/qr are modified like
+  // the Fortran intent(inout) arrays (GLM averaging).
+  void riemann_point(double* ql, double* qr, double* f) const {
+    const int N = nv;
+    double ul[9], ur[9], fl[9], fr[9], wl[9], wr[9], ui[9], wcl[9], wcr[9];
+    double clm, clp, crm, crp;
+    if (p.eqsys == EQ_MHD) glm(ql, qr);
+    prim2cons(1, ql, ul); prim2cons(1, qr, ur);
+    if (p.rs == RS_ROE) {
+      fluxspeed(1, ql, ul, fl, nullptr, nullptr);
+      fluxspeed(1, qr, ur, fr, nullptr, nullptr);
+      roe_point(ql, qr, ul, ur, fl, fr, f);
+      return;
+    }
+    fluxspeed(1, ql, ul, fl, &clm, &clp);
+    fluxspeed(1, qr, ur, fr, &crm, &crp);
+    double sl = fmin2(clm, crm), sr = fmax2(clp, crp);
+    if (sl >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
+    if (sr <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
+    double srml = sr - sl;
+    for (int v = 0; v < N; ++v) { wl[v] = sl * ul[v] - fl[v]; wr[v] = sr * ur[v] - fr[v]; }
+    auto hll = [&]() { for (int v = 0; v < N; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml; };
+    const int Dn = idn - 1, Mx = imx - 1, My = imy - 1, Mz = imz - 1, En = ien - 1;
+    if (p.rs == RS_HLL) { hll(); return; }
+    if (p.eqsys == EQ_HD) {
+      // riemann_hd_adi_hllc src/schemes.F90:1366-1513
+      double dn = wr[Dn] - wl[Dn];
+      double sm = (wr[Mx] - wl[Mx]) / dn;
+      double pr = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn;
+      if (sm > 0.0) {
+        double slmm = sl - sm;
+        ui[Dn] = wl[Dn] / slmm;
+        ui[Mx] = ui[Dn] * sm;
+        ui[My] = ui[Dn] * ql[ivy - 1];
+        ui[Mz] = ui[Dn] * ql[ivz - 1];
+        ui[En] = (wl[En] + sm * pr) / slmm;
+        for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+      } else if (sm < 0.0) {
+        double srmm = sr - sm;
+        ui[Dn] = wr[Dn] / srmm;
+        ui[Mx] = ui[Dn] * sm;
+        ui[My] = ui[Dn] * qr[ivy - 1];
+        ui[Mz] = ui[Dn] * qr[ivz - 1];
+        ui[En] = (wr[En] + sm * pr) / srmm;
+        for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        f[Dn] = 0.0; f[Mx] = -wl[Mx]; f[My] = 0.0; f[Mz] = 0.0; f[En] = 0.0;
+      }
+      return;
+    }
+    const int Bx = ibx - 1, By = iby - 1, Bz = ibz - 1, Bp = ibp - 1;
+    if (p.rs == RS_HLLC) {
+      // riemann_mhd_adi_hllc src/schemes.F90:3305-3571
+      double dn = wr[Dn] - wl[Dn];
+      double sm = (wr[Mx] - wl[Mx]) / dn;
+      double bx = ql[Bx];
+      double b2 = ql[Bx] * qr[Bx];
+      if (b2 > 0.0) {
+        double pt = 0.5 * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx])) + b2;
+        double vy = (wr[My] - wl[My]) / dn;
+        double vz = (wr[Mz] - wl[Mz]) / dn;
+        double by = (wr[By] - wl[By]) / srml;
+        double bz = (wr[Bz] - wl[Bz]) / srml;
+        double vb = sm * bx + vy * by + vz * bz;
+        if (sm > 0.0) {
+          double slmm = sl - sm;
+          ui[Dn] = wl[Dn] / slmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * vy; ui[Mz] = ui[Dn] * vz;
+          ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ql[Bp];
+          ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+          for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+        } else if (sm < 0.0) {
+          double srmm = sr - sm;
+          ui[Dn] = wr[Dn] / srmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * vy; ui[Mz] = ui[Dn] * vz;
+          ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = qr[Bp];
+          ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+          for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+        } else {
+          hll();
+        }
+      } else {
+        double pt = 0.5 * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx]));
+        if (sm > 0.0) {
+          double slmm = sl - sm;
+          ui[Dn] = wl[Dn] / slmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * ql[ivy - 1]; ui[Mz] = ui[Dn] * ql[ivz - 1];
+          ui[Bx] = 0.0; ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm; ui[Bp] = ql[Bp];
+          ui[En] = (wl[En] + sm * pt) / slmm;
+          for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+        } else if (sm < 0.0) {
+          double srmm = sr - sm;
+          ui[Dn] = wr[Dn] / srmm; ui[Mx] = ui[Dn] * sm; ui[My] = ui[Dn] * qr[ivy - 1]; ui[Mz] = ui[Dn] * qr[ivz - 1];
+          ui[Bx] = 0.0; ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm; ui[Bp] = qr[Bp];
+          ui[En] = (wr[En] + sm * pt) / srmm;
+          for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+        } else {
+          f[Dn] = 0.0; f[Mx] = -0.5 * (wl[Mx] + wr[Mx]); f[My] = 0.0; f[Mz] = 0.0;
+          f[Bx] = fl[Bx]; f[By] = 0.0; f[Bz] = 0.0; f[Bp] = fl[Bp]; f[En] = 0.0;
+        }
+      }
+      return;
+    }
+    // riemann_mhd_adi_hlld src/schemes.F90:3596-4203
+    double dn = wr[Dn] - wl[Dn];
+    double sm = (wr[Mx] - wl[Mx]) / dn;
+    double slmm = sl - sm, srmm = sr - sm;
+    double dnl = wl[Dn] / slmm, dnr = wr[Dn] / srmm;
+    double bx = ql[Bx];
+    double b2 = ql[Bx] * qr[Bx];
+    double pt = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn + b2;
+    double vy, vz, by, bz, vb, dv;
+    double dvl_ = 0.0, dvr_ = 0.0;
+    auto outer_left = [&]() {
+      vy = (slmm * wl[My] - bx * wl[By]) / dvl_;
+      vz = (slmm * wl[Mz] - bx * wl[Bz]) / dvl_;
+      by = (wl[Dn] * wl[By] - bx * wl[My]) / dvl_;
+      bz = (wl[Dn] * wl[Bz] - bx * wl[Mz]) / dvl_;
+      vb = sm * bx + vy * by + vz * bz;
+      ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+      ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+      ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+    };
+    auto outer_right = [&]() {
+      vy = (srmm * wr[My] - bx * wr[By]) / dvr_;
+      vz = (srmm * wr[Mz] - bx * wr[Bz]) / dvr_;
+      by = (wr[Dn] * wr[By] - bx * wr[My]) / dvr_;
+      bz = (wr[Dn] * wr[Bz] - bx * wr[Mz]) / dvr_;
+      vb = sm * bx + vy * by + vz * bz;
+      ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+      ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+      ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+    };
+    (void)dv;
+    if (b2 > 1.0e-08 * fmax2(dnl * (sl * sl), dnr * (sr * sr))) {
+      double cal = std::sqrt(b2 / dnl), car = std::sqrt(b2 / dnr);
+      double sml = sm - cal, smr = sm + car;
+      dvl_ = slmm * wl[Dn] - b2;
+      dvr_ = srmm * wr[Dn] - b2;
+      if (dvl_ > 0.0 && dvr_ > 0.0) {
+        if (sml >= 0.0) {
+          outer_left();
+          for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+        } else if (smr <= 0.0) {
+          outer_right();
+          for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+        } else {
+          outer_left();
+          for (int v = 0; v < N; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+          outer_right();
+          for (int v = 0; v < N; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+          double dvv = car * dnr + cal * dnl;
+          vy = (wcr[My] - wcl[My]) / dvv;
+          vz = (wcr[Mz] - wcl[Mz]) / dvv;
+          dvv = car + cal;
+          by = (wcr[By] - wcl[By]) / dvv;
+          bz = (wcr[Bz] - wcl[Bz]) / dvv;
+          vb = sm * bx + vy * by + vz * bz;
+          if (sm > 0.0) {
+            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+            ui[En] = -(wcl[En] + sm * pt - bx * vb) / cal;
+            for (int v = 0; v < N; ++v) f[v] = sml * ui[v] - wcl[v];
+          } else if (sm < 0.0) {
+            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+            ui[En] = (wcr[En] + sm * pt - bx * vb) / car;
+            for (int v = 0; v < N; ++v) f[v] = smr * ui[v] - wcr[v];
+          } else {
+            for (int v = 0; v < N; ++v) f[v] = (sml * wcr[v] - smr * wcl[v]) / (smr - sml);
+          }
+        }
+      } else {
+        if (dvl_ > 0.0) {
+          outer_left();
+          if (sml >= 0.0) {
+            for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+          } else {
+            for (int v = 0; v < N; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+            double dvv = srmm * dnr + cal * dnl;
+            vy = (wr[My] - wcl[My]) / dvv;
+            vz = (wr[Mz] - wcl[Mz]) / dvv;
+            dvv = sr - sml;
+            by = (wr[By] - wcl[By]) / dvv;
+            bz = (wr[Bz] - wcl[Bz]) / dvv;
+            vb = sm * bx + vy * by + vz * bz;
+            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+            ui[En] = -(wcl[En] + sm * pt - bx * vb) / cal;
+            if (sm >= 0.0) {
+              for (int v = 0; v < N; ++v) f[v] = sml * ui[v] - wcl[v];
+            } else {
+              for (int v = 0; v < N; ++v) wcr[v] = (sm - sml) * ui[v] + wcl[v];
+              for (int v = 0; v < N; ++v) f[v] = (sm * wr[v] - sr * wcr[v]) / srmm;
+            }
+          }
+        } else if (dvr_ > 0.0) {
+          outer_right();
+          if (smr <= 0.0) {
+            for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+          } else {
+            for (int v = 0; v < N; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+            double dvv = slmm * dnl - car * dnr;
+            vy = (wl[My] - wcr[My]) / dvv;
+            vz = (wl[Mz] - wcr[Mz]) / dvv;
+            dvv = sl - smr;
+            by = (wl[By] - wcr[By]) / dvv;
+            bz = (wl[Bz] - wcr[Bz]) / dvv;
+            vb = sm * bx + vy * by + vz * bz;
+            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+            ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+            ui[En] = (wcr[En] + sm * pt - bx * vb) / car;
+            if (sm <= 0.0) {
+              for (int v = 0; v < N; ++v) f[v] = smr * ui[v] - wcr[v];
+            } else {
+              for (int v = 0; v < N; ++v) wcl[v] = (sm - smr) * ui[v] + wcr[v];
+              for (int v = 0; v < N; ++v) f[v] = (sm * wl[v] - sl * wcl[v]) / slmm;
+            }
+          }
+        } else {
+          hll();
+        }
+      }
+    } else if (b2 > 0.0) {
+      vy = (wr[My] - wl[My]) / dn;
+      vz = (wr[Mz] - wl[Mz]) / dn;
+      by = (wr[By] - wl[By]) / srml;
+      bz = (wr[Bz] - wl[Bz]) / srml;
+      vb = sm * bx + vy * by + vz * bz;
+      if (sm > 0.0) {
+        ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
+        ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
+        ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+        for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+      } else if (sm < 0.0) {
+        ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
+        ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
+        ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+        for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        hll();
+      }
+    } else {
+      if (sm > 0.0) {
+        ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = wl[My] / slmm; ui[Mz] = wl[Mz] / slmm;
+        ui[Bx] = 0.0; ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm; ui[Bp] = ul[Bp];
+        ui[En] = (wl[En] + sm * pt) / slmm;
+        for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+      } else if (sm < 0.0) {
+        ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = wr[My] / srmm; ui[Mz] = wr[Mz] / srmm;
+        ui[Bx] = 0.0; ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm; ui[Bp] = ur[Bp];
+        ui[En] = (wr[En] + sm * pt) / srmm;
+        for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        hll();
+      }
+    }
+  }
+
+  // riemann_hd_adi_roe src/schemes.F90:1541-1661 and
+  // riemann_mhd_adi_roe src/schemes.F90:4230-4410 (after prim2cons/fluxspeed)
+  void roe_point(const double* ql, const double* qr, const double* ul, const double* ur,
+                 const double* fl, const double* fr, double* f) const {
+    const int N = nv;
+    double qi_[9], ci[9], al[9], li[81], ri[81];
+    double sdl = std::sqrt(ql[idn - 1]), sdr = std::sqrt(qr[idn - 1]), sds = sdl + sdr;
+    if (p.eqsys == EQ_HD) {
+      qi_[idn - 1] = sdl * sdr;
+      qi_[ivx - 1] = (sdl * ql[ivx - 1] + sdr * qr[ivx - 1]) / sds;
+      qi_[ivy - 1] = (sdl * ql[ivy - 1] + sdr * qr[ivy - 1]) / sds;
+      qi_[ivz - 1] = (sdl * ql[ivz - 1] + sdr * qr[ivz - 1]) / sds;
+      qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1]) / sdl + (ur[ien - 1] + qr[ipr - 1]) / sdr) / sds;
+      esystem_roe_hd(qi_, ci, li, ri);
+      if (ci[0] >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
+      if (ci[N - 1] <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
+      for (int v = 0; v < N; ++v) al[v] = 0.0;
+      for (int pp = 0; pp < N; ++pp)
+        for (int v = 0; v < N; ++v) al[v] = al[v] + li[pp + N * v] * (ur[pp] - ul[pp]);
+      for (int v = 0; v < N; ++v) f[v] = 0.5 * (fl[v] + fr[v]);
+      if (qi_[ivx - 1] >= 0.0) {
+        for (int pp = 0; pp < N; ++pp) {
+          double xx = -0.5 * al[pp] * std::fabs(ci[pp]);
+          for (int v = 0; v < N; ++v) f[v] = f[v] + xx * ri[pp + N * v];
+        }
+      } else {
+        for (int pp = N - 1; pp >= 0; --pp) {
+          double xx = -0.5 * al[pp] * std::fabs(ci[pp]);
+          for (int v = 0; v < N; ++v) f[v] = f[v] + xx * ri[pp + N * v];
+        }
+      }
+      return;
+    }
+    double pml = 0.5 * (ql[ibx - 1] * ql[ibx - 1] + ql[iby - 1] * ql[iby - 1] + ql[ibz - 1] * ql[ibz - 1]);
+    double pmr = 0.5 * (qr[ibx - 1] * qr[ibx - 1] + qr[iby - 1] * qr[iby - 1] + qr[ibz - 1] * qr[ibz - 1]);
+    qi_[idn - 1] = sdl * sdr;
+    qi_[ivx - 1] = (sdl * ql[ivx - 1] + sdr * qr[ivx - 1]) / sds;
+    qi_[ivy - 1] = (sdl * ql[ivy - 1] + sdr * qr[ivy - 1]) / sds;
+    qi_[ivz - 1] = (sdl * ql[ivz - 1] + sdr * qr[ivz - 1]) / sds;
+    qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1] + pml) / sdl + (ur[ien - 1] + qr[ipr - 1] + pmr) / sdr) / sds;
+    qi_[ibx - 1] = ql[ibx - 1];
+    qi_[iby - 1] = (sdr * ql[iby - 1] + sdl * qr[iby - 1]) / sds;
+    qi_[ibz - 1] = (sdr * ql[ibz - 1] + sdl * qr[ibz - 1]) / sds;
+    qi_[ibp - 1] = ql[ibp - 1];
+    double t1 = ql[iby - 1] - qr[iby - 1], t2 = ql[ibz - 1] - qr[ibz - 1];
+    double xx = 0.5 * ((t1 * t1) + (t2 * t2)) / (sds * sds);
+    double yy = 0.5 * (ql[idn - 1] + qr[idn - 1]) / qi_[idn - 1];
+    esystem_roe_mhd(xx, yy, qi_, ci, li, ri);
+    if (ci[0] >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
+    if (ci[N - 1] <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
+    f[ibx - 1] = fl[ibx - 1];
+    f[ibp - 1] = fl[ibp - 1];
+    for (int v = 0; v < N; ++v) al[v] = 0.0;
+    for (int pp = 0; pp < N; ++pp)
+      for (int v = 0; v < N; ++v) al[v] = al[v] + li[pp + N * v] * (ur[pp] - ul[pp]);
+    const int vs[7] = {idn - 1, imx - 1, imy - 1, imz - 1, ien - 1, iby - 1, ibz - 1};
+    for (int v : vs) f[v] = 0.5 * (fl[v] + fr[v]);
+    if (qi_[ivx - 1] >= 0.0) {
+      for (int pp = 0; pp < N; ++pp) {
+        double x2 = -0.5 * al[pp] * std::fabs(ci[pp]);
+        for (int v : vs) f[v] = f[v] + x2 * ri[pp + N * v];
+      }
+    } else {
+      for (int pp = N - 1; pp >= 0; --pp) {
+        double x2 = -0.5 * al[pp] * std::fabs(ci[pp]);
+        for (int v : vs) f[v] = f[v] + x2 * ri[pp + N * v];
+      }
+    }
+  }
+
+  // Riemann on a line (riemann_iface, src/schemes.F90:66-71)
+  void riemann_line(int n, double* ql, double* qr, double* f) const {
+    for (int i = 0; i < n; ++i) riemann_point(ql + (size_t)nv * i, qr + (size_t)nv * i, f + (size_t)nv * i);
+  }
+
+  // update_flux_hd_adi src/schemes.F90:1080-1223 and update_flux_mhd_adi
+  // 2970-3138, with reconstruct_interfaces 591-633.  Directional component
+  // rotation: x:(x,y,z) y:(y,z,x) z:(z,x,y).
+  void update_flux(const double* q, double* f) {
+    const size_t N = cells();
+    std::fill(f, f + (size_t)p.ndims * nv * N, 0.0);
+    std::vector<double> qs((size_t)nv * N * 2 * p.ndims);
+    std::vector<double> one(N), ones(N * 2 * p.ndims);
+    // reconstruct_interfaces: per variable, positive = density or pressure
+    for (int pv = 1; pv <= nv; ++pv) {
+      bool positive = (pv == idn || pv == ipr);
+      for (size_t c = 0; c < N; ++c) one[c] = q[(size_t)(pv - 1) + (size_t)nv * c];
+      if (p.rec == REC_TVD) interfaces_tvd(positive, one.data(), ones.data());
+      else interfaces_dir(positive, one.data(), ones.data());
+      // scatter to qs(nv,im,jm,km,2,NDIMS)
+      for (size_t sd = 0; sd < (size_t)2 * p.ndims; ++sd)
+        for (size_t c = 0; c < N; ++c) qs[(size_t)(pv - 1) + (size_t)nv * (c + N * sd)] = ones[c + N * sd];
+    }
+    static const int perm[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+    int nmax = std::max(im, std::max(jm, km));
+    std::vector<double> ql((size_t)nv * nmax), qr((size_t)nv * nmax), fx((size_t)nv * nmax);
+    for (int d = 1; d <= p.ndims; ++d) {
+      const int* pm = perm[d - 1];
+      int n = d == 1 ? im : (d == 2 ? jm : km);
+      auto run_line = [&](int i0, int j0, int k0) {
+        for (int t = 0; t < n; ++t) {
+          int i = i0, j = j0, k = k0;
+          if (d == 1) i = t + 1; else if (d == 2) j = t + 1; else k = t + 1;
+          size_t c = (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1));
+          const double* sl_ = &qs[(size_t)nv * (c + N * (0 + 2 * (size_t)(d - 1)))];
+          const double* sr_ = &qs[(size_t)nv * (c + N * (1 + 2 * (size_t)(d - 1)))];
+          double* L = &ql[(size_t)nv * t]; double* R = &qr[(size_t)nv * t];
+          for (int v = 0; v < nv; ++v) { L[v] = sl_[v]; R[v] = sr_[v]; }
+          for (int m = 0; m < 3; ++m) { L[ivx - 1 + m] = sl_[ivx - 1 + pm[m]]; R[ivx - 1 + m] = sr_[ivx - 1 + pm[m]]; }
+          if (p.eqsys == EQ_MHD)
+            for (int m = 0; m < 3; ++m) { L[ibx - 1 + m] = sl_[ibx - 1 + pm[m]]; R[ibx - 1 + m] = sr_[ibx - 1 + pm[m]]; }
+        }
+        riemann_line(n, ql.data(), qr.data(), fx.data());
+        for (int t = 0; t < n; ++t) {
+          int i = i0, j = j0, k = k0;
+          if (d == 1) i = t + 1; else if (d == 2) j = t + 1; else k = t + 1;
+          const double* F = &fx[(size_t)nv * t];
+          double tmp[9];
+          for (int v = 0; v < nv; ++v) tmp[v] = F[v];
+          for (int m = 0; m < 3; ++m) tmp[imx - 1 + pm[m]] = F[imx - 1 + m];
+          if (p.eqsys == EQ_MHD)
+            for (int m = 0; m < 3; ++m) tmp[ibx - 1 + pm[m]] = F[ibx - 1 + m];
+          for (int v = 0; v < nv; ++v) f[fi(d, v + 1, i, j, k)] = tmp[v];
+        }
+      };
+      if (d == 1) { for (int k = kbl; k <= keu; ++k) for (int j = jbl; j <= jeu; ++j) run_line(1, j, k); }
+      else if (d == 2) { for (int k = kbl; k <= keu; ++k) for (int i = ibl; i <= ieu; ++i) run_line(i, 1, k); }
+      else { for (int j = jbl; j <= jeu; ++j) for (int i = ibl; i <= ieu; ++i) run_line(i, j, 1); }
+    }
+  }
+
+  // =========================================================================
+  // EVOLUTION
+  // =========================================================================
+  // update_increment src/evolution.F90:1898-1977
+  void update_increment(const double* f, double* du) const {
+    std::fill(du, du + (size_t)nv * cells(), 0.0);
+    double dxi = 1.0 / dx, dyi = 1.0 / dy, dzi = 1.0 / dz;
+    for (int k = kbl; k <= keu; ++k)
+      for (int j = jbl; j <= jeu; ++j)
+        for (int i = ibl; i <= ieu; ++i)
+          for (int v = 1; v <= nv; ++v) {
+            double a = -dxi * (f[fi(1, v, i, j, k)] - f[fi(1, v, i - 1, j, k)])
+                       - dyi * (f[fi(2, v, i, j, k)] - f[fi(2, v, i, j - 1, k)]);
+            if (p.ndims == 3) a = a - dzi * (f[fi(3, v, i, j, k)] - f[fi(3, v, i, j, k - 1)]);
+            du[qi(v, i, j, k)] = a;
+          }
+  }
+
+  // update_primitive_variables src/equations.F90:1088-1148
+  void update_primitive_variables(const double* uu, double* qq) const {
+    for (int k = kb; k <= ke; ++k)
+      for (int j = jb; j <= je; ++j) cons2prim(in, uu + qi(1, ib, j, k), qq + qi(1, ib, j, k));
+    auto copyc = [&](int i, int j, int k, int i2, int j2, int k2) {
+      for (int v = 1; v <= nv; ++v) qq[qi(v, i, j, k)] = qq[qi(v, i2, j2, k2)];
+    };
+    for (int k = kb; k <= ke; ++k) for (int j = jb; j <= je; ++j) {
+      for (int i = ibl; i >= 1; --i) copyc(i, j, k, ib, j, k);
+      for (int i = ieu; i <= im; ++i) copyc(i, j, k, ie, j, k);
+    }
+    for (int k = kb; k <= ke; ++k) for (int i = 1; i <= im; ++i) {
+      for (int j = jbl; j >= 1; --j) copyc(i, j, k, i, jb, k);
+      for (int j = jeu; j <= jm; ++j) copyc(i, j, k, i, je, k);
+    }
+    if (p.ndims == 3)
+      for (int j = 1; j <= jm; ++j) for (int i = 1; i <= im; ++i) {
+        for (int k = kbl; k >= 1; --k) copyc(i, j, k, i, j, kb);
+        for (int k = keu; k <= km; ++k) copyc(i, j, k, i, j, ke);
+      }
+  }
+
+  // boundary_variables src/boundaries.F90:372-479 for a uniform, periodic,
+  // single-level mesh: every ghost cell is a copy of the neighbour block's
+  // interior cell at the same position (face/edge/corner copy), followed by
+  // update_ghost_cells (src/boundaries.F90:6633-6736), i.e. prim2cons in
+  // every ghost cell of the current u.
+  void boundary_variables() {
+    const int NX = nbx * in, NY = nby * jn, NZ = nbz * kn;
+    auto gidx = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+    // ghosts of each block are written from the interiors of others only, so
+    // blocks fill in parallel
+    parallel_index(blocks.size(), [&](size_t bi) {
+          const int bx = (int)(bi % nbx), by = (int)((bi / nbx) % nby), bz = (int)(bi / ((size_t)nbx * nby));
+          Block& B = blocks[bi];
+          for (int k = 1; k <= km; ++k)
+            for (int j = 1; j <= jm; ++j)
+              for (int i = 1; i <= im; ++i) {
+                bool ghost = i < ib || i > ie || j < jb || j > je || (p.ndims == 3 && (k < kb || k > ke));
+                if (!ghost) continue;
+                int gx = gidx(bx * in + (i - ib), NX), gy = gidx(by * jn + (j - jb), NY);
+                int gz = p.ndims == 3 ? gidx(bz * kn + (k - kb), NZ) : 0;
+                int sbx = gx / in, sby = gy / jn, sbz = p.ndims == 3 ? gz / kn : 0;
+                const Block& S = blocks[sbx + (size_t)nbx * (sby + (size_t)nby * sbz)];
+                int si = gx % in + ib, sj = gy % jn + jb, sk = p.ndims == 3 ? gz % kn + kb : 1;
+                for (int v = 1; v <= nv; ++v) B.q[qi(v, i, j, k)] = S.q[qi(v, si, sj, sk)];
+              }
+    });
+    parallel_blocks([&](Block& B) {
+      for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+          for (int i = 1; i <= im; ++i) {
+            bool ghost = i < ib || i > ie || j < jb || j > je || (p.ndims == 3 && (k < kb || k > ke));
+            if (ghost) prim2cons(1, &B.q[qi(1, i, j, k)], &B.u[qi(1, i, j, k)]);
+          }
+    });
+  }
+
+  // update_variables src/evolution.F90:1994-2094 (no unphysical-cell fix,
+  // no shapes: both default off)
+  void update_variables() {
+    parallel_blocks([&](Block& B) { update_primitive_variables(B.u, B.q.data()); });
+    boundary_variables();
+  }
+
+  // new_time_step src/evolution.F90:379-493 (viscosity = resistivity = 0)
+  void new_time_step(double dtnext) {
+    const double eps = DBL_MIN;  // tiny(cmax)
+    cmax = eps;
+    std::vector<double> cms(blocks.size());
+    parallel_index(blocks.size(), [&](size_t b) { cms[b] = maxspeed(blocks[b].q.data()); });
+    for (double cm : cms) cmax = fmax2(cmax, cm);
+    cmax2 = cmax * cmax;
+    double dx_min = fmin2(dx, dy);
+    if (p.ndims == 3) dx_min = fmin2(dx_min, dz);
+    dtn = cfl * dx_min / fmax2(cmax + 2.0 * fmax2(p.viscosity, p.resistivity) / dx_min, eps);
+    if (dtnext > 0.0) dt = fmin2(dtn, dtnext);
+  }
+
+  template <class F> void parallel_index(size_t n, F fn) {
+    if (nthreads <= 1 || n < 2) { for (size_t i = 0; i < n; ++i) fn(i); return; }
+    std::vector<std::thread> th;
+    int T = std::min<int>(nthreads, (int)n);
+    for (int t = 0; t < T; ++t)
+      th.emplace_back([&, t]() { for (size_t i = t; i < n; i += T) fn(i); });
+    for (auto& x : th) x.join();
+  }
+  template <class F> void parallel_blocks(F fn) {
+    parallel_index(blocks.size(), [&](size_t b) { fn(blocks[b]); });
+  }
+
+  // update_fluxes src/evolution.F90:1807-1881 (boundary_fluxes is a no-op
+  // on a single-level mesh)
+  void update_fluxes() {
+    parallel_blocks([&](Block& B) { update_flux(B.q.data(), B.f.data()); });
+  }
+
+  // One stage: fluxes, then per block increment + combination.  `comb`
+  // receives (u0, u1, du, cell-count) of a block.
+  template <class C> void stage(C comb) {
+    update_fluxes();
+    parallel_blocks([&](Block& B) {
+      std::vector<double> du((size_t)nv * cells());
+      update_increment(B.f.data(), du.data());
+      comb(B, du.data());
+    });
+  }
+  void psi_decay(Block& B) {
+    if (ibp > 0) for (size_t c = 0; c < cells(); ++c) B.u[(size_t)(ibp - 1) + (size_t)nv * c] = decay * B.u[(size_t)(ibp - 1) + (size_t)nv * c];
+  }
+
+  // evolve_euler 517, evolve_rk2 628-770, evolve_ssprk2 791-986,
+  // evolve_rk3 1005-1208, evolve_ssprk34 1228-1472, evolve_ssprk35 1492-1793
+  // (src/evolution.F90)
+  void evolve() {
+    const size_t M = (size_t)nv * cells();
+    switch (p.ta) {
+      case TA_EULER:
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = B.u0[c] + dt * du[c];
+          B.u = B.u0.data(); psi_decay(B);
+        });
+        update_variables();
+        break;
+      case TA_RK2:
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u0[c] + dt * du[c];
+          B.u = B.u1.data();
+        });
+        update_variables();
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = 0.5 * (B.u0[c] + B.u1[c] + dt * du[c]);
+          B.u = B.u0.data(); psi_decay(B);
+        });
+        update_variables();
+        break;
+      case TA_SSPRK2: {
+        double ft = 1.0 / (p.stages - 1), fl = 1.0 / p.stages, fr = 1.0 - fl;
+        double ds = ft * dt;
+        for (auto& B : blocks) { B.u1 = B.u0; B.u = B.u1.data(); }
+        for (int n = 1; n <= p.stages - 1; ++n) {
+          stage([&](Block& B, const double* du) {
+            for (size_t c = 0; c < M; ++c) B.u1[c] = B.u1[c] + ds * du[c];
+          });
+          update_variables();
+        }
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = fl * B.u0[c] + fr * (B.u1[c] + ds * du[c]);
+          B.u = B.u0.data(); psi_decay(B);
+        });
+        update_variables();
+        break;
+      }
+      case TA_RK3: {
+        const double f21 = 3.0 / 4.0, f22 = 1.0 / 4.0, f31 = 1.0 / 3.0, f32 = 2.0 / 3.0;
+        double ds = dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u0[c] + ds * du[c];
+          B.u = B.u1.data();
+        });
+        update_variables();
+        ds = f22 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = f21 * B.u0[c] + f22 * B.u1[c] + ds * du[c];
+        });
+        update_variables();
+        ds = f32 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = f31 * B.u0[c] + f32 * B.u1[c] + ds * du[c];
+          B.u = B.u0.data(); psi_decay(B);
+        });
+        update_variables();
+        break;
+      }
+      case TA_SSPRK34: {
+        const double b1 = 1.0 / 2.0, b3 = 1.0 / 6.0, a31 = 2.0 / 3.0, a33 = 1.0 / 3.0;
+        double ds = b1 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u0[c] + ds * du[c];
+          B.u = B.u1.data();
+        });
+        update_variables();
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u1[c] + ds * du[c];
+        });
+        update_variables();
+        ds = b3 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = a31 * B.u0[c] + a33 * B.u1[c] + ds * du[c];
+        });
+        update_variables();
+        ds = b1 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = B.u1[c] + ds * du[c];
+          B.u = B.u0.data(); psi_decay(B);
+        });
+        update_variables();
+        break;
+      }
+      case TA_SSPRK35: {
+        const double b1 = 3.77268915331368e-01, b3 = 2.42995220537396e-01;
+        const double b4 = 2.38458932846290e-01, b5 = 2.87632146308408e-01;
+        const double a31 = 3.55909775063327e-01, a33 = 6.44090224936673e-01;
+        const double a41 = 3.67933791638137e-01, a44 = 6.32066208361863e-01;
+        const double a53 = 2.37593836598569e-01, a55 = 7.62406163401431e-01;
+        double ds = b1 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u0[c] + ds * du[c];
+          B.u = B.u1.data();
+        });
+        update_variables();
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = B.u1[c] + ds * du[c];
+        });
+        update_variables();
+        ds = b3 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u1[c] = a31 * B.u0[c] + a33 * B.u1[c] + ds * du[c];
+        });
+        update_variables();
+        ds = b4 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = a41 * B.u0[c] + a44 * B.u1[c] + ds * du[c];
+          B.u = B.u0.data();
+        });
+        update_variables();
+        ds = b5 * dt;
+        stage([&](Block& B, const double* du) {
+          for (size_t c = 0; c < M; ++c) B.u0[c] = a53 * B.u1[c] + a55 * B.u0[c] + ds * du[c];
+          psi_decay(B);
+        });
+        update_variables();
+        break;
+      }
+    }
+  }
+
+  // global interior field <-> blocks; global layout (nv, NX, NY, NZ)
+  template <class F> void for_global(F fn) {
+    const int NX = nbx * in, NY = nby * jn;
+    for (int bz = 0; bz < nbz; ++bz)
+      for (int by = 0; by < nby; ++by)
+        for (int bx = 0; bx < nbx; ++bx) {
+          Block& B = blocks[bx + (size_t)nbx * (by + (size_t)nby * bz)];
+          for (int k = kb; k <= ke; ++k)
+            for (int j = jb; j <= je; ++j)
+              for (int i = ib; i <= ie; ++i) {
+                size_t g = (size_t)(bx * in + i - ib) + (size_t)NX * ((size_t)(by * jn + j - jb) + (size_t)NY * (size_t)(bz * kn + k - kb));
+                fn(B, qi(1, i, j, k), g * nv);
+              }
+        }
+  }
+};
+
+}  // namespace
+
+// ===========================================================================
+// C API of the oracle (test infrastructure only)
+// ===========================================================================
+extern "C" {
+
+void* or_create(int nkeys, const char** keys, const char** values, int* iret) {
+  Oracle* o = new Oracle();
+  *iret = 0;
+  for (int i = 0; i < nkeys; ++i) {
+    int r = apply_key(o->p, keys[i], values[i]);
+    if (r) { *iret = r; delete o; return nullptr; }
+  }
+  o->setup();
+  return o;
+}
+void or_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void or_set_threads(void* h, int n) { static_cast<Oracle*>(h)->nthreads = n < 1 ? 1 : n; }
+
+int or_nv(void* h) { return static_cast<Oracle*>(h)->nv; }
+void or_dims(void* h, int* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  out[0] = o->im; out[1] = o->jm; out[2] = o->km;
+  out[3] = o->nbx * o->in; out[4] = o->nby * o->jn; out[5] = o->nbz * o->kn;
+  out[6] = o->nbx; out[7] = o->nby; out[8] = o->nbz;
+}
+void or_spacing(void* h, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  out[0] = o->dx; out[1] = o->dy; out[2] = o->dz; out[3] = o->cfl; out[4] = o->decay;
+}
+
+// Sets the interior primitive field (global layout (nv,NX,NY,NZ)), computes
+// u = prim2cons(q) in the interior, then fills ghosts like the driver's
+// boundary_variables(0, dtnext) after generate_mesh (src/driver.F90:473).
+void or_set_prim(void* h, const double* qg) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->for_global([&](Oracle::Block& B, size_t lo, size_t g) {
+    for (int v = 0; v < o->nv; ++v) B.q[lo + v] = qg[g + v];
+    o->prim2cons(1, &B.q[lo], &B.u0[lo]);
+  });
+  for (auto& B : o->blocks) B.u = B.u0.data();
+  o->boundary_variables();
+  o->time = 0.0; o->step = 0;
+}
+void or_get_prim(void* h, double* qg) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->for_global([&](Oracle::Block& B, size_t lo, size_t g) { for (int v = 0; v < o->nv; ++v) qg[g + v] = B.q[lo + v]; });
+}
+void or_get_cons(void* h, double* ug) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->for_global([&](Oracle::Block& B, size_t lo, size_t g) { for (int v = 0; v < o->nv; ++v) ug[g + v] = B.u[lo + v]; });
+}
+// Raw block arrays (Fortran layout) of block b: which 0=u0 1=u1 2=q
+void or_get_block(void* h, int b, int which, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  auto& B = o->blocks[b];
+  const std::vector<double>& a = which == 0 ? B.u0 : (which == 1 ? B.u1 : B.q);
+  std::memcpy(out, a.data(), a.size() * sizeof(double));
+}
+
+void or_new_time_step(void* h, double dtnext, double* cmax, double* dt) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->new_time_step(dtnext);
+  *cmax = o->cmax; *dt = o->dt;
+}
+// advance (src/evolution.F90:292-372, toplev==1) plus the driver's
+// time/step update (src/driver.F90:579-585)
+void or_advance(void* h, double dtnext, double* time, double* dt) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->new_time_step(dtnext);
+  o->evolve();
+  o->time = o->time + o->dt;
+  o->step += 1;
+  *time = o->time; *dt = o->dt;
+}
+void or_scalars(void* h, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  out[0] = o->time; out[1] = o->dt; out[2] = o->cmax; out[3] = (double)o->step; out[4] = (double)o->nonpositive;
+}
+
+// ---- unit-level entry points ------------------------------------------------
+void or_set_cmax(void* h, double cmax) { Oracle* o = static_cast<Oracle*>(h); o->cmax = cmax; o->cmax2 = cmax * cmax; }
+void or_prim2cons(void* h, int n, const double* q, double* u) { static_cast<Oracle*>(h)->prim2cons(n, q, u); }
+void or_cons2prim(void* h, int n, const double* u, double* q) { static_cast<Oracle*>(h)->cons2prim(n, u, q); }
+void or_fluxspeed(void* h, int n, const double* q, const double* u, double* f, double* cm, double* cp) {
+  static_cast<Oracle*>(h)->fluxspeed(n, q, u, f, cm, cp);
+}
+double or_maxspeed(void* h, const double* q) { return static_cast<Oracle*>(h)->maxspeed(q); }
+void or_riemann(void* h, int n, const double* ql, const double* qr, double* f) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::vector<double> l(ql, ql + (size_t)o->nv * n), r(qr, qr + (size_t)o->nv * n);
+  o->riemann_line(n, l.data(), r.data(), f);
+}
+void or_reconstruct(void* h, int n, const double* f, double* fl, double* fr) {
+  static_cast<Oracle*>(h)->reconstruct(n, f, fl, fr);
+}
+void or_update_flux(void* h, const double* q, double* f) { static_cast<Oracle*>(h)->update_flux(q, f); }
+
+}  // extern "C"

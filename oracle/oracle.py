@@ -1,0 +1,196 @@
+"""ctypes binding of the CPU oracle (``liboracle.so``).
+
+Test infrastructure only: tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of bench.py use it as the checker.
+The product path never imports this module.
+
+The oracle restates AMUN's per-stage update in FP64 C++ (see
+``amun_oracle.cpp`` for the file:line citations).  Parity status: unpinned by
+the reference (AMUN ships no tests or golden data and cannot be compiled
+here); the restatement is pinned by analytic invariants in tests/.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile."""
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "amun_oracle.cpp"))
+    ):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        d, i, vp = C.POINTER(C.c_double), C.c_int, C.c_void_p
+        L.or_create.restype = vp
+        L.or_create.argtypes = [i, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(i)]
+        L.or_destroy.argtypes = [vp]
+        L.or_set_threads.argtypes = [vp, i]
+        L.or_nv.argtypes = [vp]
+        L.or_nv.restype = i
+        L.or_dims.argtypes = [vp, C.POINTER(i)]
+        L.or_spacing.argtypes = [vp, d]
+        L.or_set_prim.argtypes = [vp, d]
+        L.or_get_prim.argtypes = [vp, d]
+        L.or_get_cons.argtypes = [vp, d]
+        L.or_get_block.argtypes = [vp, i, i, d]
+        L.or_new_time_step.argtypes = [vp, C.c_double, d, d]
+        L.or_advance.argtypes = [vp, C.c_double, d, d]
+        L.or_scalars.argtypes = [vp, d]
+        L.or_set_cmax.argtypes = [vp, C.c_double]
+        L.or_prim2cons.argtypes = [vp, i, d, d]
+        L.or_cons2prim.argtypes = [vp, i, d, d]
+        L.or_fluxspeed.argtypes = [vp, i, d, d, d, d, d]
+        L.or_maxspeed.argtypes = [vp, d]
+        L.or_maxspeed.restype = C.c_double
+        L.or_riemann.argtypes = [vp, i, d, d, d]
+        L.or_reconstruct.argtypes = [vp, i, d, d, d]
+        L.or_update_flux.argtypes = [vp, d, d]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """One oracle instance: a uniform periodic block mesh plus the selected
+    equations/reconstruction/Riemann/integrator (reference parameter keys)."""
+
+    def __init__(self, params: dict, threads: int = 1):
+        L = lib()
+        keys = [str(k).encode() for k in params]
+        vals = [str(v).encode() for v in params.values()]
+        ka = (C.c_char_p * len(keys))(*keys)
+        va = (C.c_char_p * len(vals))(*vals)
+        iret = C.c_int(0)
+        self.h = L.or_create(len(keys), ka, va, C.byref(iret))
+        if not self.h:
+            raise ValueError(f"oracle rejected parameters (iret={iret.value})")
+        self.L = L
+        L.or_set_threads(self.h, threads)
+        self.nv = L.or_nv(self.h)
+        dims = (C.c_int * 9)()
+        L.or_dims(self.h, dims)
+        self.im, self.jm, self.km = dims[0], dims[1], dims[2]
+        self.shape = (dims[3], dims[4], dims[5])  # NX, NY, NZ
+        self.nblocks = (dims[6], dims[7], dims[8])
+        sp = (C.c_double * 5)()
+        L.or_spacing(self.h, sp)
+        self.dx, self.dy, self.dz, self.cfl, self.decay = list(sp)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.or_destroy(h)
+            self.h = None
+
+    # global fields are (NZ, NY, NX, nv) C-order == Fortran (nv,NX,NY,NZ)
+    def field_shape(self):
+        NX, NY, NZ = self.shape
+        return (NZ, NY, NX, self.nv)
+
+    def set_prim(self, q: np.ndarray):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.field_shape())
+        self.L.or_set_prim(self.h, _p(q))
+
+    def prim(self) -> np.ndarray:
+        out = np.empty(self.field_shape())
+        self.L.or_get_prim(self.h, _p(out))
+        return out
+
+    def cons(self) -> np.ndarray:
+        out = np.empty(self.field_shape())
+        self.L.or_get_cons(self.h, _p(out))
+        return out
+
+    def new_time_step(self, dtnext: float):
+        cm, dt = C.c_double(), C.c_double()
+        self.L.or_new_time_step(self.h, dtnext, C.byref(cm), C.byref(dt))
+        return cm.value, dt.value
+
+    def advance(self, dtnext: float):
+        t, dt = C.c_double(), C.c_double()
+        self.L.or_advance(self.h, dtnext, C.byref(t), C.byref(dt))
+        return t.value, dt.value
+
+    def scalars(self) -> dict:
+        s = (C.c_double * 5)()
+        self.L.or_scalars(self.h, s)
+        return dict(time=s[0], dt=s[1], cmax=s[2], step=int(s[3]), nonpositive=int(s[4]))
+
+    # ---- unit level --------------------------------------------------------
+    def set_cmax(self, cmax: float):
+        self.L.or_set_cmax(self.h, cmax)
+
+    def prim2cons(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        u = np.empty_like(q)
+        self.L.or_prim2cons(self.h, q.size // self.nv, _p(q), _p(u))
+        return u
+
+    def cons2prim(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        q = np.empty_like(u)
+        self.L.or_cons2prim(self.h, u.size // self.nv, _p(u), _p(q))
+        return q
+
+    def fluxspeed(self, q, u):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        n = q.size // self.nv
+        f = np.empty_like(q)
+        cm, cp = np.empty(n), np.empty(n)
+        self.L.or_fluxspeed(self.h, n, _p(q), _p(u), _p(f), _p(cm), _p(cp))
+        return f, cm, cp
+
+    def maxspeed(self, qblock):
+        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        return self.L.or_maxspeed(self.h, _p(qblock))
+
+    def riemann(self, ql, qr):
+        ql = np.ascontiguousarray(ql, dtype=np.float64)
+        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        f = np.empty_like(ql)
+        self.L.or_riemann(self.h, ql.size // self.nv, _p(ql), _p(qr), _p(f))
+        return f
+
+    def reconstruct(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        fl, fr = np.empty_like(f), np.empty_like(f)
+        self.L.or_reconstruct(self.h, f.size, _p(f), _p(fl), _p(fr))
+        return fl, fr
+
+    def update_flux(self, qblock):
+        """Per-block update_flux in the Fortran layouts: q(nv,im,jm,km) given
+        as a C array of shape (km,jm,im,nv); returns f(NDIMS,nv,im,jm,km) as
+        shape (km,jm,im,nv,NDIMS)."""
+        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        nd = 3 if self.km > 1 else 2
+        f = np.zeros((self.km, self.jm, self.im, self.nv, nd))
+        self.L.or_update_flux(self.h, _p(qblock), _p(f))
+        return f
+
+    def block(self, b: int, which: str = "q"):
+        out = np.empty((self.km, self.jm, self.im, self.nv))
+        self.L.or_get_block(self.h, b, {"u0": 0, "u1": 1, "q": 2}[which], _p(out))
+        return out

@@ -1,0 +1,119 @@
+"""C ABI and host logic that need no GPU: the library loads, exports every
+symbol declared in include/amun_gpu.h, parses parameter keys like the
+reference, refuses to run without a device, and the host mesh helpers."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from amun_b200 import _native as N
+from amun_b200.mesh import UniformMesh
+from amun_b200.params import geometry, parse_parameter_text, to_native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "amun_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(amun_gpu_\w+)\s*\(", text)))
+
+
+def test_library_exports_header_symbols():
+    L = C.CDLL(N.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+
+
+def test_default_params_match_reference_defaults():
+    L = N.lib()
+    p = N.amun_params()
+    L.amun_gpu_default_params(C.byref(p))
+    # src/equations.F90:158-201, src/interpolations.F90:82,160-166,
+    # src/schemes.F90:104, src/evolution.F90:70-80
+    assert p.eqsys == N.AMUN_EQ_HD and p.reconstruction == N.AMUN_REC_TVD
+    assert p.limiter == 1 and p.riemann == 0 and p.time_advance == 1
+    assert p.cfl == 0.5 and p.alpha == 2.0 and p.eps == np.finfo(float).eps
+    assert abs(p.gamma - 5.0 / 3.0) < 1e-15 and p.ncells == 8 and p.nghosts == 2
+
+
+@pytest.mark.parametrize("key,val,field,expect", [
+    ("riemann_solver", "HLLC", "riemann", 1), ("riemann_solver", "hlld", "riemann", 2),
+    ("riemann_solver", "roe", "riemann", 3), ("riemann_solver", "whatever", "riemann", 0),
+    ("reconstruction", "WENO5-Z", "reconstruction", 1), ("limiter", "monotonized_central", "limiter", 2),
+    ("limiter", "vanalbada", "limiter", 5), ("extrema_limiter", "va", "extrema_limiter", 0),
+    ("time_advance", "SSPRK(5,3)", "time_advance", 5), ("time_advance", "rk3", "time_advance", 3),
+    ("time_advance", "unknown", "time_advance", 1), ("equation_system", "MHD", "eqsys", 1),
+    ("fix_positivity", "yes", "fix_positivity", 1), ("clip_extrema", "off", "clip_extrema", 0),
+])
+def test_set_param_aliases(key, val, field, expect):
+    L = N.lib()
+    p = N.amun_params()
+    L.amun_gpu_default_params(C.byref(p))
+    assert L.amun_gpu_set_param(C.byref(p), key.encode(), val.encode()) == 0
+    assert getattr(p, field) == expect
+
+
+@pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "iso", 110),
+                                          ("reconstruction", "nope", 200)])
+def test_set_param_reference_error_codes(key, val, code):
+    L = N.lib()
+    p = N.amun_params()
+    L.amun_gpu_default_params(C.byref(p))
+    assert L.amun_gpu_set_param(C.byref(p), key.encode(), val.encode()) == code
+
+
+def test_no_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L = N.lib()
+    p = to_native({"equation_system": "hd"})
+    rc = L.amun_gpu_init(C.byref(p))
+    assert rc == 903
+    assert b"no CUDA device" in L.amun_gpu_last_error()
+    assert L.amun_gpu_advance(0.1, None, None) != 0
+
+
+def test_parameter_text():
+    text = """
+# problem
+problem = "blast"   # comment
+gamma   = 1.6667d+00
+riemann_solver = 'hllc'
+ncells = 16
+"""
+    d = parse_parameter_text(text)
+    assert d == {"problem": "blast", "gamma": "1.6667d+00", "riemann_solver": "hllc", "ncells": "16"}
+
+
+@pytest.mark.parametrize("ndims", [2, 3])
+def test_mesh_blocks_round_trip(ndims):
+    geo = geometry(dict(ndims=ndims, ncells=8, nghosts=3, xblocks=2, yblocks=1, zblocks=1, maxlev=2))
+    m = UniformMesh(geo)
+    assert m.nblocks == (4 * 2 * (2 if ndims == 3 else 1))
+    rng = np.random.default_rng(0)
+    f = rng.normal(size=m.shape + (5,))
+    blocks = m.to_blocks(f)
+    assert blocks.shape == (m.nblocks, m.km, m.jm, m.im, 5)
+    assert np.array_equal(m.from_blocks(blocks), f)
+    # ghost cells hold the periodic neighbour's interior
+    ng, nc = m.ng, m.nc
+    b0 = blocks[0]
+    ks = slice(ng, ng + nc) if ndims == 3 else slice(0, 1)
+    assert np.array_equal(b0[ks, ng:ng + nc, 0:ng], f[:nc if ndims == 3 else 1, :nc, -ng:])
+
+
+def test_mesh_descriptors_periodic():
+    m = UniformMesh(geometry(dict(ndims=2, ncells=8, xblocks=3, yblocks=2, maxlev=1)))
+    d = m.descriptors()
+    for b in range(m.nblocks):
+        bx, by, _ = m.block_coords(b)
+        assert d[b].neighbor[13] == b
+        right = d[b].neighbor[2 + 3 * 1 + 9 * 1]
+        assert right == ((bx + 1) % 3) + 3 * by
+        assert d[b].neighbor[0] == -1 or True
+        assert all(d[b].neighbor[n] == -1 for n in range(27) if n // 9 != 1)
