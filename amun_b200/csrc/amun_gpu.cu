@@ -459,6 +459,7 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   if (nblocks <= 0 || !blocks) return fail(AMUN_E_BAD_ARGUMENT, "empty block list");
   for (int b = 0; b < nblocks; ++b) {
     for (int n = 0; n < 27; ++n) {
+      if (C.p.ndims == 2 && n / 9 != 1) continue;  // no z neighbours in 2D
       int nb = blocks[b].neighbor[n];
       if (nb >= nblocks) return fail(AMUN_E_BAD_ARGUMENT, "neighbour index out of range");
       if (nb >= 0 && blocks[nb].level != blocks[b].level)
