@@ -119,6 +119,23 @@ int cuda_fail(cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call);       \
   } while (0)
 
+// Every copy and memset goes through the library stream and completes before
+// the call returns.  (Plain cudaMemcpy/cudaMemset run on the legacy default
+// stream, which does not order against a non-blocking stream: a kernel on
+// C.stream could read a buffer whose host-to-device DMA has not finished.)
+cudaError_t h2d(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, C.stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(C.stream);
+}
+cudaError_t d2h(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(C.stream);
+}
+cudaError_t dset(void* dst, int value, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(dst, value, bytes, C.stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(C.stream);
+}
+
 bool bulk() { return C.p.precision == AMUN_FP32_BULK; }
 size_t rsize() { return bulk() ? sizeof(float) : sizeof(double); }
 
@@ -433,7 +450,7 @@ int amun_gpu_init(const amun_params* p) {
   if (!C.own_stream) CK(cudaStreamCreateWithFlags(&C.own_stream, cudaStreamNonBlocking));
   if (!C.stream) C.stream = C.own_stream;
   if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
-  CK(cudaMemset(C.sc, 0, sizeof(DevScalars)));
+  CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
   C.nv = p->eqsys == AMUN_EQ_MHD ? 9 : 5;
   C.gamma = p->gamma;
@@ -485,10 +502,10 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   CK(cudaMalloc(&C.u0, ubytes * sizeof(double)));
   CK(cudaMalloc(&C.u1, ubytes * rs));
   CK(cudaMalloc(&C.du, ubytes * rs));
-  CK(cudaMemset(C.q[0], 0, qbytes));
-  CK(cudaMemset(C.q[1], 0, qbytes));
-  CK(cudaMemset(C.u0, 0, ubytes * sizeof(double)));
-  CK(cudaMemset(C.u1, 0, ubytes * rs));
+  CK(dset(C.q[0], 0, qbytes));
+  CK(dset(C.q[1], 0, qbytes));
+  CK(dset(C.u0, 0, ubytes * sizeof(double)));
+  CK(dset(C.u1, 0, ubytes * rs));
   C.pool_bytes = (long long)(2 * qbytes + ubytes * (sizeof(double) + 2 * rs));
   std::vector<int> nbr(27 * (size_t)nblocks);
   std::vector<double> binv(3 * (size_t)nblocks);
@@ -504,8 +521,8 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   }
   CK(cudaMalloc(&C.nbr, nbr.size() * sizeof(int)));
   CK(cudaMalloc(&C.binv, binv.size() * sizeof(double)));
-  CK(cudaMemcpy(C.nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(C.binv, binv.data(), binv.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(h2d(C.nbr, nbr.data(), nbr.size() * sizeof(int)));
+  CK(h2d(C.binv, binv.data(), binv.size() * sizeof(double)));
   C.cur = 0;
   C.ms_valid = false;
   return 0;
@@ -614,7 +631,7 @@ int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt) {
   unsigned long long bits;
   double cm = h.cmax;
   memcpy(&bits, &cm, sizeof(bits));
-  CK(cudaMemcpy(&C.sc->ms_bits, &bits, sizeof(bits), cudaMemcpyHostToDevice));
+  CK(h2d(&C.sc->ms_bits, &bits, sizeof(bits)));
   if (cmax) *cmax = h.cmax;
   if (dt) *dt = h.dt;
   C.host_cmax = h.cmax;
@@ -702,7 +719,7 @@ int amun_gpu_status(amun_status* s) {
   if (!C.inited || !C.sc) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   DevScalars h;
   CK(cudaStreamSynchronize(C.stream));
-  CK(cudaMemcpy(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost));
+  CK(d2h(&h, C.sc, sizeof(h)));
   s->time = h.time; s->dt = h.dt; s->dtn = h.dtn; s->cmax = h.cmax; s->step = h.step;
   s->nonpositive = (long long)h.nonpositive;
   s->device_bytes = C.pool_bytes;
@@ -713,9 +730,9 @@ int amun_gpu_set_time(double time, double dt) {
   if (!C.inited || !C.sc) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   CK(cudaStreamSynchronize(C.stream));
   DevScalars h;
-  CK(cudaMemcpy(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost));
+  CK(d2h(&h, C.sc, sizeof(h)));
   h.time = time; h.dt = dt;
-  CK(cudaMemcpy(C.sc, &h, sizeof(h), cudaMemcpyHostToDevice));
+  CK(h2d(C.sc, &h, sizeof(h)));
   return 0;
 }
 
@@ -733,15 +750,15 @@ int amun_gpu_update_flux_block(const double* dx, const double* q, double* f) {
   CK(cudaMalloc(&df.p, cells * C.nv * nd * sizeof(double)));
   CK(cudaMalloc(&dsc.p, unit_block_flux_scratch(u)));
   CK(cudaMalloc(&dnp.p, sizeof(unsigned long long)));
-  CK(cudaMemcpy(dq.p, q, cells * C.nv * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemset(df.p, 0, cells * C.nv * nd * sizeof(double)));
-  CK(cudaMemset(dqs.p, 0, cells * C.nv * 2 * nd * sizeof(double)));
-  CK(cudaMemset(dnp.p, 0, sizeof(unsigned long long)));
+  CK(h2d(dq.p, q, cells * C.nv * sizeof(double)));
+  CK(dset(df.p, 0, cells * C.nv * nd * sizeof(double)));
+  CK(dset(dqs.p, 0, cells * C.nv * 2 * nd * sizeof(double)));
+  CK(dset(dnp.p, 0, sizeof(unsigned long long)));
   cudaError_t e = unit_block_flux(u, (const double*)dq.p, (double*)dqs.p, (double*)df.p, (double*)dsc.p,
                                   (unsigned long long*)dnp.p, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "update_flux_block");
   CK(cudaStreamSynchronize(C.stream));
-  CK(cudaMemcpy(f, df.p, cells * C.nv * nd * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(d2h(f, df.p, cells * C.nv * nd * sizeof(double)));
   return 0;
 }
 
@@ -752,12 +769,12 @@ int amun_gpu_riemann(int n, const double* ql, const double* qr, double* f) {
   size_t bytes = (size_t)n * C.nv * sizeof(double);
   DevBuf a, b, o;
   CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&b.p, bytes)); CK(cudaMalloc(&o.p, bytes));
-  CK(cudaMemcpy(a.p, ql, bytes, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b.p, qr, bytes, cudaMemcpyHostToDevice));
+  CK(h2d(a.p, ql, bytes));
+  CK(h2d(b.p, qr, bytes));
   cudaError_t e = unit_riemann(u, n, (const double*)a.p, (const double*)b.p, (double*)o.p, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "riemann");
   CK(cudaStreamSynchronize(C.stream));
-  CK(cudaMemcpy(f, o.p, bytes, cudaMemcpyDeviceToHost));
+  CK(d2h(f, o.p, bytes));
   return 0;
 }
 
@@ -768,16 +785,16 @@ static int pointwise(int op, int n, const double* x, const double* y, double* ou
   size_t bytes = (size_t)n * C.nv * sizeof(double);
   DevBuf a, b, o, m, p;
   CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&o.p, bytes));
-  CK(cudaMemcpy(a.p, x, bytes, cudaMemcpyHostToDevice));
-  if (y) { CK(cudaMalloc(&b.p, bytes)); CK(cudaMemcpy(b.p, y, bytes, cudaMemcpyHostToDevice)); }
+  CK(h2d(a.p, x, bytes));
+  if (y) { CK(cudaMalloc(&b.p, bytes)); CK(h2d(b.p, y, bytes)); }
   if (op == 2) { CK(cudaMalloc(&m.p, n * sizeof(double))); CK(cudaMalloc(&p.p, n * sizeof(double))); }
   cudaError_t e = unit_pointwise(u, op, n, (const double*)a.p, (const double*)b.p, (double*)o.p, (double*)m.p,
                                  (double*)p.p, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "pointwise");
   CK(cudaStreamSynchronize(C.stream));
-  CK(cudaMemcpy(out, o.p, bytes, cudaMemcpyDeviceToHost));
-  if (op == 2 && cm) CK(cudaMemcpy(cm, m.p, n * sizeof(double), cudaMemcpyDeviceToHost));
-  if (op == 2 && cp) CK(cudaMemcpy(cp, p.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(d2h(out, o.p, bytes));
+  if (op == 2 && cm) CK(d2h(cm, m.p, n * sizeof(double)));
+  if (op == 2 && cp) CK(d2h(cp, p.p, n * sizeof(double)));
   return 0;
 }
 
@@ -797,13 +814,13 @@ int amun_gpu_maxspeed(const double* q, double* maxspeed) {
   size_t bytes = (size_t)im * jm * km * C.nv * sizeof(double);
   DevBuf a, o;
   CK(cudaMalloc(&a.p, bytes)); CK(cudaMalloc(&o.p, sizeof(unsigned long long)));
-  CK(cudaMemcpy(a.p, q, bytes, cudaMemcpyHostToDevice));
-  CK(cudaMemset(o.p, 0, sizeof(unsigned long long)));
+  CK(h2d(a.p, q, bytes));
+  CK(dset(o.p, 0, sizeof(unsigned long long)));
   cudaError_t e = unit_maxspeed(u, (const double*)a.p, (unsigned long long*)o.p, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
   CK(cudaStreamSynchronize(C.stream));
   unsigned long long bits;
-  CK(cudaMemcpy(&bits, o.p, sizeof(bits), cudaMemcpyDeviceToHost));
+  CK(d2h(&bits, o.p, sizeof(bits)));
   double v;
   memcpy(&v, &bits, sizeof(v));
   *maxspeed = v;
@@ -815,7 +832,7 @@ int amun_gpu_set_cmax(double cmax) {
   if (C.inited && C.sc) {
     CK(cudaStreamSynchronize(C.stream));
     double v[2] = {cmax, cmax * cmax};
-    CK(cudaMemcpy(C.sc, v, sizeof(v), cudaMemcpyHostToDevice));
+    CK(h2d(C.sc, v, sizeof(v)));
   }
   return 0;
 }

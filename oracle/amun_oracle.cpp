@@ -37,7 +37,7 @@ namespace {
 // src/interpolations.F90:144-495, src/evolution.F90:115-230,
 // src/coordinates.F90:160-357).  Defaults are the reference defaults.
 // ---------------------------------------------------------------------------
-enum { EQ_HD = 0, EQ_MHD = 1 };
+enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
 enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE };
@@ -60,6 +60,10 @@ struct Params {
   int minlev = 1, maxlev = 1;
   double xmin = 0, xmax = 1, ymin = 0, ymax = 1, zmin = 0, zmax = 1;
   double viscosity = 0, resistivity = 0;
+  // relativistic recovery (src/equations.F90:184-201, 313-318)
+  double tol = 1.0e-10, pmin = 1.0e-16;
+  int nrmax = 100, nrext = 2;
+  bool states_4vec = false;
 };
 
 bool is_one_of(const std::string& s, std::initializer_list<const char*> l) {
@@ -81,10 +85,19 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "equation_system") {
     if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p.eqsys = EQ_HD;
     else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p.eqsys = EQ_MHD;
+    else if (is_one_of(v, {"srmhd", "SRMHD"})) p.eqsys = EQ_SRMHD;
     else return 100;  // src/equations.F90:830
   } else if (key == "equation_of_state") {
     if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) return 110;
-  } else if (key == "reconstruction") {
+  } else if (key == "primitive_solver") {
+    // only the 1D(W) Newton recovery is restated (src/equations.F90:5665-5788)
+    if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"})) return 110;
+  } else if (key == "tolerance") p.tol = atof(v.c_str());
+  else if (key == "nr_maxit") p.nrmax = atoi(v.c_str());
+  else if (key == "nr_extra") p.nrext = atoi(v.c_str());
+  else if (key == "pmin") p.pmin = atof(v.c_str());
+  else if (key == "state_variables") p.states_4vec = is_one_of(v, {"4vec", "4-vector", "4VEC", "4-VECTOR"});
+  else if (key == "reconstruction") {
     if (is_one_of(v, {"tvd", "TVD"})) p.rec = REC_TVD;
     else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p.rec = REC_WENO5Z;
     else return 200;  // src/interpolations.F90:382
@@ -139,6 +152,261 @@ inline double fmin2(double a, double b) { return a < b ? a : b; }
 inline double fmax2(double a, double b) { return a > b ? a : b; }
 
 // ---------------------------------------------------------------------------
+// ALGEBRA: real roots of polynomials (src/algebra.F90).  Arrays are 1-based
+// through the A()/X() accessors; Fortran integer powers x**2/x**3/x**4 are
+// the products gfortran expands them to; real powers use pow().
+// ---------------------------------------------------------------------------
+const double PI2 = 6.28318530717958647692528676655900e+00;  // src/constants.F90:40
+
+// sort src/algebra.F90:1040-1082 (straight insertion, ascending)
+void alg_sort(int n, double* x) {
+  if (n < 2) return;
+  for (int k = 2; k <= n; ++k) {
+    double y = x[k - 1];
+    int l;
+    for (l = k - 1; l >= 1; --l) {
+      if (x[l - 1] <= y) break;
+      x[l] = x[l - 1];
+    }
+    x[l] = y;  // l == 0 when the loop ran out
+  }
+}
+
+// quadratic src/algebra.F90:86-242: a(1..3) = a0, a1, a2
+int alg_quadratic(const double* a, double* x) {
+  double m = fmax2(fmax2(std::fabs(a[0]), std::fabs(a[1])), std::fabs(a[2]));
+  double b1 = a[0] / m, b2 = a[1] / m, b3 = a[2] / m;
+  int nr;
+  if (b3 != 0.0) {
+    if (b1 != 0.0) {
+      double bh = 0.5 * b2;
+      double dl = bh * bh - b3 * b1;
+      if (dl > 0.0) {
+        double dr = std::sqrt(dl);
+        if (b2 > 0.0) { double tm = -bh - dr; x[0] = tm / b3; x[1] = b1 / tm; }
+        else if (b2 < 0.0) { double tm = -bh + dr; x[0] = b1 / tm; x[1] = tm / b3; }
+        else { x[1] = dr / b3; x[0] = -x[1]; }
+        nr = 2;
+      } else if (dl == 0.0) {
+        x[0] = -0.5 * b2 / b3; x[1] = x[0]; nr = 2;
+      } else {
+        x[0] = 0.0; x[1] = 0.0; nr = 0;
+      }
+    } else {
+      double tm = -b2 / b3;
+      if (tm >= 0.0) { x[0] = 0.0; x[1] = tm; } else { x[0] = tm; x[1] = 0.0; }
+      nr = 2;
+    }
+  } else {
+    x[1] = 0.0;
+    if (b2 != 0.0) { x[0] = -b1 / b2; nr = 1; }
+    else { x[0] = 0.0; nr = 0; }
+  }
+  return nr;
+}
+
+// quadratic_normalized src/algebra.F90:269-375: x^2 + a(2) x + a(1)
+int alg_quadratic_normalized(const double* a, double* x) {
+  int nr;
+  if (a[0] != 0.0) {
+    double bh = 0.5 * a[1];
+    double dl = bh * bh - a[0];
+    if (dl > 0.0) {
+      double dr = std::sqrt(dl);
+      if (a[1] > 0.0) { double tm = bh + dr; x[0] = -a[0] / tm; x[1] = -tm; }
+      else if (a[1] < 0.0) { double tm = bh - dr; x[0] = -tm; x[1] = -a[0] / tm; }
+      else { x[0] = dr; x[1] = -dr; }
+      nr = 2;
+    } else if (dl == 0.0) {
+      x[0] = -bh; x[1] = -bh; nr = 2;
+    } else {
+      x[0] = 0.0; x[1] = 0.0; nr = 0;
+    }
+  } else {
+    x[0] = 0.0; x[1] = -a[1]; nr = 2;
+  }
+  return nr;
+}
+
+// cubic src/algebra.F90:398-614: a(1..4) = a0..a3
+int alg_cubic(const double* a, double* x) {
+  const double c0 = 1.0 / 3.0;
+  auto A = [&](int i) { return a[i - 1]; };
+  int nr;
+  if (A(4) != 0.0) {
+    if (A(1) != 0.0) {
+      double a33 = A(3) * A(3) * A(3);
+      double ac = 2.0 * a33 - 9.0 * A(4) * A(3) * A(2) + 27.0 * (A(4) * A(4)) * A(1);
+      double bc = A(3) * A(3) - 3.0 * A(4) * A(2);
+      double a2 = ac * ac;
+      double b3 = bc * bc * bc;
+      double qc = a2 - 4.0 * b3;
+      if (qc > 0.0) {
+        double cc = 0.5 * (std::sqrt(qc) + ac);
+        double dc = fsign(1.0, cc) * std::pow(std::fabs(cc), c0);
+        double ec;
+        if (cc == 0.0) {
+          ec = b3 / a2;
+          ec = 2.0 * ec * (1.0 / std::sqrt(1.0 - 4.0 * ec) + 1.0 / ac);
+        } else {
+          ec = b3 / cc;
+        }
+        ec = fsign(1.0, ec) * std::pow(std::fabs(ec), c0);
+        x[0] = -c0 * (A(3) + dc + ec) / A(4);
+        x[1] = 0.0; x[2] = 0.0;
+        nr = 1;
+      } else if (qc == 0.0) {
+        if (bc != 0.0) {
+          x[0] = 0.5 * (9.0 * A(4) * A(1) - A(3) * A(2)) / bc;
+          x[1] = x[0];
+          x[2] = (-9.0 * A(4) * A(1) + 4.0 * A(3) * A(2) - a33 / A(4)) / bc;
+          nr = 3;
+        } else {
+          x[0] = x[1] = x[2] = -c0 * A(3) / A(4);
+          nr = 3;
+        }
+      } else {
+        double th = 3.0 * A(4);
+        qc = bc / (th * th);
+        double rc = 0.5 * ac / (th * th * th);
+        double abc = std::fabs(bc);
+        double cs = fsign(0.5, ac * bc) * std::sqrt(ac * ac / (abc * abc * abc));
+        if (cs <= 1.0) {
+          th = std::acos(cs);
+          ac = -2.0 * std::sqrt(qc);
+          bc = -c0 * (A(3) / A(4));
+          x[0] = ac * std::cos(c0 * th) + bc;
+          x[1] = ac * std::cos(c0 * (th + PI2)) + bc;
+          x[2] = ac * std::cos(c0 * (th - PI2)) + bc;
+          nr = 3;
+        } else {
+          ac = -fsign(1.0, rc) * std::pow(std::fabs(rc) + std::sqrt(rc * rc - qc * qc * qc), c0);
+          if (ac != 0.0) bc = qc / ac; else bc = 0.0;
+          x[0] = (ac + bc) - c0 * (A(3) / A(4));
+          x[1] = 0.0; x[2] = 0.0;
+          nr = 1;
+        }
+      }
+    } else {
+      x[2] = 0.0;
+      nr = alg_quadratic(a + 1, x) + 1;
+    }
+  } else {
+    x[2] = 0.0;
+    nr = alg_quadratic(a, x);
+  }
+  alg_sort(nr, x);
+  return nr;
+}
+
+// cubic_normalized src/algebra.F90:636-797: x^3 + a(3) x^2 + a(2) x + a(1)
+int alg_cubic_normalized(const double* a, double* x) {
+  const double c0 = 1.0 / 3.0, c1 = 1.0 / 2.7e+01, c2 = 1.0 / 4.0;
+  auto A = [&](int i) { return a[i - 1]; };
+  int nr;
+  if (A(1) != 0.0) {
+    double ac = c0 * (A(3) * A(3) - 3.0 * A(2));
+    double bc = c1 * (2.0 * (A(3) * A(3) * A(3)) - 9.0 * A(3) * A(2) + 2.7e+01 * A(1));
+    double a3 = c1 * (ac * ac * ac);
+    double b2 = c2 * (bc * bc);
+    double qc = b2 - a3;
+    if (qc > 0.0) {
+      double sq = std::sqrt(qc);
+      double ph = -0.5 * bc + sq;
+      double aa = fsign(1.0, ph) * std::pow(std::fabs(ph), c0);
+      ph = -0.5 * bc - sq;
+      double bb = fsign(1.0, ph) * std::pow(std::fabs(ph), c0);
+      x[0] = aa + bb - (c0 * A(3));
+      x[1] = 0.0; x[2] = 0.0;
+      nr = 1;
+    } else if (qc < 0.0) {
+      double cs;
+      if (bc > 0.0) cs = -std::sqrt(b2 / a3);
+      else if (bc < 0.0) cs = std::sqrt(b2 / a3);
+      else cs = 0.0;
+      double ph = std::acos(cs);
+      double aa = 2.0 * std::sqrt(c0 * ac);
+      x[0] = aa * std::cos(c0 * (ph - PI2));
+      x[1] = aa * std::cos(c0 * ph);
+      x[2] = aa * std::cos(c0 * (ph + PI2));
+      for (int i = 0; i < 3; ++i) x[i] = x[i] - (c0 * A(3));
+      nr = 3;
+    } else {
+      if (bc > 0.0) {
+        double aa = std::sqrt(c0 * ac);
+        x[0] = -2.0 * aa; x[1] = aa; x[2] = aa;
+      } else if (bc < 0.0) {
+        double aa = std::sqrt(c0 * ac);
+        x[0] = 2.0 * aa; x[1] = -aa; x[2] = -aa;
+      } else {
+        x[0] = x[1] = x[2] = 0.0;
+      }
+      for (int i = 0; i < 3; ++i) x[i] = x[i] - (c0 * A(3));
+      nr = 3;
+    }
+  } else {
+    x[2] = 0.0;
+    nr = alg_quadratic_normalized(a + 1, x) + 1;
+  }
+  alg_sort(nr, x);
+  return nr;
+}
+
+// quartic src/algebra.F90:820-1017 (Hacke 1941): a(1..5) = a0..a4
+int alg_quartic(const double* a, double* x) {
+  auto A = [&](int i) { return a[i - 1]; };
+  int nr;
+  if (A(5) != 0.0) {
+    if (A(1) != 0.0) {
+      double a4s = A(4) * A(4), a5s = A(5) * A(5);
+      double pc = (-3.0 * a4s + 8.0 * A(5) * A(3)) / (8.0 * a5s);
+      double qc = (a4s * A(4) - 4.0 * A(5) * A(4) * A(3) + 8.0 * a5s * A(2)) / (8.0 * (a5s * A(5)));
+      double rc = (-3.0 * (a4s * a4s) + 16.0 * A(5) * a4s * A(3) - 64.0 * a5s * A(4) * A(2) +
+                   256.0 * (a5s * A(5)) * A(1)) / (256.0 * (a5s * a5s));
+      double b[4], z[3], y[2], c[3];
+      b[3] = 8.0;
+      b[2] = -4.0 * pc;
+      b[1] = -8.0 * rc;
+      b[0] = 4.0 * pc * rc - qc * qc;
+      nr = alg_cubic(b, z);
+      if (nr > 0) {
+        double zm = z[0];
+        double k2 = 2.0 * zm - pc;
+        double l2 = zm * zm - rc;
+        if (k2 > 0.0 || l2 > 0.0) {
+          double kc, lc;
+          if (k2 > l2) { kc = std::sqrt(k2); lc = 0.5 * qc / kc; }
+          else if (l2 > k2) { lc = std::sqrt(l2); kc = 0.5 * qc / lc; }
+          else { kc = std::sqrt(k2); lc = std::sqrt(l2); }
+          c[2] = 1.0; c[1] = -kc; c[0] = zm + lc;
+          int m = alg_quadratic(c, y);
+          for (int n = 1; n <= m; ++n) x[n - 1] = y[n - 1] - 0.25 * A(4) / A(5);
+          nr = m;
+          c[2] = 1.0; c[1] = kc; c[0] = zm - lc;
+          m = alg_quadratic(c, y);
+          for (int n = 1; n <= m; ++n) x[nr + n - 1] = y[n - 1] - 0.25 * A(4) / A(5);
+          nr = nr + m;
+          for (int n = nr + 1; n <= 4; ++n) x[n - 1] = 0.0;
+        } else {
+          x[0] = x[1] = x[2] = x[3] = 0.0;
+          nr = 0;
+        }
+      } else {
+        x[0] = x[1] = x[2] = x[3] = 0.0;
+      }
+    } else {
+      x[3] = 0.0;
+      nr = alg_cubic(a + 1, x) + 1;
+    }
+  } else {
+    x[3] = 0.0;
+    nr = alg_cubic(a, x);
+  }
+  alg_sort(nr, x);
+  return nr;
+}
+
+// ---------------------------------------------------------------------------
 // The oracle state: equation constants, coordinates and the block data.
 // ---------------------------------------------------------------------------
 struct Oracle {
@@ -146,8 +414,9 @@ struct Oracle {
   // equation indices (src/equations.F90:335-485), 1-based
   int nv = 5, idn = 1, ivx = 2, ivy = 3, ivz = 4, imx = 2, imy = 3, imz = 4;
   int ibx = -1, iby = -1, ibz = -1, ibp = -1, ipr = 5, ien = 5;
-  double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5;
+  double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5, gammaxi = 0.4;
   double cmax = 0.0, cmax2 = 0.0;
+  mutable std::atomic<long> c2p_failures{0};  // failed relativistic recoveries (p set to 0)
   // evolution (src/evolution.F90:60-90)
   double cfl = 0.5, decay = 1.0, time = 0.0, dt = 0.0, dtn = 1.0;
   long step = 0;
@@ -181,7 +450,10 @@ struct Oracle {
       ibx = 5; iby = 6; ibz = 7; ibp = 8; ipr = ien = 9;
     }
     if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
+    // SRMHD offers HLL and HLLC only (src/schemes.F90:472-498)
+    if (p.eqsys == EQ_SRMHD && p.rs != RS_HLLC) p.rs = RS_HLL;
     gamma = p.gamma; gammam1 = gamma - 1.0; gammam1i = 1.0 / gammam1;
+    gammaxi = gammam1 / gamma;
     // evolution: CFL rescale and decay (src/evolution.F90:164-213)
     cfl = p.cfl;
     if (p.ta == TA_SSPRK2) { p.stages = std::max(2, std::min(9, p.stages)); cfl = (p.stages - 1) * cfl; }
@@ -212,10 +484,278 @@ struct Oracle {
   }
 
   // =========================================================================
+  // SPECIAL RELATIVISTIC MHD (adiabatic)
+  // =========================================================================
+  // prim2cons_srmhd_adi src/equations.F90:4590-4653
+  void prim2cons_sr(const double* Q, double* U) const {
+    double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+    double bb = Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1];
+    double vb = Q[ivx - 1] * Q[ibx - 1] + Q[ivy - 1] * Q[iby - 1] + Q[ivz - 1] * Q[ibz - 1];
+    double vm = 1.0 - vv;
+    double vs = std::sqrt(vm);
+    double ww = (Q[idn - 1] + Q[ipr - 1] / gammaxi) / vm;
+    double wt = ww + bb;
+    U[idn - 1] = Q[idn - 1] / vs;
+    U[imx - 1] = wt * Q[ivx - 1] - vb * Q[ibx - 1];
+    U[imy - 1] = wt * Q[ivy - 1] - vb * Q[iby - 1];
+    U[imz - 1] = wt * Q[ivz - 1] - vb * Q[ibz - 1];
+    U[ibx - 1] = Q[ibx - 1];
+    U[iby - 1] = Q[iby - 1];
+    U[ibz - 1] = Q[ibz - 1];
+    U[ibp - 1] = Q[ibp - 1];
+    U[ien - 1] = wt - Q[ipr - 1] - U[idn - 1] - 0.5 * (vm * bb + vb * vb);
+  }
+
+  // nr_function_srmhd_adi_1d src/equations.F90:5371-5424
+  void nr_function(double mm, double bb, double mb, double en, double dn, double w, double& f, double* df) const {
+    double ww = w * w;
+    double wt = w + bb;
+    double wd = wt * wt;
+    double ss = mb * mb;
+    double sw = ss / ww;
+    double ws = (w + wt) * sw;
+    double fn = (mm * bb - ss) / wd;
+    double dv = wd - mm - ws;
+    double ds = std::sqrt(dv);
+    double gm2 = wd / dv;
+    double gm = wt / ds;
+    double pr = gammaxi * (w - gm * dn) / gm2;
+    f = w - pr - en + 0.5 * (bb + fn);
+    if (df) {
+      double dg = (1.0 - wt * (wt - sw + ws / w) / dv) / ds;
+      double dp = gammaxi * (1.0 - (2.0 * w / gm - dn) * dg) / gm2;
+      *df = 1.0 - dp - fn / wt;
+    }
+  }
+  // nr_pressure_srmhd_adi_1d src/equations.F90:5314-5347
+  void nr_pressure(double mm, double bb, double mb, double en, double w, double& pp, double& dp) const {
+    double wt = w + bb;
+    double wd = wt * wt;
+    double ss = mb * mb;
+    double fn = (mm * bb - ss) / wd;
+    pp = w - en + 0.5 * (bb + fn);
+    dp = 1.0 - fn / wt;
+  }
+  // nr_velocity_srmhd_adi_1d src/equations.F90:5249-5286
+  double nr_velocity(double mm, double bb, double mb, double w) const {
+    double ss = mb * mb;
+    double ww = w * w;
+    double wt = w + bb;
+    double wt2 = wt * wt;
+    return (mm * ww + (w + wt) * ss) / (ww * wt2);
+  }
+
+  // nr_initial_brackets_srmhd_adi src/equations.F90:5459-5635
+  bool nr_initial_brackets(double mm, double bb, double mb, double en, double dn, double& wl, double& wu,
+                           double& wc, double& fl, double& fu) const {
+    double dd = dn * dn;
+    double ss = mb * mb;
+    double ec = en + p.pmin;
+    wu = en + p.pmin;
+    double a[5], x[4];
+    a[2] = 2.5 * bb - ec;
+    a[1] = 2.0 * (bb - ec) * bb;
+    a[0] = 0.5 * (((bb - 2.0 * ec) * bb + mm) * bb - ss);
+    int nr = alg_cubic_normalized(a, x);
+    if (nr > 0) {
+      wl = x[nr - 1];
+      a[4] = 1.0;
+      a[3] = 2.0 * bb;
+      a[2] = bb * bb - dd - mm;
+      a[1] = -2.0 * (ss + dd * bb);
+      a[0] = -(ss + dd * bb) * bb;
+      nr = alg_quartic(a, x);
+      if (nr > 0) wl = fmax2(wl, x[nr - 1]);
+    } else {
+      bool keep = true;
+      int it = p.nrmax;
+      wl = wu;
+      while (keep) {
+        double f, df;
+        nr_pressure(mm, bb, mb, ec, wl, f, df);
+        double dw = f / df;
+        wl = wl - dw;
+        double err = std::fabs(dw / wl);
+        it = it - 1;
+        keep = (err > p.tol) && it > 0;
+      }
+    }
+    nr_function(mm, bb, mb, en, dn, wl, fl, nullptr);
+    if (fl <= 0.0) {
+      if (wu <= wl) wu = 2.0 * wl;
+      nr_function(mm, bb, mb, en, dn, wu, fu, nullptr);
+      int it = p.nrmax;
+      bool keep = fl * fu > 0.0;
+      while (keep) {
+        it = it - 1;
+        wl = wu;
+        fl = fu;
+        wu = 2.0 * wu;
+        nr_function(mm, bb, mb, en, dn, wu, fu, nullptr);
+        keep = (fl * fu > 0.0) && it > 0;
+      }
+      if (it > 0 && fu >= 0.0) {
+        wc = wl - fl * (wu - wl) / (fu - fl);
+        return true;
+      }
+      return false;
+    }
+    return false;
+  }
+
+  // nr_iterate_srmhd_adi_1dw src/equations.F90:5665-5788
+  bool nr_iterate_1dw(double mm, double bb, double mb, double en, double dn, double& w, double& vv) const {
+    double wl, wu, fl, fu;
+    if (!nr_initial_brackets(mm, bb, mb, en, dn, wl, wu, w, fl, fu)) return false;
+    bool keep = true;
+    int it = p.nrmax, cn = p.nrext;
+    while (keep) {
+      double f, df;
+      nr_function(mm, bb, mb, en, dn, w, f, &df);
+      if (f > fl && f < 0.0) { wl = w; fl = f; }
+      if (f < fu && f > 0.0) { wu = w; fu = f; }
+      double dw = f / df;
+      w = w - dw;
+      double err = std::fabs(dw / w);
+      if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+      else keep = it > 0;
+      if (w < wl || w > wu) w = 0.5 * (wl + wu);
+      it = it - 1;
+    }
+    vv = nr_velocity(mm, bb, mb, w);
+    return true;
+  }
+
+  // cons2prim_srmhd_adi src/equations.F90:4671-4790.  On failure only the
+  // pressure is set (to zero); the other entries of q keep their values.
+  void cons2prim_sr(const double* U, double* Q) const {
+    double mm = U[imx - 1] * U[imx - 1] + U[imy - 1] * U[imy - 1] + U[imz - 1] * U[imz - 1];
+    double mb = U[imx - 1] * U[ibx - 1] + U[imy - 1] * U[iby - 1] + U[imz - 1] * U[ibz - 1];
+    double bb = U[ibx - 1] * U[ibx - 1] + U[iby - 1] * U[iby - 1] + U[ibz - 1] * U[ibz - 1];
+    double en = U[ien - 1] + U[idn - 1];
+    double dn = U[idn - 1];
+    double w = 0.0, vv = 0.0;
+    if (nr_iterate_1dw(mm, bb, mb, en, dn, w, vv)) {
+      double vm = 1.0 - vv;
+      double vs = std::sqrt(vm);
+      double wt = w + bb;
+      double fc = mb / w;
+      Q[idn - 1] = dn * vs;
+      Q[ivx - 1] = (U[imx - 1] + fc * U[ibx - 1]) / wt;
+      Q[ivy - 1] = (U[imy - 1] + fc * U[iby - 1]) / wt;
+      Q[ivz - 1] = (U[imz - 1] + fc * U[ibz - 1]) / wt;
+      Q[ibx - 1] = U[ibx - 1];
+      Q[iby - 1] = U[iby - 1];
+      Q[ibz - 1] = U[ibz - 1];
+      Q[ibp - 1] = U[ibp - 1];
+      Q[ipr - 1] = w - en + 0.5 * (bb + (bb * mm - mb * mb) / (wt * wt));
+      if (Q[ipr - 1] <= 0.0) { Q[ipr - 1] = 0.0; ++c2p_failures; }
+    } else {
+      Q[ipr - 1] = 0.0;
+      ++c2p_failures;
+    }
+  }
+
+  // fluxspeed_srmhd_adi src/equations.F90:4821-5101
+  void fluxspeed_sr(const double* Q, const double* U, double* F, double* cm, double* cp) const {
+    double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+    double bb = Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1];
+    double vb = Q[ivx - 1] * Q[ibx - 1] + Q[ivy - 1] * Q[iby - 1] + Q[ivz - 1] * Q[ibz - 1];
+    double vm = 1.0 - vv;
+    double bx = Q[ibx - 1] * vm + vb * Q[ivx - 1];
+    double by = Q[iby - 1] * vm + vb * Q[ivy - 1];
+    double bz = Q[ibz - 1] * vm + vb * Q[ivz - 1];
+    double b2 = bb * vm + vb * vb;
+    double pm = 0.5 * b2;
+    double pt = Q[ipr - 1] + pm;
+    F[idn - 1] = U[idn - 1] * Q[ivx - 1];
+    F[imx - 1] = U[imx - 1] * Q[ivx - 1] - Q[ibx - 1] * bx + pt;
+    F[imy - 1] = U[imy - 1] * Q[ivx - 1] - Q[ibx - 1] * by;
+    F[imz - 1] = U[imz - 1] * Q[ivx - 1] - Q[ibx - 1] * bz;
+    F[ibx - 1] = Q[ibp - 1];
+    F[ibp - 1] = cmax2 * Q[ibx - 1];
+    F[iby - 1] = Q[ivx - 1] * Q[iby - 1] - Q[ibx - 1] * Q[ivy - 1];
+    F[ibz - 1] = Q[ivx - 1] * Q[ibz - 1] - Q[ibx - 1] * Q[ivz - 1];
+    F[ien - 1] = U[imx - 1] - F[idn - 1];
+    if (!cm || !cp) return;
+    double a[5], x[4] = {0, 0, 0, 0};
+    int nr;
+    if (vv > 0.0) {
+      double rh = Q[idn - 1] + Q[ipr - 1] / gammaxi;
+      double vs = std::sqrt(vm);
+      if (Q[ibx - 1] != 0.0) {
+        double c2 = gamma * Q[ipr - 1] / rh;
+        double v1 = std::fabs(Q[ivx - 1]);
+        double v2 = v1 * v1;
+        double fa = rh * (1.0 - c2);
+        double fb = c2 * (rh - vb * vb) + b2;
+        double fc = fsign(1.0, Q[ivx - 1]) * Q[ibx - 1] * vs;
+        double fd = c2 * fc * fc;
+        double fe = 1.0 - v2;
+        double ff = c2 * vb * fc;
+        double fg = v1 * vs;
+        a[4] = fa + fb * vm;
+        a[3] = 2.0 * (ff * vm + fb * fg);
+        a[2] = -fd * vm + 4.0 * ff * fg - fb * fe;
+        a[1] = -2.0 * (fd * fg + fe * ff);
+        a[0] = fd * fe;
+        nr = alg_quartic(a, x);
+        for (int n = 0; n < nr; ++n) x[n] = fsign(1.0, Q[ivx - 1]) * (std::fabs(v1) + x[n] * vs);
+      } else {
+        double c2 = gamma * Q[ipr - 1] / rh;
+        double cc = (1.0 - c2) / vm;
+        double gn = b2 - c2 * vb * vb;
+        a[2] = rh * (c2 + cc) + gn;
+        a[1] = -2.0 * rh * cc * Q[ivx - 1];
+        a[0] = rh * (cc * (Q[ivx - 1] * Q[ivx - 1]) - c2) - gn;
+        nr = alg_quadratic(a, x);
+      }
+    } else {
+      double rh = Q[idn - 1] + Q[ipr - 1] / gammaxi;
+      double vs = std::sqrt(vm);
+      double rt = rh + b2;
+      double c2 = gamma * Q[ipr - 1] / rh;
+      double t = Q[ibx - 1] * vs + vb * Q[ivx - 1] / vs;
+      double ca = t * t;
+      a[2] = 1.0;
+      a[1] = -((rh + ca) * c2 + b2) / rt;
+      a[0] = c2 * ca / rt;
+      nr = alg_quadratic(a, x);
+      if (nr > 0) {
+        double zm = fmin2(x[0], x[1]);
+        double zp = fmax2(x[0], x[1]);
+        if (zm >= 0.0) {
+          zm = std::sqrt(zm); zp = std::sqrt(zp);
+          x[0] = zp; x[1] = zm; x[2] = -zm; x[3] = -zp;
+          nr = 4;
+        } else if (zp >= 0.0) {
+          zp = std::sqrt(zp);
+          x[0] = zp; x[1] = -zp;
+          nr = 2;
+        } else {
+          x[0] = x[1] = x[2] = x[3] = 0.0;
+          nr = 0;
+        }
+      }
+    }
+    if (nr > 1) {
+      double mn = x[0], mx = x[0];
+      for (int n = 1; n < nr; ++n) { if (x[n] < mn) mn = x[n]; if (x[n] > mx) mx = x[n]; }
+      *cm = mn; *cp = mx;
+    } else {
+      *cm = -1.0; *cp = 1.0;
+    }
+  }
+
+  // =========================================================================
   // EQUATIONS
   // =========================================================================
   // prim2cons_hd_adi src/equations.F90:1762-1810, prim2cons_mhd_adi 2815-2868
   void prim2cons(int n, const double* q, double* u) const {
+    if (p.eqsys == EQ_SRMHD) {
+      for (int i = 0; i < n; ++i) prim2cons_sr(q + (size_t)nv * i, u + (size_t)nv * i);
+      return;
+    }
     for (int i = 0; i < n; ++i) {
       const double* Q = q + (size_t)nv * i; double* U = u + (size_t)nv * i;
       U[idn - 1] = Q[idn - 1];
@@ -238,6 +778,10 @@ struct Oracle {
 
   // cons2prim_hd_adi src/equations.F90:1828-1876, cons2prim_mhd_adi 2886-2939
   void cons2prim(int n, const double* u, double* q) const {
+    if (p.eqsys == EQ_SRMHD) {
+      for (int i = 0; i < n; ++i) cons2prim_sr(u + (size_t)nv * i, q + (size_t)nv * i);
+      return;
+    }
     for (int i = 0; i < n; ++i) {
       const double* U = u + (size_t)nv * i; double* Q = q + (size_t)nv * i;
       Q[idn - 1] = U[idn - 1];
@@ -261,6 +805,12 @@ struct Oracle {
   // fluxspeed_hd_adi src/equations.F90:1896-1958,
   // fluxspeed_mhd_adi src/equations.F90:2959-3045
   void fluxspeed(int n, const double* q, const double* u, double* f, double* cm, double* cp) const {
+    if (p.eqsys == EQ_SRMHD) {
+      for (int i = 0; i < n; ++i)
+        fluxspeed_sr(q + (size_t)nv * i, u + (size_t)nv * i, f + (size_t)nv * i, cm ? cm + i : nullptr,
+                     cp ? cp + i : nullptr);
+      return;
+    }
     for (int i = 0; i < n; ++i) {
       const double* Q = q + (size_t)nv * i; const double* U = u + (size_t)nv * i; double* F = f + (size_t)nv * i;
       if (p.eqsys == EQ_HD) {
@@ -308,6 +858,7 @@ struct Oracle {
 
   // maxspeed_hd_adi src/equations.F90:1974-2044, maxspeed_mhd_adi 3060-3131
   double maxspeed(const double* qq) const {
+    if (p.eqsys == EQ_SRMHD) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
     double ms = 0.0;
     for (int k = kb; k <= ke; ++k)
       for (int j = jb; j <= je; ++j)
@@ -779,8 +1330,14 @@ struct Oracle {
     const int N = nv;
     double ul[9], ur[9], fl[9], fr[9], wl[9], wr[9], ui[9], wcl[9], wcr[9];
     double clm, clp, crm, crp;
-    if (p.eqsys == EQ_MHD) glm(ql, qr);
+    if (p.eqsys != EQ_HD) glm(ql, qr);
     prim2cons(1, ql, ul); prim2cons(1, qr, ur);
+    if (p.eqsys == EQ_SRMHD && p.rs == RS_HLLC) {
+      fluxspeed(1, ql, ul, fl, &clm, &clp);
+      fluxspeed(1, qr, ur, fr, &crm, &crp);
+      srmhd_hllc_point(ql, qr, ul, ur, fl, fr, fmin2(clm, crm), fmax2(clp, crp), f);
+      return;
+    }
     if (p.rs == RS_ROE) {
       fluxspeed(1, ql, ul, fl, nullptr, nullptr);
       fluxspeed(1, qr, ur, fr, nullptr, nullptr);
@@ -1031,6 +1588,110 @@ struct Oracle {
 
   // riemann_hd_adi_roe src/schemes.F90:1541-1661 and
   // riemann_mhd_adi_roe src/schemes.F90:4230-4410 (after prim2cons/fluxspeed)
+  // riemann_srmhd_adi_hllc src/schemes.F90:5382-5734 (Mignone & Bodo 2006),
+  // after prim2cons and fluxspeed
+  void srmhd_hllc_point(const double* ql, const double* qr, const double* ul, const double* ur,
+                        const double* fl, const double* fr, double sl, double sr, double* f) const {
+    const int N = nv;
+    if (sl >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
+    if (sr <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
+    const int Dn = idn - 1, Mx = imx - 1, My = imy - 1, Mz = imz - 1, En = ien - 1;
+    const int Bx = ibx - 1, By = iby - 1, Bz = ibz - 1, Bp = ibp - 1;
+    double srml = sr - sl;
+    double wl[9], wr[9], uh[9], fh[9], us[9], a[3], x[2], vs[3];
+    for (int v = 0; v < N; ++v) {
+      wl[v] = sl * ul[v] - fl[v];
+      wr[v] = sr * ur[v] - fr[v];
+      uh[v] = (wr[v] - wl[v]) / srml;
+      fh[v] = (sl * wr[v] - sr * wl[v]) / srml;
+    }
+    wl[En] = wl[En] + wl[Dn];
+    wr[En] = wr[En] + wr[Dn];
+    double bx2 = ql[Bx] * qr[Bx];
+    auto use_hll = [&]() { for (int v = 0; v < N; ++v) f[v] = fh[v]; };
+    if (bx2 >= 1.0e-16) {
+      double uu = uh[By] * uh[By] + uh[Bz] * uh[Bz];
+      double ff = fh[By] * fh[By] + fh[Bz] * fh[Bz];
+      double uf = uh[By] * fh[By] + uh[Bz] * fh[Bz];
+      a[0] = uh[Mx] - uf;
+      a[1] = uu + ff - (fh[Mx] + uh[En] + uh[Dn]);
+      a[2] = fh[En] + fh[Dn] - uf;
+      int nr = alg_quadratic(a, x);
+      if (nr < 1) { use_hll(); return; }
+      double sm = x[0];
+      if ((sm <= sl) || (sm >= sr)) { use_hll(); return; }
+      us[Bx] = ql[Bx]; us[By] = uh[By]; us[Bz] = uh[Bz]; us[Bp] = ql[Bp];
+      vs[0] = sm;
+      vs[1] = (us[By] * sm - fh[By]) / us[Bx];
+      vs[2] = (us[Bz] * sm - fh[Bz]) / us[Bx];
+      double vv = vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2];
+      double vb = vs[0] * us[Bx] + vs[1] * us[By] + vs[2] * us[Bz];
+      double gi = 1.0 - vv;
+      double pt = fh[Mx] + gi * bx2 - (fh[En] + fh[Dn] - us[Bx] * vb) * sm;
+      if (pt <= 0.0) { use_hll(); return; }
+      if (sm > 0.0) {
+        double dv = sl - sm;
+        double fc = (sl - ql[ivx - 1]) / dv;
+        us[Dn] = fc * ul[Dn];
+        us[My] = (sl * ul[My] - fl[My] - us[Bx] * (gi * us[By] + vs[1] * vb)) / dv;
+        us[Mz] = (sl * ul[Mz] - fl[Mz] - us[Bx] * (gi * us[Bz] + vs[2] * vb)) / dv;
+        us[En] = (sl * (ul[En] + ul[Dn]) - (fl[En] + fl[Dn]) + pt * sm - us[Bx] * vb) / dv - us[Dn];
+        us[Mx] = (us[En] + us[Dn] + pt) * sm - us[Bx] * vb;
+        for (int v = 0; v < N; ++v) f[v] = fl[v] + sl * (us[v] - ul[v]);
+      } else if (sm < 0.0) {
+        double dv = sr - sm;
+        double fc = (sr - qr[ivx - 1]) / dv;
+        us[Dn] = fc * ur[Dn];
+        us[My] = (sr * ur[My] - fr[My] - us[Bx] * (gi * us[By] + vs[1] * vb)) / dv;
+        us[Mz] = (sr * ur[Mz] - fr[Mz] - us[Bx] * (gi * us[Bz] + vs[2] * vb)) / dv;
+        us[En] = (sr * (ur[En] + ur[Dn]) - (fr[En] + fr[Dn]) + pt * sm - us[Bx] * vb) / dv - us[Dn];
+        us[Mx] = (us[En] + us[Dn] + pt) * sm - us[Bx] * vb;
+        for (int v = 0; v < N; ++v) f[v] = fr[v] + sr * (us[v] - ur[v]);
+      } else {
+        use_hll();
+      }
+    } else {
+      a[0] = uh[Mx];
+      a[1] = -(fh[Mx] + uh[En] + uh[Dn]);
+      a[2] = fh[En] + fh[Dn];
+      int nr = alg_quadratic(a, x);
+      if (nr < 1) { use_hll(); return; }
+      double sm = x[0];
+      if ((sm <= sl) || (sm >= sr)) { use_hll(); return; }
+      double pt = fh[Mx] - (fh[En] + fh[Dn]) * sm;
+      if (pt <= 0.0) { use_hll(); return; }
+      if (sm > 0.0) {
+        double dv = sl - sm;
+        us[Dn] = wl[Dn] / dv;
+        us[My] = wl[My] / dv;
+        us[Mz] = wl[Mz] / dv;
+        us[En] = (wl[En] + pt * sm) / dv;
+        us[Mx] = (us[En] + pt) * sm;
+        us[En] = us[En] - us[Dn];
+        us[Bx] = 0.0;
+        us[By] = wl[By] / dv;
+        us[Bz] = wl[Bz] / dv;
+        us[Bp] = ql[Bp];
+        for (int v = 0; v < N; ++v) f[v] = fl[v] + sl * (us[v] - ul[v]);
+      } else if (sm < 0.0) {
+        double dv = sr - sm;
+        us[Dn] = wr[Dn] / dv;
+        us[My] = wr[My] / dv;
+        us[Mz] = wr[Mz] / dv;
+        us[En] = (wr[En] + pt * sm) / dv;
+        us[Mx] = (us[En] + pt) * sm;
+        us[En] = us[En] - us[Dn];
+        us[Bx] = 0.0;
+        us[By] = wr[By] / dv;
+        us[Bz] = wr[Bz] / dv;
+        us[Bp] = qr[Bp];
+        for (int v = 0; v < N; ++v) f[v] = fr[v] + sr * (us[v] - ur[v]);
+      } else {
+        use_hll();
+      }
+    }
+  }
+
   void roe_point(const double* ql, const double* qr, const double* ul, const double* ur,
                  const double* fl, const double* fr, double* f) const {
     const int N = nv;
