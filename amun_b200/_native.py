@@ -11,7 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libamun_gpu.so")
 
-AMUN_EQ_HD, AMUN_EQ_MHD = 0, 1
+AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD = 0, 1, 2
 AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
 AMUN_FP64, AMUN_FP32_BULK = 0, 1
 
@@ -30,7 +30,8 @@ class amun_params(C.Structure):
         ("extrema_limiter", C.c_int), ("riemann", C.c_int), ("time_advance", C.c_int), ("stages", C.c_int),
         ("fix_positivity", C.c_int), ("clip_extrema", C.c_int), ("precision", C.c_int), ("ncells", C.c_int),
         ("nghosts", C.c_int), ("gamma", C.c_double), ("cfl", C.c_double), ("alpha", C.c_double),
-        ("eps", C.c_double),
+        ("eps", C.c_double), ("tolerance", C.c_double), ("pmin", C.c_double), ("nr_maxit", C.c_int),
+        ("nr_extra", C.c_int), ("states_4vec", C.c_int),
     ]
 
 
@@ -40,7 +41,8 @@ class amun_block_desc(C.Structure):
 
 class amun_status(C.Structure):
     _fields_ = [("time", C.c_double), ("dt", C.c_double), ("dtn", C.c_double), ("cmax", C.c_double),
-                ("step", C.c_longlong), ("nonpositive", C.c_longlong), ("device_bytes", C.c_longlong)]
+                ("step", C.c_longlong), ("nonpositive", C.c_longlong), ("c2p_failures", C.c_longlong),
+                ("device_bytes", C.c_longlong)]
 
 
 _lib = None

@@ -32,9 +32,11 @@ UNITS = {
     "kernels_fp64.cu": ["-fmad=false"],
     "kernels_fp64_hd.cu": ["-fmad=false"],
     "kernels_fp64_mhd.cu": ["-fmad=false"],
+    "kernels_fp64_srmhd.cu": ["-fmad=false"],
     "kernels_fp32.cu": [],
     "kernels_fp32_hd.cu": [],
     "kernels_fp32_mhd.cu": [],
+    "kernels_fp32_srmhd.cu": [],
 }
 
 

@@ -248,9 +248,20 @@ void tile_shape(int& LP, int& LW) {
 
 MethodConst method_const() {
   MethodConst m;
-  m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.eps = C.p.eps; m.decay = C.decay;
+  m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.gammaxi = C.gammam1 / C.gamma;
+  m.eps = C.p.eps; m.decay = C.decay;
   m.lim = C.p.limiter; m.clim = C.p.extrema_limiter; m.positivity = C.p.fix_positivity; m.clip = C.p.clip_extrema;
+  m.tol = C.p.tolerance; m.pmin = C.p.pmin; m.nrmax = C.p.nr_maxit; m.nrext = C.p.nr_extra;
+  m.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
   return m;
+}
+
+// the Riemann solver each system offers (src/schemes.F90:159-503)
+int effective_solver() {
+  int rs = C.p.riemann;
+  if (C.p.eqsys == AMUN_EQ_HD && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
+  if (C.p.eqsys == AMUN_EQ_SRMHD && rs != AMUN_RS_HLLC) rs = AMUN_RS_HLL;
+  return rs;
 }
 
 template <typename R>
@@ -274,13 +285,12 @@ int launch_stage(const StageDesc& st) {
   a.m = method_const();
   a.st = st;
   a.LP = LP; a.LW = LW;
-  int rs = C.p.riemann;
-  if (C.nv == 5 && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
+  const int rs = effective_solver();
   for (int d = 0; d < C.g.ndims; ++d) {
     a.first = d == 0;
     a.last = d == C.g.ndims - 1;
     ProfScope ps(d);
-    cudaError_t e = Launch<R, R>::sweep(C.nv, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
+    cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
   }
   C.cur = 1 - C.cur;
@@ -310,10 +320,10 @@ int evolve_launches() { return bulk() ? launch_evolve<float>() : launch_evolve<d
 int ensure_maxspeed() {
   if (C.ms_valid) return 0;
   CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
-  cudaError_t e = bulk() ? Launch<float, float>::maxspeed(C.nv, (const float*)C.q[C.cur], C.g, C.gamma, C.sc,
+  cudaError_t e = bulk() ? Launch<float, float>::maxspeed(C.p.eqsys, (const float*)C.q[C.cur], C.g, C.gamma, C.sc,
                                                           C.nblocks, C.stream)
-                         : Launch<double, double>::maxspeed(C.nv, (const double*)C.q[C.cur], C.g, C.gamma, C.sc,
-                                                            C.nblocks, C.stream);
+                         : Launch<double, double>::maxspeed(C.p.eqsys, (const double*)C.q[C.cur], C.g, C.gamma,
+                                                            C.sc, C.nblocks, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
   C.ms_valid = true;
   return 0;
@@ -344,7 +354,11 @@ UnitArgs unit_args(int im, int jm, int km) {
   UnitArgs u;
   u.nv = C.nv; u.ndims = C.p.ndims; u.im = im; u.jm = jm; u.km = km; u.ng = C.p.nghosts;
   u.rec = C.p.reconstruction; u.lim = C.p.limiter; u.clim = C.p.extrema_limiter;
-  u.rs = (C.nv == 5 && C.p.riemann == AMUN_RS_HLLD) ? AMUN_RS_HLL : C.p.riemann;
+  u.rs = effective_solver();
+  u.eq = C.p.eqsys;
+  u.gammaxi = C.gammam1 / C.gamma;
+  u.tol = C.p.tolerance; u.pmin = C.p.pmin; u.nrmax = C.p.nr_maxit; u.nrext = C.p.nr_extra;
+  u.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
   u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax;
   return u;
@@ -379,6 +393,11 @@ void amun_gpu_default_params(amun_params* p) {
   p->cfl = 0.5;
   p->alpha = 2.0;
   p->eps = 2.220446049250313e-16;  // epsilon(1d0)
+  p->tolerance = 1.0e-10;
+  p->pmin = 1.0e-16;
+  p->nr_maxit = 100;
+  p->nr_extra = 2;
+  p->states_4vec = 0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -390,11 +409,20 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "equation_system") {
     if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p->eqsys = AMUN_EQ_HD;
     else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p->eqsys = AMUN_EQ_MHD;
+    else if (is_one_of(v, {"srmhd", "SRMHD"})) p->eqsys = AMUN_EQ_SRMHD;
     else return fail(100, std::string("equation system not implemented: ") + v);
   } else if (k == "equation_of_state") {
     if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"}))
       return fail(110, std::string("equation of state not implemented: ") + v);
-  } else if (k == "reconstruction") {
+  } else if (k == "primitive_solver") {
+    if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"}))
+      return fail(AMUN_E_UNSUPPORTED, std::string("primitive solver not implemented here: ") + v);
+  } else if (k == "tolerance") p->tolerance = atof(v);
+  else if (k == "pmin") p->pmin = atof(v);
+  else if (k == "nr_maxit") p->nr_maxit = atoi(v);
+  else if (k == "nr_extra") p->nr_extra = atoi(v);
+  else if (k == "state_variables") p->states_4vec = is_one_of(v, {"4vec", "4-vector", "4VEC", "4-VECTOR"});
+  else if (k == "reconstruction") {
     if (is_one_of(v, {"tvd", "TVD"})) p->reconstruction = AMUN_REC_TVD;
     else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p->reconstruction = AMUN_REC_WENO5Z;
     else return fail(200, std::string("reconstruction not implemented: ") + v);
@@ -437,7 +465,8 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
 int amun_gpu_init(const amun_params* p) {
   if (!p) return fail(AMUN_E_BAD_ARGUMENT, "null params");
   if (p->ndims != 2 && p->ndims != 3) return fail(AMUN_E_BAD_ARGUMENT, "ndims must be 2 or 3");
-  if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD) return fail(100, "equation system not implemented");
+  if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD && p->eqsys != AMUN_EQ_SRMHD)
+    return fail(100, "equation system not implemented");
   if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
     return fail(200, "reconstruction not implemented");
   int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;
@@ -452,7 +481,7 @@ int amun_gpu_init(const amun_params* p) {
   if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
   CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
-  C.nv = p->eqsys == AMUN_EQ_MHD ? 9 : 5;
+  C.nv = p->eqsys == AMUN_EQ_HD ? 5 : 9;
   C.gamma = p->gamma;
   C.gammam1 = C.gamma - 1.0;
   C.gammam1i = 1.0 / C.gammam1;
@@ -582,19 +611,19 @@ static int download_range(int first, int count, double* u0, double* u1, double* 
     CK(cudaStreamSynchronize(C.stream));
   }
   if (u0) {
-    e = bulk() ? Launch<float, float>::download_u0(C.nv, C.u0, (const float*)C.q[C.cur], C.staging, g, C.gammam1i,
-                                                   first, count, C.stream)
-               : Launch<double, double>::download_u0(C.nv, C.u0, (const double*)C.q[C.cur], C.staging, g,
-                                                     C.gammam1i, first, count, C.stream);
+    e = bulk() ? Launch<float, float>::download_u0(C.p.eqsys, C.u0, (const float*)C.q[C.cur], C.staging, g,
+                                                   method_const(), first, count, C.stream)
+               : Launch<double, double>::download_u0(C.p.eqsys, C.u0, (const double*)C.q[C.cur], C.staging, g,
+                                                     method_const(), first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "download u0");
     CK(cudaMemcpyAsync(u0, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   if (u1) {
-    e = bulk() ? Launch<float, float>::download_u1(C.nv, (const float*)C.u1, (const float*)C.q[C.cur], C.staging, g,
-                                                   C.gammam1i, first, count, C.stream)
-               : Launch<double, double>::download_u1(C.nv, (const double*)C.u1, (const double*)C.q[C.cur],
-                                                     C.staging, g, C.gammam1i, first, count, C.stream);
+    e = bulk() ? Launch<float, float>::download_u1(C.p.eqsys, (const float*)C.u1, (const float*)C.q[C.cur],
+                                                   C.staging, g, method_const(), first, count, C.stream)
+               : Launch<double, double>::download_u1(C.p.eqsys, (const double*)C.u1, (const double*)C.q[C.cur],
+                                                     C.staging, g, method_const(), first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "download u1");
     CK(cudaMemcpyAsync(u1, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
     CK(cudaStreamSynchronize(C.stream));
@@ -722,6 +751,7 @@ int amun_gpu_status(amun_status* s) {
   CK(d2h(&h, C.sc, sizeof(h)));
   s->time = h.time; s->dt = h.dt; s->dtn = h.dtn; s->cmax = h.cmax; s->step = h.step;
   s->nonpositive = (long long)h.nonpositive;
+  s->c2p_failures = (long long)h.c2p_failures;
   s->device_bytes = C.pool_bytes;
   return 0;
 }

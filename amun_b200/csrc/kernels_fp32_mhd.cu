@@ -1,7 +1,7 @@
-// Sweep kernels of the fp32 mode for the MHD system (NV=9).
+// Sweep kernels of the fp32 mode for the MHD system.
 #define AMUN_SWEEP_IMPL
 #include "launch.cuh"
 namespace amun {
-template cudaError_t sweep_nv<float, float, 9>(int, int, int, const SweepArgs<float, float>&, dim3, int, size_t,
+template cudaError_t sweep_eq<float, float, EQ_MHD>(int, int, int, const SweepArgs<float, float>&, dim3, int, size_t,
                                               cudaStream_t);
 }

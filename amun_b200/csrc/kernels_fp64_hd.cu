@@ -1,7 +1,7 @@
-// Sweep kernels of the fp64 mode for the HD system (NV=5).
+// Sweep kernels of the fp64 mode for the HD system.
 #define AMUN_SWEEP_IMPL
 #include "launch.cuh"
 namespace amun {
-template cudaError_t sweep_nv<double, double, 5>(int, int, int, const SweepArgs<double, double>&, dim3, int, size_t,
+template cudaError_t sweep_eq<double, double, EQ_HD>(int, int, int, const SweepArgs<double, double>&, dim3, int, size_t,
                                               cudaStream_t);
 }

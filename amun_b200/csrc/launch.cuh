@@ -1,5 +1,5 @@
 // launch.cuh -- host-side launchers of the stage kernels, one explicit
-// instantiation per precision mode (see kernels_*.cu).
+// instantiation per precision mode and equation system (see kernels_*.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include "sweep.cuh"
@@ -7,19 +7,19 @@
 namespace amun {
 
 template <typename R, typename U1T> struct Launch {
-  static cudaError_t sweep(int nv, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
+  static cudaError_t sweep(int eq, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
                            size_t smem, cudaStream_t s);
   static cudaError_t ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s);
-  static cudaError_t maxspeed(int nv, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
+  static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
                               cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
   static cudaError_t upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_u0(const double* fu, double* u0, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_u1(const double* fu, U1T* u1, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
   static cudaError_t download_q(const R* q, double* fq, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
-  static cudaError_t download_u0(int nv, const double* u0, const R* q, double* fu, const Geo& g, double gammam1i,
-                                 int b0, int nb, cudaStream_t s);
-  static cudaError_t download_u1(int nv, const U1T* u1, const R* q, double* fu, const Geo& g, double gammam1i,
+  static cudaError_t download_u0(int eq, const double* u0, const R* q, double* fu, const Geo& g,
+                                 const MethodConst& m, int b0, int nb, cudaStream_t s);
+  static cudaError_t download_u1(int eq, const U1T* u1, const R* q, double* fu, const Geo& g, const MethodConst& m,
                                  int b0, int nb, cudaStream_t s);
 };
 
@@ -30,16 +30,16 @@ inline int grid_for(long long n, int threads, int max_blocks = 148 * 16) {
   return (int)b;
 }
 
-// sweep dispatch per variable count; instantiated in kernels_<prec>_<eq>.cu so
-// the large solver kernels compile in parallel
-template <typename R, typename U1T, int NV>
-cudaError_t sweep_nv(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
+// sweep dispatch per equation system; instantiated in kernels_<prec>_<eq>.cu
+// so the large solver kernels compile in parallel
+template <typename R, typename U1T, int EQ>
+cudaError_t sweep_eq(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                      cudaStream_t s);
 
 #ifdef AMUN_SWEEP_IMPL
-template <typename R, typename U1T, int NV, int REC, int RS, int DIR>
+template <typename R, typename U1T, int EQ, int REC, int RS, int DIR>
 static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
-  auto k = sweep_kernel<NV, REC, RS, DIR, R, U1T>;
+  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -50,48 +50,55 @@ static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, 
   return cudaGetLastError();
 }
 
-template <typename R, typename U1T, int NV, int REC, int RS>
+template <typename R, typename U1T, int EQ, int REC, int RS>
 static cudaError_t go_dir(int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
   switch (dir) {
-    case 0: return go_sweep<R, U1T, NV, REC, RS, 0>(a, grid, threads, smem, s);
-    case 1: return go_sweep<R, U1T, NV, REC, RS, 1>(a, grid, threads, smem, s);
-    default: return go_sweep<R, U1T, NV, REC, RS, 2>(a, grid, threads, smem, s);
+    case 0: return go_sweep<R, U1T, EQ, REC, RS, 0>(a, grid, threads, smem, s);
+    case 1: return go_sweep<R, U1T, EQ, REC, RS, 1>(a, grid, threads, smem, s);
+    default: return go_sweep<R, U1T, EQ, REC, RS, 2>(a, grid, threads, smem, s);
   }
 }
 
-template <typename R, typename U1T, int NV, int REC>
+// the solvers each system offers (src/schemes.F90:159-503)
+template <typename R, typename U1T, int EQ, int REC>
 static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                          cudaStream_t s) {
-  if constexpr (NV == 5) {
+  if constexpr (EQ == EQ_HD) {
     switch (rs) {
-      case RS_HLLC: return go_dir<R, U1T, NV, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
-      case RS_ROE: return go_dir<R, U1T, NV, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, NV, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+    }
+  } else if constexpr (EQ == EQ_MHD) {
+    switch (rs) {
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
+      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
   } else {
     switch (rs) {
-      case RS_HLLC: return go_dir<R, U1T, NV, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
-      case RS_HLLD: return go_dir<R, U1T, NV, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
-      case RS_ROE: return go_dir<R, U1T, NV, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, NV, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
   }
 }
 
-template <typename R, typename U1T, int NV>
-cudaError_t sweep_nv(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
+template <typename R, typename U1T, int EQ>
+cudaError_t sweep_eq(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                      cudaStream_t s) {
-  if (rec == REC_WENO5Z) return go_rs<R, U1T, NV, REC_WENO5Z>(rs, dir, a, grid, threads, smem, s);
-  return go_rs<R, U1T, NV, REC_TVD>(rs, dir, a, grid, threads, smem, s);
+  if (rec == REC_WENO5Z) return go_rs<R, U1T, EQ, REC_WENO5Z>(rs, dir, a, grid, threads, smem, s);
+  return go_rs<R, U1T, EQ, REC_TVD>(rs, dir, a, grid, threads, smem, s);
 }
 #endif  // AMUN_SWEEP_IMPL
 
 #ifdef AMUN_LAUNCH_IMPL
 template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::sweep(int nv, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
+cudaError_t Launch<R, U1T>::sweep(int eq, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
                                   int threads, size_t smem, cudaStream_t s) {
-  if (nv == 5) return sweep_nv<R, U1T, 5>(rec, rs, dir, a, grid, threads, smem, s);
-  return sweep_nv<R, U1T, 9>(rec, rs, dir, a, grid, threads, smem, s);
+  if (eq == EQ_HD) return sweep_eq<R, U1T, EQ_HD>(rec, rs, dir, a, grid, threads, smem, s);
+  if (eq == EQ_MHD) return sweep_eq<R, U1T, EQ_MHD>(rec, rs, dir, a, grid, threads, smem, s);
+  return sweep_eq<R, U1T, EQ_SRMHD>(rec, rs, dir, a, grid, threads, smem, s);
 }
 
 template <typename R, typename U1T>
@@ -106,13 +113,14 @@ cudaError_t Launch<R, U1T>::ghost(R* q, const int* nbr, const Geo& g, int nv, in
 }
 
 template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::maxspeed(int nv, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
+cudaError_t Launch<R, U1T>::maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
                                      cudaStream_t s) {
   long long n = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1) * nblocks;
   int threads = 256;
   int grid = grid_for(n, threads);
-  if (nv == 5) maxspeed_kernel<5, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
-  else maxspeed_kernel<9, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  if (eq == EQ_HD) maxspeed_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  else if (eq == EQ_MHD) maxspeed_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  else maxspeed_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
   return cudaGetLastError();
 }
 
@@ -149,21 +157,26 @@ cudaError_t Launch<R, U1T>::download_q(const R* q, double* fq, const Geo& g, int
   download_q_kernel<R><<<grid_for(n, 256), 256, 0, s>>>(q, fq, g, nv, b0, nb);
   return cudaGetLastError();
 }
-template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::download_u0(int nv, const double* u0, const R* q, double* fu, const Geo& g,
-                                        double gammam1i, int b0, int nb, cudaStream_t s) {
+
+template <typename R, typename UT>
+static cudaError_t download_u_any(int eq, const UT* u, const R* q, double* fu, const Geo& g, const MethodConst& m,
+                                  int b0, int nb, cudaStream_t s) {
   long long n = (long long)g.IM * g.JM * g.KM * nb;
-  if (nv == 5) download_u_kernel<5, R, double><<<grid_for(n, 256), 256, 0, s>>>(u0, q, fu, g, gammam1i, b0, nb);
-  else download_u_kernel<9, R, double><<<grid_for(n, 256), 256, 0, s>>>(u0, q, fu, g, gammam1i, b0, nb);
+  int grid = grid_for(n, 256);
+  if (eq == EQ_HD) download_u_kernel<EQ_HD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
+  else if (eq == EQ_MHD) download_u_kernel<EQ_MHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
+  else download_u_kernel<EQ_SRMHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   return cudaGetLastError();
 }
 template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::download_u1(int nv, const U1T* u1, const R* q, double* fu, const Geo& g,
-                                        double gammam1i, int b0, int nb, cudaStream_t s) {
-  long long n = (long long)g.IM * g.JM * g.KM * nb;
-  if (nv == 5) download_u_kernel<5, R, U1T><<<grid_for(n, 256), 256, 0, s>>>(u1, q, fu, g, gammam1i, b0, nb);
-  else download_u_kernel<9, R, U1T><<<grid_for(n, 256), 256, 0, s>>>(u1, q, fu, g, gammam1i, b0, nb);
-  return cudaGetLastError();
+cudaError_t Launch<R, U1T>::download_u0(int eq, const double* u0, const R* q, double* fu, const Geo& g,
+                                        const MethodConst& m, int b0, int nb, cudaStream_t s) {
+  return download_u_any<R, double>(eq, u0, q, fu, g, m, b0, nb, s);
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::download_u1(int eq, const U1T* u1, const R* q, double* fu, const Geo& g,
+                                        const MethodConst& m, int b0, int nb, cudaStream_t s) {
+  return download_u_any<R, U1T>(eq, u1, q, fu, g, m, b0, nb, s);
 }
 #endif  // AMUN_LAUNCH_IMPL
 

@@ -17,23 +17,37 @@ enum { LIM_ZERO = 0, LIM_MM = 1, LIM_MC = 2, LIM_SB = 3, LIM_VL = 4, LIM_VA = 5 
 enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_ROE = 3 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 
-template <int NV> struct Var;
-template <> struct Var<5> {
+// equation systems (src/equations.F90:322-833)
+enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2 };
+
+template <int EQ> struct Var;
+template <> struct Var<EQ_HD> {
+  static constexpr int NV = 5;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, PR = 4, EN = 4;
   static constexpr int BX = -1, BY = -1, BZ = -1, BP = -1;
-  static constexpr bool MHD = false;
+  static constexpr bool MHD = false, SR = false;
 };
-template <> struct Var<9> {
+template <> struct Var<EQ_MHD> {
+  static constexpr int NV = 9;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
-  static constexpr bool MHD = true;
+  static constexpr bool MHD = true, SR = false;
+};
+template <> struct Var<EQ_SRMHD> {
+  static constexpr int NV = 9;
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
+  static constexpr bool MHD = true, SR = true;
 };
 
 // Equation and method constants in the working precision R.
 template <typename R> struct Phys {
-  R gamma, gammam1, gammam1i;
+  R gamma, gammam1, gammam1i, gammaxi;
   R eps;      // reconstruction epsilon (WENO-Z, van Albada)
   R cmax, cmax2;
   int lim, clim;
+  // relativistic recovery: tolerance, pmin, nr_maxit, nr_extra
+  // (src/equations.F90:184-201, 313-318)
+  double tol, pmin;
+  int nrmax, nrext;
 };
 
 template <typename R> __device__ __forceinline__ R d_abs(R x) { return x < R(0) ? -x : (x == R(0) ? R(0) : x); }
@@ -72,13 +86,19 @@ __device__ __forceinline__ R limiter(int which, R x, R a, R b, R eps) {
   }
 }
 
+}  // namespace amun
+#include "srmhd.cuh"
+namespace amun {
+
 // ---------------------------------------------------------------------------
 // Conversions and physical fluxes
 // ---------------------------------------------------------------------------
 // prim2cons_hd_adi src/equations.F90:1762-1810; prim2cons_mhd_adi 2815-2868
-template <int NV, typename R>
+template <int EQ, typename R>
 __device__ __forceinline__ void prim2cons(const R* q, R* u, const Phys<R>& P) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
+  if constexpr (V::SR) { prim2cons_sr(q, u, P); return; }
   u[V::DN] = q[V::DN];
   u[V::VX] = q[V::DN] * q[V::VX];
   u[V::VY] = q[V::DN] * q[V::VY];
@@ -97,9 +117,15 @@ __device__ __forceinline__ void prim2cons(const R* q, R* u, const Phys<R>& P) {
 }
 
 // cons2prim_hd_adi src/equations.F90:1828-1876; cons2prim_mhd_adi 2886-2939
-template <int NV, typename R>
+template <int EQ, typename R>
 __device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
+  if constexpr (V::SR) {
+    static_assert(sizeof(R) == 8, "the relativistic recovery runs in FP64");
+    cons2prim_sr(u, q, P);
+    return;
+  }
   q[V::DN] = u[V::DN];
   q[V::VX] = u[V::VX] / u[V::DN];
   q[V::VY] = u[V::VY] / u[V::DN];
@@ -119,9 +145,11 @@ __device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
 
 // fluxspeed_hd_adi src/equations.F90:1896-1958;
 // fluxspeed_mhd_adi src/equations.F90:2959-3045
-template <int NV, bool SPEEDS, typename R>
+template <int EQ, bool SPEEDS, typename R>
 __device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R& cp, const Phys<R>& P) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
+  if constexpr (V::SR) { fluxspeed_sr<SPEEDS>(q, u, f, cm, cp, P); return; }
   if constexpr (!V::MHD) {
     f[V::DN] = u[V::VX];
     f[V::VX] = q[V::VX] * u[V::VX];
@@ -166,9 +194,11 @@ __device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R
 
 // maxspeed_hd_adi src/equations.F90:1974-2044 / maxspeed_mhd_adi 3060-3131,
 // the per-cell term |v| + c
-template <int NV, typename R>
+template <int EQ, typename R>
 __device__ __forceinline__ double cell_speed(const R* q, double gamma) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
+  if constexpr (V::SR) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
   double vx = q[V::VX], vy = q[V::VY], vz = q[V::VZ];
   double vv = vx * vx + vy * vy + vz * vz;
   double v = sqrt(vv);
@@ -248,9 +278,10 @@ __device__ __forceinline__ void clip_cell(R fm1, R f0, R fp1, int clim, R eps, R
 // Riemann solvers on rotated primitive states (normal component first).
 // ---------------------------------------------------------------------------
 // GLM averaging of Bx and psi (e.g. src/schemes.F90:3196-3215)
-template <int NV, typename R>
+template <int EQ, typename R>
 __device__ __forceinline__ void glm_average(R* ql, R* qr, const Phys<R>& P) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
   R bx = R(0.5) * ((qr[V::BX] + ql[V::BX]) - (qr[V::BP] - ql[V::BP]) / P.cmax);
   R bp = R(0.5) * ((qr[V::BP] + ql[V::BP]) - (qr[V::BX] - ql[V::BX]) * P.cmax);
   ql[V::BX] = bx; qr[V::BX] = bx; ql[V::BP] = bp; qr[V::BP] = bp;
@@ -259,7 +290,7 @@ __device__ __forceinline__ void glm_average(R* ql, R* qr, const Phys<R>& P) {
 // esystem_roe_hd_adi src/equations.F90:2075-2180 (l[var*5+wave], r[wave*5+var])
 template <typename R>
 __device__ void esystem_roe_hd(const R* q, R* c, R* l, R* r, const Phys<R>& P) {
-  using V = Var<5>;
+  using V = Var<EQ_HD>;
 #pragma unroll
   for (int m = 0; m < 25; ++m) { l[m] = R(0); r[m] = R(0); }
   auto L = [&](int var, int wave) -> R& { return l[var * 5 + wave]; };
@@ -306,7 +337,7 @@ __device__ void esystem_roe_hd(const R* q, R* c, R* l, R* r, const Phys<R>& P) {
 // Returns false when the eigenvectors are not needed (3237-3238).
 template <typename R>
 __device__ bool esystem_roe_mhd(R x, R y, const R* q, R* c, R* l, R* r, const Phys<R>& P) {
-  using V = Var<9>;
+  using V = Var<EQ_MHD>;
   for (int m = 0; m < 81; ++m) { l[m] = R(0); r[m] = R(0); }
   auto L = [&](int var, int wave) -> R& { return l[var * 9 + wave]; };
   auto Rm = [&](int wave, int var) -> R& { return r[wave * 9 + var]; };
@@ -457,18 +488,19 @@ __device__ bool esystem_roe_mhd(R x, R y, const R* q, R* c, R* l, R* r, const Ph
 // riemann_mhd_adi_hllc src/schemes.F90:3305-3571
 // riemann_mhd_adi_hlld src/schemes.F90:3596-4203
 // riemann_mhd_adi_roe  src/schemes.F90:4230-4410
-template <int NV, int RS, typename R>
+template <int EQ, int RS, typename R>
 __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV;
   constexpr int Dn = V::DN, Mx = V::VX, My = V::VY, Mz = V::VZ, En = V::EN;
   R ul[NV], ur[NV], fl[NV], fr[NV];
   R clm, clp, crm, crp;
-  if constexpr (V::MHD) glm_average<NV>(ql, qr, P);
-  prim2cons<NV>(ql, ul, P);
-  prim2cons<NV>(qr, ur, P);
+  if constexpr (V::MHD) glm_average<EQ>(ql, qr, P);
+  prim2cons<EQ>(ql, ul, P);
+  prim2cons<EQ>(qr, ur, P);
   if constexpr (RS == RS_ROE) {
-    fluxspeed<NV, false>(ql, ul, fl, clm, clp, P);
-    fluxspeed<NV, false>(qr, ur, fr, crm, crp, P);
+    fluxspeed<EQ, false>(ql, ul, fl, clm, clp, P);
+    fluxspeed<EQ, false>(qr, ur, fr, crm, crp, P);
     R qi[NV], ci[NV], al[NV], li[NV * NV], ri[NV * NV];
     R sdl = d_sqrt(ql[Dn]), sdr = d_sqrt(qr[Dn]), sds = sdl + sdr;
     bool full;
@@ -542,9 +574,13 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     }
     return;
   } else {
-    fluxspeed<NV, true>(ql, ul, fl, clm, clp, P);
-    fluxspeed<NV, true>(qr, ur, fr, crm, crp, P);
+    fluxspeed<EQ, true>(ql, ul, fl, clm, clp, P);
+    fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
     R sl = d_min(clm, crm), sr = d_max(clp, crp);
+    if constexpr (V::SR && RS == RS_HLLC) {
+      srmhd_hllc(ql, qr, ul, ur, fl, fr, sl, sr, f);
+      return;
+    }
     if (sl >= R(0)) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) f[v] = fl[v];
@@ -559,7 +595,7 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     R wl[NV], wr[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) { wl[v] = sl * ul[v] - fl[v]; wr[v] = sr * ur[v] - fr[v]; }
-    if constexpr (RS == RS_HLL) {
+    if constexpr (RS == RS_HLL || V::SR) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
       return;
@@ -839,9 +875,10 @@ template <> struct Rot<0> { static constexpr int p0 = 0, p1 = 1, p2 = 2; };
 template <> struct Rot<1> { static constexpr int p0 = 1, p1 = 2, p2 = 0; };
 template <> struct Rot<2> { static constexpr int p0 = 2, p1 = 0, p2 = 1; };
 
-template <int NV, int DIR, typename R>
+template <int EQ, int DIR, typename R>
 __device__ __forceinline__ void rotate(const R* in, R* out) {
-  using V = Var<NV>; using T = Rot<DIR>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV; using T = Rot<DIR>;
 #pragma unroll
   for (int v = 0; v < NV; ++v) out[v] = in[v];
   out[V::VX + 0] = in[V::VX + T::p0]; out[V::VX + 1] = in[V::VX + T::p1]; out[V::VX + 2] = in[V::VX + T::p2];
@@ -849,9 +886,10 @@ __device__ __forceinline__ void rotate(const R* in, R* out) {
     out[V::BX + 0] = in[V::BX + T::p0]; out[V::BX + 1] = in[V::BX + T::p1]; out[V::BX + 2] = in[V::BX + T::p2];
   }
 }
-template <int NV, int DIR, typename R>
+template <int EQ, int DIR, typename R>
 __device__ __forceinline__ void unrotate(const R* in, R* out) {
-  using V = Var<NV>; using T = Rot<DIR>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV; (void)NV; using T = Rot<DIR>;
 #pragma unroll
   for (int v = 0; v < NV; ++v) out[v] = in[v];
   out[V::VX + T::p0] = in[V::VX + 0]; out[V::VX + T::p1] = in[V::VX + 1]; out[V::VX + T::p2] = in[V::VX + 2];

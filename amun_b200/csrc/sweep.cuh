@@ -37,6 +37,7 @@ struct DevScalars {
   unsigned long long ms_bits;      // max |v|+c of the current state, as bits
   unsigned long long nonpositive;  // positive variable not positive (TVD)
   long long step;
+  unsigned long long c2p_failures;  // relativistic recoveries that failed (p := 0)
 };
 
 // One SSPRK stage combination.  ds = dscoef * dt.
@@ -51,9 +52,21 @@ struct StageDesc {
 };
 
 struct MethodConst {
-  double gamma, gammam1, gammam1i, eps, decay;
+  double gamma, gammam1, gammam1i, gammaxi, eps, decay;
   int lim, clim, positivity, clip;
+  // relativistic recovery and 4-vector reconstruction
+  double tol, pmin;
+  int nrmax, nrext, states_4vec;
 };
+
+template <typename R> __device__ __forceinline__ Phys<R> make_phys(const MethodConst& m, double cmax, double cmax2) {
+  Phys<R> P;
+  P.gamma = R(m.gamma); P.gammam1 = R(m.gammam1); P.gammam1i = R(m.gammam1i); P.gammaxi = R(m.gammaxi);
+  P.eps = R(m.eps); P.cmax = R(cmax); P.cmax2 = R(cmax2);
+  P.lim = m.lim; P.clim = m.clim;
+  P.tol = m.tol; P.pmin = m.pmin; P.nrmax = m.nrmax; P.nrext = m.nrext;
+  return P;
+}
 
 template <typename R, typename U1T> struct SweepArgs {
   const R* q;          // stage input primitives (padded)
@@ -91,11 +104,13 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* t
   }
 }
 
-template <int NV, int REC, int RS, int DIR, typename R, typename U1T>
+template <int EQ, int REC, int RS, int DIR, typename R, typename U1T>
 __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
+  const bool four = V::SR && a.m.states_4vec;
   constexpr int RR = (REC == REC_WENO5Z) ? 2 : 1;
   const Geo& g = a.g;
   const int LP = a.LP, LW = a.LW;
@@ -135,8 +150,14 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
   for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
     int pp, ll; decode(t, NPQ, pp, ll);
     long long c = (long long)(p0 - RR - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+    R qc[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) Qs[sidx(v, pp, ll, NPQ)] = ld_ro(qb + c + v * g.qvs);
+    for (int v = 0; v < NV; ++v) qc[v] = ld_ro(qb + c + v * g.qvs);
+    if constexpr (V::SR) {
+      if (four) to_four_velocity(qc);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Qs[sidx(v, pp, ll, NPQ)] = qc[v];
   }
   __syncthreads();
 
@@ -146,6 +167,7 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
     for (int t = threadIdx.x; t < NPF * LW; t += blockDim.x) {
       int pp, ll; decode(t, NPF, pp, ll);
       const int cq = pp + RR;  // index of this cell in Qs
+      R fRv[NV], fLv[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         R fR, fL;
@@ -170,11 +192,21 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
             // multi-dimensional slopes, halved together while q <= sum|dq|
             const long long c = (long long)(p0 - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
             const R* qv = qb + (long long)v * g.qvs + c;
+            // neighbour value, as a 4-vector density when the states are
+            // reconstructed in 4-vector form
+            auto nq = [&](long long off) -> R {
+              if (V::SR && four && v == V::DN) {
+                const R* qc = qb + c + off;
+                R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
+                return ld_ro(qc) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
+              }
+              return ld_ro(qv + off);
+            };
             R dq[3];
-            dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sX), ld_ro(qv + sX) - f0, eps);
-            dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sY), ld_ro(qv + sY) - f0, eps);
+            dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sX), nq(sX) - f0, eps);
+            dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sY), nq(sY) - f0, eps);
             dq[2] = R(0);
-            if (g.ndims == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - ld_ro(qv - sZ), ld_ro(qv + sZ) - f0, eps);
+            if (g.ndims == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sZ), nq(sZ) - f0, eps);
             if (f0 > R(0)) {
               for (int it = 0; it < 4096; ++it) {
                 R s = d_fabs(dq[0]) + d_fabs(dq[1]);
@@ -192,8 +224,16 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
           fR = f0 + dqd;
           fL = f0 - dqd;
         }
-        FLs[sidx(v, pp, ll, NPF)] = fR;
-        FRs[sidx(v, pp, ll, NPF)] = fL;
+        fRv[v] = fR;
+        fLv[v] = fL;
+      }
+      if constexpr (V::SR) {
+        if (four) { from_four_velocity(fRv); from_four_velocity(fLv); }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        FLs[sidx(v, pp, ll, NPF)] = fRv[v];
+        FRs[sidx(v, pp, ll, NPF)] = fLv[v];
       }
     }
   }
@@ -201,19 +241,16 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
 
   // ---- Riemann problems at interfaces (p0-1)+1/2 .. (p0+LP-1)+1/2 -------------
   {
-    Phys<R> P;
-    P.gamma = R(a.m.gamma); P.gammam1 = R(a.m.gammam1); P.gammam1i = R(a.m.gammam1i);
-    P.eps = R(a.m.eps); P.cmax = R(a.sc->cmax); P.cmax2 = R(a.sc->cmax2);
-    P.lim = a.m.lim; P.clim = a.m.clim;
+    const Phys<R> P = make_phys<R>(a.m, a.sc->cmax, a.sc->cmax2);
     for (int t = threadIdx.x; t < NPI * LW; t += blockDim.x) {
       int pp, ll; decode(t, NPI, pp, ll);
       R ql[NV], qr[NV], tl[NV], tr[NV], f[NV], fo[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) { tl[v] = FLs[sidx(v, pp, ll, NPF)]; tr[v] = FRs[sidx(v, pp + 1, ll, NPF)]; }
-      rotate<NV, DIR>(tl, ql);
-      rotate<NV, DIR>(tr, qr);
-      riemann<NV, RS>(ql, qr, f, P);
-      unrotate<NV, DIR>(f, fo);
+      rotate<EQ, DIR>(tl, ql);
+      rotate<EQ, DIR>(tr, qr);
+      riemann<EQ, RS>(ql, qr, f, P);
+      unrotate<EQ, DIR>(f, fo);
 #pragma unroll
       for (int v = 0; v < NV; ++v) Fs[sidx(v, pp, ll, NPI)] = fo[v];
     }
@@ -278,15 +315,22 @@ __global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
     }
     // cons2prim of the new state (update_primitive_variables,
     // src/equations.F90:1088-1148)
-    Phys<double> Pd;
-    Pd.gamma = a.m.gamma; Pd.gammam1 = a.m.gammam1; Pd.gammam1i = a.m.gammam1i;
+    const Phys<double> Pd = make_phys<double>(a.m, 0.0, 0.0);
     double qn[NV];
-    cons2prim<NV>(un, qn, Pd);
     const long long co = (long long)b * g.qbs + (long long)(p0 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+    if constexpr (V::SR) {
+      // a failed recovery keeps the previous primitive state and sets p = 0
+      // (src/equations.F90:4745-4777)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qn[v] = (double)a.q[co + v * g.qvs];
+      if (!cons2prim_sr(un, qn, Pd)) atomicAdd(&a.sc->c2p_failures, 1ull);
+    } else {
+      cons2prim<EQ>(un, qn, Pd);
+    }
     R qs[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) { qs[v] = (R)qn[v]; a.qout[co + v * g.qvs] = qs[v]; }
-    if (final_stage) vmax = fmax(vmax, cell_speed<NV>(qs, a.m.gamma));
+    if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma));
   }
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
 }
@@ -352,7 +396,7 @@ __global__ void ghost_copy_kernel(R* q, const int* nbr, Geo g, int nv, long long
 
 // max over interior cells of |v|+c (maxspeed_*, src/equations.F90:1974,
 // 3060), accumulated into sc->ms_bits
-template <int NV, typename R>
+template <int EQ, typename R>
 __global__ void maxspeed_kernel(const R* q, Geo g, double gamma, DevScalars* sc, int nblocks) {
   const long long ncell = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1);
   const long long total = ncell * nblocks;
@@ -361,10 +405,11 @@ __global__ void maxspeed_kernel(const R* q, Geo g, double gamma, DevScalars* sc,
     long long b = t / ncell, c = t - b * ncell;
     int i = (int)(c % g.nc), j = (int)((c / g.nc) % g.nc), k = (int)(c / ((long long)g.nc * g.nc));
     long long o = b * g.qbs + ((long long)(g.ndims == 3 ? k + g.ng : 0) * g.JM + (j + g.ng)) * g.IM + (i + g.ng);
+    constexpr int NV = Var<EQ>::NV;
     R qc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = q[o + v * g.qvs];
-    vmax = fmax(vmax, cell_speed<NV>(qc, gamma));
+    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma));
   }
   block_max_atomic(vmax, &sc->ms_bits);
 }
@@ -436,8 +481,9 @@ __global__ void download_q_kernel(const R* q, double* fq, Geo g, int nv, int b0,
 // u (Fortran layout, all cells): interior from the state array, ghosts from
 // prim2cons of the ghost primitives (update_ghost_cells,
 // src/boundaries.F90:6633-6736)
-template <int NV, typename R, typename UT>
-__global__ void download_u_kernel(const UT* u, const R* q, double* fu, Geo g, double gammam1i, int b0, int nb) {
+template <int EQ, typename R, typename UT>
+__global__ void download_u_kernel(const UT* u, const R* q, double* fu, Geo g, MethodConst m, int b0, int nb) {
+  constexpr int NV = Var<EQ>::NV;
   const long long cells = (long long)g.IM * g.JM * g.KM;
   const long long total = cells * nb;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
@@ -454,8 +500,8 @@ __global__ void download_u_kernel(const UT* u, const R* q, double* fu, Geo g, do
       double qc[NV], uc[NV];
       const R* src = q + (b0 + bb) * g.qbs + c;
       for (int v = 0; v < NV; ++v) qc[v] = (double)src[v * g.qvs];
-      Phys<double> P; P.gammam1i = gammam1i;
-      prim2cons<NV>(qc, uc, P);
+      const Phys<double> P = make_phys<double>(m, 0.0, 0.0);
+      prim2cons<EQ>(qc, uc, P);
       for (int v = 0; v < NV; ++v) dst[v] = uc[v];
     }
   }

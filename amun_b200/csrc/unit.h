@@ -7,9 +7,11 @@
 namespace amun {
 
 struct UnitArgs {
-  int nv, ndims, im, jm, km, ng;
+  int nv, eq, ndims, im, jm, km, ng;
   int rec, lim, clim, rs, clip, positivity;
-  double gamma, eps, cmax;
+  double gamma, gammaxi, eps, cmax;
+  double tol, pmin;
+  int nrmax, nrext, states_4vec;
 };
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,

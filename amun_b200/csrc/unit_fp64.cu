@@ -30,9 +30,10 @@ __global__ void tvd_ghost_copy(const double* q, double* qs, BlockDims d) {
   }
 }
 
-template <int NV>
+template <int EQ>
 __global__ void tvd_box(const double* q, double* qs, BlockDims d, int lim, double eps, unsigned long long* nonpos) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
   const int nx = d.im - 2 * d.ng + 2, ny = d.jm - 2 * d.ng + 2, nz = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
   const long long cells = (long long)d.im * d.jm * d.km;
   const long long n = (long long)nx * ny * nz;
@@ -75,10 +76,11 @@ __global__ void tvd_box(const double* q, double* qs, BlockDims d, int lim, doubl
 // 1343-1381): one thread per (variable, line); the line is reconstructed
 // with reconstruct_weno5z (1937-2083) including its line-end fallbacks, then
 // clip_extrema (5081-5175) and fix_positivity (4987-5062) run sequentially.
-template <int NV>
+template <int EQ>
 __global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int lim, int clim, double eps,
                           int clip, int positivity, double* scratch) {
-  using V = Var<NV>;
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
   const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
   int a0, a1, n;  // line counts
   long long stride, s0, s1;
@@ -149,8 +151,9 @@ __global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int
 }
 
 // Riemann along every flux line of direction dir; f(NDIMS,nv,im,jm,km).
-template <int NV, int RS, int DIR>
+template <int EQ, int RS, int DIR>
 __global__ void block_riemann(const double* qs, double* f, BlockDims d, Phys<double> P) {
+  constexpr int NV = Var<EQ>::NV;
   const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
   const long long sx = 1, sy = d.im, sz = (long long)d.im * d.jm;
   const long long cells = (long long)d.im * d.jm * d.km;
@@ -172,36 +175,40 @@ __global__ void block_riemann(const double* qs, double* f, BlockDims d, Phys<dou
       tl[v] = qs[((long long)(2 * DIR + 0) * cells + cc) * NV + v];
       tr[v] = qs[((long long)(2 * DIR + 1) * cells + cc) * NV + v];
     }
-    rotate<NV, DIR>(tl, ql);
-    rotate<NV, DIR>(tr, qr);
-    riemann<NV, RS>(ql, qr, fx, P);
-    unrotate<NV, DIR>(fx, fo);
+    rotate<EQ, DIR>(tl, ql);
+    rotate<EQ, DIR>(tr, qr);
+    riemann<EQ, RS>(ql, qr, fx, P);
+    unrotate<EQ, DIR>(fx, fo);
     for (int v = 0; v < NV; ++v) f[(cc * NV + v) * d.ndims + DIR] = fo[v];
   }
 }
 
-template <int NV, int RS>
+template <int EQ, int RS>
 __global__ void line_riemann(int n, const double* ql_, const double* qr_, double* f_, Phys<double> P) {
+  constexpr int NV = Var<EQ>::NV;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     double ql[NV], qr[NV], f[NV];
     for (int v = 0; v < NV; ++v) { ql[v] = ql_[t * NV + v]; qr[v] = qr_[t * NV + v]; }
-    riemann<NV, RS>(ql, qr, f, P);
+    riemann<EQ, RS>(ql, qr, f, P);
     for (int v = 0; v < NV; ++v) f_[t * NV + v] = f[v];
   }
 }
 
-template <int NV>
+template <int EQ>
 __global__ void pointwise(int op, int n, const double* a, const double* b, double* o, double* cm, double* cp,
                           Phys<double> P) {
+  constexpr int NV = Var<EQ>::NV;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     double x[NV], y[NV], z[NV];
     for (int v = 0; v < NV; ++v) x[v] = a[t * NV + v];
-    if (op == 0) prim2cons<NV>(x, z, P);
-    else if (op == 1) cons2prim<NV>(x, z, P);
-    else {
+    if (op == 0) prim2cons<EQ>(x, z, P);
+    else if (op == 1) {
+      for (int v = 0; v < NV; ++v) z[v] = 0.0;
+      cons2prim<EQ>(x, z, P);
+    } else {
       for (int v = 0; v < NV; ++v) y[v] = b[t * NV + v];
       double m, p;
-      fluxspeed<NV, true>(x, y, z, m, p, P);
+      fluxspeed<EQ, true>(x, y, z, m, p, P);
       if (cm) cm[t] = m;
       if (cp) cp[t] = p;
     }
@@ -209,8 +216,9 @@ __global__ void pointwise(int op, int n, const double* a, const double* b, doubl
   }
 }
 
-template <int NV>
+template <int EQ>
 __global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsigned long long* out) {
+  constexpr int NV = Var<EQ>::NV;
   const int nx = d.im - 2 * d.ng, ny = d.jm - 2 * d.ng, nz = d.ndims == 3 ? d.km - 2 * d.ng : 1;
   const long long n = (long long)nx * ny * nz;
   double vmax = 0.0;
@@ -220,7 +228,7 @@ __global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsig
     long long c = i + (long long)d.im * (j + (long long)d.jm * k);
     double qc[NV];
     for (int v = 0; v < NV; ++v) qc[v] = q[c * NV + v];
-    vmax = fmax(vmax, cell_speed<NV>(qc, gamma));
+    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma));
   }
   unsigned mask = 0xffffffffu;
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(mask, vmax, o));
@@ -228,100 +236,134 @@ __global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsig
 }
 
 // ---------------------------------------------------------------------------
-template <int NV, int RS>
+template <int EQ, int RS>
 static cudaError_t riemann_dirs(const double* qs, double* f, BlockDims d, const Phys<double>& P, cudaStream_t s) {
   for (int dir = 0; dir < d.ndims; ++dir) {
     const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
     long long total = dir == 0 ? (long long)nj * nk * d.im : (dir == 1 ? (long long)ni * nk * d.jm : (long long)ni * nj * d.km);
     int grid = (int)((total + 255) / 256);
-    if (dir == 0) block_riemann<NV, RS, 0><<<grid, 256, 0, s>>>(qs, f, d, P);
-    else if (dir == 1) block_riemann<NV, RS, 1><<<grid, 256, 0, s>>>(qs, f, d, P);
-    else block_riemann<NV, RS, 2><<<grid, 256, 0, s>>>(qs, f, d, P);
+    if (dir == 0) block_riemann<EQ, RS, 0><<<grid, 256, 0, s>>>(qs, f, d, P);
+    else if (dir == 1) block_riemann<EQ, RS, 1><<<grid, 256, 0, s>>>(qs, f, d, P);
+    else block_riemann<EQ, RS, 2><<<grid, 256, 0, s>>>(qs, f, d, P);
   }
   return cudaGetLastError();
 }
 
-template <int NV>
-static cudaError_t block_flux_nv(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,
+// 4-vector states for SRMHD reconstruction (src/schemes.F90:5043-5100):
+// to 4-velocity before reconstructing, face states back afterwards
+__global__ void four_vector_kernel(double* q, long long n, int forward) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double* c = q + t * 9;
+    if (forward) to_four_velocity(c); else from_four_velocity(c);
+  }
+}
+
+static Phys<double> unit_phys(const UnitArgs& u) {
+  Phys<double> P{};
+  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0); P.gammaxi = u.gammaxi;
+  P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax; P.lim = u.lim; P.clim = u.clim;
+  P.tol = u.tol; P.pmin = u.pmin; P.nrmax = u.nrmax; P.nrext = u.nrext;
+  return P;
+}
+
+template <int EQ>
+static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,
                                  unsigned long long* nonpos, cudaStream_t s) {
+  constexpr int NV = Var<EQ>::NV;
   BlockDims d{NV, u.ndims, u.im, u.jm, u.km, u.ng};
   long long cells = (long long)u.im * u.jm * u.km;
+  const bool four = Var<EQ>::SR && u.states_4vec;
+  const double* qr = q;
+  if (four) {
+    // reconstruct 4-vector states: the converted copy lives in the scratch tail
+    double* qq = scratch + unit_block_flux_scratch(u) / sizeof(double) - cells * NV;
+    cudaMemcpyAsync(qq, q, cells * NV * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    four_vector_kernel<<<(int)((cells + 255) / 256), 256, 0, s>>>(qq, cells, 1);
+    qr = qq;
+  }
+  tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(qr, qs, d);
   if (u.rec == REC_TVD) {
-    tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(q, qs, d);
     const long long nbox = (long long)(u.im - 2 * u.ng + 2) * (u.jm - 2 * u.ng + 2) * (u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1);
-    tvd_box<NV><<<(int)((nbox + 255) / 256), 256, 0, s>>>(q, qs, d, u.lim, u.eps, nonpos);
+    tvd_box<EQ><<<(int)((nbox + 255) / 256), 256, 0, s>>>(qr, qs, d, u.lim, u.eps, nonpos);
   } else {
-    tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(q, qs, d);
     for (int dir = 0; dir < u.ndims; ++dir) {
       const int ni = u.im - 2 * u.ng + 2, nj = u.jm - 2 * u.ng + 2, nk = u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1;
       long long lines = (dir == 0 ? (long long)nj * nk : (dir == 1 ? (long long)ni * nk : (long long)ni * nj)) * NV;
-      dir_lines<NV><<<(int)((lines + 127) / 128), 128, 0, s>>>(q, qs, d, dir, u.lim, u.clim, u.eps, u.clip,
+      dir_lines<EQ><<<(int)((lines + 127) / 128), 128, 0, s>>>(qr, qs, d, dir, u.lim, u.clim, u.eps, u.clip,
                                                                u.positivity, scratch);
     }
   }
-  Phys<double> P{};
-  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
-  P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax; P.lim = u.lim; P.clim = u.clim;
-  if (NV == 5) {
-    switch (u.rs) {
-      case RS_HLLC: return riemann_dirs<NV, RS_HLLC>(qs, f, d, P, s);
-      case RS_ROE: return riemann_dirs<NV, RS_ROE>(qs, f, d, P, s);
-      default: return riemann_dirs<NV, RS_HLL>(qs, f, d, P, s);
-    }
+  if (four) {
+    long long nstates = cells * 2 * u.ndims;
+    four_vector_kernel<<<(int)((nstates + 255) / 256), 256, 0, s>>>(qs, nstates, 0);
   }
-  switch (u.rs) {
-    case RS_HLLC: return riemann_dirs<NV, RS_HLLC>(qs, f, d, P, s);
-    case RS_HLLD: return riemann_dirs<NV, RS_HLLD>(qs, f, d, P, s);
-    case RS_ROE: return riemann_dirs<NV, RS_ROE>(qs, f, d, P, s);
-    default: return riemann_dirs<NV, RS_HLL>(qs, f, d, P, s);
+  const Phys<double> P = unit_phys(u);
+  if constexpr (EQ == EQ_HD) {
+    switch (u.rs) {
+      case RS_HLLC: return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
+      case RS_ROE: return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
+      default: return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
+    }
+  } else if constexpr (EQ == EQ_MHD) {
+    switch (u.rs) {
+      case RS_HLLC: return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
+      case RS_HLLD: return riemann_dirs<EQ, RS_HLLD>(qs, f, d, P, s);
+      case RS_ROE: return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
+      default: return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
+    }
+  } else {
+    if (u.rs == RS_HLLC) return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
+    return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
   }
 }
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,
                             unsigned long long* nonpos, cudaStream_t s) {
-  if (u.nv == 5) return block_flux_nv<5>(u, q, qs, f, scratch, nonpos, s);
-  return block_flux_nv<9>(u, q, qs, f, scratch, nonpos, s);
+  if (u.eq == EQ_HD) return block_flux_eq<EQ_HD>(u, q, qs, f, scratch, nonpos, s);
+  if (u.eq == EQ_MHD) return block_flux_eq<EQ_MHD>(u, q, qs, f, scratch, nonpos, s);
+  return block_flux_eq<EQ_SRMHD>(u, q, qs, f, scratch, nonpos, s);
 }
 
 size_t unit_block_flux_scratch(const UnitArgs& u) {
   int n = u.im > u.jm ? u.im : u.jm;
   if (u.km > n) n = u.km;
   long long lines = (long long)(n + 2) * (n + 2) * u.nv;
-  return (size_t)lines * 3 * n * sizeof(double);
+  long long cells = (long long)u.im * u.jm * u.km;
+  return (size_t)(lines * 3 * n + cells * u.nv) * sizeof(double);
 }
 
 cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const double* qr, double* f, cudaStream_t s) {
-  Phys<double> P{};
-  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
-  P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax;
+  const Phys<double> P = unit_phys(u);
   int grid = (n + 127) / 128;
   if (grid < 1) grid = 1;
-  if (u.nv == 5) {
+  if (u.eq == EQ_HD) {
     switch (u.rs) {
-      case RS_HLLC: line_riemann<5, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-      case RS_ROE: line_riemann<5, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-      default: line_riemann<5, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_HLLC: line_riemann<EQ_HD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_ROE: line_riemann<EQ_HD, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      default: line_riemann<EQ_HD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+    }
+  } else if (u.eq == EQ_MHD) {
+    switch (u.rs) {
+      case RS_HLLC: line_riemann<EQ_MHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_HLLD: line_riemann<EQ_MHD, RS_HLLD><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_ROE: line_riemann<EQ_MHD, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      default: line_riemann<EQ_MHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
     }
   } else {
-    switch (u.rs) {
-      case RS_HLLC: line_riemann<9, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-      case RS_HLLD: line_riemann<9, RS_HLLD><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-      case RS_ROE: line_riemann<9, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-      default: line_riemann<9, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
-    }
+    if (u.rs == RS_HLLC) line_riemann<EQ_SRMHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+    else line_riemann<EQ_SRMHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   }
   return cudaGetLastError();
 }
 
 cudaError_t unit_pointwise(const UnitArgs& u, int op, int n, const double* a, const double* b, double* o, double* cm,
                            double* cp, cudaStream_t s) {
-  Phys<double> P{};
-  P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0);
-  P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax;
+  const Phys<double> P = unit_phys(u);
   int grid = (n + 127) / 128;
   if (grid < 1) grid = 1;
-  if (u.nv == 5) pointwise<5><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
-  else pointwise<9><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  if (u.eq == EQ_HD) pointwise<EQ_HD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else if (u.eq == EQ_MHD) pointwise<EQ_MHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else pointwise<EQ_SRMHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   return cudaGetLastError();
 }
 
@@ -330,8 +372,9 @@ cudaError_t unit_maxspeed(const UnitArgs& u, const double* q, unsigned long long
   long long n = (long long)(u.im - 2 * u.ng) * (u.jm - 2 * u.ng) * (u.ndims == 3 ? u.km - 2 * u.ng : 1);
   int grid = (int)((n + 255) / 256);
   if (grid > 4096) grid = 4096;
-  if (u.nv == 5) block_maxspeed<5><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
-  else block_maxspeed<9><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  if (u.eq == EQ_HD) block_maxspeed<EQ_HD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  else if (u.eq == EQ_MHD) block_maxspeed<EQ_MHD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  else block_maxspeed<EQ_SRMHD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
   return cudaGetLastError();
 }
 

@@ -166,6 +166,21 @@ def turbulence(mesh, gamma: float, seed: int = 0, mach: float = 1.0) -> np.ndarr
     return q
 
 
+def srmhd_turbulence(mesh, seed: int = 0, lorentz_max: float = 10.0) -> np.ndarray:
+    """Relativistic MHD box: rho=1, p=1, B=(0.5,0,0), psi=0; velocity the
+    random-phase field of `turbulence` rescaled so the largest Lorentz factor
+    is `lorentz_max` (max |v|^2 = 1 - 1/lorentz_max^2)."""
+    q = uniform(mesh, MHD_NV, 1.0, 1.0, mag=(0.5, 0.0, 0.0))
+    shp = mesh.shape if mesh.ndims == 3 else mesh.shape[1:]
+    v = random_phase_field(shp, seed)
+    if mesh.ndims == 2:
+        v = v[None]
+    vmax = math.sqrt(1.0 - 1.0 / lorentz_max ** 2)
+    v *= vmax / math.sqrt(np.max(np.sum(v * v, axis=-1)))
+    q[..., VX:VZ + 1] = v
+    return q
+
+
 def smooth_mhd(mesh, seed: int = 0) -> np.ndarray:
     """2D smooth MHD state: rho = 1 + 0.01 * (random Fourier modes with
     integer 1<=|k|<=4, normalised to max 1), p = 1,

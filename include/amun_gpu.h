@@ -33,7 +33,7 @@ extern "C" {
 #define AMUN_E_NO_BLOCKS       905
 
 /* equation_system / equation_of_state (src/equations.F90:322-833) */
-enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1 };
+enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2 };
 /* reconstruction (src/interpolations.F90:226-382) */
 enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
 /* limiter / extrema_limiter (src/interpolations.F90:389-445) */
@@ -69,6 +69,12 @@ typedef struct amun_params {
   double cfl;           /*                        "cfl"                       */
   double alpha;         /*                        "alpha" (GLM psi decay)     */
   double eps;           /*                        "eps" (WENO-Z, van Albada)  */
+  /* relativistic recovery (src/equations.F90:184-201, 313-318) */
+  double tolerance;     /*                        "tolerance"                 */
+  double pmin;          /*                        "pmin"                      */
+  int nr_maxit;         /*                        "nr_maxit"                  */
+  int nr_extra;         /*                        "nr_extra"                  */
+  int states_4vec;      /* 0/1                    "state_variables" = "4vec"  */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block
@@ -86,6 +92,8 @@ typedef struct amun_status {
   long long step;
   long long nonpositive;  /* "Positive variable is not positive" events of
                              interfaces_tvd (src/interpolations.F90:813-823) */
+  long long c2p_failures; /* relativistic recoveries that failed or gave
+                             p <= 0 (src/equations.F90:4745-4777)           */
   long long device_bytes; /* bytes of device memory held by the block pool    */
 } amun_status;
 

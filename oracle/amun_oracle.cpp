@@ -1773,6 +1773,22 @@ struct Oracle {
     std::fill(f, f + (size_t)p.ndims * nv * N, 0.0);
     std::vector<double> qs((size_t)nv * N * 2 * p.ndims);
     std::vector<double> one(N), ones(N * 2 * p.ndims);
+    // update_flux_srmhd_adi with state_variables = "4vec" (src/schemes.F90:
+    // 5043-5100): reconstruct D = rho Gamma and u = Gamma v, convert back after
+    const bool four = p.eqsys == EQ_SRMHD && p.states_4vec;
+    std::vector<double> qq;
+    if (four) {
+      qq.assign(q, q + (size_t)nv * N);
+      for (size_t c = 0; c < N; ++c) {
+        double* Q = &qq[(size_t)nv * c];
+        double vm = std::sqrt(1.0 - (Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1]));
+        Q[idn - 1] = Q[idn - 1] / vm;
+        Q[ivx - 1] = Q[ivx - 1] / vm;
+        Q[ivy - 1] = Q[ivy - 1] / vm;
+        Q[ivz - 1] = Q[ivz - 1] / vm;
+      }
+      q = qq.data();
+    }
     // reconstruct_interfaces: per variable, positive = density or pressure
     for (int pv = 1; pv <= nv; ++pv) {
       bool positive = (pv == idn || pv == ipr);
@@ -1782,6 +1798,16 @@ struct Oracle {
       // scatter to qs(nv,im,jm,km,2,NDIMS)
       for (size_t sd = 0; sd < (size_t)2 * p.ndims; ++sd)
         for (size_t c = 0; c < N; ++c) qs[(size_t)(pv - 1) + (size_t)nv * (c + N * sd)] = ones[c + N * sd];
+    }
+    if (four) {
+      for (size_t c = 0; c < N * 2 * p.ndims; ++c) {
+        double* Q = &qs[(size_t)nv * c];
+        double vm = std::sqrt(1.0 + (Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1]));
+        Q[idn - 1] = Q[idn - 1] / vm;
+        Q[ivx - 1] = Q[ivx - 1] / vm;
+        Q[ivy - 1] = Q[ivy - 1] / vm;
+        Q[ivz - 1] = Q[ivz - 1] / vm;
+      }
     }
     static const int perm[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
     int nmax = std::max(im, std::max(jm, km));
