@@ -105,7 +105,10 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* t
 }
 
 template <int EQ, int REC, int RS, int DIR, typename R, typename U1T>
-__global__ void __launch_bounds__(288) sweep_kernel(const SweepArgs<R, U1T> a) {
+#ifndef AMUN_SWEEP_MIN_BLOCKS
+#define AMUN_SWEEP_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const SweepArgs<R, U1T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sm = reinterpret_cast<R*>(smem_raw);
   using V = Var<EQ>;

@@ -27,7 +27,7 @@ class Simulation:
         self.native = to_native(self.params)
         self.geo = geometry(self.params)
         self.mesh = UniformMesh(self.geo)
-        self.nv = 9 if self.native.eqsys == N.AMUN_EQ_MHD else 5
+        self.nv = 5 if self.native.eqsys == N.AMUN_EQ_HD else 9
         N.check(self.L.amun_gpu_init(C.byref(self.native)))
         self._desc = self.mesh.descriptors()
         N.check(self.L.amun_gpu_set_blocks(self.mesh.nblocks, self._desc))
@@ -44,8 +44,11 @@ class Simulation:
         N.check(self.L.amun_gpu_set_time(0.0, 0.0))
 
     def upload_blocks(self, u0: np.ndarray, q: np.ndarray):
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
         u0 = np.ascontiguousarray(u0, dtype=np.float64)
         q = np.ascontiguousarray(q, dtype=np.float64)
+        if u0.shape != shp or q.shape != shp:
+            raise ValueError(f"expected block arrays of shape {shp}")
         N.check(self.L.amun_gpu_upload_blocks(0, self.mesh.nblocks, N.dptr(u0), N.dptr(q)))
 
     def download_blocks(self, u0: np.ndarray | None = None, q: np.ndarray | None = None):
@@ -54,6 +57,9 @@ class Simulation:
             u0 = np.empty(shp)
         if q is None:
             q = np.empty(shp)
+        if u0.shape != shp or q.shape != shp or u0.dtype != np.float64 or q.dtype != np.float64 \
+                or not (u0.flags["C_CONTIGUOUS"] and q.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"expected C-contiguous float64 block arrays of shape {shp}")
         N.check(self.L.amun_gpu_download_blocks(0, self.mesh.nblocks, N.dptr(u0), N.dptr(q)))
         return u0, q
 
@@ -89,32 +95,40 @@ class Simulation:
         s = N.amun_status()
         N.check(self.L.amun_gpu_status(C.byref(s)))
         return dict(time=s.time, dt=s.dt, dtn=s.dtn, cmax=s.cmax, step=s.step,
-                    nonpositive=s.nonpositive, device_bytes=s.device_bytes)
+                    nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes)
+
+    def _states(self, a: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.ndim == 0 or a.shape[-1] != self.nv:
+            raise ValueError(f"expected states with {self.nv} variables in the last axis, got shape {a.shape}")
+        return a
 
     # ---- per-procedure entry points (FP64) -------------------------------------
     def prim2cons(self, q: np.ndarray) -> np.ndarray:
-        q = np.ascontiguousarray(q, dtype=np.float64)
+        q = self._states(q)
         u = np.empty_like(q)
         N.check(self.L.amun_gpu_prim2cons(q.size // self.nv, N.dptr(q), N.dptr(u)))
         return u
 
     def cons2prim(self, u: np.ndarray) -> np.ndarray:
-        u = np.ascontiguousarray(u, dtype=np.float64)
+        u = self._states(u)
         q = np.empty_like(u)
         N.check(self.L.amun_gpu_cons2prim(u.size // self.nv, N.dptr(u), N.dptr(q)))
         return q
 
     def fluxspeed(self, q: np.ndarray, u: np.ndarray):
-        q = np.ascontiguousarray(q, dtype=np.float64)
-        u = np.ascontiguousarray(u, dtype=np.float64)
+        q, u = self._states(q), self._states(u)
+        if q.shape != u.shape:
+            raise ValueError("q and u differ in shape")
         n = q.size // self.nv
         f, cm, cp = np.empty_like(q), np.empty(n), np.empty(n)
         N.check(self.L.amun_gpu_fluxspeed(n, N.dptr(q), N.dptr(u), N.dptr(f), N.dptr(cm), N.dptr(cp)))
         return f, cm, cp
 
     def riemann(self, ql: np.ndarray, qr: np.ndarray) -> np.ndarray:
-        ql = np.ascontiguousarray(ql, dtype=np.float64)
-        qr = np.ascontiguousarray(qr, dtype=np.float64)
+        ql, qr = self._states(ql), self._states(qr)
+        if ql.shape != qr.shape:
+            raise ValueError("ql and qr differ in shape")
         f = np.empty_like(ql)
         N.check(self.L.amun_gpu_riemann(ql.size // self.nv, N.dptr(ql), N.dptr(qr), N.dptr(f)))
         return f
@@ -124,7 +138,9 @@ class Simulation:
 
     def update_flux_block(self, qblock: np.ndarray) -> np.ndarray:
         """update_flux on one block array (km,jm,im,nv) -> f (km,jm,im,nv,NDIMS)."""
-        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        qblock = self._states(qblock)
+        if qblock.shape != (self.mesh.km, self.mesh.jm, self.mesh.im, self.nv):
+            raise ValueError(f"expected one block array of shape {(self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)}")
         nd = self.mesh.ndims
         f = np.zeros(qblock.shape + (nd,))
         dx = np.array([self.mesh.dx, self.mesh.dy, self.mesh.dz][:nd])
@@ -132,7 +148,9 @@ class Simulation:
         return f
 
     def maxspeed_block(self, qblock: np.ndarray) -> float:
-        qblock = np.ascontiguousarray(qblock, dtype=np.float64)
+        qblock = self._states(qblock)
+        if qblock.shape != (self.mesh.km, self.mesh.jm, self.mesh.im, self.nv):
+            raise ValueError("expected one block array")
         out = C.c_double()
         N.check(self.L.amun_gpu_maxspeed(N.dptr(qblock), C.byref(out)))
         return out.value
