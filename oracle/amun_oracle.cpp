@@ -1825,7 +1825,7 @@ struct Oracle {
           double* L = &ql[(size_t)nv * t]; double* R = &qr[(size_t)nv * t];
           for (int v = 0; v < nv; ++v) { L[v] = sl_[v]; R[v] = sr_[v]; }
           for (int m = 0; m < 3; ++m) { L[ivx - 1 + m] = sl_[ivx - 1 + pm[m]]; R[ivx - 1 + m] = sr_[ivx - 1 + pm[m]]; }
-          if (p.eqsys == EQ_MHD)
+          if (p.eqsys != EQ_HD)
             for (int m = 0; m < 3; ++m) { L[ibx - 1 + m] = sl_[ibx - 1 + pm[m]]; R[ibx - 1 + m] = sr_[ibx - 1 + pm[m]]; }
         }
         riemann_line(n, ql.data(), qr.data(), fx.data());
@@ -1836,7 +1836,7 @@ struct Oracle {
           double tmp[9];
           for (int v = 0; v < nv; ++v) tmp[v] = F[v];
           for (int m = 0; m < 3; ++m) tmp[imx - 1 + pm[m]] = F[imx - 1 + m];
-          if (p.eqsys == EQ_MHD)
+          if (p.eqsys != EQ_HD)
             for (int m = 0; m < 3; ++m) tmp[ibx - 1 + pm[m]] = F[ibx - 1 + m];
           for (int v = 0; v < nv; ++v) f[fi(d, v + 1, i, j, k)] = tmp[v];
         }
@@ -2198,6 +2198,7 @@ void or_advance(void* h, double dtnext, double* time, double* dt) {
 void or_scalars(void* h, double* out) {
   Oracle* o = static_cast<Oracle*>(h);
   out[0] = o->time; out[1] = o->dt; out[2] = o->cmax; out[3] = (double)o->step; out[4] = (double)o->nonpositive;
+  out[5] = (double)o->c2p_failures;
 }
 
 // ---- unit-level entry points ------------------------------------------------

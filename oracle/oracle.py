@@ -134,9 +134,10 @@ class Oracle:
         return t.value, dt.value
 
     def scalars(self) -> dict:
-        s = (C.c_double * 5)()
+        s = (C.c_double * 6)()
         self.L.or_scalars(self.h, s)
-        return dict(time=s[0], dt=s[1], cmax=s[2], step=int(s[3]), nonpositive=int(s[4]))
+        return dict(time=s[0], dt=s[1], cmax=s[2], step=int(s[3]), nonpositive=int(s[4]),
+                    c2p_failures=int(s[5]))
 
     # ---- unit level --------------------------------------------------------
     def set_cmax(self, cmax: float):

@@ -2,8 +2,10 @@
 
 The SR root solvers use cube roots, acos and cos, which CUDA and the host
 math library round differently in the last ulp, so these comparisons use a
-relative tolerance (1e-10 per state after several steps, 1e-11 per
-procedure) instead of bit equality."""
+relative tolerance instead of bit equality: 1e-11 per state for the
+pointwise procedures, and for fields 1e-10 of each variable's largest
+magnitude (components that are zero in the initial state, such as psi and
+Bz, grow from round-off and have no meaningful pointwise relative error)."""
 import numpy as np
 import pytest
 
@@ -27,6 +29,18 @@ def close(a, b, rtol, what):
     assert not np.isnan(a).any(), f"{what}: NaN on the GPU"
     err = np.max(np.abs(a - b) / (np.abs(b) + 1e-12))
     assert err <= rtol, f"{what}: max relative difference {err:.3e} > {rtol}"
+
+
+def close_field(a, b, rtol, what, vaxis=-1):
+    """Agreement per variable, relative to that variable's largest |value|."""
+    a, b = np.moveaxis(np.asarray(a), vaxis, -1), np.moveaxis(np.asarray(b), vaxis, -1)
+    assert not np.isnan(b).any(), f"{what}: NaN in the oracle"
+    assert not np.isnan(a).any(), f"{what}: NaN on the GPU"
+    nv = a.shape[-1]
+    a, b = a.reshape(-1, nv), b.reshape(-1, nv)
+    scale = np.maximum(np.max(np.abs(b), axis=0), 1e-300)
+    err = np.max(np.abs(a - b), axis=0) / scale
+    assert np.all(err <= rtol), f"{what}: per-variable relative difference {err} > {rtol}"
 
 
 def sr(rs="hll", rec="tvd", **kw):
@@ -75,32 +89,58 @@ def test_update_flux_block(Sim, oracle_mod, rec, four):
     o.set_cmax(1.0)
     mesh = UniformMesh(geometry(p))
     q = mesh.to_blocks(problems.srmhd_turbulence(mesh, seed=1, lorentz_max=4.0))[0]
-    close(s.update_flux_block(q), o.update_flux(q), 1e-10, f"update_flux {rec} 4vec={four}")
+    close_field(s.update_flux_block(q), o.update_flux(q), 1e-10, f"update_flux {rec} 4vec={four}", vaxis=-2)
 
 
-@pytest.mark.parametrize("rs,four", [("hll", False), ("hllc", False), ("hll", True)])
-def test_srmhd_steps(Sim, oracle_mod, rs, four):
-    """The relativistic configuration's scheme (TVD-MC, HLL, SSPRK(2,2),
-    FP64 Newton recovery with tolerance 1e-12 and at most 50 iterations) on a
-    16^3 periodic box with Lorentz factors up to 10."""
+@pytest.mark.parametrize("rs,four,lorentz", [("hll", False, 2.5), ("hllc", False, 2.5),
+                                            ("hll", True, 10.0), ("hllc", True, 10.0)])
+def test_srmhd_steps(Sim, oracle_mod, rs, four, lorentz):
+    """The relativistic configuration's scheme (TVD-MC, SSPRK(2,2), FP64
+    Newton recovery with tolerance 1e-12 and at most 50 iterations) on a
+    16^3 periodic box: primitive-state reconstruction at Lorentz factors up
+    to 2.5, 4-vector reconstruction up to 10."""
     p = sr(rs, "tvd", ndims=3, ncells=16, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1,
            state_variables="4vec" if four else "primitive")
     s, o = Sim(p), oracle_mod.Oracle(p)
-    q0 = problems.srmhd_turbulence(s.mesh, seed=0)
+    q0 = problems.srmhd_turbulence(s.mesh, seed=0, lorentz_max=lorentz)
     s.set_primitive(q0)
     o.set_prim(q0)
     for _ in range(4):
         ts, dts = s.advance(1.0)
         to, dto = o.advance(1.0)
         assert dts == dto  # cmax = 1 for SRMHD: dt depends on the mesh only
-    close(s.conserved(), o.cons(), 1e-10, f"srmhd {rs} 4vec={four}")
-    assert s.status()["c2p_failures"] == 0
+    close_field(s.conserved(), o.cons(), 1e-10, f"srmhd {rs} 4vec={four}")
+    # HLLC at Lorentz factor 10 fails 4 recoveries in the 4th step (2 cells
+    # end at p = 0) in both implementations
+    assert s.status()["c2p_failures"] == o.scalars()["c2p_failures"]
+
+
+def test_srmhd_recovery_failure_parity(Sim, oracle_mod):
+    """Primitive-state reconstruction at Lorentz factor 10 produces states
+    whose recovery fails; the reference then sets the pressure to zero
+    (src/equations.F90:4749-4776).  After one step the GPU fails in the same
+    cells, counts the same number of failures, and agrees elsewhere."""
+    p = sr("hll", "tvd", ndims=3, ncells=16, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1)
+    s, o = Sim(p), oracle_mod.Oracle(p)
+    q0 = problems.srmhd_turbulence(s.mesh, seed=0, lorentz_max=10.0)
+    s.set_primitive(q0)
+    o.set_prim(q0)
+    s.advance(1.0)
+    o.advance(1.0)
+    qs, qo = s.primitive(), o.prim()
+    failed = qo[..., 8] == 0.0
+    assert failed.any()
+    assert np.array_equal(qs[..., 8] == 0.0, failed)
+    assert s.status()["c2p_failures"] == o.scalars()["c2p_failures"]
+    close_field(s.conserved(), o.cons(), 1e-10, "conserved after failures")
 
 
 def test_srmhd_fp32_bulk(Sim, oracle_mod):
     """FP32 fluxes with the FP64 Newton recovery: density within 1e-4
-    relative L1 of the FP64 oracle after 10 steps at Lorentz factor 10."""
-    p = sr("hll", "tvd", ndims=3, ncells=16, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1)
+    relative L1 of the FP64 oracle after 10 steps at Lorentz factor 10
+    (4-vector reconstruction)."""
+    p = sr("hll", "tvd", ndims=3, ncells=16, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1,
+           state_variables="4vec")
     s, o = Sim(p, "fp32"), oracle_mod.Oracle(p)
     q0 = problems.srmhd_turbulence(s.mesh, seed=0)
     s.set_primitive(q0)
@@ -111,4 +151,4 @@ def test_srmhd_fp32_bulk(Sim, oracle_mod):
     d_s, d_o = s.conserved()[..., 0], o.cons()[..., 0]
     l1 = np.sum(np.abs(d_s - d_o)) / np.sum(np.abs(d_o))
     assert l1 <= 1e-4, l1
-    assert s.status()["c2p_failures"] == 0
+    assert s.status()["c2p_failures"] == 0 == o.scalars()["c2p_failures"]

@@ -7,8 +7,9 @@ from helpers import params
 
 
 def sr_params(rs="hll", **kw):
-    p = params("srmhd", "tvd", rs, "rk2", ncells=8, gamma=4.0 / 3.0, tolerance=1e-12, nr_maxit=50, **kw)
-    return p
+    base = dict(ncells=8, gamma=4.0 / 3.0, tolerance=1e-12, nr_maxit=50)
+    base.update(kw)
+    return params("srmhd", "tvd", rs, "rk2", **base)
 
 
 def sr_states(rng, n, gmax=10.0, bmax=2.0):
@@ -118,3 +119,30 @@ def test_root_solvers_via_speeds(oracle_mod):
     _, cm, cp = o.fluxspeed(q, o.prim2cons(q))
     assert np.all(np.isfinite(cm)) and np.all(np.isfinite(cp))
     assert np.all(np.abs(cm) <= 1.0 + 1e-12) and np.all(np.abs(cp) <= 1.0 + 1e-12)
+
+
+@pytest.mark.parametrize("rs,four", [("hll", False), ("hllc", False), ("hllc", True)])
+def test_transpose_symmetry(oracle_mod, rs, four):
+    """A 2D state symmetric under x<->y (with vx<->vy, Bx<->By) stays
+    symmetric: the y sweep rotates velocity and magnetic field alike
+    (src/schemes.F90:5140-5166)."""
+    p = sr_params(rs, ncells=16, xmin=0, xmax=1, ymin=0, ymax=1,
+                  state_variables="4vec" if four else "primitive")
+    o = oracle_mod.Oracle(p)
+    NY, NX = o.field_shape()[1:3]
+    y, x = np.meshgrid((np.arange(NY) + 0.5) / NY, (np.arange(NX) + 0.5) / NX, indexing="ij")
+    q = np.zeros(o.field_shape())
+    q[0, ..., 0] = 1.0 + 0.2 * np.sin(2 * np.pi * x) + 0.2 * np.sin(2 * np.pi * y)
+    q[0, ..., 1] = 0.4 * np.sin(2 * np.pi * (x + 2 * y))
+    q[0, ..., 2] = 0.4 * np.sin(2 * np.pi * (y + 2 * x))
+    q[0, ..., 4] = 0.5 + 0.3 * np.sin(2 * np.pi * y)
+    q[0, ..., 5] = 0.5 + 0.3 * np.sin(2 * np.pi * x)
+    q[0, ..., 8] = 1.0
+    o.set_prim(q)
+    for _ in range(4):
+        o.advance(1.0)
+    r = o.prim()[0]
+    rt = np.transpose(r, (1, 0, 2)).copy()
+    rt[..., [1, 2]] = rt[..., [2, 1]]
+    rt[..., [4, 5]] = rt[..., [5, 4]]
+    assert np.allclose(r, rt, rtol=1e-12, atol=1e-14)
