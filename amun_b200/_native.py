@@ -75,6 +75,7 @@ def lib():
         "amun_gpu_status": (i, [C.POINTER(amun_status)]),
         "amun_gpu_set_time": (i, [d, d]),
         "amun_gpu_update_flux_block": (i, [_D, _D, _D]),
+        "amun_gpu_update_flux_block_noalloc": (i, [_D, C.c_void_p, C.c_void_p]),
         "amun_gpu_riemann": (i, [i, _D, _D, _D]),
         "amun_gpu_prim2cons": (i, [i, _D, _D]),
         "amun_gpu_cons2prim": (i, [i, _D, _D]),

@@ -910,3 +910,66 @@ void amun_gpu_finalize(void) {
 const char* amun_gpu_last_error(void) { return C.err.c_str(); }
 
 }  // extern "C"
+
+// ---- allocation-free update_flux --------------------------------------------
+// Fixed device scratch of amun_gpu_update_flux_block_noalloc: one block's face
+// states qs(nv,im,jm,km,2,NDIMS), the WENO line scratch and the positivity
+// counter, each at a 256-byte boundary.  The array exists once per device (it
+// is part of this library's device image) and is shared by every call.
+#define AMUN_NOALLOC_SCRATCH_BYTES (32ull << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[AMUN_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_base[kNoallocMaxDevices] = {};  // address of g_noalloc_scratch per device
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int require_device_pointer(const void* p, const char* name) {
+  cudaPointerAttributes a{};
+  CK(cudaPointerGetAttributes(&a, p));
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return fail(AMUN_E_BAD_ARGUMENT, std::string(name) + " must point to device memory");
+  return 0;
+}
+}  // namespace
+
+extern "C" int amun_gpu_update_flux_block_noalloc(const double* dx, const double* q, double* f) {
+  (void)dx;  // the adiabatic flux does not use dx
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (!q || !f) return fail(AMUN_E_BAD_ARGUMENT, "null array");
+  const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
+  const int im = nc + 2 * ng, jm = im, km = nd == 3 ? im : 1;
+  UnitArgs u = unit_args(im, jm, km);
+  const size_t cells = (size_t)im * jm * km;
+  const size_t qs_bytes = cells * C.nv * 2 * nd * sizeof(double);
+  const size_t sc_bytes = unit_block_flux_scratch(u);
+  const size_t need = round256(qs_bytes) + round256(sc_bytes) + 256;
+  if (need > AMUN_NOALLOC_SCRATCH_BYTES)
+    return fail(AMUN_E_UNSUPPORTED, "update_flux_block_noalloc: a block of " + std::to_string(im) + "^" +
+                                        std::to_string(nd) + " cells needs " + std::to_string(need) +
+                                        " bytes of scratch; the fixed limit is " +
+                                        std::to_string(AMUN_NOALLOC_SCRATCH_BYTES) + " bytes");
+  if (int r = require_device_pointer(q, "q")) return r;
+  if (int r = require_device_pointer(f, "f")) return r;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail(AMUN_E_UNSUPPORTED, "device index out of range");
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_base[dev] = p;
+  }
+  unsigned char* base = static_cast<unsigned char*>(g_noalloc_base[dev]);
+  double* qs = reinterpret_cast<double*>(base);
+  double* sc = reinterpret_cast<double*>(base + round256(qs_bytes));
+  auto* nonpos = reinterpret_cast<unsigned long long*>(base + round256(qs_bytes) + round256(sc_bytes));
+  // what must start at zero: the face states outside the reconstructed
+  // range, the counter, and f outside the faces the lines write
+  CK(cudaMemsetAsync(qs, 0, qs_bytes, C.stream));
+  CK(cudaMemsetAsync(nonpos, 0, sizeof(unsigned long long), C.stream));
+  CK(cudaMemsetAsync(f, 0, cells * C.nv * nd * sizeof(double), C.stream));
+  cudaError_t e = unit_block_flux(u, q, qs, f, sc, nonpos, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "update_flux_block_noalloc");
+  return 0;
+}

@@ -158,6 +158,19 @@ int amun_gpu_set_time(double time, double dt);
  * Fortran arrays, FP64.  dx has NDIMS entries. */
 int amun_gpu_update_flux_block(const double* dx, const double* q, double* f);
 
+/* amun_gpu_update_flux_block on device arrays without allocating: no
+ * counterpart in the reference.  q and f are device pointers in the same
+ * Fortran layouts; the work is queued on the library stream (see
+ * amun_gpu_set_stream) and the call returns without synchronising.  Scratch is
+ * a fixed 32 MiB array in the library's device image, so a block whose
+ * scratch (face states + WENO line scratch) exceeds it is rejected with
+ * AMUN_E_UNSUPPORTED: 3D blocks up to 32^3 cells including ghosts (24^3 + 4
+ * ghosts, 16^3 + 4 ghosts) and 2D blocks up to about 48^2 fit.  The first call
+ * on a device looks the array up (cudaGetSymbolAddress); make it before any
+ * stream capture.  Calls share one scratch per device: two calls in flight at
+ * once (other streams or host threads) race; keep them in one stream order. */
+int amun_gpu_update_flux_block_noalloc(const double* dx, const double* q, double* f);
+
 /* riemann_iface (src/schemes.F90:66-71): n interfaces, FP64; ql/qr are not
  * modified (the reference modifies its copies for GLM-MHD). */
 int amun_gpu_riemann(int n, const double* ql, const double* qr, double* f);
