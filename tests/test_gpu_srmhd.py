@@ -31,9 +31,13 @@ def close(a, b, rtol, what):
     assert err <= rtol, f"{what}: max relative difference {err:.3e} > {rtol}"
 
 
-def close_field(a, b, rtol, what, vaxis=-1):
-    """Agreement per variable, relative to that variable's largest |value|."""
+def close_field(a, b, rtol, what, vaxis=-1, nan_ok=False):
+    """Agreement per variable, relative to that variable's largest |value|.
+    nan_ok: NaN is allowed where, and only where, the oracle has NaN."""
     a, b = np.moveaxis(np.asarray(a), vaxis, -1), np.moveaxis(np.asarray(b), vaxis, -1)
+    if nan_ok:
+        assert np.array_equal(np.isnan(a), np.isnan(b)), f"{what}: NaN in different places"
+        a, b = np.nan_to_num(a, nan=0.0), np.nan_to_num(b, nan=0.0)
     assert not np.isnan(b).any(), f"{what}: NaN in the oracle"
     assert not np.isnan(a).any(), f"{what}: NaN on the GPU"
     nv = a.shape[-1]
@@ -132,7 +136,9 @@ def test_srmhd_recovery_failure_parity(Sim, oracle_mod):
     assert failed.any()
     assert np.array_equal(qs[..., 8] == 0.0, failed)
     assert s.status()["c2p_failures"] == o.scalars()["c2p_failures"]
-    close_field(s.conserved(), o.cons(), 1e-10, "conserved after failures")
+    # the cells whose recovery failed carry NaN into the conserved state in
+    # both implementations
+    close_field(s.conserved(), o.cons(), 1e-10, "conserved after failures", nan_ok=True)
 
 
 def test_srmhd_fp32_bulk(Sim, oracle_mod):
