@@ -85,6 +85,10 @@ def lib():
         "amun_gpu_set_stream": (i, [vp]),
         "amun_gpu_profile": (i, [i, i]),
         "amun_gpu_profile_read": (i, [i, _D, C.POINTER(C.c_longlong)]),
+        "amun_gpu_forward_checkpointed": (i, [i, d, i]),
+        "amun_gpu_replay": (i, [i]),
+        "amun_gpu_adjoint": (i, [_D, _D, _D]),
+        "amun_gpu_adjoint_bytes": (i, [C.POINTER(C.c_longlong)]),
         "amun_gpu_finalize": (None, []),
         "amun_gpu_last_error": (C.c_char_p, []),
     }

@@ -39,6 +39,7 @@ FP32 = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 UNITS = {
     "amun_gpu.cu": FP64,
     "unit_fp64.cu": FP64,
+    "adjoint.cu": FP64,
     "kernels_fp64.cu": FP64,
     "kernels_fp64_hd.cu": FP64_SWEEP,
     "kernels_fp64_mhd.cu": FP64_SWEEP,

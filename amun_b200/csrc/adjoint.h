@@ -1,0 +1,50 @@
+// adjoint.h -- launchers of the discrete-adjoint kernels (adjoint.cu).
+//
+// Device arrays (per block b; the layouts of sweep.cuh):
+//   Q      [b][v][k][j][i]     stage-input primitives, padded, working precision
+//   lamU0, lamU1, lamdu        [b][v][k][j][i] interior, FP64
+//   lamQ   [b][v][k][j][i]     padded, FP64
+//   PL, PR [b][m][v][k][j][i]  padded, FP64, m = 0..4: the WENO-Z stencil
+//                              partials of a cell's right (PL) / left (PR)
+//                              face state with respect to cells c-2..c+2
+//   inv    [27 b + o]          the block whose neighbour in direction o is b
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sweep.cuh"
+
+namespace amun {
+
+struct AdjGeo {
+  Geo g;
+  int nv, eq, nblocks;
+};
+
+// lam[out] -> lamdu and lam[A], lam[B] for one stage combination
+cudaError_t adj_combination(const AdjGeo& a, const StageDesc& st, const DevScalars* rec, double decay, double* lamU0,
+                            double* lamU1, double* lamdu, cudaStream_t s);
+
+// lamU0 += lamU1, lamU1 = 0 (reverse of the U1 = U0 copy of evolve_ssprk2)
+cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStream_t s);
+
+// one direction: interface adjoints -> stencil partials -> lamQ +=
+template <typename R>
+cudaError_t adj_direction(const AdjGeo& a, int dir, const R* Q, const double* lamdu, double* PL, double* PR,
+                          double* lamQ, const double* binv, const MethodConst& m, const DevScalars* rec,
+                          cudaStream_t s);
+
+// ghost images folded into their source cells, then cons2prim^T into lamIn
+template <typename R>
+cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* lamQ, const int* inv, double gammam1, double* lamIn,
+                      cudaStream_t s);
+
+// lamq = prim2cons^T lamU (interior, SoA)
+template <typename R>
+cudaError_t adj_prim2cons(const AdjGeo& a, const R* Q, const double* lamU, double gammam1i, double* lamq,
+                          cudaStream_t s);
+
+// host block layout (nv fastest, padded; nblocks back to back) <-> interior SoA
+cudaError_t adj_from_host_layout(const AdjGeo& a, const double* aos, double* soa, cudaStream_t s);
+cudaError_t adj_to_host_layout(const AdjGeo& a, const double* soa, double* aos, cudaStream_t s);
+
+}  // namespace amun

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/amun_gpu.h"
+#include "adjoint.h"
 #include "launch.cuh"
 #include "unit.h"
 
@@ -65,6 +66,36 @@ struct Ctx {
 };
 
 Ctx C;
+
+// Recording of a forward run for the discrete adjoint: a copy of the state
+// (U0, the current primitives, the device scalars) every `interval` steps
+// plus after the last step, and each step's scalars after new_time_step.
+struct AdjCtx {
+  bool recorded = false;
+  int nsteps = 0, interval = 1, nseg = 0;
+  std::vector<double*> ck_u0;
+  std::vector<void*> ck_q;
+  DevScalars* ck_sc = nullptr;  // nseg + 1
+  DevScalars* rec = nullptr;    // nsteps
+  // reverse-pass work arrays (allocated by the first amun_gpu_adjoint)
+  void* seg_q = nullptr;        // interval x stages stage-input primitives
+  double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *lamQ = nullptr, *PL = nullptr, *PR = nullptr;
+  double* stage = nullptr;      // host-layout staging
+  int* inv = nullptr;
+  long long bytes = 0;
+};
+AdjCtx A;
+
+void adj_free() {
+  for (auto p : A.ck_u0) cudaFree(p);
+  for (auto p : A.ck_q) cudaFree(p);
+  A.ck_u0.clear();
+  A.ck_q.clear();
+  void* ptrs[] = {A.ck_sc, A.rec, A.seg_q, A.lamU0, A.lamU1, A.lamdu, A.lamQ, A.PL, A.PR, A.stage, A.inv};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  A = AdjCtx();
+}
 
 cudaEvent_t pool_event() {
   if (!C.event_pool.empty()) {
@@ -153,6 +184,7 @@ std::string strip(const char* v) {
 }
 
 void free_pool() {
+  adj_free();
   for (auto& gx : C.graph)
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   for (auto& x : C.q)
@@ -973,3 +1005,254 @@ extern "C" int amun_gpu_update_flux_block_noalloc(const double* dx, const double
   if (e != cudaSuccess) return cuda_fail(e, "update_flux_block_noalloc");
   return 0;
 }
+
+// ---- discrete adjoint ---------------------------------------------------------
+// A run recorded by amun_gpu_forward_checkpointed is differentiated by
+// amun_gpu_adjoint: per segment of `interval` steps (last segment first) the
+// segment is recomputed from its checkpoint, keeping every stage's input
+// primitives, and its steps are then reversed stage by stage (adjoint.cu).
+// Each step's dt and cmax are those recorded; they are not differentiated.
+namespace {
+
+__global__ void load_step_kernel(DevScalars* sc, const DevScalars* rec) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sc->cmax = rec->cmax;
+  sc->cmax2 = rec->cmax2;
+  sc->dt = rec->dt;
+  sc->dtn = rec->dtn;
+  sc->ms_bits = 0ull;
+}
+
+int adj_supported() {
+  if (C.p.eqsys != AMUN_EQ_HD && C.p.eqsys != AMUN_EQ_MHD)
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: adiabatic HD and MHD only");
+  if (C.p.reconstruction != AMUN_REC_WENO5Z) return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z reconstruction only");
+  if (effective_solver() != AMUN_RS_HLL) return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL Riemann solver only");
+  if (C.p.fix_positivity || C.p.clip_extrema)
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity and clip_extrema must be off");
+  if (C.p.nghosts < 4) return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4");
+  return 0;
+}
+
+size_t qpool_bytes() { return (size_t)C.g.qbs * C.nblocks * rsize(); }
+size_t upool_doubles() { return (size_t)C.g.ubs * C.nblocks; }
+
+int save_state(int slot) {
+  CK(cudaMemcpyAsync(A.ck_u0[slot], C.u0, upool_doubles() * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(A.ck_q[slot], C.q[C.cur], qpool_bytes(), cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(A.ck_sc + slot, C.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
+  return 0;
+}
+
+int restore_state(int slot) {
+  CK(cudaMemcpyAsync(C.u0, A.ck_u0[slot], upool_doubles() * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(C.q[C.cur], A.ck_q[slot], qpool_bytes(), cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(C.sc, A.ck_sc + slot, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
+  C.ms_valid = true;
+  return 0;
+}
+
+// one step with the scalars of recorded step n; stage inputs are kept in
+// seg_q slot `keep` when keep >= 0
+template <typename R>
+int replay_step(int n, int keep) {
+  load_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, A.rec + n);
+  CK(cudaGetLastError());
+  Schedule S = schedule();
+  if (S.copy_first) {
+    cudaError_t e = Launch<R, R>::copy_u0_u1(C.u0, (R*)C.u1, (long long)C.nblocks * C.g.ubs, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "copy u0->u1");
+  }
+  const size_t qb = qpool_bytes();
+  for (size_t s = 0; s < S.stages.size(); ++s) {
+    if (keep >= 0) {
+      char* dst = (char*)A.seg_q + ((size_t)keep * S.stages.size() + s) * qb;
+      CK(cudaMemcpyAsync(dst, C.q[C.cur], qb, cudaMemcpyDeviceToDevice, C.stream));
+    }
+    int r = launch_stage<R>(S.stages[s]);
+    if (r) return r;
+  }
+  end_step_kernel<<<1, 32, 0, C.stream>>>(C.sc);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// inv[27 b + o] = the block whose neighbour in direction o is b
+int build_inverse_neighbours() {
+  std::vector<int> inv(27 * (size_t)C.nblocks, -1);
+  for (int b = 0; b < C.nblocks; ++b)
+    for (int o = 0; o < 27; ++o) {
+      if (C.p.ndims == 2 && o / 9 != 1) continue;
+      int nb = o == 13 ? b : C.blocks[b].neighbor[o];
+      if (nb < 0) continue;
+      if (inv[27 * nb + o] >= 0) return fail(AMUN_E_UNSUPPORTED, "adjoint: a block is the neighbour of two blocks in one direction");
+      inv[27 * nb + o] = b;
+    }
+  if (!A.inv) CK(cudaMalloc(&A.inv, inv.size() * sizeof(int)));
+  CK(h2d(A.inv, inv.data(), inv.size() * sizeof(int)));
+  return 0;
+}
+
+template <typename R>
+int reverse_step(int n, int slot, const AdjGeo& ag) {
+  Schedule S = schedule();
+  const MethodConst m = method_const();
+  const size_t qb = qpool_bytes();
+  const int ns = (int)S.stages.size();
+  for (int s = ns - 1; s >= 0; --s) {
+    const StageDesc& st = S.stages[s];
+    cudaError_t e = adj_combination(ag, st, A.rec + n, C.decay, A.lamU0, A.lamU1, A.lamdu, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint combination");
+    CK(cudaMemsetAsync(A.lamQ, 0, (size_t)C.g.qbs * C.nblocks * sizeof(double), C.stream));
+    const R* Q = (const R*)((const char*)A.seg_q + ((size_t)slot * ns + s) * qb);
+    for (int d = 0; d < C.g.ndims; ++d) {
+      e = adj_direction<R>(ag, d, Q, A.lamdu, A.PL, A.PR, A.lamQ, C.binv, m, A.rec + n, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "adjoint flux sweep");
+    }
+    const int in = s == 0 ? (S.copy_first ? 1 : 0) : S.stages[s - 1].out_dst;
+    e = adj_cells<R>(ag, Q, A.lamQ, A.inv, C.gammam1, in == 0 ? A.lamU0 : A.lamU1, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint cons2prim");
+  }
+  if (S.copy_first) {
+    cudaError_t e = adj_fold_copy(ag, A.lamU0, A.lamU1, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint copy");
+  }
+  return 0;
+}
+
+template <typename R>
+int forward_recorded(int nsteps, double dtnext) {
+  for (int n = 0; n < nsteps; ++n) {
+    if (n % A.interval == 0) {
+      int r = save_state(n / A.interval);
+      if (r) return r;
+    }
+    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(A.rec + n, C.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
+    int r = launch_evolve<R>();
+    if (r) return r;
+    end_step_kernel<<<1, 32, 0, C.stream>>>(C.sc);
+    CK(cudaGetLastError());
+  }
+  return save_state(A.nseg);
+}
+
+template <typename R>
+int adjoint_pass(const AdjGeo& ag) {
+  for (int seg = A.nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * A.interval;
+    const int n1 = n0 + A.interval < A.nsteps ? n0 + A.interval : A.nsteps;
+    int r = restore_state(seg);
+    if (r) return r;
+    for (int n = n0; n < n1; ++n)
+      if ((r = replay_step<R>(n, n - n0))) return r;
+    for (int n = n1 - 1; n >= n0; --n)
+      if ((r = reverse_step<R>(n, n - n0, ag))) return r;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval) {
+  int r = check_ready();
+  if (r) return r;
+  if ((r = adj_supported())) return r;
+  if (nsteps <= 0 || interval <= 0) return fail(AMUN_E_BAD_ARGUMENT, "nsteps and interval must be positive");
+  adj_free();
+  A.nsteps = nsteps;
+  A.interval = interval;
+  A.nseg = (nsteps + interval - 1) / interval;
+  for (int s = 0; s <= A.nseg; ++s) {
+    double* u = nullptr;
+    void* q = nullptr;
+    CK(cudaMalloc(&u, upool_doubles() * sizeof(double)));
+    A.ck_u0.push_back(u);
+    CK(cudaMalloc(&q, qpool_bytes()));
+    A.ck_q.push_back(q);
+  }
+  CK(cudaMalloc(&A.ck_sc, (A.nseg + 1) * sizeof(DevScalars)));
+  CK(cudaMalloc(&A.rec, nsteps * sizeof(DevScalars)));
+  A.bytes = (long long)(A.nseg + 1) * (long long)(upool_doubles() * sizeof(double) + qpool_bytes());
+  if ((r = ensure_maxspeed())) return r;
+  r = bulk() ? forward_recorded<float>(nsteps, dtnext) : forward_recorded<double>(nsteps, dtnext);
+  if (r) return r;
+  C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  A.recorded = true;
+  return 0;
+}
+
+int amun_gpu_replay(int nsteps) {
+  int r = check_ready();
+  if (r) return r;
+  if (!A.recorded) return fail(AMUN_E_BAD_ARGUMENT, "no recorded run (amun_gpu_forward_checkpointed)");
+  if (nsteps <= 0 || nsteps > A.nsteps) return fail(AMUN_E_BAD_ARGUMENT, "nsteps exceeds the recorded run");
+  for (int n = 0; n < nsteps; ++n) {
+    r = bulk() ? replay_step<float>(n, -1) : replay_step<double>(n, -1);
+    if (r) return r;
+  }
+  C.ms_valid = false;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
+  int r = check_ready();
+  if (r) return r;
+  if (!A.recorded) return fail(AMUN_E_BAD_ARGUMENT, "no recorded run (amun_gpu_forward_checkpointed)");
+  if (!lam_u || (!lam_q0 && !lam_u0)) return fail(AMUN_E_BAD_ARGUMENT, "null adjoint array");
+  const Geo& g = C.g;
+  const size_t ud = upool_doubles(), qd = (size_t)g.qbs * C.nblocks;
+  const size_t ns = schedule().stages.size();
+  if (!A.seg_q) {
+    CK(cudaMalloc(&A.seg_q, (size_t)A.interval * ns * qpool_bytes()));
+    CK(cudaMalloc(&A.lamU0, ud * sizeof(double)));
+    CK(cudaMalloc(&A.lamU1, ud * sizeof(double)));
+    CK(cudaMalloc(&A.lamdu, ud * sizeof(double)));
+    CK(cudaMalloc(&A.lamQ, qd * sizeof(double)));
+    CK(cudaMalloc(&A.PL, 5 * qd * sizeof(double)));
+    CK(cudaMalloc(&A.PR, 5 * qd * sizeof(double)));
+    CK(cudaMalloc(&A.stage, qd * sizeof(double)));
+    A.bytes += (long long)((size_t)A.interval * ns * qpool_bytes() + (3 * ud + 12 * qd) * sizeof(double));
+  }
+  if ((r = build_inverse_neighbours())) return r;
+  AdjGeo ag{g, C.nv, C.p.eqsys, C.nblocks};
+  CK(cudaMemcpyAsync(A.stage, lam_u, qd * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+  cudaError_t e = adj_from_host_layout(ag, A.stage, A.lamU0, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "adjoint input");
+  CK(cudaMemsetAsync(A.lamU1, 0, ud * sizeof(double), C.stream));
+  r = bulk() ? adjoint_pass<float>(ag) : adjoint_pass<double>(ag);
+  if (r) return r;
+  if (lam_u0) {
+    e = adj_to_host_layout(ag, A.lamU0, A.stage, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint output");
+    CK(cudaMemcpyAsync(lam_u0, A.stage, qd * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  if (lam_q0) {
+    // the primitives of the initial state are the first stage input of step 0
+    e = bulk() ? adj_prim2cons<float>(ag, (const float*)A.seg_q, A.lamU0, C.gammam1i, A.lamdu, C.stream)
+               : adj_prim2cons<double>(ag, (const double*)A.seg_q, A.lamU0, C.gammam1i, A.lamdu, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint prim2cons");
+    e = adj_to_host_layout(ag, A.lamdu, A.stage, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint output");
+    CK(cudaMemcpyAsync(lam_q0, A.stage, qd * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaStreamSynchronize(C.stream));
+  }
+  // leave the recorded final state on the device
+  if ((r = restore_state(A.nseg))) return r;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_adjoint_bytes(long long* bytes) {
+  if (!bytes) return fail(AMUN_E_BAD_ARGUMENT, "null pointer");
+  *bytes = A.bytes;
+  return 0;
+}
+
+}  // extern "C"

@@ -155,5 +155,31 @@ class Simulation:
         N.check(self.L.amun_gpu_maxspeed(N.dptr(qblock), C.byref(out)))
         return out.value
 
+    # ---- discrete adjoint (no counterpart in the reference) ----------------------
+    def forward_checkpointed(self, nsteps: int, dtnext: float = 1.0e30, interval: int = 20):
+        """nsteps steps from the current state, recording what amun_gpu_adjoint
+        needs (a checkpoint every `interval` steps, each step's dt and cmax)."""
+        N.check(self.L.amun_gpu_forward_checkpointed(int(nsteps), float(dtnext), int(interval)))
+
+    def replay(self, nsteps: int):
+        """nsteps steps from the current state with the recorded dt and cmax."""
+        N.check(self.L.amun_gpu_replay(int(nsteps)))
+
+    def adjoint(self, lam_u: np.ndarray):
+        """lam_u = dJ/dU of the recorded final state as a global field
+        (NZ, NY, NX, nv) -> (dJ/dq0, dJ/dU0) as global fields."""
+        lam_u = np.asarray(lam_u, dtype=np.float64)
+        if lam_u.shape != self.mesh.shape + (self.nv,):
+            raise ValueError(f"expected a field of shape {self.mesh.shape + (self.nv,)}")
+        lb = np.ascontiguousarray(self.mesh.to_blocks(lam_u))
+        lq, lu = np.empty_like(lb), np.empty_like(lb)
+        N.check(self.L.amun_gpu_adjoint(N.dptr(lb), N.dptr(lq), N.dptr(lu)))
+        return self.mesh.from_blocks(lq), self.mesh.from_blocks(lu)
+
+    def adjoint_bytes(self) -> int:
+        b = C.c_longlong()
+        N.check(self.L.amun_gpu_adjoint_bytes(C.byref(b)))
+        return b.value
+
     def close(self):
         self.L.amun_gpu_finalize()

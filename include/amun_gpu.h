@@ -197,6 +197,34 @@ int amun_gpu_set_stream(void* stream);
 int amun_gpu_profile(int enable, int reset);
 int amun_gpu_profile_read(int kind, double* total_ms, long long* launches);
 
+/* Discrete adjoint of a run: no counterpart in the reference (AMUN has no
+ * adjoint).  Supported: adiabatic HD and MHD, WENO-Z, HLL, any SSPRK
+ * integrator, fix_positivity and clip_extrema off, nghosts >= 4, FP64 or
+ * FP32 bulk.  Each step's dt and GLM speed cmax are those of the forward run
+ * and are held constant in the derivative.
+ *
+ * amun_gpu_forward_checkpointed: nsteps steps from the current state (as
+ * amun_gpu_run without graphs), keeping a device copy of the state every
+ * `interval` steps and each step's dt and cmax.  Afterwards the device holds
+ * the final state. */
+int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval);
+
+/* nsteps (<= the recorded count) steps from the current state with the dt
+ * and cmax recorded by amun_gpu_forward_checkpointed (finite-difference
+ * checks of the adjoint at a frozen time step). */
+int amun_gpu_replay(int nsteps);
+
+/* lam_u = dJ/dU of the recorded final conserved state, in the block layout
+ * of amun_gpu_upload_blocks (nblocks x (nv,im,jm,km), ghost entries
+ * ignored).  Returns lam_q0 = dJ/dq of the initial primitive state and/or
+ * lam_u0 = dJ/dU of the initial conserved state (same layout, ghosts 0);
+ * either may be NULL.  Segments are recomputed from their checkpoints (one
+ * extra forward pass); the device holds the recorded final state after. */
+int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0);
+
+/* device bytes held by the recording and the adjoint work arrays */
+int amun_gpu_adjoint_bytes(long long* bytes);
+
 /* finalize_*: release the device pool, graphs and stream. */
 void amun_gpu_finalize(void);
 
