@@ -11,6 +11,9 @@ U^n and stage combination); the FP64 plain path, the L1 density error of the
 FP32-bulk state against FP64 after the same steps, the energy drift, the
 e2e number through the C ABI with host arrays, the roofline and a CPU
 baseline (the oracle restatement on the host cores) are reported beside it.
+The metric's second part, adjoint/forward time, is measured on the
+differentiation configuration (2D MHD 256^2, WENO-Z, HLL, SSPRK(3,3), 200
+steps, checkpoint every 20) under "adjoint".
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -159,6 +162,56 @@ def kernel_profile(sim, steps, dtnext):
         out[name] = {"total_ms": ms.value, "launches": n.value,
                      "avg_ms": (ms.value / n.value) if n.value else None}
     return out
+
+
+ADJOINT_WORKLOAD = dict(ndims=2, equation_system="mhd", equation_of_state="adi", reconstruction="weno5z",
+                        limiter="mc", riemann_solver="hll", time_advance="rk3", cfl=0.4, gamma=GAMMA, nghosts=4,
+                        ncells=256, xblocks=1, yblocks=1, maxlev=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0)
+ADJOINT_STEPS, ADJOINT_INTERVAL = 200, 20
+
+
+def adjoint_timing(torch, prec):
+    """2D MHD 256^2 (WENO-Z, HLL, SSPRK(3,3)), smooth seeded state, 200 steps:
+    the plain forward run (graphs) against the recorded forward (checkpoint
+    every 20 steps) and the adjoint call (segment recomputation + reverse) for
+    J = kinetic energy in [0,0.25]^2 at the final step, all timed with CUDA
+    events on the library's stream."""
+    from amun_b200 import problems
+    from amun_b200.adjoint import kinetic_energy
+    from amun_b200.solver import Simulation
+    sim = Simulation(ADJOINT_WORKLOAD, precision=prec)
+    stream = torch.cuda.current_stream()
+    sim.L.amun_gpu_set_stream(stream.cuda_stream)
+    q0 = problems.smooth_mhd(sim.mesh, seed=0)
+
+    def events(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    sim.set_primitive(q0)
+    sim.run(3, 1.0e30, graph=True)  # warm-up and graph capture
+    sim.set_primitive(q0)
+    fwd = events(lambda: sim.run(ADJOINT_STEPS, 1.0e30, graph=True))
+    sim.set_primitive(q0)
+    sim.forward_checkpointed(3, 1.0e30, ADJOINT_INTERVAL)  # warm-up
+    sim.set_primitive(q0)
+    rec = events(lambda: sim.forward_checkpointed(ADJOINT_STEPS, 1.0e30, ADJOINT_INTERVAL))
+    u = torch.from_numpy(sim.conserved()).requires_grad_(True)
+    kinetic_energy(u, sim.mesh).backward()
+    lam = u.grad.numpy()
+    out = {}
+    adj = events(lambda: out.setdefault("g", sim.adjoint(lam)))
+    gbytes = sim.adjoint_bytes()
+    sim.close()
+    return {"forward_ms": fwd, "recorded_forward_ms": rec, "adjoint_ms": adj,
+            "adjoint_over_forward": adj / fwd, "gradient_over_forward": (rec + adj) / fwd,
+            "steps": ADJOINT_STEPS, "checkpoint_interval": ADJOINT_INTERVAL, "device_bytes": gbytes,
+            "grad_rho_l2": float(np.sqrt(np.sum(out["g"][0][..., 0] ** 2)))}
 
 
 def cpu_baseline(threads: int, steps: int = 1):
@@ -322,6 +375,13 @@ def main():
            "h2d_bytes_per_step": 2 * bytes_per_array, "d2h_bytes_per_step": 2 * bytes_per_array,
            "ms_per_step": e2e_ms}
 
+    adjoint = {}
+    for prec in ("fp64", "fp32"):
+        try:
+            adjoint[prec] = adjoint_timing(torch, prec)
+        except Exception as exc:  # pragma: no cover
+            adjoint[prec] = {"error": str(exc)}
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         r32, r64 = results["fp32"], results["fp64"]
@@ -364,6 +424,9 @@ def main():
             "accuracy_vs_fp64": accuracy,
             "kernel_profile_fp32": r32["profile"], "kernel_profile_fp64": r64["profile"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
+                                    "J = kinetic energy in [0,0.25]^2, dJ/drho0",
+                        "fp64": adjoint["fp64"], "fp32": adjoint["fp32"]},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": clocks,
         }
