@@ -3,14 +3,17 @@
 //
 // Reverse of one stage, given lam of the stage output:
 //   adj_combination   out = comb(A, B, ds du): lamdu, lam[A], lam[B]
-//   adj_direction     per interface i+1/2 along d: recompute the WENO-Z face
-//                     states and the HLL flux, lamF = (lamdu(i+1) - lamdu(i))/dx,
-//                     reverse HLL -> lam of the two face states -> reverse
-//                     WENO-Z -> five stencil partials per side (PL, PR); then a
-//                     gather sums the partials into lamQ (no atomics, so the
-//                     result does not depend on thread order)
-//   adj_cells         lamQ of ghost cells added to the interior cells they
-//                     copy, then cons2prim^T into lam of the stage input
+//   adj_faces         all directions in one launch each:
+//                     face kernel, per interface i+1/2: recompute the WENO-Z
+//                     face states, lamF = (lamdu(i+1) - lamdu(i))/dx, reverse
+//                     HLL -> lam of the two face states (G);
+//                     WENO kernel, per cell and variable: reverse WENO-Z of
+//                     both faces -> five stencil partials (P)
+//   adj_cells         per interior cell: sum the partials aimed at the cell
+//                     and at its ghost copies in the neighbour blocks (a
+//                     gather, no atomics, so the result does not depend on
+//                     thread order), then cons2prim^T into lam of the stage
+//                     input
 #include "adjoint.cuh"
 #include "adjoint.h"
 
@@ -19,11 +22,13 @@ namespace amun {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kFaceThreads = 128;
 
-int blocks_for(long long n) {
-  long long b = (n + kThreads - 1) / kThreads;
+int blocks_of(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
   return (int)(b < 1 ? 1 : (b > 65535LL * 32 ? 65535LL * 32 : b));
 }
+int blocks_for(long long n) { return blocks_of(n, kThreads); }
 
 __global__ void comb_kernel(double* lamU0, double* lamU1, double* lamdu, StageDesc st, const DevScalars* rec,
                             double decay, int psi, long long uvs, long long ubs, long long n) {
@@ -64,136 +69,184 @@ __device__ __forceinline__ void line_cell(const Geo& g, int a, int t1, int t2, i
   else { i = ng + t1; j = ng + t2; k = a; }
 }
 
+// position a along DIR (0 .. na-1) and transverse line of flat index t, with
+// the fastest-varying index along x for coalescing
+template <int DIR>
+__device__ __forceinline__ void line_index(long long t, int na, int nc, int nt2, int& a, int& t1, int& t2) {
+  if constexpr (DIR == 0) { a = (int)(t % na); long long r = t / na; t1 = (int)(r % nc); t2 = (int)(r / nc); }
+  else if constexpr (DIR == 1) { t1 = (int)(t % nc); long long r = t / nc; a = (int)(r % na); t2 = (int)(r / na); }
+  else { t1 = (int)(t % nc); long long r = t / nc; t2 = (int)(r % nt2); a = (int)(r / nt2); }
+}
+
 template <int DIR>
 __device__ __forceinline__ long long dir_stride(const Geo& g) {
   return DIR == 0 ? 1LL : (DIR == 1 ? (long long)g.IM : (long long)g.IM * g.JM);
 }
 
+// Per interface i+1/2 along DIR (cells L = i, R = i+1 on interior lines):
+// WENO-Z face states, HLL flux reverse.  G[DIR][0] at L receives lam of L's
+// right face state, G[DIR][1] at R lam of R's left face state.
 template <int EQ, int DIR, typename R>
-__global__ void __launch_bounds__(kThreads) face_kernel(const R* __restrict__ Q, const double* __restrict__ lamdu,
-                                                        double* __restrict__ PL, double* __restrict__ PR,
-                                                        const double* __restrict__ binv, Geo g, MethodConst m,
-                                                        const DevScalars* rec) {
+__device__ __forceinline__ void face_body(long long t, int b, int nblocks, const R* __restrict__ Q,
+                                          const double* __restrict__ lamdu, double* __restrict__ G, double dxi,
+                                          const Geo& g, const Phys<R>& P, R eps) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
   const int nc = g.nc, ng = g.ng;
-  const int b = blockIdx.y;
   const int nt2 = g.ndims == 3 ? nc : 1;
-  const long long per = (long long)(nc + 1) * nc * nt2;
+  const long long qd = g.qbs * nblocks;
+  const long long sD = dir_stride<DIR>(g);
+  int f, t1, t2;
+  line_index<DIR>(t, nc + 1, nc, nt2, f, t1, t2);
+  int i, j, k;
+  line_cell<DIR>(g, ng - 1 + f, t1, t2, i, j, k);
+  const long long cL = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;  // cell L; R = L + sD
+  // interface adjoint: du(L) has -F/dx, du(R) has +F/dx (interior cells only)
+  const bool inL = f >= 1, inR = f < nc;
+  const long long iu = (long long)b * g.ubs +
+                       ((long long)(g.ndims == 3 ? k - ng : 0) * nc + (j - ng)) * nc + (i - ng);  // L if interior
+  const long long uD = DIR == 0 ? 1LL : (DIR == 1 ? (long long)nc : (long long)nc * nc);
+  R ql[NV], qr[NV], lF[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const R* q = Q + cL + v * g.qvs;
+    const R s0 = q[-2 * sD], s1 = q[-sD], s2 = q[0], s3 = q[sD], s4 = q[2 * sD], s5 = q[3 * sD];
+    ql[v] = weno5z_right_value<R>(s0, s1, s2, s3, s4, eps);  // right face of L
+    qr[v] = weno5z_right_value<R>(s5, s4, s3, s2, s1, eps);  // left face of R (mirror)
+    const double lR = inR ? lamdu[iu + uD + v * g.uvs] : 0.0;
+    const double lL = inL ? lamdu[iu + v * g.uvs] : 0.0;
+    lF[v] = R(dxi * (lR - lL));
+  }
+  R a[NV], c[NV], lql[NV], lqr[NV];
+  rotate<EQ, DIR>(ql, a);
+  rotate<EQ, DIR>(qr, c);
+  rotate<EQ, DIR>(lF, ql);  // ql reused: rotated lF
+  hll_rev<EQ>(a, c, ql, lql, lqr, P);
+  unrotate<EQ, DIR>(lql, a);
+  unrotate<EQ, DIR>(lqr, c);
+  double* G0 = G + (long long)(2 * DIR) * qd;
+  double* G1 = G0 + qd;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    G0[cL + v * g.qvs] = (double)a[v];
+    G1[cL + sD + v * g.qvs] = (double)c[v];
+  }
+}
+
+// blockIdx.z = direction
+template <int EQ, typename R>
+__global__ void __launch_bounds__(kFaceThreads) face_kernel(const R* __restrict__ Q,
+                                                            const double* __restrict__ lamdu,
+                                                            double* __restrict__ G, const double* __restrict__ binv,
+                                                            Geo g, MethodConst m, const DevScalars* rec) {
+  const int b = blockIdx.y, dir = blockIdx.z;
+  const int nt2 = g.ndims == 3 ? g.nc : 1;
+  const long long per = (long long)(g.nc + 1) * g.nc * nt2;
   const Phys<R> P = make_phys<R>(m, rec->cmax, rec->cmax2);
   const R eps = R(m.eps);
-  const double dxi = binv[3 * b + DIR];
-  const long long sD = dir_stride<DIR>(g);
+  const double dxi = binv[3 * b + dir];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
-    int f, t1, t2;
-    if constexpr (DIR == 0) { f = (int)(t % (nc + 1)); long long r = t / (nc + 1); t1 = (int)(r % nc); t2 = (int)(r / nc); }
-    else if constexpr (DIR == 1) { t1 = (int)(t % nc); long long r = t / nc; f = (int)(r % (nc + 1)); t2 = (int)(r / (nc + 1)); }
-    else { t1 = (int)(t % nc); long long r = t / nc; t2 = (int)(r % nt2); f = (int)(r / nt2); }
-    int i, j, k;
-    line_cell<DIR>(g, ng - 1 + f, t1, t2, i, j, k);
-    const long long cL = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;  // cell L; R = L + sD
-    // interface adjoint: du(L) has -F/dx, du(R) has +F/dx (interior cells only)
-    const bool inL = f >= 1, inR = f < nc;
-    long long iu = 0;
-    {
-      int ii = i - ng, jj = j - ng, kk = g.ndims == 3 ? k - ng : 0;
-      iu = (long long)b * g.ubs + ((long long)kk * nc + jj) * nc + ii;  // interior index of L (when inside)
-    }
-    const long long uD = DIR == 0 ? 1LL : (DIR == 1 ? (long long)nc : (long long)nc * nc);
-    R ql[NV], qr[NV], lF[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const R* q = Q + cL + v * g.qvs;
-      R s0 = q[-2 * sD], s1 = q[-sD], s2 = q[0], s3 = q[sD], s4 = q[2 * sD], s5 = q[3 * sD];
-      R fR, fL, dum;
-      weno5z_faces<R>(s0, s1, s2, s3, s4, eps, fR, dum);
-      weno5z_faces<R>(s1, s2, s3, s4, s5, eps, dum, fL);
-      ql[v] = fR;
-      qr[v] = fL;
-      const double lR = inR ? lamdu[iu + uD + v * g.uvs] : 0.0;
-      const double lL = inL ? lamdu[iu + v * g.uvs] : 0.0;
-      lF[v] = R(dxi * (lR - lL));
-    }
-    R qlr[NV], qrr[NV], lFr[NV], lqlr[NV], lqrr[NV], lql[NV], lqr[NV];
-    rotate<EQ, DIR>(ql, qlr);
-    rotate<EQ, DIR>(qr, qrr);
-    rotate<EQ, DIR>(lF, lFr);
-    hll_rev<EQ>(qlr, qrr, lFr, lqlr, lqrr, P);
-    unrotate<EQ, DIR>(lqlr, lql);
-    unrotate<EQ, DIR>(lqrr, lqr);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const R* q = Q + cL + v * g.qvs;
-      R s[6] = {q[-2 * sD], q[-sD], q[0], q[sD], q[2 * sD], q[3 * sD]};
-      R gl[5] = {R(0), R(0), R(0), R(0), R(0)}, gr[5] = {R(0), R(0), R(0), R(0), R(0)};
-      weno5z_right_rev(s, lql[v], gl, eps);
-      weno5z_left_rev(s + 1, lqr[v], gr, eps);
-      const long long oL = (long long)b * 5 * g.qbs + v * g.qvs + (cL - (long long)b * g.qbs);
-      const long long oR = oL + sD;
-#pragma unroll
-      for (int mm = 0; mm < 5; ++mm) {
-        PL[oL + mm * g.qbs] = (double)gl[mm];
-        PR[oR + mm * g.qbs] = (double)gr[mm];
-      }
-    }
+    if (dir == 0) face_body<EQ, 0, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
+    else if (dir == 1) face_body<EQ, 1, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
+    else face_body<EQ, 2, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
   }
 }
 
-// lamQ(c) += sum over the sources s = c-2..c+2 of their partial for c:
-// PL of s = ng-1..ng+nc-1 (right face of s is an interface next to the
-// interior), PR of s = ng..ng+nc.
-template <int DIR>
-__global__ void gather_kernel(const double* __restrict__ PL, const double* __restrict__ PR, double* __restrict__ lamQ,
-                              Geo g, int nv) {
+// Per cell c along DIR (ng-1 .. ng+nc) on interior lines and variable:
+// WENO-Z reverse of the cell's right face (lam from G[DIR][0], interfaces
+// c+1/2 next to the interior) and left face (G[DIR][1], interfaces c-1/2);
+// P[DIR][m] at c = the partial for cell c-2+m.
+template <int DIR, typename R>
+__device__ __forceinline__ void weno_body(long long t, int b, int nblocks, const R* __restrict__ Q,
+                                          const double* __restrict__ G, double* __restrict__ P, const Geo& g,
+                                          int nv, R eps) {
   const int nc = g.nc, ng = g.ng;
-  const int b = blockIdx.y;
-  const int na = nc + 6;
   const int nt2 = g.ndims == 3 ? nc : 1;
-  const long long per = (long long)na * nc * nt2;
+  const long long per_v = (long long)(nc + 2) * nc * nt2;
+  const long long qd = g.qbs * nblocks;
   const long long sD = dir_stride<DIR>(g);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
-    int a, t1, t2;
-    if constexpr (DIR == 0) { a = (int)(t % na); long long r = t / na; t1 = (int)(r % nc); t2 = (int)(r / nc); }
-    else if constexpr (DIR == 1) { t1 = (int)(t % nc); long long r = t / nc; a = (int)(r % na); t2 = (int)(r / na); }
-    else { t1 = (int)(t % nc); long long r = t / nc; t2 = (int)(r % nt2); a = (int)(r / nt2); }
-    a += ng - 3;
-    int i, j, k;
-    line_cell<DIR>(g, a, t1, t2, i, j, k);
-    const long long cell = ((long long)k * g.JM + j) * g.IM + i;
-    for (int v = 0; v < nv; ++v) {
-      double sum = 0.0;
+  const int v = (int)(t / per_v);
+  if (v >= nv) return;
+  int a, t1, t2;
+  line_index<DIR>(t - v * per_v, nc + 2, nc, nt2, a, t1, t2);
+  a += ng - 1;
+  int i, j, k;
+  line_cell<DIR>(g, a, t1, t2, i, j, k);
+  const long long cell = ((long long)k * g.JM + j) * g.IM + i;
+  const long long c = (long long)b * g.qbs + v * g.qvs + cell;
+  const double* G0 = G + (long long)(2 * DIR) * qd;
+  const double lR = a <= ng + nc - 1 ? G0[c] : 0.0;
+  const double lL = a >= ng ? G0[qd + c] : 0.0;
+  const R* q = Q + c;
+  const R st[5] = {q[-2 * sD], q[-sD], q[0], q[sD], q[2 * sD]};
+  R gg[5] = {R(0), R(0), R(0), R(0), R(0)};
+  weno5z_pair_rev(st, R(lR), R(lL), gg, eps);
+  double* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
 #pragma unroll
-      for (int mm = 0; mm < 5; ++mm) {
-        const int s = a + 2 - mm;
-        const long long o = (long long)b * 5 * g.qbs + mm * g.qbs + v * g.qvs + cell + (long long)(s - a) * sD;
-        if (s >= ng - 1 && s <= ng + nc - 1) sum += PL[o];
-        if (s >= ng && s <= ng + nc) sum += PR[o];
-      }
-      lamQ[(long long)b * g.qbs + v * g.qvs + cell] += sum;
+  for (int mm = 0; mm < 5; ++mm) Pd[mm * g.qbs] = (double)gg[mm];
+}
+
+template <typename R>
+__global__ void weno_rev_kernel(const R* __restrict__ Q, const double* __restrict__ G, double* __restrict__ P, Geo g,
+                                int nv, double eps_d) {
+  const int b = blockIdx.y, dir = blockIdx.z;
+  const int nt2 = g.ndims == 3 ? g.nc : 1;
+  const long long per = (long long)(g.nc + 2) * g.nc * nt2 * nv;
+  const R eps = R(eps_d);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
+    if (dir == 0) weno_body<0, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
+    else if (dir == 1) weno_body<1, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
+    else weno_body<2, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
+  }
+}
+
+// lq += the stencil partials aimed at padded cell (i,j,k) of block pb, over
+// the directions whose line through the cell is an interior line (the only
+// lines the WENO kernel covers) and sources s = a-2..a+2 in ng-1..ng+nc.
+template <int NV>
+__device__ __forceinline__ void gather_at(const double* __restrict__ P, const Geo& g, long long qd, int pb, int i,
+                                          int j, int k, double* lq) {
+  const int nc = g.nc, ng = g.ng;
+  const long long cell = ((long long)k * g.JM + j) * g.IM + i;
+  const bool ti = i >= ng && i < ng + nc, tj = j >= ng && j < ng + nc;
+  const bool tk = g.ndims == 2 || (k >= ng && k < ng + nc);
+  for (int d = 0; d < g.ndims; ++d) {
+    const bool line = d == 0 ? (tj && tk) : (d == 1 ? (ti && tk) : (ti && tj));
+    if (!line) continue;
+    const int a = d == 0 ? i : (d == 1 ? j : k);
+    const long long sD = d == 0 ? 1LL : (d == 1 ? (long long)g.IM : (long long)g.IM * g.JM);
+    const double* Pd = P + (long long)d * 5 * qd + (long long)pb * 5 * g.qbs;
+#pragma unroll
+    for (int mm = 0; mm < 5; ++mm) {
+      const int s = a + 2 - mm;
+      if (s < ng - 1 || s > ng + nc) continue;
+      const double* ps = Pd + mm * g.qbs + cell + (long long)(s - a) * sD;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) lq[v] += ps[v * g.qvs];
     }
   }
 }
 
+// Per interior cell: lam of its primitive state = the partials aimed at it
+// and at its ghost copies (image at c + o nc in block inv[o], for each of the
+// 26 directions o); then lamIn += cons2prim^T lam.
 template <int EQ, typename R>
-__global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ lamQ, const int* __restrict__ inv,
+__global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ P, const int* __restrict__ inv,
                             double gammam1, double* __restrict__ lamIn, Geo g) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
   const int nc = g.nc, ng = g.ng, b = blockIdx.y;
-  const long long n = g.uvs;
+  const long long qd = g.qbs * gridDim.y;
   const int nz = g.ndims == 3 ? 1 : 0;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.uvs; t += (long long)gridDim.x * blockDim.x) {
     const int ii = (int)(t % nc);
     const int jj = (int)((t / nc) % nc);
     const int kk = g.ndims == 3 ? (int)(t / ((long long)nc * nc)) : 0;
     const int i = ng + ii, j = ng + jj, k = g.ndims == 3 ? ng + kk : 0;
-    const long long cell = ((long long)k * g.JM + j) * g.IM + i;
     double lq[NV], q[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      lq[v] = lamQ[(long long)b * g.qbs + v * g.qvs + cell];
-      q[v] = (double)Q[(long long)b * g.qbs + v * g.qvs + cell];
-    }
+    for (int v = 0; v < NV; ++v) lq[v] = 0.0;
+    gather_at<NV>(P, g, qd, b, i, j, k, lq);
     for (int oz = -nz; oz <= nz; ++oz)
       for (int oy = -1; oy <= 1; ++oy)
         for (int ox = -1; ox <= 1; ++ox) {
@@ -202,10 +255,11 @@ __global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ 
           if (gi < 0 || gi >= g.IM || gj < 0 || gj >= g.JM || gk < 0 || gk >= g.KM) continue;
           const int src = inv[27 * b + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
           if (src < 0) continue;
-          const long long gc = (long long)src * g.qbs + ((long long)gk * g.JM + gj) * g.IM + gi;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) lq[v] += lamQ[gc + v * g.qvs];
+          gather_at<NV>(P, g, qd, src, gi, gj, gk, lq);
         }
+    const long long cell = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) q[v] = (double)Q[cell + v * g.qvs];
     double lu[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) lu[v] = 0.0;
@@ -285,46 +339,26 @@ cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStr
   return cudaGetLastError();
 }
 
-template <int EQ, typename R>
-static cudaError_t direction_eq(const AdjGeo& a, int dir, const R* Q, const double* lamdu, double* PL, double* PR,
-                                double* lamQ, const double* binv, const MethodConst& m, const DevScalars* rec,
-                                cudaStream_t s) {
+template <typename R>
+cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* G, double* P, const double* binv,
+                      const MethodConst& m, const DevScalars* rec, cudaStream_t s) {
   const Geo& g = a.g;
   const int nt2 = g.ndims == 3 ? g.nc : 1;
   const long long nf = (long long)(g.nc + 1) * g.nc * nt2;
-  const long long ng = (long long)(g.nc + 6) * g.nc * nt2;
-  dim3 gf(blocks_for(nf), a.nblocks), gg(blocks_for(ng), a.nblocks);
-  switch (dir) {
-    case 0:
-      face_kernel<EQ, 0, R><<<gf, kThreads, 0, s>>>(Q, lamdu, PL, PR, binv, g, m, rec);
-      gather_kernel<0><<<gg, kThreads, 0, s>>>(PL, PR, lamQ, g, a.nv);
-      break;
-    case 1:
-      face_kernel<EQ, 1, R><<<gf, kThreads, 0, s>>>(Q, lamdu, PL, PR, binv, g, m, rec);
-      gather_kernel<1><<<gg, kThreads, 0, s>>>(PL, PR, lamQ, g, a.nv);
-      break;
-    default:
-      face_kernel<EQ, 2, R><<<gf, kThreads, 0, s>>>(Q, lamdu, PL, PR, binv, g, m, rec);
-      gather_kernel<2><<<gg, kThreads, 0, s>>>(PL, PR, lamQ, g, a.nv);
-      break;
-  }
+  const long long nw = (long long)(g.nc + 2) * g.nc * nt2 * a.nv;
+  const dim3 gf(blocks_of(nf, kFaceThreads), a.nblocks, g.ndims), gw(blocks_for(nw), a.nblocks, g.ndims);
+  if (a.eq == EQ_HD) face_kernel<EQ_HD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+  else face_kernel<EQ_MHD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+  weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.eps);
   return cudaGetLastError();
 }
 
 template <typename R>
-cudaError_t adj_direction(const AdjGeo& a, int dir, const R* Q, const double* lamdu, double* PL, double* PR,
-                          double* lamQ, const double* binv, const MethodConst& m, const DevScalars* rec,
-                          cudaStream_t s) {
-  if (a.eq == EQ_HD) return direction_eq<EQ_HD, R>(a, dir, Q, lamdu, PL, PR, lamQ, binv, m, rec, s);
-  return direction_eq<EQ_MHD, R>(a, dir, Q, lamdu, PL, PR, lamQ, binv, m, rec, s);
-}
-
-template <typename R>
-cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* lamQ, const int* inv, double gammam1, double* lamIn,
+cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* P, const int* inv, double gammam1, double* lamIn,
                       cudaStream_t s) {
   dim3 grid(blocks_for(a.g.uvs), a.nblocks);
-  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, kThreads, 0, s>>>(Q, lamQ, inv, gammam1, lamIn, a.g);
-  else cell_kernel<EQ_MHD, R><<<grid, kThreads, 0, s>>>(Q, lamQ, inv, gammam1, lamIn, a.g);
+  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
+  else cell_kernel<EQ_MHD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
   return cudaGetLastError();
 }
 
@@ -349,11 +383,10 @@ cudaError_t adj_to_host_layout(const AdjGeo& a, const double* soa, double* aos, 
   return cudaGetLastError();
 }
 
-template cudaError_t adj_direction<double>(const AdjGeo&, int, const double*, const double*, double*, double*,
-                                           double*, const double*, const MethodConst&, const DevScalars*,
-                                           cudaStream_t);
-template cudaError_t adj_direction<float>(const AdjGeo&, int, const float*, const double*, double*, double*, double*,
-                                          const double*, const MethodConst&, const DevScalars*, cudaStream_t);
+template cudaError_t adj_faces<double>(const AdjGeo&, const double*, const double*, double*, double*, const double*,
+                                       const MethodConst&, const DevScalars*, cudaStream_t);
+template cudaError_t adj_faces<float>(const AdjGeo&, const float*, const double*, double*, double*, const double*,
+                                      const MethodConst&, const DevScalars*, cudaStream_t);
 template cudaError_t adj_cells<double>(const AdjGeo&, const double*, const double*, const int*, double, double*,
                                        cudaStream_t);
 template cudaError_t adj_cells<float>(const AdjGeo&, const float*, const double*, const int*, double, double*,

@@ -80,6 +80,111 @@ __device__ __forceinline__ void weno5z_left_rev(const R* f, R lam, R* g, R eps) 
   g[0] += gm[4]; g[1] += gm[3]; g[2] += gm[2]; g[3] += gm[1]; g[4] += gm[0];
 }
 
+// The right-face state fR of weno5z_faces alone (the forward value the
+// reverse pass differentiates at; one division per denominator, which moves
+// the value by rounding only).
+template <typename R>
+__device__ __forceinline__ R weno5z_right_value(R fm2, R fm1, R f0, R fp1, R fp2, R eps) {
+  const R c1 = R(13.0 / 12.0), c2 = R(0.25);
+  const R dm1 = fm1 - fm2, d0m = f0 - fm1, d0p = fp1 - f0, dp1 = fp2 - fp1;
+  const R t2m = d0m - dm1, t20 = d0p - d0m, t2p = dp1 - d0p;
+  const R tl = R(3) * d0m - dm1, tc = d0p + d0m, tr = R(3) * d0p - dp1;
+  const R bl = c1 * (t2m * t2m) + c2 * (tl * tl);
+  const R bc = c1 * (t20 * t20) + c2 * (tc * tc);
+  const R br = c1 * (t2p * t2p) + c2 * (tr * tr);
+  const R tt = d_fabs(br - bl);
+  const R wl0 = R(0.1) * (R(1) + tt / (bl + eps));
+  const R wc0 = R(0.6) * (R(1) + tt / (bc + eps));
+  const R wr0 = R(0.3) * (R(1) + tt / (br + eps));
+  const R iS = R(1) / ((wl0 + wr0) + wc0);
+  const R wl = wl0 * iS, wr = wr0 * iS, wc = R(1) - (wl + wr);
+  const R QL = R(2.0 / 6.0) * fm2 + R(-7.0 / 6.0) * fm1 + R(11.0 / 6.0) * f0;
+  const R QC = R(-1.0 / 6.0) * fm1 + R(5.0 / 6.0) * f0 + R(2.0 / 6.0) * fp1;
+  const R QR = R(2.0 / 6.0) * f0 + R(5.0 / 6.0) * fp1 + R(-1.0 / 6.0) * fp2;
+  return (wl * QL + wr * QR) + wc * QC;
+}
+
+// Reverse of both face states of one cell at once (stencil f[0..4] =
+// f(i-2..i+2)): g += (dfR/df) lamR + (dfL/df) lamL.  The smoothness
+// indicators and the alpha of the two faces are shared; fL uses the mirrored
+// weights (0.1 ar, 0.6 ac, 0.3 al) and mirrored candidate polynomials.
+template <typename R>
+__device__ __forceinline__ void weno5z_pair_rev(const R* f, R lamR, R lamL, R* g, R eps) {
+  const R c1 = R(13.0 / 12.0), c2 = R(0.25);
+  const R dl = R(0.1), dc = R(0.6), dr = R(0.3);
+  const R a11 = R(2.0 / 6.0), a12 = R(-7.0 / 6.0), a13 = R(11.0 / 6.0);
+  const R a21 = R(-1.0 / 6.0), a22 = R(5.0 / 6.0), a23 = R(2.0 / 6.0);
+  const R a31 = R(2.0 / 6.0), a32 = R(5.0 / 6.0), a33 = R(-1.0 / 6.0);
+  const R fm2 = f[0], fm1 = f[1], f0 = f[2], fp1 = f[3], fp2 = f[4];
+  const R dm1 = fm1 - fm2, d0m = f0 - fm1, d0p = fp1 - f0, dp1 = fp2 - fp1;
+  const R t2m = d0m - dm1, t20 = d0p - d0m, t2p = dp1 - d0p;
+  const R tl = R(3) * d0m - dm1, tc = d0p + d0m, tr = R(3) * d0p - dp1;
+  const R bl = c1 * (t2m * t2m) + c2 * (tl * tl);
+  const R bc = c1 * (t20 * t20) + c2 * (tc * tc);
+  const R br = c1 * (t2p * t2p) + c2 * (tr * tr);
+  const R tt = d_fabs(br - bl);
+  const R iel = R(1) / (bl + eps), iec = R(1) / (bc + eps), ier = R(1) / (br + eps);
+  const R al = R(1) + tt * iel, ac = R(1) + tt * iec, ar = R(1) + tt * ier;
+  R lal, lac, lar;
+  {  // right face: weights (dl al, dc ac, dr ar), polynomials QL, QC, QR
+    const R wl0 = dl * al, wc0 = dc * ac, wr0 = dr * ar;
+    const R iS = R(1) / ((wl0 + wr0) + wc0);
+    const R wl = wl0 * iS, wr = wr0 * iS, wc = R(1) - (wl + wr);
+    const R QL = a11 * fm2 + a12 * fm1 + a13 * f0;
+    const R QC = a21 * fm1 + a22 * f0 + a23 * fp1;
+    const R QR = a31 * f0 + a32 * fp1 + a33 * fp2;
+    const R lQL = wl * lamR, lQR = wr * lamR, lQC = wc * lamR;
+    const R lwl = (QL - QC) * lamR, lwr = (QR - QC) * lamR;
+    const R lS = -(lwl * wl + lwr * wr) * iS;
+    lal = dl * (lwl * iS + lS);
+    lac = dc * lS;
+    lar = dr * (lwr * iS + lS);
+    g[0] += a11 * lQL;
+    g[1] += a12 * lQL + a21 * lQC;
+    g[2] += a13 * lQL + a22 * lQC + a31 * lQR;
+    g[3] += a23 * lQC + a32 * lQR;
+    g[4] += a33 * lQR;
+  }
+  {  // left face: weights (dl ar, dc ac, dr al), mirrored polynomials
+    const R wl0 = dl * ar, wc0 = dc * ac, wr0 = dr * al;
+    const R iS = R(1) / ((wl0 + wr0) + wc0);
+    const R wl = wl0 * iS, wr = wr0 * iS, wc = R(1) - (wl + wr);
+    const R QL = a11 * fp2 + a12 * fp1 + a13 * f0;
+    const R QC = a21 * fp1 + a22 * f0 + a23 * fm1;
+    const R QR = a31 * f0 + a32 * fm1 + a33 * fm2;
+    const R lQL = wl * lamL, lQR = wr * lamL, lQC = wc * lamL;
+    const R lwl = (QL - QC) * lamL, lwr = (QR - QC) * lamL;
+    const R lS = -(lwl * wl + lwr * wr) * iS;
+    lar += dl * (lwl * iS + lS);
+    lac += dc * lS;
+    lal += dr * (lwr * iS + lS);
+    g[4] += a11 * lQL;
+    g[3] += a12 * lQL + a21 * lQC;
+    g[2] += a13 * lQL + a22 * lQC + a31 * lQR;
+    g[1] += a23 * lQC + a32 * lQR;
+    g[0] += a33 * lQR;
+  }
+  const R ltt = lal * iel + lac * iec + lar * ier;
+  R lbl = -lal * tt * (iel * iel);
+  const R lbc = -lac * tt * (iec * iec);
+  R lbr = -lar * tt * (ier * ier);
+  const R s = rsign(br - bl);
+  lbr += s * ltt;
+  lbl -= s * ltt;
+  R ldm1 = R(0), ld0m = R(0), ld0p = R(0), ldp1 = R(0);
+  R lt = R(2) * c1 * t2m * lbl; ld0m += lt; ldm1 -= lt;
+  lt = R(2) * c2 * tl * lbl; ld0m += R(3) * lt; ldm1 -= lt;
+  lt = R(2) * c1 * t20 * lbc; ld0p += lt; ld0m -= lt;
+  lt = R(2) * c2 * tc * lbc; ld0p += lt; ld0m += lt;
+  lt = R(2) * c1 * t2p * lbr; ldp1 += lt; ld0p -= lt;
+  lt = R(2) * c2 * tr * lbr; ld0p += R(3) * lt; ldp1 -= lt;
+  g[0] -= ldm1;
+  g[1] += ldm1 - ld0m;
+  g[2] += ld0m - ld0p;
+  g[3] += ld0p - ldp1;
+  g[4] += ldp1;
+}
+
 // Reverse of prim2cons: lq += (d u / d q)^T lu.
 template <int EQ, typename R>
 __device__ __forceinline__ void prim2cons_rev(const R* q, const R* lu, R* lq, const Phys<R>& P) {
@@ -226,9 +331,26 @@ __device__ __forceinline__ void fluxspeed_rev(const R* q, const R* u, const R* l
   }
 }
 
+// One side of the HLL reverse: lf = kf lF, lu = ku lF, plus the speed
+// adjoints; lq = (df/dq)^T lf + (dc/dq)^T lc + (du/dq)^T ((df/du)^T lf + lu).
+template <int EQ, typename R>
+__device__ __forceinline__ void hll_side_rev(const R* q, const R* lF, R kf, R ku, R lcm, R lcp, R* lq,
+                                             const Phys<R>& P) {
+  constexpr int NV = Var<EQ>::NV;
+  R u[NV], lf[NV], lu[NV];
+  prim2cons<EQ>(q, u, P);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) { lf[v] = kf * lF[v]; lu[v] = ku * lF[v]; lq[v] = R(0); }
+  fluxspeed_rev<EQ>(q, u, lf, lcm, lcp, lq, lu, P);
+  prim2cons_rev<EQ>(q, lu, lq, P);
+}
+
 // Reverse of riemann<EQ, RS_HLL> (HD: src/schemes.F90:1248-1341; MHD with the
 // GLM averaging: 3163-3274) on rotated primitive states.  ql/qr are not
-// modified; lql/lqr receive (dF/dq)^T lF.
+// modified; lql/lqr receive (dF/dq)^T lF.  A forward pass finds the case and
+// the adjoints of sl and sr; then each side is reversed on its own, so few
+// values are live at a time.  In the two-wave case, with a = lF/(sr - sl):
+// lfl = sr a, lul = -sl sr a, lfr = -sl a, lur = sl sr a.
 template <int EQ, typename R>
 __device__ __forceinline__ void hll_rev(const R* ql0, const R* qr0, const R* lF, R* lql, R* lqr, const Phys<R>& P) {
   using V = Var<EQ>;
@@ -237,46 +359,48 @@ __device__ __forceinline__ void hll_rev(const R* ql0, const R* qr0, const R* lF,
 #pragma unroll
   for (int v = 0; v < NV; ++v) { ql[v] = ql0[v]; qr[v] = qr0[v]; }
   if constexpr (V::MHD) glm_average<EQ>(ql, qr, P);
-  R ul[NV], ur[NV], fl[NV], fr[NV], clm, clp, crm, crp;
-  prim2cons<EQ>(ql, ul, P);
-  prim2cons<EQ>(qr, ur, P);
-  fluxspeed<EQ, true>(ql, ul, fl, clm, clp, P);
-  fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
-  const R sl = d_min(clm, crm), sr = d_max(clp, crp);
-  R lfl[NV], lfr[NV], lul[NV], lur[NV];
+  R clm, clp, crm, crp, sl, sr;
+  R lsl = R(0), lsr = R(0);
+  int branch;
+  {
+    R ul[NV], ur[NV], fl[NV], fr[NV];
+    prim2cons<EQ>(ql, ul, P);
+    prim2cons<EQ>(qr, ur, P);
+    fluxspeed<EQ, true>(ql, ul, fl, clm, clp, P);
+    fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
+    sl = d_min(clm, crm);
+    sr = d_max(clp, crp);
+    branch = sl >= R(0) ? 0 : (sr <= R(0) ? 1 : 2);
+    if (branch == 2) {
+      const R srml = sr - sl;
+      R lsrml = R(0);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) { lfl[v] = R(0); lfr[v] = R(0); lul[v] = R(0); lur[v] = R(0); lql[v] = R(0); lqr[v] = R(0); }
-  R lclm = R(0), lclp = R(0), lcrm = R(0), lcrp = R(0);
-  if (sl >= R(0)) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) lfl[v] = lF[v];
-  } else if (sr <= R(0)) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) lfr[v] = lF[v];
-  } else {
-    const R srml = sr - sl;
-    R lsl = R(0), lsr = R(0), lsrml = R(0);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const R wl = sl * ul[v] - fl[v], wr = sr * ur[v] - fr[v];
-      const R F = (sl * wr - sr * wl) / srml;
-      const R a = lF[v] / srml;
-      const R lwr = sl * a, lwl = -sr * a;
-      lsl += a * wr;
-      lsr -= a * wl;
-      lsrml -= a * F;
-      lsl += lwl * ul[v]; lul[v] += sl * lwl; lfl[v] -= lwl;
-      lsr += lwr * ur[v]; lur[v] += sr * lwr; lfr[v] -= lwr;
+      for (int v = 0; v < NV; ++v) {
+        const R wl = sl * ul[v] - fl[v], wr = sr * ur[v] - fr[v];
+        const R F = (sl * wr - sr * wl) / srml;
+        const R a = lF[v] / srml;
+        lsl += a * wr - sr * a * ul[v];
+        lsr += sl * a * ur[v] - a * wl;
+        lsrml -= a * F;
+      }
+      lsr += lsrml;
+      lsl -= lsrml;
     }
-    lsr += lsrml;
-    lsl -= lsrml;
-    if (clm < crm) lclm += lsl; else lcrm += lsl;
-    if (clp > crp) lclp += lsr; else lcrp += lsr;
   }
-  fluxspeed_rev<EQ>(ql, ul, lfl, lclm, lclp, lql, lul, P);
-  fluxspeed_rev<EQ>(qr, ur, lfr, lcrm, lcrp, lqr, lur, P);
-  prim2cons_rev<EQ>(ql, lul, lql, P);
-  prim2cons_rev<EQ>(qr, lur, lqr, P);
+  R lclm = R(0), lclp = R(0), lcrm = R(0), lcrp = R(0);
+  R kfl = R(0), kul = R(0), kfr = R(0), kur = R(0);
+  if (branch == 0) {
+    kfl = R(1);
+  } else if (branch == 1) {
+    kfr = R(1);
+  } else {
+    const R a = R(1) / (sr - sl);
+    kfl = sr * a; kul = -sl * sr * a; kfr = -sl * a; kur = sl * sr * a;
+    if (clm < crm) lclm = lsl; else lcrm = lsl;
+    if (clp > crp) lclp = lsr; else lcrp = lsr;
+  }
+  hll_side_rev<EQ>(ql, lF, kfl, kul, lclm, lclp, lql, P);
+  hll_side_rev<EQ>(qr, lF, kfr, kur, lcrm, lcrp, lqr, P);
   if constexpr (V::MHD) {
     // bx = (BxL+BxR)/2 - (psiR-psiL)/(2 cmax); psi = (psiL+psiR)/2 - (BxR-BxL) cmax/2
     const R lbx = lql[V::BX] + lqr[V::BX], lps = lql[V::BP] + lqr[V::BP];

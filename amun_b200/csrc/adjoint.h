@@ -3,10 +3,11 @@
 // Device arrays (per block b; the layouts of sweep.cuh):
 //   Q      [b][v][k][j][i]     stage-input primitives, padded, working precision
 //   lamU0, lamU1, lamdu        [b][v][k][j][i] interior, FP64
-//   lamQ   [b][v][k][j][i]     padded, FP64
-//   PL, PR [b][m][v][k][j][i]  padded, FP64, m = 0..4: the WENO-Z stencil
-//                              partials of a cell's right (PL) / left (PR)
-//                              face state with respect to cells c-2..c+2
+//   G      [d][side][b][v][k][j][i] padded, FP64: lam of a cell's right
+//                              (side 0) / left (side 1) face state along d
+//   P      [d][b][m][v][k][j][i] padded, FP64, m = 0..4: the WENO-Z stencil
+//                              partials of a cell's two face states along d
+//                              with respect to cells c-2..c+2
 //   inv    [27 b + o]          the block whose neighbour in direction o is b
 #pragma once
 #include <cuda_runtime.h>
@@ -27,15 +28,15 @@ cudaError_t adj_combination(const AdjGeo& a, const StageDesc& st, const DevScala
 // lamU0 += lamU1, lamU1 = 0 (reverse of the U1 = U0 copy of evolve_ssprk2)
 cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStream_t s);
 
-// one direction: interface adjoints -> stencil partials -> lamQ +=
+// all directions: interface adjoints (G) -> stencil partials (P)
 template <typename R>
-cudaError_t adj_direction(const AdjGeo& a, int dir, const R* Q, const double* lamdu, double* PL, double* PR,
-                          double* lamQ, const double* binv, const MethodConst& m, const DevScalars* rec,
-                          cudaStream_t s);
+cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* G, double* P, const double* binv,
+                      const MethodConst& m, const DevScalars* rec, cudaStream_t s);
 
-// ghost images folded into their source cells, then cons2prim^T into lamIn
+// partials gathered at each interior cell and its ghost copies, then
+// cons2prim^T into lamIn
 template <typename R>
-cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* lamQ, const int* inv, double gammam1, double* lamIn,
+cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* P, const int* inv, double gammam1, double* lamIn,
                       cudaStream_t s);
 
 // lamq = prim2cons^T lamU (interior, SoA)

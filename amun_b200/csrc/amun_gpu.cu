@@ -77,12 +77,12 @@ struct AdjCtx {
   std::vector<void*> ck_q;
   DevScalars* ck_sc = nullptr;  // nseg + 1
   DevScalars* rec = nullptr;    // nsteps
+  int ck_cap = 0, rec_cap = 0, seg_cap = 0;
   // reverse-pass work arrays (allocated by the first amun_gpu_adjoint)
   void* seg_q = nullptr;        // interval x stages stage-input primitives
-  double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *lamQ = nullptr, *PL = nullptr, *PR = nullptr;
+  double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *G = nullptr, *P = nullptr;
   double* stage = nullptr;      // host-layout staging
   int* inv = nullptr;
-  long long bytes = 0;
 };
 AdjCtx A;
 
@@ -91,7 +91,7 @@ void adj_free() {
   for (auto p : A.ck_q) cudaFree(p);
   A.ck_u0.clear();
   A.ck_q.clear();
-  void* ptrs[] = {A.ck_sc, A.rec, A.seg_q, A.lamU0, A.lamU1, A.lamdu, A.lamQ, A.PL, A.PR, A.stage, A.inv};
+  void* ptrs[] = {A.ck_sc, A.rec, A.seg_q, A.lamU0, A.lamU1, A.lamdu, A.G, A.P, A.stage, A.inv};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   A = AdjCtx();
@@ -1103,14 +1103,11 @@ int reverse_step(int n, int slot, const AdjGeo& ag) {
     const StageDesc& st = S.stages[s];
     cudaError_t e = adj_combination(ag, st, A.rec + n, C.decay, A.lamU0, A.lamU1, A.lamdu, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint combination");
-    CK(cudaMemsetAsync(A.lamQ, 0, (size_t)C.g.qbs * C.nblocks * sizeof(double), C.stream));
     const R* Q = (const R*)((const char*)A.seg_q + ((size_t)slot * ns + s) * qb);
-    for (int d = 0; d < C.g.ndims; ++d) {
-      e = adj_direction<R>(ag, d, Q, A.lamdu, A.PL, A.PR, A.lamQ, C.binv, m, A.rec + n, C.stream);
-      if (e != cudaSuccess) return cuda_fail(e, "adjoint flux sweep");
-    }
+    e = adj_faces<R>(ag, Q, A.lamdu, A.G, A.P, C.binv, m, A.rec + n, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint flux sweep");
     const int in = s == 0 ? (S.copy_first ? 1 : 0) : S.stages[s - 1].out_dst;
-    e = adj_cells<R>(ag, Q, A.lamQ, A.inv, C.gammam1, in == 0 ? A.lamU0 : A.lamU1, C.stream);
+    e = adj_cells<R>(ag, Q, A.P, A.inv, C.gammam1, in == 0 ? A.lamU0 : A.lamU1, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint cons2prim");
   }
   if (S.copy_first) {
@@ -1162,11 +1159,11 @@ int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval) {
   if (r) return r;
   if ((r = adj_supported())) return r;
   if (nsteps <= 0 || interval <= 0) return fail(AMUN_E_BAD_ARGUMENT, "nsteps and interval must be positive");
-  adj_free();
-  A.nsteps = nsteps;
-  A.interval = interval;
-  A.nseg = (nsteps + interval - 1) / interval;
-  for (int s = 0; s <= A.nseg; ++s) {
+  // buffers of an earlier recording on the same mesh are reused (a free
+  // would synchronise the device); they grow when this run needs more
+  A.recorded = false;
+  const int nseg = (nsteps + interval - 1) / interval;
+  while ((int)A.ck_u0.size() < nseg + 1) {
     double* u = nullptr;
     void* q = nullptr;
     CK(cudaMalloc(&u, upool_doubles() * sizeof(double)));
@@ -1174,9 +1171,26 @@ int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval) {
     CK(cudaMalloc(&q, qpool_bytes()));
     A.ck_q.push_back(q);
   }
-  CK(cudaMalloc(&A.ck_sc, (A.nseg + 1) * sizeof(DevScalars)));
-  CK(cudaMalloc(&A.rec, nsteps * sizeof(DevScalars)));
-  A.bytes = (long long)(A.nseg + 1) * (long long)(upool_doubles() * sizeof(double) + qpool_bytes());
+  if (A.ck_cap < nseg + 1) {
+    if (A.ck_sc) cudaFree(A.ck_sc);
+    A.ck_sc = nullptr;
+    CK(cudaMalloc(&A.ck_sc, (nseg + 1) * sizeof(DevScalars)));
+    A.ck_cap = nseg + 1;
+  }
+  if (A.rec_cap < nsteps) {
+    if (A.rec) cudaFree(A.rec);
+    A.rec = nullptr;
+    CK(cudaMalloc(&A.rec, nsteps * sizeof(DevScalars)));
+    A.rec_cap = nsteps;
+  }
+  if (A.seg_q && A.seg_cap < interval) {
+    cudaFree(A.seg_q);
+    A.seg_q = nullptr;
+    A.seg_cap = 0;
+  }
+  A.nsteps = nsteps;
+  A.interval = interval;
+  A.nseg = nseg;
   if ((r = ensure_maxspeed())) return r;
   r = bulk() ? forward_recorded<float>(nsteps, dtnext) : forward_recorded<double>(nsteps, dtnext);
   if (r) return r;
@@ -1210,14 +1224,15 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
   const size_t ns = schedule().stages.size();
   if (!A.seg_q) {
     CK(cudaMalloc(&A.seg_q, (size_t)A.interval * ns * qpool_bytes()));
+    A.seg_cap = A.interval;
+  }
+  if (!A.lamU0) {
     CK(cudaMalloc(&A.lamU0, ud * sizeof(double)));
     CK(cudaMalloc(&A.lamU1, ud * sizeof(double)));
     CK(cudaMalloc(&A.lamdu, ud * sizeof(double)));
-    CK(cudaMalloc(&A.lamQ, qd * sizeof(double)));
-    CK(cudaMalloc(&A.PL, 5 * qd * sizeof(double)));
-    CK(cudaMalloc(&A.PR, 5 * qd * sizeof(double)));
+    CK(cudaMalloc(&A.G, 2 * (size_t)g.ndims * qd * sizeof(double)));
+    CK(cudaMalloc(&A.P, 5 * (size_t)g.ndims * qd * sizeof(double)));
     CK(cudaMalloc(&A.stage, qd * sizeof(double)));
-    A.bytes += (long long)((size_t)A.interval * ns * qpool_bytes() + (3 * ud + 12 * qd) * sizeof(double));
   }
   if ((r = build_inverse_neighbours())) return r;
   AdjGeo ag{g, C.nv, C.p.eqsys, C.nblocks};
@@ -1251,7 +1266,13 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
 
 int amun_gpu_adjoint_bytes(long long* bytes) {
   if (!bytes) return fail(AMUN_E_BAD_ARGUMENT, "null pointer");
-  *bytes = A.bytes;
+  size_t b = A.ck_u0.size() * (upool_doubles() * sizeof(double) + qpool_bytes());
+  b += (size_t)(A.ck_cap + A.rec_cap) * sizeof(DevScalars);
+  if (C.inited && C.nblocks > 0) {
+    b += (size_t)A.seg_cap * schedule().stages.size() * qpool_bytes();
+    if (A.lamU0) b += (3 * upool_doubles() + (1 + 7 * (size_t)C.g.ndims) * (size_t)C.g.qbs * C.nblocks) * sizeof(double);
+  }
+  *bytes = (long long)b;
   return 0;
 }
 
