@@ -78,6 +78,7 @@ struct AdjCtx {
   DevScalars* ck_sc = nullptr;  // nseg + 1
   DevScalars* rec = nullptr;    // nsteps
   int ck_cap = 0, rec_cap = 0, seg_cap = 0;
+  double recompute_ms = 0.0, reverse_ms = 0.0;  // phases of the last adjoint
   // reverse-pass work arrays (allocated by the first amun_gpu_adjoint)
   void* seg_q = nullptr;        // interval x stages stage-input primitives
   double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *G = nullptr, *P = nullptr;
@@ -1137,17 +1138,31 @@ int forward_recorded(int nsteps, double dtnext) {
 
 template <typename R>
 int adjoint_pass(const AdjGeo& ag) {
-  for (int seg = A.nseg - 1; seg >= 0; --seg) {
+  // events around each segment's recomputation and reverse sweep (device
+  // time of the two phases, read back after the pass)
+  std::vector<cudaEvent_t> ev(3 * (size_t)A.nseg, nullptr);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  int r = 0;
+  for (int seg = A.nseg - 1; seg >= 0 && !r; --seg) {
     const int n0 = seg * A.interval;
     const int n1 = n0 + A.interval < A.nsteps ? n0 + A.interval : A.nsteps;
-    int r = restore_state(seg);
-    if (r) return r;
-    for (int n = n0; n < n1; ++n)
-      if ((r = replay_step<R>(n, n - n0))) return r;
-    for (int n = n1 - 1; n >= n0; --n)
-      if ((r = reverse_step<R>(n, n - n0, ag))) return r;
+    cudaEventRecord(ev[3 * seg], C.stream);
+    r = restore_state(seg);
+    for (int n = n0; n < n1 && !r; ++n) r = replay_step<R>(n, n - n0);
+    cudaEventRecord(ev[3 * seg + 1], C.stream);
+    for (int n = n1 - 1; n >= n0 && !r; --n) r = reverse_step<R>(n, n - n0, ag);
+    cudaEventRecord(ev[3 * seg + 2], C.stream);
   }
-  return 0;
+  A.recompute_ms = A.reverse_ms = 0.0;
+  if (!r && cudaStreamSynchronize(C.stream) == cudaSuccess) {
+    for (int seg = 0; seg < A.nseg; ++seg) {
+      float a = 0.f, b = 0.f;
+      if (cudaEventElapsedTime(&a, ev[3 * seg], ev[3 * seg + 1]) == cudaSuccess) A.recompute_ms += a;
+      if (cudaEventElapsedTime(&b, ev[3 * seg + 1], ev[3 * seg + 2]) == cudaSuccess) A.reverse_ms += b;
+    }
+  }
+  for (auto e : ev) cudaEventDestroy(e);
+  return r;
 }
 
 }  // namespace
@@ -1261,6 +1276,13 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
   // leave the recorded final state on the device
   if ((r = restore_state(A.nseg))) return r;
   CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_adjoint_timing(double* recompute_ms, double* reverse_ms) {
+  if (!recompute_ms || !reverse_ms) return fail(AMUN_E_BAD_ARGUMENT, "null pointer");
+  *recompute_ms = A.recompute_ms;
+  *reverse_ms = A.reverse_ms;
   return 0;
 }
 

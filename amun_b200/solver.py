@@ -176,6 +176,13 @@ class Simulation:
         N.check(self.L.amun_gpu_adjoint(N.dptr(lb), N.dptr(lq), N.dptr(lu)))
         return self.mesh.from_blocks(lq), self.mesh.from_blocks(lu)
 
+    def adjoint_timing(self):
+        """(recompute_ms, reverse_ms): device time of the last adjoint's
+        segment recomputation and reverse sweep."""
+        a, b = C.c_double(), C.c_double()
+        N.check(self.L.amun_gpu_adjoint_timing(C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def adjoint_bytes(self) -> int:
         b = C.c_longlong()
         N.check(self.L.amun_gpu_adjoint_bytes(C.byref(b)))

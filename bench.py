@@ -207,8 +207,13 @@ def adjoint_timing(torch, prec):
     out = {}
     adj = events(lambda: out.setdefault("g", sim.adjoint(lam)))
     gbytes = sim.adjoint_bytes()
+    recompute_ms, reverse_ms = sim.adjoint_timing()
     sim.close()
+    # both runs cover the same 200 steps x 3 stages, so reverse/forward is
+    # also the cost of one stage's adjoint over one forward stage
     return {"forward_ms": fwd, "recorded_forward_ms": rec, "adjoint_ms": adj,
+            "adjoint_recompute_ms": recompute_ms, "adjoint_reverse_ms": reverse_ms,
+            "reverse_stage_over_forward_stage": reverse_ms / fwd,
             "adjoint_over_forward": adj / fwd, "gradient_over_forward": (rec + adj) / fwd,
             "steps": ADJOINT_STEPS, "checkpoint_interval": ADJOINT_INTERVAL, "device_bytes": gbytes,
             "grad_rho_l2": float(np.sqrt(np.sum(out["g"][0][..., 0] ** 2)))}

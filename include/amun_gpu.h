@@ -225,6 +225,10 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0);
 /* device bytes held by the recording and the adjoint work arrays */
 int amun_gpu_adjoint_bytes(long long* bytes);
 
+/* device time of the last amun_gpu_adjoint: segment recomputation (forward
+ * steps from the checkpoints) and reverse sweep (the adjoint kernels) */
+int amun_gpu_adjoint_timing(double* recompute_ms, double* reverse_ms);
+
 /* finalize_*: release the device pool, graphs and stream. */
 void amun_gpu_finalize(void);
 
