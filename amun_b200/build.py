@@ -7,14 +7,16 @@ Translation units:
   kernels_fp32*.cu       FP32-bulk sweep and auxiliary kernels
 
 Every FP64 unit is compiled with -fmad=false so no multiply-add is fused
-and the arithmetic follows the reference operation by operation.  The FP64
-sweep units cap registers at two 288-thread CTAs per SM
-(AMUN_SWEEP_MIN_BLOCKS=2: 96 registers instead of 128; one CTA per SM leaves
-the FP64 pipe waiting on shared-memory and global latency, two CTAs cut the
-128^3 MHD step from 7.8 to 5.1 ms on B200 with bit-identical results).  The
-FP32-bulk units keep contraction on and use the approximate single-precision
-divide and square root with denormals flushed (2.68 -> 2.39 ms per step);
-their conserved totals and recovery stay in FP64.
+and the arithmetic follows the reference operation by operation.
+
+The sweep kernels are bound by instruction issue and latency, not by HBM,
+so occupancy decides their speed: AMUN_SWEEP_MIN_BLOCKS caps registers so
+that that many 288-thread CTAs fit on an SM.  Measured on B200 (128^3 MHD,
+WENO-Z, HLLD, SSPRK3): FP64 with 1/2/3 CTAs 7.8/5.1/4.8 ms per step (results
+bit-identical, small spills at 3); FP32 bulk with 2/3/4/5 CTAs
+2.40/1.92/1.79/1.89 ms.  The FP32 units also use the approximate
+single-precision divide and square root with denormals flushed; their
+conserved totals and the relativistic recovery stay in FP64.
 """
 from __future__ import annotations
 
@@ -33,8 +35,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-I", os.path.join(HERE, "..", "include")]
 
 FP64 = ["-fmad=false"]
-FP64_SWEEP = FP64 + ["-DAMUN_SWEEP_MIN_BLOCKS=2"]
+FP64_SWEEP = FP64 + ["-DAMUN_SWEEP_MIN_BLOCKS=3"]
 FP32 = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+FP32_SWEEP = FP32 + ["-DAMUN_SWEEP_MIN_BLOCKS=4"]
 
 UNITS = {
     "amun_gpu.cu": FP64,
@@ -45,9 +48,9 @@ UNITS = {
     "kernels_fp64_mhd.cu": FP64_SWEEP,
     "kernels_fp64_srmhd.cu": FP64_SWEEP,
     "kernels_fp32.cu": FP32,
-    "kernels_fp32_hd.cu": FP32,
-    "kernels_fp32_mhd.cu": FP32,
-    "kernels_fp32_srmhd.cu": FP32,
+    "kernels_fp32_hd.cu": FP32_SWEEP,
+    "kernels_fp32_mhd.cu": FP32_SWEEP,
+    "kernels_fp32_srmhd.cu": FP32_SWEEP,
 }
 
 
@@ -79,12 +82,16 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     def compile_one(src):
         obj = os.path.join(OBJ, src.replace(".cu", ".o"))
         srcp = os.path.join(CSRC, src)
-        if not force and not _sources_newer(obj, [srcp] + hdrs):
-            return obj, None
         cmd = [cc, *ARCH, *COMMON, *UNITS[src], "-c", srcp, "-o", obj]
+        stamp = obj + ".cmd"  # the command that built obj: a flag change rebuilds it
+        same_cmd = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+        if not force and same_cmd and not _sources_newer(obj, [srcp] + hdrs):
+            return obj, None
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             return obj, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"
+        with open(stamp, "w") as fh:
+            fh.write(" ".join(cmd))
         if verbose and r.stderr:
             print(r.stderr, file=sys.stderr)
         return obj, None
