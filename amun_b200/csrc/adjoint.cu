@@ -23,6 +23,12 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kFaceThreads = 128;
+// CTAs of the face kernel per SM the register allocation must allow (4: 128
+// registers; measured on B200, 2D MHD 256^2 FP64: the reverse sweep 87 -> 71 ms
+// per 200 steps against 158 registers at 3 CTAs)
+#ifndef AMUN_ADJ_FACE_MIN_BLOCKS
+#define AMUN_ADJ_FACE_MIN_BLOCKS 4
+#endif
 
 int blocks_of(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
@@ -135,7 +141,7 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
 
 // blockIdx.z = direction
 template <int EQ, typename R>
-__global__ void __launch_bounds__(kFaceThreads) face_kernel(const R* __restrict__ Q,
+__global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_kernel(const R* __restrict__ Q,
                                                             const double* __restrict__ lamdu,
                                                             double* __restrict__ G, const double* __restrict__ binv,
                                                             Geo g, MethodConst m, const DevScalars* rec) {
