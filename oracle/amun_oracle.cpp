@@ -29,6 +29,8 @@
 #include <thread>
 #include <algorithm>
 #include <atomic>
+#include <stdexcept>
+#include <unordered_map>
 
 namespace {
 
@@ -426,8 +428,34 @@ struct Oracle {
   double dx = 1, dy = 1, dz = 1;
   // uniform block grid at one level
   int nbx = 1, nby = 1, nbz = 1;
-  struct Block { std::vector<double> u0, u1, q, f; double* u; };
+  // A block of the mesh: its arrays, its level and its position at that
+  // level (in blocks, zero based), and its cell size (adx/ady/adz(level),
+  // src/coordinates.F90:160-249).
+  struct Block {
+    std::vector<double> u0, u1, q, f;
+    double* u;
+    int level = 1, cx = 0, cy = 0, cz = 0;
+    double dx = 1, dy = 1, dz = 1;
+  };
   std::vector<Block> blocks;
+  // blocks at several levels (set_mesh): ghost cells are filled by copy,
+  // restriction or prolongation and coarse face fluxes are corrected
+  bool amr = false;
+  int mlev = 1;  // the finest level present
+  std::unordered_map<long long, int> where;  // (level, cx, cy, cz) -> block
+  static long long bkey(int l, int x, int y, int z) {
+    return (((long long)l * 65536 + x) * 65536 + y) * 65536 + z;
+  }
+  int find_block(int l, int x, int y, int z) const {
+    auto it = where.find(bkey(l, x, y, z));
+    return it == where.end() ? -1 : it->second;
+  }
+  double level_dx(int l, int d) const {
+    const double ff = (double)(1 << (l - 1));
+    if (d == 0) return (p.xmax - p.xmin) / (p.xblocks * (in * ff));
+    if (d == 1) return (p.ymax - p.ymin) / (p.yblocks * (jn * ff));
+    return p.ndims == 3 ? (p.zmax - p.zmin) / (p.zblocks * (kn * ff)) : 1.0;
+  }
   int nthreads = 1;
   std::atomic<long> nonpositive{0};  // "Positive variable is not positive" events
 
@@ -474,12 +502,41 @@ struct Oracle {
     dz = (p.ndims == 3) ? (p.zmax - p.zmin) / (p.zblocks * (kn * ff)) : 1.0;
     nbx = p.xblocks * ff; nby = p.yblocks * ff; nbz = (p.ndims == 3) ? p.zblocks * ff : 1;
     blocks.assign((size_t)nbx * nby * nbz, Block());
-    for (auto& b : blocks) {
+    mlev = lev;
+    for (size_t bi = 0; bi < blocks.size(); ++bi) {
+      Block& b = blocks[bi];
       b.u0.assign(nv * cells(), 0.0); b.u1.assign(nv * cells(), 0.0);
       b.q.assign(nv * cells(), 0.0);
       b.f.assign((size_t)p.ndims * nv * cells(), 0.0);
       b.u = b.u0.data();
+      b.level = lev;
+      b.cx = (int)(bi % nbx); b.cy = (int)((bi / nbx) % nby); b.cz = (int)(bi / ((size_t)nbx * nby));
+      b.dx = dx; b.dy = dy; b.dz = dz;
     }
+    return 0;
+  }
+
+  // Blocks at the given levels and positions (a leaf list of the AMR tree).
+  // The mesh must be 2:1 balanced across faces, edges and corners and cover
+  // the periodic domain.
+  int set_mesh(int n, const int* levels, const int* coords) {
+    blocks.assign((size_t)n, Block());
+    where.clear();
+    mlev = 1;
+    for (int b = 0; b < n; ++b) {
+      Block& B = blocks[b];
+      B.u0.assign(nv * cells(), 0.0); B.u1.assign(nv * cells(), 0.0);
+      B.q.assign(nv * cells(), 0.0);
+      B.f.assign((size_t)p.ndims * nv * cells(), 0.0);
+      B.u = B.u0.data();
+      B.level = levels[b];
+      B.cx = coords[3 * b]; B.cy = coords[3 * b + 1]; B.cz = p.ndims == 3 ? coords[3 * b + 2] : 0;
+      B.dx = level_dx(B.level, 0); B.dy = level_dx(B.level, 1); B.dz = level_dx(B.level, 2);
+      if (B.level > mlev) mlev = B.level;
+      where[bkey(B.level, B.cx, B.cy, B.cz)] = b;
+    }
+    dx = level_dx(mlev, 0); dy = level_dx(mlev, 1); dz = level_dx(mlev, 2);
+    amr = true;
     return 0;
   }
 
@@ -1851,9 +1908,9 @@ struct Oracle {
   // EVOLUTION
   // =========================================================================
   // update_increment src/evolution.F90:1898-1977
-  void update_increment(const double* f, double* du) const {
+  void update_increment(const Block& B, const double* f, double* du) const {
     std::fill(du, du + (size_t)nv * cells(), 0.0);
-    double dxi = 1.0 / dx, dyi = 1.0 / dy, dzi = 1.0 / dz;
+    double dxi = 1.0 / B.dx, dyi = 1.0 / B.dy, dzi = 1.0 / B.dz;
     for (int k = kbl; k <= keu; ++k)
       for (int j = jbl; j <= jeu; ++j)
         for (int i = ibl; i <= ieu; ++i)
@@ -1893,6 +1950,7 @@ struct Oracle {
   // update_ghost_cells (src/boundaries.F90:6633-6736), i.e. prim2cons in
   // every ghost cell of the current u.
   void boundary_variables() {
+    if (amr) { boundary_variables_levels(); return; }
     const int NX = nbx * in, NY = nby * jn, NZ = nbz * kn;
     auto gidx = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
     // ghosts of each block are written from the interiors of others only, so
@@ -1920,6 +1978,189 @@ struct Oracle {
             bool ghost = i < ib || i > ie || j < jb || j > je || (p.ndims == 3 && (k < kb || k > ke));
             if (ghost) prim2cons(1, &B.q[qi(1, i, j, k)], &B.u[qi(1, i, j, k)]);
           }
+    });
+  }
+
+  // boundary_variables src/boundaries.F90:372-479 on a mesh with level
+  // jumps.  Each ghost cell takes the state of the place it covers: a copy of
+  // the same-level neighbour's cell (boundaries_*_copy), the mean of the 2^d
+  // cells of a finer neighbour (boundaries_*_restrict with block_*_restrict,
+  // src/boundaries.F90:5637-6070: same pairing order), or the limited linear
+  // prolongation of a coarser neighbour's cell (boundaries_*_prolong with
+  // block_*_prolong, 6071-6450: limiter_prol slopes, positivity halving,
+  // the same child combinations).  As in the reference, copies and
+  // restrictions come first; prolongations read the coarse block's cells and
+  // ghosts after them (on a 2:1 balanced mesh a prolongation never reads a
+  // ghost that is itself prolonged).
+  void ghost_position(const Block& B, int i, int j, int k, int& gx, int& gy, int& gz) const {
+    auto wrap = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+    const int f = 1 << (B.level - 1);
+    gx = wrap(B.cx * in + (i - ib), p.xblocks * f * in);
+    gy = wrap(B.cy * jn + (j - jb), p.yblocks * f * jn);
+    gz = p.ndims == 3 ? wrap(B.cz * kn + (k - kb), p.zblocks * f * kn) : 0;
+  }
+  bool is_ghost(int i, int j, int k) const {
+    return i < ib || i > ie || j < jb || j > je || (p.ndims == 3 && (k < kb || k > ke));
+  }
+  // the restricted value of variable v at coarse global cell (gx,gy,gz) of
+  // level l from the finer block at level l+1
+  double restrict_value(int l, int gx, int gy, int gz, int v) const {
+    const int fx = 2 * gx, fy = 2 * gy, fz = 2 * gz;
+    const int F = find_block(l + 1, fx / in, fy / jn, p.ndims == 3 ? fz / kn : 0);
+    if (F < 0) throw std::runtime_error("mesh: a ghost cell is covered by no block");
+    const Block& S = blocks[F];
+    const int il = fx % in + ib, jl = fy % jn + jb, ip = il + 1, jp = jl + 1;
+    if (p.ndims == 2) {
+      return 0.25 * ((S.q[qi(v, il, jl, 1)] + S.q[qi(v, ip, jp, 1)]) + (S.q[qi(v, il, jp, 1)] + S.q[qi(v, ip, jl, 1)]));
+    }
+    const int kl = fz % kn + kb, kp = kl + 1;
+    return 0.125 * (((S.q[qi(v, il, jl, kl)] + S.q[qi(v, ip, jp, kp)]) + (S.q[qi(v, il, jl, kp)] + S.q[qi(v, ip, jp, kl)])) +
+                    ((S.q[qi(v, il, jp, kp)] + S.q[qi(v, ip, jl, kl)]) + (S.q[qi(v, il, jp, kl)] + S.q[qi(v, ip, jl, kp)])));
+  }
+  // the prolonged value of variable v for the child (sx,sy,sz) (0: lower,
+  // 1: upper half) of coarse cell (i,j,k) of block C
+  double prolong_value(const Block& C, int i, int j, int k, int sx, int sy, int sz, int v) const {
+    const double q0 = C.q[qi(v, i, j, k)];
+    double dq[3] = {0.0, 0.0, 0.0};
+    dq[0] = limiter(p.plim, 0.5, q0 - C.q[qi(v, i - 1, j, k)], C.q[qi(v, i + 1, j, k)] - q0);
+    dq[1] = limiter(p.plim, 0.5, q0 - C.q[qi(v, i, j - 1, k)], C.q[qi(v, i, j + 1, k)] - q0);
+    if (p.ndims == 3) dq[2] = limiter(p.plim, 0.5, q0 - C.q[qi(v, i, j, k - 1)], C.q[qi(v, i, j, k + 1)] - q0);
+    if (v == idn || v == ipr) {
+      if (q0 > 0.0) {
+        for (int it = 0; it < 4096; ++it) {
+          double sa = std::fabs(dq[0]) + std::fabs(dq[1]);
+          if (p.ndims == 3) sa = sa + std::fabs(dq[2]);
+          if (!(q0 <= sa)) break;
+          dq[0] = 0.5 * dq[0]; dq[1] = 0.5 * dq[1]; dq[2] = 0.5 * dq[2];
+        }
+      } else {
+        dq[0] = dq[1] = dq[2] = 0.0;
+      }
+    }
+    dq[0] = 0.5 * dq[0]; dq[1] = 0.5 * dq[1]; dq[2] = 0.5 * dq[2];
+    if (p.ndims == 2) {
+      const double dq1 = dq[0] + dq[1], dq2 = dq[0] - dq[1];
+      if (sx == 0 && sy == 0) return q0 - dq1;
+      if (sx == 1 && sy == 0) return q0 + dq2;
+      if (sx == 0 && sy == 1) return q0 - dq2;
+      return q0 + dq1;
+    }
+    const double dq1 = dq[0] + dq[1] + dq[2], dq2 = dq[0] - dq[1] - dq[2];
+    const double dq3 = dq[0] - dq[1] + dq[2], dq4 = dq[0] + dq[1] - dq[2];
+    const int c = sx + 2 * sy + 4 * sz;
+    switch (c) {
+      case 0: return q0 - dq1;
+      case 1: return q0 + dq2;
+      case 2: return q0 - dq3;
+      case 3: return q0 + dq4;
+      case 4: return q0 - dq4;
+      case 5: return q0 + dq3;
+      case 6: return q0 - dq2;
+      default: return q0 + dq1;
+    }
+  }
+  void boundary_variables_levels() {
+    for (int pass = 1; pass <= 2; ++pass) {
+      // pass 2 reads only interiors and pass-1 ghosts, so blocks fill in parallel
+      parallel_index(blocks.size(), [&](size_t bi) {
+        Block& B = blocks[bi];
+        for (int k = 1; k <= km; ++k)
+          for (int j = 1; j <= jm; ++j)
+            for (int i = 1; i <= im; ++i) {
+              if (!is_ghost(i, j, k)) continue;
+              int gx, gy, gz;
+              ghost_position(B, i, j, k, gx, gy, gz);
+              const int L = B.level;
+              const int S = find_block(L, gx / in, gy / jn, p.ndims == 3 ? gz / kn : 0);
+              if (S >= 0) {
+                if (pass != 1) continue;
+                const Block& N = blocks[S];
+                const int si = gx % in + ib, sj = gy % jn + jb, sk = p.ndims == 3 ? gz % kn + kb : 1;
+                for (int v = 1; v <= nv; ++v) B.q[qi(v, i, j, k)] = N.q[qi(v, si, sj, sk)];
+                continue;
+              }
+              const int cgx = gx / 2, cgy = gy / 2, cgz = gz / 2;
+              const int Cb = L > 1 ? find_block(L - 1, cgx / in, cgy / jn, p.ndims == 3 ? cgz / kn : 0) : -1;
+              if (Cb >= 0) {
+                if (pass != 2) continue;
+                const Block& Cc = blocks[Cb];
+                const int ci = cgx % in + ib, cj = cgy % jn + jb, ck = p.ndims == 3 ? cgz % kn + kb : 1;
+                for (int v = 1; v <= nv; ++v)
+                  B.q[qi(v, i, j, k)] = prolong_value(Cc, ci, cj, ck, gx % 2, gy % 2, p.ndims == 3 ? gz % 2 : 0, v);
+                continue;
+              }
+              if (pass != 1) continue;
+              for (int v = 1; v <= nv; ++v) B.q[qi(v, i, j, k)] = restrict_value(L, gx, gy, gz, v);
+            }
+      });
+    }
+    parallel_blocks([&](Block& B) {
+      for (int k = 1; k <= km; ++k)
+        for (int j = 1; j <= jm; ++j)
+          for (int i = 1; i <= im; ++i)
+            if (is_ghost(i, j, k)) prim2cons(1, &B.q[qi(1, i, j, k)], &B.u[qi(1, i, j, k)]);
+    });
+  }
+
+  // boundary_fluxes src/boundaries.F90:494-1087 with block_update_flux
+  // 6539-6614: the flux through a face shared with finer blocks becomes the
+  // average of the finer blocks' fluxes there (2 in 2D, 4 in 3D, same
+  // pairing and division).
+  void boundary_fluxes() {
+    if (!amr) return;
+    parallel_index(blocks.size(), [&](size_t bi) {
+      Block& C = blocks[bi];
+      const int L = C.level;
+      for (int d = 1; d <= p.ndims; ++d)
+        for (int side = 0; side < 2; ++side) {
+          // global level-L index of the first cell outside the face
+          const int n1 = d == 1 ? in : (d == 2 ? jn : kn);
+          const int c0 = d == 1 ? C.cx : (d == 2 ? C.cy : C.cz);
+          const int nb = (d == 1 ? p.xblocks : (d == 2 ? p.yblocks : p.zblocks)) * (1 << L) * n1;  // level L+1 extent
+          auto wrap = [](int a, int n) { a %= n; return a < 0 ? a + n : a; };
+          // the finer cells just outside the face, along d
+          const int fo = wrap(side == 0 ? 2 * c0 * n1 - 1 : 2 * (c0 + 1) * n1, nb);
+          const int fface = side == 0 ? (d == 1 ? ie : (d == 2 ? je : ke)) : (d == 1 ? ibl : (d == 2 ? jbl : kbl));
+          const int cface = side == 0 ? (d == 1 ? ibl : (d == 2 ? jbl : kbl)) : (d == 1 ? ie : (d == 2 ? je : ke));
+          // transverse axes (a, b): x-face (y, z), y-face (x, z), z-face (x, y)
+          const int ta = d == 1 ? 2 : 1, tb = d == 3 ? 2 : 3;
+          const int na = ta == 1 ? in : jn, nbt = p.ndims == 3 ? (tb == 2 ? jn : kn) : 1;
+          const int ca0 = (ta == 1 ? C.cx : C.cy) * na;
+          const int cb0 = p.ndims == 3 ? (tb == 2 ? C.cy : C.cz) * nbt : 0;
+          for (int b_ = 0; b_ < nbt; ++b_)
+            for (int a_ = 0; a_ < na; ++a_) {
+              const int fa = 2 * (ca0 + a_), fb = 2 * (cb0 + b_);
+              int fc[3];
+              fc[d - 1] = fo;
+              fc[ta - 1] = fa;
+              if (p.ndims == 3) fc[tb - 1] = fb;
+              const int F = find_block(L + 1, fc[0] / in, fc[1] / jn, p.ndims == 3 ? fc[2] / kn : 0);
+              if (F < 0) continue;  // no finer neighbour across this part of the face
+              const Block& Fb = blocks[F];
+              int lc[3];  // local (Fortran) indices of the lower-left fine face cell
+              lc[d - 1] = fface;
+              lc[ta - 1] = fa % (ta == 1 ? in : jn) + (ta == 1 ? ib : jb);
+              if (p.ndims == 3) lc[tb - 1] = fb % (tb == 2 ? jn : kn) + (tb == 2 ? jb : kb);
+              else lc[2] = 1;
+              int cc[3];
+              cc[d - 1] = cface;
+              cc[ta - 1] = a_ + (ta == 1 ? ib : jb);
+              if (p.ndims == 3) cc[tb - 1] = b_ + (tb == 2 ? jb : kb);
+              else cc[2] = 1;
+              auto ff = [&](int v, int da, int db) {
+                int x[3] = {lc[0], lc[1], lc[2]};
+                x[ta - 1] += da;
+                if (p.ndims == 3) x[tb - 1] += db;
+                return Fb.f[fi(d, v, x[0], x[1], x[2])];
+              };
+              for (int v = 1; v <= nv; ++v) {
+                double val;
+                if (p.ndims == 2) val = (ff(v, 0, 0) + ff(v, 1, 0)) / 2.0;
+                else val = ((ff(v, 0, 0) + ff(v, 1, 1)) + (ff(v, 0, 1) + ff(v, 1, 0))) / 4.0;
+                C.f[fi(d, v, cc[0], cc[1], cc[2])] = val;
+              }
+            }
+        }
     });
   }
 
@@ -1960,6 +2201,7 @@ struct Oracle {
   // on a single-level mesh)
   void update_fluxes() {
     parallel_blocks([&](Block& B) { update_flux(B.q.data(), B.f.data()); });
+    boundary_fluxes();
   }
 
   // One stage: fluxes, then per block increment + combination.  `comb`
@@ -1968,7 +2210,7 @@ struct Oracle {
     update_fluxes();
     parallel_blocks([&](Block& B) {
       std::vector<double> du((size_t)nv * cells());
-      update_increment(B.f.data(), du.data());
+      update_increment(B, B.f.data(), du.data());
       comb(B, du.data());
     });
   }
@@ -2172,6 +2414,32 @@ void or_get_cons(void* h, double* ug) {
   Oracle* o = static_cast<Oracle*>(h);
   o->for_global([&](Oracle::Block& B, size_t lo, size_t g) { for (int v = 0; v < o->nv; ++v) ug[g + v] = B.u[lo + v]; });
 }
+// A mesh of n blocks at the given levels and positions (coords: 3 per block,
+// zero based, in blocks of that level); the state is reset to zero.
+int or_set_mesh(void* h, int n, const int* levels, const int* coords) {
+  return static_cast<Oracle*>(h)->set_mesh(n, levels, coords);
+}
+// The primitive state of every block (n blocks of Fortran arrays, back to
+// back; ghost entries ignored): u0 = prim2cons(q) in the interior, then
+// boundary_variables as after setup_problem.
+void or_set_blocks_prim(void* h, const double* qb) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t per = (size_t)o->nv * o->cells();
+  for (size_t b = 0; b < o->blocks.size(); ++b) {
+    auto& B = o->blocks[b];
+    for (int k = o->kb; k <= o->ke; ++k)
+      for (int j = o->jb; j <= o->je; ++j)
+        for (int i = o->ib; i <= o->ie; ++i) {
+          size_t lo = o->qi(1, i, j, k);
+          for (int v = 0; v < o->nv; ++v) B.q[lo + v] = qb[b * per + lo + v];
+          o->prim2cons(1, &B.q[lo], &B.u0[lo]);
+        }
+    B.u = B.u0.data();
+  }
+  o->boundary_variables();
+  o->time = 0.0; o->step = 0;
+}
+
 // Raw block arrays (Fortran layout) of block b: which 0=u0 1=u1 2=q
 void or_get_block(void* h, int b, int which, double* out) {
   Oracle* o = static_cast<Oracle*>(h);

@@ -51,6 +51,9 @@ def lib():
         L.or_get_prim.argtypes = [vp, d]
         L.or_get_cons.argtypes = [vp, d]
         L.or_get_block.argtypes = [vp, i, i, d]
+        L.or_set_mesh.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.or_set_mesh.restype = i
+        L.or_set_blocks_prim.argtypes = [vp, d]
         L.or_new_time_step.argtypes = [vp, C.c_double, d, d]
         L.or_advance.argtypes = [vp, C.c_double, d, d]
         L.or_scalars.argtypes = [vp, d]
@@ -190,6 +193,22 @@ class Oracle:
         f = np.zeros((self.km, self.jm, self.im, self.nv, nd))
         self.L.or_update_flux(self.h, _p(qblock), _p(f))
         return f
+
+    def set_mesh(self, levels, coords):
+        """Blocks at `levels` (1-based) and positions `coords` ((n, 3), zero
+        based, in blocks of each level); the state is reset."""
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        co = np.ascontiguousarray(coords, dtype=np.int32).reshape(-1, 3)
+        self.mesh_blocks = len(lv)
+        r = self.L.or_set_mesh(self.h, len(lv), lv.ctypes.data_as(C.POINTER(C.c_int)),
+                               co.ctypes.data_as(C.POINTER(C.c_int)))
+        if r != 0:
+            raise RuntimeError(f"or_set_mesh returned {r}")
+
+    def set_blocks_prim(self, qb: np.ndarray):
+        """Primitive state of every block, (nblocks, km, jm, im, nv) with
+        ghosts (ignored); u0 = prim2cons(q) and the ghost cells are filled."""
+        self.L.or_set_blocks_prim(self.h, _p(qb))
 
     def block(self, b: int, which: str = "q"):
         out = np.empty((self.km, self.jm, self.im, self.nv))
