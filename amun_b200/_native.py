@@ -31,12 +31,13 @@ class amun_params(C.Structure):
         ("fix_positivity", C.c_int), ("clip_extrema", C.c_int), ("precision", C.c_int), ("ncells", C.c_int),
         ("nghosts", C.c_int), ("gamma", C.c_double), ("cfl", C.c_double), ("alpha", C.c_double),
         ("eps", C.c_double), ("tolerance", C.c_double), ("pmin", C.c_double), ("nr_maxit", C.c_int),
-        ("nr_extra", C.c_int), ("states_4vec", C.c_int),
+        ("nr_extra", C.c_int), ("states_4vec", C.c_int), ("prolongation_limiter", C.c_int),
+        ("xblocks", C.c_int), ("yblocks", C.c_int), ("zblocks", C.c_int),
     ]
 
 
 class amun_block_desc(C.Structure):
-    _fields_ = [("level", C.c_int), ("dx", C.c_double * 3), ("neighbor", C.c_int * 27)]
+    _fields_ = [("level", C.c_int), ("dx", C.c_double * 3), ("neighbor", C.c_int * 27), ("coord", C.c_int * 3)]
 
 
 class amun_status(C.Structure):

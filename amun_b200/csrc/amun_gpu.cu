@@ -11,6 +11,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <algorithm>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/amun_gpu.h"
@@ -63,6 +65,15 @@ struct Ctx {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   long long prof_n[5] = {0, 0, 0, 0, 0};
   std::string err;
+  // meshes with level jumps (set_blocks with blocks at several levels)
+  bool amr = false;
+  GhostOp* gop = nullptr;    // copies + restrictions, then prolongations
+  long long nop1 = 0, nop2 = 0;
+  int* frole = nullptr;      // [b][dir][side]
+  int* fquad = nullptr;      // [b][dir][side][4]
+  int* blist = nullptr;      // blocks ordered finest level first
+  void* ff = nullptr;        // stored face fluxes
+  std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
 };
 
 Ctx C;
@@ -190,6 +201,11 @@ void free_pool() {
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   for (auto& x : C.q)
     if (x) { cudaFree(x); x = nullptr; }
+  void* amrp[] = {C.gop, C.frole, C.fquad, C.blist, C.ff};
+  for (void* x : amrp)
+    if (x) cudaFree(x);
+  C.gop = nullptr; C.frole = C.fquad = C.blist = nullptr; C.ff = nullptr;
+  C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   if (C.u0) cudaFree(C.u0);
   if (C.u1) cudaFree(C.u1);
   if (C.du) cudaFree(C.du);
@@ -285,6 +301,7 @@ MethodConst method_const() {
   m.eps = C.p.eps; m.decay = C.decay;
   m.lim = C.p.limiter; m.clim = C.p.extrema_limiter; m.positivity = C.p.fix_positivity; m.clip = C.p.clip_extrema;
   m.tol = C.p.tolerance; m.pmin = C.p.pmin; m.nrmax = C.p.nr_maxit; m.nrext = C.p.nr_extra;
+  m.plim = C.p.prolongation_limiter;
   m.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
   return m;
 }
@@ -296,6 +313,9 @@ int effective_solver() {
   if (C.p.eqsys == AMUN_EQ_SRMHD && rs != AMUN_RS_HLLC) rs = AMUN_RS_HLL;
   return rs;
 }
+
+template <typename R>
+cudaError_t ghost_fill(R* q);
 
 template <typename R>
 int launch_stage(const StageDesc& st) {
@@ -318,17 +338,30 @@ int launch_stage(const StageDesc& st) {
   a.m = method_const();
   a.st = st;
   a.LP = LP; a.LW = LW;
+  a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr;
   const int rs = effective_solver();
   for (int d = 0; d < C.g.ndims; ++d) {
     a.first = d == 0;
     a.last = d == C.g.ndims - 1;
     ProfScope ps(d);
-    cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
-    if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+    if (!C.amr) {
+      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+      continue;
+    }
+    // level jumps: one launch per level, finest first, so the finer face
+    // fluxes a coarse block takes are stored before it runs
+    a.frole = C.frole; a.fquad = C.fquad; a.ff = (R*)C.ff;
+    for (const auto& grp : C.lgroups) {
+      a.blist = C.blist + grp.first;
+      dim3 gl(grid.x, grp.second);
+      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, gl, threads, smem, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+    }
   }
   C.cur = 1 - C.cur;
   ProfScope ps(3);
-  cudaError_t e = Launch<R, R>::ghost((R*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream);
+  cudaError_t e = ghost_fill<R>((R*)C.q[C.cur]);
   if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
   return 0;
 }
@@ -414,6 +447,8 @@ void amun_gpu_default_params(amun_params* p) {
   p->reconstruction = AMUN_REC_TVD;
   p->limiter = AMUN_LIM_MM;
   p->extrema_limiter = AMUN_LIM_MM;
+  p->prolongation_limiter = AMUN_LIM_MM;  // src/interpolations.F90:165
+  p->xblocks = p->yblocks = p->zblocks = 1;
   p->riemann = AMUN_RS_HLL;
   p->time_advance = AMUN_TA_RK2;
   p->stages = 2;
@@ -453,20 +488,25 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   } else if (k == "tolerance") p->tolerance = atof(v);
   else if (k == "pmin") p->pmin = atof(v);
   else if (k == "nr_maxit") p->nr_maxit = atoi(v);
+  else if (k == "xblocks") p->xblocks = atoi(v);
+  else if (k == "yblocks") p->yblocks = atoi(v);
+  else if (k == "zblocks") p->zblocks = atoi(v);
   else if (k == "nr_extra") p->nr_extra = atoi(v);
   else if (k == "state_variables") p->states_4vec = is_one_of(v, {"4vec", "4-vector", "4VEC", "4-VECTOR"});
   else if (k == "reconstruction") {
     if (is_one_of(v, {"tvd", "TVD"})) p->reconstruction = AMUN_REC_TVD;
     else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p->reconstruction = AMUN_REC_WENO5Z;
     else return fail(200, std::string("reconstruction not implemented: ") + v);
-  } else if (k == "limiter" || k == "extrema_limiter") {
+  } else if (k == "limiter" || k == "extrema_limiter" || k == "prolongation_limiter") {
     int l = AMUN_LIM_ZERO;
     if (is_one_of(v, {"mm", "minmod"})) l = AMUN_LIM_MM;
     else if (is_one_of(v, {"mc", "monotonized_central"})) l = AMUN_LIM_MC;
     else if (is_one_of(v, {"sb", "superbee"})) l = AMUN_LIM_SB;
     else if (is_one_of(v, {"vl", "vanleer"})) l = AMUN_LIM_VL;
     else if (k == "limiter" && is_one_of(v, {"va", "vanalbada"})) l = AMUN_LIM_VA;
-    if (k == "limiter") p->limiter = l; else p->extrema_limiter = l;
+    if (k == "limiter") p->limiter = l;
+    else if (k == "extrema_limiter") p->extrema_limiter = l;
+    else p->prolongation_limiter = l;
   } else if (k == "riemann_solver") {
     if (is_one_of(v, {"hllc", "HLLC"})) p->riemann = AMUN_RS_HLLC;
     else if (is_one_of(v, {"hlld", "HLLD"})) p->riemann = AMUN_RS_HLLD;
@@ -533,17 +573,188 @@ int amun_gpu_init(const amun_params* p) {
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Tables of a mesh with level jumps, from the block positions: the ghost
+// operations of every block, the role of every block face in the flux
+// correction, the finer blocks of every coarse face and the blocks ordered
+// finest level first.  The mesh must be 2:1 balanced across faces, edges and
+// corners (as the reference's refinement keeps it) and cover the periodic
+// domain; every ghost cell must find the block that covers it.
+int build_level_tables(int nblocks, const amun_block_desc* d) {
+  const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
+  if (2 * ng > nc) return fail(AMUN_E_UNSUPPORTED, "blocks at several levels need ncells >= 2 nghosts");
+  if (nc % 2) return fail(AMUN_E_UNSUPPORTED, "blocks at several levels need an even ncells");
+  const int base[3] = {C.p.xblocks, C.p.yblocks, nd == 3 ? C.p.zblocks : 1};
+  auto key = [](int l, int x, int y, int z) { return (((long long)l * 65536 + x) * 65536 + y) * 65536 + z; };
+  std::unordered_map<long long, int> where;
+  int maxl = 1;
+  for (int b = 0; b < nblocks; ++b) {
+    const int l = d[b].level;
+    if (l < 1 || l > 20) return fail(AMUN_E_BAD_ARGUMENT, "block level out of range");
+    for (int a = 0; a < nd; ++a)
+      if (d[b].coord[a] < 0 || d[b].coord[a] >= base[a] << (l - 1))
+        return fail(AMUN_E_BAD_ARGUMENT, "block position outside the domain at its level");
+    if (!where.emplace(key(l, d[b].coord[0], d[b].coord[1], nd == 3 ? d[b].coord[2] : 0), b).second)
+      return fail(AMUN_E_BAD_ARGUMENT, "two blocks at the same level and position");
+    maxl = std::max(maxl, l);
+  }
+  auto find = [&](int l, const int* c) -> int {
+    if (l < 1) return -1;
+    auto it = where.find(key(l, c[0] / nc, c[1] / nc, nd == 3 ? c[2] / nc : 0));
+    return it == where.end() ? -1 : it->second;
+  };
+  auto wrap = [&](int v, int l, int a) { const int n = (base[a] << (l - 1)) * nc; v %= n; return v < 0 ? v + n : v; };
+  const Geo& g = C.g;
+  auto cell = [&](const int* c) {  // padded linear index of global cell c inside its block
+    const int i = c[0] % nc + ng, j = c[1] % nc + ng, k = nd == 3 ? c[2] % nc + ng : 0;
+    return ((long long)k * g.JM + j) * g.IM + i;
+  };
+  std::vector<GhostOp> ops1, ops2;
+  std::vector<signed char> kind((size_t)nblocks * g.qvs, -1);  // op kind of every ghost cell
+  for (int b = 0; b < nblocks; ++b) {
+    const int L = d[b].level;
+    for (int k = 0; k < g.KM; ++k)
+      for (int j = 0; j < g.JM; ++j)
+        for (int i = 0; i < g.IM; ++i) {
+          const bool inside = i >= ng && i < ng + nc && j >= ng && j < ng + nc && (nd == 2 || (k >= ng && k < ng + nc));
+          if (inside) continue;
+          int c[3] = {wrap(d[b].coord[0] * nc + i - ng, L, 0), wrap(d[b].coord[1] * nc + j - ng, L, 1),
+                      nd == 3 ? wrap(d[b].coord[2] * nc + k - ng, L, 2) : 0};
+          GhostOp op;
+          op.dst = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
+          op.pad = 0;
+          int S = find(L, c);
+          if (S >= 0) {
+            op.src = (long long)S * g.qbs + cell(c); op.kind = 0;
+            ops1.push_back(op);
+          } else {
+            int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+            int Cb = find(L - 1, cc);
+            if (Cb >= 0) {
+              op.src = (long long)Cb * g.qbs + cell(cc);
+              op.kind = 2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2);
+              ops2.push_back(op);
+            } else {
+              int fc[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
+              int F = find(L + 1, fc);
+              if (F < 0) return fail(AMUN_E_UNSUPPORTED, "a ghost cell is covered by no block at its level or the "
+                                                         "next ones (mesh not 2:1 balanced, or a gap)");
+              op.src = (long long)F * g.qbs + cell(fc); op.kind = 1;
+              ops1.push_back(op);
+            }
+          }
+          kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op.kind & 3);
+        }
+  }
+  // a prolongation reads its coarse cell and the neighbours along each
+  // direction: none of them may be a prolonged ghost itself
+  const long long st[3] = {1, g.IM, (long long)g.IM * g.JM};
+  for (const GhostOp& op : ops2) {
+    const long long sb = op.src / g.qbs, sc = op.src - sb * g.qbs;  // block, padded cell
+    for (int a = 0; a < nd; ++a)
+      for (int sgn = -1; sgn <= 1; sgn += 2)
+        if (kind[(size_t)sb * g.qvs + (size_t)(sc + sgn * st[a])] == 2)
+          return fail(AMUN_E_UNSUPPORTED, "a prolongation would read a prolonged ghost (mesh not 2:1 balanced)");
+  }
+  // face roles and the finer blocks of coarse faces
+  std::vector<int> role((size_t)nblocks * 6, 0), quad((size_t)nblocks * 24, -1);
+  const int half = nc / 2;
+  for (int b = 0; b < nblocks; ++b) {
+    const int L = d[b].level;
+    for (int a = 0; a < nd; ++a) {
+      const int ta = a == 0 ? 1 : 0, tb = a == 2 ? 1 : 2;
+      for (int side = 0; side < 2; ++side) {
+        int c[3] = {d[b].coord[0] * nc, d[b].coord[1] * nc, nd == 3 ? d[b].coord[2] * nc : 0};
+        c[a] = wrap(side == 0 ? d[b].coord[a] * nc - 1 : (d[b].coord[a] + 1) * nc, L, a);
+        int r;
+        if (find(L, c) >= 0) {
+          r = 0;
+        } else {
+          int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+          if (find(L - 1, cc) >= 0) {
+            r = 1;
+          } else {
+            r = 2;
+            for (int qb = 0; qb < (nd == 3 ? 2 : 1); ++qb)
+              for (int qa = 0; qa < 2; ++qa) {
+                int fc[3];
+                fc[a] = wrap(side == 0 ? 2 * d[b].coord[a] * nc - 1 : 2 * (d[b].coord[a] + 1) * nc, L + 1, a);
+                fc[ta] = 2 * (d[b].coord[ta] * nc + qa * half);
+                if (nd == 3) fc[tb] = 2 * (d[b].coord[tb] * nc + qb * half);
+                else fc[2] = 0;
+                const int F = find(L + 1, fc);
+                if (F < 0) return fail(AMUN_E_UNSUPPORTED, "a block face borders no block (mesh not 2:1 balanced)");
+                quad[((size_t)b * 3 + a) * 2 * 4 + side * 4 + qa + 2 * qb] = F;
+              }
+          }
+        }
+        role[((size_t)b * 3 + a) * 2 + side] = r;
+      }
+    }
+  }
+  // blocks ordered finest level first
+  std::vector<int> order(nblocks);
+  for (int b = 0; b < nblocks; ++b) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return d[x].level > d[y].level; });
+  C.lgroups.clear();
+  for (int s0 = 0; s0 < nblocks;) {
+    int e = s0;
+    while (e < nblocks && d[order[e]].level == d[order[s0]].level) ++e;
+    C.lgroups.push_back({s0, e - s0});
+    s0 = e;
+  }
+  std::vector<GhostOp> all(ops1);
+  all.insert(all.end(), ops2.begin(), ops2.end());
+  C.nop1 = (long long)ops1.size();
+  C.nop2 = (long long)ops2.size();
+  const size_t NT = (size_t)nc * (nd == 3 ? nc : 1);
+  CK(cudaMalloc(&C.gop, std::max<size_t>(all.size(), 1) * sizeof(GhostOp)));
+  CK(cudaMalloc(&C.frole, role.size() * sizeof(int)));
+  CK(cudaMalloc(&C.fquad, quad.size() * sizeof(int)));
+  CK(cudaMalloc(&C.blist, order.size() * sizeof(int)));
+  CK(cudaMalloc(&C.ff, (size_t)nblocks * 6 * C.nv * NT * rsize()));
+  if (!all.empty()) CK(h2d(C.gop, all.data(), all.size() * sizeof(GhostOp)));
+  CK(h2d(C.frole, role.data(), role.size() * sizeof(int)));
+  CK(h2d(C.fquad, quad.data(), quad.size() * sizeof(int)));
+  CK(h2d(C.blist, order.data(), order.size() * sizeof(int)));
+  C.pool_bytes += (long long)(all.size() * sizeof(GhostOp) + (role.size() + quad.size() + order.size()) * sizeof(int) +
+                              (size_t)nblocks * 6 * C.nv * NT * rsize());
+  C.amr = true;
+  return 0;
+}
+
+// ghost fill of the current primitives (same-level copies, or the level
+// tables when the mesh has level jumps)
+template <typename R>
+cudaError_t ghost_fill(R* q) {
+  if (C.amr)
+    return Launch<R, R>::amr_ghost(q, C.gop, C.nop1, C.gop + C.nop1, C.nop2, C.g, C.nv, C.p.prolongation_limiter,
+                                   C.p.eps, C.stream);
+  return Launch<R, R>::ghost(q, C.nbr, C.g, C.nv, C.nblocks, C.stream);
+}
+
+}  // namespace
+
+extern "C" {
+
 int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   if (nblocks <= 0 || !blocks) return fail(AMUN_E_BAD_ARGUMENT, "empty block list");
-  for (int b = 0; b < nblocks; ++b) {
-    for (int n = 0; n < 27; ++n) {
-      if (C.p.ndims == 2 && n / 9 != 1) continue;  // no z neighbours in 2D
-      int nb = blocks[b].neighbor[n];
-      if (nb >= nblocks) return fail(AMUN_E_BAD_ARGUMENT, "neighbour index out of range");
-      if (nb >= 0 && blocks[nb].level != blocks[b].level)
-        return fail(AMUN_E_UNSUPPORTED, "neighbours at a different level are not supported");
-      if (nb < 0 && n != 13) return fail(AMUN_E_UNSUPPORTED, "non-periodic domain boundaries are not supported");
+  bool levels_differ = false;
+  for (int b = 1; b < nblocks; ++b) levels_differ |= blocks[b].level != blocks[0].level;
+  if (!levels_differ) {
+    for (int b = 0; b < nblocks; ++b) {
+      for (int n = 0; n < 27; ++n) {
+        if (C.p.ndims == 2 && n / 9 != 1) continue;  // no z neighbours in 2D
+        int nb = blocks[b].neighbor[n];
+        if (nb >= nblocks) return fail(AMUN_E_BAD_ARGUMENT, "neighbour index out of range");
+        if (nb >= 0 && blocks[nb].level != blocks[b].level)
+          return fail(AMUN_E_BAD_ARGUMENT, "a same-level neighbour at another level");
+        if (nb < 0 && n != 13) return fail(AMUN_E_UNSUPPORTED, "non-periodic domain boundaries are not supported");
+      }
     }
   }
   free_pool();
@@ -587,6 +798,10 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   CK(h2d(C.binv, binv.data(), binv.size() * sizeof(double)));
   C.cur = 0;
   C.ms_valid = false;
+  if (levels_differ) {
+    int r = build_level_tables(nblocks, blocks);
+    if (r) { free_pool(); return r; }
+  }
   return 0;
 }
 
@@ -672,8 +887,7 @@ int amun_gpu_download_blocks(int first, int count, double* u0, double* q) {
 int amun_gpu_boundary_variables(void) {
   int r = check_ready();
   if (r) return r;
-  cudaError_t e = bulk() ? Launch<float, float>::ghost((float*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream)
-                         : Launch<double, double>::ghost((double*)C.q[C.cur], C.nbr, C.g, C.nv, C.nblocks, C.stream);
+  cudaError_t e = bulk() ? ghost_fill<float>((float*)C.q[C.cur]) : ghost_fill<double>((double*)C.q[C.cur]);
   if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
   CK(cudaStreamSynchronize(C.stream));
   return 0;
@@ -1032,6 +1246,7 @@ int adj_supported() {
   if (C.p.fix_positivity || C.p.clip_extrema)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity and clip_extrema must be off");
   if (C.p.nghosts < 4) return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4");
+  if (C.amr) return fail(AMUN_E_UNSUPPORTED, "adjoint: meshes at one level only");
   return 0;
 }
 

@@ -10,6 +10,9 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t sweep(int eq, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
                            size_t smem, cudaStream_t s);
   static cudaError_t ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s);
+  // meshes with level jumps: copies and restrictions, then prolongations
+  static cudaError_t amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
+                               const Geo& g, int nv, int plim, double eps, cudaStream_t s);
   static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
                               cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
@@ -109,6 +112,15 @@ cudaError_t Launch<R, U1T>::ghost(R* q, const int* nbr, const Geo& g, int nv, in
   int threads = 256;
   dim3 grid(grid_for(per, threads, 4096), nblocks);
   ghost_copy_kernel<R><<<grid, threads, 0, s>>>(q, nbr, g, nv, per);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
+                                      const Geo& g, int nv, int plim, double eps, cudaStream_t s) {
+  const int threads = 256;
+  if (n1 > 0) amr_copy_restrict_kernel<R><<<grid_for(n1, threads), threads, 0, s>>>(q, ops1, n1, g, nv);
+  if (n2 > 0) amr_prolong_kernel<R><<<grid_for(n2, threads), threads, 0, s>>>(q, ops2, n2, g, nv, plim, R(eps));
   return cudaGetLastError();
 }
 

@@ -57,6 +57,7 @@ struct MethodConst {
   // relativistic recovery and 4-vector reconstruction
   double tol, pmin;
   int nrmax, nrext, states_4vec;
+  int plim;  // prolongation limiter (limiter_prol)
 };
 
 template <typename R> __device__ __forceinline__ Phys<R> make_phys(const MethodConst& m, double cmax, double cmax2) {
@@ -81,6 +82,14 @@ template <typename R, typename U1T> struct SweepArgs {
   StageDesc st;
   int LP, LW;          // tile: cells along the sweep, lanes across it
   int first, last;
+  // meshes with level jumps (all null on a one-level mesh):
+  const int* blist;    // the block of each grid row (one launch per level)
+  const int* frole;    // [b][dir][side]: 0 none; 1 store this face's fluxes
+                       // (the neighbour is coarser); 2 replace them by the
+                       // mean of the finer neighbours' stored fluxes
+  const int* fquad;    // [b][dir][side][4]: finer block of each quarter of
+                       // the face (transverse halves a + 2 b)
+  R* ff;               // [b][dir][side][v][transverse] stored face fluxes
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
@@ -124,7 +133,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
 
   const int nc = g.nc, ng = g.ng;
-  const int b = blockIdx.y;
+  const int b = a.blist ? a.blist[blockIdx.y] : (int)blockIdx.y;
   int tile = blockIdx.x;
   const int ntp = nc / LP, ntl = nc / LW;
   const int tp = tile % ntp; tile /= ntp;
@@ -260,6 +269,47 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   }
   __syncthreads();
 
+  // ---- block faces next to another level (boundary_fluxes,
+  // src/boundaries.F90:494-1087, block_update_flux 6539-6614): a block
+  // whose neighbour across the face is coarser stores its face fluxes; a
+  // block whose neighbours are finer takes the mean of theirs (stored by the
+  // launch of the finer level, which runs first), in the reference's pairing
+  if (a.frole) {
+    const int rlo = tp == 0 ? a.frole[(b * 3 + DIR) * 2 + 0] : 0;
+    const int rhi = tp == ntp - 1 ? a.frole[(b * 3 + DIR) * 2 + 1] : 0;
+    if (rlo | rhi) {
+      const long long NT = (long long)nc * (g.ndims == 3 ? nc : 1);
+      const int half = nc / 2;
+      const int tb = g.ndims == 3 ? th : 0;
+      for (int side = 0; side < 2; ++side) {
+        const int role = side ? rhi : rlo;
+        if (!role) continue;
+        const int pf = side ? LP : 0;
+        const int slab = (b * 3 + DIR) * 2 + side;
+        for (int t = threadIdx.x; t < LW * NV; t += blockDim.x) {
+          const int ll = t % LW, v = t / LW;
+          const int ta = l0 - ng + ll;
+          if (role == 1) {
+            a.ff[((long long)slab * NV + v) * NT + ta + (long long)nc * tb] = Fs[sidx(v, pf, ll, NPI)];
+          } else {
+            const int fb = a.fquad[slab * 4 + ta / half + 2 * (tb / half)];
+            const int fa = 2 * (ta % half), fbb = 2 * (tb % half);
+            const R* F = a.ff + ((long long)((fb * 3 + DIR) * 2 + (1 - side)) * NV + v) * NT;
+            R val;
+            if (g.ndims == 2) {
+              val = (F[fa] + F[fa + 1]) / R(2);
+            } else {
+              val = ((F[fa + (long long)nc * fbb] + F[fa + 1 + (long long)nc * (fbb + 1)]) +
+                     (F[fa + (long long)nc * (fbb + 1)] + F[fa + 1 + (long long)nc * fbb])) / R(4);
+            }
+            Fs[sidx(v, pf, ll, NPI)] = val;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+
   // ---- flux difference, stage combination -------------------------------------
   const double* bi = a.binv + 3 * b;
   const R dsi = R(bi[DIR]);
@@ -394,6 +444,92 @@ __global__ void ghost_copy_kernel(R* q, const int* nbr, Geo g, int nv, long long
     long long dst = (long long)b * g.qbs + ((long long)k * JM + j) * IM + i;
     long long src = (long long)nb * g.qbs + ((long long)(k - oz * nc) * JM + (j - oy * nc)) * IM + (i - ox * nc);
     for (int v = 0; v < nv; ++v) q[dst + v * g.qvs] = q[src + v * g.qvs];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ghost fill on meshes with level jumps (boundary_variables,
+// src/boundaries.F90:372-479): one operation per ghost cell, built on the
+// host from the block positions.  dst/src are (block * qbs + padded cell);
+// kind & 3: 0 copy of a same-level cell (boundaries_*_copy), 1 mean of the
+// 2^d finer cells whose lower corner is src (block_*_restrict,
+// src/boundaries.F90:5637-6070, same pairing), 2 prolongation of the coarser
+// cell src (block_*_prolong, 6071-6450); kind >> 2: the child (bit d set for
+// the upper half along d).  Copies and restrictions run first; the
+// prolongations read the coarser blocks' cells and ghosts after them.
+struct GhostOp {
+  long long dst, src;
+  int kind, pad;
+};
+
+template <typename R>
+__global__ void amr_copy_restrict_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv) {
+  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const GhostOp op = ops[t];
+    for (int v = 0; v < nv; ++v) {
+      const R* s = q + op.src + v * g.qvs;
+      R val;
+      if ((op.kind & 3) == 0) {
+        val = s[0];
+      } else if (g.ndims == 2) {
+        val = R(0.25) * ((s[0] + s[sX + sY]) + (s[sY] + s[sX]));
+      } else {
+        val = R(0.125) * (((s[0] + s[sX + sY + sZ]) + (s[sZ] + s[sX + sY])) +
+                          ((s[sY + sZ] + s[sX]) + (s[sY] + s[sX + sZ])));
+      }
+      q[op.dst + v * g.qvs] = val;
+    }
+  }
+}
+
+template <typename R>
+__global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv, int plim,
+                                   R eps) {
+  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const GhostOp op = ops[t];
+    const int bits = op.kind >> 2;
+    const int sx = bits & 1, sy = (bits >> 1) & 1, sz = (bits >> 2) & 1;
+    for (int v = 0; v < nv; ++v) {
+      const R* c = q + op.src + v * g.qvs;
+      const R q0 = c[0];
+      R d0 = limiter<R>(plim, R(0.5), q0 - c[-sX], c[sX] - q0, eps);
+      R d1 = limiter<R>(plim, R(0.5), q0 - c[-sY], c[sY] - q0, eps);
+      R d2 = g.ndims == 3 ? limiter<R>(plim, R(0.5), q0 - c[-sZ], c[sZ] - q0, eps) : R(0);
+      if (v == 0 || v == nv - 1) {  // density and pressure
+        if (q0 > R(0)) {
+          for (int it = 0; it < 4096; ++it) {
+            R sa = d_fabs(d0) + d_fabs(d1);
+            if (g.ndims == 3) sa = sa + d_fabs(d2);
+            if (!(q0 <= sa)) break;
+            d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
+          }
+        } else {
+          d0 = d1 = d2 = R(0);
+        }
+      }
+      d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
+      R val;
+      if (g.ndims == 2) {
+        const R dq1 = d0 + d1, dq2 = d0 - d1;
+        const int ch = sx + 2 * sy;
+        val = ch == 0 ? q0 - dq1 : (ch == 1 ? q0 + dq2 : (ch == 2 ? q0 - dq2 : q0 + dq1));
+      } else {
+        const R dq1 = d0 + d1 + d2, dq2 = d0 - d1 - d2, dq3 = d0 - d1 + d2, dq4 = d0 + d1 - d2;
+        switch (sx + 2 * sy + 4 * sz) {
+          case 0: val = q0 - dq1; break;
+          case 1: val = q0 + dq2; break;
+          case 2: val = q0 - dq3; break;
+          case 3: val = q0 + dq4; break;
+          case 4: val = q0 - dq4; break;
+          case 5: val = q0 + dq3; break;
+          case 6: val = q0 - dq2; break;
+          default: val = q0 + dq1; break;
+        }
+      }
+      q[op.dst + v * g.qvs] = val;
+    }
   }
 }
 

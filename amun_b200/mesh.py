@@ -57,6 +57,7 @@ class UniformMesh:
             d = arr[b]
             d.level = self.level
             d.dx[0], d.dx[1], d.dx[2] = self.dx, self.dy, self.dz
+            d.coord[0], d.coord[1], d.coord[2] = bx, by, bz
             for oz in (-1, 0, 1):
                 for oy in (-1, 0, 1):
                     for ox in (-1, 0, 1):

@@ -20,13 +20,17 @@ from .params import geometry, to_native
 
 
 class Simulation:
-    def __init__(self, params: dict, precision: str = "fp64"):
+    """`mesh`: None for the uniform mesh the parameters describe, or an
+    amun_b200.amr.AMRMesh (blocks at several levels; the state is then set
+    and read as block arrays)."""
+
+    def __init__(self, params: dict, precision: str = "fp64", mesh=None):
         self.params = dict(params)
         self.params["precision"] = precision
         self.L = N.lib()
         self.native = to_native(self.params)
         self.geo = geometry(self.params)
-        self.mesh = UniformMesh(self.geo)
+        self.mesh = UniformMesh(self.geo) if mesh is None else mesh
         self.nv = 5 if self.native.eqsys == N.AMUN_EQ_HD else 9
         N.check(self.L.amun_gpu_init(C.byref(self.native)))
         self._desc = self.mesh.descriptors()
@@ -38,6 +42,15 @@ class Simulation:
         block arrays get periodic ghosts, u0 = prim2cons(q) (as
         setup_problem does), both are uploaded and ghosts refreshed."""
         qb = np.ascontiguousarray(self.mesh.to_blocks(np.asarray(q, dtype=np.float64)))
+        ub = self.prim2cons(qb)
+        self.upload_blocks(ub, qb)
+        N.check(self.L.amun_gpu_boundary_variables())
+        N.check(self.L.amun_gpu_set_time(0.0, 0.0))
+
+    def set_primitive_blocks(self, qb: np.ndarray):
+        """Set the state from block arrays of primitives (nblocks, km, jm, im,
+        nv), ghost entries ignored: u0 = prim2cons(q), upload, ghost fill."""
+        qb = np.ascontiguousarray(qb, dtype=np.float64)
         ub = self.prim2cons(qb)
         self.upload_blocks(ub, qb)
         N.check(self.L.amun_gpu_boundary_variables())

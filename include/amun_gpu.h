@@ -75,6 +75,9 @@ typedef struct amun_params {
   int nr_maxit;         /*                        "nr_maxit"                  */
   int nr_extra;         /*                        "nr_extra"                  */
   int states_4vec;      /* 0/1                    "state_variables" = "4vec"  */
+  int prolongation_limiter; /* AMUN_LIM_*         "prolongation_limiter"      */
+  int xblocks, yblocks, zblocks; /* level-1 block grid "xblocks" ... (periodic
+                           extent of every level on meshes with level jumps) */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block
@@ -84,7 +87,11 @@ typedef struct amun_block_desc {
   double dx[3];         /* adx/ady/adz of the level (src/coordinates.F90:339) */
   int neighbor[27];     /* index of the same-level neighbour block in direction
                            (ox,oy,oz) at [(ox+1) + 3(oy+1) + 9(oz+1)], -1 when
-                           there is none (non-periodic domain edge)           */
+                           there is none (a neighbour at another level, or a
+                           non-periodic domain edge)                          */
+  int coord[3];         /* position at its level, in blocks, zero based (the
+                           meta block's level coordinates); a mesh whose blocks
+                           are at several levels is connected from these      */
 } amun_block_desc;
 
 typedef struct amun_status {
