@@ -65,30 +65,20 @@ def blast(mesh, nv: int, gamma: float, dens=1.0, ratio=100.0, radius=0.1, csnd=0
     for (kk, jj, ii) in idx:
         a_xl, a_xu, a_yl, a_yu = xl[kk, jj, ii], xu[kk, jj, ii], yl[kk, jj, ii], yu[kk, jj, ii]
         if mesh.ndims == 3:
+            # sub-cells fully inside count 1, cut ones 1/2 (src/problems.F90:
+            # 620-657); counted at once rather than accumulated one by one
             a_zl = zl[kk, jj, ii]
             n = max(1, int(nsubgrid))
             fm = (np.arange(n) * 1.0) / n
             fp = (np.arange(1, n + 1) * 1.0) / n
-            xm, ym, zm = fm * dx, fm * dy, fm * dz
-            xp, yp, zp = fp * dx, fp * dy, fp * dz
-            fc_inc = dvol / n ** 3
-            acc = 0.0
-            for kc in range(n):
-                zb = (a_zl + zm[kc]) ** 2
-                zt = (a_zl + zp[kc]) ** 2
-                for jc in range(n):
-                    yb = (a_yl + ym[jc]) ** 2
-                    yt = (a_yl + yp[jc]) ** 2
-                    xb = (a_xl + xm) ** 2
-                    xt = (a_xl + xp) ** 2
-                    full = (xt + yt + zt) <= r2
-                    half = (~full) & ((xb + yb + zb) < r2)
-                    for ic in range(n):
-                        if full[ic]:
-                            acc = acc + fc_inc
-                        elif half[ic]:
-                            acc = acc + 0.5 * fc_inc
-            f = acc
+            xb, xt = (a_xl + fm * dx) ** 2, (a_xl + fp * dx) ** 2
+            yb, yt = (a_yl + fm * dy) ** 2, (a_yl + fp * dy) ** 2
+            zb, zt = (a_zl + fm * dz) ** 2, (a_zl + fp * dz) ** 2
+            top = zt[:, None, None] + yt[None, :, None] + xt[None, None, :]
+            bot = zb[:, None, None] + yb[None, :, None] + xb[None, None, :]
+            full = top <= r2
+            half = (~full) & (bot < r2)
+            f = (dvol / n ** 3) * (np.count_nonzero(full) + 0.5 * np.count_nonzero(half))
         else:
             rlu = a_xl * a_xl + a_yu * a_yu
             rul = a_xu * a_xu + a_yl * a_yl

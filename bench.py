@@ -219,6 +219,46 @@ def adjoint_timing(torch, prec):
             "grad_rho_l2": float(np.sqrt(np.sum(out["g"][0][..., 0] ** 2)))}
 
 
+AMR_WORKLOAD = dict(ndims=3, equation_system="mhd", equation_of_state="adi", reconstruction="tvd", limiter="mc",
+                    riemann_solver="hlld", time_advance="rk2", cfl=0.4, gamma=GAMMA, nghosts=4, ncells=16,
+                    xblocks=4, yblocks=4, zblocks=4, minlev=1, maxlev=4, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5,
+                    zmin=-0.5, zmax=0.5)
+
+
+def amr_mesh():
+    """The AMR blast mesh: 4^3 level-1 blocks of 16^3 cells, refined to level
+    4 wherever a block comes within 0.2 of the centre (2:1 balanced): 3424
+    leaves at levels 2-4, 14.0 M cells."""
+    from amun_b200.amr import AMRMesh
+    from amun_b200.params import geometry
+    m = AMRMesh(geometry(AMR_WORKLOAD))
+    m.refine_where(lambda lo, hi, level: float(np.linalg.norm(np.clip(0.0, lo, hi))) < 0.2)
+    return m
+
+
+def amr_timing(torch, prec, steps=10, warmup=3):
+    """3D MHD AMR blast (ratio 1000, p_amb 0.1, B = (1,1,0)/sqrt(2), 10
+    sub-cells per edge cell), TVD-MC, HLLD, SSPRK(2,2): zone-updates/s over
+    all leaf cells, graph-replayed steps timed with CUDA events."""
+    from amun_b200 import problems
+    from amun_b200.solver import Simulation
+    mesh = amr_mesh()
+    qb = mesh.blocks_from(lambda v: problems.blast(v, NV, GAMMA, dens=1.0, ratio=1000.0, radius=0.1,
+                                                   csnd=math.sqrt(GAMMA * 0.1), buni=1.0, angle=45.0,
+                                                   nsubgrid=10), NV)
+    sim = Simulation(AMR_WORKLOAD, precision=prec, mesh=mesh)
+    sim.L.amun_gpu_set_stream(torch.cuda.current_stream().cuda_stream)
+    sim.set_primitive_blocks(qb)
+    ms = timed_run(sim, torch, steps, warmup, 1.0e30)
+    lv = mesh.levels()
+    out = {"value": mesh.ncells_total * steps / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
+           "steps": steps, "leaves": int(mesh.nblocks), "cells": int(mesh.ncells_total),
+           "leaves_per_level": {int(l): int((lv == l).sum()) for l in np.unique(lv)},
+           "device_bytes": sim.status()["device_bytes"]}
+    sim.close()
+    return out
+
+
 def cpu_baseline(threads: int, steps: int = 1):
     """The oracle (FP64 C++ restatement of the reference) on the host cores:
     a 64^3 sample of the same scheme (64 blocks of 16^3, block-parallel
@@ -380,6 +420,13 @@ def main():
            "h2d_bytes_per_step": 2 * bytes_per_array, "d2h_bytes_per_step": 2 * bytes_per_array,
            "ms_per_step": e2e_ms}
 
+    amr = {}
+    for prec in ("fp64", "fp32"):
+        try:
+            amr[prec] = amr_timing(torch, prec)
+        except Exception as exc:  # pragma: no cover
+            amr[prec] = {"error": str(exc)}
+
     adjoint = {}
     for prec in ("fp64", "fp32"):
         try:
@@ -429,6 +476,9 @@ def main():
             "accuracy_vs_fp64": accuracy,
             "kernel_profile_fp32": r32["profile"], "kernel_profile_fp64": r64["profile"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "amr_blast3d": {"workload": "mhd3d AMR blast, 4^3 level-1 blocks of 16^3 cells, levels 1-4, "
+                                        "tvd-mc hlld ssprk(2,2) cfl0.4, ratio 1000",
+                            "fp64": amr["fp64"], "fp32": amr["fp32"]},
             "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
                                     "J = kinetic energy in [0,0.25]^2, dJ/drho0",
                         "fp64": adjoint["fp64"], "fp32": adjoint["fp32"]},
