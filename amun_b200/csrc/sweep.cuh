@@ -335,30 +335,26 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     // stage combination (all cells updated by this stage are interior)
     const double dt = a.sc->dt;
     const double ds = a.st.dscoef * dt;
-    double un[NV];
+    double un[NV], Av[NV], Bv[NV];
+    // all operands are loaded before the first store, so the loads issue
+    // together instead of waiting behind stores that might alias them
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const long long o = ci + v * g.uvs;
-      double A = a.st.a_src == 0 ? a.u0[o] : (double)a.u1[o];
+      Av[v] = a.st.a_src == 0 ? a.u0[o] : (double)a.u1[o];
+      Bv[v] = a.st.form == 0 ? 0.0 : (a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o]);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const long long o = ci + v * g.uvs;
+      const double A = Av[v], B = Bv[v];
       double dd = (double)dloc[v];
       double r;
       switch (a.st.form) {
         case 0: r = A + ds * dd; break;
-        case 1: {
-          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
-          r = (a.st.ca * A + a.st.cb * B) + ds * dd;
-          break;
-        }
-        case 2: {
-          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
-          r = 0.5 * ((A + B) + ds * dd);
-          break;
-        }
-        default: {
-          double B = a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o];
-          r = a.st.ca * A + a.st.cb * (B + ds * dd);
-          break;
-        }
+        case 1: r = (a.st.ca * A + a.st.cb * B) + ds * dd; break;
+        case 2: r = 0.5 * ((A + B) + ds * dd); break;
+        default: r = a.st.ca * A + a.st.cb * (B + ds * dd); break;
       }
       if constexpr (V::MHD) {
         if (a.st.final_stage && v == V::BP) r = a.m.decay * r;
