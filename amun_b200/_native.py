@@ -91,6 +91,7 @@ def lib():
         "amun_gpu_adjoint": (i, [_D, _D, _D]),
         "amun_gpu_adjoint_bytes": (i, [C.POINTER(C.c_longlong)]),
         "amun_gpu_adjoint_timing": (i, [_D, _D]),
+        "amun_gpu_autotune": (i, [i, C.POINTER(C.c_int), C.POINTER(C.c_int), _D]),
         "amun_gpu_finalize": (None, []),
         "amun_gpu_last_error": (C.c_char_p, []),
     }

@@ -74,6 +74,8 @@ struct Ctx {
   int* blist = nullptr;      // blocks ordered finest level first
   void* ff = nullptr;        // stored face fluxes
   std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
+  // sweep tile chosen by amun_gpu_autotune (0: the default shape)
+  int tile_LP = 0, tile_LW = 0;
 };
 
 Ctx C;
@@ -205,6 +207,7 @@ void free_pool() {
   for (void* x : amrp)
     if (x) cudaFree(x);
   C.gop = nullptr; C.frole = C.fquad = C.blist = nullptr; C.ff = nullptr;
+  C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   if (C.u0) cudaFree(C.u0);
   if (C.u1) cudaFree(C.u1);
@@ -286,6 +289,11 @@ Schedule schedule() {
 
 // tile shape of the sweep kernels: LP cells along the sweep, LW lanes
 void tile_shape(int& LP, int& LW) {
+  if (C.tile_LP > 0 && C.g.nc % C.tile_LP == 0 && C.g.nc % C.tile_LW == 0) {
+    LP = C.tile_LP;
+    LW = C.tile_LW;
+    return;
+  }
   int nc = C.g.nc;
   LP = 1;
   for (int d = 32; d >= 1; --d)
@@ -1491,6 +1499,81 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
   // leave the recorded final state on the device
   if ((r = restore_state(A.nseg))) return r;
   CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_autotune(int reps, int* best_lp, int* best_lw, double* best_ms) {
+  int r = check_ready();
+  if (r) return r;
+  if (reps < 1) reps = 1;
+  const int nc = C.g.nc;
+  // candidates: LP cells along the sweep x LW lanes, both dividing ncells,
+  // at most 288 threads ((LP + 2) LW) and 200 KB of shared memory
+  std::vector<std::pair<int, int>> cand;
+  const int RR = C.p.reconstruction == AMUN_REC_WENO5Z ? 2 : 1;
+  for (int lp = 4; lp <= nc && lp <= 128; lp *= 2) {
+    if (nc % lp) continue;
+    std::vector<int> lws;
+    for (int lw = 1; lw <= nc; ++lw)
+      if (nc % lw == 0 && (lp + 2) * lw <= 288) lws.push_back(lw);
+    if (lws.empty()) continue;
+    const int big = lws.back();
+    for (int lw : lws) {
+      if (lw != big && 2 * lw != big && 4 * lw != big) continue;
+      const size_t smem = (size_t)C.nv * ((lp + 2 * RR + 2) + 2 * (lp + 2)) * lw * rsize();
+      if (smem <= 200 * 1024) cand.push_back({lp, lw});
+    }
+  }
+  if (cand.empty()) return fail(AMUN_E_UNSUPPORTED, "autotune: no tile shape fits");
+  // the state is put back after every trial
+  const size_t ub = (size_t)C.g.ubs * C.nblocks * sizeof(double), qb = (size_t)C.g.qbs * C.nblocks * rsize();
+  DevBuf su, sq, ss;
+  CK(cudaMalloc(&su.p, ub));
+  CK(cudaMalloc(&sq.p, qb));
+  CK(cudaMalloc(&ss.p, sizeof(DevScalars)));
+  if ((r = ensure_maxspeed())) return r;
+  const int cur0 = C.cur;
+  CK(cudaMemcpyAsync(su.p, C.u0, ub, cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(sq.p, C.q[cur0], qb, cudaMemcpyDeviceToDevice, C.stream));
+  CK(cudaMemcpyAsync(ss.p, C.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
+  auto restore = [&]() -> int {
+    C.cur = cur0;
+    CK(cudaMemcpyAsync(C.u0, su.p, ub, cudaMemcpyDeviceToDevice, C.stream));
+    CK(cudaMemcpyAsync(C.q[cur0], sq.p, qb, cudaMemcpyDeviceToDevice, C.stream));
+    CK(cudaMemcpyAsync(C.sc, ss.p, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
+    return 0;
+  };
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  int blp = 0, blw = 0;
+  for (const auto& c : cand) {
+    C.tile_LP = c.first;
+    C.tile_LW = c.second;
+    if ((r = step_launches(1.0e30)) || (r = restore())) break;  // warm-up
+    cudaEventRecord(e0, C.stream);
+    for (int n = 0; n < reps && !r; ++n) r = step_launches(1.0e30);
+    cudaEventRecord(e1, C.stream);
+    if (r || (r = restore())) break;
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / reps < best) { best = ms / reps; blp = c.first; blw = c.second; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  C.tile_LP = blp;
+  C.tile_LW = blw;
+  // captured step graphs hold the old tile
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  if (r) return r;
+  if (best_lp) *best_lp = blp;
+  if (best_lw) *best_lw = blw;
+  if (best_ms) *best_ms = best;
   return 0;
 }
 

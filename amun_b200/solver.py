@@ -101,6 +101,13 @@ class Simulation:
     def run(self, nsteps: int, dtnext: float, graph: bool = True):
         N.check(self.L.amun_gpu_run(int(nsteps), dtnext, 1 if graph else 0))
 
+    def autotune(self, reps: int = 3):
+        """Time every sweep tile shape that fits over `reps` steps and keep
+        the fastest (the state is restored); returns (LP, LW, ms per step)."""
+        lp, lw, ms = C.c_int(), C.c_int(), C.c_double()
+        N.check(self.L.amun_gpu_autotune(int(reps), C.byref(lp), C.byref(lw), C.byref(ms)))
+        return lp.value, lw.value, ms.value
+
     def boundary_variables(self):
         N.check(self.L.amun_gpu_boundary_variables())
 

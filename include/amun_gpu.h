@@ -232,6 +232,14 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0);
 /* device bytes held by the recording and the adjoint work arrays */
 int amun_gpu_adjoint_bytes(long long* bytes);
 
+/* The sweep tile (LP cells along the sweep x LW lanes across it) picked by
+ * timing: every tile shape that fits is timed over `reps` steps of the
+ * configured scheme on the current mesh (CUDA events, eager launches) and the
+ * fastest is kept for later steps; the device state is restored after every
+ * trial.  No counterpart in the reference (its loops have no tile).  Returns
+ * the chosen shape and its time per step. */
+int amun_gpu_autotune(int reps, int* best_lp, int* best_lw, double* best_ms);
+
 /* device time of the last amun_gpu_adjoint: segment recomputation (forward
  * steps from the checkpoints) and reverse sweep (the adjoint kernels) */
 int amun_gpu_adjoint_timing(double* recompute_ms, double* reverse_ms);
