@@ -66,6 +66,7 @@ def lib():
         "amun_gpu_set_blocks": (i, [i, C.POINTER(amun_block_desc)]),
         "amun_gpu_upload": (i, [i, _D, _D, _D]),
         "amun_gpu_upload_blocks": (i, [i, i, _D, _D]),
+        "amun_gpu_upload_conserved": (i, [i, i, _D]),
         "amun_gpu_download": (i, [i, _D, _D, _D]),
         "amun_gpu_download_blocks": (i, [i, i, _D, _D]),
         "amun_gpu_boundary_variables": (i, []),

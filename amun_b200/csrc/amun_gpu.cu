@@ -850,6 +850,22 @@ int amun_gpu_upload_blocks(int first, int count, const double* u0, const double*
   return upload_range(first, count, u0, nullptr, q);
 }
 
+int amun_gpu_upload_conserved(int first, int count, const double* u0) {
+  if (!u0) return fail(AMUN_E_BAD_ARGUMENT, "null array");
+  int r = upload_range(first, count, u0, nullptr, nullptr);
+  if (r) return r;
+  cudaError_t e = bulk() ? Launch<float, float>::cons2prim_blocks(C.p.eqsys, C.u0, (float*)C.q[C.cur], C.g,
+                                                                  method_const(), C.sc, first, count, C.stream)
+                         : Launch<double, double>::cons2prim_blocks(C.p.eqsys, C.u0, (double*)C.q[C.cur], C.g,
+                                                                    method_const(), C.sc, first, count, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cons2prim");
+  e = bulk() ? ghost_fill<float>((float*)C.q[C.cur]) : ghost_fill<double>((double*)C.q[C.cur]);
+  if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  C.ms_valid = false;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
 static int download_range(int first, int count, double* u0, double* u1, double* q) {
   int r = check_ready();
   if (r) return r;

@@ -16,6 +16,8 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
                               cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
+  static cudaError_t cons2prim_blocks(int eq, const double* u0, R* q, const Geo& g, const MethodConst& m,
+                                      DevScalars* sc, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_u0(const double* fu, double* u0, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_u1(const double* fu, U1T* u1, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
@@ -112,6 +114,17 @@ cudaError_t Launch<R, U1T>::ghost(R* q, const int* nbr, const Geo& g, int nv, in
   int threads = 256;
   dim3 grid(grid_for(per, threads, 4096), nblocks);
   ghost_copy_kernel<R><<<grid, threads, 0, s>>>(q, nbr, g, nv, per);
+  return cudaGetLastError();
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::cons2prim_blocks(int eq, const double* u0, R* q, const Geo& g, const MethodConst& m,
+                                             DevScalars* sc, int b0, int nb, cudaStream_t s) {
+  const int threads = 256;
+  const int grid = grid_for(g.uvs * nb, threads);
+  if (eq == EQ_HD) cons2prim_blocks_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
+  else if (eq == EQ_MHD) cons2prim_blocks_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
+  else cons2prim_blocks_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   return cudaGetLastError();
 }
 

@@ -616,6 +616,36 @@ __global__ void download_q_kernel(const R* q, double* fq, Geo g, int nv, int b0,
 // u (Fortran layout, all cells): interior from the state array, ghosts from
 // prim2cons of the ghost primitives (update_ghost_cells,
 // src/boundaries.F90:6633-6736)
+// update_primitive_variables (src/equations.F90:1088-1148) on the interior
+// cells of blocks b0 .. b0+nb-1: Q = cons2prim(U0).  A failed relativistic
+// recovery keeps the cell's previous primitive state with p = 0
+// (src/equations.F90:4749-4777) and is counted.
+template <int EQ, typename R>
+__global__ void cons2prim_blocks_kernel(const double* u0, R* q, Geo g, MethodConst m, DevScalars* sc, int b0, int nb) {
+  constexpr int NV = Var<EQ>::NV;
+  const long long total = g.uvs * nb;
+  const Phys<double> Pd = make_phys<double>(m, 0.0, 0.0);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const long long bb = t / g.uvs, ic = t - bb * g.uvs;
+    const int ii = (int)(ic % g.nc), jj = (int)((ic / g.nc) % g.nc);
+    const int kk = g.ndims == 3 ? (int)(ic / ((long long)g.nc * g.nc)) : 0;
+    const long long c = (b0 + bb) * g.qbs +
+                        ((long long)(g.ndims == 3 ? kk + g.ng : 0) * g.JM + (jj + g.ng)) * g.IM + (ii + g.ng);
+    double uc[NV], qc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) uc[v] = u0[(b0 + bb) * g.ubs + v * g.uvs + ic];
+    if constexpr (Var<EQ>::SR) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qc[v] = (double)q[c + v * g.qvs];
+      if (!cons2prim_sr(uc, qc, Pd)) atomicAdd(&sc->c2p_failures, 1ull);
+    } else {
+      cons2prim<EQ>(uc, qc, Pd);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) q[c + v * g.qvs] = (R)qc[v];
+  }
+}
+
 template <int EQ, typename R, typename UT>
 __global__ void download_u_kernel(const UT* u, const R* q, double* fu, Geo g, MethodConst m, int b0, int nb) {
   constexpr int NV = Var<EQ>::NV;

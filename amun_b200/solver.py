@@ -64,6 +64,23 @@ class Simulation:
             raise ValueError(f"expected block arrays of shape {shp}")
         N.check(self.L.amun_gpu_upload_blocks(0, self.mesh.nblocks, N.dptr(u0), N.dptr(q)))
 
+    def upload_conserved(self, u0: np.ndarray):
+        """Upload conserved block arrays only; the primitives and ghost cells
+        are rebuilt on the device (update_variables)."""
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        if u0.shape != shp:
+            raise ValueError(f"expected block arrays of shape {shp}")
+        N.check(self.L.amun_gpu_upload_conserved(0, self.mesh.nblocks, N.dptr(u0)))
+
+    def download_conserved(self, u0: np.ndarray):
+        """Download conserved block arrays only (ghost cells rebuilt from Q)."""
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
+        if u0.shape != shp or u0.dtype != np.float64 or not u0.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"expected a C-contiguous float64 block array of shape {shp}")
+        N.check(self.L.amun_gpu_download_blocks(0, self.mesh.nblocks, N.dptr(u0), None))
+        return u0
+
     def download_blocks(self, u0: np.ndarray | None = None, q: np.ndarray | None = None):
         shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
         if u0 is None:

@@ -392,9 +392,10 @@ def main():
     accuracy = {"steps": acc_steps, "l1_density_rel": l1, "linf_density_rel": linf,
                 "energy_drift_rel": (en32 - en64) / en64, "mass_drift_rel": (mass32 - mass64) / mass64}
 
-    # e2e through the C ABI with host arrays: each step uploads u0 and q of
-    # every block (Fortran layout, pinned host memory), advances one step and
-    # downloads u0 and q, as a caller that owns the arrays does.
+    # e2e through the C ABI with host arrays: each step uploads the conserved
+    # block arrays (Fortran layout, pinned host memory; the primitives and
+    # ghosts are rebuilt on the device), advances one step and downloads the
+    # conserved arrays, as a caller that owns U does.
     sim = Simulation(WORKLOAD, precision="fp32")
     stream = torch.cuda.current_stream()
     sim.L.amun_gpu_set_stream(stream.cuda_stream)
@@ -406,23 +407,23 @@ def main():
     uh[...] = sim.prim2cons(qh)
     e2e_steps = max(3, min(args.steps, 10))
     for _ in range(2):
-        sim.upload_blocks(uh, qh)
+        sim.upload_conserved(uh)
         sim.advance(dtnext)
-        sim.download_blocks(uh, qh)
+        sim.download_conserved(uh)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
     for _ in range(e2e_steps):
-        sim.upload_blocks(uh, qh)
+        sim.upload_conserved(uh)
         sim.advance(dtnext)
-        sim.download_blocks(uh, qh)
+        sim.download_conserved(uh)
     b.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(a.elapsed_time(b)) / e2e_steps
     sim.close()
     bytes_per_array = int(np.prod(shp)) * 8
     e2e = {"value": ws * NCELL / (e2e_ms * 1e-3), "unit": "zone-updates/s",
-           "h2d_bytes_per_step": 2 * bytes_per_array, "d2h_bytes_per_step": 2 * bytes_per_array,
+           "h2d_bytes_per_step": bytes_per_array, "d2h_bytes_per_step": bytes_per_array,
            "ms_per_step": e2e_ms}
 
     amr = {}

@@ -128,6 +128,13 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks);
 int amun_gpu_upload(int block, const double* u0, const double* u1, const double* q);
 /* Same for `count` consecutive blocks stored back to back. */
 int amun_gpu_upload_blocks(int first, int count, const double* u0, const double* q);
+
+/* Conserved state only, for a caller that keeps U and derives Q from it:
+ * u0 of blocks first .. first+count-1 (Fortran layout, ghost entries
+ * ignored) is uploaded, then update_variables (src/evolution.F90:1994-2094)
+ * runs on the device: Q = cons2prim(U) in the interior and the ghost fill of
+ * every block.  Half the host traffic of amun_gpu_upload_blocks. */
+int amun_gpu_upload_conserved(int first, int count, const double* u0);
 /* Copy one block's arrays device -> host (any pointer may be NULL).  Ghost
  * cells of u0 and u1 are prim2cons of the ghost primitives
  * (update_ghost_cells, src/boundaries.F90:6633). */
