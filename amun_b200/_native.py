@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libamun_gpu.so")
 
 AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD = 0, 1, 2
+AMUN_EOS_ADI, AMUN_EOS_ISO = 0, 1
 AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
 AMUN_FP64, AMUN_FP32_BULK = 0, 1
 
@@ -32,7 +33,8 @@ class amun_params(C.Structure):
         ("nghosts", C.c_int), ("gamma", C.c_double), ("cfl", C.c_double), ("alpha", C.c_double),
         ("eps", C.c_double), ("tolerance", C.c_double), ("pmin", C.c_double), ("nr_maxit", C.c_int),
         ("nr_extra", C.c_int), ("states_4vec", C.c_int), ("prolongation_limiter", C.c_int),
-        ("xblocks", C.c_int), ("yblocks", C.c_int), ("zblocks", C.c_int),
+        ("xblocks", C.c_int), ("yblocks", C.c_int), ("zblocks", C.c_int), ("eos", C.c_int),
+        ("csnd", C.c_double),
     ]
 
 

@@ -310,6 +310,7 @@ MethodConst method_const() {
   m.lim = C.p.limiter; m.clim = C.p.extrema_limiter; m.positivity = C.p.fix_positivity; m.clip = C.p.clip_extrema;
   m.tol = C.p.tolerance; m.pmin = C.p.pmin; m.nrmax = C.p.nr_maxit; m.nrext = C.p.nr_extra;
   m.plim = C.p.prolongation_limiter;
+  m.csnd = C.p.csnd;
   m.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
   return m;
 }
@@ -319,6 +320,8 @@ int effective_solver() {
   int rs = C.p.riemann;
   if (C.p.eqsys == AMUN_EQ_HD && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
   if (C.p.eqsys == AMUN_EQ_SRMHD && rs != AMUN_RS_HLLC) rs = AMUN_RS_HLL;
+  if (rs == AMUN_RS_HLLDM) rs = AMUN_RS_HLL;  // HLLD-M exists for isothermal MHD only
+  if (C.p.eqsys == EQ_HD_ISO || C.p.eqsys == EQ_MHD_ISO) rs = AMUN_RS_HLL;
   return rs;
 }
 
@@ -394,10 +397,10 @@ int evolve_launches() { return bulk() ? launch_evolve<float>() : launch_evolve<d
 int ensure_maxspeed() {
   if (C.ms_valid) return 0;
   CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
-  cudaError_t e = bulk() ? Launch<float, float>::maxspeed(C.p.eqsys, (const float*)C.q[C.cur], C.g, C.gamma, C.sc,
-                                                          C.nblocks, C.stream)
+  cudaError_t e = bulk() ? Launch<float, float>::maxspeed(C.p.eqsys, (const float*)C.q[C.cur], C.g, C.gamma,
+                                                          C.p.csnd, C.sc, C.nblocks, C.stream)
                          : Launch<double, double>::maxspeed(C.p.eqsys, (const double*)C.q[C.cur], C.g, C.gamma,
-                                                            C.sc, C.nblocks, C.stream);
+                                                            C.p.csnd, C.sc, C.nblocks, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
   C.ms_valid = true;
   return 0;
@@ -434,7 +437,7 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.tol = C.p.tolerance; u.pmin = C.p.pmin; u.nrmax = C.p.nr_maxit; u.nrext = C.p.nr_extra;
   u.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
-  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax;
+  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd;
   return u;
 }
 
@@ -474,6 +477,8 @@ void amun_gpu_default_params(amun_params* p) {
   p->nr_maxit = 100;
   p->nr_extra = 2;
   p->states_4vec = 0;
+  p->eos = AMUN_EOS_ADI;
+  p->csnd = 1.0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -488,8 +493,9 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"srmhd", "SRMHD"})) p->eqsys = AMUN_EQ_SRMHD;
     else return fail(100, std::string("equation system not implemented: ") + v);
   } else if (k == "equation_of_state") {
-    if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"}))
-      return fail(110, std::string("equation of state not implemented: ") + v);
+    if (is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) p->eos = AMUN_EOS_ADI;
+    else if (is_one_of(v, {"iso", "ISO", "isothermal", "ISOTHERMAL"})) p->eos = AMUN_EOS_ISO;
+    else return fail(110, std::string("equation of state not implemented: ") + v);
   } else if (k == "primitive_solver") {
     if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"}))
       return fail(AMUN_E_UNSUPPORTED, std::string("primitive solver not implemented here: ") + v);
@@ -519,6 +525,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     if (is_one_of(v, {"hllc", "HLLC"})) p->riemann = AMUN_RS_HLLC;
     else if (is_one_of(v, {"hlld", "HLLD"})) p->riemann = AMUN_RS_HLLD;
     else if (is_one_of(v, {"roe", "ROE"})) p->riemann = AMUN_RS_ROE;
+    else if (is_one_of(v, {"hlldm", "hlld-m", "HLLDM", "HLLD-M"})) p->riemann = AMUN_RS_HLLDM;
     else p->riemann = AMUN_RS_HLL;
   } else if (k == "time_advance") {
     if (is_one_of(v, {"euler", "EULER"})) p->time_advance = AMUN_TA_EULER;
@@ -537,6 +544,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   } else if (k == "ncells") p->ncells = atoi(v);
   else if (k == "nghosts") p->nghosts = atoi(v);
   else if (k == "gamma") p->gamma = atof(v);
+  else if (k == "csnd") p->csnd = atof(v);
   else if (k == "cfl") p->cfl = atof(v);
   else if (k == "alpha") p->alpha = atof(v);
   else if (k == "eps") p->eps = atof(v);
@@ -548,6 +556,15 @@ int amun_gpu_init(const amun_params* p) {
   if (p->ndims != 2 && p->ndims != 3) return fail(AMUN_E_BAD_ARGUMENT, "ndims must be 2 or 3");
   if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD && p->eqsys != AMUN_EQ_SRMHD)
     return fail(100, "equation system not implemented");
+  if (p->eos != AMUN_EOS_ADI && p->eos != AMUN_EOS_ISO) return fail(110, "equation of state not implemented");
+  if (p->eos == AMUN_EOS_ISO) {
+    // src/schemes.F90:159-300: the relativistic system is adiabatic only;
+    // of the isothermal solvers this library carries HLL (the default)
+    if (p->eqsys == AMUN_EQ_SRMHD) return fail(110, "the relativistic system has no isothermal equation of state");
+    if (p->riemann == AMUN_RS_ROE || (p->eqsys == AMUN_EQ_MHD && (p->riemann == AMUN_RS_HLLD ||
+                                                                   p->riemann == AMUN_RS_HLLDM)))
+      return fail(AMUN_E_UNSUPPORTED, "isothermal systems: HLL Riemann solver only");
+  }
   if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
     return fail(200, "reconstruction not implemented");
   int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;
@@ -563,6 +580,11 @@ int amun_gpu_init(const amun_params* p) {
   CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
   C.nv = p->eqsys == AMUN_EQ_HD ? 5 : 9;
+  if (p->eos == AMUN_EOS_ISO) {
+    // kernels take the isothermal systems as systems of their own
+    C.p.eqsys = p->eqsys == AMUN_EQ_HD ? EQ_HD_ISO : EQ_MHD_ISO;
+    C.nv -= 1;
+  }
   C.gamma = p->gamma;
   C.gammam1 = C.gamma - 1.0;
   C.gammam1i = 1.0 / C.gammam1;
@@ -736,11 +758,14 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
 
 // ghost fill of the current primitives (same-level copies, or the level
 // tables when the mesh has level jumps)
+// pressure variable (last) of the adiabatic systems; none when isothermal
+int pressure_index() { return (C.p.eqsys == EQ_HD_ISO || C.p.eqsys == EQ_MHD_ISO) ? -1 : C.nv - 1; }
+
 template <typename R>
 cudaError_t ghost_fill(R* q) {
   if (C.amr)
-    return Launch<R, R>::amr_ghost(q, C.gop, C.nop1, C.gop + C.nop1, C.nop2, C.g, C.nv, C.p.prolongation_limiter,
-                                   C.p.eps, C.stream);
+    return Launch<R, R>::amr_ghost(q, C.gop, C.nop1, C.gop + C.nop1, C.nop2, C.g, C.nv, pressure_index(),
+                                   C.p.prolongation_limiter, C.p.eps, C.stream);
   return Launch<R, R>::ghost(q, C.nbr, C.g, C.nv, C.nblocks, C.stream);
 }
 

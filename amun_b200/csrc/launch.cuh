@@ -12,9 +12,9 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s);
   // meshes with level jumps: copies and restrictions, then prolongations
   static cudaError_t amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
-                               const Geo& g, int nv, int plim, double eps, cudaStream_t s);
-  static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
-                              cudaStream_t s);
+                               const Geo& g, int nv, int ipr, int plim, double eps, cudaStream_t s);
+  static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, double csnd, DevScalars* sc,
+                              int nblocks, cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
   static cudaError_t cons2prim_blocks(int eq, const double* u0, R* q, const Geo& g, const MethodConst& m,
                                       DevScalars* sc, int b0, int nb, cudaStream_t s);
@@ -81,11 +81,15 @@ static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
       case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
       default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
-  } else {
+  } else if constexpr (EQ == EQ_SRMHD) {
     switch (rs) {
       case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
       default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
+  } else {
+    // isothermal systems: HLL (riemann_hd_iso_hll, riemann_mhd_iso_hll)
+    (void)rs;
+    return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
   }
 }
 
@@ -103,6 +107,8 @@ cudaError_t Launch<R, U1T>::sweep(int eq, int rec, int rs, int dir, const SweepA
                                   int threads, size_t smem, cudaStream_t s) {
   if (eq == EQ_HD) return sweep_eq<R, U1T, EQ_HD>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_MHD) return sweep_eq<R, U1T, EQ_MHD>(rec, rs, dir, a, grid, threads, smem, s);
+  if (eq == EQ_HD_ISO) return sweep_eq<R, U1T, EQ_HD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
+  if (eq == EQ_MHD_ISO) return sweep_eq<R, U1T, EQ_MHD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
   return sweep_eq<R, U1T, EQ_SRMHD>(rec, rs, dir, a, grid, threads, smem, s);
 }
 
@@ -124,28 +130,32 @@ cudaError_t Launch<R, U1T>::cons2prim_blocks(int eq, const double* u0, R* q, con
   const int grid = grid_for(g.uvs * nb, threads);
   if (eq == EQ_HD) cons2prim_blocks_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else if (eq == EQ_MHD) cons2prim_blocks_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
+  else if (eq == EQ_HD_ISO) cons2prim_blocks_kernel<EQ_HD_ISO, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
+  else if (eq == EQ_MHD_ISO) cons2prim_blocks_kernel<EQ_MHD_ISO, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else cons2prim_blocks_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   return cudaGetLastError();
 }
 
 template <typename R, typename U1T>
 cudaError_t Launch<R, U1T>::amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
-                                      const Geo& g, int nv, int plim, double eps, cudaStream_t s) {
+                                      const Geo& g, int nv, int ipr, int plim, double eps, cudaStream_t s) {
   const int threads = 256;
   if (n1 > 0) amr_copy_restrict_kernel<R><<<grid_for(n1, threads), threads, 0, s>>>(q, ops1, n1, g, nv);
-  if (n2 > 0) amr_prolong_kernel<R><<<grid_for(n2, threads), threads, 0, s>>>(q, ops2, n2, g, nv, plim, R(eps));
+  if (n2 > 0) amr_prolong_kernel<R><<<grid_for(n2, threads), threads, 0, s>>>(q, ops2, n2, g, nv, ipr, plim, R(eps));
   return cudaGetLastError();
 }
 
 template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::maxspeed(int eq, const R* q, const Geo& g, double gamma, DevScalars* sc, int nblocks,
-                                     cudaStream_t s) {
+cudaError_t Launch<R, U1T>::maxspeed(int eq, const R* q, const Geo& g, double gamma, double csnd, DevScalars* sc,
+                                     int nblocks, cudaStream_t s) {
   long long n = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1) * nblocks;
   int threads = 256;
   int grid = grid_for(n, threads);
-  if (eq == EQ_HD) maxspeed_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
-  else if (eq == EQ_MHD) maxspeed_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
-  else maxspeed_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(q, g, gamma, sc, nblocks);
+  if (eq == EQ_HD) maxspeed_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
+  else if (eq == EQ_MHD) maxspeed_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
+  else if (eq == EQ_HD_ISO) maxspeed_kernel<EQ_HD_ISO, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
+  else if (eq == EQ_MHD_ISO) maxspeed_kernel<EQ_MHD_ISO, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
+  else maxspeed_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   return cudaGetLastError();
 }
 
@@ -190,6 +200,8 @@ static cudaError_t download_u_any(int eq, const UT* u, const R* q, double* fu, c
   int grid = grid_for(n, 256);
   if (eq == EQ_HD) download_u_kernel<EQ_HD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else if (eq == EQ_MHD) download_u_kernel<EQ_MHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
+  else if (eq == EQ_HD_ISO) download_u_kernel<EQ_HD_ISO, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
+  else if (eq == EQ_MHD_ISO) download_u_kernel<EQ_MHD_ISO, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else download_u_kernel<EQ_SRMHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   return cudaGetLastError();
 }

@@ -4,9 +4,10 @@
 // procedure with the same operation order, so the FP64 build (compiled with
 // -fmad=false) reproduces the reference arithmetic bit for bit.
 //
-// Variable order (src/equations.F90:335-485), 0-based here:
+// Variable order (src/equations.F90:322-485), 0-based here:
 //   HD  (NV=5): dens, velx, vely, velz, pres
 //   MHD (NV=9): dens, velx, vely, velz, magx, magy, magz, bpsi, pres
+//   isothermal HD (NV=4) and MHD (NV=8): the same without pres
 // Conserved variables use the same slots (momenta, energy in the pres slot).
 #pragma once
 #include <cstdint>
@@ -17,25 +18,37 @@ enum { LIM_ZERO = 0, LIM_MM = 1, LIM_MC = 2, LIM_SB = 3, LIM_VL = 4, LIM_VA = 5 
 enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_ROE = 3 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 
-// equation systems (src/equations.F90:322-833)
-enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2 };
+// equation systems (src/equations.F90:322-833); *_ISO: isothermal equation
+// of state (p = csnd^2 rho, no energy equation)
+enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_HD_ISO = 3, EQ_MHD_ISO = 4 };
 
 template <int EQ> struct Var;
 template <> struct Var<EQ_HD> {
   static constexpr int NV = 5;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, PR = 4, EN = 4;
   static constexpr int BX = -1, BY = -1, BZ = -1, BP = -1;
-  static constexpr bool MHD = false, SR = false;
+  static constexpr bool MHD = false, SR = false, ISO = false;
 };
 template <> struct Var<EQ_MHD> {
   static constexpr int NV = 9;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
-  static constexpr bool MHD = true, SR = false;
+  static constexpr bool MHD = true, SR = false, ISO = false;
 };
 template <> struct Var<EQ_SRMHD> {
   static constexpr int NV = 9;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
-  static constexpr bool MHD = true, SR = true;
+  static constexpr bool MHD = true, SR = true, ISO = false;
+};
+template <> struct Var<EQ_HD_ISO> {
+  static constexpr int NV = 4;
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, PR = -1, EN = -1;
+  static constexpr int BX = -1, BY = -1, BZ = -1, BP = -1;
+  static constexpr bool MHD = false, SR = false, ISO = true;
+};
+template <> struct Var<EQ_MHD_ISO> {
+  static constexpr int NV = 8;
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = -1, EN = -1;
+  static constexpr bool MHD = true, SR = false, ISO = true;
 };
 
 // Equation and method constants in the working precision R.
@@ -43,6 +56,7 @@ template <typename R> struct Phys {
   R gamma, gammam1, gammam1i, gammaxi;
   R eps;      // reconstruction epsilon (WENO-Z, van Albada)
   R cmax, cmax2;
+  R csnd, csnd2;  // isothermal sound speed (src/equations.F90:847-851)
   int lim, clim;
   // relativistic recovery: tolerance, pmin, nr_maxit, nr_extra
   // (src/equations.F90:184-201, 313-318)
@@ -99,6 +113,15 @@ __device__ __forceinline__ void prim2cons(const R* q, R* u, const Phys<R>& P) {
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
   if constexpr (V::SR) { prim2cons_sr(q, u, P); return; }
+  if constexpr (V::ISO) {
+    // prim2cons_hd_iso src/equations.F90:1360-1403, prim2cons_mhd_iso 2220-2267
+    u[V::DN] = q[V::DN];
+    u[V::VX] = q[V::DN] * q[V::VX];
+    u[V::VY] = q[V::DN] * q[V::VY];
+    u[V::VZ] = q[V::DN] * q[V::VZ];
+    if constexpr (V::MHD) { u[V::BX] = q[V::BX]; u[V::BY] = q[V::BY]; u[V::BZ] = q[V::BZ]; u[V::BP] = q[V::BP]; }
+    return;
+  }
   u[V::DN] = q[V::DN];
   u[V::VX] = q[V::DN] * q[V::VX];
   u[V::VY] = q[V::DN] * q[V::VY];
@@ -126,6 +149,15 @@ __device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
     cons2prim_sr(u, q, P);
     return;
   }
+  if constexpr (V::ISO) {
+    // cons2prim_hd_iso src/equations.F90:1421-1464, cons2prim_mhd_iso 2285-2332
+    q[V::DN] = u[V::DN];
+    q[V::VX] = u[V::VX] / u[V::DN];
+    q[V::VY] = u[V::VY] / u[V::DN];
+    q[V::VZ] = u[V::VZ] / u[V::DN];
+    if constexpr (V::MHD) { q[V::BX] = u[V::BX]; q[V::BY] = u[V::BY]; q[V::BZ] = u[V::BZ]; q[V::BP] = u[V::BP]; }
+    return;
+  }
   q[V::DN] = u[V::DN];
   q[V::VX] = u[V::VX] / u[V::DN];
   q[V::VY] = u[V::VY] / u[V::DN];
@@ -150,6 +182,47 @@ __device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
   if constexpr (V::SR) { fluxspeed_sr<SPEEDS>(q, u, f, cm, cp, P); return; }
+  if constexpr (V::ISO && !V::MHD) {
+    // fluxspeed_hd_iso src/equations.F90:1484-1542
+    f[V::DN] = u[V::VX];
+    f[V::VX] = q[V::VX] * u[V::VX];
+    f[V::VY] = q[V::VX] * u[V::VY];
+    f[V::VZ] = q[V::VX] * u[V::VZ];
+    f[V::VX] = f[V::VX] + P.csnd2 * q[V::DN];
+    if constexpr (SPEEDS) {
+      cm = q[V::VX] - P.csnd;
+      cp = q[V::VX] + P.csnd;
+    }
+    return;
+  }
+  if constexpr (V::ISO) {
+    // fluxspeed_mhd_iso src/equations.F90:2352-2435
+    R bx2 = q[V::BX] * q[V::BX];
+    R by2 = q[V::BY] * q[V::BY];
+    R bz2 = q[V::BZ] * q[V::BZ];
+    R bb = bx2 + by2 + bz2;
+    R pt = P.csnd2 * q[V::DN] + R(0.5) * bb;
+    f[V::DN] = u[V::VX];
+    f[V::VX] = q[V::VX] * u[V::VX] - bx2;
+    f[V::VY] = q[V::VX] * u[V::VY] - q[V::BX] * q[V::BY];
+    f[V::VZ] = q[V::VX] * u[V::VZ] - q[V::BX] * q[V::BZ];
+    f[V::VX] = f[V::VX] + pt;
+    f[V::BX] = q[V::BP];
+    f[V::BY] = q[V::VX] * q[V::BY] - q[V::BX] * q[V::VY];
+    f[V::BZ] = q[V::VX] * q[V::BZ] - q[V::BX] * q[V::VZ];
+    f[V::BP] = P.cmax2 * q[V::BX];
+    if constexpr (SPEEDS) {
+      R fa = P.csnd2 * q[V::DN];
+      R fb = fa + bb;
+      R fc = fb * fb - R(4) * fa * bx2;
+      R cf;
+      if (fc > R(0)) cf = d_sqrt(R(0.5) * (fb + d_sqrt(fc)) / q[V::DN]);
+      else cf = d_sqrt(R(0.5) * fb / q[V::DN]);
+      cm = q[V::VX] - cf;
+      cp = q[V::VX] + cf;
+    }
+    return;
+  }
   if constexpr (!V::MHD) {
     f[V::DN] = u[V::VX];
     f[V::VX] = q[V::VX] * u[V::VX];
@@ -195,7 +268,7 @@ __device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R
 // maxspeed_hd_adi src/equations.F90:1974-2044 / maxspeed_mhd_adi 3060-3131,
 // the per-cell term |v| + c
 template <int EQ, typename R>
-__device__ __forceinline__ double cell_speed(const R* q, double gamma) {
+__device__ __forceinline__ double cell_speed(const R* q, double gamma, double csnd) {
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
   if constexpr (V::SR) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
@@ -203,7 +276,14 @@ __device__ __forceinline__ double cell_speed(const R* q, double gamma) {
   double vv = vx * vx + vy * vy + vz * vz;
   double v = sqrt(vv);
   double c;
-  if constexpr (!V::MHD) {
+  if constexpr (V::ISO && !V::MHD) {
+    c = csnd;  // maxspeed_hd_iso src/equations.F90:1558-1624
+  } else if constexpr (V::ISO) {
+    // maxspeed_mhd_iso src/equations.F90:2450-2521: sqrt(csnd2 + |B|^2 / rho)
+    double bx = q[V::BX], by = q[V::BY], bz = q[V::BZ];
+    double bb = bx * bx + by * by + bz * bz;
+    c = sqrt(csnd * csnd + bb / (double)q[V::DN]);
+  } else if constexpr (!V::MHD) {
     c = sqrt(gamma * (double)q[V::PR] / (double)q[V::DN]);
   } else {
     double bx = q[V::BX], by = q[V::BY], bz = q[V::BZ];

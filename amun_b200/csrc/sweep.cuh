@@ -58,12 +58,14 @@ struct MethodConst {
   double tol, pmin;
   int nrmax, nrext, states_4vec;
   int plim;  // prolongation limiter (limiter_prol)
+  double csnd;  // isothermal sound speed
 };
 
 template <typename R> __device__ __forceinline__ Phys<R> make_phys(const MethodConst& m, double cmax, double cmax2) {
   Phys<R> P;
   P.gamma = R(m.gamma); P.gammam1 = R(m.gammam1); P.gammam1i = R(m.gammam1i); P.gammaxi = R(m.gammaxi);
   P.eps = R(m.eps); P.cmax = R(cmax); P.cmax2 = R(cmax2);
+  P.csnd = R(m.csnd); P.csnd2 = R(m.csnd * m.csnd);
   P.lim = m.lim; P.clim = m.clim;
   P.tol = m.tol; P.pmin = m.pmin; P.nrmax = m.nrmax; P.nrext = m.nrext;
   return P;
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     R qs[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) { qs[v] = (R)qn[v]; a.qout[co + v * g.qvs] = qs[v]; }
-    if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma));
+    if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma, a.m.csnd));
   }
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
 }
@@ -480,8 +482,8 @@ __global__ void amr_copy_restrict_kernel(R* q, const GhostOp* __restrict__ ops, 
 }
 
 template <typename R>
-__global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv, int plim,
-                                   R eps) {
+__global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv, int ipr,
+                                   int plim, R eps) {
   const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const GhostOp op = ops[t];
@@ -493,7 +495,7 @@ __global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long l
       R d0 = limiter<R>(plim, R(0.5), q0 - c[-sX], c[sX] - q0, eps);
       R d1 = limiter<R>(plim, R(0.5), q0 - c[-sY], c[sY] - q0, eps);
       R d2 = g.ndims == 3 ? limiter<R>(plim, R(0.5), q0 - c[-sZ], c[sZ] - q0, eps) : R(0);
-      if (v == 0 || v == nv - 1) {  // density and pressure
+      if (v == 0 || v == ipr) {  // density and pressure (ipr < 0: isothermal)
         if (q0 > R(0)) {
           for (int it = 0; it < 4096; ++it) {
             R sa = d_fabs(d0) + d_fabs(d1);
@@ -532,7 +534,7 @@ __global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long l
 // max over interior cells of |v|+c (maxspeed_*, src/equations.F90:1974,
 // 3060), accumulated into sc->ms_bits
 template <int EQ, typename R>
-__global__ void maxspeed_kernel(const R* q, Geo g, double gamma, DevScalars* sc, int nblocks) {
+__global__ void maxspeed_kernel(const R* q, Geo g, double gamma, double csnd, DevScalars* sc, int nblocks) {
   const long long ncell = (long long)g.nc * g.nc * (g.ndims == 3 ? g.nc : 1);
   const long long total = ncell * nblocks;
   double vmax = 0.0;
@@ -544,7 +546,7 @@ __global__ void maxspeed_kernel(const R* q, Geo g, double gamma, DevScalars* sc,
     R qc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = q[o + v * g.qvs];
-    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma));
+    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma, csnd));
   }
   block_max_atomic(vmax, &sc->ms_bits);
 }

@@ -9,7 +9,7 @@ namespace amun {
 struct UnitArgs {
   int nv, eq, ndims, im, jm, km, ng;
   int rec, lim, clim, rs, clip, positivity;
-  double gamma, gammaxi, eps, cmax;
+  double gamma, gammaxi, eps, cmax, csnd;
   double tol, pmin;
   int nrmax, nrext, states_4vec;
 };

@@ -217,7 +217,7 @@ __global__ void pointwise(int op, int n, const double* a, const double* b, doubl
 }
 
 template <int EQ>
-__global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsigned long long* out) {
+__global__ void block_maxspeed(const double* q, BlockDims d, double gamma, double csnd, unsigned long long* out) {
   constexpr int NV = Var<EQ>::NV;
   const int nx = d.im - 2 * d.ng, ny = d.jm - 2 * d.ng, nz = d.ndims == 3 ? d.km - 2 * d.ng : 1;
   const long long n = (long long)nx * ny * nz;
@@ -228,7 +228,7 @@ __global__ void block_maxspeed(const double* q, BlockDims d, double gamma, unsig
     long long c = i + (long long)d.im * (j + (long long)d.jm * k);
     double qc[NV];
     for (int v = 0; v < NV; ++v) qc[v] = q[c * NV + v];
-    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma));
+    vmax = fmax(vmax, cell_speed<EQ>(qc, gamma, csnd));
   }
   unsigned mask = 0xffffffffu;
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(mask, vmax, o));
@@ -263,6 +263,7 @@ static Phys<double> unit_phys(const UnitArgs& u) {
   P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0); P.gammaxi = u.gammaxi;
   P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax; P.lim = u.lim; P.clim = u.clim;
   P.tol = u.tol; P.pmin = u.pmin; P.nrmax = u.nrmax; P.nrext = u.nrext;
+  P.csnd = u.csnd; P.csnd2 = u.csnd * u.csnd;
   return P;
 }
 
@@ -311,8 +312,10 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
       case RS_ROE: return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
       default: return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
     }
-  } else {
+  } else if constexpr (EQ == EQ_SRMHD) {
     if (u.rs == RS_HLLC) return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
+    return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
+  } else {
     return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
   }
 }
@@ -321,6 +324,8 @@ cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, doub
                             unsigned long long* nonpos, cudaStream_t s) {
   if (u.eq == EQ_HD) return block_flux_eq<EQ_HD>(u, q, qs, f, scratch, nonpos, s);
   if (u.eq == EQ_MHD) return block_flux_eq<EQ_MHD>(u, q, qs, f, scratch, nonpos, s);
+  if (u.eq == EQ_HD_ISO) return block_flux_eq<EQ_HD_ISO>(u, q, qs, f, scratch, nonpos, s);
+  if (u.eq == EQ_MHD_ISO) return block_flux_eq<EQ_MHD_ISO>(u, q, qs, f, scratch, nonpos, s);
   return block_flux_eq<EQ_SRMHD>(u, q, qs, f, scratch, nonpos, s);
 }
 
@@ -349,6 +354,10 @@ cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const doubl
       case RS_ROE: line_riemann<EQ_MHD, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
       default: line_riemann<EQ_MHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
     }
+  } else if (u.eq == EQ_HD_ISO) {
+    line_riemann<EQ_HD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+  } else if (u.eq == EQ_MHD_ISO) {
+    line_riemann<EQ_MHD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   } else {
     if (u.rs == RS_HLLC) line_riemann<EQ_SRMHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
     else line_riemann<EQ_SRMHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
@@ -363,6 +372,8 @@ cudaError_t unit_pointwise(const UnitArgs& u, int op, int n, const double* a, co
   if (grid < 1) grid = 1;
   if (u.eq == EQ_HD) pointwise<EQ_HD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else if (u.eq == EQ_MHD) pointwise<EQ_MHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else if (u.eq == EQ_HD_ISO) pointwise<EQ_HD_ISO><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else if (u.eq == EQ_MHD_ISO) pointwise<EQ_MHD_ISO><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else pointwise<EQ_SRMHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   return cudaGetLastError();
 }
@@ -372,9 +383,11 @@ cudaError_t unit_maxspeed(const UnitArgs& u, const double* q, unsigned long long
   long long n = (long long)(u.im - 2 * u.ng) * (u.jm - 2 * u.ng) * (u.ndims == 3 ? u.km - 2 * u.ng : 1);
   int grid = (int)((n + 255) / 256);
   if (grid > 4096) grid = 4096;
-  if (u.eq == EQ_HD) block_maxspeed<EQ_HD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
-  else if (u.eq == EQ_MHD) block_maxspeed<EQ_MHD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
-  else block_maxspeed<EQ_SRMHD><<<grid, 256, 0, s>>>(q, d, u.gamma, out);
+  if (u.eq == EQ_HD) block_maxspeed<EQ_HD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
+  else if (u.eq == EQ_MHD) block_maxspeed<EQ_MHD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
+  else if (u.eq == EQ_HD_ISO) block_maxspeed<EQ_HD_ISO><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
+  else if (u.eq == EQ_MHD_ISO) block_maxspeed<EQ_MHD_ISO><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
+  else block_maxspeed<EQ_SRMHD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   return cudaGetLastError();
 }
 

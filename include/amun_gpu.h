@@ -34,13 +34,14 @@ extern "C" {
 
 /* equation_system / equation_of_state (src/equations.F90:322-833) */
 enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2 };
+enum { AMUN_EOS_ADI = 0, AMUN_EOS_ISO = 1 };
 /* reconstruction (src/interpolations.F90:226-382) */
 enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
 /* limiter / extrema_limiter (src/interpolations.F90:389-445) */
 enum { AMUN_LIM_ZERO = 0, AMUN_LIM_MM = 1, AMUN_LIM_MC = 2, AMUN_LIM_SB = 3,
        AMUN_LIM_VL = 4, AMUN_LIM_VA = 5 };
 /* riemann_solver (src/schemes.F90:159-503) */
-enum { AMUN_RS_HLL = 0, AMUN_RS_HLLC = 1, AMUN_RS_HLLD = 2, AMUN_RS_ROE = 3 };
+enum { AMUN_RS_HLL = 0, AMUN_RS_HLLC = 1, AMUN_RS_HLLD = 2, AMUN_RS_ROE = 3, AMUN_RS_HLLDM = 4 };
 /* time_advance (src/evolution.F90:164-209) */
 enum { AMUN_TA_EULER = 0, AMUN_TA_RK2 = 1, AMUN_TA_SSPRK2 = 2, AMUN_TA_RK3 = 3,
        AMUN_TA_SSPRK34 = 4, AMUN_TA_SSPRK35 = 5 };
@@ -78,6 +79,9 @@ typedef struct amun_params {
   int prolongation_limiter; /* AMUN_LIM_*         "prolongation_limiter"      */
   int xblocks, yblocks, zblocks; /* level-1 block grid "xblocks" ... (periodic
                            extent of every level on meshes with level jumps) */
+  int eos;              /* AMUN_EOS_*             "equation_of_state"         */
+  double csnd;          /*                        "csnd" (isothermal sound
+                           speed, src/equations.F90:176, 847-851)            */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block

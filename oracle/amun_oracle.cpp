@@ -42,7 +42,7 @@ namespace {
 enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
-enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE };
+enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
 
 struct Params {
@@ -55,6 +55,8 @@ struct Params {
   int stages = 2;
   bool positivity = false, clip = false, mlp = false;
   double gamma = 5.0 / 3.0;
+  bool iso = false;     // isothermal equation of state (src/equations.F90:322-485)
+  double csnd = 1.0;    // isothermal sound speed (src/equations.F90:176, 847)
   double cfl = 0.5, alpha = 2.0;
   double eps = DBL_EPSILON;
   int ncells = 8, nghosts = 2;
@@ -90,7 +92,9 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"srmhd", "SRMHD"})) p.eqsys = EQ_SRMHD;
     else return 100;  // src/equations.F90:830
   } else if (key == "equation_of_state") {
-    if (!is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) return 110;
+    if (is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) p.iso = false;
+    else if (is_one_of(v, {"iso", "ISO", "isothermal", "ISOTHERMAL"})) p.iso = true;
+    else return 110;
   } else if (key == "primitive_solver") {
     // only the 1D(W) Newton recovery is restated (src/equations.F90:5665-5788)
     if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"})) return 110;
@@ -116,6 +120,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     if (is_one_of(v, {"hllc", "HLLC"})) p.rs = RS_HLLC;
     else if (is_one_of(v, {"hlld", "HLLD"})) p.rs = RS_HLLD;
     else if (is_one_of(v, {"roe", "ROE"})) p.rs = RS_ROE;
+    else if (is_one_of(v, {"hlldm", "hlld-m", "HLLDM", "HLLD-M"})) p.rs = RS_HLLDM;
     else p.rs = RS_HLL;
   } else if (key == "time_advance") {
     if (is_one_of(v, {"euler", "EULER"})) p.ta = TA_EULER;
@@ -130,6 +135,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "clip_extrema") p.clip = is_on(v);
   else if (key == "mlp_limiting") p.mlp = is_on(v);
   else if (key == "gamma") p.gamma = atof(v.c_str());
+  else if (key == "csnd") p.csnd = atof(v.c_str());
   else if (key == "cfl") p.cfl = atof(v.c_str());
   else if (key == "alpha") p.alpha = atof(v.c_str());
   else if (key == "eps") p.eps = atof(v.c_str());
@@ -417,6 +423,8 @@ struct Oracle {
   int nv = 5, idn = 1, ivx = 2, ivy = 3, ivz = 4, imx = 2, imy = 3, imz = 4;
   int ibx = -1, iby = -1, ibz = -1, ibp = -1, ipr = 5, ien = 5;
   double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5, gammaxi = 0.4;
+  double csnd = 1.0, csnd2 = 1.0;  // src/equations.F90:847-851
+  bool iso = false;
   double cmax = 0.0, cmax2 = 0.0;
   mutable std::atomic<long> c2p_failures{0};  // failed relativistic recoveries (p set to 0)
   // evolution (src/evolution.F90:60-90)
@@ -477,6 +485,17 @@ struct Oracle {
       nv = 9; idn = 1; ivx = 2; ivy = 3; ivz = 4; imx = 2; imy = 3; imz = 4;
       ibx = 5; iby = 6; ibz = 7; ibp = 8; ipr = ien = 9;
     }
+    // isothermal: no energy equation, ipr = ien = 0 (src/equations.F90:335-392)
+    iso = p.iso;
+    if (iso) {
+      if (p.eqsys == EQ_SRMHD) return 110;
+      nv -= 1; ipr = ien = 0;
+      // of the isothermal solvers (src/schemes.F90:159-300) HLL is restated
+      if (p.rs == RS_ROE || (p.eqsys == EQ_MHD && (p.rs == RS_HLLD || p.rs == RS_HLLDM))) return 904;
+      p.rs = RS_HLL;
+    }
+    csnd = p.csnd; csnd2 = csnd * csnd;
+    if (p.rs == RS_HLLDM) p.rs = RS_HLL;  // HLLD-M exists for isothermal MHD only
     if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
     // SRMHD offers HLL and HLLC only (src/schemes.F90:472-498)
     if (p.eqsys == EQ_SRMHD && p.rs != RS_HLLC) p.rs = RS_HLL;
@@ -819,7 +838,12 @@ struct Oracle {
       U[imx - 1] = Q[idn - 1] * Q[ivx - 1];
       U[imy - 1] = Q[idn - 1] * Q[ivy - 1];
       U[imz - 1] = Q[idn - 1] * Q[ivz - 1];
-      if (p.eqsys == EQ_HD) {
+      if (iso) {
+        // prim2cons_hd_iso src/equations.F90:1360-1403, prim2cons_mhd_iso 2220-2267
+        if (p.eqsys == EQ_MHD) {
+          U[ibx - 1] = Q[ibx - 1]; U[iby - 1] = Q[iby - 1]; U[ibz - 1] = Q[ibz - 1]; U[ibp - 1] = Q[ibp - 1];
+        }
+      } else if (p.eqsys == EQ_HD) {
         double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
         double ei = gammam1i * Q[ipr - 1];
         U[ien - 1] = ei + ek;
@@ -845,7 +869,12 @@ struct Oracle {
       Q[ivx - 1] = U[imx - 1] / U[idn - 1];
       Q[ivy - 1] = U[imy - 1] / U[idn - 1];
       Q[ivz - 1] = U[imz - 1] / U[idn - 1];
-      if (p.eqsys == EQ_HD) {
+      if (iso) {
+        // cons2prim_hd_iso src/equations.F90:1421-1464, cons2prim_mhd_iso 2285-2332
+        if (p.eqsys == EQ_MHD) {
+          Q[ibx - 1] = U[ibx - 1]; Q[iby - 1] = U[iby - 1]; Q[ibz - 1] = U[ibz - 1]; Q[ibp - 1] = U[ibp - 1];
+        }
+      } else if (p.eqsys == EQ_HD) {
         double ek = 0.5 * (U[imx - 1] * Q[ivx - 1] + U[imy - 1] * Q[ivy - 1] + U[imz - 1] * Q[ivz - 1]);
         double ei = U[ien - 1] - ek;
         Q[ipr - 1] = gammam1 * ei;
@@ -870,7 +899,44 @@ struct Oracle {
     }
     for (int i = 0; i < n; ++i) {
       const double* Q = q + (size_t)nv * i; const double* U = u + (size_t)nv * i; double* F = f + (size_t)nv * i;
-      if (p.eqsys == EQ_HD) {
+      if (iso && p.eqsys == EQ_HD) {
+        // fluxspeed_hd_iso src/equations.F90:1484-1542
+        F[idn - 1] = U[imx - 1];
+        F[imx - 1] = Q[ivx - 1] * U[imx - 1];
+        F[imy - 1] = Q[ivx - 1] * U[imy - 1];
+        F[imz - 1] = Q[ivx - 1] * U[imz - 1];
+        F[imx - 1] = F[imx - 1] + csnd2 * Q[idn - 1];
+        if (cm && cp) {
+          cm[i] = Q[ivx - 1] - csnd;
+          cp[i] = Q[ivx - 1] + csnd;
+        }
+      } else if (iso) {
+        // fluxspeed_mhd_iso src/equations.F90:2352-2435
+        double bx2 = Q[ibx - 1] * Q[ibx - 1];
+        double by2 = Q[iby - 1] * Q[iby - 1];
+        double bz2 = Q[ibz - 1] * Q[ibz - 1];
+        double bb = bx2 + by2 + bz2;
+        double pt = csnd2 * Q[idn - 1] + 0.5 * bb;
+        F[idn - 1] = U[imx - 1];
+        F[imx - 1] = Q[ivx - 1] * U[imx - 1] - bx2;
+        F[imy - 1] = Q[ivx - 1] * U[imy - 1] - Q[ibx - 1] * Q[iby - 1];
+        F[imz - 1] = Q[ivx - 1] * U[imz - 1] - Q[ibx - 1] * Q[ibz - 1];
+        F[imx - 1] = F[imx - 1] + pt;
+        F[ibx - 1] = Q[ibp - 1];
+        F[iby - 1] = Q[ivx - 1] * Q[iby - 1] - Q[ibx - 1] * Q[ivy - 1];
+        F[ibz - 1] = Q[ivx - 1] * Q[ibz - 1] - Q[ibx - 1] * Q[ivz - 1];
+        F[ibp - 1] = cmax2 * Q[ibx - 1];
+        if (cm && cp) {
+          double fa = csnd2 * Q[idn - 1];
+          double fb = fa + bb;
+          double fc = fb * fb - 4.0 * fa * bx2;
+          double cf;
+          if (fc > 0.0) cf = std::sqrt(0.5 * (fb + std::sqrt(fc)) / Q[idn - 1]);
+          else cf = std::sqrt(0.5 * fb / Q[idn - 1]);
+          cm[i] = Q[ivx - 1] - cf;
+          cp[i] = Q[ivx - 1] + cf;
+        }
+      } else if (p.eqsys == EQ_HD) {
         F[idn - 1] = U[imx - 1];
         F[imx - 1] = Q[ivx - 1] * U[imx - 1];
         F[imy - 1] = Q[ivx - 1] * U[imy - 1];
@@ -924,7 +990,13 @@ struct Oracle {
           double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
           double v = std::sqrt(vv);
           double c;
-          if (p.eqsys == EQ_HD) {
+          if (iso && p.eqsys == EQ_HD) {
+            c = csnd;  // maxspeed_hd_iso src/equations.F90:1558-1624
+          } else if (iso) {
+            // maxspeed_mhd_iso src/equations.F90:2450-2521
+            double bb = Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1];
+            c = std::sqrt(csnd2 + bb / Q[idn - 1]);
+          } else if (p.eqsys == EQ_HD) {
             c = std::sqrt(gamma * Q[ipr - 1] / Q[idn - 1]);
           } else {
             double bb = Q[ibx - 1] * Q[ibx - 1] + Q[iby - 1] * Q[iby - 1] + Q[ibz - 1] * Q[ibz - 1];
@@ -2375,7 +2447,8 @@ void* or_create(int nkeys, const char** keys, const char** values, int* iret) {
     int r = apply_key(o->p, keys[i], values[i]);
     if (r) { *iret = r; delete o; return nullptr; }
   }
-  o->setup();
+  int r = o->setup();
+  if (r) { *iret = r; delete o; return nullptr; }
   return o;
 }
 void or_destroy(void* h) { delete static_cast<Oracle*>(h); }

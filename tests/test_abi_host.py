@@ -48,6 +48,8 @@ def test_default_params_match_reference_defaults():
     ("time_advance", "SSPRK(5,3)", "time_advance", 5), ("time_advance", "rk3", "time_advance", 3),
     ("time_advance", "unknown", "time_advance", 1), ("equation_system", "MHD", "eqsys", 1),
     ("fix_positivity", "yes", "fix_positivity", 1), ("clip_extrema", "off", "clip_extrema", 0),
+    ("equation_of_state", "isothermal", "eos", N.AMUN_EOS_ISO), ("equation_of_state", "ADI", "eos", N.AMUN_EOS_ADI),
+    ("csnd", "0.25", "csnd", 0.25), ("riemann_solver", "hlld-m", "riemann", 4),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()
@@ -57,7 +59,7 @@ def test_set_param_aliases(key, val, field, expect):
     assert getattr(p, field) == expect
 
 
-@pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "iso", 110),
+@pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "polytropic", 110),
                                           ("reconstruction", "nope", 200)])
 def test_set_param_reference_error_codes(key, val, code):
     L = N.lib()
