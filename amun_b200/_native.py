@@ -11,7 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libamun_gpu.so")
 
-AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD = 0, 1, 2
+AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD, AMUN_EQ_SRHD = 0, 1, 2, 3
 AMUN_EOS_ADI, AMUN_EOS_ISO = 0, 1
 AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
 AMUN_FP64, AMUN_FP32_BULK = 0, 1

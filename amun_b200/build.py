@@ -47,12 +47,14 @@ UNITS = {
     "kernels_fp64_hd.cu": FP64_SWEEP,
     "kernels_fp64_mhd.cu": FP64_SWEEP,
     "kernels_fp64_srmhd.cu": FP64_SWEEP,
+    "kernels_fp64_srhd.cu": FP64_SWEEP,
     "kernels_fp64_hd_iso.cu": FP64_SWEEP,
     "kernels_fp64_mhd_iso.cu": FP64_SWEEP,
     "kernels_fp32.cu": FP32,
     "kernels_fp32_hd.cu": FP32_SWEEP,
     "kernels_fp32_mhd.cu": FP32_SWEEP,
     "kernels_fp32_srmhd.cu": FP32_SWEEP,
+    "kernels_fp32_srhd.cu": FP32_SWEEP,
     "kernels_fp32_hd_iso.cu": FP32_SWEEP,
     "kernels_fp32_mhd_iso.cu": FP32_SWEEP,
 }

@@ -303,6 +303,8 @@ void tile_shape(int& LP, int& LW) {
     if (nc % d == 0 && (LP + 2) * d <= 288) { LW = d; break; }
 }
 
+bool relativistic() { return C.p.eqsys == AMUN_EQ_SRMHD || C.p.eqsys == AMUN_EQ_SRHD; }
+
 MethodConst method_const() {
   MethodConst m;
   m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.gammaxi = C.gammam1 / C.gamma;
@@ -311,7 +313,7 @@ MethodConst method_const() {
   m.tol = C.p.tolerance; m.pmin = C.p.pmin; m.nrmax = C.p.nr_maxit; m.nrext = C.p.nr_extra;
   m.plim = C.p.prolongation_limiter;
   m.csnd = C.p.csnd;
-  m.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
+  m.states_4vec = relativistic() ? C.p.states_4vec : 0;
   return m;
 }
 
@@ -319,7 +321,8 @@ MethodConst method_const() {
 int effective_solver() {
   int rs = C.p.riemann;
   if (C.p.eqsys == AMUN_EQ_HD && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
-  if (C.p.eqsys == AMUN_EQ_SRMHD && rs != AMUN_RS_HLLC) rs = AMUN_RS_HLL;
+  if (relativistic()) return (rs == AMUN_RS_HLLC || rs == AMUN_RS_HLLCM) ? AMUN_RS_HLLC : AMUN_RS_HLL;
+  if (rs == AMUN_RS_HLLCM) rs = AMUN_RS_HLL;  // HLLC-M names exist for the relativistic systems only
   if (rs == AMUN_RS_HLLDM) rs = AMUN_RS_HLL;  // HLLD-M exists for isothermal MHD only
   if (C.p.eqsys == EQ_HD_ISO || C.p.eqsys == EQ_MHD_ISO) rs = AMUN_RS_HLL;
   return rs;
@@ -435,7 +438,7 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.eq = C.p.eqsys;
   u.gammaxi = C.gammam1 / C.gamma;
   u.tol = C.p.tolerance; u.pmin = C.p.pmin; u.nrmax = C.p.nr_maxit; u.nrext = C.p.nr_extra;
-  u.states_4vec = C.p.eqsys == AMUN_EQ_SRMHD ? C.p.states_4vec : 0;
+  u.states_4vec = relativistic() ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
   u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd;
   return u;
@@ -491,6 +494,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p->eqsys = AMUN_EQ_HD;
     else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p->eqsys = AMUN_EQ_MHD;
     else if (is_one_of(v, {"srmhd", "SRMHD"})) p->eqsys = AMUN_EQ_SRMHD;
+    else if (is_one_of(v, {"srhd", "SRHD"})) p->eqsys = AMUN_EQ_SRHD;
     else return fail(100, std::string("equation system not implemented: ") + v);
   } else if (k == "equation_of_state") {
     if (is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) p->eos = AMUN_EOS_ADI;
@@ -526,6 +530,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"hlld", "HLLD"})) p->riemann = AMUN_RS_HLLD;
     else if (is_one_of(v, {"roe", "ROE"})) p->riemann = AMUN_RS_ROE;
     else if (is_one_of(v, {"hlldm", "hlld-m", "HLLDM", "HLLD-M"})) p->riemann = AMUN_RS_HLLDM;
+    else if (is_one_of(v, {"hllcm", "HLLCM", "hllc-m", "HLLC-M"})) p->riemann = AMUN_RS_HLLCM;
     else p->riemann = AMUN_RS_HLL;
   } else if (k == "time_advance") {
     if (is_one_of(v, {"euler", "EULER"})) p->time_advance = AMUN_TA_EULER;
@@ -554,13 +559,14 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
 int amun_gpu_init(const amun_params* p) {
   if (!p) return fail(AMUN_E_BAD_ARGUMENT, "null params");
   if (p->ndims != 2 && p->ndims != 3) return fail(AMUN_E_BAD_ARGUMENT, "ndims must be 2 or 3");
-  if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD && p->eqsys != AMUN_EQ_SRMHD)
+  if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD && p->eqsys != AMUN_EQ_SRMHD && p->eqsys != AMUN_EQ_SRHD)
     return fail(100, "equation system not implemented");
   if (p->eos != AMUN_EOS_ADI && p->eos != AMUN_EOS_ISO) return fail(110, "equation of state not implemented");
   if (p->eos == AMUN_EOS_ISO) {
     // src/schemes.F90:159-300: the relativistic system is adiabatic only;
     // of the isothermal solvers this library carries HLL (the default)
-    if (p->eqsys == AMUN_EQ_SRMHD) return fail(110, "the relativistic system has no isothermal equation of state");
+    if (p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD)
+      return fail(110, "the relativistic systems have no isothermal equation of state");
     if (p->riemann == AMUN_RS_ROE || (p->eqsys == AMUN_EQ_MHD && (p->riemann == AMUN_RS_HLLD ||
                                                                    p->riemann == AMUN_RS_HLLDM)))
       return fail(AMUN_E_UNSUPPORTED, "isothermal systems: HLL Riemann solver only");
@@ -579,7 +585,7 @@ int amun_gpu_init(const amun_params* p) {
   if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
   CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
-  C.nv = p->eqsys == AMUN_EQ_HD ? 5 : 9;
+  C.nv = (p->eqsys == AMUN_EQ_HD || p->eqsys == AMUN_EQ_SRHD) ? 5 : 9;
   if (p->eos == AMUN_EOS_ISO) {
     // kernels take the isothermal systems as systems of their own
     C.p.eqsys = p->eqsys == AMUN_EQ_HD ? EQ_HD_ISO : EQ_MHD_ISO;

@@ -81,7 +81,7 @@ static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
       case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
       default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
-  } else if constexpr (EQ == EQ_SRMHD) {
+  } else if constexpr (EQ == EQ_SRMHD || EQ == EQ_SRHD) {
     switch (rs) {
       case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
       default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
@@ -107,6 +107,7 @@ cudaError_t Launch<R, U1T>::sweep(int eq, int rec, int rs, int dir, const SweepA
                                   int threads, size_t smem, cudaStream_t s) {
   if (eq == EQ_HD) return sweep_eq<R, U1T, EQ_HD>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_MHD) return sweep_eq<R, U1T, EQ_MHD>(rec, rs, dir, a, grid, threads, smem, s);
+  if (eq == EQ_SRHD) return sweep_eq<R, U1T, EQ_SRHD>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_HD_ISO) return sweep_eq<R, U1T, EQ_HD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_MHD_ISO) return sweep_eq<R, U1T, EQ_MHD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
   return sweep_eq<R, U1T, EQ_SRMHD>(rec, rs, dir, a, grid, threads, smem, s);
@@ -130,6 +131,7 @@ cudaError_t Launch<R, U1T>::cons2prim_blocks(int eq, const double* u0, R* q, con
   const int grid = grid_for(g.uvs * nb, threads);
   if (eq == EQ_HD) cons2prim_blocks_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else if (eq == EQ_MHD) cons2prim_blocks_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
+  else if (eq == EQ_SRHD) cons2prim_blocks_kernel<EQ_SRHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else if (eq == EQ_HD_ISO) cons2prim_blocks_kernel<EQ_HD_ISO, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else if (eq == EQ_MHD_ISO) cons2prim_blocks_kernel<EQ_MHD_ISO, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
   else cons2prim_blocks_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(u0, q, g, m, sc, b0, nb);
@@ -153,6 +155,7 @@ cudaError_t Launch<R, U1T>::maxspeed(int eq, const R* q, const Geo& g, double ga
   int grid = grid_for(n, threads);
   if (eq == EQ_HD) maxspeed_kernel<EQ_HD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   else if (eq == EQ_MHD) maxspeed_kernel<EQ_MHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
+  else if (eq == EQ_SRHD) maxspeed_kernel<EQ_SRHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   else if (eq == EQ_HD_ISO) maxspeed_kernel<EQ_HD_ISO, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   else if (eq == EQ_MHD_ISO) maxspeed_kernel<EQ_MHD_ISO, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   else maxspeed_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
@@ -200,6 +203,7 @@ static cudaError_t download_u_any(int eq, const UT* u, const R* q, double* fu, c
   int grid = grid_for(n, 256);
   if (eq == EQ_HD) download_u_kernel<EQ_HD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else if (eq == EQ_MHD) download_u_kernel<EQ_MHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
+  else if (eq == EQ_SRHD) download_u_kernel<EQ_SRHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else if (eq == EQ_HD_ISO) download_u_kernel<EQ_HD_ISO, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else if (eq == EQ_MHD_ISO) download_u_kernel<EQ_MHD_ISO, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);
   else download_u_kernel<EQ_SRMHD, R, UT><<<grid, 256, 0, s>>>(u, q, fu, g, m, b0, nb);

@@ -8,6 +8,7 @@
 //   HD  (NV=5): dens, velx, vely, velz, pres
 //   MHD (NV=9): dens, velx, vely, velz, magx, magy, magz, bpsi, pres
 //   isothermal HD (NV=4) and MHD (NV=8): the same without pres
+//   SRHD (NV=5) as HD, SRMHD (NV=9) as MHD
 // Conserved variables use the same slots (momenta, energy in the pres slot).
 #pragma once
 #include <cstdint>
@@ -20,7 +21,7 @@ enum { REC_TVD = 0, REC_WENO5Z = 1 };
 
 // equation systems (src/equations.F90:322-833); *_ISO: isothermal equation
 // of state (p = csnd^2 rho, no energy equation)
-enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_HD_ISO = 3, EQ_MHD_ISO = 4 };
+enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3, EQ_HD_ISO = 4, EQ_MHD_ISO = 5 };
 
 template <int EQ> struct Var;
 template <> struct Var<EQ_HD> {
@@ -38,6 +39,12 @@ template <> struct Var<EQ_SRMHD> {
   static constexpr int NV = 9;
   static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, BX = 4, BY = 5, BZ = 6, BP = 7, PR = 8, EN = 8;
   static constexpr bool MHD = true, SR = true, ISO = false;
+};
+template <> struct Var<EQ_SRHD> {
+  static constexpr int NV = 5;
+  static constexpr int DN = 0, VX = 1, VY = 2, VZ = 3, PR = 4, EN = 4;
+  static constexpr int BX = -1, BY = -1, BZ = -1, BP = -1;
+  static constexpr bool MHD = false, SR = true, ISO = false;
 };
 template <> struct Var<EQ_HD_ISO> {
   static constexpr int NV = 4;
@@ -102,7 +109,15 @@ __device__ __forceinline__ R limiter(int which, R x, R a, R b, R eps) {
 
 }  // namespace amun
 #include "srmhd.cuh"
+#include "srhd.cuh"
 namespace amun {
+
+// the relativistic recovery of one cell (FP64); false when it failed
+template <int EQ>
+__device__ __forceinline__ bool sr_recover(const double* u, double* q, const Phys<double>& P) {
+  if constexpr (Var<EQ>::MHD) return cons2prim_sr(u, q, P);
+  else return cons2prim_srhd(u, q, P);
+}
 
 // ---------------------------------------------------------------------------
 // Conversions and physical fluxes
@@ -112,7 +127,8 @@ template <int EQ, typename R>
 __device__ __forceinline__ void prim2cons(const R* q, R* u, const Phys<R>& P) {
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
-  if constexpr (V::SR) { prim2cons_sr(q, u, P); return; }
+  if constexpr (V::SR && V::MHD) { prim2cons_sr(q, u, P); return; }
+  if constexpr (V::SR) { prim2cons_srhd(q, u, P); return; }
   if constexpr (V::ISO) {
     // prim2cons_hd_iso src/equations.F90:1360-1403, prim2cons_mhd_iso 2220-2267
     u[V::DN] = q[V::DN];
@@ -146,7 +162,7 @@ __device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
   constexpr int NV = V::NV; (void)NV;
   if constexpr (V::SR) {
     static_assert(sizeof(R) == 8, "the relativistic recovery runs in FP64");
-    cons2prim_sr(u, q, P);
+    sr_recover<EQ>(u, q, P);
     return;
   }
   if constexpr (V::ISO) {
@@ -181,7 +197,8 @@ template <int EQ, bool SPEEDS, typename R>
 __device__ __forceinline__ void fluxspeed(const R* q, const R* u, R* f, R& cm, R& cp, const Phys<R>& P) {
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
-  if constexpr (V::SR) { fluxspeed_sr<SPEEDS>(q, u, f, cm, cp, P); return; }
+  if constexpr (V::SR && V::MHD) { fluxspeed_sr<SPEEDS>(q, u, f, cm, cp, P); return; }
+  if constexpr (V::SR) { fluxspeed_srhd<SPEEDS>(q, u, f, cm, cp, P); return; }
   if constexpr (V::ISO && !V::MHD) {
     // fluxspeed_hd_iso src/equations.F90:1484-1542
     f[V::DN] = u[V::VX];
@@ -271,7 +288,8 @@ template <int EQ, typename R>
 __device__ __forceinline__ double cell_speed(const R* q, double gamma, double csnd) {
   using V = Var<EQ>;
   constexpr int NV = V::NV; (void)NV;
-  if constexpr (V::SR) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
+  if constexpr (V::SR && V::MHD) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
+  if constexpr (V::SR) return srhd_cell_speed(q, gamma, (gamma - 1.0) / gamma);
   double vx = q[V::VX], vy = q[V::VY], vz = q[V::VZ];
   double vv = vx * vx + vy * vy + vz * vz;
   double v = sqrt(vv);
@@ -658,7 +676,8 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
     R sl = d_min(clm, crm), sr = d_max(clp, crp);
     if constexpr (V::SR && RS == RS_HLLC) {
-      srmhd_hllc(ql, qr, ul, ur, fl, fr, sl, sr, f);
+      if constexpr (V::MHD) srmhd_hllc(ql, qr, ul, ur, fl, fr, sl, sr, f);
+      else srhd_hllc(ul, ur, fl, fr, sl, sr, f);
       return;
     }
     if (sl >= R(0)) {

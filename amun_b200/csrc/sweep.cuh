@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       // (src/equations.F90:4745-4777)
 #pragma unroll
       for (int v = 0; v < NV; ++v) qn[v] = (double)a.q[co + v * g.qvs];
-      if (!cons2prim_sr(un, qn, Pd)) atomicAdd(&a.sc->c2p_failures, 1ull);
+      if (!sr_recover<EQ>(un, qn, Pd)) atomicAdd(&a.sc->c2p_failures, 1ull);
     } else {
       cons2prim<EQ>(un, qn, Pd);
     }
@@ -639,7 +639,7 @@ __global__ void cons2prim_blocks_kernel(const double* u0, R* q, Geo g, MethodCon
     if constexpr (Var<EQ>::SR) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) qc[v] = (double)q[c + v * g.qvs];
-      if (!cons2prim_sr(uc, qc, Pd)) atomicAdd(&sc->c2p_failures, 1ull);
+      if (!sr_recover<EQ>(uc, qc, Pd)) atomicAdd(&sc->c2p_failures, 1ull);
     } else {
       cons2prim<EQ>(uc, qc, Pd);
     }

@@ -249,11 +249,11 @@ static cudaError_t riemann_dirs(const double* qs, double* f, BlockDims d, const 
   return cudaGetLastError();
 }
 
-// 4-vector states for SRMHD reconstruction (src/schemes.F90:5043-5100):
-// to 4-velocity before reconstructing, face states back afterwards
-__global__ void four_vector_kernel(double* q, long long n, int forward) {
+// 4-vector states for SRHD / SRMHD reconstruction (src/schemes.F90:4475-4525,
+// 5043-5100): to 4-velocity before reconstructing, face states back afterwards
+__global__ void four_vector_kernel(double* q, long long n, int nv, int forward) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    double* c = q + t * 9;
+    double* c = q + t * nv;
     if (forward) to_four_velocity(c); else from_four_velocity(c);
   }
 }
@@ -279,7 +279,7 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
     // reconstruct 4-vector states: the converted copy lives in the scratch tail
     double* qq = scratch + unit_block_flux_scratch(u) / sizeof(double) - cells * NV;
     cudaMemcpyAsync(qq, q, cells * NV * sizeof(double), cudaMemcpyDeviceToDevice, s);
-    four_vector_kernel<<<(int)((cells + 255) / 256), 256, 0, s>>>(qq, cells, 1);
+    four_vector_kernel<<<(int)((cells + 255) / 256), 256, 0, s>>>(qq, cells, NV, 1);
     qr = qq;
   }
   tvd_ghost_copy<<<(int)((cells + 255) / 256), 256, 0, s>>>(qr, qs, d);
@@ -296,7 +296,7 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
   }
   if (four) {
     long long nstates = cells * 2 * u.ndims;
-    four_vector_kernel<<<(int)((nstates + 255) / 256), 256, 0, s>>>(qs, nstates, 0);
+    four_vector_kernel<<<(int)((nstates + 255) / 256), 256, 0, s>>>(qs, nstates, NV, 0);
   }
   const Phys<double> P = unit_phys(u);
   if constexpr (EQ == EQ_HD) {
@@ -312,7 +312,7 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
       case RS_ROE: return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
       default: return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
     }
-  } else if constexpr (EQ == EQ_SRMHD) {
+  } else if constexpr (EQ == EQ_SRMHD || EQ == EQ_SRHD) {
     if (u.rs == RS_HLLC) return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
     return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
   } else {
@@ -325,6 +325,7 @@ cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, doub
   if (u.eq == EQ_HD) return block_flux_eq<EQ_HD>(u, q, qs, f, scratch, nonpos, s);
   if (u.eq == EQ_MHD) return block_flux_eq<EQ_MHD>(u, q, qs, f, scratch, nonpos, s);
   if (u.eq == EQ_HD_ISO) return block_flux_eq<EQ_HD_ISO>(u, q, qs, f, scratch, nonpos, s);
+  if (u.eq == EQ_SRHD) return block_flux_eq<EQ_SRHD>(u, q, qs, f, scratch, nonpos, s);
   if (u.eq == EQ_MHD_ISO) return block_flux_eq<EQ_MHD_ISO>(u, q, qs, f, scratch, nonpos, s);
   return block_flux_eq<EQ_SRMHD>(u, q, qs, f, scratch, nonpos, s);
 }
@@ -354,6 +355,9 @@ cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const doubl
       case RS_ROE: line_riemann<EQ_MHD, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
       default: line_riemann<EQ_MHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
     }
+  } else if (u.eq == EQ_SRHD) {
+    if (u.rs == RS_HLLC) line_riemann<EQ_SRHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+    else line_riemann<EQ_SRHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   } else if (u.eq == EQ_HD_ISO) {
     line_riemann<EQ_HD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   } else if (u.eq == EQ_MHD_ISO) {
@@ -373,6 +377,7 @@ cudaError_t unit_pointwise(const UnitArgs& u, int op, int n, const double* a, co
   if (u.eq == EQ_HD) pointwise<EQ_HD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else if (u.eq == EQ_MHD) pointwise<EQ_MHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else if (u.eq == EQ_HD_ISO) pointwise<EQ_HD_ISO><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
+  else if (u.eq == EQ_SRHD) pointwise<EQ_SRHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else if (u.eq == EQ_MHD_ISO) pointwise<EQ_MHD_ISO><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   else pointwise<EQ_SRMHD><<<grid, 128, 0, s>>>(op, n, a, b, o, cm, cp, P);
   return cudaGetLastError();
@@ -386,6 +391,7 @@ cudaError_t unit_maxspeed(const UnitArgs& u, const double* q, unsigned long long
   if (u.eq == EQ_HD) block_maxspeed<EQ_HD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   else if (u.eq == EQ_MHD) block_maxspeed<EQ_MHD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   else if (u.eq == EQ_HD_ISO) block_maxspeed<EQ_HD_ISO><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
+  else if (u.eq == EQ_SRHD) block_maxspeed<EQ_SRHD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   else if (u.eq == EQ_MHD_ISO) block_maxspeed<EQ_MHD_ISO><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   else block_maxspeed<EQ_SRMHD><<<grid, 256, 0, s>>>(q, d, u.gamma, u.csnd, out);
   return cudaGetLastError();

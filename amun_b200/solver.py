@@ -31,7 +31,7 @@ class Simulation:
         self.native = to_native(self.params)
         self.geo = geometry(self.params)
         self.mesh = UniformMesh(self.geo) if mesh is None else mesh
-        self.nv = (5 if self.native.eqsys == N.AMUN_EQ_HD else 9) - (self.native.eos == N.AMUN_EOS_ISO)
+        self.nv = (5 if self.native.eqsys in (N.AMUN_EQ_HD, N.AMUN_EQ_SRHD) else 9) - (self.native.eos == N.AMUN_EOS_ISO)
         N.check(self.L.amun_gpu_init(C.byref(self.native)))
         self._desc = self.mesh.descriptors()
         N.check(self.L.amun_gpu_set_blocks(self.mesh.nblocks, self._desc))

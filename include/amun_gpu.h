@@ -33,7 +33,7 @@ extern "C" {
 #define AMUN_E_NO_BLOCKS       905
 
 /* equation_system / equation_of_state (src/equations.F90:322-833) */
-enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2 };
+enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2, AMUN_EQ_SRHD = 3 };
 enum { AMUN_EOS_ADI = 0, AMUN_EOS_ISO = 1 };
 /* reconstruction (src/interpolations.F90:226-382) */
 enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
@@ -41,7 +41,8 @@ enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
 enum { AMUN_LIM_ZERO = 0, AMUN_LIM_MM = 1, AMUN_LIM_MC = 2, AMUN_LIM_SB = 3,
        AMUN_LIM_VL = 4, AMUN_LIM_VA = 5 };
 /* riemann_solver (src/schemes.F90:159-503) */
-enum { AMUN_RS_HLL = 0, AMUN_RS_HLLC = 1, AMUN_RS_HLLD = 2, AMUN_RS_ROE = 3, AMUN_RS_HLLDM = 4 };
+enum { AMUN_RS_HLL = 0, AMUN_RS_HLLC = 1, AMUN_RS_HLLD = 2, AMUN_RS_ROE = 3, AMUN_RS_HLLDM = 4,
+       AMUN_RS_HLLCM = 5 /* "hllcm": HLLC for the relativistic systems */ };
 /* time_advance (src/evolution.F90:164-209) */
 enum { AMUN_TA_EULER = 0, AMUN_TA_RK2 = 1, AMUN_TA_SSPRK2 = 2, AMUN_TA_RK3 = 3,
        AMUN_TA_SSPRK34 = 4, AMUN_TA_SSPRK35 = 5 };

@@ -39,10 +39,10 @@ namespace {
 // src/interpolations.F90:144-495, src/evolution.F90:115-230,
 // src/coordinates.F90:160-357).  Defaults are the reference defaults.
 // ---------------------------------------------------------------------------
-enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2 };
+enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
-enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM };
+enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM, RS_HLLCM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
 
 struct Params {
@@ -90,6 +90,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     if (is_one_of(v, {"hd", "HD", "hydro", "HYDRO", "hydrodynamic", "HYDRODYNAMIC"})) p.eqsys = EQ_HD;
     else if (is_one_of(v, {"mhd", "MHD", "magnetohydrodynamic", "MAGNETOHYDRODYNAMIC"})) p.eqsys = EQ_MHD;
     else if (is_one_of(v, {"srmhd", "SRMHD"})) p.eqsys = EQ_SRMHD;
+    else if (is_one_of(v, {"srhd", "SRHD"})) p.eqsys = EQ_SRHD;
     else return 100;  // src/equations.F90:830
   } else if (key == "equation_of_state") {
     if (is_one_of(v, {"adi", "ADI", "adiabatic", "ADIABATIC"})) p.iso = false;
@@ -121,6 +122,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"hlld", "HLLD"})) p.rs = RS_HLLD;
     else if (is_one_of(v, {"roe", "ROE"})) p.rs = RS_ROE;
     else if (is_one_of(v, {"hlldm", "hlld-m", "HLLDM", "HLLD-M"})) p.rs = RS_HLLDM;
+    else if (is_one_of(v, {"hllcm", "HLLCM", "hllc-m", "HLLC-M"})) p.rs = RS_HLLCM;
     else p.rs = RS_HLL;
   } else if (key == "time_advance") {
     if (is_one_of(v, {"euler", "EULER"})) p.ta = TA_EULER;
@@ -425,6 +427,7 @@ struct Oracle {
   double gamma = 5.0 / 3.0, gammam1 = 2.0 / 3.0, gammam1i = 1.5, gammaxi = 0.4;
   double csnd = 1.0, csnd2 = 1.0;  // src/equations.F90:847-851
   bool iso = false;
+  bool mhd = false, sr = false;  // magnetic field present; special relativistic
   double cmax = 0.0, cmax2 = 0.0;
   mutable std::atomic<long> c2p_failures{0};  // failed relativistic recoveries (p set to 0)
   // evolution (src/evolution.F90:60-90)
@@ -478,7 +481,9 @@ struct Oracle {
 
   int setup() {
     // equations (src/equations.F90:322-485)
-    if (p.eqsys == EQ_HD) {
+    mhd = p.eqsys == EQ_MHD || p.eqsys == EQ_SRMHD;
+    sr = p.eqsys == EQ_SRMHD || p.eqsys == EQ_SRHD;
+    if (!mhd) {
       nv = 5; idn = 1; ivx = 2; ivy = 3; ivz = 4; imx = 2; imy = 3; imz = 4;
       ibx = iby = ibz = ibp = -1; ipr = ien = 5;
     } else {
@@ -488,17 +493,20 @@ struct Oracle {
     // isothermal: no energy equation, ipr = ien = 0 (src/equations.F90:335-392)
     iso = p.iso;
     if (iso) {
-      if (p.eqsys == EQ_SRMHD) return 110;
+      if (sr) return 110;
       nv -= 1; ipr = ien = 0;
       // of the isothermal solvers (src/schemes.F90:159-300) HLL is restated
       if (p.rs == RS_ROE || (p.eqsys == EQ_MHD && (p.rs == RS_HLLD || p.rs == RS_HLLDM))) return 904;
       p.rs = RS_HLL;
     }
     csnd = p.csnd; csnd2 = csnd * csnd;
+    // the relativistic systems offer HLL and HLLC ("hllcm" included,
+    // src/schemes.F90:400-498); elsewhere "hllcm" names nothing
+    if (sr) p.rs = (p.rs == RS_HLLC || p.rs == RS_HLLCM) ? RS_HLLC : RS_HLL;
+    if (p.rs == RS_HLLCM) p.rs = RS_HLL;
     if (p.rs == RS_HLLDM) p.rs = RS_HLL;  // HLLD-M exists for isothermal MHD only
     if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
     // SRMHD offers HLL and HLLC only (src/schemes.F90:472-498)
-    if (p.eqsys == EQ_SRMHD && p.rs != RS_HLLC) p.rs = RS_HLL;
     gamma = p.gamma; gammam1 = gamma - 1.0; gammam1i = 1.0 / gammam1;
     gammaxi = gammam1 / gamma;
     // evolution: CFL rescale and decay (src/evolution.F90:164-213)
@@ -824,12 +832,184 @@ struct Oracle {
   }
 
   // =========================================================================
+  // SPECIAL RELATIVISTIC HD (adiabatic); variables as HD, conserved
+  // D, m_x, m_y, m_z, E - D
+  // =========================================================================
+  // prim2cons_srhd_adi src/equations.F90:3478-3532
+  void prim2cons_srhd(const double* Q, double* U) const {
+    double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+    double vm = 1.0 - vv;
+    double vs = std::sqrt(vm);
+    double ww = (Q[idn - 1] + Q[ipr - 1] / gammaxi) / vm;
+    U[idn - 1] = Q[idn - 1] / vs;
+    U[imx - 1] = ww * Q[ivx - 1];
+    U[imy - 1] = ww * Q[ivy - 1];
+    U[imz - 1] = ww * Q[ivz - 1];
+    U[ien - 1] = ww - Q[ipr - 1] - U[idn - 1];
+  }
+
+  // nr_function_srhd_adi_1d src/equations.F90:3853-3881
+  void nr_function_srhd(double mm, double en, double dn, double w, double& f, double* df) const {
+    double vv = mm / (w * w);
+    double vm = 1.0 - vv;
+    double vs = std::sqrt(vm);
+    f = (1.0 - gammaxi * vm) * w + gammaxi * dn * vs - en;
+    if (df) *df = 1.0 - gammaxi * (1.0 + (1.0 - dn / (vs * w)) * vv);
+  }
+
+  // nr_iterate_srhd_adi_1dw src/equations.F90:3911-4091.  Where the lower
+  // bracket is itself the root the reference leaves vv from an earlier call;
+  // here vv = mm / w^2 of that root.
+  bool nr_iterate_srhd_1dw(double mm, double en, double dn, double& w, double& vv) const {
+    double wl = std::sqrt(mm + dn * dn);
+    if (!(en > wl)) return false;  // "The state is not physical!"
+    wl = wl + gammaxi * p.pmin;
+    double wu = en + p.pmin;
+    double fl, fu;
+    nr_function_srhd(mm, en, dn, wl, fl, nullptr);
+    if (fl < 0.0) {
+      if (wu <= wl) wu = 2.0 * wl;
+      nr_function_srhd(mm, en, dn, wu, fu, nullptr);
+      int it = p.nrmax;
+      bool keep = fl * fu > 0.0;
+      while (keep) {
+        it = it - 1;
+        wl = wu;
+        fl = fu;
+        wu = 2.0 * wu;
+        nr_function_srhd(mm, en, dn, wu, fu, nullptr);
+        keep = (fl * fu > 0.0) && it > 0;
+      }
+      if (!(it > 0 && fu >= 0.0)) return false;  // "Could not find the upper bracket!"
+      w = wl - fl * (wu - wl) / (fu - fl);
+      keep = true;
+      it = p.nrmax;
+      int cn = p.nrext;
+      while (keep) {
+        double f, df;
+        nr_function_srhd(mm, en, dn, w, f, &df);
+        if (f > fl && f < 0.0) { wl = w; fl = f; }
+        if (f < fu && f > 0.0) { wu = w; fu = f; }
+        double dw = f / df;
+        w = w - dw;
+        double err = std::fabs(dw / w);
+        if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+        else keep = it > 0;
+        if (w < wl || w > wu) w = 0.5 * (wl + wu);
+        it = it - 1;
+      }
+      vv = mm / (w * w);
+      return true;
+    }
+    if (fl == 0.0) {
+      w = wl;
+      vv = mm / (w * w);
+      return true;
+    }
+    return false;  // "Positive function for lower bracket!"
+  }
+
+  // cons2prim_srhd_adi src/equations.F90:3550-3639.  On failure only the
+  // pressure is set (to zero); the other entries of q keep their values.
+  void cons2prim_srhd(const double* U, double* Q) const {
+    double mm = U[imx - 1] * U[imx - 1] + U[imy - 1] * U[imy - 1] + U[imz - 1] * U[imz - 1];
+    double en = U[ien - 1] + U[idn - 1];
+    double dn = U[idn - 1];
+    double w = 0.0, vv = 0.0;
+    if (nr_iterate_srhd_1dw(mm, en, dn, w, vv)) {
+      double vm = 1.0 - vv;
+      double vs = std::sqrt(vm);
+      Q[idn - 1] = dn * vs;
+      Q[ivx - 1] = U[imx - 1] / w;
+      Q[ivy - 1] = U[imy - 1] / w;
+      Q[ivz - 1] = U[imz - 1] / w;
+      Q[ipr - 1] = w - en;
+    } else {
+      Q[ipr - 1] = 0.0;
+      ++c2p_failures;
+    }
+  }
+
+  // fluxspeed_srhd_adi src/equations.F90:3665-3731
+  void fluxspeed_srhd(const double* Q, const double* U, double* F, double* cm, double* cp) const {
+    F[idn - 1] = U[idn - 1] * Q[ivx - 1];
+    F[imx - 1] = U[imx - 1] * Q[ivx - 1] + Q[ipr - 1];
+    F[imy - 1] = U[imy - 1] * Q[ivx - 1];
+    F[imz - 1] = U[imz - 1] * Q[ivx - 1];
+    F[ien - 1] = U[imx - 1] - F[idn - 1];
+    if (cm && cp) {
+      double ww = Q[idn - 1] + Q[ipr - 1] / gammaxi;
+      double c2 = gamma * Q[ipr - 1] / ww;
+      double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+      double ss = c2 * (1.0 - vv) / (1.0 - c2);
+      double fc = 1.0 + ss;
+      double cc = std::sqrt(ss * (fc - Q[ivx - 1] * Q[ivx - 1]));
+      *cm = (Q[ivx - 1] - cc) / fc;
+      *cp = (Q[ivx - 1] + cc) / fc;
+    }
+  }
+
+  // riemann_srhd_adi_hllc src/schemes.F90:4775-4968, one interface
+  void srhd_hllc_point(const double* ul, const double* ur, const double* fl, const double* fr, double sl, double sr,
+                       double* f) const {
+    const int N = nv;
+    if (sl >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
+    if (sr <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
+    const int Dn = idn - 1, Mx = imx - 1, My = imy - 1, Mz = imz - 1, En = ien - 1;
+    double srml = sr - sl;
+    double wl[5], wr[5], uh[5], fh[5], us[5], a[3], x[2];
+    for (int v = 0; v < N; ++v) {
+      wl[v] = sl * ul[v] - fl[v];
+      wr[v] = sr * ur[v] - fr[v];
+      uh[v] = (wr[v] - wl[v]) / srml;
+      fh[v] = (sl * wr[v] - sr * wl[v]) / srml;
+    }
+    wl[En] = wl[En] + wl[Dn];
+    wr[En] = wr[En] + wr[Dn];
+    auto use_hll = [&]() { for (int v = 0; v < N; ++v) f[v] = fh[v]; };
+    a[0] = uh[Mx];
+    a[1] = -(fh[Mx] + uh[En] + uh[Dn]);
+    a[2] = fh[En] + fh[Dn];
+    int nr = alg_quadratic(a, x);
+    if (nr < 1) { use_hll(); return; }
+    double sm = x[0];
+    if ((sm <= sl) || (sm >= sr)) { use_hll(); return; }
+    double pr = fh[Mx] - (fh[En] + fh[Dn]) * sm;
+    if (pr <= 0.0) { use_hll(); return; }
+    if (sm > 0.0) {
+      double dv = sl - sm;
+      us[Dn] = wl[Dn] / dv;
+      us[My] = wl[My] / dv;
+      us[Mz] = wl[Mz] / dv;
+      us[En] = (wl[En] + pr * sm) / dv;
+      us[Mx] = (us[En] + pr) * sm;
+      us[En] = us[En] - us[Dn];
+      for (int v = 0; v < N; ++v) f[v] = fl[v] + sl * (us[v] - ul[v]);
+    } else if (sm < 0.0) {
+      double dv = sr - sm;
+      us[Dn] = wr[Dn] / dv;
+      us[My] = wr[My] / dv;
+      us[Mz] = wr[Mz] / dv;
+      us[En] = (wr[En] + pr * sm) / dv;
+      us[Mx] = (us[En] + pr) * sm;
+      us[En] = us[En] - us[Dn];
+      for (int v = 0; v < N; ++v) f[v] = fr[v] + sr * (us[v] - ur[v]);
+    } else {
+      f[Dn] = 0.0; f[Mx] = pr; f[My] = 0.0; f[Mz] = 0.0; f[En] = 0.0;
+    }
+  }
+
+  // =========================================================================
   // EQUATIONS
   // =========================================================================
   // prim2cons_hd_adi src/equations.F90:1762-1810, prim2cons_mhd_adi 2815-2868
   void prim2cons(int n, const double* q, double* u) const {
     if (p.eqsys == EQ_SRMHD) {
       for (int i = 0; i < n; ++i) prim2cons_sr(q + (size_t)nv * i, u + (size_t)nv * i);
+      return;
+    }
+    if (p.eqsys == EQ_SRHD) {
+      for (int i = 0; i < n; ++i) prim2cons_srhd(q + (size_t)nv * i, u + (size_t)nv * i);
       return;
     }
     for (int i = 0; i < n; ++i) {
@@ -863,6 +1043,10 @@ struct Oracle {
       for (int i = 0; i < n; ++i) cons2prim_sr(u + (size_t)nv * i, q + (size_t)nv * i);
       return;
     }
+    if (p.eqsys == EQ_SRHD) {
+      for (int i = 0; i < n; ++i) cons2prim_srhd(u + (size_t)nv * i, q + (size_t)nv * i);
+      return;
+    }
     for (int i = 0; i < n; ++i) {
       const double* U = u + (size_t)nv * i; double* Q = q + (size_t)nv * i;
       Q[idn - 1] = U[idn - 1];
@@ -891,6 +1075,12 @@ struct Oracle {
   // fluxspeed_hd_adi src/equations.F90:1896-1958,
   // fluxspeed_mhd_adi src/equations.F90:2959-3045
   void fluxspeed(int n, const double* q, const double* u, double* f, double* cm, double* cp) const {
+    if (p.eqsys == EQ_SRHD) {
+      for (int i = 0; i < n; ++i)
+        fluxspeed_srhd(q + (size_t)nv * i, u + (size_t)nv * i, f + (size_t)nv * i, cm ? cm + i : nullptr,
+                       cp ? cp + i : nullptr);
+      return;
+    }
     if (p.eqsys == EQ_SRMHD) {
       for (int i = 0; i < n; ++i)
         fluxspeed_sr(q + (size_t)nv * i, u + (size_t)nv * i, f + (size_t)nv * i, cm ? cm + i : nullptr,
@@ -983,6 +1173,23 @@ struct Oracle {
   double maxspeed(const double* qq) const {
     if (p.eqsys == EQ_SRMHD) return 1.0;  // maxspeed_srmhd_adi src/equations.F90:5116-5150
     double ms = 0.0;
+    if (p.eqsys == EQ_SRHD) {
+      // maxspeed_srhd_adi src/equations.F90:3746-3820
+      for (int k = kb; k <= ke; ++k)
+        for (int j = jb; j <= je; ++j)
+          for (int i = ib; i <= ie; ++i) {
+            const double* Q = qq + qi(1, i, j, k);
+            double vv = Q[ivx - 1] * Q[ivx - 1] + Q[ivy - 1] * Q[ivy - 1] + Q[ivz - 1] * Q[ivz - 1];
+            double v = std::sqrt(vv);
+            double ww = Q[idn - 1] + Q[ipr - 1] / gammaxi;
+            double c2 = gamma * Q[ipr - 1] / ww;
+            double ss = c2 * (1.0 - vv) / (1.0 - c2);
+            double fc = 1.0 + ss;
+            double cc = std::sqrt(ss * (fc - vv));
+            ms = fmax2(ms, (v + cc) / fc);
+          }
+      return ms;
+    }
     for (int k = kb; k <= ke; ++k)
       for (int j = jb; j <= je; ++j)
         for (int i = ib; i <= ie; ++i) {
@@ -1459,12 +1666,18 @@ struct Oracle {
     const int N = nv;
     double ul[9], ur[9], fl[9], fr[9], wl[9], wr[9], ui[9], wcl[9], wcr[9];
     double clm, clp, crm, crp;
-    if (p.eqsys != EQ_HD) glm(ql, qr);
+    if (mhd) glm(ql, qr);
     prim2cons(1, ql, ul); prim2cons(1, qr, ur);
     if (p.eqsys == EQ_SRMHD && p.rs == RS_HLLC) {
       fluxspeed(1, ql, ul, fl, &clm, &clp);
       fluxspeed(1, qr, ur, fr, &crm, &crp);
       srmhd_hllc_point(ql, qr, ul, ur, fl, fr, fmin2(clm, crm), fmax2(clp, crp), f);
+      return;
+    }
+    if (p.eqsys == EQ_SRHD && p.rs == RS_HLLC) {
+      fluxspeed(1, ql, ul, fl, &clm, &clp);
+      fluxspeed(1, qr, ur, fr, &crm, &crp);
+      srhd_hllc_point(ul, ur, fl, fr, fmin2(clm, crm), fmax2(clp, crp), f);
       return;
     }
     if (p.rs == RS_ROE) {
@@ -1904,7 +2117,7 @@ struct Oracle {
     std::vector<double> one(N), ones(N * 2 * p.ndims);
     // update_flux_srmhd_adi with state_variables = "4vec" (src/schemes.F90:
     // 5043-5100): reconstruct D = rho Gamma and u = Gamma v, convert back after
-    const bool four = p.eqsys == EQ_SRMHD && p.states_4vec;
+    const bool four = sr && p.states_4vec;
     std::vector<double> qq;
     if (four) {
       qq.assign(q, q + (size_t)nv * N);
@@ -1954,7 +2167,7 @@ struct Oracle {
           double* L = &ql[(size_t)nv * t]; double* R = &qr[(size_t)nv * t];
           for (int v = 0; v < nv; ++v) { L[v] = sl_[v]; R[v] = sr_[v]; }
           for (int m = 0; m < 3; ++m) { L[ivx - 1 + m] = sl_[ivx - 1 + pm[m]]; R[ivx - 1 + m] = sr_[ivx - 1 + pm[m]]; }
-          if (p.eqsys != EQ_HD)
+          if (mhd)
             for (int m = 0; m < 3; ++m) { L[ibx - 1 + m] = sl_[ibx - 1 + pm[m]]; R[ibx - 1 + m] = sr_[ibx - 1 + pm[m]]; }
         }
         riemann_line(n, ql.data(), qr.data(), fx.data());
@@ -1965,7 +2178,7 @@ struct Oracle {
           double tmp[9];
           for (int v = 0; v < nv; ++v) tmp[v] = F[v];
           for (int m = 0; m < 3; ++m) tmp[imx - 1 + pm[m]] = F[imx - 1 + m];
-          if (p.eqsys != EQ_HD)
+          if (mhd)
             for (int m = 0; m < 3; ++m) tmp[ibx - 1 + pm[m]] = F[ibx - 1 + m];
           for (int v = 0; v < nv; ++v) f[fi(d, v + 1, i, j, k)] = tmp[v];
         }
