@@ -323,8 +323,11 @@ int effective_solver() {
   if (C.p.eqsys == AMUN_EQ_HD && rs == AMUN_RS_HLLD) rs = AMUN_RS_HLL;
   if (relativistic()) return (rs == AMUN_RS_HLLC || rs == AMUN_RS_HLLCM) ? AMUN_RS_HLLC : AMUN_RS_HLL;
   if (rs == AMUN_RS_HLLCM) rs = AMUN_RS_HLL;  // HLLC-M names exist for the relativistic systems only
-  if (rs == AMUN_RS_HLLDM) rs = AMUN_RS_HLL;  // HLLD-M exists for isothermal MHD only
-  if (C.p.eqsys == EQ_HD_ISO || C.p.eqsys == EQ_MHD_ISO) rs = AMUN_RS_HLL;
+  // isothermal: HD offers Roe and HLL, MHD HLLD, HLLD-M, Roe and HLL
+  // (src/schemes.F90:159-300); HLLD-M exists for isothermal MHD only
+  if (C.p.eqsys == EQ_HD_ISO) return rs == AMUN_RS_ROE ? rs : AMUN_RS_HLL;
+  if (C.p.eqsys == EQ_MHD_ISO) return rs == AMUN_RS_HLLC ? AMUN_RS_HLL : rs;
+  if (rs == AMUN_RS_HLLDM) rs = AMUN_RS_HLL;
   return rs;
 }
 
@@ -562,15 +565,9 @@ int amun_gpu_init(const amun_params* p) {
   if (p->eqsys != AMUN_EQ_HD && p->eqsys != AMUN_EQ_MHD && p->eqsys != AMUN_EQ_SRMHD && p->eqsys != AMUN_EQ_SRHD)
     return fail(100, "equation system not implemented");
   if (p->eos != AMUN_EOS_ADI && p->eos != AMUN_EOS_ISO) return fail(110, "equation of state not implemented");
-  if (p->eos == AMUN_EOS_ISO) {
-    // src/schemes.F90:159-300: the relativistic system is adiabatic only;
-    // of the isothermal solvers this library carries HLL (the default)
-    if (p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD)
-      return fail(110, "the relativistic systems have no isothermal equation of state");
-    if (p->riemann == AMUN_RS_ROE || (p->eqsys == AMUN_EQ_MHD && (p->riemann == AMUN_RS_HLLD ||
-                                                                   p->riemann == AMUN_RS_HLLDM)))
-      return fail(AMUN_E_UNSUPPORTED, "isothermal systems: HLL Riemann solver only");
-  }
+  // src/equations.F90:537-833: the relativistic systems are adiabatic only
+  if (p->eos == AMUN_EOS_ISO && (p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD))
+    return fail(110, "the relativistic systems have no isothermal equation of state");
   if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
     return fail(200, "reconstruction not implemented");
   int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;

@@ -86,10 +86,16 @@ static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
       case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
       default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
     }
-  } else {
-    // isothermal systems: HLL (riemann_hd_iso_hll, riemann_mhd_iso_hll)
-    (void)rs;
+  } else if constexpr (EQ == EQ_HD_ISO) {
+    if (rs == RS_ROE) return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
     return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+  } else {
+    switch (rs) {
+      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
+      case RS_HLLDM: return go_dir<R, U1T, EQ, REC, RS_HLLDM>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+    }
   }
 }
 

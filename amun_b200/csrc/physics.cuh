@@ -16,7 +16,7 @@
 namespace amun {
 
 enum { LIM_ZERO = 0, LIM_MM = 1, LIM_MC = 2, LIM_SB = 3, LIM_VL = 4, LIM_VA = 5 };
-enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_ROE = 3 };
+enum { RS_HLL = 0, RS_HLLC = 1, RS_HLLD = 2, RS_ROE = 3, RS_HLLDM = 4 };
 enum { REC_TVD = 0, REC_WENO5Z = 1 };
 
 // equation systems (src/equations.F90:322-833); *_ISO: isothermal equation
@@ -577,6 +577,304 @@ __device__ bool esystem_roe_mhd(R x, R y, const R* q, R* c, R* l, R* r, const Ph
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Isothermal solvers
+// ---------------------------------------------------------------------------
+// esystem_roe_hd_iso src/equations.F90:1655-1738.  l[var * 4 + wave],
+// r[wave * 4 + var]; entries the reference never sets stay zero.
+template <typename R>
+__device__ void esystem_roe_hd_iso(const R* q, R* c, R* l, R* r, const Phys<R>& P) {
+  using V = Var<EQ_HD_ISO>;
+  for (int m = 0; m < 16; ++m) { l[m] = R(0); r[m] = R(0); }
+  auto L = [&](int var, int wave) -> R& { return l[var * 4 + wave]; };
+  auto Rm = [&](int wave, int var) -> R& { return r[wave * 4 + var]; };
+  const R ch = R(0.5) / P.csnd;
+  L(V::VX, 0) = -ch; L(V::VY, 1) = R(1); L(V::VZ, 2) = R(1); L(V::VX, 3) = ch;
+  Rm(0, V::DN) = R(1); Rm(1, V::VY) = R(1); Rm(2, V::VZ) = R(1); Rm(3, V::DN) = R(1);
+  c[0] = q[V::VX] - P.csnd;
+  c[1] = q[V::VX];
+  c[2] = q[V::VX];
+  c[3] = q[V::VX] + P.csnd;
+  L(V::DN, 0) = ch * c[3];
+  L(V::DN, 1) = -q[V::VY];
+  L(V::DN, 2) = -q[V::VZ];
+  L(V::DN, 3) = -ch * c[0];
+  Rm(0, V::VX) = c[0]; Rm(0, V::VY) = q[V::VY]; Rm(0, V::VZ) = q[V::VZ];
+  Rm(3, V::VX) = c[3]; Rm(3, V::VY) = q[V::VY]; Rm(3, V::VZ) = q[V::VZ];
+}
+
+// esystem_roe_mhd_iso src/equations.F90:2552-2791.  l[var * 8 + wave],
+// r[wave * 8 + var]; waves 4 and 8 (entropy-like and psi) have zero
+// vectors.  Returns false (vectors not set) when the flow is supersonic.
+template <typename R>
+__device__ bool esystem_roe_mhd_iso(R x, R y, const R* q, R* c, R* l, R* r, const Phys<R>& P) {
+  using V = Var<EQ_MHD_ISO>;
+  R di = R(1) / q[V::DN];
+  R casq = q[V::BX] * q[V::BX] * di;
+  R ca = d_sqrt(casq);
+  R btsq = q[V::BY] * q[V::BY] + q[V::BZ] * q[V::BZ];
+  R bt_starsq = btsq * y;
+  R twid_csq = P.csnd2 + x;
+  R ct2 = bt_starsq * di;
+  R tsum = casq + ct2 + twid_csq;
+  R tdif = casq + ct2 - twid_csq;
+  R cf2_cs2 = d_sqrt(tdif * tdif + R(4) * twid_csq * ct2);
+  R cfsq = R(0.5) * (tsum + cf2_cs2);
+  R cf = d_sqrt(cfsq);
+  R cssq = twid_csq * casq / cfsq;
+  R cs = d_sqrt(cssq);
+  c[0] = q[V::VX] - cf; c[1] = q[V::VX] - ca; c[2] = q[V::VX] - cs; c[3] = q[V::VX];
+  c[4] = q[V::VX] + cs; c[5] = q[V::VX] + ca; c[6] = q[V::VX] + cf; c[7] = c[6];
+  if (c[0] >= R(0)) return false;
+  if (c[6] <= R(0)) return false;
+  for (int m = 0; m < 64; ++m) { l[m] = R(0); r[m] = R(0); }
+  auto L = [&](int var, int wave) -> R& { return l[var * 8 + wave]; };
+  auto Rm = [&](int wave, int var) -> R& { return r[wave * 8 + var]; };
+  R bt = d_sqrt(btsq);
+  R bt_star = d_sqrt(bt_starsq);
+  R bet2, bet3;
+  if (bt == R(0)) { bet2 = R(1); bet3 = R(0); }
+  else { bet2 = q[V::BY] / bt; bet3 = q[V::BZ] / bt; }
+  R bet2_star = bet2 / d_sqrt(y);
+  R bet3_star = bet3 / d_sqrt(y);
+  R bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+  R alpha_f, alpha_s;
+  if ((cfsq - cssq) == R(0)) { alpha_f = R(1); alpha_s = R(0); }
+  else if ((twid_csq - cssq) <= R(0)) { alpha_f = R(0); alpha_s = R(1); }
+  else if ((cfsq - twid_csq) <= R(0)) { alpha_f = R(1); alpha_s = R(0); }
+  else {
+    alpha_f = d_sqrt((twid_csq - cssq) / (cfsq - cssq));
+    alpha_s = d_sqrt((cfsq - twid_csq) / (cfsq - cssq));
+  }
+  R sqrtd = d_sqrt(q[V::DN]);
+  R s = fsign(R(1), q[V::BX]);
+  R twid_c = d_sqrt(twid_csq);
+  R qf = cf * alpha_f * s;
+  R qs = cs * alpha_s * s;
+  R af_prime = twid_c * alpha_f / sqrtd;
+  R as_prime = twid_c * alpha_s / sqrtd;
+  Rm(0, V::DN) = alpha_f;
+  Rm(0, V::VX) = alpha_f * c[0];
+  Rm(0, V::VY) = alpha_f * q[V::VY] + qs * bet2_star;
+  Rm(0, V::VZ) = alpha_f * q[V::VZ] + qs * bet3_star;
+  Rm(0, V::BY) = as_prime * bet2_star;
+  Rm(0, V::BZ) = as_prime * bet3_star;
+  Rm(1, V::VY) = -bet3;
+  Rm(1, V::VZ) = bet2;
+  Rm(1, V::BY) = -bet3 * s / sqrtd;
+  Rm(1, V::BZ) = bet2 * s / sqrtd;
+  Rm(2, V::DN) = alpha_s;
+  Rm(2, V::VX) = alpha_s * c[2];
+  Rm(2, V::VY) = alpha_s * q[V::VY] - qf * bet2_star;
+  Rm(2, V::VZ) = alpha_s * q[V::VZ] - qf * bet3_star;
+  Rm(2, V::BY) = -af_prime * bet2_star;
+  Rm(2, V::BZ) = -af_prime * bet3_star;
+  Rm(4, V::DN) = alpha_s;
+  Rm(4, V::VX) = alpha_s * c[4];
+  Rm(4, V::VY) = alpha_s * q[V::VY] + qf * bet2_star;
+  Rm(4, V::VZ) = alpha_s * q[V::VZ] + qf * bet3_star;
+  Rm(4, V::BY) = Rm(2, V::BY);
+  Rm(4, V::BZ) = Rm(2, V::BZ);
+  Rm(5, V::VY) = bet3;
+  Rm(5, V::VZ) = -bet2;
+  Rm(5, V::BY) = Rm(1, V::BY);
+  Rm(5, V::BZ) = Rm(1, V::BZ);
+  Rm(6, V::DN) = alpha_f;
+  Rm(6, V::VX) = alpha_f * c[6];
+  Rm(6, V::VY) = alpha_f * q[V::VY] - qs * bet2_star;
+  Rm(6, V::VZ) = alpha_f * q[V::VZ] - qs * bet3_star;
+  Rm(6, V::BY) = Rm(0, V::BY);
+  Rm(6, V::BZ) = Rm(0, V::BZ);
+  R norm = R(0.5) / twid_csq;
+  R cff = norm * alpha_f * cf;
+  R css = norm * alpha_s * cs;
+  qf = qf * norm;
+  qs = qs * norm;
+  R af = norm * af_prime * q[V::DN];
+  R as = norm * as_prime * q[V::DN];
+  R afpb = norm * af_prime * bt_star;
+  R aspb = norm * as_prime * bt_star;
+  R q2_star = bet2_star / bet_starsq;
+  R q3_star = bet3_star / bet_starsq;
+  R vqstr = q[V::VY] * q2_star + q[V::VZ] * q3_star;
+  L(V::DN, 0) = cff * c[6] - qs * vqstr - aspb;
+  L(V::VX, 0) = -cff;
+  L(V::VY, 0) = qs * q2_star;
+  L(V::VZ, 0) = qs * q3_star;
+  L(V::BY, 0) = as * q2_star;
+  L(V::BZ, 0) = as * q3_star;
+  L(V::DN, 1) = R(0.5) * (q[V::VY] * bet3 - q[V::VZ] * bet2);
+  L(V::VY, 1) = -R(0.5) * bet3;
+  L(V::VZ, 1) = R(0.5) * bet2;
+  L(V::BY, 1) = -R(0.5) * sqrtd * bet3 * s;
+  L(V::BZ, 1) = R(0.5) * sqrtd * bet2 * s;
+  L(V::DN, 2) = css * c[4] + qf * vqstr + afpb;
+  L(V::VX, 2) = -css;
+  L(V::VY, 2) = -qf * q2_star;
+  L(V::VZ, 2) = -qf * q3_star;
+  L(V::BY, 2) = -af * q2_star;
+  L(V::BZ, 2) = -af * q3_star;
+  L(V::DN, 4) = -css * c[2] - qf * vqstr + afpb;
+  L(V::VX, 4) = css;
+  L(V::VY, 4) = -L(V::VY, 2);
+  L(V::VZ, 4) = -L(V::VZ, 2);
+  L(V::BY, 4) = L(V::BY, 2);
+  L(V::BZ, 4) = L(V::BZ, 2);
+  L(V::DN, 5) = -L(V::DN, 1);
+  L(V::VY, 5) = -L(V::VY, 1);
+  L(V::VZ, 5) = -L(V::VZ, 1);
+  L(V::BY, 5) = L(V::BY, 1);
+  L(V::BZ, 5) = L(V::BZ, 1);
+  L(V::DN, 6) = -cff * c[0] + qs * vqstr - aspb;
+  L(V::VX, 6) = cff;
+  L(V::VY, 6) = -L(V::VY, 0);
+  L(V::VZ, 6) = -L(V::VZ, 0);
+  L(V::BY, 6) = L(V::BY, 0);
+  L(V::BZ, 6) = L(V::BZ, 0);
+  return true;
+}
+
+// riemann_mhd_iso_hlld src/schemes.F90:2007-2364 (Mignone 2007) and, with
+// MOD, riemann_mhd_iso_hlldm 2388-2751 (one density across the fan).  Entered
+// with sl < 0 < sr and wl = sl ul - fl, wr = sr ur - fr.
+template <bool MOD, typename R>
+__device__ void mhd_iso_hlld(const R* ql, const R* qr, const R* ul, const R* ur, const R* wl, const R* wr, R sl,
+                             R sr, R* f) {
+  using V = Var<EQ_MHD_ISO>;
+  constexpr int NV = V::NV;
+  constexpr int Dn = V::DN, Mx = V::VX, My = V::VY, Mz = V::VZ, Bx = V::BX, By = V::BY, Bz = V::BZ, Bp = V::BP;
+  const R srml = sr - sl;
+  R dn = wr[Dn] - wl[Dn];
+  const R sm = (wr[Mx] - wl[Mx]) / dn;
+  const R bx = ql[Bx];
+  const R b2 = ql[Bx] * qr[Bx];
+  const R slmm = sl - sm, srmm = sr - sm;
+  R dnl = R(0), dnr = R(0), sml, smr, dvl, dvr;
+  bool alfven;
+  if constexpr (MOD) {
+    dn = dn / srml;
+    const R ca2 = b2 / dn;
+    alfven = ca2 > R(1.0e-08) * d_max(sl * sl, sr * sr);
+    if (alfven) {
+      const R ca = d_sqrt(ca2);
+      sml = sm - ca;
+      smr = sm + ca;
+      dvl = slmm * slmm * dn - b2;
+      dvr = srmm * srmm * dn - b2;
+    }
+  } else {
+    dnl = wl[Dn] / slmm;
+    dnr = wr[Dn] / srmm;
+    alfven = b2 > R(1.0e-08) * d_max(dnl * (sl * sl), dnr * (sr * sr));
+    if (alfven) {
+      sml = sm - d_sqrt(b2 / dnl);
+      smr = sm + d_sqrt(b2 / dnr);
+      dvl = slmm * wl[Dn] - b2;
+      dvr = srmm * wr[Dn] - b2;
+    }
+  }
+  R ui[NV];
+  // the outer (Alfven-side) state on the left or right
+  auto star = [&](bool left) {
+    const R* w = left ? wl : wr;
+    const R mm = left ? slmm : srmm;
+    const R dv = left ? dvl : dvr;
+    const R d = MOD ? dn : (left ? dnl : dnr);
+    ui[Dn] = d;
+    ui[Mx] = d * sm;
+    ui[My] = d * (mm * w[My] - bx * w[By]) / dv;
+    ui[Mz] = d * (mm * w[Mz] - bx * w[Bz]) / dv;
+    ui[Bx] = bx;
+    if constexpr (MOD) {
+      ui[By] = (mm * d * w[By] - bx * w[My]) / dv;
+      ui[Bz] = (mm * d * w[Bz] - bx * w[Mz]) / dv;
+    } else {
+      ui[By] = (w[Dn] * w[By] - bx * w[My]) / dv;
+      ui[Bz] = (w[Dn] * w[Bz] - bx * w[Mz]) / dv;
+    }
+    ui[Bp] = left ? ul[Bp] : ur[Bp];
+  };
+  auto hll = [&]() {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+  };
+  if (alfven) {
+    if (d_min(dvl, dvr) > R(0)) {
+      if (sml >= R(0)) {
+        star(true);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+      } else if (smr <= R(0)) {
+        star(false);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        R wcl[NV], wcr[NV];
+        star(true);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+        star(false);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = (sml * wcr[v] - smr * wcl[v]) / (smr - sml);
+      }
+    } else if (dvl > R(0)) {
+      star(true);
+      if (sml >= R(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+      } else {
+        R wcl[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = (sml * wr[v] - sr * wcl[v]) / (sr - sml);
+      }
+    } else if (dvr > R(0)) {
+      star(false);
+      if (smr <= R(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+      } else {
+        R wcr[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = (sl * wcr[v] - smr * wl[v]) / (smr - sl);
+      }
+    } else {
+      hll();
+    }
+  } else if (b2 > R(0)) {
+    hll();
+  } else if (sm > R(0)) {
+    ui[Dn] = MOD ? dn : dnl;
+    ui[Mx] = ui[Dn] * sm;
+    ui[My] = wl[My] / slmm;
+    ui[Mz] = wl[Mz] / slmm;
+    ui[Bx] = R(0);
+    ui[By] = wl[By] / slmm;
+    ui[Bz] = wl[Bz] / slmm;
+    ui[Bp] = ul[Bp];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
+  } else if (sm < R(0)) {
+    ui[Dn] = MOD ? dn : dnr;
+    ui[Mx] = ui[Dn] * sm;
+    ui[My] = wr[My] / srmm;
+    ui[Mz] = wr[Mz] / srmm;
+    ui[Bx] = R(0);
+    ui[By] = wr[By] / srmm;
+    ui[Bz] = wr[Bz] / srmm;
+    ui[Bp] = ur[Bp];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
+  } else {
+    hll();
+  }
+}
+
 // One interface of the selected solver.  ql/qr are rotated primitive states
 // and are modified (GLM averaging) like the Fortran intent(inout) arrays.
 // riemann_hd_adi_hll  src/schemes.F90:1248-1341
@@ -602,7 +900,15 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     R qi[NV], ci[NV], al[NV], li[NV * NV], ri[NV * NV];
     R sdl = d_sqrt(ql[Dn]), sdr = d_sqrt(qr[Dn]), sds = sdl + sdr;
     bool full;
-    if constexpr (!V::MHD) {
+    if constexpr (V::ISO && !V::MHD) {
+      // riemann_hd_iso_roe src/schemes.F90:939-1057
+      qi[Dn] = sdl * sdr;
+      qi[Mx] = (sdl * ql[Mx] + sdr * qr[Mx]) / sds;
+      qi[My] = (sdl * ql[My] + sdr * qr[My]) / sds;
+      qi[Mz] = (sdl * ql[Mz] + sdr * qr[Mz]) / sds;
+      esystem_roe_hd_iso(qi, ci, li, ri, P);
+      full = true;
+    } else if constexpr (!V::MHD) {
       qi[Dn] = sdl * sdr;
       qi[Mx] = (sdl * ql[Mx] + sdr * qr[Mx]) / sds;
       qi[My] = (sdl * ql[My] + sdr * qr[My]) / sds;
@@ -617,7 +923,8 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       qi[Mx] = (sdl * ql[Mx] + sdr * qr[Mx]) / sds;
       qi[My] = (sdl * ql[My] + sdr * qr[My]) / sds;
       qi[Mz] = (sdl * ql[Mz] + sdr * qr[Mz]) / sds;
-      qi[En] = ((ul[En] + ql[V::PR] + pml) / sdl + (ur[En] + qr[V::PR] + pmr) / sdr) / sds;
+      if constexpr (!V::ISO) qi[En] = ((ul[En] + ql[V::PR] + pml) / sdl + (ur[En] + qr[V::PR] + pmr) / sdr) / sds;
+      (void)pml; (void)pmr;
       qi[V::BX] = ql[V::BX];
       qi[V::BY] = (sdr * ql[V::BY] + sdl * qr[V::BY]) / sds;
       qi[V::BZ] = (sdr * ql[V::BZ] + sdl * qr[V::BZ]) / sds;
@@ -625,7 +932,9 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       R t1 = ql[V::BY] - qr[V::BY], t2 = ql[V::BZ] - qr[V::BZ];
       R xx = R(0.5) * ((t1 * t1) + (t2 * t2)) / (sds * sds);
       R yy = R(0.5) * (ql[Dn] + qr[Dn]) / qi[Dn];
-      full = esystem_roe_mhd(xx, yy, qi, ci, li, ri, P);
+      // riemann_mhd_iso_roe src/schemes.F90:2778-2947 for the isothermal system
+      if constexpr (V::ISO) full = esystem_roe_mhd_iso(xx, yy, qi, ci, li, ri, P);
+      else full = esystem_roe_mhd(xx, yy, qi, ci, li, ri, P);
     }
     (void)full;
     if (ci[0] >= R(0)) {
@@ -697,6 +1006,10 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     if constexpr (RS == RS_HLL || V::SR) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+      return;
+    } else if constexpr (V::ISO) {
+      static_assert(V::MHD && (RS == RS_HLLD || RS == RS_HLLDM), "isothermal: HLL, Roe, HLLD, HLLD-M");
+      mhd_iso_hlld<RS == RS_HLLDM>(ql, qr, ul, ur, wl, wr, sl, sr, f);
       return;
     } else if constexpr (!V::MHD) {
       // HD HLLC

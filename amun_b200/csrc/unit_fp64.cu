@@ -315,8 +315,16 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
   } else if constexpr (EQ == EQ_SRMHD || EQ == EQ_SRHD) {
     if (u.rs == RS_HLLC) return riemann_dirs<EQ, RS_HLLC>(qs, f, d, P, s);
     return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
-  } else {
+  } else if constexpr (EQ == EQ_HD_ISO) {
+    if (u.rs == RS_ROE) return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
     return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
+  } else {
+    switch (u.rs) {
+      case RS_HLLD: return riemann_dirs<EQ, RS_HLLD>(qs, f, d, P, s);
+      case RS_HLLDM: return riemann_dirs<EQ, RS_HLLDM>(qs, f, d, P, s);
+      case RS_ROE: return riemann_dirs<EQ, RS_ROE>(qs, f, d, P, s);
+      default: return riemann_dirs<EQ, RS_HLL>(qs, f, d, P, s);
+    }
   }
 }
 
@@ -359,9 +367,15 @@ cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const doubl
     if (u.rs == RS_HLLC) line_riemann<EQ_SRHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
     else line_riemann<EQ_SRHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   } else if (u.eq == EQ_HD_ISO) {
-    line_riemann<EQ_HD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+    if (u.rs == RS_ROE) line_riemann<EQ_HD_ISO, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+    else line_riemann<EQ_HD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
   } else if (u.eq == EQ_MHD_ISO) {
-    line_riemann<EQ_MHD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
+    switch (u.rs) {
+      case RS_HLLD: line_riemann<EQ_MHD_ISO, RS_HLLD><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_HLLDM: line_riemann<EQ_MHD_ISO, RS_HLLDM><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      case RS_ROE: line_riemann<EQ_MHD_ISO, RS_ROE><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+      default: line_riemann<EQ_MHD_ISO, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P); break;
+    }
   } else {
     if (u.rs == RS_HLLC) line_riemann<EQ_SRMHD, RS_HLLC><<<grid, 128, 0, s>>>(n, ql, qr, f, P);
     else line_riemann<EQ_SRMHD, RS_HLL><<<grid, 128, 0, s>>>(n, ql, qr, f, P);

@@ -495,18 +495,18 @@ struct Oracle {
     if (iso) {
       if (sr) return 110;
       nv -= 1; ipr = ien = 0;
-      // of the isothermal solvers (src/schemes.F90:159-300) HLL is restated
-      if (p.rs == RS_ROE || (p.eqsys == EQ_MHD && (p.rs == RS_HLLD || p.rs == RS_HLLDM))) return 904;
-      p.rs = RS_HLL;
+      // isothermal solvers (src/schemes.F90:159-300): HD Roe or HLL; MHD
+      // HLLD, HLLD-M, Roe or HLL
+      if (p.eqsys == EQ_HD) p.rs = p.rs == RS_ROE ? RS_ROE : RS_HLL;
+      else if (p.rs == RS_HLLC || p.rs == RS_HLLCM) p.rs = RS_HLL;
     }
     csnd = p.csnd; csnd2 = csnd * csnd;
     // the relativistic systems offer HLL and HLLC ("hllcm" included,
     // src/schemes.F90:400-498); elsewhere "hllcm" names nothing
     if (sr) p.rs = (p.rs == RS_HLLC || p.rs == RS_HLLCM) ? RS_HLLC : RS_HLL;
     if (p.rs == RS_HLLCM) p.rs = RS_HLL;
-    if (p.rs == RS_HLLDM) p.rs = RS_HLL;  // HLLD-M exists for isothermal MHD only
+    if (p.rs == RS_HLLDM && !iso) p.rs = RS_HLL;  // HLLD-M exists for isothermal MHD only
     if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
-    // SRMHD offers HLL and HLLC only (src/schemes.F90:472-498)
     gamma = p.gamma; gammam1 = gamma - 1.0; gammam1i = 1.0 / gammam1;
     gammaxi = gammam1 / gamma;
     // evolution: CFL rescale and decay (src/evolution.F90:164-213)
@@ -1696,6 +1696,10 @@ struct Oracle {
     auto hll = [&]() { for (int v = 0; v < N; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml; };
     const int Dn = idn - 1, Mx = imx - 1, My = imy - 1, Mz = imz - 1, En = ien - 1;
     if (p.rs == RS_HLL) { hll(); return; }
+    if (iso) {
+      mhd_iso_hlld_point(p.rs == RS_HLLDM, ql, qr, ul, ur, wl, wr, sl, sr, f);
+      return;
+    }
     if (p.eqsys == EQ_HD) {
       // riemann_hd_adi_hllc src/schemes.F90:1366-1513
       double dn = wr[Dn] - wl[Dn];
@@ -2034,18 +2038,242 @@ struct Oracle {
     }
   }
 
+  // esystem_roe_hd_iso src/equations.F90:1655-1738 (same l/r layout as
+  // esystem_roe_hd)
+  void esystem_roe_hd_iso(const double* q, double* c, double* l, double* r) const {
+    const int N = nv;
+    std::fill(l, l + N * N, 0.0); std::fill(r, r + N * N, 0.0);
+    auto L = [&](int var, int wave) -> double& { return l[(var - 1) + N * (wave - 1)]; };
+    auto R = [&](int wave, int var) -> double& { return r[(wave - 1) + N * (var - 1)]; };
+    const double ch = 0.5 / csnd;
+    L(ivx, 1) = -ch; L(ivy, 2) = 1.0; L(ivz, 3) = 1.0; L(ivx, 4) = ch;
+    R(1, idn) = 1.0; R(2, ivy) = 1.0; R(3, ivz) = 1.0; R(4, idn) = 1.0;
+    c[0] = q[ivx - 1] - csnd; c[1] = q[ivx - 1]; c[2] = q[ivx - 1]; c[3] = q[ivx - 1] + csnd;
+    L(idn, 1) = ch * c[3];
+    L(idn, 2) = -q[ivy - 1];
+    L(idn, 3) = -q[ivz - 1];
+    L(idn, 4) = -ch * c[0];
+    R(1, ivx) = c[0]; R(1, ivy) = q[ivy - 1]; R(1, ivz) = q[ivz - 1];
+    R(4, ivx) = c[3]; R(4, ivy) = q[ivy - 1]; R(4, ivz) = q[ivz - 1];
+  }
+
+  // esystem_roe_mhd_iso src/equations.F90:2552-2791; false (vectors not
+  // set) when the flow is supersonic
+  bool esystem_roe_mhd_iso(double x, double y, const double* q, double* c, double* l, double* r) const {
+    const int N = nv;
+    double di = 1.0 / q[idn - 1];
+    double casq = q[ibx - 1] * q[ibx - 1] * di;
+    double ca = std::sqrt(casq);
+    double btsq = q[iby - 1] * q[iby - 1] + q[ibz - 1] * q[ibz - 1];
+    double bt_starsq = btsq * y;
+    double twid_csq = csnd2 + x;
+    double ct2 = bt_starsq * di;
+    double tsum = casq + ct2 + twid_csq;
+    double tdif = casq + ct2 - twid_csq;
+    double cf2_cs2 = std::sqrt(tdif * tdif + 4.0 * twid_csq * ct2);
+    double cfsq = 0.5 * (tsum + cf2_cs2);
+    double cf = std::sqrt(cfsq);
+    double cssq = twid_csq * casq / cfsq;
+    double cs = std::sqrt(cssq);
+    const double vx = q[ivx - 1];
+    c[0] = vx - cf; c[1] = vx - ca; c[2] = vx - cs; c[3] = vx; c[4] = vx + cs; c[5] = vx + ca; c[6] = vx + cf;
+    c[7] = c[6];
+    if (c[0] >= 0.0) return false;
+    if (c[6] <= 0.0) return false;
+    std::fill(l, l + N * N, 0.0); std::fill(r, r + N * N, 0.0);
+    auto L = [&](int var, int wave) -> double& { return l[(var - 1) + N * (wave - 1)]; };
+    auto R = [&](int wave, int var) -> double& { return r[(wave - 1) + N * (var - 1)]; };
+    double bt = std::sqrt(btsq), bt_star = std::sqrt(bt_starsq);
+    double bet2, bet3;
+    if (bt == 0.0) { bet2 = 1.0; bet3 = 0.0; }
+    else { bet2 = q[iby - 1] / bt; bet3 = q[ibz - 1] / bt; }
+    double bet2_star = bet2 / std::sqrt(y), bet3_star = bet3 / std::sqrt(y);
+    double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+    double alpha_f, alpha_s;
+    if ((cfsq - cssq) == 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+    else if ((twid_csq - cssq) <= 0.0) { alpha_f = 0.0; alpha_s = 1.0; }
+    else if ((cfsq - twid_csq) <= 0.0) { alpha_f = 1.0; alpha_s = 0.0; }
+    else {
+      alpha_f = std::sqrt((twid_csq - cssq) / (cfsq - cssq));
+      alpha_s = std::sqrt((cfsq - twid_csq) / (cfsq - cssq));
+    }
+    double sqrtd = std::sqrt(q[idn - 1]);
+    double sg = std::copysign(1.0, q[ibx - 1]);
+    double twid_c = std::sqrt(twid_csq);
+    double qf = cf * alpha_f * sg, qs = cs * alpha_s * sg;
+    double af_prime = twid_c * alpha_f / sqrtd, as_prime = twid_c * alpha_s / sqrtd;
+    const double vy = q[ivy - 1], vz = q[ivz - 1];
+    R(1, idn) = alpha_f; R(1, ivx) = alpha_f * c[0];
+    R(1, ivy) = alpha_f * vy + qs * bet2_star; R(1, ivz) = alpha_f * vz + qs * bet3_star;
+    R(1, iby) = as_prime * bet2_star; R(1, ibz) = as_prime * bet3_star;
+    R(2, ivy) = -bet3; R(2, ivz) = bet2;
+    R(2, iby) = -bet3 * sg / sqrtd; R(2, ibz) = bet2 * sg / sqrtd;
+    R(3, idn) = alpha_s; R(3, ivx) = alpha_s * c[2];
+    R(3, ivy) = alpha_s * vy - qf * bet2_star; R(3, ivz) = alpha_s * vz - qf * bet3_star;
+    R(3, iby) = -af_prime * bet2_star; R(3, ibz) = -af_prime * bet3_star;
+    R(5, idn) = alpha_s; R(5, ivx) = alpha_s * c[4];
+    R(5, ivy) = alpha_s * vy + qf * bet2_star; R(5, ivz) = alpha_s * vz + qf * bet3_star;
+    R(5, iby) = R(3, iby); R(5, ibz) = R(3, ibz);
+    R(6, ivy) = bet3; R(6, ivz) = -bet2;
+    R(6, iby) = R(2, iby); R(6, ibz) = R(2, ibz);
+    R(7, idn) = alpha_f; R(7, ivx) = alpha_f * c[6];
+    R(7, ivy) = alpha_f * vy - qs * bet2_star; R(7, ivz) = alpha_f * vz - qs * bet3_star;
+    R(7, iby) = R(1, iby); R(7, ibz) = R(1, ibz);
+    double norm = 0.5 / twid_csq;
+    double cff = norm * alpha_f * cf, css = norm * alpha_s * cs;
+    qf = qf * norm;
+    qs = qs * norm;
+    double af = norm * af_prime * q[idn - 1], as = norm * as_prime * q[idn - 1];
+    double afpb = norm * af_prime * bt_star, aspb = norm * as_prime * bt_star;
+    double q2_star = bet2_star / bet_starsq, q3_star = bet3_star / bet_starsq;
+    double vqstr = vy * q2_star + vz * q3_star;
+    L(idn, 1) = cff * c[6] - qs * vqstr - aspb;
+    L(ivx, 1) = -cff; L(ivy, 1) = qs * q2_star; L(ivz, 1) = qs * q3_star;
+    L(iby, 1) = as * q2_star; L(ibz, 1) = as * q3_star;
+    L(idn, 2) = 0.5 * (vy * bet3 - vz * bet2);
+    L(ivy, 2) = -0.5 * bet3; L(ivz, 2) = 0.5 * bet2;
+    L(iby, 2) = -0.5 * sqrtd * bet3 * sg; L(ibz, 2) = 0.5 * sqrtd * bet2 * sg;
+    L(idn, 3) = css * c[4] + qf * vqstr + afpb;
+    L(ivx, 3) = -css; L(ivy, 3) = -qf * q2_star; L(ivz, 3) = -qf * q3_star;
+    L(iby, 3) = -af * q2_star; L(ibz, 3) = -af * q3_star;
+    L(idn, 5) = -css * c[2] - qf * vqstr + afpb;
+    L(ivx, 5) = css; L(ivy, 5) = -L(ivy, 3); L(ivz, 5) = -L(ivz, 3);
+    L(iby, 5) = L(iby, 3); L(ibz, 5) = L(ibz, 3);
+    L(idn, 6) = -L(idn, 2); L(ivy, 6) = -L(ivy, 2); L(ivz, 6) = -L(ivz, 2);
+    L(iby, 6) = L(iby, 2); L(ibz, 6) = L(ibz, 2);
+    L(idn, 7) = -cff * c[0] + qs * vqstr - aspb;
+    L(ivx, 7) = cff; L(ivy, 7) = -L(ivy, 1); L(ivz, 7) = -L(ivz, 1);
+    L(iby, 7) = L(iby, 1); L(ibz, 7) = L(ibz, 1);
+    return true;
+  }
+
+  // riemann_mhd_iso_hlld src/schemes.F90:2007-2364 and, with mod,
+  // riemann_mhd_iso_hlldm 2388-2751; entered with sl < 0 < sr
+  void mhd_iso_hlld_point(bool mod, const double* ql, const double* qr, const double* ul, const double* ur,
+                          const double* wl, const double* wr, double sl, double sr, double* f) const {
+    const int N = nv;
+    const int Dn = idn - 1, Mx = imx - 1, My = imy - 1, Mz = imz - 1;
+    const int Bx = ibx - 1, By = iby - 1, Bz = ibz - 1, Bp = ibp - 1;
+    double srml = sr - sl;
+    double dn = wr[Dn] - wl[Dn];
+    double sm = (wr[Mx] - wl[Mx]) / dn;
+    double bx = ql[Bx], b2 = ql[Bx] * qr[Bx];
+    double slmm = sl - sm, srmm = sr - sm;
+    double dnl = 0.0, dnr = 0.0, sml = 0.0, smr = 0.0, dvl = 0.0, dvr = 0.0;
+    bool alfven;
+    if (mod) {
+      dn = dn / srml;
+      double ca2 = b2 / dn;
+      alfven = ca2 > 1.0e-08 * fmax2(sl * sl, sr * sr);
+      if (alfven) {
+        double ca = std::sqrt(ca2);
+        sml = sm - ca; smr = sm + ca;
+        dvl = slmm * slmm * dn - b2;
+        dvr = srmm * srmm * dn - b2;
+      }
+    } else {
+      dnl = wl[Dn] / slmm;
+      dnr = wr[Dn] / srmm;
+      alfven = b2 > 1.0e-08 * fmax2(dnl * (sl * sl), dnr * (sr * sr));
+      if (alfven) {
+        sml = sm - std::sqrt(b2 / dnl);
+        smr = sm + std::sqrt(b2 / dnr);
+        dvl = slmm * wl[Dn] - b2;
+        dvr = srmm * wr[Dn] - b2;
+      }
+    }
+    double ui[8], wcl[8], wcr[8];
+    auto star = [&](bool left) {
+      const double* w = left ? wl : wr;
+      double mm = left ? slmm : srmm, dv = left ? dvl : dvr;
+      double d = mod ? dn : (left ? dnl : dnr);
+      ui[Dn] = d;
+      ui[Mx] = d * sm;
+      ui[My] = d * (mm * w[My] - bx * w[By]) / dv;
+      ui[Mz] = d * (mm * w[Mz] - bx * w[Bz]) / dv;
+      ui[Bx] = bx;
+      if (mod) {
+        ui[By] = (mm * d * w[By] - bx * w[My]) / dv;
+        ui[Bz] = (mm * d * w[Bz] - bx * w[Mz]) / dv;
+      } else {
+        ui[By] = (w[Dn] * w[By] - bx * w[My]) / dv;
+        ui[Bz] = (w[Dn] * w[Bz] - bx * w[Mz]) / dv;
+      }
+      ui[Bp] = left ? ul[Bp] : ur[Bp];
+    };
+    auto hll = [&]() { for (int v = 0; v < N; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml; };
+    if (alfven) {
+      if (fmin2(dvl, dvr) > 0.0) {
+        if (sml >= 0.0) {
+          star(true);
+          for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+        } else if (smr <= 0.0) {
+          star(false);
+          for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+        } else {
+          star(true);
+          for (int v = 0; v < N; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+          star(false);
+          for (int v = 0; v < N; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+          for (int v = 0; v < N; ++v) f[v] = (sml * wcr[v] - smr * wcl[v]) / (smr - sml);
+        }
+      } else if (dvl > 0.0) {
+        star(true);
+        if (sml >= 0.0) {
+          for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+        } else {
+          for (int v = 0; v < N; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
+          for (int v = 0; v < N; ++v) f[v] = (sml * wr[v] - sr * wcl[v]) / (sr - sml);
+        }
+      } else if (dvr > 0.0) {
+        star(false);
+        if (smr <= 0.0) {
+          for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+        } else {
+          for (int v = 0; v < N; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
+          for (int v = 0; v < N; ++v) f[v] = (sl * wcr[v] - smr * wl[v]) / (smr - sl);
+        }
+      } else {
+        hll();
+      }
+    } else if (b2 > 0.0) {
+      hll();
+    } else if (sm > 0.0) {
+      ui[Dn] = mod ? dn : dnl;
+      ui[Mx] = ui[Dn] * sm;
+      ui[My] = wl[My] / slmm; ui[Mz] = wl[Mz] / slmm;
+      ui[Bx] = 0.0; ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm;
+      ui[Bp] = ul[Bp];
+      for (int v = 0; v < N; ++v) f[v] = sl * ui[v] - wl[v];
+    } else if (sm < 0.0) {
+      ui[Dn] = mod ? dn : dnr;
+      ui[Mx] = ui[Dn] * sm;
+      ui[My] = wr[My] / srmm; ui[Mz] = wr[Mz] / srmm;
+      ui[Bx] = 0.0; ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm;
+      ui[Bp] = ur[Bp];
+      for (int v = 0; v < N; ++v) f[v] = sr * ui[v] - wr[v];
+    } else {
+      hll();
+    }
+  }
+
   void roe_point(const double* ql, const double* qr, const double* ul, const double* ur,
                  const double* fl, const double* fr, double* f) const {
     const int N = nv;
     double qi_[9], ci[9], al[9], li[81], ri[81];
     double sdl = std::sqrt(ql[idn - 1]), sdr = std::sqrt(qr[idn - 1]), sds = sdl + sdr;
     if (p.eqsys == EQ_HD) {
+      // riemann_hd_iso_roe src/schemes.F90:939-1057 when isothermal
       qi_[idn - 1] = sdl * sdr;
       qi_[ivx - 1] = (sdl * ql[ivx - 1] + sdr * qr[ivx - 1]) / sds;
       qi_[ivy - 1] = (sdl * ql[ivy - 1] + sdr * qr[ivy - 1]) / sds;
       qi_[ivz - 1] = (sdl * ql[ivz - 1] + sdr * qr[ivz - 1]) / sds;
-      qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1]) / sdl + (ur[ien - 1] + qr[ipr - 1]) / sdr) / sds;
-      esystem_roe_hd(qi_, ci, li, ri);
+      if (iso) {
+        esystem_roe_hd_iso(qi_, ci, li, ri);
+      } else {
+        qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1]) / sdl + (ur[ien - 1] + qr[ipr - 1]) / sdr) / sds;
+        esystem_roe_hd(qi_, ci, li, ri);
+      }
       if (ci[0] >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
       if (ci[N - 1] <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
       for (int v = 0; v < N; ++v) al[v] = 0.0;
@@ -2071,7 +2299,7 @@ struct Oracle {
     qi_[ivx - 1] = (sdl * ql[ivx - 1] + sdr * qr[ivx - 1]) / sds;
     qi_[ivy - 1] = (sdl * ql[ivy - 1] + sdr * qr[ivy - 1]) / sds;
     qi_[ivz - 1] = (sdl * ql[ivz - 1] + sdr * qr[ivz - 1]) / sds;
-    qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1] + pml) / sdl + (ur[ien - 1] + qr[ipr - 1] + pmr) / sdr) / sds;
+    if (!iso) qi_[ipr - 1] = ((ul[ien - 1] + ql[ipr - 1] + pml) / sdl + (ur[ien - 1] + qr[ipr - 1] + pmr) / sdr) / sds;
     qi_[ibx - 1] = ql[ibx - 1];
     qi_[iby - 1] = (sdr * ql[iby - 1] + sdl * qr[iby - 1]) / sds;
     qi_[ibz - 1] = (sdr * ql[ibz - 1] + sdl * qr[ibz - 1]) / sds;
@@ -2079,7 +2307,9 @@ struct Oracle {
     double t1 = ql[iby - 1] - qr[iby - 1], t2 = ql[ibz - 1] - qr[ibz - 1];
     double xx = 0.5 * ((t1 * t1) + (t2 * t2)) / (sds * sds);
     double yy = 0.5 * (ql[idn - 1] + qr[idn - 1]) / qi_[idn - 1];
-    esystem_roe_mhd(xx, yy, qi_, ci, li, ri);
+    // riemann_mhd_iso_roe src/schemes.F90:2778-2947 when isothermal
+    if (iso) esystem_roe_mhd_iso(xx, yy, qi_, ci, li, ri);
+    else esystem_roe_mhd(xx, yy, qi_, ci, li, ri);
     if (ci[0] >= 0.0) { for (int v = 0; v < N; ++v) f[v] = fl[v]; return; }
     if (ci[N - 1] <= 0.0) { for (int v = 0; v < N; ++v) f[v] = fr[v]; return; }
     f[ibx - 1] = fl[ibx - 1];
@@ -2087,7 +2317,8 @@ struct Oracle {
     for (int v = 0; v < N; ++v) al[v] = 0.0;
     for (int pp = 0; pp < N; ++pp)
       for (int v = 0; v < N; ++v) al[v] = al[v] + li[pp + N * v] * (ur[pp] - ul[pp]);
-    const int vs[7] = {idn - 1, imx - 1, imy - 1, imz - 1, ien - 1, iby - 1, ibz - 1};
+    std::vector<int> vs = {idn - 1, imx - 1, imy - 1, imz - 1, iby - 1, ibz - 1};
+    if (!iso) vs.insert(vs.begin() + 4, ien - 1);
     for (int v : vs) f[v] = 0.5 * (fl[v] + fr[v]);
     if (qi_[ivx - 1] >= 0.0) {
       for (int pp = 0; pp < N; ++pp) {

@@ -34,11 +34,12 @@ def smooth_iso(mesh, nv, seed=0, amp=0.3):
     return q
 
 
-@pytest.mark.parametrize("eq", ["hd", "mhd"])
-def test_pointwise_and_riemann(eq):
+@pytest.mark.parametrize("eq,rs", [("hd", "hll"), ("hd", "roe"), ("mhd", "hll"), ("mhd", "roe"), ("mhd", "hlld"),
+                                   ("mhd", "hlldm")])
+def test_pointwise_and_riemann(eq, rs):
     from amun_b200.solver import Simulation
     import oracle
-    p = iso_params(eq, ncells=8, csnd=0.7)
+    p = iso_params(eq, ncells=8, csnd=0.7, riemann_solver=rs)
     s, o = Simulation(p), oracle.Oracle(p)
     try:
         assert s.nv == o.nv == (4 if eq == "hd" else 8)
@@ -56,17 +57,23 @@ def test_pointwise_and_riemann(eq):
         qr[:500, 1] += 6.0
         ql[500:1000, 1] -= 6.0
         qr[500:1000, 1] -= 6.0
-        assert_same(s.riemann(ql, qr), o.riemann(ql, qr), "riemann")
+        if s.nv == 8:
+            ql[1000:1500, 4] = qr[1000:1500, 4] = 0.0      # Bx = 0
+            ql[1500:2000, 4] = qr[1500:2000, 4] = 1e-6     # weak Bx
+            ql[2000:2500, 5:7] = qr[2000:2500, 5:7] = 0.0  # no transverse field
+            ql[2000:2500, 4] = qr[2000:2500, 4] = 3.0
+        assert_same(s.riemann(ql, qr), o.riemann(ql, qr), f"riemann {rs}")
     finally:
         s.close()
 
 
 @pytest.mark.parametrize("ndims", [2, 3])
-@pytest.mark.parametrize("eq,rec", [("hd", "tvd"), ("mhd", "weno5z"), ("mhd", "tvd")])
-def test_update_flux_block(ndims, eq, rec):
+@pytest.mark.parametrize("eq,rec,rs", [("hd", "tvd", "hll"), ("hd", "weno5z", "roe"), ("mhd", "weno5z", "hll"),
+                                       ("mhd", "tvd", "hlld"), ("mhd", "weno5z", "hlldm"), ("mhd", "tvd", "roe")])
+def test_update_flux_block(ndims, eq, rec, rs):
     from amun_b200.solver import Simulation
     import oracle
-    p = iso_params(eq, rec, ndims=ndims, ncells=8 if ndims == 3 else 12, csnd=0.6)
+    p = iso_params(eq, rec, ndims=ndims, ncells=8 if ndims == 3 else 12, csnd=0.6, riemann_solver=rs)
     s, o = Simulation(p), oracle.Oracle(p)
     try:
         rng = np.random.default_rng(5)
@@ -79,12 +86,13 @@ def test_update_flux_block(ndims, eq, rec):
         s.close()
 
 
-@pytest.mark.parametrize("eq,rec,ta,nd", [("hd", "tvd", "rk2", 2), ("hd", "weno5z", "rk3", 3),
-                                         ("mhd", "weno5z", "rk3", 2), ("mhd", "tvd", "ssprk(4,3)", 3)])
-def test_steps_match_oracle(eq, rec, ta, nd):
+@pytest.mark.parametrize("eq,rec,ta,nd,rs", [("hd", "tvd", "rk2", 2, "hll"), ("hd", "weno5z", "rk3", 3, "roe"),
+                                            ("mhd", "weno5z", "rk3", 2, "hlld"), ("mhd", "tvd", "ssprk(4,3)", 3, "hll"),
+                                            ("mhd", "weno5z", "rk2", 3, "hlldm"), ("mhd", "tvd", "rk3", 2, "roe")])
+def test_steps_match_oracle(eq, rec, ta, nd, rs):
     from amun_b200.solver import Simulation
     import oracle
-    p = iso_params(eq, rec, ta, ndims=nd, ncells=16 if nd == 2 else 8, maxlev=2, csnd=0.8)
+    p = iso_params(eq, rec, ta, ndims=nd, ncells=16 if nd == 2 else 8, maxlev=2, csnd=0.8, riemann_solver=rs)
     mesh = UniformMesh(geometry(p))
     s, o = Simulation(p), oracle.Oracle(p)
     try:
@@ -95,7 +103,7 @@ def test_steps_match_oracle(eq, rec, ta, nd):
             ts, dts = s.advance(1.0e30)
             to, dto = o.advance(1.0e30)
             assert ts == to and dts == dto
-        assert_same(s.conserved(), o.cons(), f"iso {eq}/{rec}/{ta}")
+        assert_same(s.conserved(), o.cons(), f"iso {eq}/{rec}/{ta}/{rs}")
         s.run(3, 1.0e30, graph=True)
         for _ in range(3):
             o.advance(1.0e30)

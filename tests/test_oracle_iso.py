@@ -162,22 +162,51 @@ def test_isothermal_mhd_without_field_is_isothermal_hd(oracle_mod):
     assert np.all(pm.cons()[..., 4:] == 0.0)
 
 
-@pytest.mark.parametrize("eq,rs", [("hd", "roe"), ("mhd", "hlld"), ("mhd", "hlldm"), ("mhd", "roe")])
-def test_unrestated_isothermal_solvers_are_refused(oracle_mod, eq, rs):
-    with pytest.raises(ValueError, match="iret"):
-        oracle_mod.Oracle(params(eq, "tvd", rs, equation_of_state="iso"))
-
-
 def test_relativistic_isothermal_is_refused(oracle_mod):
     with pytest.raises(ValueError, match="iret"):
         oracle_mod.Oracle(params("srmhd", "tvd", "hll", equation_of_state="iso"))
 
 
-@pytest.mark.parametrize("eq,rs,code", [("hd", "roe", 904), ("mhd", "hlld", 904), ("srmhd", "hll", 110)])
-def test_library_refuses_the_same_before_touching_a_device(eq, rs, code):
+@pytest.mark.parametrize("eq,code", [("srmhd", 110), ("srhd", 110)])
+def test_library_refuses_the_same_before_touching_a_device(eq, code):
     """amun_gpu_init checks the system before it looks for a device."""
     from amun_b200 import _native as N
     from amun_b200.params import to_native
-    p = to_native(params(eq, "tvd", rs, equation_of_state="iso"))
+    p = to_native(params(eq, "tvd", "hll", equation_of_state="iso"))
     assert p.eos == N.AMUN_EOS_ISO
     assert N.lib().amun_gpu_init(C.byref(p)) == code
+
+
+@pytest.mark.parametrize("eq,rs", [("hd", "roe"), ("mhd", "roe"), ("mhd", "hlld"), ("mhd", "hlldm")])
+def test_solvers_agree_with_hll_on_smooth_flow(oracle_mod, eq, rs):
+    """Every isothermal solver is consistent (f(q, q) = F(q)) and, on a
+    smooth flow, stays within the discretisation error of HLL."""
+    cs = 0.8
+    o = oracle_mod.Oracle(iso_params(eq, csnd=cs, riemann_solver=rs))
+    o.set_cmax(1.7)
+    rng = np.random.default_rng(9)
+    q = iso_prim(rng, 400, o.nv)
+    f = o.riemann(q, q)
+    fp, _, _ = o.fluxspeed(q, o.prim2cons(q))
+    assert np.allclose(f, fp, rtol=1e-11, atol=1e-11)
+    kw = dict(ncells=32, csnd=cs, cfl=0.4)
+    a = oracle_mod.Oracle(iso_params(eq, "weno5z", "rk3", riemann_solver=rs, **kw))
+    b = oracle_mod.Oracle(iso_params(eq, "weno5z", "rk3", **kw))
+    NZ, NY, NX, nv = a.field_shape()
+    y, x = np.meshgrid((np.arange(NY) + 0.5) / NY, (np.arange(NX) + 0.5) / NX, indexing="ij")
+    q0 = np.zeros(a.field_shape())
+    q0[0, ..., 0] = 1.0 + 0.2 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y)
+    q0[0, ..., 1] = 0.3 * np.sin(2 * np.pi * y)
+    q0[0, ..., 2] = 0.2 * np.cos(2 * np.pi * x)
+    if nv == 8:
+        q0[0, ..., 4] = 0.5
+        q0[0, ..., 5] = 0.3 * np.sin(2 * np.pi * x)
+    a.set_prim(q0)
+    b.set_prim(q0)
+    dt = 0.4 * (1.0 / 32) / 2.5
+    for _ in range(8):
+        a.advance(dt)
+        b.advance(dt)
+    d = np.abs(a.cons()[..., 0] - b.cons()[..., 0]).mean()
+    # ~1e-8 here, against a change of ~6e-3 of the state itself
+    assert 0.0 < d < 1e-6, d
