@@ -313,6 +313,7 @@ MethodConst method_const() {
   m.tol = C.p.tolerance; m.pmin = C.p.pmin; m.nrmax = C.p.nr_maxit; m.nrext = C.p.nr_extra;
   m.plim = C.p.prolongation_limiter;
   m.csnd = C.p.csnd;
+  m.c2p = C.p.c2p;
   m.states_4vec = relativistic() ? C.p.states_4vec : 0;
   return m;
 }
@@ -443,7 +444,7 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.tol = C.p.tolerance; u.pmin = C.p.pmin; u.nrmax = C.p.nr_maxit; u.nrext = C.p.nr_extra;
   u.states_4vec = relativistic() ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
-  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd;
+  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd; u.c2p = C.p.c2p;
   return u;
 }
 
@@ -485,6 +486,7 @@ void amun_gpu_default_params(amun_params* p) {
   p->states_4vec = 0;
   p->eos = AMUN_EOS_ADI;
   p->csnd = 1.0;
+  p->c2p = AMUN_C2P_1DW;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -504,8 +506,11 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"iso", "ISO", "isothermal", "ISOTHERMAL"})) p->eos = AMUN_EOS_ISO;
     else return fail(110, std::string("equation of state not implemented: ") + v);
   } else if (k == "primitive_solver") {
-    if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"}))
-      return fail(AMUN_E_UNSUPPORTED, std::string("primitive solver not implemented here: ") + v);
+    // read for every system, checked by the relativistic ones only
+    if (is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"})) p->c2p = AMUN_C2P_1DW;
+    else if (is_one_of(v, {"2dwv", "2Dwv", "2D(w,v)", "2D(W,v)"})) p->c2p = AMUN_C2P_2DWV;
+    else if (is_one_of(v, {"2dwu", "2Dwu", "2D(w,u)", "2D(W,u)"})) p->c2p = AMUN_C2P_2DWU;
+    else p->c2p = -1;
   } else if (k == "tolerance") p->tolerance = atof(v);
   else if (k == "pmin") p->pmin = atof(v);
   else if (k == "nr_maxit") p->nr_maxit = atoi(v);
@@ -568,6 +573,9 @@ int amun_gpu_init(const amun_params* p) {
   // src/equations.F90:537-833: the relativistic systems are adiabatic only
   if (p->eos == AMUN_EOS_ISO && (p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD))
     return fail(110, "the relativistic systems have no isothermal equation of state");
+  if ((p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD) &&
+      (p->c2p < AMUN_C2P_1DW || p->c2p > AMUN_C2P_2DWU))
+    return fail(110, "primitive solver not implemented");
   if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
     return fail(200, "reconstruction not implemented");
   int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;

@@ -69,6 +69,7 @@ template <typename R> struct Phys {
   // (src/equations.F90:184-201, 313-318)
   double tol, pmin;
   int nrmax, nrext;
+  int c2p;  // recovery method: 0 1D(W), 1 2D(W,v^2), 2 2D(W,u^2) (primitive_solver)
 };
 
 template <typename R> __device__ __forceinline__ R d_abs(R x) { return x < R(0) ? -x : (x == R(0) ? R(0) : x); }

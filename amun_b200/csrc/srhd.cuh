@@ -1,5 +1,5 @@
 // srhd.cuh -- special relativistic hydrodynamics (adiabatic): conversions,
-// fluxes and signal speeds, the 1D(W) Newton recovery and the HLLC solver.
+// fluxes and signal speeds, the Newton recoveries and the HLLC solver.
 // Included from physics.cuh after Phys and the algebra of srmhd.cuh.
 // Variables (src/equations.F90:537-600): dens, velx, vely, velz, pres; the
 // conserved slots are D, m_x, m_y, m_z, E - D.
@@ -31,22 +31,17 @@ __device__ __forceinline__ void srhd_nr_function(double mm, double en, double dn
   if (df) *df = 1.0 - gammaxi * (1.0 + (1.0 - dn / (vs * w)) * vv);
 }
 
-// cons2prim_srhd_adi src/equations.F90:3550-3639 with nr_iterate_srhd_adi_1dw
-// 3911-4091.  Returns false when no physical state was found; then only
-// q[4] is written (0) and the rest keeps the previous primitive state, like
-// the reference writing into the caller's q.  Where the lower bracket is
-// itself the root (f(wl) == 0) the reference leaves v^2 from an earlier
-// call; here v^2 = m^2 / W^2 of that root.  Every loop is bounded by nr_maxit
-// and nr_extra.
-__device__ inline bool cons2prim_srhd(const double* u, double* q, const Phys<double>& P) {
-  const double mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
-  const double en = u[4] + u[0];
-  const double dn = u[0];
+// nr_iterate_srhd_adi_1dw src/equations.F90:3911-4091.  Where the lower
+// bracket is itself the root (f(wl) == 0) the reference leaves v^2 from an
+// earlier call; here v^2 = m^2 / W^2 of that root.  Every loop is bounded by
+// nr_maxit and nr_extra.
+__device__ inline bool srhd_iterate_1dw(double mm, double en, double dn, const Phys<double>& P, double& w,
+                                        double& vv) {
   double wl = sqrt(mm + dn * dn);
-  if (!(en > wl)) { q[4] = 0.0; return false; }  // not a physical state
+  if (!(en > wl)) return false;  // not a physical state
   wl = wl + P.gammaxi * P.pmin;
   double wu = en + P.pmin;
-  double fl, fu, w;
+  double fl, fu;
   srhd_nr_function(mm, en, dn, wl, P.gammaxi, fl, nullptr);
   if (fl < 0.0) {
     if (wu <= wl) wu = 2.0 * wl;
@@ -61,7 +56,7 @@ __device__ inline bool cons2prim_srhd(const double* u, double* q, const Phys<dou
       srhd_nr_function(mm, en, dn, wu, P.gammaxi, fu, nullptr);
       keep = (fl * fu > 0.0) && it > 0;
     }
-    if (!(it > 0 && fu >= 0.0)) { q[4] = 0.0; return false; }  // no upper bracket
+    if (!(it > 0 && fu >= 0.0)) return false;  // no upper bracket
     w = wl - fl * (wu - wl) / (fu - fl);
     keep = true;
     it = P.nrmax;
@@ -83,10 +78,137 @@ __device__ inline bool cons2prim_srhd(const double* u, double* q, const Phys<dou
   } else if (fl == 0.0) {
     w = wl;
   } else {
-    q[4] = 0.0;  // the root lies below the lower bracket
+    return false;  // the root lies below the lower bracket
+  }
+  vv = mm / (w * w);
+  return true;
+}
+
+// the brackets of the two-variable recoveries (nr_iterate_srhd_adi_2dwv
+// src/equations.F90:4128-4215 and 2dwu 4360-4447): lower W from |m| and D,
+// upper doubled until it lies above, then doubled until f changes sign
+__device__ inline bool srhd_brackets_2d(double mm, double en, double dn, const Phys<double>& P, double& wl,
+                                        double& wc) {
+  wl = sqrt(mm + dn * dn) + P.gammaxi * P.pmin;
+  double wu = en + P.pmin;
+  bool keep = wl >= wu;
+  int it = P.nrmax;
+  while (keep) {
+    wu = 2.0 * wu;
+    it = it - 1;
+    keep = (wl >= wu) && it > 0;
+  }
+  if (it <= 0) return false;
+  double fl, fu;
+  srhd_nr_function(mm, en, dn, wl, P.gammaxi, fl, nullptr);
+  srhd_nr_function(mm, en, dn, wu, P.gammaxi, fu, nullptr);
+  keep = fl * fu > 0.0;
+  it = P.nrmax;
+  while (keep) {
+    wl = wu;
+    fl = fu;
+    wu = 2.0 * wu;
+    srhd_nr_function(mm, en, dn, wu, P.gammaxi, fu, nullptr);
+    it = it - 1;
+    keep = (fl * fu > 0.0) && it > 0;
+  }
+  if (it <= 0) return false;
+  wc = wl - fl * (wu - wl) / (fu - fl);
+  return true;
+}
+
+// nr_iterate_srhd_adi_2dwv src/equations.F90:4128-4330: Newton on (W, v^2)
+__device__ inline bool srhd_iterate_2dwv(double mm, double en, double dn, const Phys<double>& P, double& w,
+                                         double& vv) {
+  double wl;
+  if (!srhd_brackets_2d(mm, en, dn, P, wl, w)) return false;
+  vv = mm / (w * w);
+  bool keep = true;
+  int it = P.nrmax, cn = P.nrext;
+  while (keep) {
+    double ww = w * w;
+    double vm = 1.0 - vv;
+    double vs = sqrt(vm);
+    double gd = P.gammaxi * dn;
+    double gv = 1.0 - P.gammaxi * vm;
+    double f = gv * w - en + gd * vs;
+    double g = vv * ww - mm;
+    double dfw = gv;
+    double dfv = P.gammaxi * w - 0.5 * gd / vs;
+    double dgw = 2.0 * vv * w;
+    double dgv = ww;
+    double det = dfw * dgv - dfv * dgw;
+    double jfw = dgv / det, jgw = -dfv / det, jfv = -dgw / det, jgv = dfw / det;
+    double dw = f * jfw + g * jgw;
+    double dv = f * jfv + g * jgv;
+    w = w - dw;
+    vv = vv - dv;
+    if (w < wl) return false;
+    if (vv < 0.0 || vv >= 1.0) return false;
+    double err = fmax(fabs(dw / w), fabs(dv));
+    if (err < P.tol) { keep = cn > 0; cn = cn - 1; }
+    else keep = it > 0;
+    it = it - 1;
+    if (it < -(P.nrext + 2)) break;  // unreachable bound, kept for the loop limit
+  }
+  return true;
+}
+
+// nr_iterate_srhd_adi_2dwu src/equations.F90:4360-4566: Newton on (W, u^2)
+__device__ inline bool srhd_iterate_2dwu(double mm, double en, double dn, const Phys<double>& P, double& w,
+                                         double& vv) {
+  double wl;
+  if (!srhd_brackets_2d(mm, en, dn, P, wl, w)) return false;
+  double uu = mm / (w * w - mm);
+  bool keep = true;
+  int it = P.nrmax, cn = P.nrext;
+  while (keep) {
+    double ww = w * w;
+    double up = 1.0 + uu;
+    double gm = sqrt(up);
+    double gd = P.gammaxi * dn;
+    double f = (up - P.gammaxi) * w - up * en + gm * gd;
+    double g = uu * ww - up * mm;
+    double dfw = up - P.gammaxi;
+    double dfu = w - en + 0.5 * gd / gm;
+    double dgw = 2.0 * uu * w;
+    double dgu = ww - mm;
+    double det = dfw * dgu - dfu * dgw;
+    double jfw = dgu / det, jgw = -dfu / det, jfu = -dgw / det, jgu = dfw / det;
+    double dw = f * jfw + g * jgw;
+    double du = f * jfu + g * jgu;
+    w = w - dw;
+    uu = uu - du;
+    if (w < wl) return false;
+    if (uu < 0.0) return false;
+    double err = fmax(fabs(dw / w), fabs(du));
+    if (err < P.tol) { keep = cn > 0; cn = cn - 1; }
+    else keep = it > 0;
+    it = it - 1;
+    if (it < -(P.nrext + 2)) break;  // unreachable bound, kept for the loop limit
+  }
+  vv = uu / (1.0 + uu);
+  return true;
+}
+
+// cons2prim_srhd_adi src/equations.F90:3550-3639 with the recovery chosen by
+// primitive_solver (src/equations.F90:605-640).  Returns false when no
+// physical state was found; then only q[4] is written (0) and the rest keeps
+// the previous primitive state, like the reference writing into the
+// caller's q.
+__device__ inline bool cons2prim_srhd(const double* u, double* q, const Phys<double>& P) {
+  const double mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  const double en = u[4] + u[0];
+  const double dn = u[0];
+  double w, vv;
+  bool info;
+  if (P.c2p == 1) info = srhd_iterate_2dwv(mm, en, dn, P, w, vv);
+  else if (P.c2p == 2) info = srhd_iterate_2dwu(mm, en, dn, P, w, vv);
+  else info = srhd_iterate_1dw(mm, en, dn, P, w, vv);
+  if (!info) {
+    q[4] = 0.0;
     return false;
   }
-  const double vv = mm / (w * w);
   const double vm = 1.0 - vv;
   const double vs = sqrt(vm);
   q[0] = dn * vs;

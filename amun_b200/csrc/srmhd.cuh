@@ -356,21 +356,21 @@ __device__ inline bool sr_brackets(double mm, double bb, double mb, double en, d
   return false;
 }
 
-// cons2prim_srmhd_adi src/equations.F90:4671-4790 with
-// nr_iterate_srmhd_adi_1dw 5665-5788.  Returns false when the recovery failed
-// or gave p <= 0; then only q[PR] is written (0), like the reference.  All
-// loops are bounded by nr_maxit, nr_extra and the bracket doubling limit.
-__device__ inline bool cons2prim_sr(const double* u, double* q, const Phys<double>& P) {
-  double mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
-  double mb = u[1] * u[4] + u[2] * u[5] + u[3] * u[6];
-  double bb = u[4] * u[4] + u[5] * u[5] + u[6] * u[6];
-  double en = u[8] + u[0];
-  double dn = u[0];
-  double wl, wu, w, fl, fu;
-  if (!sr_brackets(mm, bb, mb, en, dn, P, wl, wu, w, fl, fu)) {
-    q[8] = 0.0;
-    return false;
-  }
+// nr_velocity_srmhd_adi_1d src/equations.F90:5249-5286
+__device__ __forceinline__ double sr_velocity(double mm, double bb, double mb, double w) {
+  double ss = mb * mb;
+  double ww = w * w;
+  double wt = w + bb;
+  double wt2 = wt * wt;
+  return (mm * ww + (w + wt) * ss) / (ww * wt2);
+}
+
+// nr_iterate_srmhd_adi_1dw src/equations.F90:5665-5788.  All loops are
+// bounded by nr_maxit, nr_extra and the bracket doubling limit.
+__device__ inline bool sr_iterate_1dw(double mm, double bb, double mb, double en, double dn, const Phys<double>& P,
+                                      double& w, double& vv) {
+  double wl, wu, fl, fu;
+  if (!sr_brackets(mm, bb, mb, en, dn, P, wl, wu, w, fl, fu)) return false;
   bool keep = true;
   int it = P.nrmax, cn = P.nrext;
   while (keep) {
@@ -387,11 +387,119 @@ __device__ inline bool cons2prim_sr(const double* u, double* q, const Phys<doubl
     it = it - 1;
     if (it < -(P.nrext + 2)) break;  // unreachable bound, kept for the loop limit
   }
-  // nr_velocity_srmhd_adi_1d (5249-5286)
-  double ss = mb * mb;
-  double ww = w * w;
-  double wtv = w + bb;
-  double vv = (mm * ww + (w + wtv) * ss) / (ww * (wtv * wtv));
+  vv = sr_velocity(mm, bb, mb, w);
+  return true;
+}
+
+// nr_iterate_srmhd_adi_2dwv src/equations.F90:5819-5996: Newton on (W, v^2).
+// Without brackets the lower bracket is taken as the root.
+__device__ inline bool sr_iterate_2dwv(double mm, double bb, double mb, double en, double dn, const Phys<double>& P,
+                                       double& w, double& vv) {
+  double wl, wu, fl, fu;
+  if (!sr_brackets(mm, bb, mb, en, dn, P, wl, wu, w, fl, fu)) {
+    w = wl;
+    vv = sr_velocity(mm, bb, mb, w);
+    return true;
+  }
+  vv = sr_velocity(mm, bb, mb, w);
+  bool keep = true;
+  int it = P.nrmax, cn = P.nrext;
+  while (keep) {
+    double mw = (mb / w) * (mb / w);
+    double wt = w + bb;
+    double wt2 = wt * wt;
+    double vm = 1.0 - vv;
+    double vs = sqrt(vm);
+    double f = w - en - P.gammaxi * (w * vm - dn * vs) + 0.5 * ((1.0 + vv) * bb - mw);
+    double g = vv * wt2 - (wt + w) * mw - mm;
+    double dfw = 1.0 - P.gammaxi * vm + mw / w;
+    double dfv = -(P.gammaxi * (0.5 * dn / vs - w)) + 0.5 * bb;
+    double dgw = 2.0 * wt * (vv + mw / w);
+    double dgv = wt2;
+    double det = dfw * dgv - dfv * dgw;
+    double jfw = dgv / det, jgw = -dfv / det, jfv = -dgw / det, jgv = dfw / det;
+    double dw = f * jfw + g * jgw;
+    double dv = f * jfv + g * jgv;
+    w = w - dw;
+    vv = vv - dv;
+    if (w < wl) return false;
+    if (vv < 0.0 || vv >= 1.0) return false;
+    double err = fmax(fabs(dw / w), fabs(dv));
+    if (err < P.tol) { keep = cn > 0; cn = cn - 1; }
+    else keep = it > 0;
+    it = it - 1;
+    if (it < -(P.nrext + 2)) break;  // unreachable bound, kept for the loop limit
+  }
+  return true;
+}
+
+// nr_iterate_srmhd_adi_2dwu src/equations.F90:6020-6206: Newton on (W, u^2),
+// u^2 = v^2 / (1 - v^2)
+__device__ inline bool sr_iterate_2dwu(double mm, double bb, double mb, double en, double dn, const Phys<double>& P,
+                                       double& w, double& vv) {
+  double wl, wu, fl, fu;
+  if (!sr_brackets(mm, bb, mb, en, dn, P, wl, wu, w, fl, fu)) {
+    w = wl;
+    vv = sr_velocity(mm, bb, mb, w);
+    return true;
+  }
+  vv = sr_velocity(mm, bb, mb, w);
+  double uu = vv / (1.0 - vv);
+  bool keep = true;
+  int it = P.nrmax, cn = P.nrext;
+  while (keep) {
+    double up = 1.0 + uu;
+    double gm = sqrt(up);
+    double ss = mb * mb;
+    double ww = w * w;
+    double wt = w + bb;
+    double wt2 = wt * wt;
+    double wd = w - gm * dn;
+    double wp = wt / up;
+    double f = w - en - P.gammaxi * wd / up + 0.5 * (bb * (1.0 + uu / up) - ss / ww);
+    double g = wp * wt * uu - (w + wt) * ss / ww - mm;
+    double dfw = 1.0 - P.gammaxi / up + ss / ww / w;
+    double dfu = 0.5 * (P.gammaxi * (w + wd) + bb) / (up * up);
+    double dgw = 2.0 * wt * (uu / up + ss / ww / w);
+    double dgu = wp * wp;
+    (void)wt2;
+    double det = dfw * dgu - dfu * dgw;
+    double jfw = dgu / det, jgw = -dfu / det, jfu = -dgw / det, jgu = dfw / det;
+    double dw = f * jfw + g * jgw;
+    double du = f * jfu + g * jgu;
+    w = w - dw;
+    uu = uu - du;
+    if (w < wl) return false;
+    if (uu < 0.0) return false;
+    double err = fmax(fabs(dw / w), fabs(du));
+    if (err < P.tol) { keep = cn > 0; cn = cn - 1; }
+    else keep = it > 0;
+    it = it - 1;
+    if (it < -(P.nrext + 2)) break;  // unreachable bound, kept for the loop limit
+  }
+  vv = uu / (1.0 + uu);
+  return true;
+}
+
+// cons2prim_srmhd_adi src/equations.F90:4671-4790 with the recovery chosen
+// by primitive_solver (src/equations.F90:747-780).  Returns false when the
+// recovery failed or gave p <= 0; then only q[PR] is written (0), like the
+// reference.
+__device__ inline bool cons2prim_sr(const double* u, double* q, const Phys<double>& P) {
+  double mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  double mb = u[1] * u[4] + u[2] * u[5] + u[3] * u[6];
+  double bb = u[4] * u[4] + u[5] * u[5] + u[6] * u[6];
+  double en = u[8] + u[0];
+  double dn = u[0];
+  double w, vv;
+  bool info;
+  if (P.c2p == 1) info = sr_iterate_2dwv(mm, bb, mb, en, dn, P, w, vv);
+  else if (P.c2p == 2) info = sr_iterate_2dwu(mm, bb, mb, en, dn, P, w, vv);
+  else info = sr_iterate_1dw(mm, bb, mb, en, dn, P, w, vv);
+  if (!info) {
+    q[8] = 0.0;
+    return false;
+  }
   double vm = 1.0 - vv;
   double vs = sqrt(vm);
   double wt = w + bb;

@@ -57,6 +57,7 @@ struct MethodConst {
   // relativistic recovery and 4-vector reconstruction
   double tol, pmin;
   int nrmax, nrext, states_4vec;
+  int c2p;  // relativistic recovery method
   int plim;  // prolongation limiter (limiter_prol)
   double csnd;  // isothermal sound speed
 };
@@ -67,7 +68,7 @@ template <typename R> __device__ __forceinline__ Phys<R> make_phys(const MethodC
   P.eps = R(m.eps); P.cmax = R(cmax); P.cmax2 = R(cmax2);
   P.csnd = R(m.csnd); P.csnd2 = R(m.csnd * m.csnd);
   P.lim = m.lim; P.clim = m.clim;
-  P.tol = m.tol; P.pmin = m.pmin; P.nrmax = m.nrmax; P.nrext = m.nrext;
+  P.tol = m.tol; P.pmin = m.pmin; P.nrmax = m.nrmax; P.nrext = m.nrext; P.c2p = m.c2p;
   return P;
 }
 

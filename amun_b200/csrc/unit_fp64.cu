@@ -262,7 +262,7 @@ static Phys<double> unit_phys(const UnitArgs& u) {
   Phys<double> P{};
   P.gamma = u.gamma; P.gammam1 = u.gamma - 1.0; P.gammam1i = 1.0 / (u.gamma - 1.0); P.gammaxi = u.gammaxi;
   P.eps = u.eps; P.cmax = u.cmax; P.cmax2 = u.cmax * u.cmax; P.lim = u.lim; P.clim = u.clim;
-  P.tol = u.tol; P.pmin = u.pmin; P.nrmax = u.nrmax; P.nrext = u.nrext;
+  P.tol = u.tol; P.pmin = u.pmin; P.nrmax = u.nrmax; P.nrext = u.nrext; P.c2p = u.c2p;
   P.csnd = u.csnd; P.csnd2 = u.csnd * u.csnd;
   return P;
 }

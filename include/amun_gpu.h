@@ -35,6 +35,8 @@ extern "C" {
 /* equation_system / equation_of_state (src/equations.F90:322-833) */
 enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2, AMUN_EQ_SRHD = 3 };
 enum { AMUN_EOS_ADI = 0, AMUN_EOS_ISO = 1 };
+/* primitive_solver: 1D(W), 2D(W,v^2), 2D(W,u^2) (src/equations.F90:605-640) */
+enum { AMUN_C2P_1DW = 0, AMUN_C2P_2DWV = 1, AMUN_C2P_2DWU = 2 };
 /* reconstruction (src/interpolations.F90:226-382) */
 enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
 /* limiter / extrema_limiter (src/interpolations.F90:389-445) */
@@ -83,6 +85,9 @@ typedef struct amun_params {
   int eos;              /* AMUN_EOS_*             "equation_of_state"         */
   double csnd;          /*                        "csnd" (isothermal sound
                            speed, src/equations.F90:176, 847-851)            */
+  int c2p;              /* AMUN_C2P_*             "primitive_solver" (the
+                           relativistic recovery, src/equations.F90:605-640,
+                           747-780); -1 for a name the reference rejects      */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block

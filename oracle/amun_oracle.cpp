@@ -68,6 +68,7 @@ struct Params {
   double tol = 1.0e-10, pmin = 1.0e-16;
   int nrmax = 100, nrext = 2;
   bool states_4vec = false;
+  int c2p = 0;  // primitive_solver: 0 1D(W), 1 2D(W,v^2), 2 2D(W,u^2), -1 unknown
 };
 
 bool is_one_of(const std::string& s, std::initializer_list<const char*> l) {
@@ -97,8 +98,11 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"iso", "ISO", "isothermal", "ISOTHERMAL"})) p.iso = true;
     else return 110;
   } else if (key == "primitive_solver") {
-    // only the 1D(W) Newton recovery is restated (src/equations.F90:5665-5788)
-    if (!is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"})) return 110;
+    // src/equations.F90:605-640, 747-780: checked by the relativistic systems
+    if (is_one_of(v, {"1Dw", "1dw", "1DW", "1D(w)", "1D(W)"})) p.c2p = 0;
+    else if (is_one_of(v, {"2dwv", "2Dwv", "2D(w,v)", "2D(W,v)"})) p.c2p = 1;
+    else if (is_one_of(v, {"2dwu", "2Dwu", "2D(w,u)", "2D(W,u)"})) p.c2p = 2;
+    else p.c2p = -1;
   } else if (key == "tolerance") p.tol = atof(v.c_str());
   else if (key == "nr_maxit") p.nrmax = atoi(v.c_str());
   else if (key == "nr_extra") p.nrext = atoi(v.c_str());
@@ -501,6 +505,7 @@ struct Oracle {
       else if (p.rs == RS_HLLC || p.rs == RS_HLLCM) p.rs = RS_HLL;
     }
     csnd = p.csnd; csnd2 = csnd * csnd;
+    if (sr && p.c2p < 0) return 110;
     // the relativistic systems offer HLL and HLLC ("hllcm" included,
     // src/schemes.F90:400-498); elsewhere "hllcm" names nothing
     if (sr) p.rs = (p.rs == RS_HLLC || p.rs == RS_HLLCM) ? RS_HLLC : RS_HLL;
@@ -710,6 +715,91 @@ struct Oracle {
     return true;
   }
 
+  // nr_iterate_srmhd_adi_2dwv src/equations.F90:5819-5996: Newton on
+  // (W, v^2); without brackets the lower bracket is taken as the root.
+  // Fortran max(a, b) is restated as fmax.
+  bool nr_iterate_2dwv(double mm, double bb, double mb, double en, double dn, double& w, double& vv) const {
+    double wl, wu, fl, fu;
+    if (!nr_initial_brackets(mm, bb, mb, en, dn, wl, wu, w, fl, fu)) {
+      w = wl;
+      vv = nr_velocity(mm, bb, mb, w);
+      return true;
+    }
+    vv = nr_velocity(mm, bb, mb, w);
+    bool keep = true;
+    int it = p.nrmax, cn = p.nrext;
+    while (keep) {
+      double mw = (mb / w) * (mb / w);
+      double wt = w + bb;
+      double wt2 = wt * wt;
+      double vm = 1.0 - vv;
+      double vs = std::sqrt(vm);
+      double f = w - en - gammaxi * (w * vm - dn * vs) + 0.5 * ((1.0 + vv) * bb - mw);
+      double g = vv * wt2 - (wt + w) * mw - mm;
+      double dfw = 1.0 - gammaxi * vm + mw / w;
+      double dfv = -(gammaxi * (0.5 * dn / vs - w)) + 0.5 * bb;
+      double dgw = 2.0 * wt * (vv + mw / w);
+      double dgv = wt2;
+      double det = dfw * dgv - dfv * dgw;
+      double jfw = dgv / det, jgw = -dfv / det, jfv = -dgw / det, jgv = dfw / det;
+      double dw = f * jfw + g * jgw;
+      double dv = f * jfv + g * jgv;
+      w = w - dw;
+      vv = vv - dv;
+      if (w < wl) return false;
+      if (vv < 0.0 || vv >= 1.0) return false;
+      double err = std::fmax(std::fabs(dw / w), std::fabs(dv));
+      if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+      else keep = it > 0;
+      it = it - 1;
+    }
+    return true;
+  }
+
+  // nr_iterate_srmhd_adi_2dwu src/equations.F90:6020-6206: Newton on
+  // (W, u^2), u^2 = v^2 / (1 - v^2)
+  bool nr_iterate_2dwu(double mm, double bb, double mb, double en, double dn, double& w, double& vv) const {
+    double wl, wu, fl, fu;
+    if (!nr_initial_brackets(mm, bb, mb, en, dn, wl, wu, w, fl, fu)) {
+      w = wl;
+      vv = nr_velocity(mm, bb, mb, w);
+      return true;
+    }
+    vv = nr_velocity(mm, bb, mb, w);
+    double uu = vv / (1.0 - vv);
+    bool keep = true;
+    int it = p.nrmax, cn = p.nrext;
+    while (keep) {
+      double up = 1.0 + uu;
+      double gm = std::sqrt(up);
+      double ss = mb * mb;
+      double ww = w * w;
+      double wt = w + bb;
+      double wd = w - gm * dn;
+      double wp = wt / up;
+      double f = w - en - gammaxi * wd / up + 0.5 * (bb * (1.0 + uu / up) - ss / ww);
+      double g = wp * wt * uu - (w + wt) * ss / ww - mm;
+      double dfw = 1.0 - gammaxi / up + ss / ww / w;
+      double dfu = 0.5 * (gammaxi * (w + wd) + bb) / (up * up);
+      double dgw = 2.0 * wt * (uu / up + ss / ww / w);
+      double dgu = wp * wp;
+      double det = dfw * dgu - dfu * dgw;
+      double jfw = dgu / det, jgw = -dfu / det, jfu = -dgw / det, jgu = dfw / det;
+      double dw = f * jfw + g * jgw;
+      double du = f * jfu + g * jgu;
+      w = w - dw;
+      uu = uu - du;
+      if (w < wl) return false;
+      if (uu < 0.0) return false;
+      double err = std::fmax(std::fabs(dw / w), std::fabs(du));
+      if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+      else keep = it > 0;
+      it = it - 1;
+    }
+    vv = uu / (1.0 + uu);
+    return true;
+  }
+
   // cons2prim_srmhd_adi src/equations.F90:4671-4790.  On failure only the
   // pressure is set (to zero); the other entries of q keep their values.
   void cons2prim_sr(const double* U, double* Q) const {
@@ -719,7 +809,10 @@ struct Oracle {
     double en = U[ien - 1] + U[idn - 1];
     double dn = U[idn - 1];
     double w = 0.0, vv = 0.0;
-    if (nr_iterate_1dw(mm, bb, mb, en, dn, w, vv)) {
+    bool info = p.c2p == 1 ? nr_iterate_2dwv(mm, bb, mb, en, dn, w, vv)
+              : p.c2p == 2 ? nr_iterate_2dwu(mm, bb, mb, en, dn, w, vv)
+                           : nr_iterate_1dw(mm, bb, mb, en, dn, w, vv);
+    if (info) {
       double vm = 1.0 - vv;
       double vs = std::sqrt(vm);
       double wt = w + bb;
@@ -909,6 +1002,107 @@ struct Oracle {
     return false;  // "Positive function for lower bracket!"
   }
 
+  // the brackets of nr_iterate_srhd_adi_2dwv src/equations.F90:4128-4215
+  // and 2dwu 4360-4447
+  bool srhd_brackets_2d(double mm, double en, double dn, double& wl, double& wc) const {
+    wl = std::sqrt(mm + dn * dn) + gammaxi * p.pmin;
+    double wu = en + p.pmin;
+    bool keep = wl >= wu;
+    int it = p.nrmax;
+    while (keep) {
+      wu = 2.0 * wu;
+      it = it - 1;
+      keep = (wl >= wu) && it > 0;
+    }
+    if (it <= 0) return false;  // "Could not find the upper limit for enthalpy!"
+    double fl, fu;
+    nr_function_srhd(mm, en, dn, wl, fl, nullptr);
+    nr_function_srhd(mm, en, dn, wu, fu, nullptr);
+    keep = fl * fu > 0.0;
+    it = p.nrmax;
+    while (keep) {
+      wl = wu;
+      fl = fu;
+      wu = 2.0 * wu;
+      nr_function_srhd(mm, en, dn, wu, fu, nullptr);
+      it = it - 1;
+      keep = (fl * fu > 0.0) && it > 0;
+    }
+    if (it <= 0) return false;  // "No initial brackets found!"
+    wc = wl - fl * (wu - wl) / (fu - fl);
+    return true;
+  }
+
+  // nr_iterate_srhd_adi_2dwv src/equations.F90:4128-4330
+  bool nr_iterate_srhd_2dwv(double mm, double en, double dn, double& w, double& vv) const {
+    double wl;
+    if (!srhd_brackets_2d(mm, en, dn, wl, w)) return false;
+    vv = mm / (w * w);
+    bool keep = true;
+    int it = p.nrmax, cn = p.nrext;
+    while (keep) {
+      double ww = w * w;
+      double vm = 1.0 - vv;
+      double vs = std::sqrt(vm);
+      double gd = gammaxi * dn;
+      double gv = 1.0 - gammaxi * vm;
+      double f = gv * w - en + gd * vs;
+      double g = vv * ww - mm;
+      double dfw = gv;
+      double dfv = gammaxi * w - 0.5 * gd / vs;
+      double dgw = 2.0 * vv * w;
+      double dgv = ww;
+      double det = dfw * dgv - dfv * dgw;
+      double jfw = dgv / det, jgw = -dfv / det, jfv = -dgw / det, jgv = dfw / det;
+      double dw = f * jfw + g * jgw;
+      double dv = f * jfv + g * jgv;
+      w = w - dw;
+      vv = vv - dv;
+      if (w < wl) return false;
+      if (vv < 0.0 || vv >= 1.0) return false;
+      double err = std::fmax(std::fabs(dw / w), std::fabs(dv));
+      if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+      else keep = it > 0;
+      it = it - 1;
+    }
+    return true;
+  }
+
+  // nr_iterate_srhd_adi_2dwu src/equations.F90:4360-4566
+  bool nr_iterate_srhd_2dwu(double mm, double en, double dn, double& w, double& vv) const {
+    double wl;
+    if (!srhd_brackets_2d(mm, en, dn, wl, w)) return false;
+    double uu = mm / (w * w - mm);
+    bool keep = true;
+    int it = p.nrmax, cn = p.nrext;
+    while (keep) {
+      double ww = w * w;
+      double up = 1.0 + uu;
+      double gm = std::sqrt(up);
+      double gd = gammaxi * dn;
+      double f = (up - gammaxi) * w - up * en + gm * gd;
+      double g = uu * ww - up * mm;
+      double dfw = up - gammaxi;
+      double dfu = w - en + 0.5 * gd / gm;
+      double dgw = 2.0 * uu * w;
+      double dgu = ww - mm;
+      double det = dfw * dgu - dfu * dgw;
+      double jfw = dgu / det, jgw = -dfu / det, jfu = -dgw / det, jgu = dfw / det;
+      double dw = f * jfw + g * jgw;
+      double du = f * jfu + g * jgu;
+      w = w - dw;
+      uu = uu - du;
+      if (w < wl) return false;
+      if (uu < 0.0) return false;
+      double err = std::fmax(std::fabs(dw / w), std::fabs(du));
+      if (err < p.tol) { keep = cn > 0; cn = cn - 1; }
+      else keep = it > 0;
+      it = it - 1;
+    }
+    vv = uu / (1.0 + uu);
+    return true;
+  }
+
   // cons2prim_srhd_adi src/equations.F90:3550-3639.  On failure only the
   // pressure is set (to zero); the other entries of q keep their values.
   void cons2prim_srhd(const double* U, double* Q) const {
@@ -916,7 +1110,10 @@ struct Oracle {
     double en = U[ien - 1] + U[idn - 1];
     double dn = U[idn - 1];
     double w = 0.0, vv = 0.0;
-    if (nr_iterate_srhd_1dw(mm, en, dn, w, vv)) {
+    bool info = p.c2p == 1 ? nr_iterate_srhd_2dwv(mm, en, dn, w, vv)
+              : p.c2p == 2 ? nr_iterate_srhd_2dwu(mm, en, dn, w, vv)
+                           : nr_iterate_srhd_1dw(mm, en, dn, w, vv);
+    if (info) {
       double vm = 1.0 - vv;
       double vs = std::sqrt(vm);
       Q[idn - 1] = dn * vs;

@@ -50,6 +50,9 @@ def test_default_params_match_reference_defaults():
     ("fix_positivity", "yes", "fix_positivity", 1), ("clip_extrema", "off", "clip_extrema", 0),
     ("equation_of_state", "isothermal", "eos", N.AMUN_EOS_ISO), ("equation_of_state", "ADI", "eos", N.AMUN_EOS_ADI),
     ("csnd", "0.25", "csnd", 0.25), ("riemann_solver", "hlld-m", "riemann", 4),
+    ("riemann_solver", "hllc-m", "riemann", 5), ("equation_system", "SRHD", "eqsys", N.AMUN_EQ_SRHD),
+    ("primitive_solver", "2D(W,v)", "c2p", 1), ("primitive_solver", "2dwu", "c2p", 2),
+    ("primitive_solver", "1D(W)", "c2p", 0), ("primitive_solver", "newton", "c2p", -1),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()

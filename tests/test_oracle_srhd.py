@@ -164,3 +164,30 @@ def test_unphysical_state_fails_like_the_reference(oracle_mod):
 def test_isothermal_relativistic_is_refused(oracle_mod):
     with pytest.raises(ValueError, match="iret"):
         oracle_mod.Oracle(params("srhd", "tvd", "hll", equation_of_state="iso"))
+
+
+@pytest.mark.parametrize("eq", ["srhd", "srmhd"])
+@pytest.mark.parametrize("c2p", ["2dwv", "2D(W,u)"])
+def test_two_variable_recoveries(oracle_mod, eq, c2p):
+    """primitive_solver 2D(W,v^2) and 2D(W,u^2) (src/equations.F90:4128-4566,
+    5819-6206) recover the same states as 1D(W), to the Newton tolerance."""
+    kw = dict(ncells=8, gamma=G, tolerance=1e-12, nr_maxit=50)
+    a = oracle_mod.Oracle(params(eq, "tvd", "hll", "rk2", primitive_solver=c2p, **kw))
+    b = oracle_mod.Oracle(params(eq, "tvd", "hll", "rk2", **kw))
+    rng = np.random.default_rng(8)
+    if eq == "srhd":
+        q = srhd_states(rng, 2000, gmax=8.0)
+    else:
+        from test_oracle_srmhd import sr_states
+        q = sr_states(rng, 2000, gmax=8.0)
+    u = b.prim2cons(q)
+    qa, qb = a.cons2prim(u), b.cons2prim(u)
+    assert a.scalars()["c2p_failures"] == 0
+    assert np.allclose(qa, q, rtol=1e-8, atol=1e-10)
+    assert np.allclose(qa, qb, rtol=1e-8, atol=1e-10)
+
+
+def test_unknown_recovery_is_refused_by_relativistic_systems_only(oracle_mod):
+    with pytest.raises(ValueError, match="iret=110"):
+        oracle_mod.Oracle(srhd_params(primitive_solver="3D"))
+    oracle_mod.Oracle(params("hd", "tvd", "hll", "rk2", primitive_solver="3D"))
