@@ -314,6 +314,7 @@ MethodConst method_const() {
   m.plim = C.p.prolongation_limiter;
   m.csnd = C.p.csnd;
   m.c2p = C.p.c2p;
+  m.mlp = C.p.mlp;
   m.states_4vec = relativistic() ? C.p.states_4vec : 0;
   return m;
 }
@@ -444,7 +445,7 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.tol = C.p.tolerance; u.pmin = C.p.pmin; u.nrmax = C.p.nr_maxit; u.nrext = C.p.nr_extra;
   u.states_4vec = relativistic() ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
-  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd; u.c2p = C.p.c2p;
+  u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd; u.c2p = C.p.c2p; u.mlp = C.p.mlp;
   return u;
 }
 
@@ -487,6 +488,7 @@ void amun_gpu_default_params(amun_params* p) {
   p->eos = AMUN_EOS_ADI;
   p->csnd = 1.0;
   p->c2p = AMUN_C2P_1DW;
+  p->mlp = 0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -550,6 +552,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else p->time_advance = AMUN_TA_RK2;
   } else if (k == "stages") p->stages = atoi(v);
   else if (k == "fix_positivity") p->fix_positivity = is_on(v);
+  else if (k == "mlp_limiting") p->mlp = is_on(v);
   else if (k == "clip_extrema") p->clip_extrema = is_on(v);
   else if (k == "precision") {
     if (is_one_of(v, {"fp32", "FP32", "fp32_bulk", "bulk"})) p->precision = AMUN_FP32_BULK;
@@ -1303,8 +1306,8 @@ int adj_supported() {
     return fail(AMUN_E_UNSUPPORTED, "adjoint: adiabatic HD and MHD only");
   if (C.p.reconstruction != AMUN_REC_WENO5Z) return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z reconstruction only");
   if (effective_solver() != AMUN_RS_HLL) return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL Riemann solver only");
-  if (C.p.fix_positivity || C.p.clip_extrema)
-    return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity and clip_extrema must be off");
+  if (C.p.fix_positivity || C.p.clip_extrema || C.p.mlp)
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity, clip_extrema and mlp_limiting must be off");
   if (C.p.nghosts < 4) return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4");
   if (C.amr) return fail(AMUN_E_UNSUPPORTED, "adjoint: meshes at one level only");
   return 0;

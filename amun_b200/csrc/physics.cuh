@@ -108,6 +108,72 @@ __device__ __forceinline__ R limiter(int which, R x, R a, R b, R eps) {
   }
 }
 
+// mlp_limiting src/interpolations.F90:1171-1321, the slopes of one cell:
+// minmod half-differences in every direction, reduced by the
+// multi-dimensional limiting process when their sum exceeds the distance of
+// the cell value to the extremes of its 3^d neighbourhood.  Qn(di, dj, dk)
+// is the variable at a neighbour, indices clamped to the block.
+template <typename R, typename F>
+__device__ __forceinline__ void mlp_slopes(F Qn, int ndims, R* dq) {
+  const R q0 = Qn(0, 0, 0);
+  const R xm = Qn(-1, 0, 0), xp = Qn(1, 0, 0), ym = Qn(0, -1, 0), yp = Qn(0, 1, 0);
+  R zm = q0, zp = q0;
+  dq[0] = limiter<R>(LIM_MM, R(0.5), q0 - xm, xp - q0, R(0));
+  dq[1] = limiter<R>(LIM_MM, R(0.5), q0 - ym, yp - q0, R(0));
+  dq[2] = R(0);
+  if (ndims == 3) {
+    zm = Qn(0, 0, -1);
+    zp = Qn(0, 0, 1);
+    dq[2] = limiter<R>(LIM_MM, R(0.5), q0 - zm, zp - q0, R(0));
+  }
+  const int k0 = ndims == 3 ? -1 : 0, k1 = ndims == 3 ? 1 : 0;
+  R qmn = Qn(-1, -1, k0), qmx = qmn;
+  for (int dk = k0; dk <= k1; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        const R x = Qn(di, dj, dk);
+        qmn = d_min(qmn, x);
+        qmx = d_max(qmx, x);
+      }
+  const R dqc = d_min(qmx - q0, q0 - qmn);
+  R sdq = d_fabs(dq[0]) + d_fabs(dq[1]);
+  if (ndims == 3) sdq = sdq + d_fabs(dq[2]);
+  if (!(sdq > dqc)) return;
+  R dqm[3], ap[3];
+  dqm[0] = d_fabs(xp - xm);
+  dqm[1] = d_fabs(yp - ym);
+  dqm[2] = d_fabs(zp - zm);
+  R sm = d_fabs(dqm[0]) + d_fabs(dqm[1]);
+  if (ndims == 3) sm = sm + d_fabs(dqm[2]);
+  const R fc = dqc / d_max(R(1.0e-16), sm);
+  ap[0] = fc * d_fabs(dqm[0]);
+  ap[1] = fc * d_fabs(dqm[1]);
+  ap[2] = fc * d_fabs(dqm[2]);
+  if (ndims == 3) {
+    R hh[3], uu[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+      const int np1 = (n + 1) % 3, np2 = (n + 2) % 3;
+      hh[n] = d_max(ap[n] - d_fabs(dq[n]), R(0));
+      uu[n] = ap[n] - hh[n];
+      uu[np1] = ap[np1] + R(0.5) * hh[n];
+      uu[np2] = ap[np2] + R(0.5) * hh[n];
+      const R f2 = hh[n] / (hh[n] + R(1.0e-16));
+      const R fl = f2 * (d_max(ap[np1] - d_fabs(dq[np1]), R(0)) - d_max(ap[np2] - d_fabs(dq[np2]), R(0)));
+      ap[n] = uu[n];
+      ap[np1] = uu[np1] - fl;
+      ap[np2] = uu[np2] + fl;
+    }
+  } else {
+    const R fl = d_max(ap[0] - d_fabs(dq[0]), R(0)) - d_max(ap[1] - d_fabs(dq[1]), R(0));
+    ap[0] = ap[0] - fl;
+    ap[1] = ap[1] + fl;
+  }
+  dq[0] = fsign(ap[0], dq[0]);
+  dq[1] = fsign(ap[1], dq[1]);
+  if (ndims == 3) dq[2] = fsign(ap[2], dq[2]);
+}
+
 }  // namespace amun
 #include "srmhd.cuh"
 #include "srhd.cuh"

@@ -58,6 +58,7 @@ struct MethodConst {
   double tol, pmin;
   int nrmax, nrext, states_4vec;
   int c2p;  // relativistic recovery method
+  int mlp;  // multi-dimensional limiting process (mlp_limiting)
   int plim;  // prolongation limiter (limiter_prol)
   double csnd;  // isothermal sound speed
 };
@@ -238,6 +239,43 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
           }
           fR = f0 + dqd;
           fL = f0 - dqd;
+        }
+        if (a.m.mlp) {
+          // mlp_limiting src/interpolations.F90:1171-1321 for this cell's
+          // two faces along DIR (in the reconstruction frame: 4-vector
+          // states when four)
+          const int P = p0 - 1 + pp, Lc = l0 + ll;
+          const int ci = DIR == 0 ? P : Lc, cj = DIR == 1 ? P : (DIR == 0 ? Lc : t0), ck = DIR == 2 ? P : t0;
+          auto qat = [&](int i, int j, int k) -> R {
+            i = i < 0 ? 0 : (i >= g.IM ? g.IM - 1 : i);
+            j = j < 0 ? 0 : (j >= g.JM ? g.JM - 1 : j);
+            k = g.ndims == 3 ? (k < 0 ? 0 : (k >= g.KM ? g.KM - 1 : k)) : 0;
+            const R* qc = qb + ((long long)k * g.JM + j) * g.IM + i;
+            if (V::SR && four && v <= 3) {
+              R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
+              return ld_ro(qc + (long long)v * g.qvs) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
+            }
+            return ld_ro(qc + (long long)v * g.qvs);
+          };
+          R dq[3];
+          mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ci + di, cj + dj, ck + dk); }, g.ndims, dq);
+          R fLcur = fL;
+          if (REC == REC_TVD && P == 1) {
+            // two ghost layers: the first cell of the line (a ghost copy,
+            // both faces = q) is limited first, with its lower neighbour
+            // clamped to itself, and writes this cell's left face
+            const int ai = DIR == 0 ? 0 : ci, aj = DIR == 1 ? 0 : cj, ak = DIR == 2 ? 0 : ck;
+            R dq0[3];
+            mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ai + di, aj + dj, ak + dk); }, g.ndims, dq0);
+            const R q00 = qat(ai, aj, ak);
+            if (d_max(d_fabs(q00 - q00), d_fabs(fL - q00)) > d_fabs(dq0[DIR])) fLcur = q00 - dq0[DIR];
+          }
+          if (d_max(d_fabs(fR - f0), d_fabs(fLcur - f0)) > d_fabs(dq[DIR])) {
+            fR = f0 + dq[DIR];
+            fL = f0 - dq[DIR];
+          } else {
+            fL = fLcur;
+          }
         }
         fRv[v] = fR;
         fLv[v] = fL;

@@ -11,7 +11,7 @@ struct UnitArgs {
   int rec, lim, clim, rs, clip, positivity;
   double gamma, gammaxi, eps, cmax, csnd;
   double tol, pmin;
-  int nrmax, nrext, states_4vec, c2p;
+  int nrmax, nrext, states_4vec, c2p, mlp;
 };
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,

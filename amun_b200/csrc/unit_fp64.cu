@@ -72,6 +72,49 @@ __global__ void tvd_box(const double* q, double* qs, BlockDims d, int lim, doubl
   }
 }
 
+// ---- mlp_limiting (src/interpolations.F90:1171-1321) -------------------------
+// The reference limits the cells one after another in storage order; a cell
+// rewrites its own two faces along each direction, except the first cell of
+// a line (index 0, its lower neighbour clamped to itself), which rewrites the
+// left face of the second.  Phase 0 runs the directions along which a cell
+// is first, phase 1 the others: the same result in two parallel passes.
+template <int EQ>
+__global__ void mlp_cells(const double* q, double* qs, BlockDims d, int phase) {
+  constexpr int NV = Var<EQ>::NV;
+  const long long cells = (long long)d.im * d.jm * d.km;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * NV;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(t % NV);
+    const long long c = t / NV;
+    const int i = (int)(c % d.im), j = (int)((c / d.im) % d.jm), k = (int)(c / ((long long)d.im * d.jm));
+    const int pos[3] = {i, j, k};
+    bool any = false;
+    for (int dd = 0; dd < d.ndims; ++dd) any = any || ((pos[dd] == 0) == (phase == 0));
+    if (!any) continue;
+    auto Qn = [&](int di, int dj, int dk) {
+      int ii = i + di, jj = j + dj, kk = k + dk;
+      ii = ii < 0 ? 0 : (ii >= d.im ? d.im - 1 : ii);
+      jj = jj < 0 ? 0 : (jj >= d.jm ? d.jm - 1 : jj);
+      kk = d.ndims == 3 ? (kk < 0 ? 0 : (kk >= d.km ? d.km - 1 : kk)) : 0;
+      return q[((long long)kk * d.jm * d.im + (long long)jj * d.im + ii) * NV + v];
+    };
+    double dq[3];
+    mlp_slopes<double>(Qn, d.ndims, dq);
+    const double q0 = Qn(0, 0, 0);
+    const long long st[3] = {1, d.im, (long long)d.im * d.jm};
+    for (int dd = 0; dd < d.ndims; ++dd) {
+      if ((pos[dd] == 0) != (phase == 0)) continue;
+      const long long cl = pos[dd] == 0 ? c : c - st[dd];
+      double& fr = qs[((long long)(2 * dd + 0) * cells + c) * NV + v];
+      double& fl = qs[((long long)(2 * dd + 1) * cells + cl) * NV + v];
+      if (d_max(fabs(fr - q0), fabs(fl - q0)) > fabs(dq[dd])) {
+        fr = q0 + dq[dd];
+        fl = q0 - dq[dd];
+      }
+    }
+  }
+}
+
 // ---- interfaces_dir + reconstruct (src/interpolations.F90:867-959,
 // 1343-1381): one thread per (variable, line); the line is reconstructed
 // with reconstruct_weno5z (1937-2083) including its line-end fallbacks, then
@@ -293,6 +336,11 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
       dir_lines<EQ><<<(int)((lines + 127) / 128), 128, 0, s>>>(qr, qs, d, dir, u.lim, u.clim, u.eps, u.clip,
                                                                u.positivity, scratch);
     }
+  }
+  if (u.mlp) {
+    const int grid = (int)((cells * NV + 255) / 256);
+    mlp_cells<EQ><<<grid, 256, 0, s>>>(qr, qs, d, 0);
+    mlp_cells<EQ><<<grid, 256, 0, s>>>(qr, qs, d, 1);
   }
   if (four) {
     long long nstates = cells * 2 * u.ndims;

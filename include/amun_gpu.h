@@ -88,6 +88,8 @@ typedef struct amun_params {
   int c2p;              /* AMUN_C2P_*             "primitive_solver" (the
                            relativistic recovery, src/equations.F90:605-640,
                            747-780); -1 for a name the reference rejects      */
+  int mlp;              /* 0/1                    "mlp_limiting"
+                           (src/interpolations.F90:452-457)                  */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block

@@ -1630,6 +1630,79 @@ struct Oracle {
     }
   }
 
+  // mlp_limiting src/interpolations.F90:1171-1321 (Multi-dimensional
+  // Limiting Process): in place over every cell in storage order, with the
+  // neighbour indices clamped to the block.  Fortran min/max are restated
+  // as fmin2/fmax2.
+  void mlp_limiting(const double* qv, double* qs) const {
+    const size_t N = cells();
+    const int nd = p.ndims;
+    auto Q = [&](int i, int j, int k) { return qv[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1))]; };
+    auto QS = [&](int i, int j, int k, int s, int d) -> double& {
+      return qs[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)) + N * ((size_t)(s - 1) + 2 * (size_t)(d - 1))];
+    };
+    auto mm = [&](double a, double b) { return 0.5 * (fsign(0.5, a) + fsign(0.5, b)) * fmin2(std::fabs(a), std::fabs(b)); };
+    for (int k = 1; k <= km; ++k) {
+      int km1 = nd == 3 ? std::max(1, k - 1) : k, kp1 = nd == 3 ? std::min(km, k + 1) : k;
+      for (int j = 1; j <= jm; ++j) {
+        int jm1 = std::max(1, j - 1), jp1 = std::min(jm, j + 1);
+        for (int i = 1; i <= im; ++i) {
+          int im1 = std::max(1, i - 1), ip1 = std::min(im, i + 1);
+          double q0 = Q(i, j, k);
+          double dq[3] = {0, 0, 0}, dqm[3] = {0, 0, 0}, ap[3] = {0, 0, 0};
+          dq[0] = mm(q0 - Q(im1, j, k), Q(ip1, j, k) - q0);
+          dq[1] = mm(q0 - Q(i, jm1, k), Q(i, jp1, k) - q0);
+          if (nd == 3) dq[2] = mm(q0 - Q(i, j, km1), Q(i, j, kp1) - q0);
+          double qmn = Q(im1, jm1, km1), qmx = qmn;
+          for (int kk = km1; kk <= kp1; ++kk)
+            for (int jj = jm1; jj <= jp1; ++jj)
+              for (int ii = im1; ii <= ip1; ++ii) { qmn = fmin2(qmn, Q(ii, jj, kk)); qmx = fmax2(qmx, Q(ii, jj, kk)); }
+          double dqc = fmin2(qmx - q0, q0 - qmn);
+          double sdq = std::fabs(dq[0]) + std::fabs(dq[1]);
+          if (nd == 3) sdq = sdq + std::fabs(dq[2]);
+          if (sdq > dqc) {
+            dqm[0] = std::fabs(Q(ip1, j, k) - Q(im1, j, k));
+            dqm[1] = std::fabs(Q(i, jp1, k) - Q(i, jm1, k));
+            if (nd == 3) dqm[2] = std::fabs(Q(i, j, kp1) - Q(i, j, km1));
+            double sm = std::fabs(dqm[0]) + std::fabs(dqm[1]);
+            if (nd == 3) sm = sm + std::fabs(dqm[2]);
+            double fc = dqc / fmax2(1.0e-16, sm);
+            for (int m = 0; m < nd; ++m) ap[m] = fc * std::fabs(dqm[m]);
+            if (nd == 3) {
+              double hh[3], uu[3];
+              for (int n = 0; n < 3; ++n) {
+                hh[n] = fmax2(ap[n] - std::fabs(dq[n]), 0.0);
+                int np1 = (n + 1) % 3, np2 = (n + 2) % 3;
+                uu[n] = ap[n] - hh[n];
+                uu[np1] = ap[np1] + 0.5 * hh[n];
+                uu[np2] = ap[np2] + 0.5 * hh[n];
+                double f2 = hh[n] / (hh[n] + 1.0e-16);
+                double fl = f2 * (fmax2(ap[np1] - std::fabs(dq[np1]), 0.0) - fmax2(ap[np2] - std::fabs(dq[np2]), 0.0));
+                ap[n] = uu[n];
+                ap[np1] = uu[np1] - fl;
+                ap[np2] = uu[np2] + fl;
+              }
+            } else {
+              double fl = fmax2(ap[0] - std::fabs(dq[0]), 0.0) - fmax2(ap[1] - std::fabs(dq[1]), 0.0);
+              ap[0] = ap[0] - fl;
+              ap[1] = ap[1] + fl;
+            }
+            for (int m = 0; m < nd; ++m) dq[m] = fsign(ap[m], dq[m]);
+          }
+          const int lo[3] = {im1, jm1, km1};
+          for (int d = 1; d <= nd; ++d) {
+            int i2 = d == 1 ? lo[0] : i, j2 = d == 2 ? lo[1] : j, k2 = d == 3 ? lo[2] : k;
+            double a = QS(i, j, k, 1, d) - q0, b = QS(i2, j2, k2, 2, d) - q0;
+            if (fmax2(std::fabs(a), std::fabs(b)) > std::fabs(dq[d - 1])) {
+              QS(i, j, k, 1, d) = q0 + dq[d - 1];
+              QS(i2, j2, k2, 2, d) = q0 - dq[d - 1];
+            }
+          }
+        }
+      }
+    }
+  }
+
   // interfaces_tvd src/interpolations.F90:729-848.  qv(im,jm,km) one variable;
   // out qs(im,jm,km,2,NDIMS).
   void interfaces_tvd(bool positive, const double* qv, double* qs) {
@@ -1674,6 +1747,7 @@ struct Oracle {
             QS(i, j, k - 1, 2, 3) = Q(i, j, k) - dq[2];
           }
         }
+    if (p.mlp) mlp_limiting(qv, qs);
   }
 
   // the "copy ghost zones" block shared by interfaces_tvd / interfaces_dir
@@ -1844,6 +1918,7 @@ struct Oracle {
         for (int j = jbl; j <= jeu; ++j)
           for (int i = ibl; i <= ieu; ++i) line(3, i, j, 1, pp);
     }
+    if (p.mlp) mlp_limiting(qv, qs);
   }
 
   // =========================================================================
