@@ -34,7 +34,8 @@ class amun_params(C.Structure):
         ("eps", C.c_double), ("tolerance", C.c_double), ("pmin", C.c_double), ("nr_maxit", C.c_int),
         ("nr_extra", C.c_int), ("states_4vec", C.c_int), ("prolongation_limiter", C.c_int),
         ("xblocks", C.c_int), ("yblocks", C.c_int), ("zblocks", C.c_int), ("eos", C.c_int),
-        ("csnd", C.c_double), ("c2p", C.c_int), ("mlp", C.c_int),
+        ("csnd", C.c_double), ("c2p", C.c_int), ("mlp", C.c_int), ("limo3_rad", C.c_double),
+        ("ppm_const", C.c_double), ("kappa", C.c_double), ("kbeta", C.c_double),
     ]
 
 

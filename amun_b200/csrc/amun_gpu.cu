@@ -45,6 +45,7 @@ struct Ctx {
   void* du = nullptr;
   int* nbr = nullptr;
   double* binv = nullptr;
+  double* bdx = nullptr;  // per block dx, dy, dz
   DevScalars* sc = nullptr;
   double* staging = nullptr;
   size_t staging_bytes = 0;
@@ -214,8 +215,9 @@ void free_pool() {
   if (C.du) cudaFree(C.du);
   if (C.nbr) cudaFree(C.nbr);
   if (C.binv) cudaFree(C.binv);
+  if (C.bdx) cudaFree(C.bdx);
   if (C.staging) cudaFree(C.staging);
-  C.u0 = nullptr; C.u1 = nullptr; C.du = nullptr; C.nbr = nullptr; C.binv = nullptr; C.staging = nullptr;
+  C.u0 = nullptr; C.u1 = nullptr; C.du = nullptr; C.nbr = nullptr; C.binv = nullptr; C.bdx = nullptr; C.staging = nullptr;
   C.staging_bytes = 0;
   C.pool_bytes = 0;
   C.nblocks = 0;
@@ -305,6 +307,18 @@ void tile_shape(int& LP, int& LW) {
 
 bool relativistic() { return C.p.eqsys == AMUN_EQ_SRMHD || C.p.eqsys == AMUN_EQ_SRHD; }
 
+// the sweep variant: TVD and WENO-Z have their own; the other methods and
+// mlp_limiting run in the generic one (three-cell halo)
+int sweep_variant() {
+  const int r = C.p.reconstruction;
+  if (C.p.mlp || (r != AMUN_REC_TVD && r != AMUN_REC_WENO5Z)) return REC_GEN;
+  return r;
+}
+int sweep_halo() {
+  const int v = sweep_variant();
+  return v == REC_GEN ? 3 : (v == AMUN_REC_WENO5Z ? 2 : 1);
+}
+
 MethodConst method_const() {
   MethodConst m;
   m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.gammaxi = C.gammam1 / C.gamma;
@@ -315,6 +329,8 @@ MethodConst method_const() {
   m.csnd = C.p.csnd;
   m.c2p = C.p.c2p;
   m.mlp = C.p.mlp;
+  m.rec = C.p.reconstruction;
+  m.rc.rad = C.p.limo3_rad; m.rc.ppm = C.p.ppm_const; m.rc.kappa = C.p.kappa; m.rc.kbeta = C.p.kbeta;
   m.states_4vec = relativistic() ? C.p.states_4vec : 0;
   return m;
 }
@@ -340,7 +356,7 @@ template <typename R>
 int launch_stage(const StageDesc& st) {
   int LP, LW;
   tile_shape(LP, LW);
-  const int RR = C.p.reconstruction == AMUN_REC_WENO5Z ? 2 : 1;
+  const int RR = sweep_halo();
   const int threads = (((LP + 2) * LW + 31) / 32) * 32;
   const size_t smem = (size_t)C.nv * ((LP + 2 * RR + 2) + 2 * (LP + 2)) * LW * sizeof(R);
   const int nthird = C.g.ndims == 3 ? C.g.nc : 1;
@@ -353,6 +369,7 @@ int launch_stage(const StageDesc& st) {
   a.qout = (R*)C.q[1 - C.cur];
   a.sc = C.sc;
   a.binv = C.binv;
+  a.bdx = C.bdx;
   a.g = C.g;
   a.m = method_const();
   a.st = st;
@@ -364,7 +381,7 @@ int launch_stage(const StageDesc& st) {
     a.last = d == C.g.ndims - 1;
     ProfScope ps(d);
     if (!C.amr) {
-      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, grid, threads, smem, C.stream);
+      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, sweep_variant(), rs, d, a, grid, threads, smem, C.stream);
       if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
       continue;
     }
@@ -374,7 +391,7 @@ int launch_stage(const StageDesc& st) {
     for (const auto& grp : C.lgroups) {
       a.blist = C.blist + grp.first;
       dim3 gl(grid.x, grp.second);
-      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, C.p.reconstruction, rs, d, a, gl, threads, smem, C.stream);
+      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, sweep_variant(), rs, d, a, gl, threads, smem, C.stream);
       if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
     }
   }
@@ -446,7 +463,21 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.states_4vec = relativistic() ? C.p.states_4vec : 0;
   u.clip = C.p.clip_extrema; u.positivity = C.p.fix_positivity;
   u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd; u.c2p = C.p.c2p; u.mlp = C.p.mlp;
+  u.h[0] = u.h[1] = u.h[2] = 0.0;
+  u.rad = C.p.limo3_rad; u.ppm = C.p.ppm_const; u.kappa = C.p.kappa; u.kbeta = C.p.kbeta;
   return u;
+}
+
+// the block's cell sizes (host array of NDIMS entries), which WENO3 and
+// LimO3 use; the other methods do not read them and accept NULL
+int unit_cell_sizes(const double* dx, UnitArgs& u) {
+  if (!dx) {
+    if (C.p.reconstruction == AMUN_REC_WENO3 || C.p.reconstruction == AMUN_REC_LIMO3)
+      return fail(AMUN_E_BAD_ARGUMENT, "dx is needed by this reconstruction");
+    return 0;
+  }
+  for (int d = 0; d < C.p.ndims; ++d) u.h[d] = dx[d];
+  return 0;
 }
 
 // scratch device buffers for the unit entry points
@@ -489,6 +520,10 @@ void amun_gpu_default_params(amun_params* p) {
   p->csnd = 1.0;
   p->c2p = AMUN_C2P_1DW;
   p->mlp = 0;
+  p->limo3_rad = 0.5;
+  p->ppm_const = 1.25;
+  p->kappa = 1.0;
+  p->kbeta = 1.0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -524,6 +559,17 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "reconstruction") {
     if (is_one_of(v, {"tvd", "TVD"})) p->reconstruction = AMUN_REC_TVD;
     else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p->reconstruction = AMUN_REC_WENO5Z;
+    else if (is_one_of(v, {"weno3", "WENO3"})) p->reconstruction = AMUN_REC_WENO3;
+    else if (is_one_of(v, {"limo3", "LIMO3", "LimO3"})) p->reconstruction = AMUN_REC_LIMO3;
+    else if (is_one_of(v, {"ppm", "PPM"})) p->reconstruction = AMUN_REC_PPM;
+    else if (is_one_of(v, {"weno5yc", "weno5-yc", "WENO5YC", "WENO5-YC"})) p->reconstruction = AMUN_REC_WENO5YC;
+    else if (is_one_of(v, {"weno5ns", "weno5-ns", "WENO5NS", "WENO5-NS"})) p->reconstruction = AMUN_REC_WENO5NS;
+    else if (is_one_of(v, {"mp5", "MP5"})) p->reconstruction = AMUN_REC_MP5;
+    else if (is_one_of(v, {"mp7", "MP7"})) p->reconstruction = AMUN_REC_MP7;
+    else if (is_one_of(v, {"crweno5z", "crweno5-z", "CRWENO5Z", "CRWENO5-Z", "crweno5yc", "crweno5-yc", "CRWENO5YC",
+                           "CRWENO5-YC", "crweno5ns", "crweno5-ns", "CRWENO5NS", "CRWENO5-NS", "crmp5", "CRMP5",
+                           "crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD", "crmp7", "CRMP7", "gp", "GP", "mgp", "MGP"}))
+      return fail(AMUN_E_UNSUPPORTED, std::string("reconstruction not implemented here: ") + v);
     else return fail(200, std::string("reconstruction not implemented: ") + v);
   } else if (k == "limiter" || k == "extrema_limiter" || k == "prolongation_limiter") {
     int l = AMUN_LIM_ZERO;
@@ -553,6 +599,10 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   } else if (k == "stages") p->stages = atoi(v);
   else if (k == "fix_positivity") p->fix_positivity = is_on(v);
   else if (k == "mlp_limiting") p->mlp = is_on(v);
+  else if (k == "limo3_rad") p->limo3_rad = atof(v);
+  else if (k == "ppm_const") p->ppm_const = atof(v);
+  else if (k == "kappa") p->kappa = atof(v);
+  else if (k == "kbeta") p->kbeta = atof(v);
   else if (k == "clip_extrema") p->clip_extrema = is_on(v);
   else if (k == "precision") {
     if (is_one_of(v, {"fp32", "FP32", "fp32_bulk", "bulk"})) p->precision = AMUN_FP32_BULK;
@@ -579,9 +629,11 @@ int amun_gpu_init(const amun_params* p) {
   if ((p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD) &&
       (p->c2p < AMUN_C2P_1DW || p->c2p > AMUN_C2P_2DWU))
     return fail(110, "primitive solver not implemented");
-  if (p->reconstruction != AMUN_REC_TVD && p->reconstruction != AMUN_REC_WENO5Z)
+  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_MP7)
     return fail(200, "reconstruction not implemented");
-  int need = p->reconstruction == AMUN_REC_WENO5Z ? 3 : 2;
+  // the stencil reach of each method beyond its cell, plus the cell itself
+  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4};
+  int need = kNeed[p->reconstruction];
   if (p->nghosts < need || p->ncells < p->nghosts)
     return fail(AMUN_E_BAD_ARGUMENT, "nghosts too small for the reconstruction stencil (or ncells < nghosts)");
   int ndev = 0;
@@ -593,6 +645,8 @@ int amun_gpu_init(const amun_params* p) {
   if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
   CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
+  // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
+  if (C.p.reconstruction == AMUN_REC_LIMO3) C.p.eps = C.p.eps > 1.0e-12 ? C.p.eps : 1.0e-12;
   C.nv = (p->eqsys == AMUN_EQ_HD || p->eqsys == AMUN_EQ_SRHD) ? 5 : 9;
   if (p->eos == AMUN_EOS_ISO) {
     // kernels take the isothermal systems as systems of their own
@@ -828,12 +882,15 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   CK(dset(C.u1, 0, ubytes * rs));
   C.pool_bytes = (long long)(2 * qbytes + ubytes * (sizeof(double) + 2 * rs));
   std::vector<int> nbr(27 * (size_t)nblocks);
-  std::vector<double> binv(3 * (size_t)nblocks);
+  std::vector<double> binv(3 * (size_t)nblocks), bdx(3 * (size_t)nblocks);
   C.dx_min = 1e300;
   for (int b = 0; b < nblocks; ++b) {
     for (int n = 0; n < 27; ++n) nbr[27 * b + n] = blocks[b].neighbor[n];
     nbr[27 * b + 13] = b;
-    for (int d = 0; d < 3; ++d) binv[3 * b + d] = 1.0 / blocks[b].dx[d];
+    for (int d = 0; d < 3; ++d) {
+      binv[3 * b + d] = 1.0 / blocks[b].dx[d];
+      bdx[3 * b + d] = blocks[b].dx[d];
+    }
     // dx_min of the finest level (src/evolution.F90:465-475)
     double m = blocks[b].dx[0] < blocks[b].dx[1] ? blocks[b].dx[0] : blocks[b].dx[1];
     if (nd == 3) m = m < blocks[b].dx[2] ? m : blocks[b].dx[2];
@@ -843,6 +900,8 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   CK(cudaMalloc(&C.binv, binv.size() * sizeof(double)));
   CK(h2d(C.nbr, nbr.data(), nbr.size() * sizeof(int)));
   CK(h2d(C.binv, binv.data(), binv.size() * sizeof(double)));
+  CK(cudaMalloc(&C.bdx, bdx.size() * sizeof(double)));
+  CK(h2d(C.bdx, bdx.data(), bdx.size() * sizeof(double)));
   C.cur = 0;
   C.ms_valid = false;
   if (levels_differ) {
@@ -1077,12 +1136,12 @@ int amun_gpu_set_time(double time, double dt) {
 }
 
 int amun_gpu_update_flux_block(const double* dx, const double* q, double* f) {
-  (void)dx;  // the adiabatic HD/MHD flux of the reference does not use dx
   if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   if (!q || !f) return fail(AMUN_E_BAD_ARGUMENT, "null array");
   const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
   const int im = nc + 2 * ng, jm = im, km = nd == 3 ? im : 1;
   UnitArgs u = unit_args(im, jm, km);
+  if (int r = unit_cell_sizes(dx, u)) return r;
   size_t cells = (size_t)im * jm * km;
   DevBuf dq, dqs, df, dsc, dnp;
   CK(cudaMalloc(&dq.p, cells * C.nv * sizeof(double)));
@@ -1245,12 +1304,12 @@ int require_device_pointer(const void* p, const char* name) {
 }  // namespace
 
 extern "C" int amun_gpu_update_flux_block_noalloc(const double* dx, const double* q, double* f) {
-  (void)dx;  // the adiabatic flux does not use dx
   if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   if (!q || !f) return fail(AMUN_E_BAD_ARGUMENT, "null array");
   const int nc = C.p.ncells, ng = C.p.nghosts, nd = C.p.ndims;
   const int im = nc + 2 * ng, jm = im, km = nd == 3 ? im : 1;
   UnitArgs u = unit_args(im, jm, km);
+  if (int r = unit_cell_sizes(dx, u)) return r;
   const size_t cells = (size_t)im * jm * km;
   const size_t qs_bytes = cells * C.nv * 2 * nd * sizeof(double);
   const size_t sc_bytes = unit_block_flux_scratch(u);
@@ -1565,7 +1624,7 @@ int amun_gpu_autotune(int reps, int* best_lp, int* best_lw, double* best_ms) {
   // candidates: LP cells along the sweep x LW lanes, both dividing ncells,
   // at most 288 threads ((LP + 2) LW) and 200 KB of shared memory
   std::vector<std::pair<int, int>> cand;
-  const int RR = C.p.reconstruction == AMUN_REC_WENO5Z ? 2 : 1;
+  const int RR = sweep_halo();
   for (int lp = 4; lp <= nc && lp <= 128; lp *= 2) {
     if (nc % lp) continue;
     std::vector<int> lws;

@@ -103,7 +103,8 @@ template <typename R, typename U1T, int EQ>
 cudaError_t sweep_eq(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                      cudaStream_t s) {
   if (rec == REC_WENO5Z) return go_rs<R, U1T, EQ, REC_WENO5Z>(rs, dir, a, grid, threads, smem, s);
-  return go_rs<R, U1T, EQ, REC_TVD>(rs, dir, a, grid, threads, smem, s);
+  if (rec == REC_TVD) return go_rs<R, U1T, EQ, REC_TVD>(rs, dir, a, grid, threads, smem, s);
+  return go_rs<R, U1T, EQ, REC_GEN>(rs, dir, a, grid, threads, smem, s);
 }
 #endif  // AMUN_SWEEP_IMPL
 

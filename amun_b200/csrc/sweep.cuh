@@ -23,6 +23,12 @@
 #include "physics.cuh"
 
 namespace amun {
+// the sweep variant that chooses its reconstruction at run time and can
+// apply mlp_limiting (the TVD and WENO-Z variants carry neither)
+enum { REC_GEN = 100 };
+}
+
+namespace amun {
 
 struct Geo {
   int nc, ng, ndims;
@@ -59,6 +65,8 @@ struct MethodConst {
   int nrmax, nrext, states_4vec;
   int c2p;  // relativistic recovery method
   int mlp;  // multi-dimensional limiting process (mlp_limiting)
+  int rec;  // reconstruction method (run-time choice of the generic sweep)
+  RecConst rc;
   int plim;  // prolongation limiter (limiter_prol)
   double csnd;  // isothermal sound speed
 };
@@ -81,6 +89,7 @@ template <typename R, typename U1T> struct SweepArgs {
   R* qout;             // stage output primitives (padded)
   DevScalars* sc;
   const double* binv;  // per block 1/dx, 1/dy, 1/dz
+  const double* bdx;   // per block dx, dy, dz
   Geo g;
   MethodConst m;
   StageDesc st;
@@ -117,6 +126,48 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* t
   }
 }
 
+// mlp_limiting (src/interpolations.F90:1171-1321) for one cell's two faces
+// along DIR: fR (the left state of its right interface) and fL (the right
+// state of its left interface), in the reconstruction frame.  With two ghost
+// layers the first cell of a line (TVD: a ghost copy, both faces q; the
+// others: its right face the line-end average) is limited first with its
+// lower neighbour clamped to itself, and rewrites the second cell's left
+// face; that is reproduced for the second cell (P == 1).
+template <int EQ, int DIR, typename R>
+__device__ __forceinline__ void mlp_faces(const R* qb, const Geo& g, bool four, int rec, int P, int Lc, int t0, int v,
+                                          R f0, R& fR, R& fL) {
+  using V = Var<EQ>;
+  const int ci = DIR == 0 ? P : Lc, cj = DIR == 1 ? P : (DIR == 0 ? Lc : t0), ck = DIR == 2 ? P : t0;
+  auto qat = [&](int i, int j, int k) -> R {
+    i = i < 0 ? 0 : (i >= g.IM ? g.IM - 1 : i);
+    j = j < 0 ? 0 : (j >= g.JM ? g.JM - 1 : j);
+    k = g.ndims == 3 ? (k < 0 ? 0 : (k >= g.KM ? g.KM - 1 : k)) : 0;
+    const R* qc = qb + ((long long)k * g.JM + j) * g.IM + i;
+    if (V::SR && four && v <= 3) {
+      R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
+      return ld_ro(qc + (long long)v * g.qvs) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
+    }
+    return ld_ro(qc + (long long)v * g.qvs);
+  };
+  R dq[3];
+  mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ci + di, cj + dj, ck + dk); }, g.ndims, dq);
+  R fLcur = fL;
+  if (P == 1) {
+    const int ai = DIR == 0 ? 0 : ci, aj = DIR == 1 ? 0 : cj, ak = DIR == 2 ? 0 : ck;
+    R dq0[3];
+    mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ai + di, aj + dj, ak + dk); }, g.ndims, dq0);
+    const R q00 = qat(ai, aj, ak);
+    const R r0 = rec == REC_TVD ? q00 : R(0.5) * (q00 + f0);
+    if (d_max(d_fabs(r0 - q00), d_fabs(fL - q00)) > d_fabs(dq0[DIR])) fLcur = q00 - dq0[DIR];
+  }
+  if (d_max(d_fabs(fR - f0), d_fabs(fLcur - f0)) > d_fabs(dq[DIR])) {
+    fR = f0 + dq[DIR];
+    fL = f0 - dq[DIR];
+  } else {
+    fL = fLcur;
+  }
+}
+
 template <int EQ, int REC, int RS, int DIR, typename R, typename U1T>
 #ifndef AMUN_SWEEP_MIN_BLOCKS
 #define AMUN_SWEEP_MIN_BLOCKS 1
@@ -127,7 +178,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   using V = Var<EQ>;
   constexpr int NV = V::NV;
   const bool four = V::SR && a.m.states_4vec;
-  constexpr int RR = (REC == REC_WENO5Z) ? 2 : 1;
+  constexpr int RR = REC == REC_WENO5Z ? 2 : (REC == REC_GEN ? 3 : 1);
   const Geo& g = a.g;
   const int LP = a.LP, LW = a.LW;
   const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
@@ -163,9 +214,14 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   };
 
   // ---- load the tile and its halo --------------------------------------------
+  // (the generic variant's three-cell halo is clamped to the block: methods
+  // with shorter stencils run with fewer ghost layers and never read it)
+  const int PM = DIR == 0 ? g.IM : (DIR == 1 ? g.JM : g.KM);
   for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
     int pp, ll; decode(t, NPQ, pp, ll);
-    long long c = (long long)(p0 - RR - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+    int pi = p0 - RR - 1 + pp;
+    if constexpr (REC == REC_GEN) pi = pi < 0 ? 0 : (pi >= PM ? PM - 1 : pi);
+    long long c = (long long)pi * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
     R qc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = ld_ro(qb + c + v * g.qvs);
@@ -175,11 +231,64 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
 #pragma unroll
     for (int v = 0; v < NV; ++v) Qs[sidx(v, pp, ll, NPQ)] = qc[v];
   }
+  (void)PM;
   __syncthreads();
 
   // ---- reconstruct both faces of cells p0-1 .. p0+LP ---------------------------
+  const bool mlp = REC == REC_GEN && a.m.mlp;
   {
     const R eps = R(a.m.eps);
+    // interfaces_tvd src/interpolations.F90:729-848 for one variable of one
+    // cell: limited half-slopes, for the positive variables in every
+    // direction and halved together while q <= sum|dq|
+    auto tvd = [&](int v, int pp, int ll, R f0, R fm1, R fp1, bool positive, R& fR, R& fL) {
+      R dqd;
+      if (!positive) {
+        dqd = limiter<R>(a.m.lim, R(0.5), f0 - fm1, fp1 - f0, eps);
+      } else {
+        const long long c = (long long)(p0 - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+        const R* qv = qb + (long long)v * g.qvs + c;
+        // neighbour value, as a 4-vector density when the states are
+        // reconstructed in 4-vector form
+        auto nq = [&](long long off) -> R {
+          if (V::SR && four && v == V::DN) {
+            const R* qc = qb + c + off;
+            R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
+            return ld_ro(qc) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
+          }
+          return ld_ro(qv + off);
+        };
+        R dq[3];
+        dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sX), nq(sX) - f0, eps);
+        dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sY), nq(sY) - f0, eps);
+        dq[2] = R(0);
+        if (g.ndims == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sZ), nq(sZ) - f0, eps);
+        if (f0 > R(0)) {
+          for (int it = 0; it < 4096; ++it) {
+            R s = d_fabs(dq[0]) + d_fabs(dq[1]);
+            if (g.ndims == 3) s = s + d_fabs(dq[2]);
+            if (!(f0 <= s)) break;
+            dq[0] = R(0.5) * dq[0]; dq[1] = R(0.5) * dq[1]; dq[2] = R(0.5) * dq[2];
+          }
+        } else {
+          dq[0] = dq[1] = dq[2] = R(0);
+          // counted once per cell and stage: in the x sweep, tile cells only
+          if (DIR == 0 && pp >= 1 && pp <= LP) atomicAdd(&a.sc->nonpositive, 1ull);
+        }
+        dqd = dq[DIR];
+      }
+      fR = f0 + dqd;
+      fL = f0 - dqd;
+    };
+    // interfaces_dir src/interpolations.F90:867-959 -> reconstruct 1343-1381:
+    // clip_extrema and fix_positivity restated per cell
+    auto dir_fix = [&](R fm1, R f0, R fp1, bool positive, R& fR, R& fL) {
+      if (a.m.clip) clip_cell(fm1, f0, fp1, a.m.clim, eps, fR, fL);
+      // fix_positivity src/interpolations.F90:4987-5062 per cell
+      if (positive && a.m.positivity && (fR <= R(0) || fL <= R(0))) { fR = f0; fL = f0; }
+    };
+    const R h = REC == REC_GEN ? R(a.bdx[3 * b + DIR]) : R(0);
+    (void)h;
     for (int t = threadIdx.x; t < NPF * LW; t += blockDim.x) {
       int pp, ll; decode(t, NPF, pp, ll);
       const int cq = pp + RR;  // index of this cell in Qs
@@ -188,100 +297,34 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       for (int v = 0; v < NV; ++v) {
         R fR, fL;
         const R f0 = Qs[sidx(v, cq, ll, NPQ)];
+        const R fm1 = Qs[sidx(v, cq - 1, ll, NPQ)], fp1 = Qs[sidx(v, cq + 1, ll, NPQ)];
         const bool positive = (v == V::DN || v == V::PR);
         if constexpr (REC == REC_WENO5Z) {
-          // interfaces_dir src/interpolations.F90:867-959 -> reconstruct
-          // 1343-1381 -> reconstruct_weno5z (main loop, 1997-2066)
-          const R fm2 = Qs[sidx(v, cq - 2, ll, NPQ)], fm1 = Qs[sidx(v, cq - 1, ll, NPQ)];
-          const R fp1 = Qs[sidx(v, cq + 1, ll, NPQ)], fp2 = Qs[sidx(v, cq + 2, ll, NPQ)];
+          // reconstruct_weno5z (main loop, 1997-2066)
+          const R fm2 = Qs[sidx(v, cq - 2, ll, NPQ)], fp2 = Qs[sidx(v, cq + 2, ll, NPQ)];
           weno5z_faces(fm2, fm1, f0, fp1, fp2, eps, fR, fL);
-          if (a.m.clip) clip_cell(fm1, f0, fp1, a.m.clim, eps, fR, fL);
-          // fix_positivity src/interpolations.F90:4987-5062 per cell
-          if (positive && a.m.positivity && (fR <= R(0) || fL <= R(0))) { fR = f0; fL = f0; }
+          dir_fix(fm1, f0, fp1, positive, fR, fL);
+        } else if constexpr (REC == REC_TVD) {
+          tvd(v, pp, ll, f0, fm1, fp1, positive, fR, fL);
         } else {
-          // interfaces_tvd src/interpolations.F90:729-848
-          const R fm1 = Qs[sidx(v, cq - 1, ll, NPQ)], fp1 = Qs[sidx(v, cq + 1, ll, NPQ)];
-          R dqd;
-          if (!positive) {
-            dqd = limiter<R>(a.m.lim, R(0.5), f0 - fm1, fp1 - f0, eps);
+          // any method, chosen at run time (src/interpolations.F90:226-382)
+          const int rec = a.m.rec;
+          if (rec == REC_TVD) {
+            tvd(v, pp, ll, f0, fm1, fp1, positive, fR, fL);
           } else {
-            // multi-dimensional slopes, halved together while q <= sum|dq|
-            const long long c = (long long)(p0 - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
-            const R* qv = qb + (long long)v * g.qvs + c;
-            // neighbour value, as a 4-vector density when the states are
-            // reconstructed in 4-vector form
-            auto nq = [&](long long off) -> R {
-              if (V::SR && four && v == V::DN) {
-                const R* qc = qb + c + off;
-                R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
-                return ld_ro(qc) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
-              }
-              return ld_ro(qv + off);
-            };
-            R dq[3];
-            dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sX), nq(sX) - f0, eps);
-            dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sY), nq(sY) - f0, eps);
-            dq[2] = R(0);
-            if (g.ndims == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - nq(-sZ), nq(sZ) - f0, eps);
-            if (f0 > R(0)) {
-              for (int it = 0; it < 4096; ++it) {
-                R s = d_fabs(dq[0]) + d_fabs(dq[1]);
-                if (g.ndims == 3) s = s + d_fabs(dq[2]);
-                if (!(f0 <= s)) break;
-                dq[0] = R(0.5) * dq[0]; dq[1] = R(0.5) * dq[1]; dq[2] = R(0.5) * dq[2];
-              }
-            } else {
-              dq[0] = dq[1] = dq[2] = R(0);
-              // counted once per cell and stage: in the x sweep, tile cells only
-              if (DIR == 0 && pp >= 1 && pp <= LP) atomicAdd(&a.sc->nonpositive, 1ull);
-            }
-            dqd = dq[DIR];
-          }
-          fR = f0 + dqd;
-          fL = f0 - dqd;
-        }
-        if (a.m.mlp) {
-          // mlp_limiting src/interpolations.F90:1171-1321 for this cell's
-          // two faces along DIR (in the reconstruction frame: 4-vector
-          // states when four)
-          const int P = p0 - 1 + pp, Lc = l0 + ll;
-          const int ci = DIR == 0 ? P : Lc, cj = DIR == 1 ? P : (DIR == 0 ? Lc : t0), ck = DIR == 2 ? P : t0;
-          auto qat = [&](int i, int j, int k) -> R {
-            i = i < 0 ? 0 : (i >= g.IM ? g.IM - 1 : i);
-            j = j < 0 ? 0 : (j >= g.JM ? g.JM - 1 : j);
-            k = g.ndims == 3 ? (k < 0 ? 0 : (k >= g.KM ? g.KM - 1 : k)) : 0;
-            const R* qc = qb + ((long long)k * g.JM + j) * g.IM + i;
-            if (V::SR && four && v <= 3) {
-              R vx = ld_ro(qc + g.qvs), vy = ld_ro(qc + 2 * g.qvs), vz = ld_ro(qc + 3 * g.qvs);
-              return ld_ro(qc + (long long)v * g.qvs) / d_sqrt(R(1) - (vx * vx + vy * vy + vz * vz));
-            }
-            return ld_ro(qc + (long long)v * g.qvs);
-          };
-          R dq[3];
-          mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ci + di, cj + dj, ck + dk); }, g.ndims, dq);
-          R fLcur = fL;
-          if (REC == REC_TVD && P == 1) {
-            // two ghost layers: the first cell of the line (a ghost copy,
-            // both faces = q) is limited first, with its lower neighbour
-            // clamped to itself, and writes this cell's left face
-            const int ai = DIR == 0 ? 0 : ci, aj = DIR == 1 ? 0 : cj, ak = DIR == 2 ? 0 : ck;
-            R dq0[3];
-            mlp_slopes<R>([&](int di, int dj, int dk) { return qat(ai + di, aj + dj, ak + dk); }, g.ndims, dq0);
-            const R q00 = qat(ai, aj, ak);
-            if (d_max(d_fabs(q00 - q00), d_fabs(fL - q00)) > d_fabs(dq0[DIR])) fLcur = q00 - dq0[DIR];
-          }
-          if (d_max(d_fabs(fR - f0), d_fabs(fLcur - f0)) > d_fabs(dq[DIR])) {
-            fR = f0 + dq[DIR];
-            fL = f0 - dq[DIR];
-          } else {
-            fL = fLcur;
+            R st[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) st[k] = Qs[sidx(v, cq - 3 + k, ll, NPQ)];
+            if (rec == REC_WENO5Z) weno5z_faces(st[1], fm1, f0, fp1, st[5], eps, fR, fL);
+            else dir_faces<R>(rec, st, h, eps, a.m.rc, fR, fL);
+            dir_fix(fm1, f0, fp1, positive, fR, fL);
           }
         }
         fRv[v] = fR;
         fLv[v] = fL;
       }
       if constexpr (V::SR) {
-        if (four) { from_four_velocity(fRv); from_four_velocity(fLv); }
+        if (four && !mlp) { from_four_velocity(fRv); from_four_velocity(fLv); }
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
@@ -291,6 +334,36 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     }
   }
   __syncthreads();
+
+  // ---- mlp_limiting src/interpolations.F90:1171-1321: a separate pass over
+  // the staged faces (in the reconstruction frame: 4-vector states when
+  // four), converted back afterwards; generic variant only
+  if constexpr (REC == REC_GEN) {
+    if (mlp) {
+      for (int t = threadIdx.x; t < NPF * LW * NV; t += blockDim.x) {
+        const int v = t / (NPF * LW);
+        int pp, ll; decode(t - v * (NPF * LW), NPF, pp, ll);
+        mlp_faces<EQ, DIR, R>(qb, g, four, a.m.rec, p0 - 1 + pp, l0 + ll, t0, v, Qs[sidx(v, pp + RR, ll, NPQ)],
+                              FLs[sidx(v, pp, ll, NPF)], FRs[sidx(v, pp, ll, NPF)]);
+      }
+      __syncthreads();
+      if constexpr (V::SR) {
+        if (four) {
+          for (int t = threadIdx.x; t < NPF * LW; t += blockDim.x) {
+            int pp, ll; decode(t, NPF, pp, ll);
+            R a4[NV], b4[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { a4[v] = FLs[sidx(v, pp, ll, NPF)]; b4[v] = FRs[sidx(v, pp, ll, NPF)]; }
+            from_four_velocity(a4);
+            from_four_velocity(b4);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { FLs[sidx(v, pp, ll, NPF)] = a4[v]; FRs[sidx(v, pp, ll, NPF)] = b4[v]; }
+          }
+          __syncthreads();
+        }
+      }
+    }
+  }
 
   // ---- Riemann problems at interfaces (p0-1)+1/2 .. (p0+LP-1)+1/2 -------------
   {

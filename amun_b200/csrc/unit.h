@@ -12,6 +12,8 @@ struct UnitArgs {
   double gamma, gammaxi, eps, cmax, csnd;
   double tol, pmin;
   int nrmax, nrext, states_4vec, c2p, mlp;
+  double h[3];                      // dx, dy, dz of the block
+  double rad, ppm, kappa, kbeta;    // reconstruction constants
 };
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,

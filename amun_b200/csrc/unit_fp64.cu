@@ -115,13 +115,157 @@ __global__ void mlp_cells(const double* q, double* qs, BlockDims d, int phase) {
   }
 }
 
+// ---- the line forms of the explicit reconstructions, line ends included
+// (src/interpolations.F90:1469-1913, 2107-2441, 3675-3901, 5209-5284): the
+// main loops through the per-cell forms of recon.cuh, the ends as written.
+__device__ void line_ends_average(int n, const double* f, double* fl, double* fr) {
+  fl[0] = 0.5 * (f[0] + f[1]);
+  fr[n - 2] = 0.5 * (f[n - 2] + f[n - 1]);
+  fl[n - 1] = f[n - 1];
+  fr[n - 1] = f[n - 1];
+}
+__device__ void line_ends_weno5(int n, const double* f, double* fl, double* fr, int lim, double eps) {
+  fl[0] = 0.5 * (f[0] + f[1]);
+  double df = limiter<double>(lim, 0.5, f[1] - f[0], f[2] - f[1], eps);
+  fr[0] = f[1] - df;
+  fl[1] = f[1] + df;
+  const int i = n - 2;
+  df = limiter<double>(lim, 0.5, f[i] - f[i - 1], f[i + 1] - f[i], eps);
+  fr[i - 1] = f[i] - df;
+  fl[i] = f[i] + df;
+  fr[i] = 0.5 * (f[i] + f[n - 1]);
+  fl[n - 1] = f[n - 1];
+  fr[n - 1] = f[n - 1];
+}
+// reconstruct_ppm src/interpolations.F90:1746-1913 on a whole line; fi and
+// df2 are scratch of n entries each
+__device__ void line_ppm(int n, const double* f, double* fl, double* fr, double* fi, double* df2, double pc) {
+  fi[0] = 0.5 * (f[0] + f[1]);
+  for (int i = 1; i <= n - 3; ++i) fi[i] = (7.0 * (f[i] + f[i + 1]) - (f[i - 1] + f[i + 2])) / 12.0;
+  fi[n - 2] = 0.5 * (f[n - 2] + f[n - 1]);
+  fi[n - 1] = f[n - 1];
+  df2[0] = 0.0;
+  for (int i = 1; i <= n - 2; ++i) df2[i] = (f[i + 1] + f[i - 1]) - 2.0 * f[i];
+  df2[n - 1] = 0.0;
+  for (int i = 1; i <= n - 3; ++i) {
+    if ((f[i + 1] - fi[i]) * (fi[i] - f[i]) < 0.0) {
+      const double df2c = 3.0 * ((f[i + 1] + f[i]) - 2.0 * fi[i]);
+      const double df2m = df2[i], df2p = df2[i + 1];
+      double df2l;
+      if (d_min(d_min(df2c, df2m), df2p) * d_max(d_max(df2c, df2m), df2p) > 0.0)
+        df2l = fsign(d_min(pc * d_min(fabs(df2m), fabs(df2p)), fabs(df2c)), df2c);
+      else
+        df2l = 0.0;
+      fi[i] = 0.5 * (f[i] + f[i + 1]) - df2l / 6.0;
+    }
+  }
+  for (int i = 1; i <= n - 2; ++i) {
+    double alm = fi[i - 1] - f[i];
+    double alp = fi[i] - f[i];
+    const bool cm = fabs(alm) >= 2.0 * fabs(alp);
+    const bool cp = fabs(alp) >= 2.0 * fabs(alm);
+    bool ext = false;
+    if (alm * alp > 0.0) {
+      ext = true;
+    } else if (cm || cp) {
+      const int im2 = i - 1 > 0 ? i - 1 : 0;  // max(1, i - 1), 1-based
+      const double dfm = fi[i - 1] - fi[im2];
+      const double dfp = fi[i + 1] - fi[i];
+      const double dcm = f[i] - f[i - 1];
+      const double dcp = f[i + 1] - f[i];
+      if (d_min(fabs(dfm), fabs(dfp)) >= d_min(fabs(dcm), fabs(dcp))) ext = dfm * dfp < 0.0;
+      else ext = dcm * dcp < 0.0;
+    }
+    if (ext) {
+      const double df2s = 6.0 * (alm + alp);
+      const double df2m = df2[i - 1], df2c = df2[i], df2p = df2[i + 1];
+      if (d_min(d_min(d_min(df2s, df2c), df2m), df2p) * d_max(d_max(d_max(df2s, df2c), df2m), df2p) > 0.0) {
+        const double df2l = fsign(d_min(pc * d_min(d_min(fabs(df2m), fabs(df2c)), fabs(df2p)), fabs(df2s)), df2s);
+        if (fabs(df2l) > 0.0) {
+          alm = alm * df2l / df2s;
+          alp = alp * df2l / df2s;
+        } else {
+          alm = 0.0;
+          alp = 0.0;
+        }
+      } else {
+        alm = 0.0;
+        alp = 0.0;
+      }
+    } else {
+      if (cp) {
+        const double sgn = fsign(1.0, alp);
+        const double amx = -(0.25 * (alp * alp) / (alp + alm));
+        const double dfp = f[i + 1] - f[i];
+        if (sgn * amx >= sgn * dfp) {
+          const double del = dfp * (dfp - alm);
+          if (del >= 0.0) alp = -2.0 * (dfp + sgn * sqrt(del));
+          else alp = -2.0 * alm;
+        }
+      }
+      if (cm) {
+        const double sgn = fsign(1.0, alm);
+        const double amx = -(0.25 * (alm * alm) / (alp + alm));
+        const double dfm = f[i - 1] - f[i];
+        if (sgn * amx >= sgn * dfm) {
+          const double del = dfm * (dfm - alp);
+          if (del >= 0.0) alm = -2.0 * (dfm + sgn * sqrt(del));
+          else alm = -2.0 * alp;
+        }
+      }
+    }
+    fr[i - 1] = f[i] + alm;
+    fl[i] = f[i] + alp;
+  }
+  fl[0] = fi[0];
+  fr[n - 2] = fi[n - 1];
+  fl[n - 1] = fi[n - 1];
+  fr[n - 1] = f[n - 1];
+}
+// reconstruct_mp5 / reconstruct_mp7 (src/interpolations.F90:3675-3901) with
+// mp_limiting (5209-5284) on a whole line read in direction dir (+1 / -1):
+// u[0..n-1] receives the limited left states of the (possibly reversed) line
+__device__ void line_mp(int order, int n, const double* fc, int dir, double* u, double kappa, double kbeta, double eps) {
+  auto F = [&](int i) { return dir > 0 ? fc[i] : fc[n - 1 - i]; };
+  const double ce2[2] = {0.5, 0.5};
+  const double ce3[3] = {-1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0};
+  const double ce5[5] = {2.0 / 60.0, -13.0 / 60.0, 47.0 / 60.0, 27.0 / 60.0, -3.0 / 60.0};
+  const double ce7[7] = {-3.0 / 420.0, 25.0 / 420.0, -101.0 / 420.0, 319.0 / 420.0, 214.0 / 420.0, -38.0 / 420.0,
+                         4.0 / 420.0};
+  auto sum = [&](const double* c, int m, int i0) {
+    double s = 0.0;
+    for (int k = 0; k < m; ++k) s = s + c[k] * F(i0 + k);
+    return s;
+  };
+  if (order == 5) {
+    for (int i = 2; i <= n - 3; ++i) u[i] = sum(ce5, 5, i - 2);
+    u[0] = sum(ce2, 2, 0);
+    u[1] = sum(ce3, 3, 0);
+    u[n - 2] = sum(ce3, 3, n - 3);
+  } else {
+    for (int i = 3; i <= n - 4; ++i) u[i] = sum(ce7, 7, i - 3);
+    u[0] = sum(ce2, 2, 0);
+    u[1] = sum(ce3, 3, 0);
+    u[2] = sum(ce5, 5, 0);
+    u[n - 3] = sum(ce5, 5, n - 5);
+    u[n - 2] = sum(ce3, 3, n - 3);
+  }
+  u[n - 1] = F(n - 1);
+  // dm(k) (1-based) = f(k) - f(k-1) for k = 2..n, zero outside
+  auto dm = [&](int k) { return (k >= 2 && k <= n) ? F(k - 1) - F(k - 2) : 0.0; };
+  for (int i1 = 1; i1 <= n - 1; ++i1)
+    u[i1 - 1] = mp_limit_core(dm(i1 - 1), dm(i1), dm(i1 + 1), dm(i1 + 2), F(i1 - 1), F(i1), u[i1 - 1], kappa, kbeta,
+                              eps);
+}
+
 // ---- interfaces_dir + reconstruct (src/interpolations.F90:867-959,
 // 1343-1381): one thread per (variable, line); the line is reconstructed
-// with reconstruct_weno5z (1937-2083) including its line-end fallbacks, then
-// clip_extrema (5081-5175) and fix_positivity (4987-5062) run sequentially.
+// by the chosen method including its line ends (reconstruct_weno5z
+// 1937-2083 and the line forms above), then clip_extrema (5081-5175) and
+// fix_positivity (4987-5062) run sequentially.
 template <int EQ>
-__global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int lim, int clim, double eps,
-                          int clip, int positivity, double* scratch) {
+__global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int rec, double h, RecConst rc, int lim,
+                          int clim, double eps, int clip, int positivity, double* scratch) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
   const int ni = d.im - 2 * d.ng + 2, nj = d.jm - 2 * d.ng + 2, nk = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
@@ -139,29 +283,49 @@ __global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int
     int c0 = (int)(l % a0) + d.ng - 1, c1 = (int)(l / a0) + (d.ndims == 3 || dir == 2 ? d.ng - 1 : 0);
     if (d.ndims == 2 && dir != 2) c1 = 0;
     long long base = c0 * s0 + c1 * s1;
-    double* f = scratch + t * 3LL * n;
+    double* f = scratch + t * 5LL * n;
     double* fl = f + n;
     double* fr = fl + n;
+    double* w1 = fr + n;
+    double* w2 = w1 + n;
     for (int p = 0; p < n; ++p) f[p] = q[(base + p * stride) * NV + v];
-    // main loop, i = 3 .. n-2 (1-based)
-    for (int i = 2; i <= n - 3; ++i) {
-      double a, b;
-      weno5z_faces<double>(f[i - 2], f[i - 1], f[i], f[i + 1], f[i + 2], eps, a, b);
-      fl[i] = a;
-      fr[i - 1] = b;
+    // reconstruct 1343-1381 by method: main loops, then the line ends
+    auto cell = [&](int i, double* st) {
+      for (int k = 0; k < 7; ++k) {
+        const int j = i - 3 + k;
+        st[k] = (j >= 0 && j < n) ? f[j] : 0.0;
+      }
+    };
+    if (rec == REC_WENO5Z || rec == REC_WENO5YC || rec == REC_WENO5NS) {
+      for (int i = 2; i <= n - 3; ++i) {  // i = 3 .. n-2 (1-based)
+        double a, b, st[7];
+        cell(i, st);
+        if (rec == REC_WENO5Z) weno5z_faces<double>(st[1], st[2], st[3], st[4], st[5], eps, a, b);
+        else if (rec == REC_WENO5YC) weno5_variant_faces<false>(st, eps, a, b);
+        else weno5_variant_faces<true>(st, eps, a, b);
+        fl[i] = a;
+        fr[i - 1] = b;
+      }
+      line_ends_weno5(n, f, fl, fr, lim, eps);  // (2069-2079)
+    } else if (rec == REC_WENO3 || rec == REC_LIMO3) {
+      for (int i = 1; i <= n - 2; ++i) {  // i = 2 .. n-1 (1-based)
+        double a, b, st[7];
+        cell(i, st);
+        if (rec == REC_WENO3) weno3_faces<double>(st, h, a, b);
+        else limo3_faces<double>(st, h, rc.rad, eps, a, b);
+        fl[i] = a;
+        fr[i - 1] = b;
+      }
+      line_ends_average(n, f, fl, fr);
+    } else if (rec == REC_PPM) {
+      line_ppm(n, f, fl, fr, w1, w2, rc.ppm);
+    } else {
+      const int order = rec == REC_MP5 ? 5 : 7;
+      line_mp(order, n, f, +1, fl, rc.kappa, rc.kbeta, eps);
+      line_mp(order, n, f, -1, w1, rc.kappa, rc.kbeta, eps);
+      for (int k = 0; k <= n - 2; ++k) fr[k] = w1[n - 2 - k];
+      line_ends_average(n, f, fl, fr);
     }
-    // line ends (2069-2079)
-    fl[0] = 0.5 * (f[0] + f[1]);
-    double df = limiter<double>(lim, 0.5, f[1] - f[0], f[2] - f[1], eps);
-    fr[0] = f[1] - df;
-    fl[1] = f[1] + df;
-    int i = n - 2;  // 0-based of Fortran n-1
-    df = limiter<double>(lim, 0.5, f[i] - f[i - 1], f[i + 1] - f[i], eps);
-    fr[i - 1] = f[i] - df;
-    fl[i] = f[i] + df;
-    fr[i] = 0.5 * (f[i] + f[n - 1]);
-    fl[n - 1] = f[n - 1];
-    fr[n - 1] = f[n - 1];
     if (clip) {
       for (int ii = 0; ii < n; ++ii) {
         int im1 = ii > 0 ? ii - 1 : 0, ip1 = ii < n - 1 ? ii + 1 : n - 1;
@@ -333,8 +497,9 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
     for (int dir = 0; dir < u.ndims; ++dir) {
       const int ni = u.im - 2 * u.ng + 2, nj = u.jm - 2 * u.ng + 2, nk = u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1;
       long long lines = (dir == 0 ? (long long)nj * nk : (dir == 1 ? (long long)ni * nk : (long long)ni * nj)) * NV;
-      dir_lines<EQ><<<(int)((lines + 127) / 128), 128, 0, s>>>(qr, qs, d, dir, u.lim, u.clim, u.eps, u.clip,
-                                                               u.positivity, scratch);
+      const RecConst rc{u.rad, u.ppm, u.kappa, u.kbeta};
+      dir_lines<EQ><<<(int)((lines + 127) / 128), 128, 0, s>>>(qr, qs, d, dir, u.rec, u.h[dir], rc, u.lim, u.clim,
+                                                               u.eps, u.clip, u.positivity, scratch);
     }
   }
   if (u.mlp) {
@@ -391,7 +556,7 @@ size_t unit_block_flux_scratch(const UnitArgs& u) {
   if (u.km > n) n = u.km;
   long long lines = (long long)(n + 2) * (n + 2) * u.nv;
   long long cells = (long long)u.im * u.jm * u.km;
-  return (size_t)(lines * 3 * n + cells * u.nv) * sizeof(double);
+  return (size_t)(lines * 5 * n + cells * u.nv) * sizeof(double);
 }
 
 cudaError_t unit_riemann(const UnitArgs& u, int n, const double* ql, const double* qr, double* f, cudaStream_t s) {

@@ -38,7 +38,8 @@ enum { AMUN_EOS_ADI = 0, AMUN_EOS_ISO = 1 };
 /* primitive_solver: 1D(W), 2D(W,v^2), 2D(W,u^2) (src/equations.F90:605-640) */
 enum { AMUN_C2P_1DW = 0, AMUN_C2P_2DWV = 1, AMUN_C2P_2DWU = 2 };
 /* reconstruction (src/interpolations.F90:226-382) */
-enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1 };
+enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1, AMUN_REC_WENO3 = 2, AMUN_REC_LIMO3 = 3, AMUN_REC_PPM = 4,
+       AMUN_REC_WENO5YC = 5, AMUN_REC_WENO5NS = 6, AMUN_REC_MP5 = 7, AMUN_REC_MP7 = 8 };
 /* limiter / extrema_limiter (src/interpolations.F90:389-445) */
 enum { AMUN_LIM_ZERO = 0, AMUN_LIM_MM = 1, AMUN_LIM_MC = 2, AMUN_LIM_SB = 3,
        AMUN_LIM_VL = 4, AMUN_LIM_VA = 5 };
@@ -90,6 +91,10 @@ typedef struct amun_params {
                            747-780); -1 for a name the reference rejects      */
   int mlp;              /* 0/1                    "mlp_limiting"
                            (src/interpolations.F90:452-457)                  */
+  /* reconstruction constants (src/interpolations.F90:80-106, 209-212) */
+  double limo3_rad;     /*                        "limo3_rad"                 */
+  double ppm_const;     /*                        "ppm_const"                 */
+  double kappa, kbeta;  /*                        "kappa", "kbeta" (MP)       */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block
@@ -180,12 +185,14 @@ int amun_gpu_status(amun_status* s);
 int amun_gpu_set_time(double time, double dt);
 
 /* update_flux_iface (src/schemes.F90:58-65) for one block: the exact
- * stand-in of update_flux_{hd,mhd}_adi (src/schemes.F90:1080, 2970) on the
- * Fortran arrays, FP64.  dx has NDIMS entries. */
+ * stand-in of update_flux_* (src/schemes.F90:656-5219) on the Fortran
+ * arrays, FP64.  dx (host) has NDIMS entries; only WENO3 and LimO3 read it,
+ * the other methods accept NULL. */
 int amun_gpu_update_flux_block(const double* dx, const double* q, double* f);
 
 /* amun_gpu_update_flux_block on device arrays without allocating: no
- * counterpart in the reference.  q and f are device pointers in the same
+ * counterpart in the reference.  dx is a host array as above; q and f are
+ * device pointers in the same
  * Fortran layouts; the work is queued on the library stream (see
  * amun_gpu_set_stream) and the call returns without synchronising.  Scratch is
  * a fixed 32 MiB array in the library's device image, so a block whose

@@ -40,7 +40,7 @@ namespace {
 // src/coordinates.F90:160-357).  Defaults are the reference defaults.
 // ---------------------------------------------------------------------------
 enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3 };
-enum { REC_TVD = 0, REC_WENO5Z = 1 };
+enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7 };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
 enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM, RS_HLLCM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
@@ -69,6 +69,8 @@ struct Params {
   int nrmax = 100, nrext = 2;
   bool states_4vec = false;
   int c2p = 0;  // primitive_solver: 0 1D(W), 1 2D(W,v^2), 2 2D(W,u^2), -1 unknown
+  // reconstruction constants (src/interpolations.F90:80-106, 209-212)
+  double rad = 0.5, ppm_const = 1.25, kappa = 1.0, kbeta = 1.0;
 };
 
 bool is_one_of(const std::string& s, std::initializer_list<const char*> l) {
@@ -111,6 +113,13 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "reconstruction") {
     if (is_one_of(v, {"tvd", "TVD"})) p.rec = REC_TVD;
     else if (is_one_of(v, {"weno5z", "weno5-z", "WENO5Z", "WENO5-Z"})) p.rec = REC_WENO5Z;
+    else if (is_one_of(v, {"weno3", "WENO3"})) p.rec = REC_WENO3;
+    else if (is_one_of(v, {"limo3", "LIMO3", "LimO3"})) p.rec = REC_LIMO3;
+    else if (is_one_of(v, {"ppm", "PPM"})) p.rec = REC_PPM;
+    else if (is_one_of(v, {"weno5yc", "weno5-yc", "WENO5YC", "WENO5-YC"})) p.rec = REC_WENO5YC;
+    else if (is_one_of(v, {"weno5ns", "weno5-ns", "WENO5NS", "WENO5-NS"})) p.rec = REC_WENO5NS;
+    else if (is_one_of(v, {"mp5", "MP5"})) p.rec = REC_MP5;
+    else if (is_one_of(v, {"mp7", "MP7"})) p.rec = REC_MP7;
     else return 200;  // src/interpolations.F90:382
   } else if (key == "limiter" || key == "extrema_limiter" || key == "prolongation_limiter") {
     int l = LIM_ZERO;
@@ -140,6 +149,10 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "fix_positivity") p.positivity = is_on(v);
   else if (key == "clip_extrema") p.clip = is_on(v);
   else if (key == "mlp_limiting") p.mlp = is_on(v);
+  else if (key == "limo3_rad") p.rad = atof(v.c_str());
+  else if (key == "ppm_const") p.ppm_const = atof(v.c_str());
+  else if (key == "kappa") p.kappa = atof(v.c_str());
+  else if (key == "kbeta") p.kbeta = atof(v.c_str());
   else if (key == "gamma") p.gamma = atof(v.c_str());
   else if (key == "csnd") p.csnd = atof(v.c_str());
   else if (key == "cfl") p.cfl = atof(v.c_str());
@@ -505,6 +518,8 @@ struct Oracle {
       else if (p.rs == RS_HLLC || p.rs == RS_HLLCM) p.rs = RS_HLL;
     }
     csnd = p.csnd; csnd2 = csnd * csnd;
+    // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
+    if (p.rec == REC_LIMO3) p.eps = fmax2(1.0e-12, p.eps);
     if (sr && p.c2p < 0) return 110;
     // the relativistic systems offer HLL and HLLC ("hllcm" included,
     // src/schemes.F90:400-498); elsewhere "hllcm" names nothing
@@ -1881,15 +1896,317 @@ struct Oracle {
     }
   }
 
+  // reconstruct_weno3 src/interpolations.F90:1469-1574
+  void reconstruct_weno3(int n, double h, const double* fv, double* flv, double* frv) const {
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto fl = [&](int i) -> double& { return flv[i - 1]; };
+    auto fr = [&](int i) -> double& { return frv[i - 1]; };
+    const double dp = 2.0 / 3.0, dm = 1.0 / 3.0;
+    const double h2 = h * h;
+    for (int i = 2; i <= n - 1; ++i) {
+      int im1 = i - 1, ip1 = i + 1;
+      double dfl = f(i) - f(im1), dfr = f(ip1) - f(i);
+      double t = dfr - dfl;
+      double ww = t * t;
+      double bp = dfr * dfr, bm = dfl * dfl;
+      double ap = 1.0 + ww / (bp + h2), am = 1.0 + ww / (bm + h2);
+      double wp = dp * ap, wm = dm * am;
+      ww = 2.0 * (wp + wm);
+      double fp = f(i) + f(ip1), fm = -f(im1) + 3.0 * f(i);
+      fl(i) = (wp * fp + wm * fm) / ww;
+      wp = dp * am; wm = dm * ap;
+      ww = 2.0 * (wp + wm);
+      fp = f(i) + f(im1); fm = -f(ip1) + 3.0 * f(i);
+      fr(im1) = (wp * fp + wm * fm) / ww;
+    }
+    int i = n - 1;
+    fl(1) = 0.5 * (f(1) + f(2));
+    fr(i) = 0.5 * (f(i) + f(n));
+    fl(n) = f(n);
+    fr(n) = f(n);
+  }
+
+  // reconstruct_limo3 src/interpolations.F90:1598-1719
+  void reconstruct_limo3(int n, double h, const double* fv, double* flv, double* frv) const {
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto fl = [&](int i) -> double& { return flv[i - 1]; };
+    auto fr = [&](int i) -> double& { return frv[i - 1]; };
+    const double eps = p.eps;
+    double rdx = p.rad * h, rdx2 = rdx * rdx;
+    auto phi = [&](double th, double xl, double xi) {
+      double f1 = (2.0 + th) / 6.0, f2;
+      if (th >= 0.0) f2 = fmax2(0.0, fmin2(fmin2(f1, th), 0.8));
+      else f2 = fmax2(0.0, fmin2(f1, -0.25 * th));
+      return xl * f1 + xi * f2;
+    };
+    for (int i = 2; i <= n - 1; ++i) {
+      int im1 = i - 1, ip1 = i + 1;
+      double dfl = f(i) - f(im1), dfr = f(ip1) - f(i);
+      double et = (dfl * dfl + dfr * dfr) / rdx2;
+      double xi = fmax2(0.0, 0.5 * fmin2(2.0, 1.0 + (et - 1.0) / eps));
+      double xl = 1.0 - xi;
+      if (std::fabs(dfr) > eps) fl(i) = f(i) + dfr * phi(dfl / dfr, xl, xi);
+      else fl(i) = f(i);
+      if (std::fabs(dfl) > eps) fr(im1) = f(i) - dfl * phi(dfr / dfl, xl, xi);
+      else fr(im1) = f(i);
+    }
+    int i = n - 1;
+    fl(1) = 0.5 * (f(1) + f(2));
+    fr(i) = 0.5 * (f(i) + f(n));
+    fl(n) = f(n);
+    fr(n) = f(n);
+  }
+
+  // reconstruct_ppm src/interpolations.F90:1746-1913
+  void reconstruct_ppm(int n, const double* fv, double* flv, double* frv) const {
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto fl = [&](int i) -> double& { return flv[i - 1]; };
+    auto fr = [&](int i) -> double& { return frv[i - 1]; };
+    const double pc = p.ppm_const;
+    std::vector<double> fi(n + 1), df2(n + 1);
+    fi[1] = 0.5 * (f(1) + f(2));
+    for (int i = 2; i <= n - 2; ++i) fi[i] = (7.0 * (f(i) + f(i + 1)) - (f(i - 1) + f(i + 2))) / 12.0;
+    fi[n - 1] = 0.5 * (f(n - 1) + f(n));
+    fi[n] = f(n);
+    df2[1] = 0.0;
+    for (int i = 2; i <= n - 1; ++i) df2[i] = (f(i + 1) + f(i - 1)) - 2.0 * f(i);
+    df2[n] = 0.0;
+    for (int i = 2; i <= n - 2; ++i) {
+      int ip1 = i + 1;
+      if ((f(ip1) - fi[i]) * (fi[i] - f(i)) < 0.0) {
+        double df2c = 3.0 * ((f(ip1) + f(i)) - 2.0 * fi[i]);
+        double df2m = df2[i], df2p = df2[ip1];
+        double df2l;
+        if (fmin2(fmin2(df2c, df2m), df2p) * fmax2(fmax2(df2c, df2m), df2p) > 0.0)
+          df2l = fsign(fmin2(pc * fmin2(std::fabs(df2m), std::fabs(df2p)), std::fabs(df2c)), df2c);
+        else
+          df2l = 0.0;
+        fi[i] = 0.5 * (f(i) + f(ip1)) - df2l / 6.0;
+      }
+    }
+    for (int i = 2; i <= n - 1; ++i) {
+      int im1 = i - 1, ip1 = i + 1;
+      double alm = fi[im1] - f(i), alp = fi[i] - f(i);
+      bool cm = std::fabs(alm) >= 2.0 * std::fabs(alp);
+      bool cp = std::fabs(alp) >= 2.0 * std::fabs(alm);
+      bool ext = false;
+      if (alm * alp > 0.0) {
+        ext = true;
+      } else if (cm || cp) {
+        int im2 = std::max(1, i - 1);
+        double dfm = fi[im1] - fi[im2], dfp = fi[ip1] - fi[i];
+        double dcm = f(i) - f(im1), dcp = f(ip1) - f(i);
+        if (fmin2(std::fabs(dfm), std::fabs(dfp)) >= fmin2(std::fabs(dcm), std::fabs(dcp))) ext = dfm * dfp < 0.0;
+        else ext = dcm * dcp < 0.0;
+      }
+      if (ext) {
+        double df2s = 6.0 * (alm + alp);
+        double df2m = df2[im1], df2c = df2[i], df2p = df2[ip1];
+        if (fmin2(fmin2(fmin2(df2s, df2c), df2m), df2p) * fmax2(fmax2(fmax2(df2s, df2c), df2m), df2p) > 0.0) {
+          double df2l = fsign(fmin2(pc * fmin2(fmin2(std::fabs(df2m), std::fabs(df2c)), std::fabs(df2p)),
+                                    std::fabs(df2s)), df2s);
+          if (std::fabs(df2l) > 0.0) { alm = alm * df2l / df2s; alp = alp * df2l / df2s; }
+          else { alm = 0.0; alp = 0.0; }
+        } else {
+          alm = 0.0; alp = 0.0;
+        }
+      } else {
+        if (cp) {
+          double sgn = fsign(1.0, alp);
+          double amx = -(0.25 * (alp * alp) / (alp + alm));
+          double dfp = f(ip1) - f(i);
+          if (sgn * amx >= sgn * dfp) {
+            double del = dfp * (dfp - alm);
+            if (del >= 0.0) alp = -2.0 * (dfp + sgn * std::sqrt(del));
+            else alp = -2.0 * alm;
+          }
+        }
+        if (cm) {
+          double sgn = fsign(1.0, alm);
+          double amx = -(0.25 * (alm * alm) / (alp + alm));
+          double dfm = f(im1) - f(i);
+          if (sgn * amx >= sgn * dfm) {
+            double del = dfm * (dfm - alp);
+            if (del >= 0.0) alm = -2.0 * (dfm + sgn * std::sqrt(del));
+            else alm = -2.0 * alp;
+          }
+        }
+      }
+      fr(im1) = f(i) + alm;
+      fl(i) = f(i) + alp;
+    }
+    fl(1) = fi[1];
+    fr(n - 1) = fi[n];
+    fl(n) = fi[n];
+    fr(n) = f(n);
+  }
+
+  // reconstruct_weno5yc src/interpolations.F90:2107-2254 (ns false) and
+  // reconstruct_weno5ns 2278-2441 (ns true)
+  void reconstruct_weno5v(bool ns, int n, const double* fv, double* flv, double* frv) const {
+    std::vector<double> dfm(n + 1), dfp(n + 1), df2(n + 1);
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto fl = [&](int i) -> double& { return flv[i - 1]; };
+    auto fr = [&](int i) -> double& { return frv[i - 1]; };
+    const double dl = 0.1, dc = 0.6, dr = 0.3;
+    const double a11 = 2.0 / 6.0, a12 = -7.0 / 6.0, a13 = 11.0 / 6.0;
+    const double a21 = -1.0 / 6.0, a22 = 5.0 / 6.0, a23 = 2.0 / 6.0;
+    const double a31 = 2.0 / 6.0, a32 = 5.0 / 6.0, a33 = -1.0 / 6.0;
+    const double eps = p.eps;
+    for (int i = 1; i <= n - 1; ++i) { dfp[i] = f(i + 1) - f(i); dfm[i + 1] = dfp[i]; }
+    dfm[1] = dfp[1];
+    dfp[n] = dfm[n];
+    for (int i = 1; i <= n; ++i) {
+      double t = dfp[i] - dfm[i];
+      df2[i] = ns ? 0.5 * std::fabs(t) : (13.0 / 12.0) * (t * t);
+    }
+    for (int i = 3; i <= n - 2; ++i) {
+      int im2 = i - 2, im1 = i - 1, ip1 = i + 1, ip2 = i + 2;
+      double wl, wc, wr;
+      if (!ns) {
+        double t;
+        t = 3.0 * dfm[i] - dfm[im1]; double bl = df2[im1] + 0.25 * (t * t);
+        t = dfp[i] + dfm[i];         double bc = df2[i] + 0.25 * (t * t);
+        t = 3.0 * dfp[i] - dfp[ip1]; double br = df2[ip1] + 0.25 * (t * t);
+        t = (6.0 * f(i) - 4.0 * (f(im1) + f(ip1))) + (f(im2) + f(ip2));
+        double tt = t * t;
+        double al = 1.0 + tt / (bl + eps), ac = 1.0 + tt / (bc + eps), ar = 1.0 + tt / (br + eps);
+        wl = dl * al; wc = dc * ac; wr = dr * ar;
+        double ww = (wl + wr) + wc;
+        wl = wl / ww; wr = wr / ww; wc = 1.0 - (wl + wr);
+        fl(i) = (wl * (a11 * f(im2) + a12 * f(im1) + a13 * f(i)) + wr * (a31 * f(i) + a32 * f(ip1) + a33 * f(ip2))) +
+                wc * (a21 * f(im1) + a22 * f(i) + a23 * f(ip1));
+        wl = dl * ar; wc = dc * ac; wr = dr * al;
+        ww = (wl + wr) + wc;
+        wl = wl / ww; wr = wr / ww; wc = 1.0 - (wl + wr);
+        fr(im1) = (wl * (a11 * f(ip2) + a12 * f(ip1) + a13 * f(i)) + wr * (a31 * f(i) + a32 * f(im1) + a33 * f(im2))) +
+                  wc * (a21 * f(ip1) + a22 * f(i) + a23 * f(im1));
+      } else {
+        const double xi = 0.4;
+        auto weights = [&](double df, double bl, double bc, double br) {
+          double l3 = (df * df) * df;
+          double t = bl - br, u = l3 / (1.0 + l3);
+          double zt = 0.5 * ((t * t) + (u * u));
+          t = bl + eps; double al = dl * (1.0 + zt / (t * t));
+          t = bc + eps; double ac = dc * (1.0 + zt / (t * t));
+          t = br + eps; double ar = dr * (1.0 + zt / (t * t));
+          double aa = (al + ar) + ac;
+          wl = al / aa; wr = ar / aa; wc = 1.0 - (wl + wr);
+        };
+        double df = std::fabs(dfp[i]), lq = xi * df;
+        weights(df, df2[im1] + xi * std::fabs(2.0 * dfm[i] - dfm[im1]), df2[i] + lq, df2[ip1] + lq);
+        fl(i) = (wl * (a11 * f(im2) + a12 * f(im1) + a13 * f(i)) + wr * (a31 * f(i) + a32 * f(ip1) + a33 * f(ip2))) +
+                wc * (a21 * f(im1) + a22 * f(i) + a23 * f(ip1));
+        df = std::fabs(dfm[i]); lq = xi * df;
+        weights(df, df2[ip1] + xi * std::fabs(2.0 * dfp[i] - dfp[ip1]), df2[i] + lq, df2[im1] + lq);
+        fr(im1) = (wl * (a11 * f(ip2) + a12 * f(ip1) + a13 * f(i)) + wr * (a31 * f(i) + a32 * f(im1) + a33 * f(im2))) +
+                  wc * (a21 * f(ip1) + a22 * f(i) + a23 * f(im1));
+      }
+    }
+    fl(1) = 0.5 * (f(1) + f(2));
+    double df = limiter(p.lim, 0.5, dfm[2], dfp[2]);
+    fr(1) = f(2) - df;
+    fl(2) = f(2) + df;
+    int i = n - 1;
+    df = limiter(p.lim, 0.5, dfm[i], dfp[i]);
+    fr(i - 1) = f(i) - df;
+    fl(i) = f(i) + df;
+    fr(i) = 0.5 * (f(i) + f(n));
+    fl(n) = f(n);
+    fr(n) = f(n);
+  }
+
+  // minmod, median src/interpolations.F90:4880-4974
+  static double mp_minmod(double a, double b) { return (fsign(0.5, a) + fsign(0.5, b)) * fmin2(std::fabs(a), std::fabs(b)); }
+
+  // mp_limiting src/interpolations.F90:5209-5284
+  void mp_limiting(int n, const double* fv, double* vv) const {
+    auto f = [&](int i) { return fv[i - 1]; };
+    auto v = [&](int i) -> double& { return vv[i - 1]; };
+    std::vector<double> dm(n + 3, 0.0);
+    for (int i = 2; i <= n; ++i) dm[i] = f(i) - f(i - 1);
+    for (int i = 1; i <= n - 1; ++i) {
+      int ip1 = i + 1;
+      double df = dm[i] * dm[ip1] >= 0.0 ? p.kappa * dm[i] : p.kbeta * dm[i];
+      double fmp = f(i) + mp_minmod(dm[ip1], df);
+      double ds = (v(i) - f(i)) * (v(i) - fmp);
+      if (ds > p.eps) {
+        int im1 = i - 1, ip2 = i + 2;
+        double dm1 = dm[i] - dm[im1], dc0 = dm[ip1] - dm[i], dp1 = dm[ip2] - dm[ip1];
+        double dc4 = 4.0 * dc0;
+        double dml = 0.5 * mp_minmod(mp_minmod(dc4 - dm1, 4.0 * dm1 - dc0), mp_minmod(dc0, dm1));
+        double dmr = 0.5 * mp_minmod(mp_minmod(dc4 - dp1, 4.0 * dp1 - dc0), mp_minmod(dc0, dp1));
+        double fmd = f(i) + 0.5 * dm[ip1] - dmr;
+        double ful = f(i) + df;
+        double flc = f(i) + 0.5 * df + dml;
+        double fmx = fmax2(fmin2(fmin2(f(i), f(ip1)), fmd), fmin2(fmin2(f(i), ful), flc));
+        double fmn = fmin2(fmax2(fmax2(f(i), f(ip1)), fmd), fmax2(fmax2(f(i), ful), flc));
+        v(i) = v(i) + mp_minmod(fmn - v(i), fmx - v(i));
+      }
+    }
+  }
+
+  // reconstruct_mp5 src/interpolations.F90:3675-3770 (order 5) and
+  // reconstruct_mp7 3799-3901 (order 7)
+  void reconstruct_mp(int order, int n, const double* fc, double* flv, double* frv) const {
+    static const double ce2[2] = {0.5, 0.5};
+    static const double ce3[3] = {-1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0};
+    static const double ce5[5] = {2.0 / 60.0, -13.0 / 60.0, 47.0 / 60.0, 27.0 / 60.0, -3.0 / 60.0};
+    static const double ce7[7] = {-3.0 / 420.0, 25.0 / 420.0, -101.0 / 420.0, 319.0 / 420.0, 214.0 / 420.0,
+                                  -38.0 / 420.0, 4.0 / 420.0};
+    std::vector<double> u(n), fi(n);
+    auto pass = [&](const double* g) {
+      auto sum = [&](const double* c, int m, int i0) {  // i0 1-based
+        double s = 0.0;
+        for (int k = 0; k < m; ++k) s = s + c[k] * g[i0 - 1 + k];
+        return s;
+      };
+      if (order == 5) {
+        for (int i = 3; i <= n - 2; ++i) u[i - 1] = sum(ce5, 5, i - 2);
+        u[0] = sum(ce2, 2, 1);
+        u[1] = sum(ce3, 3, 1);
+        u[n - 2] = sum(ce3, 3, n - 2);
+      } else {
+        for (int i = 4; i <= n - 3; ++i) u[i - 1] = sum(ce7, 7, i - 3);
+        u[0] = sum(ce2, 2, 1);
+        u[1] = sum(ce3, 3, 1);
+        u[2] = sum(ce5, 5, 1);
+        u[n - 3] = sum(ce5, 5, n - 4);
+        u[n - 2] = sum(ce3, 3, n - 2);
+      }
+      u[n - 1] = g[n - 1];
+      mp_limiting(n, g, u.data());
+    };
+    pass(fc);
+    for (int i = 0; i < n; ++i) flv[i] = u[i];
+    for (int i = 0; i < n; ++i) fi[i] = fc[n - 1 - i];
+    pass(fi.data());
+    for (int k = 1; k <= n - 1; ++k) frv[k - 1] = u[n - 1 - k];
+    int i = n - 1;
+    flv[0] = 0.5 * (fc[0] + fc[1]);
+    frv[i - 1] = 0.5 * (fc[i - 1] + fc[n - 1]);
+    flv[n - 1] = fc[n - 1];
+    frv[n - 1] = fc[n - 1];
+  }
+
   // reconstruct src/interpolations.F90:1343-1381
-  void reconstruct(int n, const double* f, double* fl, double* fr) const {
-    if (p.rec == REC_WENO5Z) reconstruct_weno5z(n, f, fl, fr);
-    else reconstruct_tvd(n, f, fl, fr);
+  void reconstruct(int n, const double* f, double* fl, double* fr, double h = 0.0) const {
+    switch (p.rec) {
+      case REC_WENO5Z: reconstruct_weno5z(n, f, fl, fr); break;
+      case REC_WENO3: reconstruct_weno3(n, h, f, fl, fr); break;
+      case REC_LIMO3: reconstruct_limo3(n, h, f, fl, fr); break;
+      case REC_PPM: reconstruct_ppm(n, f, fl, fr); break;
+      case REC_WENO5YC: reconstruct_weno5v(false, n, f, fl, fr); break;
+      case REC_WENO5NS: reconstruct_weno5v(true, n, f, fl, fr); break;
+      case REC_MP5: reconstruct_mp(5, n, f, fl, fr); break;
+      case REC_MP7: reconstruct_mp(7, n, f, fl, fr); break;
+      default: reconstruct_tvd(n, f, fl, fr); break;
+    }
     if (p.clip) clip_extrema(n, f, fl, fr);
   }
 
   // interfaces_dir src/interpolations.F90:867-959
-  void interfaces_dir(bool positive, const double* qv, double* qs) {
+  void interfaces_dir(bool positive, const double* qv, double* qs, const double* h) {
     const size_t N = cells();
     ghost_copy(qv, qs);
     std::vector<double> f(std::max(im, std::max(jm, km))), fl(f.size()), fr(f.size());
@@ -1901,7 +2218,7 @@ struct Oracle {
       double* qr = qs + N * (1 + 2 * (size_t)(d - 1));
       for (int t = 0; t < n; ++t) f[t] = qv[base + t * stride];
       if (!pos_pass) {
-        reconstruct(n, f.data(), fl.data(), fr.data());
+        reconstruct(n, f.data(), fl.data(), fr.data(), h[d - 1]);
       } else {
         for (int t = 0; t < n; ++t) { fl[t] = ql[base + t * stride]; fr[t] = qr[base + t * stride]; }
         fix_positivity(n, f.data(), fl.data(), fr.data());
@@ -2613,7 +2930,9 @@ struct Oracle {
   // update_flux_hd_adi src/schemes.F90:1080-1223 and update_flux_mhd_adi
   // 2970-3138, with reconstruct_interfaces 591-633.  Directional component
   // rotation: x:(x,y,z) y:(y,z,x) z:(z,x,y).
-  void update_flux(const double* q, double* f) {
+  void update_flux(const double* q, double* f, const double* h = nullptr) {
+    const double hg[3] = {dx, dy, dz};
+    if (!h) h = hg;
     const size_t N = cells();
     std::fill(f, f + (size_t)p.ndims * nv * N, 0.0);
     std::vector<double> qs((size_t)nv * N * 2 * p.ndims);
@@ -2639,7 +2958,7 @@ struct Oracle {
       bool positive = (pv == idn || pv == ipr);
       for (size_t c = 0; c < N; ++c) one[c] = q[(size_t)(pv - 1) + (size_t)nv * c];
       if (p.rec == REC_TVD) interfaces_tvd(positive, one.data(), ones.data());
-      else interfaces_dir(positive, one.data(), ones.data());
+      else interfaces_dir(positive, one.data(), ones.data(), h);
       // scatter to qs(nv,im,jm,km,2,NDIMS)
       for (size_t sd = 0; sd < (size_t)2 * p.ndims; ++sd)
         for (size_t c = 0; c < N; ++c) qs[(size_t)(pv - 1) + (size_t)nv * (c + N * sd)] = ones[c + N * sd];
@@ -2988,7 +3307,10 @@ struct Oracle {
   // update_fluxes src/evolution.F90:1807-1881 (boundary_fluxes is a no-op
   // on a single-level mesh)
   void update_fluxes() {
-    parallel_blocks([&](Block& B) { update_flux(B.q.data(), B.f.data()); });
+    parallel_blocks([&](Block& B) {
+      const double hb[3] = {B.dx, B.dy, B.dz};
+      update_flux(B.q.data(), B.f.data(), hb);
+    });
     boundary_fluxes();
   }
 

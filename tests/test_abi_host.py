@@ -53,6 +53,9 @@ def test_default_params_match_reference_defaults():
     ("riemann_solver", "hllc-m", "riemann", 5), ("equation_system", "SRHD", "eqsys", N.AMUN_EQ_SRHD),
     ("primitive_solver", "2D(W,v)", "c2p", 1), ("primitive_solver", "2dwu", "c2p", 2),
     ("primitive_solver", "1D(W)", "c2p", 0), ("primitive_solver", "newton", "c2p", -1),
+    ("reconstruction", "LimO3", "reconstruction", 3), ("reconstruction", "weno5-ns", "reconstruction", 6),
+    ("reconstruction", "MP7", "reconstruction", 8), ("limo3_rad", "0.25", "limo3_rad", 0.25),
+    ("ppm_const", "2", "ppm_const", 2.0), ("kappa", "4", "kappa", 4.0), ("mlp_limiting", "on", "mlp", 1),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()
@@ -63,6 +66,7 @@ def test_set_param_aliases(key, val, field, expect):
 
 
 @pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "polytropic", 110),
+                                          ("reconstruction", "crweno5z", 904), ("reconstruction", "gp", 904),
                                           ("reconstruction", "nope", 200)])
 def test_set_param_reference_error_codes(key, val, code):
     L = N.lib()
