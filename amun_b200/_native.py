@@ -36,6 +36,8 @@ class amun_params(C.Structure):
         ("xblocks", C.c_int), ("yblocks", C.c_int), ("zblocks", C.c_int), ("eos", C.c_int),
         ("csnd", C.c_double), ("c2p", C.c_int), ("mlp", C.c_int), ("limo3_rad", C.c_double),
         ("ppm_const", C.c_double), ("kappa", C.c_double), ("kbeta", C.c_double),
+        ("viscosity", C.c_double), ("resistivity", C.c_double), ("glm_sources", C.c_int), ("gravity", C.c_int),
+        ("gacc", C.c_double),
     ]
 
 

@@ -307,11 +307,21 @@ void tile_shape(int& LP, int& LW) {
 
 bool relativistic() { return C.p.eqsys == AMUN_EQ_SRMHD || C.p.eqsys == AMUN_EQ_SRHD; }
 
-// the sweep variant: TVD and WENO-Z have their own; the other methods and
-// mlp_limiting run in the generic one (three-cell halo)
+// max(viscosity, resistivity) of new_time_step (src/evolution.F90:478-479)
+double visc_res() { return C.p.viscosity > C.p.resistivity ? C.p.viscosity : C.p.resistivity; }
+
+// update_sources has work (src/sources.F90:227-615): gravity, viscosity,
+// and for the magnetised systems GLM source terms or resistivity
+bool sources_on() {
+  const bool mhd = C.p.eqsys == AMUN_EQ_MHD || C.p.eqsys == AMUN_EQ_SRMHD || C.p.eqsys == EQ_MHD_ISO;
+  return C.p.gravity || C.p.viscosity > 0.0 || (mhd && (C.p.glm_sources > 0 || C.p.resistivity > 0.0));
+}
+
+// the sweep variant: TVD and WENO-Z have their own; the other methods,
+// mlp_limiting and the source terms run in the generic one (three-cell halo)
 int sweep_variant() {
   const int r = C.p.reconstruction;
-  if (C.p.mlp || (r != AMUN_REC_TVD && r != AMUN_REC_WENO5Z)) return REC_GEN;
+  if (C.p.mlp || sources_on() || (r != AMUN_REC_TVD && r != AMUN_REC_WENO5Z)) return REC_GEN;
   return r;
 }
 int sweep_halo() {
@@ -331,6 +341,12 @@ MethodConst method_const() {
   m.mlp = C.p.mlp;
   m.rec = C.p.reconstruction;
   m.rc.rad = C.p.limo3_rad; m.rc.ppm = C.p.ppm_const; m.rc.kappa = C.p.kappa; m.rc.kbeta = C.p.kbeta;
+  m.gravity = C.p.gravity;
+  m.gacc[0] = 0.0; m.gacc[1] = C.p.gacc; m.gacc[2] = 0.0;  // gacc_rayleigh_taylor (src/gravity.F90:283-330)
+  m.visc = C.p.viscosity;
+  m.resist = C.p.resistivity;
+  m.glm = C.p.glm_sources;
+  m.src = sources_on();
   m.states_4vec = relativistic() ? C.p.states_4vec : 0;
   return m;
 }
@@ -435,7 +451,7 @@ int ensure_maxspeed() {
 int step_launches(double dtnext) {
   {
     ProfScope ps(4);
-    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, visc_res());
     CK(cudaGetLastError());
   }
   int r = evolve_launches();
@@ -524,6 +540,11 @@ void amun_gpu_default_params(amun_params* p) {
   p->ppm_const = 1.25;
   p->kappa = 1.0;
   p->kbeta = 1.0;
+  p->viscosity = 0.0;
+  p->resistivity = 0.0;
+  p->glm_sources = 0;
+  p->gravity = 0;
+  p->gacc = -1.0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -603,6 +624,17 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "ppm_const") p->ppm_const = atof(v);
   else if (k == "kappa") p->kappa = atof(v);
   else if (k == "kbeta") p->kbeta = atof(v);
+  else if (k == "viscosity") p->viscosity = atof(v);
+  else if (k == "resistivity") p->resistivity = atof(v);
+  else if (k == "gacc") p->gacc = atof(v);
+  else if (k == "glm_source_terms") {
+    if (is_one_of(v, {"eglm", "EGLM"})) p->glm_sources = 1;
+    else if (is_one_of(v, {"heglm", "HEGLM"})) p->glm_sources = 2;
+    else p->glm_sources = 0;
+  } else if (k == "problem") {
+    // the one problem of the reference with gravity (src/gravity.F90:137-146)
+    p->gravity = is_one_of(v, {"rt", "rayleightaylor", "rayleigh-taylor"}) ? 1 : 0;
+  }
   else if (k == "clip_extrema") p->clip_extrema = is_on(v);
   else if (k == "precision") {
     if (is_one_of(v, {"fp32", "FP32", "fp32_bulk", "bulk"})) p->precision = AMUN_FP32_BULK;
@@ -1019,7 +1051,7 @@ int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt) {
   int r = check_ready();
   if (r) return r;
   if ((r = ensure_maxspeed())) return r;
-  new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+  new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, visc_res());
   CK(cudaGetLastError());
   DevScalars h;
   CK(cudaMemcpyAsync(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
@@ -1367,6 +1399,7 @@ int adj_supported() {
   if (effective_solver() != AMUN_RS_HLL) return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL Riemann solver only");
   if (C.p.fix_positivity || C.p.clip_extrema || C.p.mlp)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity, clip_extrema and mlp_limiting must be off");
+  if (sources_on()) return fail(AMUN_E_UNSUPPORTED, "adjoint: no source terms");
   if (C.p.nghosts < 4) return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4");
   if (C.amr) return fail(AMUN_E_UNSUPPORTED, "adjoint: meshes at one level only");
   return 0;
@@ -1462,7 +1495,7 @@ int forward_recorded(int nsteps, double dtnext) {
       int r = save_state(n / A.interval);
       if (r) return r;
     }
-    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, 0.0);
+    new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, visc_res());
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(A.rec + n, C.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
     int r = launch_evolve<R>();

@@ -67,6 +67,11 @@ struct MethodConst {
   int mlp;  // multi-dimensional limiting process (mlp_limiting)
   int rec;  // reconstruction method (run-time choice of the generic sweep)
   RecConst rc;
+  // source terms (update_sources, src/sources.F90:227-615): a uniform
+  // gravitational acceleration, viscosity, GLM source terms (1 EGLM,
+  // 2 HEGLM) and resistivity; src says whether any is on
+  int src, gravity, glm;
+  double gacc[3], visc, resist;
   int plim;  // prolongation limiter (limiter_prol)
   double csnd;  // isothermal sound speed
 };
@@ -123,6 +128,148 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* t
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
     if (lane == 0 && v > 0.0) atomicMax(target, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// update_sources (src/sources.F90:227-615) for one interior cell, added to
+// its increment du after the flux differences, in the reference's order:
+// gravity, viscosity, GLM source terms, resistivity.  The derivatives are
+// those of src/operators.F90:538-711 away from the block edge (centred
+// first and second differences), evaluated on the stage's primitive
+// variables read through L1/L2.
+template <int EQ, typename R>
+__device__ __forceinline__ void add_sources(R* du, const R* qb, const Geo& g, int i, int j, int k, const double* hb,
+                                            const MethodConst& m) {
+  using V = Var<EQ>;
+  const bool d3 = g.ndims == 3;
+  auto Q = [&](int v, int di, int dj, int dk) -> R {
+    return ld_ro(qb + (long long)v * g.qvs + ((long long)(k + dk) * g.JM + (j + dj)) * g.IM + (i + di));
+  };
+  const R h[3] = {R(hb[0]), R(hb[1]), R(hb[2])};
+  // centred first derivative of variable v along d at offset (oi, oj, ok)
+  auto D1 = [&](int v, int d, int oi, int oj, int ok) -> R {
+    const int ei = d == 0, ej = d == 1, ek = d == 2;
+    return R(0.5) * (Q(v, oi + ei, oj + ej, ok + ek) - Q(v, oi - ei, oj - ej, ok - ek)) / h[d];
+  };
+  auto D2 = [&](int v, int d) -> R {
+    const int ei = d == 0, ej = d == 1, ek = d == 2;
+    return ((Q(v, ei, ej, ek) + Q(v, -ei, -ej, -ek)) - R(2) * Q(v, 0, 0, 0)) / (h[d] * h[d]);
+  };
+  constexpr int DN = V::DN, VX = V::VX, VY = V::VY, VZ = V::VZ, EN = V::EN;
+  if (m.gravity) {
+    const R rho = Q(DN, 0, 0, 0);
+    const R gx = rho * R(m.gacc[0]), gy = rho * R(m.gacc[1]);
+    du[VX] = du[VX] + gx;
+    du[VY] = du[VY] + gy;
+    if (d3) {
+      const R gz = rho * R(m.gacc[2]);
+      du[VZ] = du[VZ] + gz;
+      if constexpr (EN >= 0)
+        du[EN] = du[EN] + gx * Q(VX, 0, 0, 0) + gy * Q(VY, 0, 0, 0) + gz * Q(VZ, 0, 0, 0);
+    } else {
+      if constexpr (EN >= 0) du[EN] = du[EN] + gx * Q(VX, 0, 0, 0) + gy * Q(VY, 0, 0, 0);
+    }
+  }
+  if (m.visc > 0.0) {
+    // the viscous stress tensor at a neighbour (xx, yy, zz, xy, xz, yz)
+    const R mu = R(m.visc);
+    auto stress = [&](int oi, int oj, int ok, R* T) {
+      const R dvxdx = D1(VX, 0, oi, oj, ok), dvxdy = D1(VX, 1, oi, oj, ok), dvxdz = d3 ? D1(VX, 2, oi, oj, ok) : R(0);
+      const R dvydx = D1(VY, 0, oi, oj, ok), dvydy = D1(VY, 1, oi, oj, ok), dvydz = d3 ? D1(VY, 2, oi, oj, ok) : R(0);
+      const R dvzdx = D1(VZ, 0, oi, oj, ok), dvzdy = D1(VZ, 1, oi, oj, ok), dvzdz = d3 ? D1(VZ, 2, oi, oj, ok) : R(0);
+      const R gc = mu * Q(DN, oi, oj, ok);
+      const R fc = R(2) * gc;
+      const R divv = (dvxdx + dvydy + dvzdz) / R(3);
+      T[0] = fc * (dvxdx - divv);
+      T[1] = fc * (dvydy - divv);
+      T[2] = fc * (dvzdz - divv);
+      T[3] = gc * (dvxdy + dvydx);
+      T[4] = gc * (dvxdz + dvzdx);
+      T[5] = gc * (dvydz + dvzdy);
+    };
+    // the tensor and velocity at the 2 ndims face neighbours
+    R Tm[3][6], Tp[3][6], em[3][3], ep[3][3];
+    for (int d = 0; d < g.ndims; ++d) {
+      const int ei = d == 0, ej = d == 1, ek = d == 2;
+      stress(-ei, -ej, -ek, Tm[d]);
+      stress(ei, ej, ek, Tp[d]);
+      // rows contracted with the velocity: (v . T_x, v . T_y, v . T_z)
+      auto contract = [&](const R* T, int oi, int oj, int ok, R* e) {
+        const R vx = Q(VX, oi, oj, ok), vy = Q(VY, oi, oj, ok), vz = Q(VZ, oi, oj, ok);
+        e[0] = vx * T[0] + vy * T[3] + vz * T[4];
+        e[1] = vx * T[3] + vy * T[1] + vz * T[5];
+        e[2] = vx * T[4] + vy * T[5] + vz * T[2];
+      };
+      contract(Tm[d], -ei, -ej, -ek, em[d]);
+      contract(Tp[d], ei, ej, ek, ep[d]);
+    }
+    // divergence of the tensor rows: row x = (xx, xy, xz), y = (xy, yy, yz),
+    // z = (xz, yz, zz); component of direction d
+    const int rowc[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+    R db[3];
+    for (int r = 0; r < 3; ++r) {
+      R s = R(0);
+      for (int d = 0; d < g.ndims; ++d) s = s + R(0.5) * (Tp[d][rowc[r][d]] - Tm[d][rowc[r][d]]) / h[d];
+      db[r] = s;
+    }
+    du[VX] = du[VX] + db[0];
+    du[VY] = du[VY] + db[1];
+    du[VZ] = du[VZ] + db[2];
+    if constexpr (EN >= 0) {
+      R s = R(0);
+      for (int d = 0; d < g.ndims; ++d) s = s + R(0.5) * (ep[d][d] - em[d][d]) / h[d];
+      du[EN] = du[EN] + s;
+    }
+  }
+  if constexpr (V::MHD) {
+    constexpr int BX = V::BX, BY = V::BY, BZ = V::BZ, BP = V::BP;
+    const R bx = Q(BX, 0, 0, 0), by = Q(BY, 0, 0, 0), bz = Q(BZ, 0, 0, 0);
+    if (m.glm > 0) {
+      R db = R(0);
+      db = db + D1(BX, 0, 0, 0, 0);
+      db = db + D1(BY, 1, 0, 0, 0);
+      if (d3) db = db + D1(BZ, 2, 0, 0, 0);
+      du[VX] = du[VX] - db * bx;
+      du[VY] = du[VY] - db * by;
+      du[VZ] = du[VZ] - db * bz;
+      if constexpr (EN >= 0) {
+        const R gpx = D1(BP, 0, 0, 0, 0), gpy = D1(BP, 1, 0, 0, 0), gpz = d3 ? D1(BP, 2, 0, 0, 0) : R(0);
+        du[EN] = du[EN] - (bx * gpx + by * gpy + bz * gpz);
+      }
+      if (m.glm > 1) {
+        const R vx = Q(VX, 0, 0, 0), vy = Q(VY, 0, 0, 0), vz = Q(VZ, 0, 0, 0);
+        du[BX] = du[BX] - db * vx;
+        du[BY] = du[BY] - db * vy;
+        du[BZ] = du[BZ] - db * vz;
+        if constexpr (EN >= 0) du[EN] = du[EN] - db * (vx * bx + vy * by + vz * bz);
+      }
+    }
+    if (m.resist > 0.0) {
+      const R eta = R(m.resist);
+      auto lap = [&](int v) {
+        R s = D2(v, 0);
+        s = s + D2(v, 1);
+        if (d3) s = s + D2(v, 2);
+        return s;
+      };
+      const R ex = eta * lap(BX), ey = eta * lap(BY), ez = eta * lap(BZ);
+      du[BX] = du[BX] + ex;
+      du[BY] = du[BY] + ey;
+      du[BZ] = du[BZ] + ez;
+      if constexpr (EN >= 0) {
+        du[EN] = du[EN] + (bx * ex + by * ey + bz * ez);
+        R j1, j2;
+        if (d3) {
+          j1 = D1(BZ, 1, 0, 0, 0) - D1(BY, 2, 0, 0, 0);
+          j2 = D1(BX, 2, 0, 0, 0) - D1(BZ, 0, 0, 0, 0);
+        } else {
+          j1 = D1(BZ, 1, 0, 0, 0);
+          j2 = -D1(BZ, 0, 0, 0, 0);
+        }
+        const R j3 = D1(BY, 0, 0, 0, 0) - D1(BX, 1, 0, 0, 0);
+        du[EN] = du[EN] + eta * (j1 * j1 + j2 * j2 + j3 * j3);
+      }
+    }
   }
 }
 
@@ -445,6 +592,13 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
 #pragma unroll
       for (int v = 0; v < NV; ++v) a.du[ci + v * g.uvs] = dloc[v];
       continue;
+    }
+    if constexpr (REC == REC_GEN) {
+      if (a.m.src) {
+        const int Pc = p0 + pp, Lc = l0 + ll;
+        const int xi = DIR == 0 ? Pc : Lc, yj = DIR == 1 ? Pc : (DIR == 0 ? Lc : t0), zk = DIR == 2 ? Pc : t0;
+        add_sources<EQ, R>(dloc, qb, g, xi, yj, zk, a.bdx + 3 * b, a.m);
+      }
     }
     // stage combination (all cells updated by this stage are interior)
     const double dt = a.sc->dt;

@@ -95,6 +95,13 @@ typedef struct amun_params {
   double limo3_rad;     /*                        "limo3_rad"                 */
   double ppm_const;     /*                        "ppm_const"                 */
   double kappa, kbeta;  /*                        "kappa", "kbeta" (MP)       */
+  /* source terms (src/sources.F90:94-169, src/gravity.F90:101-164) */
+  double viscosity;     /*                        "viscosity"                 */
+  double resistivity;   /*                        "resistivity"               */
+  int glm_sources;      /* 0 none, 1 EGLM, 2 HEGLM "glm_source_terms"        */
+  int gravity;          /* 0/1: "problem" = rt / rayleightaylor / rayleigh-
+                           taylor switches the uniform acceleration on      */
+  double gacc;          /*                        "gacc" (y component)        */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block

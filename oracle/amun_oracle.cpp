@@ -64,6 +64,9 @@ struct Params {
   int minlev = 1, maxlev = 1;
   double xmin = 0, xmax = 1, ymin = 0, ymax = 1, zmin = 0, zmax = 1;
   double viscosity = 0, resistivity = 0;
+  int glm_sources = 0;     // glm_source_terms: 0 none, 1 EGLM, 2 HEGLM
+  bool gravity = false;    // problem = rt (src/gravity.F90:137-146)
+  double gacc = -1.0;
   // relativistic recovery (src/equations.F90:184-201, 313-318)
   double tol = 1.0e-10, pmin = 1.0e-16;
   int nrmax = 100, nrext = 2;
@@ -150,6 +153,14 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "clip_extrema") p.clip = is_on(v);
   else if (key == "mlp_limiting") p.mlp = is_on(v);
   else if (key == "limo3_rad") p.rad = atof(v.c_str());
+  else if (key == "viscosity") p.viscosity = atof(v.c_str());
+  else if (key == "resistivity") p.resistivity = atof(v.c_str());
+  else if (key == "gacc") p.gacc = atof(v.c_str());
+  else if (key == "glm_source_terms") {
+    if (is_one_of(v, {"eglm", "EGLM"})) p.glm_sources = 1;
+    else if (is_one_of(v, {"heglm", "HEGLM"})) p.glm_sources = 2;
+    else p.glm_sources = 0;
+  } else if (key == "problem") p.gravity = is_one_of(v, {"rt", "rayleightaylor", "rayleigh-taylor"});
   else if (key == "ppm_const") p.ppm_const = atof(v.c_str());
   else if (key == "kappa") p.kappa = atof(v.c_str());
   else if (key == "kbeta") p.kbeta = atof(v.c_str());
@@ -445,6 +456,7 @@ struct Oracle {
   double csnd = 1.0, csnd2 = 1.0;  // src/equations.F90:847-851
   bool iso = false;
   bool mhd = false, sr = false;  // magnetic field present; special relativistic
+  bool sources_on = false;       // update_sources has work
   double cmax = 0.0, cmax2 = 0.0;
   mutable std::atomic<long> c2p_failures{0};  // failed relativistic recoveries (p set to 0)
   // evolution (src/evolution.F90:60-90)
@@ -526,6 +538,7 @@ struct Oracle {
     if (sr) p.rs = (p.rs == RS_HLLC || p.rs == RS_HLLCM) ? RS_HLLC : RS_HLL;
     if (p.rs == RS_HLLCM) p.rs = RS_HLL;
     if (p.rs == RS_HLLDM && !iso) p.rs = RS_HLL;  // HLLD-M exists for isothermal MHD only
+    sources_on = p.gravity || p.viscosity > 0.0 || (mhd && (p.glm_sources > 0 || p.resistivity > 0.0));
     if (p.rs == RS_HLLD && p.eqsys == EQ_HD) p.rs = RS_HLL;  // not offered for HD
     gamma = p.gamma; gammam1 = gamma - 1.0; gammam1i = 1.0 / gammam1;
     gammaxi = gammam1 / gamma;
@@ -3278,7 +3291,7 @@ struct Oracle {
     boundary_variables();
   }
 
-  // new_time_step src/evolution.F90:379-493 (viscosity = resistivity = 0)
+  // new_time_step src/evolution.F90:379-493
   void new_time_step(double dtnext) {
     const double eps = DBL_MIN;  // tiny(cmax)
     cmax = eps;
@@ -3314,6 +3327,202 @@ struct Oracle {
     boundary_fluxes();
   }
 
+  // derivative_1st / derivative_2nd src/operators.F90:538-711 on one
+  // (im,jm,km) array: centred inside, one-sided (first) or zero (second) on
+  // the array's edge layers
+  void derivative_1st(int dir, double dh, const std::vector<double>& u, std::vector<double>& v) const {
+    auto A = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)); };
+    const int m0 = dir == 1 ? im : (dir == 2 ? jm : km);
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+          const int c = dir == 1 ? i : (dir == 2 ? j : k);
+          auto at = [&](int cc) { return dir == 1 ? u[A(cc, j, k)] : (dir == 2 ? u[A(i, cc, k)] : u[A(i, j, cc)]); };
+          double r;
+          if (c == 1) r = (at(2) - at(1)) / dh;
+          else if (c == m0) r = (at(m0) - at(m0 - 1)) / dh;
+          else r = 0.5 * (at(c + 1) - at(c - 1)) / dh;
+          v[A(i, j, k)] = r;
+        }
+  }
+  void derivative_2nd(int dir, double dh, const std::vector<double>& u, std::vector<double>& v) const {
+    auto A = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)); };
+    const int m0 = dir == 1 ? im : (dir == 2 ? jm : km);
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+          const int c = dir == 1 ? i : (dir == 2 ? j : k);
+          auto at = [&](int cc) { return dir == 1 ? u[A(cc, j, k)] : (dir == 2 ? u[A(i, cc, k)] : u[A(i, j, cc)]); };
+          v[A(i, j, k)] = (c == 1 || c == m0) ? 0.0 : ((at(c + 1) + at(c - 1)) - 2.0 * at(c)) / (dh * dh);
+        }
+  }
+
+  // update_sources src/sources.F90:227-615 on one block: gravity
+  // (gacc_rayleigh_taylor, src/gravity.F90:283-330), viscosity, GLM source
+  // terms and resistivity, with gradient / divergence / laplace / curl of
+  // src/operators.F90:181-519
+  void update_sources(const Block& B, double* du) const {
+    const size_t N = cells();
+    const int nd = p.ndims;
+    const double dh[3] = {B.dx, B.dy, B.dz};
+    auto var = [&](int pv) {
+      std::vector<double> a(N);
+      for (size_t c = 0; c < N; ++c) a[c] = B.q[(size_t)(pv - 1) + (size_t)nv * c];
+      return a;
+    };
+    auto DU = [&](int pv, size_t c) -> double& { return du[(size_t)(pv - 1) + (size_t)nv * c]; };
+    std::vector<double> w(N);
+    // gradient: v = 0, then derivative_1st per direction
+    auto gradient = [&](const std::vector<double>& u, std::vector<double>* g3) {
+      for (int d = 0; d < 3; ++d) std::fill(g3[d].begin(), g3[d].end(), 0.0);
+      for (int d = 1; d <= nd; ++d) derivative_1st(d, dh[d - 1], u, g3[d - 1]);
+    };
+    // divergence: v = 0, v = v + derivative_1st per direction
+    auto divergence = [&](const std::vector<double>* u3, std::vector<double>& v) {
+      std::fill(v.begin(), v.end(), 0.0);
+      for (int d = 1; d <= nd; ++d) {
+        derivative_1st(d, dh[d - 1], u3[d - 1], w);
+        for (size_t c = 0; c < N; ++c) v[c] = v[c] + w[c];
+      }
+    };
+    const std::vector<double> rho = var(idn), vx = var(ivx), vy = var(ivy), vz = var(ivz);
+    if (p.gravity) {
+      const double ga[3] = {0.0, p.gacc, 0.0};
+      for (size_t c = 0; c < N; ++c) {
+        double gx = rho[c] * ga[0], gy = rho[c] * ga[1], gz = nd == 3 ? rho[c] * ga[2] : 0.0;
+        DU(imx, c) = DU(imx, c) + gx;
+        DU(imy, c) = DU(imy, c) + gy;
+        if (nd == 3) DU(imz, c) = DU(imz, c) + gz;
+        if (ien > 0) {
+          if (nd == 2) DU(ien, c) = DU(ien, c) + gx * vx[c] + gy * vy[c];
+          else DU(ien, c) = DU(ien, c) + gx * vx[c] + gy * vy[c] + gz * vz[c];
+        }
+      }
+    }
+    if (p.viscosity > 0.0) {
+      // T[row][col]
+      std::vector<double> T[3][3];
+      for (auto& r : T) for (auto& x : r) x.assign(N, 0.0);
+      std::vector<double> g3[3];
+      for (auto& x : g3) x.assign(N, 0.0);
+      const std::vector<double>* vel[3] = {&vx, &vy, &vz};
+      for (int r = 0; r < 3; ++r) {
+        gradient(*vel[r], g3);
+        for (int c2 = 0; c2 < 3; ++c2) T[r][c2] = g3[c2];
+      }
+      for (size_t c = 0; c < N; ++c) {
+        double gc = p.viscosity * rho[c], fc = 2.0 * gc;
+        double dvxdx = T[0][0][c], dvxdy = T[0][1][c], dvxdz = T[0][2][c];
+        double dvydx = T[1][0][c], dvydy = T[1][1][c], dvydz = T[1][2][c];
+        double dvzdx = T[2][0][c], dvzdy = T[2][1][c], dvzdz = T[2][2][c];
+        double divv = (dvxdx + dvydy + dvzdz) / 3.0;
+        T[0][0][c] = fc * (dvxdx - divv);
+        T[1][1][c] = fc * (dvydy - divv);
+        T[2][2][c] = fc * (dvzdz - divv);
+        T[0][1][c] = gc * (dvxdy + dvydx);
+        T[0][2][c] = gc * (dvxdz + dvzdx);
+        T[1][2][c] = gc * (dvydz + dvzdy);
+        T[1][0][c] = T[0][1][c];
+        T[2][0][c] = T[0][2][c];
+        T[2][1][c] = T[1][2][c];
+      }
+      std::vector<double> db(N);
+      const int mom[3] = {imx, imy, imz};
+      for (int r = 0; r < 3; ++r) {
+        divergence(T[r], db);
+        for (size_t c = 0; c < N; ++c) DU(mom[r], c) = DU(mom[r], c) + db[c];
+      }
+      if (ien > 0) {
+        for (size_t c = 0; c < N; ++c) {
+          double gx = vx[c] * T[0][0][c] + vy[c] * T[0][1][c] + vz[c] * T[0][2][c];
+          double gy = vx[c] * T[1][0][c] + vy[c] * T[1][1][c] + vz[c] * T[1][2][c];
+          double gz = vx[c] * T[2][0][c] + vy[c] * T[2][1][c] + vz[c] * T[2][2][c];
+          T[0][0][c] = gx;
+          T[0][1][c] = gy;
+          T[0][2][c] = gz;
+        }
+        divergence(T[0], db);
+        for (size_t c = 0; c < N; ++c) DU(ien, c) = DU(ien, c) + db[c];
+      }
+    }
+    if (ibx > 0) {
+      const std::vector<double> B3[3] = {var(ibx), var(iby), var(ibz)};
+      std::vector<double> db(N);
+      if (p.glm_sources > 0) {
+        divergence(B3, db);
+        for (size_t c = 0; c < N; ++c) {
+          DU(imx, c) = DU(imx, c) - db[c] * B3[0][c];
+          DU(imy, c) = DU(imy, c) - db[c] * B3[1][c];
+          DU(imz, c) = DU(imz, c) - db[c] * B3[2][c];
+        }
+        if (ien > 0 && ibp > 0) {
+          std::vector<double> g3[3];
+          for (auto& x : g3) x.assign(N, 0.0);
+          gradient(var(ibp), g3);
+          for (size_t c = 0; c < N; ++c)
+            DU(ien, c) = DU(ien, c) - (B3[0][c] * g3[0][c] + B3[1][c] * g3[1][c] + B3[2][c] * g3[2][c]);
+        }
+        if (p.glm_sources > 1) {
+          for (size_t c = 0; c < N; ++c) {
+            DU(ibx, c) = DU(ibx, c) - db[c] * vx[c];
+            DU(iby, c) = DU(iby, c) - db[c] * vy[c];
+            DU(ibz, c) = DU(ibz, c) - db[c] * vz[c];
+          }
+          if (ien > 0)
+            for (size_t c = 0; c < N; ++c)
+              DU(ien, c) = DU(ien, c) - db[c] * (vx[c] * B3[0][c] + vy[c] * B3[1][c] + vz[c] * B3[2][c]);
+        }
+      }
+      if (p.resistivity > 0.0) {
+        std::vector<double> L[3];
+        for (int r = 0; r < 3; ++r) {
+          L[r].assign(N, 0.0);
+          derivative_2nd(1, dh[0], B3[r], w);
+          L[r] = w;
+          derivative_2nd(2, dh[1], B3[r], w);
+          for (size_t c = 0; c < N; ++c) L[r][c] = L[r][c] + w[c];
+          if (nd == 3) {
+            derivative_2nd(3, dh[2], B3[r], w);
+            for (size_t c = 0; c < N; ++c) L[r][c] = L[r][c] + w[c];
+          }
+          for (size_t c = 0; c < N; ++c) L[r][c] = p.resistivity * L[r][c];
+        }
+        for (size_t c = 0; c < N; ++c) {
+          DU(ibx, c) = DU(ibx, c) + L[0][c];
+          DU(iby, c) = DU(iby, c) + L[1][c];
+          DU(ibz, c) = DU(ibz, c) + L[2][c];
+        }
+        if (ien > 0) {
+          for (size_t c = 0; c < N; ++c)
+            DU(ien, c) = DU(ien, c) + (B3[0][c] * L[0][c] + B3[1][c] * L[1][c] + B3[2][c] * L[2][c]);
+          // curl src/operators.F90:328-434
+          std::vector<double> j1(N), j2(N), j3(N);
+          derivative_1st(2, dh[1], B3[2], w);
+          j1 = w;
+          if (nd == 3) {
+            derivative_1st(3, dh[2], B3[1], w);
+            for (size_t c = 0; c < N; ++c) j1[c] = j1[c] - w[c];
+            derivative_1st(3, dh[2], B3[0], w);
+            j2 = w;
+            derivative_1st(1, dh[0], B3[2], w);
+            for (size_t c = 0; c < N; ++c) j2[c] = j2[c] - w[c];
+          } else {
+            derivative_1st(1, dh[0], B3[2], w);
+            for (size_t c = 0; c < N; ++c) j2[c] = -w[c];
+          }
+          derivative_1st(1, dh[0], B3[1], w);
+          j3 = w;
+          derivative_1st(2, dh[1], B3[0], w);
+          for (size_t c = 0; c < N; ++c) j3[c] = j3[c] - w[c];
+          for (size_t c = 0; c < N; ++c) {
+            double d2 = j1[c] * j1[c] + j2[c] * j2[c] + j3[c] * j3[c];
+            DU(ien, c) = DU(ien, c) + p.resistivity * d2;
+          }
+        }
+      }
+    }
+  }
+
   // One stage: fluxes, then per block increment + combination.  `comb`
   // receives (u0, u1, du, cell-count) of a block.
   template <class C> void stage(C comb) {
@@ -3321,6 +3530,7 @@ struct Oracle {
     parallel_blocks([&](Block& B) {
       std::vector<double> du((size_t)nv * cells());
       update_increment(B, B.f.data(), du.data());
+      if (sources_on) update_sources(B, du.data());
       comb(B, du.data());
     });
   }

@@ -56,6 +56,9 @@ def test_default_params_match_reference_defaults():
     ("reconstruction", "LimO3", "reconstruction", 3), ("reconstruction", "weno5-ns", "reconstruction", 6),
     ("reconstruction", "MP7", "reconstruction", 8), ("limo3_rad", "0.25", "limo3_rad", 0.25),
     ("ppm_const", "2", "ppm_const", 2.0), ("kappa", "4", "kappa", 4.0), ("mlp_limiting", "on", "mlp", 1),
+    ("viscosity", "0.01", "viscosity", 0.01), ("resistivity", "1e-3", "resistivity", 1e-3),
+    ("glm_source_terms", "HEGLM", "glm_sources", 2), ("glm_source_terms", "none", "glm_sources", 0),
+    ("problem", "rayleigh-taylor", "gravity", 1), ("problem", "blast", "gravity", 0), ("gacc", "-2", "gacc", -2.0),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()
