@@ -37,7 +37,8 @@ class amun_params(C.Structure):
         ("csnd", C.c_double), ("c2p", C.c_int), ("mlp", C.c_int), ("limo3_rad", C.c_double),
         ("ppm_const", C.c_double), ("kappa", C.c_double), ("kbeta", C.c_double),
         ("viscosity", C.c_double), ("resistivity", C.c_double), ("glm_sources", C.c_int), ("gravity", C.c_int),
-        ("gacc", C.c_double),
+        ("gacc", C.c_double), ("fix_unphysical", C.c_int), ("ngavg", C.c_int), ("npavg", C.c_int),
+        ("dmin", C.c_double),
     ]
 
 
@@ -48,7 +49,7 @@ class amun_block_desc(C.Structure):
 class amun_status(C.Structure):
     _fields_ = [("time", C.c_double), ("dt", C.c_double), ("dtn", C.c_double), ("cmax", C.c_double),
                 ("step", C.c_longlong), ("nonpositive", C.c_longlong), ("c2p_failures", C.c_longlong),
-                ("device_bytes", C.c_longlong)]
+                ("device_bytes", C.c_longlong), ("unphysical_cells", C.c_longlong)]
 
 
 _lib = None

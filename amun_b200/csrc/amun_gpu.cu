@@ -77,6 +77,10 @@ struct Ctx {
   std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
   // sweep tile chosen by amun_gpu_autotune (0: the default shape)
   int tile_LP = 0, tile_LW = 0;
+  // correct_unphysical_states: the replacement list (cell index, values)
+  int* fix_idx = nullptr;
+  void* fix_val = nullptr;
+  int fix_cap = 0;
 };
 
 Ctx C;
@@ -208,6 +212,9 @@ void free_pool() {
   for (void* x : amrp)
     if (x) cudaFree(x);
   C.gop = nullptr; C.frole = C.fquad = C.blist = nullptr; C.ff = nullptr;
+  if (C.fix_idx) cudaFree(C.fix_idx);
+  if (C.fix_val) cudaFree(C.fix_val);
+  C.fix_idx = nullptr; C.fix_val = nullptr; C.fix_cap = 0;
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   if (C.u0) cudaFree(C.u0);
@@ -415,6 +422,21 @@ int launch_stage(const StageDesc& st) {
   ProfScope ps(3);
   cudaError_t e = ghost_fill<R>((R*)C.q[C.cur]);
   if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  if (C.p.fix_unphysical) {
+    // correct_unphysical_states after the boundary update
+    // (src/evolution.F90:2043-2068); the maximum speed of the final stage's
+    // state is taken again afterwards, from the corrected primitives
+    FixConst f{C.p.ngavg, C.p.npavg, C.fix_cap, C.p.dmin, C.p.pmin};
+    void* u = st.out_dst == 0 ? (void*)C.u0 : C.u1;
+    e = Launch<R, R>::fix_unphysical(C.p.eqsys, (R*)C.q[C.cur], u, st.out_dst == 0 || !bulk(), C.g, C.nblocks,
+                                     method_const(), f, C.fix_idx, (R*)C.fix_val, C.sc, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "correct_unphysical_states");
+    if (st.final_stage) {
+      CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
+      e = Launch<R, R>::maxspeed(C.p.eqsys, (const R*)C.q[C.cur], C.g, C.gamma, C.p.csnd, C.sc, C.nblocks, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "maxspeed");
+    }
+  }
   return 0;
 }
 
@@ -545,6 +567,10 @@ void amun_gpu_default_params(amun_params* p) {
   p->glm_sources = 0;
   p->gravity = 0;
   p->gacc = -1.0;
+  p->fix_unphysical = 0;
+  p->ngavg = 2;
+  p->npavg = 4;
+  p->dmin = 1.0e-16;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -627,6 +653,10 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "viscosity") p->viscosity = atof(v);
   else if (k == "resistivity") p->resistivity = atof(v);
   else if (k == "gacc") p->gacc = atof(v);
+  else if (k == "fix_unphysical_cells") p->fix_unphysical = is_on(v);
+  else if (k == "ngavg") p->ngavg = atoi(v);
+  else if (k == "npavg") p->npavg = atoi(v);
+  else if (k == "dmin") p->dmin = atof(v);
   else if (k == "glm_source_terms") {
     if (is_one_of(v, {"eglm", "EGLM"})) p->glm_sources = 1;
     else if (is_one_of(v, {"heglm", "HEGLM"})) p->glm_sources = 2;
@@ -677,6 +707,9 @@ int amun_gpu_init(const amun_params* p) {
   if (!C.sc) CK(cudaMalloc(&C.sc, sizeof(DevScalars)));
   CK(dset(C.sc, 0, sizeof(DevScalars)));
   C.p = *p;
+  // src/equations.F90:923-924
+  if (C.p.ngavg < 1) C.p.ngavg = 1;
+  if (C.p.npavg < 2) C.p.npavg = 2;
   // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
   if (C.p.reconstruction == AMUN_REC_LIMO3) C.p.eps = C.p.eps > 1.0e-12 ? C.p.eps : 1.0e-12;
   C.nv = (p->eqsys == AMUN_EQ_HD || p->eqsys == AMUN_EQ_SRHD) ? 5 : 9;
@@ -934,6 +967,14 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   CK(h2d(C.binv, binv.data(), binv.size() * sizeof(double)));
   CK(cudaMalloc(&C.bdx, bdx.size() * sizeof(double)));
   CK(h2d(C.bdx, bdx.data(), bdx.size() * sizeof(double)));
+  if (C.p.fix_unphysical) {
+    // room for 1/64 of the padded cells (at least 4096) per fix pass
+    const long long cells = (long long)g.qvs * nblocks;
+    C.fix_cap = (int)std::min<long long>(std::max<long long>(cells / 64, 4096), 1LL << 30);
+    CK(cudaMalloc(&C.fix_idx, (size_t)C.fix_cap * sizeof(int)));
+    CK(cudaMalloc(&C.fix_val, (size_t)C.fix_cap * C.nv * rsize()));
+    C.pool_bytes += (long long)C.fix_cap * (sizeof(int) + C.nv * rsize());
+  }
   C.cur = 0;
   C.ms_valid = false;
   if (levels_differ) {
@@ -1154,6 +1195,10 @@ int amun_gpu_status(amun_status* s) {
   s->nonpositive = (long long)h.nonpositive;
   s->c2p_failures = (long long)h.c2p_failures;
   s->device_bytes = C.pool_bytes;
+  s->unphysical_cells = (long long)h.unphysical;
+  if (h.fix_overflow)
+    return fail(AMUN_E_UNSUPPORTED, "correct_unphysical_states: " + std::to_string(h.fix_overflow) +
+                                        " cells beyond the replacement list were left uncorrected");
   return 0;
 }
 

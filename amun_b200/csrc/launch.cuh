@@ -16,6 +16,10 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, double csnd, DevScalars* sc,
                               int nblocks, cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
+  // correct_unphysical_states on every block; u is U0 (u_double) or U1
+  static cudaError_t fix_unphysical(int eq, R* q, void* u, bool u_double, const Geo& g, int nblocks,
+                                    const MethodConst& m, const FixConst& f, int* idx, R* val, DevScalars* sc,
+                                    cudaStream_t s);
   static cudaError_t cons2prim_blocks(int eq, const double* u0, R* q, const Geo& g, const MethodConst& m,
                                       DevScalars* sc, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
@@ -167,6 +171,32 @@ cudaError_t Launch<R, U1T>::maxspeed(int eq, const R* q, const Geo& g, double ga
   else if (eq == EQ_MHD_ISO) maxspeed_kernel<EQ_MHD_ISO, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   else maxspeed_kernel<EQ_SRMHD, R><<<grid, threads, 0, s>>>(q, g, gamma, csnd, sc, nblocks);
   return cudaGetLastError();
+}
+
+template <int EQ, typename R, typename U1T>
+static cudaError_t fix_unphysical_eq(R* q, void* u, bool u_double, const Geo& g, int nblocks, const MethodConst& m,
+                                     const FixConst& f, int* idx, R* val, DevScalars* sc, cudaStream_t s) {
+  const long long n = (long long)g.IM * g.JM * g.KM * nblocks;
+  cudaError_t e = cudaMemsetAsync(&sc->fix_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  unphysical_scan_kernel<EQ, R><<<grid_for(n, 256), 256, 0, s>>>(q, g, nblocks, f, idx, val, sc);
+  const int ga = grid_for(f.cap, 256, 1024);
+  if (u_double) unphysical_apply_kernel<EQ, R, double><<<ga, 256, 0, s>>>(q, (double*)u, g, m, idx, val, f.cap, sc);
+  else unphysical_apply_kernel<EQ, R, U1T><<<ga, 256, 0, s>>>(q, (U1T*)u, g, m, idx, val, f.cap, sc);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::fix_unphysical(int eq, R* q, void* u, bool u_double, const Geo& g, int nblocks,
+                                           const MethodConst& m, const FixConst& f, int* idx, R* val,
+                                           DevScalars* sc, cudaStream_t s) {
+  switch (eq) {
+    case EQ_HD: return fix_unphysical_eq<EQ_HD, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+    case EQ_MHD: return fix_unphysical_eq<EQ_MHD, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+    case EQ_SRMHD: return fix_unphysical_eq<EQ_SRMHD, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+    case EQ_SRHD: return fix_unphysical_eq<EQ_SRHD, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+    case EQ_HD_ISO: return fix_unphysical_eq<EQ_HD_ISO, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+    default: return fix_unphysical_eq<EQ_MHD_ISO, R, U1T>(q, u, u_double, g, nblocks, m, f, idx, val, sc, s);
+  }
 }
 
 template <typename R, typename U1T>

@@ -44,6 +44,9 @@ struct DevScalars {
   unsigned long long nonpositive;  // positive variable not positive (TVD)
   long long step;
   unsigned long long c2p_failures;  // relativistic recoveries that failed (p := 0)
+  unsigned long long unphysical;    // cells replaced by correct_unphysical_states
+  unsigned long long fix_overflow;  // of those, cells beyond the fix list (not replaced)
+  unsigned long long fix_count;     // entries of the current fix pass (reset per pass)
 };
 
 // One SSPRK stage combination.  ds = dscoef * dt.
@@ -650,6 +653,106 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma, a.m.csnd));
   }
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
+}
+
+// ---------------------------------------------------------------------------
+// correct_unphysical_states (src/equations.F90:1168-1330), run on every block
+// after the ghost fill when fix_unphysical_cells is on.  Pass 1: each cell
+// of a padded block with rho <= 0 or p <= 0 gets the mean of the physical
+// cells of the smallest window (half-width 1 .. ngavg, clipped to the block)
+// holding more than npavg of them, or, with fewer than npavg, its own state
+// with rho and p raised to dmin / pmin; the replacements go to a list (all
+// reads see the state before any replacement).  Pass 2 writes them to q and,
+// for interior cells, prim2cons into the stage's U.
+// ---------------------------------------------------------------------------
+struct FixConst {
+  int ngavg, npavg, cap;
+  double dmin, pmin;
+};
+
+template <int EQ, typename R>
+__global__ void unphysical_scan_kernel(const R* q, Geo g, int nblocks, FixConst f, int* idx, R* val,
+                                       DevScalars* sc) {
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
+  const long long cells = (long long)g.IM * g.JM * g.KM;
+  auto physical = [&](const R* qb, long long c) {
+    bool ph = qb[c + V::DN * g.qvs] > R(0);
+    if constexpr (V::PR >= 0) ph = ph && qb[c + V::PR * g.qvs] > R(0);
+    return ph;
+  };
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * nblocks;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long b = t / cells, c = t - b * cells;
+    const R* qb = q + b * g.qbs;
+    if (physical(qb, c)) continue;
+    const int i = (int)(c % g.IM), j = (int)((c / g.IM) % g.JM), k = (int)(c / ((long long)g.IM * g.JM));
+    int np = 0, p = 1, il = i, iu = i, jl = j, ju = j, kl = k, ku = k;
+    while (np <= f.npavg && p <= f.ngavg) {
+      il = i - p < 0 ? 0 : i - p; iu = i + p > g.IM - 1 ? g.IM - 1 : i + p;
+      jl = j - p < 0 ? 0 : j - p; ju = j + p > g.JM - 1 ? g.JM - 1 : j + p;
+      kl = k - p < 0 ? 0 : k - p; ku = k + p > g.KM - 1 ? g.KM - 1 : k + p;
+      np = 0;
+      for (int kk = kl; kk <= ku; ++kk)
+        for (int jj = jl; jj <= ju; ++jj)
+          for (int ii = il; ii <= iu; ++ii)
+            if (physical(qb, ((long long)kk * g.JM + jj) * g.IM + ii)) ++np;
+      p = p + 1;
+    }
+    R qn[NV];
+    if (np >= f.npavg) {
+      for (int v = 0; v < NV; ++v) {
+        R s = R(0);
+        for (int kk = kl; kk <= ku; ++kk)
+          for (int jj = jl; jj <= ju; ++jj)
+            for (int ii = il; ii <= iu; ++ii) {
+              const long long cc = ((long long)kk * g.JM + jj) * g.IM + ii;
+              if (physical(qb, cc)) s = s + qb[cc + v * g.qvs];
+            }
+        qn[v] = s / R(np);
+      }
+    } else {
+      for (int v = 0; v < NV; ++v) qn[v] = qb[c + v * g.qvs];
+      qn[V::DN] = d_max(R(f.dmin), qn[V::DN]);
+      if constexpr (V::PR >= 0) qn[V::PR] = d_max(R(f.pmin), qb[c + V::PR * g.qvs]);
+    }
+    atomicAdd(&sc->unphysical, 1ull);
+    const unsigned long long n = atomicAdd(&sc->fix_count, 1ull);
+    if (n >= (unsigned long long)f.cap) {
+      atomicAdd(&sc->fix_overflow, 1ull);
+      continue;
+    }
+    idx[n] = (int)t;
+    for (int v = 0; v < NV; ++v) val[n * NV + v] = qn[v];
+  }
+}
+
+template <int EQ, typename R, typename UT>
+__global__ void unphysical_apply_kernel(R* q, UT* u, Geo g, MethodConst m, const int* idx, const R* val, int cap,
+                                        const DevScalars* sc) {
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
+  const unsigned long long total = sc->fix_count;
+  const long long n = (long long)(total < (unsigned long long)cap ? total : (unsigned long long)cap);
+  const long long cells = (long long)g.IM * g.JM * g.KM;
+  const Phys<double> P = make_phys<double>(m, 0.0, 0.0);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long t = idx[e];
+    const long long b = t / cells, c = t - b * cells;
+    double qd[NV], ud[NV];
+    for (int v = 0; v < NV; ++v) {
+      q[b * g.qbs + c + v * g.qvs] = val[e * NV + v];
+      qd[v] = (double)val[e * NV + v];
+    }
+    const int i = (int)(c % g.IM), j = (int)((c / g.IM) % g.JM), k = (int)(c / ((long long)g.IM * g.JM));
+    const bool interior = i >= g.ng && i < g.ng + g.nc && j >= g.ng && j < g.ng + g.nc &&
+                          (g.ndims == 2 || (k >= g.ng && k < g.ng + g.nc));
+    if (!interior) continue;
+    prim2cons<EQ>(qd, ud, P);
+    const long long ic = (long long)(i - g.ng) + (long long)g.nc * ((j - g.ng) + (long long)g.nc *
+                                                                     (g.ndims == 3 ? k - g.ng : 0));
+    for (int v = 0; v < NV; ++v) u[b * g.ubs + ic + v * g.uvs] = (UT)ud[v];
+  }
 }
 
 // ---------------------------------------------------------------------------

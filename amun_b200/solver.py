@@ -132,7 +132,8 @@ class Simulation:
         s = N.amun_status()
         N.check(self.L.amun_gpu_status(C.byref(s)))
         return dict(time=s.time, dt=s.dt, dtn=s.dtn, cmax=s.cmax, step=s.step,
-                    nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes)
+                    nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes,
+                    unphysical_cells=s.unphysical_cells)
 
     def _states(self, a: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float64)

@@ -102,6 +102,10 @@ typedef struct amun_params {
   int gravity;          /* 0/1: "problem" = rt / rayleightaylor / rayleigh-
                            taylor switches the uniform acceleration on      */
   double gacc;          /*                        "gacc" (y component)        */
+  /* correct_unphysical_states (src/equations.F90:887-925, 1168-1330) */
+  int fix_unphysical;   /* 0/1                    "fix_unphysical_cells"      */
+  int ngavg, npavg;     /*                        "ngavg" (>= 1), "npavg" (>= 2) */
+  double dmin;          /*                        "dmin"                      */
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block
@@ -126,6 +130,7 @@ typedef struct amun_status {
   long long c2p_failures; /* relativistic recoveries that failed or gave
                              p <= 0 (src/equations.F90:4745-4777)           */
   long long device_bytes; /* bytes of device memory held by the block pool    */
+  long long unphysical_cells; /* cells replaced by correct_unphysical_states  */
 } amun_status;
 
 /* Fill *p with the reference defaults (hd/adi, tvd/mm, hll, rk2, cfl 0.5 ...). */

@@ -67,6 +67,10 @@ struct Params {
   int glm_sources = 0;     // glm_source_terms: 0 none, 1 EGLM, 2 HEGLM
   bool gravity = false;    // problem = rt (src/gravity.F90:137-146)
   double gacc = -1.0;
+  // correct_unphysical_states (src/equations.F90:184, 206-208, 887-925)
+  bool fix_unphysical = false;
+  int ngavg = 2, npavg = 4;
+  double dmin = 1.0e-16;
   // relativistic recovery (src/equations.F90:184-201, 313-318)
   double tol = 1.0e-10, pmin = 1.0e-16;
   int nrmax = 100, nrext = 2;
@@ -156,6 +160,10 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "viscosity") p.viscosity = atof(v.c_str());
   else if (key == "resistivity") p.resistivity = atof(v.c_str());
   else if (key == "gacc") p.gacc = atof(v.c_str());
+  else if (key == "fix_unphysical_cells") p.fix_unphysical = is_on(v);
+  else if (key == "ngavg") p.ngavg = atoi(v.c_str());
+  else if (key == "npavg") p.npavg = atoi(v.c_str());
+  else if (key == "dmin") p.dmin = atof(v.c_str());
   else if (key == "glm_source_terms") {
     if (is_one_of(v, {"eglm", "EGLM"})) p.glm_sources = 1;
     else if (is_one_of(v, {"heglm", "HEGLM"})) p.glm_sources = 2;
@@ -459,6 +467,7 @@ struct Oracle {
   bool sources_on = false;       // update_sources has work
   double cmax = 0.0, cmax2 = 0.0;
   mutable std::atomic<long> c2p_failures{0};  // failed relativistic recoveries (p set to 0)
+  long long unphysical_cells = 0;             // cells replaced by correct_unphysical_states
   // evolution (src/evolution.F90:60-90)
   double cfl = 0.5, decay = 1.0, time = 0.0, dt = 0.0, dtn = 1.0;
   long step = 0;
@@ -533,6 +542,8 @@ struct Oracle {
     // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
     if (p.rec == REC_LIMO3) p.eps = fmax2(1.0e-12, p.eps);
     if (sr && p.c2p < 0) return 110;
+    p.ngavg = std::max(1, p.ngavg);
+    p.npavg = std::max(2, p.npavg);
     // the relativistic systems offer HLL and HLLC ("hllcm" included,
     // src/schemes.F90:400-498); elsewhere "hllcm" names nothing
     if (sr) p.rs = (p.rs == RS_HLLC || p.rs == RS_HLLCM) ? RS_HLLC : RS_HLL;
@@ -3284,11 +3295,77 @@ struct Oracle {
     });
   }
 
-  // update_variables src/evolution.F90:1994-2094 (no unphysical-cell fix,
-  // no shapes: both default off)
+  // correct_unphysical_states src/equations.F90:1168-1330 on one block:
+  // every cell (ghosts included) with rho <= 0 or p <= 0 takes the mean of
+  // the physical cells of the smallest clipped window of half-width up to
+  // ngavg that holds more than npavg of them, or else its own state with rho
+  // and p raised to dmin / pmin; all read the state before any replacement
+  long long correct_unphysical_states(Block& B) const {
+    const size_t N = cells();
+    auto A = [&](int i, int j, int k) { return (size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)); };
+    std::vector<char> physical(N);
+    for (size_t c = 0; c < N; ++c) {
+      bool ph = B.q[(size_t)(idn - 1) + (size_t)nv * c] > 0.0;
+      if (ipr > 0) ph = ph && B.q[(size_t)(ipr - 1) + (size_t)nv * c] > 0.0;
+      physical[c] = ph;
+    }
+    std::vector<size_t> where;
+    std::vector<double> qn;
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+          if (physical[A(i, j, k)]) continue;
+          int np = 0, pp = 1, il = i, iu = i, jl = j, ju = j, kl = k, ku = k;
+          while (np <= p.npavg && pp <= p.ngavg) {
+            il = std::max(1, i - pp); iu = std::min(im, i + pp);
+            jl = std::max(1, j - pp); ju = std::min(jm, j + pp);
+            kl = std::max(1, k - pp); ku = std::min(km, k + pp);
+            np = 0;
+            for (int kk = kl; kk <= ku; ++kk)
+              for (int jj = jl; jj <= ju; ++jj)
+                for (int ii = il; ii <= iu; ++ii) np += physical[A(ii, jj, kk)] ? 1 : 0;
+            pp = pp + 1;
+          }
+          std::vector<double> q(nv);
+          const size_t c = A(i, j, k);
+          if (np >= p.npavg) {
+            for (int v = 0; v < nv; ++v) {
+              double sum = 0.0;
+              for (int kk = kl; kk <= ku; ++kk)
+                for (int jj = jl; jj <= ju; ++jj)
+                  for (int ii = il; ii <= iu; ++ii) {
+                    const size_t cc = A(ii, jj, kk);
+                    if (physical[cc]) sum = sum + B.q[(size_t)v + (size_t)nv * cc];
+                  }
+              q[v] = sum / np;
+            }
+          } else {
+            for (int v = 0; v < nv; ++v) q[v] = B.q[(size_t)v + (size_t)nv * c];
+            q[idn - 1] = fmax2(p.dmin, B.q[(size_t)(idn - 1) + (size_t)nv * c]);
+            if (ipr > 0) q[ipr - 1] = fmax2(p.pmin, B.q[(size_t)(ipr - 1) + (size_t)nv * c]);
+          }
+          where.push_back(c);
+          qn.insert(qn.end(), q.begin(), q.end());
+        }
+    const size_t nc = where.size();
+    if (nc == 0) return 0;
+    std::vector<double> un(qn.size());
+    prim2cons((int)nc, qn.data(), un.data());
+    for (size_t n = 0; n < nc; ++n)
+      for (int v = 0; v < nv; ++v) {
+        B.q[(size_t)v + (size_t)nv * where[n]] = qn[(size_t)nv * n + v];
+        B.u[(size_t)v + (size_t)nv * where[n]] = un[(size_t)nv * n + v];
+      }
+    return (long long)nc;
+  }
+
+  // update_variables src/evolution.F90:1994-2094, with
+  // correct_unphysical_states when fix_unphysical_cells is on (no shapes)
   void update_variables() {
     parallel_blocks([&](Block& B) { update_primitive_variables(B.u, B.q.data()); });
     boundary_variables();
+    if (p.fix_unphysical)
+      for (auto& B : blocks) unphysical_cells += correct_unphysical_states(B);
   }
 
   // new_time_step src/evolution.F90:379-493
@@ -3788,6 +3865,7 @@ void or_scalars(void* h, double* out) {
   Oracle* o = static_cast<Oracle*>(h);
   out[0] = o->time; out[1] = o->dt; out[2] = o->cmax; out[3] = (double)o->step; out[4] = (double)o->nonpositive;
   out[5] = (double)o->c2p_failures;
+  out[6] = (double)o->unphysical_cells;
 }
 
 // ---- unit-level entry points ------------------------------------------------

@@ -137,10 +137,10 @@ class Oracle:
         return t.value, dt.value
 
     def scalars(self) -> dict:
-        s = (C.c_double * 6)()
+        s = (C.c_double * 7)()
         self.L.or_scalars(self.h, s)
         return dict(time=s[0], dt=s[1], cmax=s[2], step=int(s[3]), nonpositive=int(s[4]),
-                    c2p_failures=int(s[5]))
+                    c2p_failures=int(s[5]), unphysical_cells=int(s[6]))
 
     # ---- unit level --------------------------------------------------------
     def set_cmax(self, cmax: float):

@@ -59,6 +59,8 @@ def test_default_params_match_reference_defaults():
     ("viscosity", "0.01", "viscosity", 0.01), ("resistivity", "1e-3", "resistivity", 1e-3),
     ("glm_source_terms", "HEGLM", "glm_sources", 2), ("glm_source_terms", "none", "glm_sources", 0),
     ("problem", "rayleigh-taylor", "gravity", 1), ("problem", "blast", "gravity", 0), ("gacc", "-2", "gacc", -2.0),
+    ("fix_unphysical_cells", "Y", "fix_unphysical", 1), ("ngavg", "3", "ngavg", 3), ("npavg", "6", "npavg", 6),
+    ("dmin", "1e-10", "dmin", 1e-10),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()
