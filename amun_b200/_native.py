@@ -15,6 +15,11 @@ AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD, AMUN_EQ_SRHD = 0, 1, 2, 3
 AMUN_EOS_ADI, AMUN_EOS_ISO = 0, 1
 AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
 AMUN_FP64, AMUN_FP32_BULK = 0, 1
+# library errors (include/amun_gpu.h)
+AMUN_E_NOT_INITIALIZED, AMUN_E_BAD_ARGUMENT, AMUN_E_CUDA, AMUN_E_UNSUPPORTED, AMUN_E_NO_BLOCKS = 901, 902, 903, 904, 905
+# refinement_variables bits: dens velx vely velz magx magy magz bpsi pres vort jabs
+(AMUN_REF_DENS, AMUN_REF_VELX, AMUN_REF_VELY, AMUN_REF_VELZ, AMUN_REF_MAGX, AMUN_REF_MAGY, AMUN_REF_MAGZ,
+ AMUN_REF_BPSI, AMUN_REF_PRES, AMUN_REF_VORT, AMUN_REF_JABS) = (1 << n for n in range(11))
 
 
 class AmunError(RuntimeError):
@@ -38,7 +43,9 @@ class amun_params(C.Structure):
         ("ppm_const", C.c_double), ("kappa", C.c_double), ("kbeta", C.c_double),
         ("viscosity", C.c_double), ("resistivity", C.c_double), ("glm_sources", C.c_int), ("gravity", C.c_int),
         ("gacc", C.c_double), ("fix_unphysical", C.c_int), ("ngavg", C.c_int), ("npavg", C.c_int),
-        ("dmin", C.c_double),
+        ("dmin", C.c_double), ("ref_mask", C.c_int), ("crefmin", C.c_double), ("crefmax", C.c_double),
+        ("epsref", C.c_double), ("vortmin", C.c_double), ("vortmax", C.c_double), ("jabsmin", C.c_double),
+        ("jabsmax", C.c_double),
     ]
 
 
@@ -73,6 +80,8 @@ def lib():
         "amun_gpu_upload": (i, [i, _D, _D, _D]),
         "amun_gpu_upload_blocks": (i, [i, i, _D, _D]),
         "amun_gpu_upload_conserved": (i, [i, i, _D]),
+        "amun_gpu_refinement_criterion": (i, [C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+        "amun_gpu_regrid": (i, [i, C.POINTER(amun_block_desc), C.POINTER(C.c_int)]),
         "amun_gpu_download": (i, [i, _D, _D, _D]),
         "amun_gpu_download_blocks": (i, [i, i, _D, _D]),
         "amun_gpu_boundary_variables": (i, []),

@@ -13,6 +13,7 @@ a face, edge or corner differ by at most one level.
 """
 from __future__ import annotations
 
+import copy
 import itertools
 
 import numpy as np
@@ -52,6 +53,7 @@ class AMRMesh:
         self.ylen = geo["ymax"] - geo["ymin"]
         self.zlen = geo["zmax"] - geo["zmin"] if self.ndims == 3 else 1.0
         self.maxlev = int(geo["maxlev"])
+        self.minlev = int(geo.get("minlev", 1))
         self.im = self.nc + 2 * self.ng
         self.jm = self.im
         self.km = self.im if self.ndims == 3 else 1
@@ -131,6 +133,131 @@ class AMRMesh:
                 if pred(lo, hi, level):
                     self.refine(leaf)
             self.balance()
+
+    # ---- mesh update ------------------------------------------------------------
+    def _offsets(self):
+        offs = [o for o in itertools.product((-1, 0, 1), repeat=3) if any(o)]
+        return [o for o in offs if o[2] == 0] if self.ndims == 2 else offs
+
+    def _touching(self, level, x, y, z, o):
+        """Leaves inside the subdivided position (level, x, y, z) that touch
+        the block it neighbours in direction -o."""
+        ex, ey, ez = self.extent(level + 1)
+        subs = [(0,) if d == 1 else ((1,) if d == -1 else (0, 1)) for d in o]
+        if self.ndims == 2:
+            subs[2] = (0,)
+        out = set()
+        for c in subs[2]:
+            for b in subs[1]:
+                for a in subs[0]:
+                    key = (level + 1, (2 * x + a) % ex, (2 * y + b) % ey, (2 * z + c) % ez)
+                    if key in self.leaves:
+                        out.add(key)
+                    elif level + 1 < self.maxlev:
+                        out |= self._touching(level + 1, key[1], key[2], key[3], o)
+        return out
+
+    def neighbours(self, leaf):
+        """Leaves touching `leaf` across a face, an edge or a corner (the
+        faces / edges / corners pointers of src/blocks.F90:4369-4463)."""
+        l, cx, cy, cz = leaf
+        out = set()
+        for o in self._offsets():
+            c = self.cover(l, cx + o[0], cy + o[1], cz + o[2])
+            if c is not None:
+                out.add(c)
+            else:
+                ex, ey, ez = self.extent(l)
+                out |= self._touching(l, (cx + o[0]) % ex, (cy + o[1]) % ey, (cz + o[2]) % ez, o)
+        out.discard(leaf)
+        return out
+
+    def is_balanced(self) -> bool:
+        """Neighbours across faces, edges and corners differ by at most one level."""
+        return all(abs(n[0] - t[0]) <= 1 for t in self.leaves for n in self.neighbours(t))
+
+    def update_plan(self, criterion):
+        """The mesh after update_mesh (src/mesh.F90:756-821) for the per-block
+        criterion (-1 derefine, 0 keep, 1 refine, block-index order) and, per
+        new block, where its data comes from: (new AMRMesh, src (n, 9) int32)
+        with rows {0, old} kept, {1, parent, px + 2 py + 4 pz} prolonged and
+        {2, children by position} restricted.
+
+        The flags follow check_data_block_refinement (src/mesh.F90:1455-1680:
+        the minlev / maxlev clamps), update_neighbor_refinement (1694-1748
+        with reset_neighbors_refinement, src/blocks.F90:4297-4352, from the
+        finest level down) and prepare_sibling_derefinement (1768-2055: a
+        parent derefines only when all its children are leaves flagged -1).
+        Within a level the leaves are visited in block-index order."""
+        order = self.order
+        index = {t: b for b, t in enumerate(order)}
+        crit = np.asarray(criterion).reshape(-1)
+        if len(crit) != len(order):
+            raise ValueError("one criterion per block")
+        ref = {}
+        for t, c in zip(order, crit):
+            r, l = int(c), t[0]
+            if l < self.minlev:
+                r = 1
+            if l == self.minlev:
+                r = max(0, r)
+            if l == self.maxlev:
+                r = min(0, r)
+            if l > self.maxlev:
+                r = -1
+            ref[t] = r
+        for l in range(self.maxlev, 0, -1):
+            for t in order:
+                if t[0] != l:
+                    continue
+                for n in sorted(self.neighbours(t), key=lambda x: index[x]):
+                    if ref[t] == 1:
+                        ref[n] = max(0, ref[n])
+                        if n[0] < l:
+                            ref[n] = 1
+                    elif ref[t] == 0:
+                        if n[0] < l:
+                            ref[n] = max(0, ref[n])
+                    else:
+                        if n[0] < l:
+                            ref[n] = max(0, ref[n])
+                        if ref[n] == 1:
+                            ref[t] = 0
+        derefine = set()
+        for l in range(2, self.maxlev + 1):
+            for t in order:
+                if t[0] != l or ref[t] != -1:
+                    continue
+                parent = (l - 1, t[1] // 2, t[2] // 2, t[3] // 2)
+                sibs = self._children(parent)
+                if all(ref.get(s) == -1 for s in sibs):
+                    derefine.add(parent)
+                else:
+                    for s in sibs:
+                        if s in ref:
+                            ref[s] = max(0, ref[s])
+        new = set(self.leaves)
+        for parent in derefine:
+            new.difference_update(self._children(parent))
+            new.add(parent)
+        for t in order:
+            if ref[t] == 1 and t[0] < self.maxlev and t in new:
+                new.discard(t)
+                new.update(self._children(t))
+        mesh = copy.copy(self)
+        mesh.leaves = new
+        src = np.zeros((len(new), 9), dtype=np.int32)
+        for b, t in enumerate(mesh.order):
+            if t in index:
+                src[b, :2] = (0, index[t])
+            elif t in derefine:
+                src[b, 0] = 2
+                for c, ch in enumerate(self._children(t)):
+                    src[b, 1 + c] = index[ch]
+            else:
+                l, cx, cy, cz = t
+                src[b, :3] = (1, index[(l - 1, cx // 2, cy // 2, cz // 2)], (cx & 1) + 2 * (cy & 1) + 4 * (cz & 1))
+        return mesh, src
 
     # ---- blocks -----------------------------------------------------------------
     @property

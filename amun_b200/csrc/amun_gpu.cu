@@ -18,6 +18,7 @@
 #include "../../include/amun_gpu.h"
 #include "adjoint.h"
 #include "launch.cuh"
+#include "regrid.h"
 #include "unit.h"
 
 using namespace amun;
@@ -571,6 +572,14 @@ void amun_gpu_default_params(amun_params* p) {
   p->ngavg = 2;
   p->npavg = 4;
   p->dmin = 1.0e-16;
+  p->ref_mask = AMUN_REF_DENS | AMUN_REF_PRES;  // "dens pres"
+  p->crefmin = 0.2;
+  p->crefmax = 0.8;
+  p->epsref = 1.0e-2;
+  p->vortmin = 1.0e-3;
+  p->vortmax = 1.0e-1;
+  p->jabsmin = 1.0e-3;
+  p->jabsmax = 1.0e-1;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -657,6 +666,20 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "ngavg") p->ngavg = atoi(v);
   else if (k == "npavg") p->npavg = atoi(v);
   else if (k == "dmin") p->dmin = atof(v);
+  else if (k == "refinement_variables") {
+    // index(variables, name) > 0 for each name (src/refinement.F90:150-160)
+    static const char* names[] = {"dens", "velx", "vely", "velz", "magx", "magy", "magz", "bpsi", "pres", "vort",
+                                  "jabs"};
+    p->ref_mask = 0;
+    for (int n = 0; n < 11; ++n)
+      if (vs.find(names[n]) != std::string::npos) p->ref_mask |= 1 << n;
+  } else if (k == "crefmin") p->crefmin = atof(v);
+  else if (k == "crefmax") p->crefmax = atof(v);
+  else if (k == "epsref") p->epsref = atof(v);
+  else if (k == "vortmin") p->vortmin = atof(v);
+  else if (k == "vortmax") p->vortmax = atof(v);
+  else if (k == "jabsmin") p->jabsmin = atof(v);
+  else if (k == "jabsmax") p->jabsmax = atof(v);
   else if (k == "glm_source_terms") {
     if (is_one_of(v, {"eglm", "EGLM"})) p->glm_sources = 1;
     else if (is_one_of(v, {"heglm", "HEGLM"})) p->glm_sources = 2;
@@ -1181,6 +1204,114 @@ int amun_gpu_run(int nsteps, double dtnext, int use_graph) {
   }
   C.ms_valid = true;
   CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+// names of the primitive variables (pvars, src/equations.F90:335-722) as
+// bits of refinement_variables
+static int ref_bit(int v) {
+  const bool hd = C.p.eqsys == AMUN_EQ_HD || C.p.eqsys == AMUN_EQ_SRHD || C.p.eqsys == EQ_HD_ISO;
+  static const int hdb[5] = {AMUN_REF_DENS, AMUN_REF_VELX, AMUN_REF_VELY, AMUN_REF_VELZ, AMUN_REF_PRES};
+  static const int mhdb[9] = {AMUN_REF_DENS, AMUN_REF_VELX, AMUN_REF_VELY, AMUN_REF_VELZ, AMUN_REF_MAGX,
+                              AMUN_REF_MAGY, AMUN_REF_MAGZ, AMUN_REF_BPSI, AMUN_REF_PRES};
+  return hd ? hdb[v] : mhdb[v];
+}
+
+int amun_gpu_refinement_criterion(int* criterion, float* errors) {
+  int r = check_ready();
+  if (r) return r;
+  if (!criterion) return fail(AMUN_E_BAD_ARGUMENT, "null criterion array");
+  const int nv = C.nv, ns = nv + 2;
+  const bool mhd = C.p.eqsys == AMUN_EQ_MHD || C.p.eqsys == AMUN_EQ_SRMHD || C.p.eqsys == EQ_MHD_ISO;
+  std::vector<int> sel(nv);
+  for (int v = 0; v < nv; ++v) sel[v] = (C.p.ref_mask & ref_bit(v)) ? 1 : 0;
+  const int vort = (C.p.ref_mask & AMUN_REF_VORT) ? 1 : 0;
+  const int jabs = mhd && (C.p.ref_mask & AMUN_REF_JABS) ? 1 : 0;
+  DevBuf dsel, derr;
+  CK(cudaMalloc(&dsel.p, nv * sizeof(int)));
+  CK(cudaMalloc(&derr.p, (size_t)C.nblocks * ns * sizeof(float)));
+  CK(h2d(dsel.p, sel.data(), nv * sizeof(int)));
+  cudaError_t e = bulk() ? regrid_errors<float>(C.p.eqsys, (const float*)C.q[C.cur], C.g, C.nblocks, (const int*)dsel.p,
+                                                vort, jabs, C.p.epsref, (float*)derr.p, C.stream)
+                         : regrid_errors<double>(C.p.eqsys, (const double*)C.q[C.cur], C.g, C.nblocks,
+                                                 (const int*)dsel.p, vort, jabs, C.p.epsref, (float*)derr.p, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "refinement indicators");
+  std::vector<float> err((size_t)C.nblocks * ns);
+  CK(cudaStreamSynchronize(C.stream));
+  CK(d2h(err.data(), derr.p, err.size() * sizeof(float)));
+  // check_refinement_criterion src/refinement.F90:257-336
+  for (int b = 0; b < C.nblocks; ++b) {
+    int c = -1;
+    const float* eb = err.data() + (size_t)b * ns;
+    for (int v = 0; v < nv; ++v) {
+      if (!sel[v]) continue;
+      if ((double)eb[v] > C.p.crefmin) c = c > 0 ? c : 0;
+      if ((double)eb[v] > C.p.crefmax) c = 1;
+    }
+    if (vort) {
+      if ((double)eb[nv] > C.p.vortmin) c = c > 0 ? c : 0;
+      if ((double)eb[nv] > C.p.vortmax) c = 1;
+    }
+    if (jabs) {
+      if ((double)eb[nv + 1] > C.p.jabsmin) c = c > 0 ? c : 0;
+      if ((double)eb[nv + 1] > C.p.jabsmax) c = 1;
+    }
+    criterion[b] = c;
+  }
+  if (errors) memcpy(errors, err.data(), err.size() * sizeof(float));
+  return 0;
+}
+
+int amun_gpu_regrid(int nblocks, const amun_block_desc* blocks, const int* src) {
+  int r = check_ready();
+  if (r) return r;
+  if (nblocks <= 0 || !blocks || !src) return fail(AMUN_E_BAD_ARGUMENT, "empty block list or sources");
+  const int nch = 1 << C.p.ndims;
+  for (int b = 0; b < nblocks; ++b) {
+    const int* s = src + 9 * b;
+    const int nref = s[0] == 0 ? 1 : (s[0] == 1 ? 1 : (s[0] == 2 ? nch : -1));
+    if (nref < 0) return fail(AMUN_E_BAD_ARGUMENT, "regrid: unknown source kind");
+    for (int n = 1; n <= nref; ++n)
+      if (s[n] < 0 || s[n] >= C.nblocks) return fail(AMUN_E_BAD_ARGUMENT, "regrid: source block out of range");
+    if (s[0] == 1 && (s[2] < 0 || s[2] >= nch)) return fail(AMUN_E_BAD_ARGUMENT, "regrid: child position out of range");
+    if (s[0] == 1 && (C.p.nghosts % 2)) return fail(AMUN_E_UNSUPPORTED, "regrid: prolong_block needs an even nghosts");
+  }
+  // the old pool stays alive until its data has moved
+  double* ou0 = C.u0;
+  void* oq = C.q[C.cur];
+  C.u0 = nullptr;
+  C.q[C.cur] = nullptr;
+  auto release = [&]() {
+    if (ou0) cudaFree(ou0);
+    if (oq) cudaFree(oq);
+  };
+  r = amun_gpu_set_blocks(nblocks, blocks);
+  if (r) { release(); return r; }
+  DevBuf dsrc;
+  cudaError_t e = cudaMalloc(&dsrc.p, (size_t)nblocks * 9 * sizeof(int));
+  if (e == cudaSuccess) e = h2d(dsrc.p, src, (size_t)nblocks * 9 * sizeof(int));
+  if (e == cudaSuccess)
+    e = bulk() ? regrid_transfer<float>(C.p.eqsys, ou0, (const float*)oq, C.u0, (float*)C.q[C.cur], C.g, nblocks,
+                                        (const int*)dsrc.p, method_const(), C.sc, C.stream)
+               : regrid_transfer<double>(C.p.eqsys, ou0, (const double*)oq, C.u0, (double*)C.q[C.cur], C.g, nblocks,
+                                         (const int*)dsrc.p, method_const(), C.sc, C.stream);
+  if (e == cudaSuccess)
+    e = bulk() ? ghost_fill<float>((float*)C.q[C.cur]) : ghost_fill<double>((double*)C.q[C.cur]);
+  if (e == cudaSuccess && C.p.fix_unphysical) {
+    // update_variables ends with correct_unphysical_states
+    // (src/evolution.F90:2043-2068); the kept blocks were corrected after
+    // their last stage and have nothing to replace
+    FixConst f{C.p.ngavg, C.p.npavg, C.fix_cap, C.p.dmin, C.p.pmin};
+    e = bulk() ? Launch<float, float>::fix_unphysical(C.p.eqsys, (float*)C.q[C.cur], C.u0, true, C.g, C.nblocks,
+                                                      method_const(), f, C.fix_idx, (float*)C.fix_val, C.sc, C.stream)
+               : Launch<double, double>::fix_unphysical(C.p.eqsys, (double*)C.q[C.cur], C.u0, true, C.g, C.nblocks,
+                                                        method_const(), f, C.fix_idx, (double*)C.fix_val, C.sc,
+                                                        C.stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.stream);
+  release();
+  if (e != cudaSuccess) return cuda_fail(e, "regrid");
+  C.ms_valid = false;
   return 0;
 }
 

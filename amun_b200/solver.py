@@ -73,6 +73,41 @@ class Simulation:
             raise ValueError(f"expected block arrays of shape {shp}")
         N.check(self.L.amun_gpu_upload_conserved(0, self.mesh.nblocks, N.dptr(u0)))
 
+    # ---- mesh updates ----------------------------------------------------------
+    def refinement_criterion(self):
+        """check_refinement_criterion of every block on the device: (criterion
+        (nblocks,) int32 in {-1, 0, 1}, indicators (nblocks, nv + 2) float32)."""
+        crit = np.zeros(self.mesh.nblocks, dtype=np.int32)
+        err = np.zeros((self.mesh.nblocks, self.nv + 2), dtype=np.float32)
+        N.check(self.L.amun_gpu_refinement_criterion(crit.ctypes.data_as(C.POINTER(C.c_int)),
+                                                     err.ctypes.data_as(C.POINTER(C.c_float))))
+        return crit, err
+
+    def regrid(self, mesh, src: np.ndarray):
+        """Move the state onto a new mesh on the device: src (nblocks, 9) per
+        new block {0, old} copy, {1, parent, child position} prolong, {2,
+        children...} restrict (amun_gpu_regrid)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        if src.shape != (mesh.nblocks, 9):
+            raise ValueError(f"expected sources of shape {(mesh.nblocks, 9)}")
+        desc = mesh.descriptors()
+        N.check(self.L.amun_gpu_regrid(mesh.nblocks, desc, src.ctypes.data_as(C.POINTER(C.c_int))))
+        self.mesh = mesh
+        self._desc = desc
+
+    def update_mesh(self):
+        """One mesh update (src/mesh.F90:756-821 then update_variables): the
+        criterion on the device, the new leaves on the host, the data moved
+        on the device.  Returns the source rows (None when nothing changed)."""
+        if not hasattr(self.mesh, "update_plan"):
+            return None
+        crit, _ = self.refinement_criterion()
+        mesh, src = self.mesh.update_plan(crit)
+        if mesh.leaves == self.mesh.leaves:
+            return None
+        self.regrid(mesh, src)
+        return src
+
     def download_conserved(self, u0: np.ndarray):
         """Download conserved block arrays only (ghost cells rebuilt from Q)."""
         shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)

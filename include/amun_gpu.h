@@ -35,6 +35,10 @@ extern "C" {
 /* equation_system / equation_of_state (src/equations.F90:322-833) */
 enum { AMUN_EQ_HD = 0, AMUN_EQ_MHD = 1, AMUN_EQ_SRMHD = 2, AMUN_EQ_SRHD = 3 };
 enum { AMUN_EOS_ADI = 0, AMUN_EOS_ISO = 1 };
+/* refinement_variables names (src/refinement.F90:150-160) */
+enum { AMUN_REF_DENS = 1, AMUN_REF_VELX = 2, AMUN_REF_VELY = 4, AMUN_REF_VELZ = 8, AMUN_REF_MAGX = 16,
+       AMUN_REF_MAGY = 32, AMUN_REF_MAGZ = 64, AMUN_REF_BPSI = 128, AMUN_REF_PRES = 256, AMUN_REF_VORT = 512,
+       AMUN_REF_JABS = 1024 };
 /* primitive_solver: 1D(W), 2D(W,v^2), 2D(W,u^2) (src/equations.F90:605-640) */
 enum { AMUN_C2P_1DW = 0, AMUN_C2P_2DWV = 1, AMUN_C2P_2DWU = 2 };
 /* reconstruction (src/interpolations.F90:226-382) */
@@ -106,6 +110,10 @@ typedef struct amun_params {
   int fix_unphysical;   /* 0/1                    "fix_unphysical_cells"      */
   int ngavg, npavg;     /*                        "ngavg" (>= 1), "npavg" (>= 2) */
   double dmin;          /*                        "dmin"                      */
+  /* refinement criterion (src/refinement.F90:40-193): the names found in
+     "refinement_variables" as bits of AMUN_REF_* */
+  int ref_mask;
+  double crefmin, crefmax, epsref, vortmin, vortmax, jabsmin, jabsmax;
 } amun_params;
 
 /* One leaf block of the mesh, built from the reference's meta block
@@ -164,6 +172,26 @@ int amun_gpu_upload_blocks(int first, int count, const double* u0, const double*
  * runs on the device: Q = cons2prim(U) in the interior and the ghost fill of
  * every block.  Half the host traffic of amun_gpu_upload_blocks. */
 int amun_gpu_upload_conserved(int first, int count, const double* u0);
+
+/* check_refinement_criterion (src/refinement.F90:257-336) of every block,
+ * evaluated on the device: criterion[b] = -1 (derefine), 0 (keep), 1
+ * (refine) from the indicators of "refinement_variables" (host array of
+ * nblocks).  errors may be NULL, else it receives nv + 2 floats per block:
+ * second_derivative_error of every variable (0 when not selected), the
+ * vorticity and the current-density magnitudes. */
+int amun_gpu_refinement_criterion(int* criterion, float* errors);
+
+/* A mesh update done on the device (the data movement of
+ * refine_selected_blocks / derefine_selected_blocks, src/mesh.F90:1031-1435,
+ * 2069-2257): blocks describes the new leaf list as for amun_gpu_set_blocks
+ * and src[9 b ...] where each new block's data comes from in the current
+ * pool: {0, old} copied; {1, parent, px + 2 py + 4 pz} prolonged from the
+ * old parent (prolong_block); {2, c0, .., c(2^d - 1)} restricted from the
+ * old children in position order (restrict_block).  Afterwards the changed
+ * blocks' primitives are cons2prim of their new U and every ghost is filled
+ * (update_variables after update_mesh, src/evolution.F90:335-343).  Needs an
+ * even nghosts when a block is prolonged.  Time and step are kept. */
+int amun_gpu_regrid(int nblocks, const amun_block_desc* blocks, const int* src);
 /* Copy one block's arrays device -> host (any pointer may be NULL).  Ghost
  * cells of u0 and u1 are prim2cons of the ghost primitives
  * (update_ghost_cells, src/boundaries.F90:6633). */

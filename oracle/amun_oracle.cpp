@@ -71,6 +71,10 @@ struct Params {
   bool fix_unphysical = false;
   int ngavg = 2, npavg = 4;
   double dmin = 1.0e-16;
+  // refinement criterion (src/refinement.F90:40-193)
+  std::string refvars = "dens pres";
+  double crefmin = 0.2, crefmax = 0.8, epsref = 1.0e-2;
+  double vortmin = 1.0e-3, vortmax = 1.0e-1, jabsmin = 1.0e-3, jabsmax = 1.0e-1;
   // relativistic recovery (src/equations.F90:184-201, 313-318)
   double tol = 1.0e-10, pmin = 1.0e-16;
   int nrmax = 100, nrext = 2;
@@ -164,6 +168,14 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "ngavg") p.ngavg = atoi(v.c_str());
   else if (key == "npavg") p.npavg = atoi(v.c_str());
   else if (key == "dmin") p.dmin = atof(v.c_str());
+  else if (key == "refinement_variables") p.refvars = v;
+  else if (key == "crefmin") p.crefmin = atof(v.c_str());
+  else if (key == "crefmax") p.crefmax = atof(v.c_str());
+  else if (key == "epsref") p.epsref = atof(v.c_str());
+  else if (key == "vortmin") p.vortmin = atof(v.c_str());
+  else if (key == "vortmax") p.vortmax = atof(v.c_str());
+  else if (key == "jabsmin") p.jabsmin = atof(v.c_str());
+  else if (key == "jabsmax") p.jabsmax = atof(v.c_str());
   else if (key == "glm_source_terms") {
     if (is_one_of(v, {"eglm", "EGLM"})) p.glm_sources = 1;
     else if (is_one_of(v, {"heglm", "HEGLM"})) p.glm_sources = 2;
@@ -608,6 +620,259 @@ struct Oracle {
     }
     dx = level_dx(mlev, 0); dy = level_dx(mlev, 1); dz = level_dx(mlev, 2);
     amr = true;
+    return 0;
+  }
+
+  // =========================================================================
+  // MESH UPDATE: refinement criterion and block data movement
+  // =========================================================================
+  // names of the primitive variables (pvars, src/equations.F90:335-722);
+  // the isothermal systems drop the last one (pres)
+  const char* pvar_name(int v) const {
+    static const char* hd[5] = {"dens", "velx", "vely", "velz", "pres"};
+    static const char* mh[9] = {"dens", "velx", "vely", "velz", "magx", "magy", "magz", "bpsi", "pres"};
+    return mhd ? mh[v] : hd[v];
+  }
+
+  // second_derivative_error src/refinement.F90:359-462: real(4) differences
+  // of the real(8) primitives, the ratio formed in real(8) and stored in
+  // real(4), the maximum over the cells ibl..ieu
+  float second_derivative_error(int iqt, const Block& B) const {
+    const double eps = DBL_EPSILON;
+    auto ratio = [&](double qm, double qc, double qp) -> float {
+      const float fr = (float)(qp - qc);
+      const float fl = (float)(qm - qc);
+      const float fc = (float)(std::fabs(qp) + std::fabs(qm) + 2.0 * std::fabs(qc));
+      const double den = (double)(std::fabs(fr) + std::fabs(fl)) + p.epsref * (double)fc + eps;
+      return (float)((double)std::fabs(fr + fl) / den);
+    };
+    auto Q = [&](int i, int j, int k) { return B.q[qi(iqt, i, j, k)]; };
+    float error = 0.0f;
+    for (int k = kbl; k <= keu; ++k)
+      for (int j = jbl; j <= jeu; ++j)
+        for (int i = ibl; i <= ieu; ++i) {
+          const float fx = ratio(Q(i - 1, j, k), Q(i, j, k), Q(i + 1, j, k));
+          const float fy = ratio(Q(i, j - 1, k), Q(i, j, k), Q(i, j + 1, k));
+          error = std::max(std::max(error, fx), fy);
+          if (p.ndims == 3) error = std::max(error, ratio(Q(i, j, k - 1), Q(i, j, k), Q(i, j, k + 1)));
+        }
+    return error;
+  }
+
+  // vorticity_magnitude / current_density_magnitude src/refinement.F90:
+  // 466-590: curl (src/operators.F90:328-434) with unit spacing, its squared
+  // magnitude in real(8), the maximum in real(4), then the square root
+  float curl_magnitude(const Block& B, int ax, int ay, int az) const {
+    auto d1 = [&](int v, int d, int i, int j, int k) {
+      const int ei = d == 1, ej = d == 2, ek = d == 3;
+      return 0.5 * (B.q[qi(v, i + ei, j + ej, k + ek)] - B.q[qi(v, i - ei, j - ej, k - ek)]) / 1.0;
+    };
+    float wmax = 0.0f;
+    for (int k = kbl; k <= keu; ++k)
+      for (int j = jbl; j <= jeu; ++j)
+        for (int i = ibl; i <= ieu; ++i) {
+          double w1, w2;
+          if (p.ndims == 3) {
+            w1 = d1(az, 2, i, j, k) - d1(ay, 3, i, j, k);
+            w2 = d1(ax, 3, i, j, k) - d1(az, 1, i, j, k);
+          } else {
+            w1 = d1(az, 2, i, j, k);
+            w2 = -d1(az, 1, i, j, k);
+          }
+          const double w3 = d1(ay, 1, i, j, k) - d1(ax, 2, i, j, k);
+          wmax = std::max(wmax, (float)(w1 * w1 + w2 * w2 + w3 * w3));
+        }
+    return std::sqrt(wmax);
+  }
+
+  // check_refinement_criterion src/refinement.F90:257-336 of every block;
+  // errs (optional) receives per block the indicator of every variable (zero
+  // when not selected), the vorticity and the current density
+  void refinement_criterion(int* crit, float* errs) const {
+    const int ns = nv + 2;
+    const bool vort = p.refvars.find("vort") != std::string::npos;
+    const bool jabs = mhd && p.refvars.find("jabs") != std::string::npos;
+    for (size_t b = 0; b < blocks.size(); ++b) {
+      const Block& B = blocks[b];
+      int c = -1;
+      for (int v = 0; v < nv; ++v) {
+        float cref = 0.0f;
+        if (p.refvars.find(pvar_name(v)) != std::string::npos) {
+          cref = second_derivative_error(v + 1, B);
+          if (cref > p.crefmin) c = std::max(c, 0);
+          if (cref > p.crefmax) c = std::max(c, 1);
+        }
+        if (errs) errs[b * ns + v] = cref;
+      }
+      const float cv = vort ? curl_magnitude(B, ivx, ivy, ivz) : 0.0f;
+      const float cj = jabs ? curl_magnitude(B, ibx, iby, ibz) : 0.0f;
+      if (vort) {
+        if (cv > p.vortmin) c = std::max(c, 0);
+        if (cv > p.vortmax) c = std::max(c, 1);
+      }
+      if (jabs) {
+        if (cj > p.jabsmin) c = std::max(c, 0);
+        if (cj > p.jabsmax) c = std::max(c, 1);
+      }
+      if (errs) { errs[b * ns + nv] = cv; errs[b * ns + nv + 1] = cj; }
+      crit[b] = c;
+    }
+  }
+
+  // a block's conserved array as the reference holds it after a step: u0
+  // inside, prim2cons of the ghost primitives outside (update_ghost_cells,
+  // src/boundaries.F90:6633-6736)
+  std::vector<double> full_conserved(const Block& B) const {
+    std::vector<double> u(B.u0);
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+          const bool in_ = i >= ib && i <= ie && j >= jb && j <= je && (p.ndims == 2 || (k >= kb && k <= ke));
+          if (!in_) prim2cons(1, &B.q[qi(1, i, j, k)], &u[qi(1, i, j, k)]);
+        }
+    return u;
+  }
+
+  // prolong_block src/mesh.F90:1031-1240: the parent's cells ib-nh .. ie+nh
+  // onto a fine array of twice the size, of which the child at (px, py, pz)
+  // takes the window starting at (px in, py jn, pz kn)
+  std::vector<double> prolong_block(const Block& P, int px, int py, int pz) const {
+    const std::vector<double> up = full_conserved(P);
+    const int nh = ng / 2;
+    const int d1 = 2 * (in + ng), d2 = 2 * (jn + ng), d3 = p.ndims == 3 ? 2 * (kn + ng) : 1;
+    std::vector<double> uf((size_t)nv * d1 * d2 * d3, 0.0);
+    auto F = [&](int v, int i, int j, int k) -> double& {
+      return uf[(size_t)(v - 1) + (size_t)nv * ((size_t)(i - 1) + (size_t)d1 * ((size_t)(j - 1) + (size_t)d2 * (k - 1)))];
+    };
+    auto U = [&](int v, int i, int j, int k) { return up[qi(v, i, j, k)]; };
+    const int il = ib - nh, iu = ie + nh, jl = jb - nh, ju = je + nh;
+    const int kl = p.ndims == 3 ? kb - nh : 1, ku = p.ndims == 3 ? ke + nh : 1;
+    for (int k = kl; k <= ku; ++k) {
+      const int kc = p.ndims == 3 ? 2 * (k - kl) + 1 : 1, kp = kc + 1;
+      for (int j = jl; j <= ju; ++j) {
+        const int jc = 2 * (j - jl) + 1, jp = jc + 1;
+        for (int i = il; i <= iu; ++i) {
+          const int ic = 2 * (i - il) + 1, ip = ic + 1;
+          for (int v = 1; v <= nv; ++v) {
+            const double u0 = U(v, i, j, k);
+            double du[3] = {0.0, 0.0, 0.0};
+            du[0] = limiter(p.plim, 0.5, u0 - U(v, i - 1, j, k), U(v, i + 1, j, k) - u0);
+            du[1] = limiter(p.plim, 0.5, u0 - U(v, i, j - 1, k), U(v, i, j + 1, k) - u0);
+            if (p.ndims == 3) du[2] = limiter(p.plim, 0.5, u0 - U(v, i, j, k - 1), U(v, i, j, k + 1) - u0);
+            if (v == idn || v == ien) {
+              if (u0 > 0.0) {
+                for (;;) {
+                  double sa = std::fabs(du[0]) + std::fabs(du[1]);
+                  if (p.ndims == 3) sa = sa + std::fabs(du[2]);
+                  if (!(u0 <= sa)) break;
+                  for (double& x : du) x = 0.5 * x;
+                }
+              } else {
+                du[0] = du[1] = du[2] = 0.0;
+              }
+            }
+            for (double& x : du) x = 0.5 * x;
+            if (p.ndims == 2) {
+              const double du1 = du[0] + du[1], du2 = du[0] - du[1];
+              F(v, ic, jc, 1) = u0 - du1;
+              F(v, ip, jc, 1) = u0 + du2;
+              F(v, ic, jp, 1) = u0 - du2;
+              F(v, ip, jp, 1) = u0 + du1;
+            } else {
+              const double du1 = du[0] + du[1] + du[2], du2 = du[0] - du[1] - du[2];
+              const double du3 = du[0] - du[1] + du[2], du4 = du[0] + du[1] - du[2];
+              F(v, ic, jc, kc) = u0 - du1;
+              F(v, ip, jc, kc) = u0 + du2;
+              F(v, ic, jp, kc) = u0 - du3;
+              F(v, ip, jp, kc) = u0 + du4;
+              F(v, ic, jc, kp) = u0 - du4;
+              F(v, ip, jc, kp) = u0 + du3;
+              F(v, ic, jp, kp) = u0 - du2;
+              F(v, ip, jp, kp) = u0 + du1;
+            }
+          }
+        }
+      }
+    }
+    std::vector<double> u((size_t)nv * cells());
+    const int oi = px * in, oj = py * jn, ok = p.ndims == 3 ? pz * kn : 0;
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i)
+          for (int v = 1; v <= nv; ++v) u[qi(v, i, j, k)] = F(v, oi + i, oj + j, ok + k);
+    return u;
+  }
+
+  // restrict_block src/mesh.F90:1258-1435 for the parent's interior; ch[c]
+  // is the child at position c = px + 2 py + 4 pz
+  std::vector<double> restrict_block(const Block* const* ch) const {
+    std::vector<double> u((size_t)nv * cells(), 0.0);
+    const int hx = in / 2, hy = jn / 2, hz = kn / 2;
+    for (int k = kb; k <= ke; ++k)
+      for (int j = jb; j <= je; ++j)
+        for (int i = ib; i <= ie; ++i) {
+          const int I = i - ib, J = j - jb, K = k - kb;
+          const int cx = I / hx, cy = J / hy, cz = p.ndims == 3 ? K / hz : 0;
+          const Block& Ch = *ch[cx + 2 * cy + 4 * cz];
+          const int li = ib + 2 * (I - cx * hx), lj = jb + 2 * (J - cy * hy);
+          const int lk = p.ndims == 3 ? kb + 2 * (K - cz * hz) : 1;
+          for (int v = 1; v <= nv; ++v) {
+            auto c = [&](int a, int b2, int d) { return Ch.u0[qi(v, li + a, lj + b2, lk + d)]; };
+            double r;
+            if (p.ndims == 2)
+              r = 0.25 * ((c(0, 0, 0) + c(1, 1, 0)) + (c(0, 1, 0) + c(1, 0, 0)));
+            else
+              r = 0.125 * (((c(0, 0, 0) + c(1, 1, 1)) + (c(0, 0, 1) + c(1, 1, 0))) +
+                           ((c(0, 1, 1) + c(1, 0, 0)) + (c(0, 1, 0) + c(1, 0, 1))));
+            u[qi(v, i, j, k)] = r;
+          }
+        }
+    return u;
+  }
+
+  // the data movement of update_mesh (src/mesh.F90:756-821,
+  // derefine_selected_blocks / refine_selected_blocks 2069-2257) onto the
+  // leaves (levels, coords); src holds 9 ints per new block: {0, old} kept,
+  // {1, parent, px + 2 py + 4 pz} prolonged, {2, children by position}
+  // restricted.  Then update_variables (src/evolution.F90:337-343): the
+  // primitives of the new blocks and the ghost cells of all.
+  int regrid(int n, const int* levels, const int* coords, const int* src) {
+    const int nch = 1 << p.ndims;
+    for (int b = 0; b < n; ++b) {
+      const int* s = src + 9 * b;
+      const int nref = s[0] == 2 ? nch : 1;
+      if (s[0] < 0 || s[0] > 2) return 1;
+      for (int c = 1; c <= nref; ++c)
+        if (s[c] < 0 || s[c] >= (int)blocks.size()) return 1;
+    }
+    std::vector<Block> old = std::move(blocks);
+    std::vector<std::vector<double>> nu((size_t)n);
+    for (int b = 0; b < n; ++b) {
+      const int* s = src + 9 * b;
+      if (s[0] == 1) {
+        nu[b] = prolong_block(old[s[1]], s[2] & 1, (s[2] >> 1) & 1, (s[2] >> 2) & 1);
+      } else if (s[0] == 2) {
+        const Block* ch[8];
+        for (int c = 0; c < nch; ++c) ch[c] = &old[s[1 + c]];
+        nu[b] = restrict_block(ch);
+      }
+    }
+    set_mesh(n, levels, coords);
+    for (int b = 0; b < n; ++b) {
+      const int* s = src + 9 * b;
+      Block& B = blocks[b];
+      if (s[0] == 0) {
+        B.u0 = old[s[1]].u0;
+        B.q = old[s[1]].q;
+      } else {
+        B.u0 = std::move(nu[b]);
+        update_primitive_variables(B.u0.data(), B.q.data());
+      }
+      B.u = B.u0.data();
+    }
+    boundary_variables();
+    if (p.fix_unphysical)
+      for (auto& B : blocks) unphysical_cells += correct_unphysical_states(B);
     return 0;
   }
 
@@ -3777,6 +4042,12 @@ void* or_create(int nkeys, const char** keys, const char** values, int* iret) {
   return o;
 }
 void or_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void or_refinement_criterion(void* h, int* crit, float* errs) {
+  static_cast<Oracle*>(h)->refinement_criterion(crit, errs);
+}
+int or_regrid(void* h, int n, const int* levels, const int* coords, const int* src) {
+  return static_cast<Oracle*>(h)->regrid(n, levels, coords, src);
+}
 void or_set_threads(void* h, int n) { static_cast<Oracle*>(h)->nthreads = n < 1 ? 1 : n; }
 
 int or_nv(void* h) { return static_cast<Oracle*>(h)->nv; }

@@ -54,6 +54,10 @@ def lib():
         L.or_set_mesh.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.or_set_mesh.restype = i
         L.or_set_blocks_prim.argtypes = [vp, d]
+        L.or_refinement_criterion.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+        L.or_refinement_criterion.restype = None
+        L.or_regrid.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.or_regrid.restype = i
         L.or_new_time_step.argtypes = [vp, C.c_double, d, d]
         L.or_advance.argtypes = [vp, C.c_double, d, d]
         L.or_scalars.argtypes = [vp, d]
@@ -97,6 +101,7 @@ class Oracle:
         self.im, self.jm, self.km = dims[0], dims[1], dims[2]
         self.shape = (dims[3], dims[4], dims[5])  # NX, NY, NZ
         self.nblocks = (dims[6], dims[7], dims[8])
+        self.mesh_blocks = dims[6] * dims[7] * dims[8]
         sp = (C.c_double * 5)()
         L.or_spacing(self.h, sp)
         self.dx, self.dy, self.dz, self.cfl, self.decay = list(sp)
@@ -204,6 +209,31 @@ class Oracle:
                                co.ctypes.data_as(C.POINTER(C.c_int)))
         if r != 0:
             raise RuntimeError(f"or_set_mesh returned {r}")
+
+    def refinement_criterion(self):
+        """check_refinement_criterion of every block: (criterion (n,) int32,
+        indicators (n, nv + 2) float32: variables, vorticity, current)."""
+        n = self.mesh_blocks
+        crit = np.zeros(n, dtype=np.int32)
+        err = np.zeros((n, self.nv + 2), dtype=np.float32)
+        self.L.or_refinement_criterion(self.h, crit.ctypes.data_as(C.POINTER(C.c_int)),
+                                       err.ctypes.data_as(C.POINTER(C.c_float)))
+        return crit, err
+
+    def regrid(self, levels, coords, src):
+        """Move the state onto the leaves (levels, coords): src (n, 9) per
+        new block {0, old} kept, {1, parent, child position} prolonged, {2,
+        children by position} restricted; primitives and ghosts rebuilt."""
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        co = np.ascontiguousarray(coords, dtype=np.int32).reshape(-1, 3)
+        sr = np.ascontiguousarray(src, dtype=np.int32).reshape(-1, 9)
+        if len(sr) != len(lv):
+            raise ValueError("one source row per new block")
+        r = self.L.or_regrid(self.h, len(lv), lv.ctypes.data_as(C.POINTER(C.c_int)),
+                             co.ctypes.data_as(C.POINTER(C.c_int)), sr.ctypes.data_as(C.POINTER(C.c_int)))
+        if r != 0:
+            raise RuntimeError(f"or_regrid returned {r}")
+        self.mesh_blocks = len(lv)
 
     def set_blocks_prim(self, qb: np.ndarray):
         """Primitive state of every block, (nblocks, km, jm, im, nv) with

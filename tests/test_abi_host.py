@@ -61,6 +61,9 @@ def test_default_params_match_reference_defaults():
     ("problem", "rayleigh-taylor", "gravity", 1), ("problem", "blast", "gravity", 0), ("gacc", "-2", "gacc", -2.0),
     ("fix_unphysical_cells", "Y", "fix_unphysical", 1), ("ngavg", "3", "ngavg", 3), ("npavg", "6", "npavg", 6),
     ("dmin", "1e-10", "dmin", 1e-10),
+    ("refinement_variables", "dens pres", "ref_mask", N.AMUN_REF_DENS | N.AMUN_REF_PRES),
+    ("refinement_variables", "vort jabs magx", "ref_mask", N.AMUN_REF_VORT | N.AMUN_REF_JABS | N.AMUN_REF_MAGX),
+    ("crefmin", "0.3", "crefmin", 0.3), ("epsref", "0.05", "epsref", 0.05), ("jabsmax", "2", "jabsmax", 2.0),
 ])
 def test_set_param_aliases(key, val, field, expect):
     L = N.lib()
@@ -90,6 +93,10 @@ def test_no_device_fails_loudly():
     assert rc == 903
     assert b"no CUDA device" in L.amun_gpu_last_error()
     assert L.amun_gpu_advance(0.1, None, None) != 0
+    crit = (C.c_int * 4)()
+    assert L.amun_gpu_refinement_criterion(crit, None) == N.AMUN_E_NOT_INITIALIZED
+    src = (C.c_int * 9)()
+    assert L.amun_gpu_regrid(1, None, src) == N.AMUN_E_NOT_INITIALIZED
 
 
 def test_parameter_text():
