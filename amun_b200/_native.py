@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libamun_gpu.so")
 
 AMUN_EQ_HD, AMUN_EQ_MHD, AMUN_EQ_SRMHD, AMUN_EQ_SRHD = 0, 1, 2, 3
 AMUN_EOS_ADI, AMUN_EOS_ISO = 0, 1
-AMUN_REC_TVD, AMUN_REC_WENO5Z = 0, 1
+AMUN_REC_TVD, AMUN_REC_WENO5Z, AMUN_REC_GP = 0, 1, 9
 AMUN_FP64, AMUN_FP32_BULK = 0, 1
 # library errors (include/amun_gpu.h)
 AMUN_E_NOT_INITIALIZED, AMUN_E_BAD_ARGUMENT, AMUN_E_CUDA, AMUN_E_UNSUPPORTED, AMUN_E_NO_BLOCKS = 901, 902, 903, 904, 905
@@ -45,7 +45,7 @@ class amun_params(C.Structure):
         ("gacc", C.c_double), ("fix_unphysical", C.c_int), ("ngavg", C.c_int), ("npavg", C.c_int),
         ("dmin", C.c_double), ("ref_mask", C.c_int), ("crefmin", C.c_double), ("crefmax", C.c_double),
         ("epsref", C.c_double), ("vortmin", C.c_double), ("vortmax", C.c_double), ("jabsmin", C.c_double),
-        ("jabsmax", C.c_double),
+        ("jabsmax", C.c_double), ("ngp", C.c_int), ("sgp", C.c_double),
     ]
 
 

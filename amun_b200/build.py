@@ -6,6 +6,8 @@ Translation units:
   kernels_fp64*.cu       FP64 sweep and auxiliary kernels
   kernels_fp32*.cu       FP32-bulk sweep and auxiliary kernels
 
+gp_weights.cpp is host C++ (quadruple precision through libquadmath).
+
 Every FP64 unit is compiled with -fmad=false so no multiply-add is fused
 and the arithmetic follows the reference operation by operation.
 
@@ -41,6 +43,7 @@ FP32_SWEEP = FP32 + ["-DAMUN_SWEEP_MIN_BLOCKS=4"]
 
 UNITS = {
     "amun_gpu.cu": FP64,
+    "gp_weights.cpp": [],
     "unit_fp64.cu": FP64,
     "adjoint.cu": FP64,
     "kernels_fp64.cu": FP64,
@@ -87,7 +90,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     cc = nvcc()
 
     def compile_one(src):
-        obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+        obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
         srcp = os.path.join(CSRC, src)
         cmd = [cc, *ARCH, *COMMON, *UNITS[src], "-c", srcp, "-o", obj]
         stamp = obj + ".cmd"  # the command that built obj: a flag change rebuilds it
@@ -111,7 +114,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
     objs = [o for o, _ in results]
     if force or _sources_newer(LIB, objs):
-        cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs]
+        cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs, "-lquadmath"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -17,6 +17,7 @@
 
 #include "../../include/amun_gpu.h"
 #include "adjoint.h"
+#include "gp_weights.h"
 #include "launch.cuh"
 #include "regrid.h"
 #include "unit.h"
@@ -39,6 +40,7 @@ struct Ctx {
   Geo g{};
   std::vector<amun_block_desc> blocks;
   double dx_min = 1.0;
+  double cgp[7] = {0, 0, 0, 0, 0, 0, 0};  // Gaussian-process weights (prepare_gp)
   // device pool
   void* q[2] = {nullptr, nullptr};
   double* u0 = nullptr;
@@ -349,6 +351,8 @@ MethodConst method_const() {
   m.mlp = C.p.mlp;
   m.rec = C.p.reconstruction;
   m.rc.rad = C.p.limo3_rad; m.rc.ppm = C.p.ppm_const; m.rc.kappa = C.p.kappa; m.rc.kbeta = C.p.kbeta;
+  m.rc.ngp = C.p.ngp;
+  for (int k = 0; k < 7; ++k) m.rc.cgp[k] = C.cgp[k];
   m.gravity = C.p.gravity;
   m.gacc[0] = 0.0; m.gacc[1] = C.p.gacc; m.gacc[2] = 0.0;  // gacc_rayleigh_taylor (src/gravity.F90:283-330)
   m.visc = C.p.viscosity;
@@ -504,6 +508,8 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.gamma = C.gamma; u.eps = C.p.eps; u.cmax = C.host_cmax; u.csnd = C.p.csnd; u.c2p = C.p.c2p; u.mlp = C.p.mlp;
   u.h[0] = u.h[1] = u.h[2] = 0.0;
   u.rad = C.p.limo3_rad; u.ppm = C.p.ppm_const; u.kappa = C.p.kappa; u.kbeta = C.p.kbeta;
+  u.ngp = C.p.ngp;
+  for (int k = 0; k < 7; ++k) u.cgp[k] = C.cgp[k];
   return u;
 }
 
@@ -580,6 +586,8 @@ void amun_gpu_default_params(amun_params* p) {
   p->vortmax = 1.0e-1;
   p->jabsmin = 1.0e-3;
   p->jabsmax = 1.0e-1;
+  p->ngp = 5;
+  p->sgp = 9.0;
 }
 
 int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
@@ -622,9 +630,10 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"weno5ns", "weno5-ns", "WENO5NS", "WENO5-NS"})) p->reconstruction = AMUN_REC_WENO5NS;
     else if (is_one_of(v, {"mp5", "MP5"})) p->reconstruction = AMUN_REC_MP5;
     else if (is_one_of(v, {"mp7", "MP7"})) p->reconstruction = AMUN_REC_MP7;
+    else if (is_one_of(v, {"gp", "GP"})) p->reconstruction = AMUN_REC_GP;
     else if (is_one_of(v, {"crweno5z", "crweno5-z", "CRWENO5Z", "CRWENO5-Z", "crweno5yc", "crweno5-yc", "CRWENO5YC",
                            "CRWENO5-YC", "crweno5ns", "crweno5-ns", "CRWENO5NS", "CRWENO5-NS", "crmp5", "CRMP5",
-                           "crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD", "crmp7", "CRMP7", "gp", "GP", "mgp", "MGP"}))
+                           "crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD", "crmp7", "CRMP7", "mgp", "MGP"}))
       return fail(AMUN_E_UNSUPPORTED, std::string("reconstruction not implemented here: ") + v);
     else return fail(200, std::string("reconstruction not implemented: ") + v);
   } else if (k == "limiter" || k == "extrema_limiter" || k == "prolongation_limiter") {
@@ -680,6 +689,8 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
   else if (k == "vortmax") p->vortmax = atof(v);
   else if (k == "jabsmin") p->jabsmin = atof(v);
   else if (k == "jabsmax") p->jabsmax = atof(v);
+  else if (k == "ngp") p->ngp = atoi(v);
+  else if (k == "sgp") p->sgp = atof(v);
   else if (k == "glm_source_terms") {
     if (is_one_of(v, {"eglm", "EGLM"})) p->glm_sources = 1;
     else if (is_one_of(v, {"heglm", "HEGLM"})) p->glm_sources = 2;
@@ -714,11 +725,17 @@ int amun_gpu_init(const amun_params* p) {
   if ((p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD) &&
       (p->c2p < AMUN_C2P_1DW || p->c2p > AMUN_C2P_2DWU))
     return fail(110, "primitive solver not implemented");
-  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_MP7)
+  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_GP)
     return fail(200, "reconstruction not implemented");
-  // the stencil reach of each method beyond its cell, plus the cell itself
-  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4};
+  // the stencil reach of each method beyond its cell, plus the cell itself;
+  // GP reaches (ngp - 1) / 2 cells and its mp_limiting two
+  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4, 3};
   int need = kNeed[p->reconstruction];
+  if (p->reconstruction == AMUN_REC_GP) {
+    if (p->ngp < 1 || p->ngp > 7 || p->ngp % 2 == 0)
+      return fail(AMUN_E_UNSUPPORTED, "gp: ngp must be odd and at most 7 (a 7-cell stencil)");
+    need = std::max(p->ngp / 2, 2) + 1;
+  }
   if (p->nghosts < need || p->ncells < p->nghosts)
     return fail(AMUN_E_BAD_ARGUMENT, "nghosts too small for the reconstruction stencil (or ncells < nghosts)");
   int ndev = 0;
@@ -733,6 +750,11 @@ int amun_gpu_init(const amun_params* p) {
   // src/equations.F90:923-924
   if (C.p.ngavg < 1) C.p.ngavg = 1;
   if (C.p.npavg < 2) C.p.npavg = 2;
+  for (int k = 0; k < 7; ++k) C.cgp[k] = 0.0;
+  if (p->reconstruction == AMUN_REC_GP && gp_weights(p->ngp, p->sgp, C.cgp) != 0) {
+    C.inited = false;
+    return fail(202, "gp: the covariance matrix could not be inverted");
+  }
   // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
   if (C.p.reconstruction == AMUN_REC_LIMO3) C.p.eps = C.p.eps > 1.0e-12 ? C.p.eps : 1.0e-12;
   C.nv = (p->eqsys == AMUN_EQ_HD || p->eqsys == AMUN_EQ_SRHD) ? 5 : 9;

@@ -9,12 +9,16 @@
 namespace amun {
 
 // reconstruction methods (src/interpolations.F90:226-382)
-enum { REC_WENO3 = 2, REC_LIMO3 = 3, REC_PPM = 4, REC_WENO5YC = 5, REC_WENO5NS = 6, REC_MP5 = 7, REC_MP7 = 8 };
+enum { REC_WENO3 = 2, REC_LIMO3 = 3, REC_PPM = 4, REC_WENO5YC = 5, REC_WENO5NS = 6, REC_MP5 = 7, REC_MP7 = 8,
+       REC_GP = 9 };
 
 // the method constants beyond eps: limo3_rad, ppm_const, kappa, kbeta
-// (src/interpolations.F90:80-106, 209-212)
+// (src/interpolations.F90:80-106, 209-212), and the Gaussian-process
+// stencil size ngp (odd, at most 7) with its weights (prepare_gp, 4438-4557)
 struct RecConst {
   double rad, ppm, kappa, kbeta;
+  int ngp;
+  double cgp[7];
 };
 
 // reconstruct_weno3 src/interpolations.F90:1469-1574, main loop
@@ -293,6 +297,40 @@ __device__ __forceinline__ void mp_faces(const R* s, R kappa, R kbeta, R eps, R&
   }
 }
 
+// reconstruct_gp src/interpolations.F90:4561-4680, main loop: the weighted
+// sum of the differences to the cell over ngp cells, then mp_limiting
+template <int NGP, typename R>
+__device__ __forceinline__ R gp_value(const R* g, const double* cgp) {
+  constexpr int M = NGP / 2;
+  R u = R(0);
+#pragma unroll
+  for (int k = 0; k < NGP; ++k) u = u + R(cgp[k]) * (g[3 - M + k] - g[3]);
+  return u + g[3];
+}
+
+template <typename R>
+__device__ __forceinline__ void gp_faces(const R* s, const RecConst& rc, R eps, R& fR, R& fL) {
+  R g[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) g[k] = s[k];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    if (side == 1) {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) g[k] = s[6 - k];
+    }
+    R u;
+    switch (rc.ngp) {
+      case 1: u = gp_value<1>(g, rc.cgp); break;
+      case 3: u = gp_value<3>(g, rc.cgp); break;
+      case 5: u = gp_value<5>(g, rc.cgp); break;
+      default: u = gp_value<7>(g, rc.cgp); break;
+    }
+    u = mp_limit(g + 1, u, R(rc.kappa), R(rc.kbeta), eps);
+    if (side == 0) fR = u; else fL = u;
+  }
+}
+
 // the explicit reconstructions by method (main-loop form)
 template <typename R>
 __device__ __forceinline__ void dir_faces(int rec, const R* s, R h, R eps, const RecConst& rc, R& fR, R& fL) {
@@ -303,6 +341,7 @@ __device__ __forceinline__ void dir_faces(int rec, const R* s, R h, R eps, const
     case REC_WENO5YC: weno5_variant_faces<false>(s, eps, fR, fL); break;
     case REC_WENO5NS: weno5_variant_faces<true>(s, eps, fR, fL); break;
     case REC_MP5: mp_faces<5>(s, R(rc.kappa), R(rc.kbeta), eps, fR, fL); break;
+    case REC_GP: gp_faces(s, rc, eps, fR, fL); break;
     default: mp_faces<7>(s, R(rc.kappa), R(rc.kbeta), eps, fR, fL); break;
   }
 }

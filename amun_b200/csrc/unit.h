@@ -14,6 +14,8 @@ struct UnitArgs {
   int nrmax, nrext, states_4vec, c2p, mlp;
   double h[3];                      // dx, dy, dz of the block
   double rad, ppm, kappa, kbeta;    // reconstruction constants
+  int ngp;                          // Gaussian-process stencil and weights
+  double cgp[7];
 };
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,

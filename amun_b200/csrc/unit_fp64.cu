@@ -258,6 +258,37 @@ __device__ void line_mp(int order, int n, const double* fc, int dir, double* u, 
                               eps);
 }
 
+// reconstruct_gp src/interpolations.F90:4561-4680, one direction of a line:
+// the line ends by the ce2/ce3/ce5 stencils, the Gaussian-process value
+// over i = 1 + mgp .. n - mgp, then mp_limiting
+__device__ void line_gp(int n, const double* fc, int dir, double* u, const RecConst& rc, double eps) {
+  auto F = [&](int i) { return dir > 0 ? fc[i] : fc[n - 1 - i]; };
+  const double ce2[2] = {0.5, 0.5};
+  const double ce3[3] = {-1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0};
+  const double ce5[5] = {2.0 / 60.0, -13.0 / 60.0, 47.0 / 60.0, 27.0 / 60.0, -3.0 / 60.0};
+  auto sum = [&](const double* c, int m, int i0) {
+    double s = 0.0;
+    for (int k = 0; k < m; ++k) s = s + c[k] * F(i0 + k);
+    return s;
+  };
+  const int mgp = rc.ngp / 2;
+  u[0] = sum(ce2, 2, 0);
+  u[1] = sum(ce3, 3, 0);
+  for (int i = 2; i <= mgp - 1; ++i) u[i] = sum(ce5, 5, i - 2);
+  for (int i = n - mgp; i <= n - 3; ++i) u[i] = sum(ce5, 5, i - 2);
+  u[n - 2] = sum(ce3, 3, n - 3);
+  u[n - 1] = F(n - 1);
+  for (int i = mgp; i <= n - 1 - mgp; ++i) {
+    double s = 0.0;
+    for (int k = 0; k < rc.ngp; ++k) s = s + rc.cgp[k] * (F(i - mgp + k) - F(i));
+    u[i] = s + F(i);
+  }
+  auto dm = [&](int k) { return (k >= 2 && k <= n) ? F(k - 1) - F(k - 2) : 0.0; };
+  for (int i1 = 1; i1 <= n - 1; ++i1)
+    u[i1 - 1] = mp_limit_core(dm(i1 - 1), dm(i1), dm(i1 + 1), dm(i1 + 2), F(i1 - 1), F(i1), u[i1 - 1], rc.kappa,
+                              rc.kbeta, eps);
+}
+
 // ---- interfaces_dir + reconstruct (src/interpolations.F90:867-959,
 // 1343-1381): one thread per (variable, line); the line is reconstructed
 // by the chosen method including its line ends (reconstruct_weno5z
@@ -319,6 +350,11 @@ __global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int
       line_ends_average(n, f, fl, fr);
     } else if (rec == REC_PPM) {
       line_ppm(n, f, fl, fr, w1, w2, rc.ppm);
+    } else if (rec == REC_GP) {
+      line_gp(n, f, +1, fl, rc, eps);
+      line_gp(n, f, -1, w1, rc, eps);
+      for (int k = 0; k <= n - 2; ++k) fr[k] = w1[n - 2 - k];
+      line_ends_average(n, f, fl, fr);
     } else {
       const int order = rec == REC_MP5 ? 5 : 7;
       line_mp(order, n, f, +1, fl, rc.kappa, rc.kbeta, eps);
@@ -497,7 +533,9 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
     for (int dir = 0; dir < u.ndims; ++dir) {
       const int ni = u.im - 2 * u.ng + 2, nj = u.jm - 2 * u.ng + 2, nk = u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1;
       long long lines = (dir == 0 ? (long long)nj * nk : (dir == 1 ? (long long)ni * nk : (long long)ni * nj)) * NV;
-      const RecConst rc{u.rad, u.ppm, u.kappa, u.kbeta};
+      RecConst rc{u.rad, u.ppm, u.kappa, u.kbeta};
+      rc.ngp = u.ngp;
+      for (int k = 0; k < 7; ++k) rc.cgp[k] = u.cgp[k];
       dir_lines<EQ><<<(int)((lines + 127) / 128), 128, 0, s>>>(qr, qs, d, dir, u.rec, u.h[dir], rc, u.lim, u.clim,
                                                                u.eps, u.clip, u.positivity, scratch);
     }

@@ -29,6 +29,7 @@
 #include <thread>
 #include <algorithm>
 #include <atomic>
+#include <quadmath.h>
 #include <stdexcept>
 #include <unordered_map>
 
@@ -40,7 +41,7 @@ namespace {
 // src/coordinates.F90:160-357).  Defaults are the reference defaults.
 // ---------------------------------------------------------------------------
 enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3 };
-enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7 };
+enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7, REC_GP };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
 enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM, RS_HLLCM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
@@ -82,6 +83,8 @@ struct Params {
   int c2p = 0;  // primitive_solver: 0 1D(W), 1 2D(W,v^2), 2 2D(W,u^2), -1 unknown
   // reconstruction constants (src/interpolations.F90:80-106, 209-212)
   double rad = 0.5, ppm_const = 1.25, kappa = 1.0, kbeta = 1.0;
+  int ngp = 5;          // Gaussian process (src/interpolations.F90:96-102)
+  double sgp = 9.0;
 };
 
 bool is_one_of(const std::string& s, std::initializer_list<const char*> l) {
@@ -131,6 +134,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"weno5ns", "weno5-ns", "WENO5NS", "WENO5-NS"})) p.rec = REC_WENO5NS;
     else if (is_one_of(v, {"mp5", "MP5"})) p.rec = REC_MP5;
     else if (is_one_of(v, {"mp7", "MP7"})) p.rec = REC_MP7;
+    else if (is_one_of(v, {"gp", "GP"})) p.rec = REC_GP;
     else return 200;  // src/interpolations.F90:382
   } else if (key == "limiter" || key == "extrema_limiter" || key == "prolongation_limiter") {
     int l = LIM_ZERO;
@@ -168,6 +172,8 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
   else if (key == "ngavg") p.ngavg = atoi(v.c_str());
   else if (key == "npavg") p.npavg = atoi(v.c_str());
   else if (key == "dmin") p.dmin = atof(v.c_str());
+  else if (key == "ngp") p.ngp = atoi(v.c_str());
+  else if (key == "sgp") p.sgp = atof(v.c_str());
   else if (key == "refinement_variables") p.refvars = v;
   else if (key == "crefmin") p.crefmin = atof(v.c_str());
   else if (key == "crefmax") p.crefmax = atof(v.c_str());
@@ -553,6 +559,10 @@ struct Oracle {
     csnd = p.csnd; csnd2 = csnd * csnd;
     // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
     if (p.rec == REC_LIMO3) p.eps = fmax2(1.0e-12, p.eps);
+    if (p.rec == REC_GP) {
+      if (p.ngp < 1 || p.ngp % 2 == 0) return 904;
+      if (prepare_gp()) return 202;
+    }
     if (sr && p.c2p < 0) return 110;
     p.ngavg = std::max(1, p.ngavg);
     p.npavg = std::max(2, p.npavg);
@@ -2478,6 +2488,109 @@ struct Oracle {
     frv[n - 1] = fc[n - 1];
   }
 
+
+  // prepare_gp src/interpolations.F90:4438-4557 in quadruple precision
+  // (max_real_kind, src/algebra.F90:42) with libquadmath; invert is
+  // src/algebra.F90:1198-1305 (Gauss-Jordan on [cov | I], no pivoting)
+  std::vector<double> cgp;
+  int prepare_gp() {
+    typedef __float128 Q;
+    const int n = p.ngp, mgp = (n - 1) / 2, w = 2 * n;
+    const double pi = 3.14159265358979323846264338327950;
+    const Q sig = (Q)(std::sqrt(2.0) * p.sgp);
+    const Q fc = (Q)(0.5 * std::sqrt(pi)) * sig;
+    std::vector<Q> g((size_t)n * w, (Q)0);
+    auto G = [&](int i, int j) -> Q& { return g[(size_t)(i - 1) * w + (j - 1)]; };
+    for (int i = 1; i <= n; ++i) {
+      for (int j = 1; j <= n; ++j) {
+        const int ip = i - 1 - mgp, jp = j - 1 - mgp;
+        const Q zl = (Q)(1.0 * (ip - jp) - 0.5) / sig;
+        const Q zr = (Q)(1.0 * (ip - jp) + 0.5) / sig;
+        G(i, j) = fc * (erfq(zr) - erfq(zl));
+      }
+      G(i, i + n) = 1;
+    }
+    for (int k = 1; k <= n - 1; ++k) {
+      if (G(k, k) == 0) {
+        if (G(k + 1, k) == 0) return 1;
+        for (int j = 1; j <= w; ++j) G(k, j) = G(k, j) + G(k + 1, j);
+      }
+      for (int j = k + 1; j <= n; ++j) {
+        const Q t = G(j, k) / G(k, k);
+        for (int i = k; i <= w; ++i) G(j, i) = G(j, i) - t * G(k, i);
+      }
+    }
+    for (int i = 1; i <= n; ++i)
+      if (G(i, i) == 0) return 1;
+    for (int i = 1; i <= n; ++i) {
+      const Q t = G(i, i);
+      for (int j = i; j <= w; ++j) G(i, j) = G(i, j) / t;
+    }
+    for (int k = n - 1; k >= 1; --k)
+      for (int i = 1; i <= k; ++i) {
+        const Q t = G(i, k + 1);
+        for (int j = k; j <= w; ++j) G(i, j) = G(i, j) - G(k + 1, j) * t;
+      }
+    auto A = [&](int i, int j) -> Q& { return G(i, j + n); };
+    for (int j = 1; j <= n; ++j)
+      for (int i = 1; i <= n; ++i)
+        if (i != j) {
+          const Q f = (Q)0.5 * (A(i, j) + A(j, i));
+          A(i, j) = f;
+          A(j, i) = f;
+        }
+    cgp.assign(n, 0.0);
+    std::vector<Q> xgp(n);
+    for (int j = 1; j <= n; ++j) {
+      const Q zr = (Q)(0.5 - 1.0 * (j - 1 - mgp)) / sig;
+      xgp[j - 1] = expq(-(zr * zr));
+    }
+    for (int j = 1; j <= n; ++j) {
+      Q s = 0;
+      for (int k = 1; k <= n; ++k) s = s + xgp[k - 1] * A(k, j);
+      cgp[j - 1] = (double)s;
+    }
+    return 0;
+  }
+
+  // reconstruct_gp src/interpolations.F90:4561-4680
+  void reconstruct_gp(int n, const double* fc, double* flv, double* frv) const {
+    static const double ce2[2] = {0.5, 0.5};
+    static const double ce3[3] = {-1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0};
+    static const double ce5[5] = {2.0 / 60.0, -13.0 / 60.0, 47.0 / 60.0, 27.0 / 60.0, -3.0 / 60.0};
+    const int ngp = p.ngp, mgp = (ngp - 1) / 2;
+    std::vector<double> u(n), fi(n);
+    auto pass = [&](const double* g) {
+      auto sum = [&](const double* c, int m, int i0) {  // i0 1-based
+        double s = 0.0;
+        for (int k = 0; k < m; ++k) s = s + c[k] * g[i0 - 1 + k];
+        return s;
+      };
+      u[0] = sum(ce2, 2, 1);
+      u[1] = sum(ce3, 3, 1);
+      for (int i = 3; i <= mgp; ++i) u[i - 1] = sum(ce5, 5, i - 2);
+      for (int i = n + 1 - mgp; i <= n - 2; ++i) u[i - 1] = sum(ce5, 5, i - 2);
+      u[n - 2] = sum(ce3, 3, n - 2);
+      u[n - 1] = g[n - 1];
+      for (int i = 1 + mgp; i <= n - mgp; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < ngp; ++k) s = s + cgp[k] * (g[i - mgp - 1 + k] - g[i - 1]);
+        u[i - 1] = s + g[i - 1];
+      }
+      mp_limiting(n, g, u.data());
+    };
+    pass(fc);
+    for (int i = 0; i < n; ++i) flv[i] = u[i];
+    for (int i = 0; i < n; ++i) fi[i] = fc[n - 1 - i];
+    pass(fi.data());
+    for (int k = 1; k <= n - 1; ++k) frv[k - 1] = u[n - 1 - k];
+    int i = n - 1;
+    flv[0] = 0.5 * (fc[0] + fc[1]);
+    frv[i - 1] = 0.5 * (fc[i - 1] + fc[n - 1]);
+    flv[n - 1] = fc[n - 1];
+    frv[n - 1] = fc[n - 1];
+  }
+
   // reconstruct src/interpolations.F90:1343-1381
   void reconstruct(int n, const double* f, double* fl, double* fr, double h = 0.0) const {
     switch (p.rec) {
@@ -2489,6 +2602,7 @@ struct Oracle {
       case REC_WENO5NS: reconstruct_weno5v(true, n, f, fl, fr); break;
       case REC_MP5: reconstruct_mp(5, n, f, fl, fr); break;
       case REC_MP7: reconstruct_mp(7, n, f, fl, fr); break;
+      case REC_GP: reconstruct_gp(n, f, fl, fr); break;
       default: reconstruct_tvd(n, f, fl, fr); break;
     }
     if (p.clip) clip_extrema(n, f, fl, fr);
@@ -4042,6 +4156,11 @@ void* or_create(int nkeys, const char** keys, const char** values, int* iret) {
   return o;
 }
 void or_destroy(void* h) { delete static_cast<Oracle*>(h); }
+int or_gp_weights(void* h, double* out) {
+  const Oracle* o = static_cast<Oracle*>(h);
+  for (size_t k = 0; k < o->cgp.size(); ++k) out[k] = o->cgp[k];
+  return (int)o->cgp.size();
+}
 void or_refinement_criterion(void* h, int* crit, float* errs) {
   static_cast<Oracle*>(h)->refinement_criterion(crit, errs);
 }

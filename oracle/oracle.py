@@ -54,6 +54,8 @@ def lib():
         L.or_set_mesh.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.or_set_mesh.restype = i
         L.or_set_blocks_prim.argtypes = [vp, d]
+        L.or_gp_weights.argtypes = [vp, d]
+        L.or_gp_weights.restype = i
         L.or_refinement_criterion.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]
         L.or_refinement_criterion.restype = None
         L.or_regrid.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -209,6 +211,13 @@ class Oracle:
                                co.ctypes.data_as(C.POINTER(C.c_int)))
         if r != 0:
             raise RuntimeError(f"or_set_mesh returned {r}")
+
+    def gp_weights(self):
+        """The Gaussian-process weights cgp of prepare_gp (empty unless
+        reconstruction = gp)."""
+        out = np.zeros(16)
+        n = self.L.or_gp_weights(self.h, _p(out))
+        return out[:n].copy()
 
     def refinement_criterion(self):
         """check_refinement_criterion of every block: (criterion (n,) int32,

@@ -63,6 +63,7 @@ def test_default_params_match_reference_defaults():
     ("dmin", "1e-10", "dmin", 1e-10),
     ("refinement_variables", "dens pres", "ref_mask", N.AMUN_REF_DENS | N.AMUN_REF_PRES),
     ("refinement_variables", "vort jabs magx", "ref_mask", N.AMUN_REF_VORT | N.AMUN_REF_JABS | N.AMUN_REF_MAGX),
+    ("reconstruction", "GP", "reconstruction", N.AMUN_REC_GP), ("ngp", "7", "ngp", 7), ("sgp", "2.5", "sgp", 2.5),
     ("crefmin", "0.3", "crefmin", 0.3), ("epsref", "0.05", "epsref", 0.05), ("jabsmax", "2", "jabsmax", 2.0),
 ])
 def test_set_param_aliases(key, val, field, expect):
@@ -74,7 +75,7 @@ def test_set_param_aliases(key, val, field, expect):
 
 
 @pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "polytropic", 110),
-                                          ("reconstruction", "crweno5z", 904), ("reconstruction", "gp", 904),
+                                          ("reconstruction", "crweno5z", 904), ("reconstruction", "mgp", 904),
                                           ("reconstruction", "nope", 200)])
 def test_set_param_reference_error_codes(key, val, code):
     L = N.lib()
@@ -93,6 +94,9 @@ def test_no_device_fails_loudly():
     assert rc == 903
     assert b"no CUDA device" in L.amun_gpu_last_error()
     assert L.amun_gpu_advance(0.1, None, None) != 0
+    # a Gaussian-process stencil beyond the sweep's seven cells is refused first
+    pg = to_native({"reconstruction": "gp", "ngp": 9, "nghosts": 4})
+    assert L.amun_gpu_init(C.byref(pg)) == 904
     crit = (C.c_int * 4)()
     assert L.amun_gpu_refinement_criterion(crit, None) == N.AMUN_E_NOT_INITIALIZED
     src = (C.c_int * 9)()

@@ -1,5 +1,5 @@
-"""The explicit reconstructions besides TVD and WENO-Z on the GPU (the
-generic sweep variant) against the oracle, bit for bit in FP64: the
+"""The explicit reconstructions besides TVD and WENO-Z (the Gaussian-process
+one included) on the GPU (the generic sweep variant) against the oracle, bit for bit in FP64: the
 per-block stand-in of update_flux (line ends included) and whole steps,
 with clip_extrema / fix_positivity / mlp_limiting, at the smallest ghost
 layers each method allows, and in FP32 bulk within 1e-5 (L1, density)."""
@@ -15,7 +15,8 @@ from amun_b200.params import geometry
 pytestmark = pytest.mark.gpu
 
 UNIT = dict(xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0)
-METHODS = [("weno3", 2), ("limo3", 2), ("ppm", 4), ("weno5yc", 3), ("weno5ns", 3), ("mp5", 3), ("mp7", 4)]
+METHODS = [("weno3", 2), ("limo3", 2), ("ppm", 4), ("weno5yc", 3), ("weno5ns", 3), ("mp5", 3), ("mp7", 4),
+           ("gp", 3)]
 
 
 @pytest.mark.parametrize("rec,ng", METHODS)
@@ -59,7 +60,33 @@ def test_steps(rec, ng, eq, rs, nd):
         s.close()
 
 
-@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2)])
+@pytest.mark.parametrize("ngp,sgp,ng", [(1, 9.0, 3), (3, 2.0, 3), (7, 9.0, 4), (7, 2.5, 4)])
+def test_gp_stencils(ngp, sgp, ng):
+    """Every Gaussian-process stencil size this build takes, block stand-in
+    and steps, bit for bit (the weights computed by the library and by the
+    oracle independently, both in quadruple precision)."""
+    from amun_b200.solver import Simulation
+    import oracle
+    p = params("mhd", "gp", "hlld", "rk2", ndims=2, ncells=16, nghosts=ng, ngp=ngp, sgp=sgp, maxlev=2, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    s, o = Simulation(p), oracle.Oracle(p)
+    try:
+        q = rough((o.km, o.jm, o.im), o.nv, seed=ngp)
+        s.set_cmax(2.0)
+        o.set_cmax(2.0)
+        assert_same(s.update_flux_block(q), o.update_flux(q), f"update_flux gp{ngp}")
+        q0 = rough(mesh.shape, s.nv, seed=5)
+        s.set_primitive(q0)
+        o.set_prim(q0)
+        for _ in range(3):
+            s.advance(1.0e30)
+            o.advance(1.0e30)
+        assert_same(s.conserved(), o.cons(), f"steps gp{ngp}")
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2), ("gp", 3)])
 def test_fp32_bulk(rec, ng):
     from amun_b200.solver import Simulation
     import oracle
