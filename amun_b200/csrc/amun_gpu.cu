@@ -84,6 +84,10 @@ struct Ctx {
   int* fix_idx = nullptr;
   void* fix_val = nullptr;
   int fix_cap = 0;
+  // compact reconstructions: one direction's face values (fl, fr), laid
+  // out as q
+  void* fcl = nullptr;
+  void* fcr = nullptr;
 };
 
 Ctx C;
@@ -218,6 +222,9 @@ void free_pool() {
   if (C.fix_idx) cudaFree(C.fix_idx);
   if (C.fix_val) cudaFree(C.fix_val);
   C.fix_idx = nullptr; C.fix_val = nullptr; C.fix_cap = 0;
+  if (C.fcl) cudaFree(C.fcl);
+  if (C.fcr) cudaFree(C.fcr);
+  C.fcl = C.fcr = nullptr;
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   if (C.u0) cudaFree(C.u0);
@@ -403,11 +410,19 @@ int launch_stage(const StageDesc& st) {
   a.st = st;
   a.LP = LP; a.LW = LW;
   a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr;
+  a.fcl = (const R*)C.fcl; a.fcr = (const R*)C.fcr;
   const int rs = effective_solver();
+  const bool compact = rec_compact(C.p.reconstruction);
   for (int d = 0; d < C.g.ndims; ++d) {
     a.first = d == 0;
     a.last = d == C.g.ndims - 1;
     ProfScope ps(d);
+    if (compact) {
+      // the line pass of this direction over the stage input
+      cudaError_t e = Launch<R, R>::compact_faces(C.p.eqsys, a.q, (R*)C.fcl, (R*)C.fcr, C.g, C.nblocks, d, a.m,
+                                                  C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "compact reconstruction");
+    }
     if (!C.amr) {
       cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, sweep_variant(), rs, d, a, grid, threads, smem, C.stream);
       if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
@@ -631,9 +646,15 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"mp5", "MP5"})) p->reconstruction = AMUN_REC_MP5;
     else if (is_one_of(v, {"mp7", "MP7"})) p->reconstruction = AMUN_REC_MP7;
     else if (is_one_of(v, {"gp", "GP"})) p->reconstruction = AMUN_REC_GP;
-    else if (is_one_of(v, {"crweno5z", "crweno5-z", "CRWENO5Z", "CRWENO5-Z", "crweno5yc", "crweno5-yc", "CRWENO5YC",
-                           "CRWENO5-YC", "crweno5ns", "crweno5-ns", "CRWENO5NS", "CRWENO5-NS", "crmp5", "CRMP5",
-                           "crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD", "crmp7", "CRMP7", "mgp", "MGP"}))
+    else if (is_one_of(v, {"crweno5z", "crweno5-z", "CRWENO5Z", "CRWENO5-Z"})) p->reconstruction = AMUN_REC_CRWENO5Z;
+    else if (is_one_of(v, {"crweno5yc", "crweno5-yc", "CRWENO5YC", "CRWENO5-YC"}))
+      p->reconstruction = AMUN_REC_CRWENO5YC;
+    else if (is_one_of(v, {"crweno5ns", "crweno5-ns", "CRWENO5NS", "CRWENO5-NS"}))
+      p->reconstruction = AMUN_REC_CRWENO5NS;
+    else if (is_one_of(v, {"crmp5", "CRMP5"})) p->reconstruction = AMUN_REC_CRMP5;
+    else if (is_one_of(v, {"crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD"})) p->reconstruction = AMUN_REC_CRMP5LD;
+    else if (is_one_of(v, {"crmp7", "CRMP7"})) p->reconstruction = AMUN_REC_CRMP7;
+    else if (is_one_of(v, {"mgp", "MGP"}))
       return fail(AMUN_E_UNSUPPORTED, std::string("reconstruction not implemented here: ") + v);
     else return fail(200, std::string("reconstruction not implemented: ") + v);
   } else if (k == "limiter" || k == "extrema_limiter" || k == "prolongation_limiter") {
@@ -725,17 +746,22 @@ int amun_gpu_init(const amun_params* p) {
   if ((p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD) &&
       (p->c2p < AMUN_C2P_1DW || p->c2p > AMUN_C2P_2DWU))
     return fail(110, "primitive solver not implemented");
-  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_GP)
+  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_CRMP7)
     return fail(200, "reconstruction not implemented");
   // the stencil reach of each method beyond its cell, plus the cell itself;
-  // GP reaches (ngp - 1) / 2 cells and its mp_limiting two
-  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4, 3};
+  // GP reaches (ngp - 1) / 2 cells and its mp_limiting two; the compact
+  // methods solve along the whole line, and the right-hand sides of crmp5ld
+  // and crmp7 reach two cells past the first compact row
+  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4, 3, 2, 2, 2, 2, 3, 3};
   int need = kNeed[p->reconstruction];
   if (p->reconstruction == AMUN_REC_GP) {
     if (p->ngp < 1 || p->ngp > 7 || p->ngp % 2 == 0)
       return fail(AMUN_E_UNSUPPORTED, "gp: ngp must be odd and at most 7 (a 7-cell stencil)");
     need = std::max(p->ngp / 2, 2) + 1;
   }
+  if (rec_compact(p->reconstruction) && p->ncells + 2 * p->nghosts > kCompactMaxLine)
+    return fail(AMUN_E_UNSUPPORTED, "compact reconstructions: block lines longer than " +
+                                        std::to_string(kCompactMaxLine) + " cells");
   if (p->nghosts < need || p->ncells < p->nghosts)
     return fail(AMUN_E_BAD_ARGUMENT, "nghosts too small for the reconstruction stencil (or ncells < nghosts)");
   int ndev = 0;
@@ -1019,6 +1045,13 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
     CK(cudaMalloc(&C.fix_idx, (size_t)C.fix_cap * sizeof(int)));
     CK(cudaMalloc(&C.fix_val, (size_t)C.fix_cap * C.nv * rsize()));
     C.pool_bytes += (long long)C.fix_cap * (sizeof(int) + C.nv * rsize());
+  }
+  if (rec_compact(C.p.reconstruction)) {
+    CK(cudaMalloc(&C.fcl, qbytes));
+    CK(cudaMalloc(&C.fcr, qbytes));
+    CK(dset(C.fcl, 0, qbytes));
+    CK(dset(C.fcr, 0, qbytes));
+    C.pool_bytes += (long long)(2 * qbytes);
   }
   C.cur = 0;
   C.ms_valid = false;

@@ -20,6 +20,9 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t fix_unphysical(int eq, R* q, void* u, bool u_double, const Geo& g, int nblocks,
                                     const MethodConst& m, const FixConst& f, int* idx, R* val, DevScalars* sc,
                                     cudaStream_t s);
+  // compact reconstructions: the face values of direction dir (line pass)
+  static cudaError_t compact_faces(int eq, const R* q, R* fcl, R* fcr, const Geo& g, int nblocks, int dir,
+                                   const MethodConst& m, cudaStream_t s);
   static cudaError_t cons2prim_blocks(int eq, const double* u0, R* q, const Geo& g, const MethodConst& m,
                                       DevScalars* sc, int b0, int nb, cudaStream_t s);
   static cudaError_t upload_q(const double* fq, R* q, const Geo& g, int nv, int b0, int nb, cudaStream_t s);
@@ -184,6 +187,75 @@ static cudaError_t fix_unphysical_eq(R* q, void* u, bool u_double, const Geo& g,
   if (u_double) unphysical_apply_kernel<EQ, R, double><<<ga, 256, 0, s>>>(q, (double*)u, g, m, idx, val, f.cap, sc);
   else unphysical_apply_kernel<EQ, R, U1T><<<ga, 256, 0, s>>>(q, (U1T*)u, g, m, idx, val, f.cap, sc);
   return cudaGetLastError();
+}
+
+// compact reconstructions: the line pass of one direction over every block
+// (one thread per block, variable and line; lines at the interior
+// transverse positions), writing the reference's fl / fr arrays in the
+// layout of q
+template <int EQ, typename R>
+__global__ void compact_faces_kernel(const R* q, R* fcl, R* fcr, Geo g, int nblocks, int dir, int rec, R kappa,
+                                     R kbeta, R eps, int four) {
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
+  const int nc = g.nc, ng = g.ng;
+  const int n = dir == 0 ? g.IM : (dir == 1 ? g.JM : g.KM);
+  const int ntr = g.ndims == 3 ? nc : 1;
+  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
+  const long long sP = dir == 0 ? sX : (dir == 1 ? sY : sZ);
+  const long long sL = dir == 0 ? sY : sX;
+  const long long sT = dir == 2 ? sY : sZ;
+  const long long total = (long long)nblocks * NV * ntr * nc;
+  R gs[kCompactMaxLine];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int l = (int)(t % nc);  // consecutive threads: neighbouring lines
+    long long r = t / nc;
+    const int v = (int)(r % NV);
+    r /= NV;
+    const int tr = (int)(r % ntr);
+    const int b = (int)(r / ntr);
+    const long long base = (long long)b * g.qbs + (long long)(ng + l) * sL + (long long)(g.ndims == 3 ? ng + tr : 0) * sT;
+    const R* qv = q + base + (long long)v * g.qvs;
+    auto f = [&](int i) -> R {
+      if constexpr (V::SR) {
+        if (four) {
+          R qc[NV];
+#pragma unroll
+          for (int w = 0; w < NV; ++w) qc[w] = ld_ro(q + base + (long long)w * g.qvs + (long long)(i - 1) * sP);
+          to_four_velocity(qc);
+          return qc[v];
+        }
+      }
+      return ld_ro(qv + (long long)(i - 1) * sP);
+    };
+    R* ol = fcl + base + (long long)v * g.qvs - sP;
+    R* orr = fcr + base + (long long)v * g.qvs - sP;
+    auto fl = [&](int i) -> R& { return ol[(long long)i * sP]; };
+    auto fr = [&](int i) -> R& { return orr[(long long)i * sP]; };
+    compact_line<R>(rec, n, ng, f, fl, fr, gs, kappa, kbeta, eps);
+  }
+}
+template <int EQ, typename R>
+static cudaError_t compact_eq(const R* q, R* fcl, R* fcr, const Geo& g, int nblocks, int dir, const MethodConst& m,
+                              cudaStream_t s) {
+  const long long lines = (long long)nblocks * Var<EQ>::NV * g.nc * (g.ndims == 3 ? g.nc : 1);
+  const bool four = Var<EQ>::SR && m.states_4vec;
+  compact_faces_kernel<EQ, R><<<grid_for(lines, 128), 128, 0, s>>>(q, fcl, fcr, g, nblocks, dir, m.rec, R(m.rc.kappa),
+                                                                  R(m.rc.kbeta), R(m.eps), four ? 1 : 0);
+  return cudaGetLastError();
+}
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::compact_faces(int eq, const R* q, R* fcl, R* fcr, const Geo& g, int nblocks, int dir,
+                                          const MethodConst& m, cudaStream_t s) {
+  switch (eq) {
+    case EQ_HD: return compact_eq<EQ_HD, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+    case EQ_MHD: return compact_eq<EQ_MHD, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+    case EQ_SRMHD: return compact_eq<EQ_SRMHD, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+    case EQ_SRHD: return compact_eq<EQ_SRHD, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+    case EQ_HD_ISO: return compact_eq<EQ_HD_ISO, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+    default: return compact_eq<EQ_MHD_ISO, R>(q, fcl, fcr, g, nblocks, dir, m, s);
+  }
 }
 template <typename R, typename U1T>
 cudaError_t Launch<R, U1T>::fix_unphysical(int eq, R* q, void* u, bool u_double, const Geo& g, int nblocks,

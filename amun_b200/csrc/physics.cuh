@@ -176,6 +176,7 @@ __device__ __forceinline__ void mlp_slopes(F Qn, int ndims, R* dq) {
 
 }  // namespace amun
 #include "recon.cuh"
+#include "compact.cuh"
 #include "srmhd.cuh"
 #include "srhd.cuh"
 namespace amun {

@@ -111,6 +111,10 @@ template <typename R, typename U1T> struct SweepArgs {
   const int* fquad;    // [b][dir][side][4]: finer block of each quarter of
                        // the face (transverse halves a + 2 b)
   R* ff;               // [b][dir][side][v][transverse] stored face fluxes
+  // compact reconstructions: this direction's face values from the line
+  // pass, in the layout of q (fcl the reference's fl, fcr its fr)
+  const R* fcl;
+  const R* fcr;
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
@@ -461,6 +465,13 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
           const int rec = a.m.rec;
           if (rec == REC_TVD) {
             tvd(v, pp, ll, f0, fm1, fp1, positive, fR, fL);
+          } else if (rec_compact(rec)) {
+            // fl(i) and fr(i-1) of this cell from the line pass
+            const long long c = (long long)b * g.qbs + (long long)v * g.qvs + (long long)(p0 - 1 + pp) * sP +
+                                (long long)(l0 + ll) * sL + (long long)t0 * sT;
+            fR = ld_ro(a.fcl + c);
+            fL = ld_ro(a.fcr + c - sP);
+            dir_fix(fm1, f0, fp1, positive, fR, fL);
           } else {
             R st[7];
 #pragma unroll

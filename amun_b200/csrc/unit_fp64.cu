@@ -350,6 +350,11 @@ __global__ void dir_lines(const double* q, double* qs, BlockDims d, int dir, int
       line_ends_average(n, f, fl, fr);
     } else if (rec == REC_PPM) {
       line_ppm(n, f, fl, fr, w1, w2, rc.ppm);
+    } else if (rec_compact(rec)) {
+      auto F = [&](int i) { return f[i - 1]; };
+      auto FL = [&](int i) -> double& { return fl[i - 1]; };
+      auto FR = [&](int i) -> double& { return fr[i - 1]; };
+      compact_line<double>(rec, n, d.ng, F, FL, FR, w1, rc.kappa, rc.kbeta, eps);
     } else if (rec == REC_GP) {
       line_gp(n, f, +1, fl, rc, eps);
       line_gp(n, f, -1, w1, rc, eps);

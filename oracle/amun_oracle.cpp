@@ -41,7 +41,8 @@ namespace {
 // src/coordinates.F90:160-357).  Defaults are the reference defaults.
 // ---------------------------------------------------------------------------
 enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3 };
-enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7, REC_GP };
+enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7, REC_GP,
+       REC_CRWENO5Z, REC_CRWENO5YC, REC_CRWENO5NS, REC_CRMP5, REC_CRMP5LD, REC_CRMP7 };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
 enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM, RS_HLLCM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
@@ -135,6 +136,12 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"mp5", "MP5"})) p.rec = REC_MP5;
     else if (is_one_of(v, {"mp7", "MP7"})) p.rec = REC_MP7;
     else if (is_one_of(v, {"gp", "GP"})) p.rec = REC_GP;
+    else if (is_one_of(v, {"crweno5z", "crweno5-z", "CRWENO5Z", "CRWENO5-Z"})) p.rec = REC_CRWENO5Z;
+    else if (is_one_of(v, {"crweno5yc", "crweno5-yc", "CRWENO5YC", "CRWENO5-YC"})) p.rec = REC_CRWENO5YC;
+    else if (is_one_of(v, {"crweno5ns", "crweno5-ns", "CRWENO5NS", "CRWENO5-NS"})) p.rec = REC_CRWENO5NS;
+    else if (is_one_of(v, {"crmp5", "CRMP5"})) p.rec = REC_CRMP5;
+    else if (is_one_of(v, {"crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD"})) p.rec = REC_CRMP5LD;
+    else if (is_one_of(v, {"crmp7", "CRMP7"})) p.rec = REC_CRMP7;
     else return 200;  // src/interpolations.F90:382
   } else if (key == "limiter" || key == "extrema_limiter" || key == "prolongation_limiter") {
     int l = LIM_ZERO;
@@ -559,6 +566,9 @@ struct Oracle {
     csnd = p.csnd; csnd2 = csnd * csnd;
     // reconstruct_limo3 raises the module eps (src/interpolations.F90:248)
     if (p.rec == REC_LIMO3) p.eps = fmax2(1.0e-12, p.eps);
+    // the right-hand sides of crmp5ld / crmp7 reach two cells past the first
+    // compact row: fewer than three ghost layers read outside the line
+    if ((p.rec == REC_CRMP5LD || p.rec == REC_CRMP7) && p.nghosts < 3) return 904;
     if (p.rec == REC_GP) {
       if (p.ngp < 1 || p.ngp % 2 == 0) return 904;
       if (prepare_gp()) return 202;
@@ -2591,6 +2601,226 @@ struct Oracle {
     frv[n - 1] = fc[n - 1];
   }
 
+  // tridiag src/algebra.F90:1115-1174 (Thomas algorithm); false when a
+  // pivot vanishes
+  static bool tridiag(int n, const double* l, const double* d, const double* u, const double* r, double* x) {
+    std::vector<double> g(n + 1);
+    double t = d[0];
+    x[0] = r[0] / t;
+    for (int i = 2; i <= n; ++i) {
+      const int j = i - 1;
+      g[i] = u[j - 1] / t;
+      t = d[i - 1] - l[i - 1] * g[i];
+      if (t == 0.0) return false;
+      x[i - 1] = (r[i - 1] - l[i - 1] * x[j - 1]) / t;
+    }
+    for (int i = n - 1; i >= 1; --i) x[i - 1] = x[i - 1] - g[i + 1] * x[i];
+    return true;
+  }
+
+  // reconstruct_crweno5z / crweno5yc / crweno5ns src/interpolations.F90:
+  // 2477-3674: compact WENO face values from two tridiagonal systems along
+  // the line, explicit third-order WENO rows in the ng cells next to each
+  // line end; the three differ in their smoothness weights only (ns has one
+  // set per side)
+  void reconstruct_crweno(int kind, int n, const double* fv, double* flv, double* frv) const {
+    const int ng_ = p.nghosts;
+    const double eps = p.eps;
+    auto f = [&](int i) { return fv[i - 1]; };
+    std::vector<double> dfm(n + 1), dfp(n + 1), df2(n + 1);
+    std::vector<double> al1(n + 1), ac1(n + 1), ar1(n + 1), al2(n + 1), ac2(n + 1), ar2(n + 1);
+    std::vector<double> a1(n), b1(n), c1v(n), r1(n), a2(n), b2(n), c2v(n), r2(n), u(n);
+    for (int i = 1; i <= n - 1; ++i) {
+      dfp[i] = f(i + 1) - f(i);
+      dfm[i + 1] = dfp[i];
+    }
+    dfm[1] = dfp[1];
+    dfp[n] = dfm[n];
+    const double c1 = 13.0 / 12.0, c2 = 0.25, xi = 0.4;
+    for (int i = 1; i <= n; ++i) {
+      const double dd = dfp[i] - dfm[i];
+      df2[i] = kind == 2 ? 0.5 * std::fabs(dd) : c1 * (dd * dd);
+    }
+    for (int i = 2; i <= n - 1; ++i) {
+      const int im1 = i - 1, ip1 = i + 1;
+      if (kind == 2) {
+        double df = std::fabs(dfp[i]);
+        double lq = xi * df;
+        double bl = df2[im1] + xi * std::fabs(2.0 * dfm[i] - dfm[im1]);
+        double bc = df2[i] + lq;
+        double br = df2[ip1] + lq;
+        double l3 = df * df * df;
+        double q3 = l3 / (1.0 + l3);
+        double zt = 0.5 * ((bl - br) * (bl - br) + q3 * q3);
+        al1[i] = 1.0 + zt / ((bl + eps) * (bl + eps));
+        ac1[i] = 1.0 + zt / ((bc + eps) * (bc + eps));
+        ar1[i] = 1.0 + zt / ((br + eps) * (br + eps));
+        df = std::fabs(dfm[i]);
+        lq = xi * df;
+        bl = df2[im1] + lq;
+        bc = df2[i] + lq;
+        br = df2[ip1] + xi * std::fabs(2.0 * dfp[i] - dfp[ip1]);
+        l3 = df * df * df;
+        q3 = l3 / (1.0 + l3);
+        zt = 0.5 * ((bl - br) * (bl - br) + q3 * q3);
+        al2[i] = 1.0 + zt / ((bl + eps) * (bl + eps));
+        ac2[i] = 1.0 + zt / ((bc + eps) * (bc + eps));
+        ar2[i] = 1.0 + zt / ((br + eps) * (br + eps));
+      } else {
+        const double sl = 3.0 * dfm[i] - dfm[im1], sc = dfp[i] + dfm[i], sr = 3.0 * dfp[i] - dfp[ip1];
+        const double bl = df2[im1] + c2 * (sl * sl);
+        const double bc = df2[i] + c2 * (sc * sc);
+        const double br = df2[ip1] + c2 * (sr * sr);
+        double tt;
+        if (kind == 0) {
+          tt = std::fabs(br - bl);
+        } else {
+          const int im2 = std::max(1, i - 2), ip2 = std::min(n, i + 2);
+          const double s = (6.0 * f(i) + (f(im2) + f(ip2))) - 4.0 * (f(im1) + f(ip1));
+          tt = s * s;
+        }
+        al1[i] = al2[i] = 1.0 + tt / (bl + eps);
+        ac1[i] = ac2[i] = 1.0 + tt / (bc + eps);
+        ar1[i] = ar2[i] = 1.0 + tt / (br + eps);
+      }
+    }
+    const double cl = 1.0 / 9.0, cc = 5.0 / 9.0, cr = 1.0 / 3.0;
+    const double dl = 0.1, dc = 0.6, dr = 0.3, dq = 0.5;
+    const double a11 = 2.0 / 6.0, a12 = -7.0 / 6.0, a13 = 11.0 / 6.0;
+    const double a21 = -1.0 / 6.0, a22 = 5.0 / 6.0, a23 = 2.0 / 6.0;
+    const double a31 = 2.0 / 6.0, a32 = 5.0 / 6.0, a33 = -1.0 / 6.0;
+    auto norm = [](double& wl, double& wc, double& wr) {
+      const double ww = (wl + wr) + wc;
+      wl = wl / ww;
+      wr = wr / ww;
+      wc = 1.0 - (wl + wr);
+    };
+    auto ident = [](std::vector<double>& a, std::vector<double>& b, std::vector<double>& c, std::vector<double>& r,
+                    int i, double v) {
+      a[i - 1] = 0.0; b[i - 1] = 1.0; c[i - 1] = 0.0; r[i - 1] = v;
+    };
+    for (int i = ng_; i <= n - ng_ + 1; ++i) {
+      const int im1 = i - 1, ip1 = i + 1;
+      double wl = cl * al1[i], wc = cc * ac1[i], wr = cr * ar1[i];
+      norm(wl, wc, wr);
+      a1[i - 1] = 2.0 * wl + wc;
+      b1[i - 1] = wl + 2.0 * (wc + wr);
+      c1v[i - 1] = wr;
+      r1[i - 1] = ((wl * f(im1) + (5.0 * (wl + wc) + wr) * f(i)) + (wc + 5.0 * wr) * f(ip1)) * dq;
+      wl = cl * ar2[i]; wc = cc * ac2[i]; wr = cr * al2[i];
+      norm(wl, wc, wr);
+      a2[i - 1] = wr;
+      b2[i - 1] = wl + 2.0 * (wc + wr);
+      c2v[i - 1] = 2.0 * wl + wc;
+      r2[i - 1] = ((wl * f(ip1) + (5.0 * (wl + wc) + wr) * f(i)) + (wc + 5.0 * wr) * f(im1)) * dq;
+    }
+    // explicit rows, left states
+    auto expl1 = [&](int i, int im2, int im1, int ip1, int ip2) {
+      double wl = dl * al1[i], wc = dc * ac1[i], wr = dr * ar1[i];
+      norm(wl, wc, wr);
+      const double ql = (a11 * f(im2) + a12 * f(im1)) + a13 * f(i);
+      const double qc = (a21 * f(im1) + a22 * f(i)) + a23 * f(ip1);
+      const double qr = (a31 * f(i) + a32 * f(ip1)) + a33 * f(ip2);
+      return (wl * ql + wr * qr) + wc * qc;
+    };
+    auto expl2 = [&](int i, int im2, int im1, int ip1, int ip2) {
+      double wl = dl * ar2[i], wc = dc * ac2[i], wr = dr * al2[i];
+      norm(wl, wc, wr);
+      const double ql = (a11 * f(ip2) + a12 * f(ip1)) + a13 * f(i);
+      const double qc = (a21 * f(ip1) + a22 * f(i)) + a23 * f(im1);
+      const double qr = (a31 * f(i) + a32 * f(im1)) + a33 * f(im2);
+      return (wl * ql + wr * qr) + wc * qc;
+    };
+    for (int i = 2; i <= ng_; ++i) {
+      const double v = expl1(i, std::max(1, i - 2), i - 1, i + 1, i + 2);
+      flv[i - 1] = v;
+      ident(a1, b1, c1v, r1, i, v);
+    }
+    ident(a1, b1, c1v, r1, 1, 0.5 * (f(1) + f(2)));
+    for (int i = n - ng_; i <= n - 1; ++i) {
+      const double v = expl1(i, i - 2, i - 1, i + 1, std::min(n, i + 2));
+      flv[i - 1] = v;
+      ident(a1, b1, c1v, r1, i, v);
+    }
+    ident(a1, b1, c1v, r1, n, f(n));
+    for (int i = 2; i <= ng_ + 1; ++i) {
+      const double v = expl2(i, std::max(1, i - 2), i - 1, i + 1, i + 2);
+      frv[i - 1] = v;
+      ident(a2, b2, c2v, r2, i, v);
+    }
+    ident(a2, b2, c2v, r2, 1, f(1));
+    for (int i = n - ng_ + 1; i <= n - 1; ++i) {
+      const double v = expl2(i, std::max(1, i - 2), std::max(1, i - 1), std::min(n, i + 1), std::min(n, i + 2));
+      frv[i - 1] = v;
+      ident(a2, b2, c2v, r2, i, v);
+    }
+    ident(a2, b2, c2v, r2, n, 0.5 * (f(n - 1) + f(n)));
+    tridiag(n, a1.data(), b1.data(), c1v.data(), r1.data(), u.data());
+    for (int i = 0; i < n; ++i) flv[i] = u[i];
+    tridiag(n, a2.data(), b2.data(), c2v.data(), r2.data(), u.data());
+    for (int i = 0; i < n - 1; ++i) frv[i] = u[i + 1];
+    const int i = n - 1;
+    flv[0] = 0.5 * (f(1) + f(2));
+    frv[i - 1] = 0.5 * (f(i) + f(n));
+    flv[n - 1] = f(n);
+    frv[n - 1] = f(n);
+  }
+
+  // reconstruct_crmp5 / crmp5ld / crmp7 src/interpolations.F90:3930-4437:
+  // a fixed compact system for the face values (explicit rows in the ng
+  // cells next to each line end), then mp_limiting, for each side
+  void reconstruct_crmp(int kind, int n, const double* fc, double* flv, double* frv) const {
+    const int ng_ = p.nghosts;
+    static const double ce2[2] = {0.5, 0.5};
+    static const double ce3[3] = {-1.0 / 6.0, 5.0 / 6.0, 2.0 / 6.0};
+    static const double ce5[5] = {2.0 / 60.0, -13.0 / 60.0, 47.0 / 60.0, 27.0 / 60.0, -3.0 / 60.0};
+    static const double ce7[7] = {-3.0 / 420.0, 25.0 / 420.0, -101.0 / 420.0, 319.0 / 420.0, 214.0 / 420.0,
+                                  -38.0 / 420.0, 4.0 / 420.0};
+    static const double di5[3] = {0.3, 0.6, 0.1}, ci5[3] = {1.0 / 30.0, 19.0 / 30.0, 10.0 / 30.0};
+    static const double dild[3] = {0.25, 0.6, 0.15}, cild[4] = {3.0 / 120.0, 67.0 / 120.0, 49.0 / 120.0, 1.0 / 120.0};
+    static const double di7[3] = {2.0 / 7.0, 4.0 / 7.0, 1.0 / 7.0};
+    static const double ci7[5] = {-1.0 / 420.0, 19.0 / 420.0, 239.0 / 420.0, 159.0 / 420.0, 4.0 / 420.0};
+    const double* di = kind == 0 ? di5 : (kind == 1 ? dild : di7);
+    std::vector<double> a(n), b(n), c(n), r(n), u(n), fi(n);
+    for (int i = 1; i <= ng_; ++i) { a[i - 1] = 0.0; b[i - 1] = 1.0; c[i - 1] = 0.0; }
+    for (int i = ng_ + 1; i <= n - ng_ - 1; ++i) { a[i - 1] = di[0]; b[i - 1] = di[1]; c[i - 1] = di[2]; }
+    for (int i = n - ng_; i <= n; ++i) { a[i - 1] = 0.0; b[i - 1] = 1.0; c[i - 1] = 0.0; }
+    auto rhs = [&](const double* g) {
+      auto sum = [&](const double* cf, int m, int i0) {  // i0 1-based
+        double s = 0.0;
+        for (int k = 0; k < m; ++k) s = s + cf[k] * g[i0 - 1 + k];
+        return s;
+      };
+      for (int i = ng_; i <= n - ng_ + 1; ++i)
+        r[i - 1] = kind == 0 ? sum(ci5, 3, i - 1) : (kind == 1 ? sum(cild, 4, i - 1) : sum(ci7, 5, i - 2));
+      r[0] = sum(ce2, 2, 1);
+      r[1] = sum(ce3, 3, 1);
+      if (kind == 2) {
+        r[2] = sum(ce5, 5, 1);
+        for (int i = 4; i <= ng_; ++i) r[i - 1] = sum(ce7, 7, i - 3);
+        for (int i = n - ng_; i <= n - 3; ++i) r[i - 1] = sum(ce7, 7, i - 3);
+        r[n - 3] = sum(ce5, 5, n - 4);
+      } else {
+        for (int i = 3; i <= ng_; ++i) r[i - 1] = sum(ce5, 5, i - 2);
+        for (int i = n - ng_; i <= n - 2; ++i) r[i - 1] = sum(ce5, 5, i - 2);
+      }
+      r[n - 2] = sum(ce3, 3, n - 2);
+      r[n - 1] = g[n - 1];
+      tridiag(n, a.data(), b.data(), c.data(), r.data(), u.data());
+      mp_limiting(n, g, u.data());
+    };
+    rhs(fc);
+    for (int i = 0; i < n; ++i) flv[i] = u[i];
+    for (int i = 0; i < n; ++i) fi[i] = fc[n - 1 - i];
+    rhs(fi.data());
+    for (int k = 1; k <= n - 1; ++k) frv[k - 1] = u[n - 1 - k];
+    const int i = n - 1;
+    flv[0] = 0.5 * (fc[0] + fc[1]);
+    frv[i - 1] = 0.5 * (fc[i - 1] + fc[n - 1]);
+    flv[n - 1] = fc[n - 1];
+    frv[n - 1] = fc[n - 1];
+  }
+
   // reconstruct src/interpolations.F90:1343-1381
   void reconstruct(int n, const double* f, double* fl, double* fr, double h = 0.0) const {
     switch (p.rec) {
@@ -2603,6 +2833,12 @@ struct Oracle {
       case REC_MP5: reconstruct_mp(5, n, f, fl, fr); break;
       case REC_MP7: reconstruct_mp(7, n, f, fl, fr); break;
       case REC_GP: reconstruct_gp(n, f, fl, fr); break;
+      case REC_CRWENO5Z: reconstruct_crweno(0, n, f, fl, fr); break;
+      case REC_CRWENO5YC: reconstruct_crweno(1, n, f, fl, fr); break;
+      case REC_CRWENO5NS: reconstruct_crweno(2, n, f, fl, fr); break;
+      case REC_CRMP5: reconstruct_crmp(0, n, f, fl, fr); break;
+      case REC_CRMP5LD: reconstruct_crmp(1, n, f, fl, fr); break;
+      case REC_CRMP7: reconstruct_crmp(2, n, f, fl, fr); break;
       default: reconstruct_tvd(n, f, fl, fr); break;
     }
     if (p.clip) clip_extrema(n, f, fl, fr);

@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 
 UNIT = dict(xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0)
 METHODS = [("weno3", 2), ("limo3", 2), ("ppm", 4), ("weno5yc", 3), ("weno5ns", 3), ("mp5", 3), ("mp7", 4),
-           ("gp", 3)]
+           ("gp", 3), ("crweno5z", 2), ("crweno5yc", 3), ("crweno5ns", 4), ("crmp5", 2), ("crmp5ld", 3),
+           ("crmp7", 3)]
 
 
 @pytest.mark.parametrize("rec,ng", METHODS)
@@ -86,7 +87,30 @@ def test_gp_stencils(ngp, sgp, ng):
         s.close()
 
 
-@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2), ("gp", 3)])
+@pytest.mark.parametrize("rec", ["crweno5ns", "crmp7"])
+def test_compact_relativistic_four_vectors(rec):
+    """The line pass reconstructs the 4-velocity states when
+    reconstruct_states_4vec is on (SRHD, bit for bit)."""
+    from amun_b200.solver import Simulation
+    import oracle
+    p = params("srhd", rec, "hllc", "rk2", ndims=2, ncells=16, nghosts=4, maxlev=2, gamma=4.0 / 3.0,
+               state_variables="4vec", **UNIT)
+    mesh = UniformMesh(geometry(p))
+    s, o = Simulation(p), oracle.Oracle(p)
+    try:
+        q0 = smooth_field(mesh.shape, 5, seed=8, amp=0.2)
+        q0[..., 1:4] *= 0.5
+        s.set_primitive(q0)
+        o.set_prim(q0)
+        for _ in range(3):
+            s.advance(1.0e30)
+            o.advance(1.0e30)
+        assert_same(s.conserved(), o.cons(), f"srhd 4-vector {rec}")
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2), ("gp", 3), ("crweno5z", 2), ("crmp5", 3)])
 def test_fp32_bulk(rec, ng):
     from amun_b200.solver import Simulation
     import oracle
