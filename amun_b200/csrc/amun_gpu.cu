@@ -41,6 +41,7 @@ struct Ctx {
   std::vector<amun_block_desc> blocks;
   double dx_min = 1.0;
   double cgp[7] = {0, 0, 0, 0, 0, 0, 0};  // Gaussian-process weights (prepare_gp)
+  double* ugp = nullptr;                  // multidimensional GP weights on the device (prepare_mgp)
   // device pool
   void* q[2] = {nullptr, nullptr};
   double* u0 = nullptr;
@@ -411,6 +412,7 @@ int launch_stage(const StageDesc& st) {
   a.LP = LP; a.LW = LW;
   a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr;
   a.fcl = (const R*)C.fcl; a.fcr = (const R*)C.fcr;
+  a.ugp = C.ugp;
   const int rs = effective_solver();
   const bool compact = rec_compact(C.p.reconstruction);
   for (int d = 0; d < C.g.ndims; ++d) {
@@ -525,6 +527,7 @@ UnitArgs unit_args(int im, int jm, int km) {
   u.rad = C.p.limo3_rad; u.ppm = C.p.ppm_const; u.kappa = C.p.kappa; u.kbeta = C.p.kbeta;
   u.ngp = C.p.ngp;
   for (int k = 0; k < 7; ++k) u.cgp[k] = C.cgp[k];
+  u.ugp = C.ugp;
   return u;
 }
 
@@ -654,8 +657,7 @@ int amun_gpu_set_param(amun_params* p, const char* key, const char* value) {
     else if (is_one_of(v, {"crmp5", "CRMP5"})) p->reconstruction = AMUN_REC_CRMP5;
     else if (is_one_of(v, {"crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD"})) p->reconstruction = AMUN_REC_CRMP5LD;
     else if (is_one_of(v, {"crmp7", "CRMP7"})) p->reconstruction = AMUN_REC_CRMP7;
-    else if (is_one_of(v, {"mgp", "MGP"}))
-      return fail(AMUN_E_UNSUPPORTED, std::string("reconstruction not implemented here: ") + v);
+    else if (is_one_of(v, {"mgp", "MGP"})) p->reconstruction = AMUN_REC_MGP;
     else return fail(200, std::string("reconstruction not implemented: ") + v);
   } else if (k == "limiter" || k == "extrema_limiter" || k == "prolongation_limiter") {
     int l = AMUN_LIM_ZERO;
@@ -746,18 +748,25 @@ int amun_gpu_init(const amun_params* p) {
   if ((p->eqsys == AMUN_EQ_SRMHD || p->eqsys == AMUN_EQ_SRHD) &&
       (p->c2p < AMUN_C2P_1DW || p->c2p > AMUN_C2P_2DWU))
     return fail(110, "primitive solver not implemented");
-  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_CRMP7)
+  if (p->reconstruction < AMUN_REC_TVD || p->reconstruction > AMUN_REC_MGP)
     return fail(200, "reconstruction not implemented");
   // the stencil reach of each method beyond its cell, plus the cell itself;
   // GP reaches (ngp - 1) / 2 cells and its mp_limiting two; the compact
   // methods solve along the whole line, and the right-hand sides of crmp5ld
   // and crmp7 reach two cells past the first compact row
-  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4, 3, 2, 2, 2, 2, 3, 3};
+  static const int kNeed[] = {2, 3, 2, 2, 4, 3, 3, 3, 4, 3, 2, 2, 2, 2, 3, 3, 2};
   int need = kNeed[p->reconstruction];
   if (p->reconstruction == AMUN_REC_GP) {
     if (p->ngp < 1 || p->ngp > 7 || p->ngp % 2 == 0)
       return fail(AMUN_E_UNSUPPORTED, "gp: ngp must be odd and at most 7 (a 7-cell stencil)");
     need = std::max(p->ngp / 2, 2) + 1;
+  }
+  if (p->reconstruction == AMUN_REC_MGP) {
+    // the multidimensional stencil reaches (ngp - 1) / 2 cells from each
+    // cell of ibl..ieu, the TVD fallback one
+    if (p->ngp < 1 || p->ngp > 7 || p->ngp % 2 == 0)
+      return fail(AMUN_E_UNSUPPORTED, "mgp: ngp must be odd and at most 7");
+    need = std::max(p->ngp / 2, 1) + 1;
   }
   if (rec_compact(p->reconstruction) && p->ncells + 2 * p->nghosts > kCompactMaxLine)
     return fail(AMUN_E_UNSUPPORTED, "compact reconstructions: block lines longer than " +
@@ -777,6 +786,17 @@ int amun_gpu_init(const amun_params* p) {
   if (C.p.ngavg < 1) C.p.ngavg = 1;
   if (C.p.npavg < 2) C.p.npavg = 2;
   for (int k = 0; k < 7; ++k) C.cgp[k] = 0.0;
+  if (C.ugp) { cudaFree(C.ugp); C.ugp = nullptr; }
+  if (p->reconstruction == AMUN_REC_MGP) {
+    const int dgp = p->ndims == 3 ? p->ngp * p->ngp * p->ngp : p->ngp * p->ngp;
+    std::vector<double> w((size_t)2 * p->ndims * dgp);
+    if (mgp_weights(p->ngp, p->sgp, p->ndims, w.data()) != 0) {
+      C.inited = false;
+      return fail(201, "mgp: the covariance matrix could not be inverted");
+    }
+    CK(cudaMalloc(&C.ugp, w.size() * sizeof(double)));
+    CK(h2d(C.ugp, w.data(), w.size() * sizeof(double)));
+  }
   if (p->reconstruction == AMUN_REC_GP && gp_weights(p->ngp, p->sgp, C.cgp) != 0) {
     C.inited = false;
     return fail(202, "gp: the covariance matrix could not be inverted");

@@ -49,6 +49,54 @@ static bool invert(int n, const std::vector<quad>& m, std::vector<quad>& r) {
   return true;
 }
 
+int mgp_weights(int ngp, double sgp, int ndims, double* ugp) {
+  const int mgp = (ngp - 1) / 2, nd = ndims;
+  const int dgp = nd == 3 ? ngp * ngp * ngp : ngp * ngp;
+  const double pi = 3.14159265358979323846264338327950;
+  const quad sig = (quad)(std::sqrt(2.0) * sgp);
+  const quad fc = (quad)(0.5 * std::sqrt(pi)) * sig;
+  auto off = [&](int m, int& a, int& b, int& c) {
+    a = m % ngp - mgp;
+    b = (m / ngp) % ngp - mgp;
+    c = nd == 3 ? m / (ngp * ngp) - mgp : 0;
+  };
+  auto cell = [&](int d) -> quad {  // erf(x + 1/2) - erf(x - 1/2) for an offset d
+    return erfq((quad)(1.0 * d + 0.5) / sig) - erfq((quad)(1.0 * d - 0.5) / sig);
+  };
+  std::vector<quad> cov((size_t)dgp * dgp), inv;
+  for (int i = 0; i < dgp; ++i) {
+    int i1, j1, k1;
+    off(i, i1, j1, k1);
+    for (int j = 0; j < dgp; ++j) {
+      int i2, j2, k2;
+      off(j, i2, j2, k2);
+      quad c = fc * cell(i1 - i2) * cell(j1 - j2);
+      if (nd == 3) c = c * cell(k1 - k2);
+      cov[(size_t)i * dgp + j] = c;
+    }
+  }
+  if (!invert(dgp, cov, inv)) return 201;
+  std::vector<quad> x((size_t)dgp);
+  for (int d = 0; d < nd; ++d)
+    for (int s = 0; s < 2; ++s) {
+      for (int m = 0; m < dgp; ++m) {
+        int o[3];
+        off(m, o[0], o[1], o[2]);
+        const quad z = (quad)(1.0 * o[d] + (s == 0 ? -0.5 : 0.5)) / sig;
+        quad v = expq(-(z * z));
+        for (int e = 0; e < nd; ++e)
+          if (e != d) v = v * cell(o[e]);
+        x[m] = v;
+      }
+      for (int j = 0; j < dgp; ++j) {
+        quad acc = 0;
+        for (int k = 0; k < dgp; ++k) acc = acc + x[k] * inv[(size_t)k * dgp + j];
+        ugp[(size_t)(d * 2 + s) * dgp + j] = (double)acc;
+      }
+    }
+  return 0;
+}
+
 int gp_weights(int ngp, double sgp, double* cgp) {
   const int mgp = (ngp - 1) / 2;
   const double pi = 3.14159265358979323846264338327950;  // constants.F90, real(8)

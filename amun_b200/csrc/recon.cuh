@@ -10,7 +10,7 @@ namespace amun {
 
 // reconstruction methods (src/interpolations.F90:226-382)
 enum { REC_WENO3 = 2, REC_LIMO3 = 3, REC_PPM = 4, REC_WENO5YC = 5, REC_WENO5NS = 6, REC_MP5 = 7, REC_MP7 = 8,
-       REC_GP = 9 };
+       REC_GP = 9, REC_MGP = 16 };
 
 // the method constants beyond eps: limo3_rad, ppm_const, kappa, kbeta
 // (src/interpolations.F90:80-106, 209-212), and the Gaussian-process

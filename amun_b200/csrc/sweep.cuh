@@ -115,6 +115,8 @@ template <typename R, typename U1T> struct SweepArgs {
   // pass, in the layout of q (fcl the reference's fl, fcr its fr)
   const R* fcl;
   const R* fcr;
+  // multidimensional GP: weights [dir][side][ngp^NDIMS points]
+  const double* ugp;
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
@@ -434,6 +436,80 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       fR = f0 + dqd;
       fL = f0 - dqd;
     };
+    // interfaces_mgp src/interpolations.F90:978-1165 for one variable of one
+    // cell: the GP face values of every direction from the ngp^NDIMS
+    // stencil (read from global memory), replaced by the TVD slopes with the
+    // positivity halving when any face is not between the cell and its
+    // neighbour across it; this direction's two faces are kept
+    auto mgp = [&](int v, int pp, int ll, R f0, bool positive, R& fR, R& fL) {
+      if constexpr (REC == REC_GEN) {
+        const long long c = (long long)(p0 - 1 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+        auto qn = [&](long long cc) -> R {
+          if constexpr (V::SR) {
+            if (four) {
+              R qc[NV];
+#pragma unroll
+              for (int w = 0; w < NV; ++w) qc[w] = ld_ro(qb + cc + (long long)w * g.qvs);
+              to_four_velocity(qc);
+              return qc[v];
+            }
+          }
+          return ld_ro(qb + cc + (long long)v * g.qvs);
+        };
+        const int nd = g.ndims, ngp = a.m.rc.ngp, mg = ngp / 2;
+        const int dgp = nd == 3 ? ngp * ngp * ngp : ngp * ngp;
+        const int nf = 2 * nd;
+        const long long st[3] = {sX, sY, sZ};
+        R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+        int m = 0;
+        const int k0 = nd == 3 ? -mg : 0, k1 = nd == 3 ? mg : 0;
+        for (int kk = k0; kk <= k1; ++kk)
+          for (int jj = -mg; jj <= mg; ++jj)
+            for (int ii = -mg; ii <= mg; ++ii, ++m) {
+              const R um = qn(c + ii * sX + jj * sY + kk * sZ) - f0;
+#pragma unroll
+              for (int fs = 0; fs < 6; ++fs)
+                if (fs < nf) acc[fs] = acc[fs] + R(a.ugp[(long long)fs * dgp + m]) * um;
+            }
+        R F[6];
+#pragma unroll
+        for (int fs = 0; fs < 6; ++fs) F[fs] = acc[fs] + f0;
+        bool flag = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          if (d < nd) {
+            flag = flag || (F[2 * d] - qn(c + st[d])) * (F[2 * d] - f0) > eps;
+            flag = flag || (F[2 * d + 1] - qn(c - st[d])) * (F[2 * d + 1] - f0) > eps;
+          }
+        }
+        if (flag) {
+          R dq[3];
+          dq[0] = limiter<R>(a.m.lim, R(0.5), f0 - qn(c - sX), qn(c + sX) - f0, eps);
+          dq[1] = limiter<R>(a.m.lim, R(0.5), f0 - qn(c - sY), qn(c + sY) - f0, eps);
+          dq[2] = R(0);
+          if (nd == 3) dq[2] = limiter<R>(a.m.lim, R(0.5), f0 - qn(c - sZ), qn(c + sZ) - f0, eps);
+          if (positive) {
+            if (f0 > R(0)) {
+              for (int it = 0; it < 4096; ++it) {
+                R s = d_fabs(dq[0]) + d_fabs(dq[1]);
+                if (nd == 3) s = s + d_fabs(dq[2]);
+                if (!(f0 <= s)) break;
+                dq[0] = R(0.5) * dq[0]; dq[1] = R(0.5) * dq[1]; dq[2] = R(0.5) * dq[2];
+              }
+            } else {
+              dq[0] = dq[1] = dq[2] = R(0);
+              if (DIR == 0 && pp >= 1 && pp <= LP) atomicAdd(&a.sc->nonpositive, 1ull);
+            }
+          }
+          F[2 * DIR] = f0 + dq[DIR];
+          F[2 * DIR + 1] = f0 - dq[DIR];
+        }
+        fR = F[2 * DIR];
+        fL = F[2 * DIR + 1];
+      } else {
+        fR = fL = f0;
+      }
+    };
     // interfaces_dir src/interpolations.F90:867-959 -> reconstruct 1343-1381:
     // clip_extrema and fix_positivity restated per cell
     auto dir_fix = [&](R fm1, R f0, R fp1, bool positive, R& fR, R& fL) {
@@ -465,6 +541,8 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
           const int rec = a.m.rec;
           if (rec == REC_TVD) {
             tvd(v, pp, ll, f0, fm1, fp1, positive, fR, fL);
+          } else if (rec == REC_MGP) {
+            mgp(v, pp, ll, f0, positive, fR, fL);
           } else if (rec_compact(rec)) {
             // fl(i) and fr(i-1) of this cell from the line pass
             const long long c = (long long)b * g.qbs + (long long)v * g.qvs + (long long)(p0 - 1 + pp) * sP +

@@ -16,6 +16,7 @@ struct UnitArgs {
   double rad, ppm, kappa, kbeta;    // reconstruction constants
   int ngp;                          // Gaussian-process stencil and weights
   double cgp[7];
+  const double* ugp;                // multidimensional GP weights (device)
 };
 
 cudaError_t unit_block_flux(const UnitArgs& u, const double* q, double* qs, double* f, double* scratch,

@@ -72,6 +72,67 @@ __global__ void tvd_box(const double* q, double* qs, BlockDims d, int lim, doubl
   }
 }
 
+// ---- interfaces_mgp (src/interpolations.F90:978-1165) ------------------------
+// the cells ibl..ieu: GP face values of every direction over the ngp^NDIMS
+// stencil, the TVD slopes where a face is not between the cell and its
+// neighbour across it
+template <int EQ>
+__global__ void mgp_box(const double* q, double* qs, BlockDims d, const double* ugp, int ngp, int lim, double eps,
+                        unsigned long long* nonpos) {
+  using V = Var<EQ>;
+  constexpr int NV = V::NV;
+  const int nx = d.im - 2 * d.ng + 2, ny = d.jm - 2 * d.ng + 2, nz = d.ndims == 3 ? d.km - 2 * d.ng + 2 : 1;
+  const long long cells = (long long)d.im * d.jm * d.km;
+  const long long n = (long long)nx * ny * nz;
+  const long long st[3] = {1, d.im, (long long)d.im * d.jm};
+  const int nd = d.ndims, mg = ngp / 2, dgp = nd == 3 ? ngp * ngp * ngp : ngp * ngp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    int i = d.ng - 1 + (int)(t % nx), j = d.ng - 1 + (int)((t / nx) % ny);
+    int k = d.ndims == 3 ? d.ng - 1 + (int)(t / ((long long)nx * ny)) : 0;
+    long long c = i * st[0] + j * st[1] + k * st[2];
+    for (int v = 0; v < NV; ++v) {
+      auto Q = [&](long long cc) { return q[cc * NV + v]; };
+      const double f0 = Q(c);
+      double F[6] = {0, 0, 0, 0, 0, 0};
+      int m = 0;
+      for (int kk = nd == 3 ? -mg : 0; kk <= (nd == 3 ? mg : 0); ++kk)
+        for (int jj = -mg; jj <= mg; ++jj)
+          for (int ii = -mg; ii <= mg; ++ii, ++m) {
+            const double um = Q(c + ii * st[0] + jj * st[1] + kk * st[2]) - f0;
+            for (int fs = 0; fs < 2 * nd; ++fs) F[fs] = F[fs] + ugp[(long long)fs * dgp + m] * um;
+          }
+      for (int fs = 0; fs < 2 * nd; ++fs) F[fs] = F[fs] + f0;
+      bool flag = false;
+      for (int dd = 0; dd < nd; ++dd) {
+        flag = flag || (F[2 * dd] - Q(c + st[dd])) * (F[2 * dd] - f0) > eps;
+        flag = flag || (F[2 * dd + 1] - Q(c - st[dd])) * (F[2 * dd + 1] - f0) > eps;
+      }
+      if (flag) {
+        double dq[3] = {0.0, 0.0, 0.0};
+        for (int dd = 0; dd < nd; ++dd) dq[dd] = limiter<double>(lim, 0.5, f0 - Q(c - st[dd]), Q(c + st[dd]) - f0, eps);
+        if (v == V::DN || v == V::PR) {
+          if (f0 > 0.0) {
+            for (int it = 0; it < 4096; ++it) {
+              double s = fabs(dq[0]) + fabs(dq[1]);
+              if (nd == 3) s = s + fabs(dq[2]);
+              if (!(f0 <= s)) break;
+              dq[0] = 0.5 * dq[0]; dq[1] = 0.5 * dq[1]; dq[2] = 0.5 * dq[2];
+            }
+          } else {
+            dq[0] = dq[1] = dq[2] = 0.0;
+            atomicAdd(nonpos, 1ull);
+          }
+        }
+        for (int dd = 0; dd < nd; ++dd) { F[2 * dd] = f0 + dq[dd]; F[2 * dd + 1] = f0 - dq[dd]; }
+      }
+      for (int dd = 0; dd < nd; ++dd) {
+        qs[((long long)(2 * dd + 0) * cells + c) * NV + v] = F[2 * dd];
+        qs[((long long)(2 * dd + 1) * cells + (c - st[dd])) * NV + v] = F[2 * dd + 1];
+      }
+    }
+  }
+}
+
 // ---- mlp_limiting (src/interpolations.F90:1171-1321) -------------------------
 // The reference limits the cells one after another in storage order; a cell
 // rewrites its own two faces along each direction, except the first cell of
@@ -534,6 +595,9 @@ static cudaError_t block_flux_eq(const UnitArgs& u, const double* q, double* qs,
   if (u.rec == REC_TVD) {
     const long long nbox = (long long)(u.im - 2 * u.ng + 2) * (u.jm - 2 * u.ng + 2) * (u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1);
     tvd_box<EQ><<<(int)((nbox + 255) / 256), 256, 0, s>>>(qr, qs, d, u.lim, u.eps, nonpos);
+  } else if (u.rec == REC_MGP) {
+    const long long nbox = (long long)(u.im - 2 * u.ng + 2) * (u.jm - 2 * u.ng + 2) * (u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1);
+    mgp_box<EQ><<<(int)((nbox + 127) / 128), 128, 0, s>>>(qr, qs, d, u.ugp, u.ngp, u.lim, u.eps, nonpos);
   } else {
     for (int dir = 0; dir < u.ndims; ++dir) {
       const int ni = u.im - 2 * u.ng + 2, nj = u.jm - 2 * u.ng + 2, nk = u.ndims == 3 ? u.km - 2 * u.ng + 2 : 1;

@@ -45,7 +45,7 @@ enum { AMUN_C2P_1DW = 0, AMUN_C2P_2DWV = 1, AMUN_C2P_2DWU = 2 };
 enum { AMUN_REC_TVD = 0, AMUN_REC_WENO5Z = 1, AMUN_REC_WENO3 = 2, AMUN_REC_LIMO3 = 3, AMUN_REC_PPM = 4,
        AMUN_REC_WENO5YC = 5, AMUN_REC_WENO5NS = 6, AMUN_REC_MP5 = 7, AMUN_REC_MP7 = 8, AMUN_REC_GP = 9,
        AMUN_REC_CRWENO5Z = 10, AMUN_REC_CRWENO5YC = 11, AMUN_REC_CRWENO5NS = 12, AMUN_REC_CRMP5 = 13,
-       AMUN_REC_CRMP5LD = 14, AMUN_REC_CRMP7 = 15 };
+       AMUN_REC_CRMP5LD = 14, AMUN_REC_CRMP7 = 15, AMUN_REC_MGP = 16 };
 /* limiter / extrema_limiter (src/interpolations.F90:389-445) */
 enum { AMUN_LIM_ZERO = 0, AMUN_LIM_MM = 1, AMUN_LIM_MC = 2, AMUN_LIM_SB = 3,
        AMUN_LIM_VL = 4, AMUN_LIM_VA = 5 };

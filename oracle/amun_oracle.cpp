@@ -42,7 +42,7 @@ namespace {
 // ---------------------------------------------------------------------------
 enum { EQ_HD = 0, EQ_MHD = 1, EQ_SRMHD = 2, EQ_SRHD = 3 };
 enum { REC_TVD = 0, REC_WENO5Z = 1, REC_WENO3, REC_LIMO3, REC_PPM, REC_WENO5YC, REC_WENO5NS, REC_MP5, REC_MP7, REC_GP,
-       REC_CRWENO5Z, REC_CRWENO5YC, REC_CRWENO5NS, REC_CRMP5, REC_CRMP5LD, REC_CRMP7 };
+       REC_CRWENO5Z, REC_CRWENO5YC, REC_CRWENO5NS, REC_CRMP5, REC_CRMP5LD, REC_CRMP7, REC_MGP };
 enum { LIM_ZERO = 0, LIM_MM, LIM_MC, LIM_SB, LIM_VL, LIM_VA };
 enum { RS_HLL = 0, RS_HLLC, RS_HLLD, RS_ROE, RS_HLLDM, RS_HLLCM };
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
@@ -142,6 +142,7 @@ int apply_key(Params& p, const std::string& key, const std::string& raw) {
     else if (is_one_of(v, {"crmp5", "CRMP5"})) p.rec = REC_CRMP5;
     else if (is_one_of(v, {"crmp5l", "crmp5ld", "CRMP5L", "CRMP5LD"})) p.rec = REC_CRMP5LD;
     else if (is_one_of(v, {"crmp7", "CRMP7"})) p.rec = REC_CRMP7;
+    else if (is_one_of(v, {"mgp", "MGP"})) p.rec = REC_MGP;
     else return 200;  // src/interpolations.F90:382
   } else if (key == "limiter" || key == "extrema_limiter" || key == "prolongation_limiter") {
     int l = LIM_ZERO;
@@ -572,6 +573,10 @@ struct Oracle {
     if (p.rec == REC_GP) {
       if (p.ngp < 1 || p.ngp % 2 == 0) return 904;
       if (prepare_gp()) return 202;
+    }
+    if (p.rec == REC_MGP) {
+      if (p.ngp < 1 || p.ngp % 2 == 0) return 904;
+      if (prepare_mgp()) return 201;
     }
     if (sr && p.c2p < 0) return 110;
     p.ngavg = std::max(1, p.ngavg);
@@ -2069,6 +2074,175 @@ struct Oracle {
           if (nd == 3) {
             QS(i, j, k, 1, 3) = Q(i, j, k) + dq[2];
             QS(i, j, k - 1, 2, 3) = Q(i, j, k) - dq[2];
+          }
+        }
+    if (p.mlp) mlp_limiting(qv, qs);
+  }
+
+  // prepare_mgp src/interpolations.F90:558-715 in quadruple precision:
+  // covariances of cell averages over the ngp^NDIMS stencil under a
+  // separable Gaussian kernel, the face vectors of each direction and side,
+  // ugp = xgp inv(cov) (no symmetrisation here); stored [dir][side][dgp]
+  std::vector<double> ugp;
+  int prepare_mgp() {
+    typedef __float128 Q;
+    const int ngp = p.ngp, mgp = (ngp - 1) / 2, nd = p.ndims;
+    const int dgp = nd == 3 ? ngp * ngp * ngp : ngp * ngp, w = 2 * dgp;
+    const double pi = 3.14159265358979323846264338327950;
+    const Q sig = (Q)(std::sqrt(2.0) * p.sgp);
+    const Q fc = (Q)(0.5 * std::sqrt(pi)) * sig;
+    // stencil point m (0-based) -> offsets, i fastest (Fortran reshape order)
+    auto off = [&](int m, int& a, int& b, int& c) {
+      a = m % ngp - mgp;
+      b = (m / ngp) % ngp - mgp;
+      c = nd == 3 ? m / (ngp * ngp) - mgp : 0;
+    };
+    std::vector<Q> g((size_t)dgp * w, (Q)0);
+    auto G = [&](int i, int j) -> Q& { return g[(size_t)(i - 1) * w + (j - 1)]; };
+    for (int i = 1; i <= dgp; ++i) {
+      int i1, j1, k1;
+      off(i - 1, i1, j1, k1);
+      for (int j = 1; j <= dgp; ++j) {
+        int i2, j2, k2;
+        off(j - 1, i2, j2, k2);
+        const Q xl = (Q)(1.0 * (i1 - i2) - 0.5) / sig, xr = (Q)(1.0 * (i1 - i2) + 0.5) / sig;
+        const Q yl = (Q)(1.0 * (j1 - j2) - 0.5) / sig, yr = (Q)(1.0 * (j1 - j2) + 0.5) / sig;
+        Q cv = fc * (erfq(xr) - erfq(xl)) * (erfq(yr) - erfq(yl));
+        if (nd == 3) {
+          const Q zl = (Q)(1.0 * (k1 - k2) - 0.5) / sig, zr = (Q)(1.0 * (k1 - k2) + 0.5) / sig;
+          cv = cv * (erfq(zr) - erfq(zl));
+        }
+        G(i, j) = cv;
+      }
+      G(i, i + dgp) = 1;
+    }
+    // invert src/algebra.F90:1198-1305
+    for (int k = 1; k <= dgp - 1; ++k) {
+      if (G(k, k) == 0) {
+        if (G(k + 1, k) == 0) return 1;
+        for (int j = 1; j <= w; ++j) G(k, j) = G(k, j) + G(k + 1, j);
+      }
+      for (int j = k + 1; j <= dgp; ++j) {
+        const Q t = G(j, k) / G(k, k);
+        for (int i = k; i <= w; ++i) G(j, i) = G(j, i) - t * G(k, i);
+      }
+    }
+    for (int i = 1; i <= dgp; ++i)
+      if (G(i, i) == 0) return 1;
+    for (int i = 1; i <= dgp; ++i) {
+      const Q t = G(i, i);
+      for (int j = i; j <= w; ++j) G(i, j) = G(i, j) / t;
+    }
+    for (int k = dgp - 1; k >= 1; --k)
+      for (int i = 1; i <= k; ++i) {
+        const Q t = G(i, k + 1);
+        for (int j = k; j <= w; ++j) G(i, j) = G(i, j) - G(k + 1, j) * t;
+      }
+    // face vectors xgp(i, side, dir)
+    std::vector<Q> xgp((size_t)dgp * 2 * nd);
+    auto X = [&](int m, int s, int d) -> Q& { return xgp[(size_t)m + (size_t)dgp * (s + 2 * d)]; };
+    for (int m = 0; m < dgp; ++m) {
+      int i1, j1, k1;
+      off(m, i1, j1, k1);
+      const Q xl = (Q)(1.0 * i1 - 0.5) / sig, xr = (Q)(1.0 * i1 + 0.5) / sig;
+      const Q yl = (Q)(1.0 * j1 - 0.5) / sig, yr = (Q)(1.0 * j1 + 0.5) / sig;
+      const Q fx = erfq(xr) - erfq(xl), fy = erfq(yr) - erfq(yl);
+      if (nd == 3) {
+        const Q zl = (Q)(1.0 * k1 - 0.5) / sig, zr = (Q)(1.0 * k1 + 0.5) / sig;
+        const Q fz = erfq(zr) - erfq(zl);
+        X(m, 0, 0) = expq(-(xl * xl)) * fy * fz;
+        X(m, 1, 0) = expq(-(xr * xr)) * fy * fz;
+        X(m, 0, 1) = expq(-(yl * yl)) * fx * fz;
+        X(m, 1, 1) = expq(-(yr * yr)) * fx * fz;
+        X(m, 0, 2) = expq(-(zl * zl)) * fx * fy;
+        X(m, 1, 2) = expq(-(zr * zr)) * fx * fy;
+      } else {
+        X(m, 0, 0) = expq(-(xl * xl)) * fy;
+        X(m, 1, 0) = expq(-(xr * xr)) * fy;
+        X(m, 0, 1) = expq(-(yl * yl)) * fx;
+        X(m, 1, 1) = expq(-(yr * yr)) * fx;
+      }
+    }
+    ugp.assign((size_t)dgp * 2 * nd, 0.0);
+    for (int d = 0; d < nd; ++d)
+      for (int s = 0; s < 2; ++s)
+        for (int j = 1; j <= dgp; ++j) {
+          Q acc = 0;
+          for (int k = 1; k <= dgp; ++k) acc = acc + X(k - 1, s, d) * G(k, j + dgp);
+          ugp[(size_t)(d * 2 + s) * dgp + (j - 1)] = (double)acc;
+        }
+    return 0;
+  }
+
+  // interfaces_mgp src/interpolations.F90:978-1165: the multidimensional GP
+  // face values of every cell of ibl..ieu, replaced by the TVD slopes (with
+  // the positivity halving) where any of them is not between the cell and
+  // its neighbour across that face
+  void interfaces_mgp(bool positive, const double* qv, double* qs) {
+    const size_t N = cells();
+    auto Q = [&](int i, int j, int k) { return qv[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1))]; };
+    auto QS = [&](int i, int j, int k, int s, int d) -> double& {
+      return qs[(size_t)(i - 1) + (size_t)im * ((size_t)(j - 1) + (size_t)jm * (k - 1)) + N * ((size_t)(s - 1) + 2 * (size_t)(d - 1))];
+    };
+    ghost_copy(qv, qs);
+    const int nd = p.ndims, ngp = p.ngp, mgp = (ngp - 1) / 2;
+    const int dgp = nd == 3 ? ngp * ngp * ngp : ngp * ngp;
+    std::vector<double> u(dgp);
+    for (int k = kbl; k <= keu; ++k)
+      for (int j = jbl; j <= jeu; ++j)
+        for (int i = ibl; i <= ieu; ++i) {
+          const double q0 = Q(i, j, k);
+          int m = 0;
+          for (int kk = nd == 3 ? k - mgp : k; kk <= (nd == 3 ? k + mgp : k); ++kk)
+            for (int jj = j - mgp; jj <= j + mgp; ++jj)
+              for (int ii = i - mgp; ii <= i + mgp; ++ii) u[m++] = Q(ii, jj, kk) - q0;
+          auto face = [&](int d, int s) {
+            const double* w = &ugp[(size_t)(d * 2 + s) * dgp];
+            double acc = 0.0;
+            for (int mm = 0; mm < dgp; ++mm) acc = acc + w[mm] * u[mm];
+            return acc + q0;
+          };
+          QS(i, j, k, 1, 1) = face(0, 0);
+          QS(i - 1, j, k, 2, 1) = face(0, 1);
+          QS(i, j, k, 1, 2) = face(1, 0);
+          QS(i, j - 1, k, 2, 2) = face(1, 1);
+          if (nd == 3) {
+            QS(i, j, k, 1, 3) = face(2, 0);
+            QS(i, j, k - 1, 2, 3) = face(2, 1);
+          }
+          bool flag = (QS(i, j, k, 1, 1) - Q(i + 1, j, k)) * (QS(i, j, k, 1, 1) - q0) > p.eps;
+          flag = flag || (QS(i - 1, j, k, 2, 1) - Q(i - 1, j, k)) * (QS(i - 1, j, k, 2, 1) - q0) > p.eps;
+          flag = flag || (QS(i, j, k, 1, 2) - Q(i, j + 1, k)) * (QS(i, j, k, 1, 2) - q0) > p.eps;
+          flag = flag || (QS(i, j - 1, k, 2, 2) - Q(i, j - 1, k)) * (QS(i, j - 1, k, 2, 2) - q0) > p.eps;
+          if (nd == 3) {
+            flag = flag || (QS(i, j, k, 1, 3) - Q(i, j, k + 1)) * (QS(i, j, k, 1, 3) - q0) > p.eps;
+            flag = flag || (QS(i, j, k - 1, 2, 3) - Q(i, j, k - 1)) * (QS(i, j, k - 1, 2, 3) - q0) > p.eps;
+          }
+          if (!flag) continue;
+          double dq[3] = {0, 0, 0};
+          dq[0] = limiter(p.lim, 0.5, Q(i, j, k) - Q(i - 1, j, k), Q(i + 1, j, k) - Q(i, j, k));
+          dq[1] = limiter(p.lim, 0.5, Q(i, j, k) - Q(i, j - 1, k), Q(i, j + 1, k) - Q(i, j, k));
+          if (nd == 3) dq[2] = limiter(p.lim, 0.5, Q(i, j, k) - Q(i, j, k - 1), Q(i, j, k + 1) - Q(i, j, k));
+          if (positive) {
+            if (q0 > 0.0) {
+              for (;;) {
+                double s = std::fabs(dq[0]) + std::fabs(dq[1]);
+                if (nd == 3) s = s + std::fabs(dq[2]);
+                if (!(q0 <= s)) break;
+                for (int d = 0; d < nd; ++d) dq[d] = 0.5 * dq[d];
+              }
+            } else {
+              ++nonpositive;
+              for (int d = 0; d < nd; ++d) dq[d] = 0.0;
+            }
+          }
+          QS(i, j, k, 1, 1) = q0 + dq[0];
+          QS(i - 1, j, k, 2, 1) = q0 - dq[0];
+          QS(i, j, k, 1, 2) = q0 + dq[1];
+          QS(i, j - 1, k, 2, 2) = q0 - dq[1];
+          if (nd == 3) {
+            QS(i, j, k, 1, 3) = q0 + dq[2];
+            QS(i, j, k - 1, 2, 3) = q0 - dq[2];
           }
         }
     if (p.mlp) mlp_limiting(qv, qs);
@@ -3597,6 +3771,7 @@ struct Oracle {
       bool positive = (pv == idn || pv == ipr);
       for (size_t c = 0; c < N; ++c) one[c] = q[(size_t)(pv - 1) + (size_t)nv * c];
       if (p.rec == REC_TVD) interfaces_tvd(positive, one.data(), ones.data());
+      else if (p.rec == REC_MGP) interfaces_mgp(positive, one.data(), ones.data());
       else interfaces_dir(positive, one.data(), ones.data(), h);
       // scatter to qs(nv,im,jm,km,2,NDIMS)
       for (size_t sd = 0; sd < (size_t)2 * p.ndims; ++sd)
@@ -4396,6 +4571,11 @@ int or_gp_weights(void* h, double* out) {
   const Oracle* o = static_cast<Oracle*>(h);
   for (size_t k = 0; k < o->cgp.size(); ++k) out[k] = o->cgp[k];
   return (int)o->cgp.size();
+}
+int or_mgp_weights(void* h, double* out) {
+  const Oracle* o = static_cast<Oracle*>(h);
+  for (size_t k = 0; k < o->ugp.size(); ++k) out[k] = o->ugp[k];
+  return (int)o->ugp.size();
 }
 void or_refinement_criterion(void* h, int* crit, float* errs) {
   static_cast<Oracle*>(h)->refinement_criterion(crit, errs);

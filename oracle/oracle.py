@@ -56,6 +56,8 @@ def lib():
         L.or_set_blocks_prim.argtypes = [vp, d]
         L.or_gp_weights.argtypes = [vp, d]
         L.or_gp_weights.restype = i
+        L.or_mgp_weights.argtypes = [vp, d]
+        L.or_mgp_weights.restype = i
         L.or_refinement_criterion.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_float)]
         L.or_refinement_criterion.restype = None
         L.or_regrid.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -217,6 +219,13 @@ class Oracle:
         reconstruction = gp)."""
         out = np.zeros(16)
         n = self.L.or_gp_weights(self.h, _p(out))
+        return out[:n].copy()
+
+    def mgp_weights(self):
+        """The multidimensional GP weights of prepare_mgp, [dir][side][point]
+        flattened (empty unless reconstruction = mgp)."""
+        out = np.zeros(2 * 3 * 7 ** 3)
+        n = self.L.or_mgp_weights(self.h, _p(out))
         return out[:n].copy()
 
     def refinement_criterion(self):

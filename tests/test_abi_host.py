@@ -65,7 +65,7 @@ def test_default_params_match_reference_defaults():
     ("refinement_variables", "vort jabs magx", "ref_mask", N.AMUN_REF_VORT | N.AMUN_REF_JABS | N.AMUN_REF_MAGX),
     ("reconstruction", "GP", "reconstruction", N.AMUN_REC_GP), ("reconstruction", "CRWENO5-Z", "reconstruction", 10),
     ("reconstruction", "crweno5ns", "reconstruction", 12), ("reconstruction", "crmp5l", "reconstruction", 14),
-    ("reconstruction", "CRMP7", "reconstruction", 15), ("ngp", "7", "ngp", 7), ("sgp", "2.5", "sgp", 2.5),
+    ("reconstruction", "CRMP7", "reconstruction", 15), ("reconstruction", "MGP", "reconstruction", 16), ("ngp", "7", "ngp", 7), ("sgp", "2.5", "sgp", 2.5),
     ("crefmin", "0.3", "crefmin", 0.3), ("epsref", "0.05", "epsref", 0.05), ("jabsmax", "2", "jabsmax", 2.0),
 ])
 def test_set_param_aliases(key, val, field, expect):
@@ -77,7 +77,7 @@ def test_set_param_aliases(key, val, field, expect):
 
 
 @pytest.mark.parametrize("key,val,code", [("equation_system", "srhd_x", 100), ("equation_of_state", "polytropic", 110),
-                                          ("reconstruction", "MGP", 904), ("reconstruction", "mgp", 904),
+                                          ("reconstruction", "crweno7", 200),
                                           ("reconstruction", "nope", 200)])
 def test_set_param_reference_error_codes(key, val, code):
     L = N.lib()

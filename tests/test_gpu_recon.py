@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 UNIT = dict(xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0)
 METHODS = [("weno3", 2), ("limo3", 2), ("ppm", 4), ("weno5yc", 3), ("weno5ns", 3), ("mp5", 3), ("mp7", 4),
            ("gp", 3), ("crweno5z", 2), ("crweno5yc", 3), ("crweno5ns", 4), ("crmp5", 2), ("crmp5ld", 3),
-           ("crmp7", 3)]
+           ("crmp7", 3), ("mgp", 3)]
 
 
 @pytest.mark.parametrize("rec,ng", METHODS)
@@ -87,7 +87,34 @@ def test_gp_stencils(ngp, sgp, ng):
         s.close()
 
 
-@pytest.mark.parametrize("rec", ["crweno5ns", "crmp7"])
+@pytest.mark.parametrize("ngp,ng,nd", [(3, 2, 2), (7, 4, 2), (3, 2, 3)])
+def test_mgp_stencils(ngp, ng, nd):
+    """The multidimensional GP at other stencil sizes, block stand-in and
+    steps, bit for bit (weights computed by the library and the oracle
+    independently, both in quadruple precision)."""
+    from amun_b200.solver import Simulation
+    import oracle
+    p = params("mhd", "mgp", "hlld", "rk2", ndims=nd, ncells=16 if nd == 2 else 8, nghosts=ng, ngp=ngp, sgp=4.0,
+               maxlev=2, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    s, o = Simulation(p), oracle.Oracle(p)
+    try:
+        q = rough((o.km, o.jm, o.im), o.nv, seed=ngp)
+        s.set_cmax(2.0)
+        o.set_cmax(2.0)
+        assert_same(s.update_flux_block(q), o.update_flux(q), f"update_flux mgp{ngp}")
+        q0 = smooth_field(mesh.shape, s.nv, seed=3, amp=0.1)
+        s.set_primitive(q0)
+        o.set_prim(q0)
+        for _ in range(3):
+            s.advance(1.0e30)
+            o.advance(1.0e30)
+        assert_same(s.conserved(), o.cons(), f"steps mgp{ngp}")
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("rec", ["crweno5ns", "crmp7", "mgp"])
 def test_compact_relativistic_four_vectors(rec):
     """The line pass reconstructs the 4-velocity states when
     reconstruct_states_4vec is on (SRHD, bit for bit)."""
@@ -110,7 +137,8 @@ def test_compact_relativistic_four_vectors(rec):
         s.close()
 
 
-@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2), ("gp", 3), ("crweno5z", 2), ("crmp5", 3)])
+@pytest.mark.parametrize("rec,ng", [("ppm", 4), ("mp5", 3), ("limo3", 2), ("gp", 3), ("crweno5z", 2), ("crmp5", 3),
+                                    ("mgp", 3)])
 def test_fp32_bulk(rec, ng):
     from amun_b200.solver import Simulation
     import oracle
