@@ -82,6 +82,10 @@ def lib():
         "amun_gpu_upload_conserved": (i, [i, i, _D]),
         "amun_gpu_refinement_criterion": (i, [C.POINTER(C.c_int), C.POINTER(C.c_float)]),
         "amun_gpu_regrid": (i, [i, C.POINTER(amun_block_desc), C.POINTER(C.c_int)]),
+        "amun_gpu_prefetch_conserved": (i, [C.c_void_p]),
+        "amun_gpu_install_prefetched": (i, []),
+        "amun_gpu_post_conserved": (i, [C.c_void_p]),
+        "amun_gpu_wait_posted": (i, []),
         "amun_gpu_download": (i, [i, _D, _D, _D]),
         "amun_gpu_download_blocks": (i, [i, i, _D, _D]),
         "amun_gpu_boundary_variables": (i, []),

@@ -89,6 +89,14 @@ struct Ctx {
   // out as q
   void* fcl = nullptr;
   void* fcr = nullptr;
+  // pipelined host traffic: staging areas for a prefetched and a posted
+  // conserved state, their copy streams and the events that order them
+  double* stg_up = nullptr;
+  double* stg_dn = nullptr;
+  size_t stg_bytes = 0;
+  cudaStream_t cs_up = nullptr, cs_dn = nullptr;
+  cudaEvent_t ev_tail = nullptr, ev_h2d = nullptr, ev_pack = nullptr, ev_d2h = nullptr;
+  bool prefetched = false, posted = false;
 };
 
 Ctx C;
@@ -226,6 +234,13 @@ void free_pool() {
   if (C.fcl) cudaFree(C.fcl);
   if (C.fcr) cudaFree(C.fcr);
   C.fcl = C.fcr = nullptr;
+  if (C.cs_up) cudaStreamSynchronize(C.cs_up);
+  if (C.cs_dn) cudaStreamSynchronize(C.cs_dn);
+  if (C.stg_up) cudaFree(C.stg_up);
+  if (C.stg_dn) cudaFree(C.stg_dn);
+  C.stg_up = C.stg_dn = nullptr;
+  C.stg_bytes = 0;
+  C.prefetched = C.posted = false;
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   if (C.u0) cudaFree(C.u0);
@@ -1135,6 +1150,30 @@ int amun_gpu_upload_conserved(int first, int count, const double* u0) {
   return 0;
 }
 
+// the staging areas, copy streams and events of the pipelined transfers
+static int pipe_ready() {
+  int r = check_ready();
+  if (r) return r;
+  const size_t bytes = (size_t)C.g.qbs * C.nblocks * sizeof(double);
+  if (C.stg_bytes != bytes) {
+    if (C.cs_up) CK(cudaStreamSynchronize(C.cs_up));
+    if (C.cs_dn) CK(cudaStreamSynchronize(C.cs_dn));
+    if (C.stg_up) cudaFree(C.stg_up);
+    if (C.stg_dn) cudaFree(C.stg_dn);
+    C.stg_up = C.stg_dn = nullptr;
+    C.stg_bytes = 0;
+    CK(cudaMalloc(&C.stg_up, bytes));
+    CK(cudaMalloc(&C.stg_dn, bytes));
+    C.stg_bytes = bytes;
+    C.prefetched = C.posted = false;
+  }
+  if (!C.cs_up) CK(cudaStreamCreateWithFlags(&C.cs_up, cudaStreamNonBlocking));
+  if (!C.cs_dn) CK(cudaStreamCreateWithFlags(&C.cs_dn, cudaStreamNonBlocking));
+  for (cudaEvent_t* ev : {&C.ev_tail, &C.ev_h2d, &C.ev_pack, &C.ev_d2h})
+    if (!*ev) CK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  return 0;
+}
+
 static int download_range(int first, int count, double* u0, double* u1, double* q) {
   int r = check_ready();
   if (r) return r;
@@ -1290,6 +1329,68 @@ static int ref_bit(int v) {
   static const int mhdb[9] = {AMUN_REF_DENS, AMUN_REF_VELX, AMUN_REF_VELY, AMUN_REF_VELZ, AMUN_REF_MAGX,
                               AMUN_REF_MAGY, AMUN_REF_MAGZ, AMUN_REF_BPSI, AMUN_REF_PRES};
   return hd ? hdb[v] : mhdb[v];
+}
+
+int amun_gpu_prefetch_conserved(const double* u0) {
+  if (!u0) return fail(AMUN_E_BAD_ARGUMENT, "null array");
+  int r = pipe_ready();
+  if (r) return r;
+  // after everything queued on the compute stream so far (the install that
+  // last read the staging area among it)
+  CK(cudaEventRecord(C.ev_tail, C.stream));
+  CK(cudaStreamWaitEvent(C.cs_up, C.ev_tail, 0));
+  CK(cudaMemcpyAsync(C.stg_up, u0, C.stg_bytes, cudaMemcpyHostToDevice, C.cs_up));
+  CK(cudaEventRecord(C.ev_h2d, C.cs_up));
+  C.prefetched = true;
+  return 0;
+}
+
+int amun_gpu_install_prefetched(void) {
+  int r = pipe_ready();
+  if (r) return r;
+  if (!C.prefetched) return fail(AMUN_E_BAD_ARGUMENT, "no prefetched state to install");
+  CK(cudaStreamWaitEvent(C.stream, C.ev_h2d, 0));
+  cudaError_t e = bulk() ? Launch<float, float>::upload_u0(C.stg_up, C.u0, C.g, C.nv, 0, C.nblocks, C.stream)
+                         : Launch<double, double>::upload_u0(C.stg_up, C.u0, C.g, C.nv, 0, C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "install u0");
+  e = bulk() ? Launch<float, float>::cons2prim_blocks(C.p.eqsys, C.u0, (float*)C.q[C.cur], C.g, method_const(), C.sc,
+                                                      0, C.nblocks, C.stream)
+             : Launch<double, double>::cons2prim_blocks(C.p.eqsys, C.u0, (double*)C.q[C.cur], C.g, method_const(),
+                                                        C.sc, 0, C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cons2prim");
+  e = bulk() ? ghost_fill<float>((float*)C.q[C.cur]) : ghost_fill<double>((double*)C.q[C.cur]);
+  if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  C.ms_valid = false;
+  C.prefetched = false;
+  return 0;
+}
+
+int amun_gpu_post_conserved(double* u0) {
+  if (!u0) return fail(AMUN_E_BAD_ARGUMENT, "null array");
+  int r = pipe_ready();
+  if (r) return r;
+  // the previous posted copy must have left the staging area
+  if (C.posted) CK(cudaStreamWaitEvent(C.stream, C.ev_d2h, 0));
+  cudaError_t e = bulk() ? Launch<float, float>::download_u0(C.p.eqsys, C.u0, (const float*)C.q[C.cur], C.stg_dn,
+                                                             C.g, method_const(), 0, C.nblocks, C.stream)
+                         : Launch<double, double>::download_u0(C.p.eqsys, C.u0, (const double*)C.q[C.cur], C.stg_dn,
+                                                               C.g, method_const(), 0, C.nblocks, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "pack u0");
+  CK(cudaEventRecord(C.ev_pack, C.stream));
+  CK(cudaStreamWaitEvent(C.cs_dn, C.ev_pack, 0));
+  CK(cudaMemcpyAsync(u0, C.stg_dn, C.stg_bytes, cudaMemcpyDeviceToHost, C.cs_dn));
+  CK(cudaEventRecord(C.ev_d2h, C.cs_dn));
+  C.posted = true;
+  return 0;
+}
+
+int amun_gpu_wait_posted(void) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (!C.posted) return 0;
+  // later work on the compute stream, and events recorded there, follow it
+  CK(cudaStreamWaitEvent(C.stream, C.ev_d2h, 0));
+  CK(cudaEventSynchronize(C.ev_d2h));
+  return 0;
 }
 
 int amun_gpu_refinement_criterion(int* criterion, float* errors) {
@@ -1554,6 +1655,10 @@ void amun_gpu_finalize(void) {
   C.prof_on = false;
   free_pool();
   if (C.sc) { cudaFree(C.sc); C.sc = nullptr; }
+  for (cudaEvent_t* ev : {&C.ev_tail, &C.ev_h2d, &C.ev_pack, &C.ev_d2h})
+    if (*ev) { cudaEventDestroy(*ev); *ev = nullptr; }
+  if (C.cs_up) { cudaStreamDestroy(C.cs_up); C.cs_up = nullptr; }
+  if (C.cs_dn) { cudaStreamDestroy(C.cs_dn); C.cs_dn = nullptr; }
   if (C.own_stream) { cudaStreamDestroy(C.own_stream); C.own_stream = nullptr; }
   C.stream = nullptr;
   C.inited = false;

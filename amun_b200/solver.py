@@ -108,6 +108,30 @@ class Simulation:
         self.regrid(mesh, src)
         return src
 
+    # ---- pipelined host traffic (independent states, one per step) -----------
+    def _pinned_state(self, a: np.ndarray):
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
+        if a.shape != shp or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"expected a C-contiguous float64 block array of shape {shp} (pinned)")
+        return a.ctypes.data_as(C.c_void_p)
+
+    def prefetch_conserved(self, u0: np.ndarray):
+        """Start copying a whole conserved state to the device (returns at
+        once; keep u0 untouched until install_prefetched has run)."""
+        N.check(self.L.amun_gpu_prefetch_conserved(self._pinned_state(u0)))
+
+    def install_prefetched(self):
+        """Make the prefetched state the current one (queued on the stream)."""
+        N.check(self.L.amun_gpu_install_prefetched())
+
+    def post_conserved(self, u0: np.ndarray):
+        """Queue the copy of the current conserved state into u0 (pinned);
+        returns at once, wait_posted waits for it."""
+        N.check(self.L.amun_gpu_post_conserved(self._pinned_state(u0)))
+
+    def wait_posted(self):
+        N.check(self.L.amun_gpu_wait_posted())
+
     def download_conserved(self, u0: np.ndarray):
         """Download conserved block arrays only (ghost cells rebuilt from Q)."""
         shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)

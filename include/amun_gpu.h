@@ -179,6 +179,30 @@ int amun_gpu_upload_blocks(int first, int count, const double* u0, const double*
  * every block.  Half the host traffic of amun_gpu_upload_blocks. */
 int amun_gpu_upload_conserved(int first, int count, const double* u0);
 
+/* Pipelined host traffic, for a caller that passes independent states
+ * through the library one step at a time: the copies run on the library's
+ * own copy streams (one per direction) and overlap the steps queued between
+ * them.  All arrays are whole states (every block, Fortran layout) in
+ * pinned host memory.
+ *   amun_gpu_prefetch_conserved(u0): starts copying u0 to a device staging
+ *     area once the work queued so far on the compute stream is done;
+ *     returns at once (u0 must stay untouched until the install has run).
+ *   amun_gpu_install_prefetched(): queues, behind that copy, what
+ *     amun_gpu_upload_conserved does with it (U0, cons2prim, ghost fill).
+ *   amun_gpu_post_conserved(u0): queues the packing of the current U (ghosts
+ *     from Q, as amun_gpu_download_blocks) into a second staging area and
+ *     its copy to u0; returns at once.
+ *   amun_gpu_wait_posted(): waits until the last posted copy has landed;
+ *     later work on the compute stream follows it.
+ * A step queued between an install and the next prefetch overlaps that
+ * prefetch's copy and the previous step's posted copy.  This replaces the
+ * per-step amun_gpu_upload_conserved / amun_gpu_download_blocks pair of a
+ * caller that owns U, without changing any result. */
+int amun_gpu_prefetch_conserved(const double* u0);
+int amun_gpu_install_prefetched(void);
+int amun_gpu_post_conserved(double* u0);
+int amun_gpu_wait_posted(void);
+
 /* check_refinement_criterion (src/refinement.F90:257-336) of every block,
  * evaluated on the device: criterion[b] = -1 (derefine), 0 (keep), 1
  * (refine) from the indicators of "refinement_variables" (host array of

@@ -40,3 +40,49 @@ def test_upload_conserved(prec):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_pipelined_transfers_match_the_serial_calls(prec):
+    """prefetch / install / post / wait: three independent states passed
+    through one step each, their copies overlapping the steps, give the
+    states the serial upload / step / download calls give, bit for bit."""
+    import torch
+    from amun_b200.solver import Simulation
+    p = params("mhd", "weno5z", "hlld", "rk3", ndims=3, ncells=16, xblocks=2, xmin=0, xmax=1, ymin=0, ymax=1,
+               zmin=0, zmax=1)
+    s = Simulation(p, prec)
+    try:
+        shp = (s.mesh.nblocks, s.mesh.km, s.mesh.jm, s.mesh.im, s.nv)
+
+        def pinned():
+            return torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+
+        ins = []
+        for seed in range(3):
+            s.set_primitive(problems.turbulence(s.mesh, 5.0 / 3.0, seed=seed))
+            u = pinned()
+            s.download_conserved(u)
+            ins.append(u)
+        serial = []
+        for u in ins:
+            s.upload_conserved(u)
+            s.advance(1.0e30)
+            o = np.empty(shp)
+            s.download_conserved(o)
+            serial.append(o)
+        outs = [pinned() for _ in ins]
+        s.prefetch_conserved(ins[0])
+        for k in range(len(ins)):
+            s.install_prefetched()
+            if k + 1 < len(ins):
+                s.prefetch_conserved(ins[k + 1])
+            s.advance(1.0e30)
+            s.post_conserved(outs[k])
+        s.wait_posted()
+        for k in range(len(ins)):
+            assert np.array_equal(outs[k], serial[k]), k
+        with pytest.raises(Exception):
+            s.install_prefetched()  # nothing prefetched
+    finally:
+        s.close()
