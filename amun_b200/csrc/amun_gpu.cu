@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <unordered_map>
 #include <vector>
+#include <thread>
 
 #include "../../include/amun_gpu.h"
 #include "adjoint.h"
@@ -881,47 +882,98 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
     const int i = c[0] % nc + ng, j = c[1] % nc + ng, k = nd == 3 ? c[2] % nc + ng : 0;
     return ((long long)k * g.JM + j) * g.IM + i;
   };
-  std::vector<GhostOp> ops1, ops2;
   std::vector<signed char> kind((size_t)nblocks * g.qvs, -1);  // op kind of every ghost cell
-  for (int b = 0; b < nblocks; ++b) {
-    const int L = d[b].level;
-    for (int k = 0; k < g.KM; ++k)
-      for (int j = 0; j < g.JM; ++j)
-        for (int i = 0; i < g.IM; ++i) {
-          const bool inside = i >= ng && i < ng + nc && j >= ng && j < ng + nc && (nd == 2 || (k >= ng && k < ng + nc));
-          if (inside) continue;
-          int c[3] = {wrap(d[b].coord[0] * nc + i - ng, L, 0), wrap(d[b].coord[1] * nc + j - ng, L, 1),
-                      nd == 3 ? wrap(d[b].coord[2] * nc + k - ng, L, 2) : 0};
-          GhostOp op;
-          op.dst = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
-          op.pad = 0;
-          int S = find(L, c);
-          if (S >= 0) {
-            op.src = (long long)S * g.qbs + cell(c); op.kind = 0;
-            ops1.push_back(op);
-          } else {
-            int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
-            int Cb = find(L - 1, cc);
-            if (Cb >= 0) {
-              op.src = (long long)Cb * g.qbs + cell(cc);
-              op.kind = 2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2);
-              ops2.push_back(op);
+  // the ghost cells of each block are independent: blocks are split into
+  // contiguous ranges over host threads, each building its own op lists,
+  // which are joined in block order (the same lists as one thread builds)
+  const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const int per = (nblocks + nth - 1) / nth;
+  std::vector<std::vector<GhostOp>> t1(nth), t2(nth);
+  std::vector<std::string> terr(nth);
+  auto work = [&](int t) {
+    // one remembered lookup per level offset: neighbouring ghost cells of a
+    // row mostly fall in the same block
+    long long mk[3] = {-1, -1, -1};
+    int mv[3] = {-1, -1, -1};
+    auto findm = [&](int slot, int l, const int* c) -> int {
+      if (l < 1) return -1;
+      const long long k = key(l, c[0] / nc, c[1] / nc, nd == 3 ? c[2] / nc : 0);
+      if (k != mk[slot]) {
+        auto it = where.find(k);
+        mk[slot] = k;
+        mv[slot] = it == where.end() ? -1 : it->second;
+      }
+      return mv[slot];
+    };
+    const int b0 = t * per, b1 = std::min(nblocks, b0 + per);
+    for (int b = b0; b < b1; ++b) {
+      const int L = d[b].level;
+      for (int k = 0; k < g.KM; ++k)
+        for (int j = 0; j < g.JM; ++j)
+          for (int i = 0; i < g.IM; ++i) {
+            const bool inside =
+                i >= ng && i < ng + nc && j >= ng && j < ng + nc && (nd == 2 || (k >= ng && k < ng + nc));
+            if (inside) continue;
+            int c[3] = {wrap(d[b].coord[0] * nc + i - ng, L, 0), wrap(d[b].coord[1] * nc + j - ng, L, 1),
+                        nd == 3 ? wrap(d[b].coord[2] * nc + k - ng, L, 2) : 0};
+            GhostOp op;
+            op.dst = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
+            op.pad = 0;
+            int S = findm(0, L, c);
+            if (S >= 0) {
+              op.src = (long long)S * g.qbs + cell(c); op.kind = 0;
+              t1[t].push_back(op);
             } else {
-              int fc[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
-              int F = find(L + 1, fc);
-              if (F < 0) return fail(AMUN_E_UNSUPPORTED, "a ghost cell is covered by no block at its level or the "
-                                                         "next ones (mesh not 2:1 balanced, or a gap)");
-              op.src = (long long)F * g.qbs + cell(fc); op.kind = 1;
-              ops1.push_back(op);
+              int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
+              int Cb = findm(1, L - 1, cc);
+              if (Cb >= 0) {
+                op.src = (long long)Cb * g.qbs + cell(cc);
+                op.kind = 2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2);
+                t2[t].push_back(op);
+              } else {
+                int fc[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
+                int F = findm(2, L + 1, fc);
+                if (F < 0) {
+                  terr[t] = "a ghost cell is covered by no block at its level or the next ones (mesh not 2:1 "
+                            "balanced, or a gap)";
+                  return;
+                }
+                op.src = (long long)F * g.qbs + cell(fc); op.kind = 1;
+                t1[t].push_back(op);
+              }
             }
+            kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op.kind & 3);
           }
-          kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op.kind & 3);
-        }
+    }
+  };
+  {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+  }
+  // one list: the copies and restrictions, then the prolongations
+  size_t n1 = 0, n2 = 0;
+  for (int t = 0; t < nth; ++t) {
+    if (!terr[t].empty()) return fail(AMUN_E_UNSUPPORTED, terr[t]);
+    n1 += t1[t].size();
+    n2 += t2[t].size();
+  }
+  std::vector<GhostOp> all;
+  all.reserve(n1 + n2);
+  for (int t = 0; t < nth; ++t) {
+    all.insert(all.end(), t1[t].begin(), t1[t].end());
+    std::vector<GhostOp>().swap(t1[t]);
+  }
+  for (int t = 0; t < nth; ++t) {
+    all.insert(all.end(), t2[t].begin(), t2[t].end());
+    std::vector<GhostOp>().swap(t2[t]);
   }
   // a prolongation reads its coarse cell and the neighbours along each
   // direction: none of them may be a prolonged ghost itself
   const long long st[3] = {1, g.IM, (long long)g.IM * g.JM};
-  for (const GhostOp& op : ops2) {
+  for (size_t o = n1; o < all.size(); ++o) {
+    const GhostOp& op = all[o];
     const long long sb = op.src / g.qbs, sc = op.src - sb * g.qbs;  // block, padded cell
     for (int a = 0; a < nd; ++a)
       for (int sgn = -1; sgn <= 1; sgn += 2)
@@ -975,10 +1027,8 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
     C.lgroups.push_back({s0, e - s0});
     s0 = e;
   }
-  std::vector<GhostOp> all(ops1);
-  all.insert(all.end(), ops2.begin(), ops2.end());
-  C.nop1 = (long long)ops1.size();
-  C.nop2 = (long long)ops2.size();
+  C.nop1 = (long long)n1;
+  C.nop2 = (long long)n2;
   const size_t NT = (size_t)nc * (nd == 3 ? nc : 1);
   CK(cudaMalloc(&C.gop, std::max<size_t>(all.size(), 1) * sizeof(GhostOp)));
   CK(cudaMalloc(&C.frole, role.size() * sizeof(int)));

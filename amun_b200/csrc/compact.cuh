@@ -23,22 +23,33 @@ constexpr int kCompactMaxLine = 264;
 // tridiag for rows produced by row(i, l, d, u, r), i = 1..n (1-based): the
 // forward elimination writes x(i) through X(i) and keeps g(i) in g[i - 1],
 // the back substitution updates X in place
+// the back substitution: each line is a chain of dependent divisions, so
+// the previous solution entry stays in a register (no store-to-load round
+// trip) and the loops are unrolled to keep several rows' loads in flight
 template <typename R, class Row, class Xf>
 __device__ __forceinline__ void thomas_rows(int n, const Row& row, const Xf& X, R* g) {
   R l, d, u, r;
   row(1, l, d, u, r);
   R t = d;
-  X(1) = r / t;
+  R xp = r / t;
+  X(1) = xp;
   R up = u;
+#pragma unroll 4
   for (int i = 2; i <= n; ++i) {
     row(i, l, d, u, r);
     const R gi = up / t;
     g[i - 1] = gi;
     t = d - l * gi;
-    X(i) = (r - l * X(i - 1)) / t;
+    xp = (r - l * xp) / t;
+    X(i) = xp;
     up = u;
   }
-  for (int i = n - 1; i >= 1; --i) X(i) = X(i) - g[i] * X(i + 1);
+  R xn = xp;
+#pragma unroll 4
+  for (int i = n - 1; i >= 1; --i) {
+    xn = X(i) - g[i] * xn;
+    X(i) = xn;
+  }
 }
 
 // reconstruct_crweno5z (kind 0), crweno5yc (1), crweno5ns (2) on a line
