@@ -723,22 +723,29 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       else { U1T s = (U1T)r; a.u1[o] = s; un[v] = (double)s; }
     }
     // cons2prim of the new state (update_primitive_variables,
-    // src/equations.F90:1088-1148)
-    const Phys<double> Pd = make_phys<double>(a.m, 0.0, 0.0);
-    double qn[NV];
+    // src/equations.F90:1088-1148): in the stage precision, except the
+    // relativistic recovery, which always iterates in double
     const long long co = (long long)b * g.qbs + (long long)(p0 + pp) * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+    R qs[NV];
     if constexpr (V::SR) {
       // a failed recovery keeps the previous primitive state and sets p = 0
       // (src/equations.F90:4745-4777)
+      const Phys<double> Pd = make_phys<double>(a.m, 0.0, 0.0);
+      double qn[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) qn[v] = (double)a.q[co + v * g.qvs];
       if (!sr_recover<EQ>(un, qn, Pd)) atomicAdd(&a.sc->c2p_failures, 1ull);
-    } else {
-      cons2prim<EQ>(un, qn, Pd);
-    }
-    R qs[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) { qs[v] = (R)qn[v]; a.qout[co + v * g.qvs] = qs[v]; }
+      for (int v = 0; v < NV; ++v) qs[v] = (R)qn[v];
+    } else {
+      const Phys<R> Pr = make_phys<R>(a.m, 0.0, 0.0);
+      R ur[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ur[v] = (R)un[v];
+      cons2prim<EQ>(ur, qs, Pr);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a.qout[co + v * g.qvs] = qs[v];
     if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma, a.m.csnd));
   }
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
