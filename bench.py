@@ -482,17 +482,17 @@ def main():
         zu = r32["zu_per_s"]
         per_gpu = zu / ws
         achieved = per_gpu * B_ZU["fp32"] / 1e9
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            try:
-                traffic = json.load(open(tpath)).get("fp32_stage_bytes_per_cell")
-            except Exception:
-                traffic = None
+        # DRAM bytes (read + write) of one FP32 step of this workload, from
+        # `ncu --set full -k regex:sweep_kernel -s 3 -c 3` on
+        # `python -m amun_b200.profile_case --precision fp32 --n 128 --steps 1`
+        # (the x, y, z sweeps of the middle stage: 120.7, 206.7 and 532.3 MB),
+        # times three stages; the ghost fills add under 1 %
+        traffic = 3 * (120.7e6 + 206.7e6 + 532.3e6) if WORKLOAD.get("ncells") == 128 else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind,
                     "kernel": "stage sweeps x/y/z + ghost fill (whole SSPRK step, 432 B/zone-update)",
-                    "traffic": traffic,
+                    "traffic": traffic, "traffic_unit": "bytes per step and GPU",
+                    "traffic_per_zone_update": traffic / NCELL if traffic else None,
                     "fp64": {"achieved": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9,
                              "frac": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9 / peak}}
         cpu = None
