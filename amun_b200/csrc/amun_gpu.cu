@@ -918,17 +918,16 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
                         nd == 3 ? wrap(d[b].coord[2] * nc + k - ng, L, 2) : 0};
             GhostOp op;
             op.dst = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
-            op.pad = 0;
             int S = findm(0, L, c);
             if (S >= 0) {
-              op.src = (long long)S * g.qbs + cell(c); op.kind = 0;
+              op.sk = op_pack((long long)S * g.qbs + cell(c), 0);
               t1[t].push_back(op);
             } else {
               int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
               int Cb = findm(1, L - 1, cc);
               if (Cb >= 0) {
-                op.src = (long long)Cb * g.qbs + cell(cc);
-                op.kind = 2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2);
+                op.sk = op_pack((long long)Cb * g.qbs + cell(cc),
+                                2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2));
                 t2[t].push_back(op);
               } else {
                 int fc[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
@@ -938,11 +937,11 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
                             "balanced, or a gap)";
                   return;
                 }
-                op.src = (long long)F * g.qbs + cell(fc); op.kind = 1;
+                op.sk = op_pack((long long)F * g.qbs + cell(fc), 1);
                 t1[t].push_back(op);
               }
             }
-            kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op.kind & 3);
+            kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op_kind(op) & 3);
           }
     }
   };
@@ -973,8 +972,8 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
   // direction: none of them may be a prolonged ghost itself
   const long long st[3] = {1, g.IM, (long long)g.IM * g.JM};
   for (size_t o = n1; o < all.size(); ++o) {
-    const GhostOp& op = all[o];
-    const long long sb = op.src / g.qbs, sc = op.src - sb * g.qbs;  // block, padded cell
+    const long long src = op_src(all[o]);
+    const long long sb = src / g.qbs, sc = src - sb * g.qbs;  // block, padded cell
     for (int a = 0; a < nd; ++a)
       for (int sgn = -1; sgn <= 1; sgn += 2)
         if (kind[(size_t)sb * g.qvs + (size_t)(sc + sgn * st[a])] == 2)

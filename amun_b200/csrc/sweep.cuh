@@ -920,20 +920,29 @@ __global__ void ghost_copy_kernel(R* q, const int* nbr, Geo g, int nv, long long
 // cell src (block_*_prolong, 6071-6450); kind >> 2: the child (bit d set for
 // the upper half along d).  Copies and restrictions run first; the
 // prolongations read the coarser blocks' cells and ghosts after them.
+// one ghost cell of a mesh with levels: the q offset it fills and, in one
+// word, the q offset it reads (low 58 bits) and its kind (the bits above:
+// 0 copy, 1 restriction, 2 | child << 2 prolongation) -- 16 bytes a ghost
 struct GhostOp {
-  long long dst, src;
-  int kind, pad;
+  long long dst, sk;
 };
+__host__ __device__ __forceinline__ long long op_src(const GhostOp& o) { return o.sk & ((1LL << 58) - 1); }
+__host__ __device__ __forceinline__ int op_kind(const GhostOp& o) { return (int)((unsigned long long)o.sk >> 58); }
+__host__ __device__ __forceinline__ long long op_pack(long long src, int kind) {
+  return src | ((long long)kind << 58);
+}
 
 template <typename R>
 __global__ void amr_copy_restrict_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv) {
   const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const GhostOp op = ops[t];
+    const long long src = op_src(op);
+    const int kind = op_kind(op);
     for (int v = 0; v < nv; ++v) {
-      const R* s = q + op.src + v * g.qvs;
+      const R* s = q + src + v * g.qvs;
       R val;
-      if ((op.kind & 3) == 0) {
+      if ((kind & 3) == 0) {
         val = s[0];
       } else if (g.ndims == 2) {
         val = R(0.25) * ((s[0] + s[sX + sY]) + (s[sY] + s[sX]));
@@ -952,10 +961,11 @@ __global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long l
   const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const GhostOp op = ops[t];
-    const int bits = op.kind >> 2;
+    const long long src = op_src(op);
+    const int bits = op_kind(op) >> 2;
     const int sx = bits & 1, sy = (bits >> 1) & 1, sz = (bits >> 2) & 1;
     for (int v = 0; v < nv; ++v) {
-      const R* c = q + op.src + v * g.qvs;
+      const R* c = q + src + v * g.qvs;
       const R q0 = c[0];
       R d0 = limiter<R>(plim, R(0.5), q0 - c[-sX], c[sX] - q0, eps);
       R d1 = limiter<R>(plim, R(0.5), q0 - c[-sY], c[sY] - q0, eps);
