@@ -103,6 +103,13 @@ def test_no_device_fails_loudly():
     assert L.amun_gpu_refinement_criterion(crit, None) == N.AMUN_E_NOT_INITIALIZED
     src = (C.c_int * 9)()
     assert L.amun_gpu_regrid(1, None, src) == N.AMUN_E_NOT_INITIALIZED
+    # the pipelined transfers check their arguments, then the library state
+    assert L.amun_gpu_prefetch_conserved(None) == N.AMUN_E_BAD_ARGUMENT
+    buf = (C.c_double * 8)()
+    assert L.amun_gpu_prefetch_conserved(buf) == N.AMUN_E_NOT_INITIALIZED
+    assert L.amun_gpu_install_prefetched() == N.AMUN_E_NOT_INITIALIZED
+    assert L.amun_gpu_post_conserved(buf) == N.AMUN_E_NOT_INITIALIZED
+    assert L.amun_gpu_wait_posted() == N.AMUN_E_NOT_INITIALIZED
 
 
 def test_parameter_text():
