@@ -14,6 +14,7 @@ a face, edge or corner differ by at most one level.
 from __future__ import annotations
 
 import copy
+import ctypes as C
 import itertools
 
 import numpy as np
@@ -280,24 +281,46 @@ class AMRMesh:
         return np.array([t[1:] for t in self.order], dtype=np.int32)
 
     def descriptors(self):
+        """The block descriptors of the leaves in block-index order: level,
+        cell size, position, and the same-level neighbour across every face,
+        edge and corner (-1 where the neighbour is at another level; z
+        neighbours -1 in 2D).  Vectorised: the neighbour keys of all leaves
+        are looked up at once in the sorted leaf keys."""
         order = self.order
-        index = {t: b for b, t in enumerate(order)}
-        arr = (N.amun_block_desc * len(order))()
-        for b, (l, cx, cy, cz) in enumerate(order):
-            d = arr[b]
-            d.level = l
-            d.dx[0], d.dx[1], d.dx[2] = self.level_dx(l)
-            d.coord[0], d.coord[1], d.coord[2] = cx, cy, cz
-            ex, ey, ez = self.extent(l)
-            for oz in (-1, 0, 1):
-                for oy in (-1, 0, 1):
-                    for ox in (-1, 0, 1):
-                        n = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)
-                        if self.ndims == 2 and oz != 0:
-                            d.neighbor[n] = -1
-                            continue
-                        key = (l, (cx + ox) % ex, (cy + oy) % ey, (cz + oz) % ez)
-                        d.neighbor[n] = index.get(key, -1)
+        nb = len(order)
+        t = np.array(order, dtype=np.int64).reshape(nb, 4)
+        lev = t[:, 0]
+        ext = np.stack([np.array(self.extent(int(l))) for l in range(1, int(lev.max()) + 1)])[lev - 1]
+
+        def enc(l, x, y, z):
+            return ((l * 65536 + x) * 65536 + y) * 65536 + z
+
+        keys = enc(lev, t[:, 1], t[:, 2], t[:, 3])
+        srt = np.argsort(keys)
+        skeys = keys[srt]
+        nbr = np.full((nb, 27), -1, dtype=np.int32)
+        for oz in (-1, 0, 1):
+            if self.ndims == 2 and oz != 0:
+                continue
+            for oy in (-1, 0, 1):
+                for ox in (-1, 0, 1):
+                    n = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)
+                    k = enc(lev, (t[:, 1] + ox) % ext[:, 0], (t[:, 2] + oy) % ext[:, 1], (t[:, 3] + oz) % ext[:, 2])
+                    pos = np.minimum(np.searchsorted(skeys, k), nb - 1)
+                    hit = skeys[pos] == k
+                    nbr[:, n] = np.where(hit, srt[pos], -1)
+        D = N.amun_block_desc
+        dt = np.dtype({"names": ["level", "dx", "neighbor", "coord"],
+                       "formats": [np.int32, (np.float64, 3), (np.int32, 27), (np.int32, 3)],
+                       "offsets": [D.level.offset, D.dx.offset, D.neighbor.offset, D.coord.offset],
+                       "itemsize": C.sizeof(D)})
+        arr = (D * nb)()
+        view = np.frombuffer(arr, dtype=dt)
+        view["level"] = lev
+        dxs = np.array([self.level_dx(l) for l in range(1, int(lev.max()) + 1)])
+        view["dx"] = dxs[lev - 1]
+        view["neighbor"] = nbr
+        view["coord"] = t[:, 1:]
         return arr
 
     def view(self, b):
