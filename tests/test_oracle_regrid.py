@@ -282,3 +282,23 @@ def test_restrict_of_prolong_is_identity(oracle_mod, nd, plim):
     o.regrid(back.levels(), back.coords(), src2)
     u1 = mesh.interior(blocks_of(o, mesh, "u0"))
     assert np.allclose(u1, u0, rtol=4e-16 * 2 ** nd, atol=1e-15)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_descriptors_match_the_leaf_neighbourhoods(nd):
+    """AMRMesh.descriptors (vectorised) against a direct walk of the leaves:
+    level, cell size, position and the same-level neighbour of every face,
+    edge and corner (periodic; -1 where none, and for z in 2D)."""
+    p, mesh = amr_case(eq="hd", ndims=nd, ncells=4, maxlev=3)
+    arr = mesh.descriptors()
+    order = mesh.order
+    index = {t: b for b, t in enumerate(order)}
+    for b, (l, cx, cy, cz) in enumerate(order):
+        d = arr[b]
+        ex, ey, ez = mesh.extent(l)
+        assert d.level == l and tuple(d.coord) == (cx, cy, cz)
+        assert tuple(d.dx) == tuple(mesh.level_dx(l))
+        for oz, oy, ox in itertools.product((-1, 0, 1), repeat=3):
+            n = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)
+            want = -1 if (nd == 2 and oz != 0) else index.get((l, (cx + ox) % ex, (cy + oy) % ey, (cz + oz) % ez), -1)
+            assert d.neighbor[n] == want, (b, n)
