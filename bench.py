@@ -268,6 +268,23 @@ def amr_timing(torch, prec, steps=10, warmup=3):
            "steps": steps, "leaves": int(mesh.nblocks), "cells": int(mesh.ncells_total),
            "leaves_per_level": {int(l): int((lv == l).sum()) for l in np.unique(lv)},
            "device_bytes": sim.status()["device_bytes"]}
+    # one mesh update after the timed steps (not part of the step time): the
+    # refinement indicators on the device, the new leaves on the host, the
+    # block data moved on the device (refinement_variables "dens pres")
+    stream = torch.cuda.current_stream()
+    sim.refinement_criterion()
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    crit, _ = sim.refinement_criterion()
+    e[1].record(stream)
+    src = sim.update_mesh()
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    kinds = np.bincount(src[:, 0], minlength=3) if src is not None else np.array([sim.mesh.nblocks, 0, 0])
+    out["update_mesh"] = {"criterion_ms": e[0].elapsed_time(e[1]), "update_ms": e[1].elapsed_time(e[2]),
+                          "leaves_after": int(sim.mesh.nblocks), "kept": int(kinds[0]),
+                          "prolonged": int(kinds[1]), "restricted": int(kinds[2])}
     sim.close()
     return out
 
