@@ -16,7 +16,8 @@ so occupancy decides their speed: AMUN_SWEEP_MIN_BLOCKS caps registers so
 that that many 288-thread CTAs fit on an SM.  Measured on B200 (128^3 MHD,
 WENO-Z, HLLD, SSPRK3): FP64 with 1/2/3 CTAs 7.8/5.1/4.8 ms per step (results
 bit-identical, small spills at 3); FP32 bulk with 2/3/4/5 CTAs
-2.40/1.92/1.79/1.89 ms.  The FP32 units also use the approximate
+2.40/1.92/1.79/1.89 ms, and 1.69/1.83 ms at 4/5 CTAs once the last
+sweep's cons2prim ran in FP32.  The FP32 units also use the approximate
 single-precision divide and square root with denormals flushed; their
 conserved totals and the relativistic recovery stay in FP64.
 """
