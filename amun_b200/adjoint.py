@@ -20,11 +20,17 @@ class Evolve(torch.autograd.Function):
         sim.set_primitive(q0.detach().cpu().numpy().astype(np.float64))
         sim.forward_checkpointed(nsteps, dtnext, interval)
         ctx.sim = sim
+        # the library keeps one recorded run per context: a later recording
+        # on the same Simulation overwrites the checkpoints this backward needs
+        ctx.recording = sim.recording
         u = torch.from_numpy(sim.conserved())
         return u.to(device=q0.device, dtype=q0.dtype)
 
     @staticmethod
     def backward(ctx, grad_u):
+        if ctx.sim.recording != ctx.recording:
+            raise RuntimeError("the Simulation recorded another run after this forward; its checkpoints are gone "
+                               "(use one Simulation per differentiated run, or call backward first)")
         lam = grad_u.detach().cpu().numpy().astype(np.float64)
         lam_q0, _ = ctx.sim.adjoint(lam)
         return torch.from_numpy(lam_q0).to(device=grad_u.device, dtype=grad_u.dtype), None, None, None, None

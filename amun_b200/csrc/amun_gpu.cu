@@ -559,6 +559,12 @@ int unit_cell_sizes(const double* dx, UnitArgs& u) {
   return 0;
 }
 
+// adds a per-call event counter of a unit entry point to the context's
+// status counter (amun_status.nonpositive)
+__global__ void add_counter_kernel(unsigned long long* dst, const unsigned long long* src) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst += *src;
+}
+
 // scratch device buffers for the unit entry points
 struct DevBuf {
   void* p = nullptr;
@@ -864,6 +870,10 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
   for (int b = 0; b < nblocks; ++b) {
     const int l = d[b].level;
     if (l < 1 || l > 20) return fail(AMUN_E_BAD_ARGUMENT, "block level out of range");
+    // the lookup key packs each block position in 16 bits
+    for (int a = 0; a < nd; ++a)
+      if ((long long)base[a] << (l - 1) > 65536)
+        return fail(AMUN_E_UNSUPPORTED, "more than 65536 blocks along a direction at level " + std::to_string(l));
     for (int a = 0; a < nd; ++a)
       if (d[b].coord[a] < 0 || d[b].coord[a] >= base[a] << (l - 1))
         return fail(AMUN_E_BAD_ARGUMENT, "block position outside the domain at its level");
@@ -1200,6 +1210,23 @@ int amun_gpu_upload_conserved(int first, int count, const double* u0) {
 }
 
 // the staging areas, copy streams and events of the pipelined transfers
+// drops the remembered device addresses of the allocation-free entry
+// point's scratch (looked up again by its next call on each device)
+static void noalloc_forget();
+
+// The pipelined copies overlap a step only from page-locked host memory: a
+// copy from pageable memory is staged by the driver and returns only when it
+// is done, so the overlap would be lost without any error.  Such arrays are
+// refused instead.
+static int require_page_locked(const void* p, const char* what) {
+  cudaPointerAttributes a{};
+  CK(cudaPointerGetAttributes(&a, p));
+  if (a.type != cudaMemoryTypeHost)
+    return fail(AMUN_E_BAD_ARGUMENT, std::string(what) +
+                                         ": the host array must be page-locked (cudaHostAlloc or cudaHostRegister)");
+  return 0;
+}
+
 static int pipe_ready() {
   int r = check_ready();
   if (r) return r;
@@ -1384,6 +1411,7 @@ int amun_gpu_prefetch_conserved(const double* u0) {
   if (!u0) return fail(AMUN_E_BAD_ARGUMENT, "null array");
   int r = pipe_ready();
   if (r) return r;
+  if ((r = require_page_locked(u0, "prefetch_conserved"))) return r;
   // after everything queued on the compute stream so far (the install that
   // last read the staging area among it)
   CK(cudaEventRecord(C.ev_tail, C.stream));
@@ -1418,6 +1446,7 @@ int amun_gpu_post_conserved(double* u0) {
   if (!u0) return fail(AMUN_E_BAD_ARGUMENT, "null array");
   int r = pipe_ready();
   if (r) return r;
+  if ((r = require_page_locked(u0, "post_conserved"))) return r;
   // the previous posted copy must have left the staging area
   if (C.posted) CK(cudaStreamWaitEvent(C.stream, C.ev_d2h, 0));
   cudaError_t e = bulk() ? Launch<float, float>::download_u0(C.p.eqsys, C.u0, (const float*)C.q[C.cur], C.stg_dn,
@@ -1589,6 +1618,8 @@ int amun_gpu_update_flux_block(const double* dx, const double* q, double* f) {
   cudaError_t e = unit_block_flux(u, (const double*)dq.p, (double*)dqs.p, (double*)df.p, (double*)dsc.p,
                                   (unsigned long long*)dnp.p, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "update_flux_block");
+  add_counter_kernel<<<1, 1, 0, C.stream>>>(&C.sc->nonpositive, (const unsigned long long*)dnp.p);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(C.stream));
   CK(d2h(f, df.p, cells * C.nv * nd * sizeof(double)));
   return 0;
@@ -1698,6 +1729,7 @@ int amun_gpu_profile_read(int kind, double* total_ms, long long* launches) {
 
 void amun_gpu_finalize(void) {
   if (C.stream) cudaStreamSynchronize(C.stream);
+  noalloc_forget();
   C.marks.clear();
   for (auto e : C.event_pool) cudaEventDestroy(e);
   C.event_pool.clear();
@@ -1777,7 +1809,13 @@ extern "C" int amun_gpu_update_flux_block_noalloc(const double* dx, const double
   CK(cudaMemsetAsync(f, 0, cells * C.nv * nd * sizeof(double), C.stream));
   cudaError_t e = unit_block_flux(u, q, qs, f, sc, nonpos, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "update_flux_block_noalloc");
+  add_counter_kernel<<<1, 1, 0, C.stream>>>(&C.sc->nonpositive, nonpos);
+  CK(cudaGetLastError());
   return 0;
+}
+
+static void noalloc_forget() {
+  for (auto& p : g_noalloc_base) p = nullptr;
 }
 
 // ---- discrete adjoint ---------------------------------------------------------

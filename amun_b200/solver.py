@@ -35,6 +35,7 @@ class Simulation:
         N.check(self.L.amun_gpu_init(C.byref(self.native)))
         self._desc = self.mesh.descriptors()
         N.check(self.L.amun_gpu_set_blocks(self.mesh.nblocks, self._desc))
+        self.recording = 0  # count of forward_checkpointed calls (one recorded run is kept)
 
     # ---- state ---------------------------------------------------------------
     def set_primitive(self, q: np.ndarray):
@@ -257,6 +258,7 @@ class Simulation:
         """nsteps steps from the current state, recording what amun_gpu_adjoint
         needs (a checkpoint every `interval` steps, each step's dt and cmax)."""
         N.check(self.L.amun_gpu_forward_checkpointed(int(nsteps), float(dtnext), int(interval)))
+        self.recording += 1
 
     def replay(self, nsteps: int):
         """nsteps steps from the current state with the recorded dt and cmax."""

@@ -183,7 +183,9 @@ int amun_gpu_upload_conserved(int first, int count, const double* u0);
  * through the library one step at a time: the copies run on the library's
  * own copy streams (one per direction) and overlap the steps queued between
  * them.  All arrays are whole states (every block, Fortran layout) in
- * pinned host memory.
+ * page-locked host memory (cudaHostAlloc / cudaHostRegister); pageable
+ * arrays are refused with AMUN_E_BAD_ARGUMENT, because their copies would
+ * not overlap anything.
  *   amun_gpu_prefetch_conserved(u0): starts copying u0 to a device staging
  *     area once the work queued so far on the compute stream is done;
  *     returns at once (u0 must stay untouched until the install has run).
@@ -269,9 +271,11 @@ int amun_gpu_update_flux_block(const double* dx, const double* q, double* f);
  * scratch (face states + WENO line scratch) exceeds it is rejected with
  * AMUN_E_UNSUPPORTED: 3D blocks up to 32^3 cells including ghosts (24^3 + 4
  * ghosts, 16^3 + 4 ghosts) and 2D blocks up to about 48^2 fit.  The first call
- * on a device looks the array up (cudaGetSymbolAddress); make it before any
- * stream capture.  Calls share one scratch per device: two calls in flight at
- * once (other streams or host threads) race; keep them in one stream order. */
+ * on a device (and the first after amun_gpu_finalize) looks the array up
+ * (cudaGetSymbolAddress); make it before any stream capture.  Positivity
+ * events are added to amun_status.nonpositive, as by the allocating entry.
+ * Calls share one scratch per device: two calls in flight at once (other
+ * streams or host threads) race; keep them in one stream order. */
 int amun_gpu_update_flux_block_noalloc(const double* dx, const double* q, double* f);
 
 /* riemann_iface (src/schemes.F90:66-71): n interfaces, FP64; ql/qr are not
