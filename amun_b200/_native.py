@@ -56,7 +56,7 @@ class amun_block_desc(C.Structure):
 class amun_status(C.Structure):
     _fields_ = [("time", C.c_double), ("dt", C.c_double), ("dtn", C.c_double), ("cmax", C.c_double),
                 ("step", C.c_longlong), ("nonpositive", C.c_longlong), ("c2p_failures", C.c_longlong),
-                ("device_bytes", C.c_longlong), ("unphysical_cells", C.c_longlong)]
+                ("device_bytes", C.c_longlong), ("unphysical_cells", C.c_longlong), ("stalls", C.c_longlong)]
 
 
 _lib = None
@@ -106,6 +106,7 @@ def lib():
         "amun_gpu_set_stream": (i, [vp]),
         "amun_gpu_profile": (i, [i, i]),
         "amun_gpu_profile_read": (i, [i, _D, C.POINTER(C.c_longlong)]),
+        "amun_gpu_set_stage_kernel": (i, [i, i, C.POINTER(i)]),
         "amun_gpu_forward_checkpointed": (i, [i, d, i]),
         "amun_gpu_replay": (i, [i]),
         "amun_gpu_adjoint": (i, [_D, _D, _D]),

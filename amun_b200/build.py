@@ -5,6 +5,7 @@ Translation units:
   unit_fp64.cu           FP64 per-procedure stand-ins
   kernels_fp64*.cu       FP64 sweep and auxiliary kernels
   kernels_fp32*.cu       FP32-bulk sweep and auxiliary kernels
+  kernels_stage_fp*.cu   fused stage kernels (one launch per SSPRK stage)
 
 gp_weights.cpp is host C++ (quadruple precision through libquadmath).
 
@@ -62,6 +63,8 @@ UNITS = {
     "kernels_fp32_srhd.cu": FP32_SWEEP,
     "kernels_fp32_hd_iso.cu": FP32_SWEEP,
     "kernels_fp32_mhd_iso.cu": FP32_SWEEP,
+    "kernels_stage_fp32.cu": FP32 + ["-DAMUN_STAGE_MIN_BLOCKS=3"],
+    "kernels_stage_fp64.cu": FP64 + ["-DAMUN_STAGE_MIN_BLOCKS=2"],
 }
 
 
@@ -79,15 +82,34 @@ def _sources_newer(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def _headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs.append(os.path.join(HERE, "..", "include", "amun_gpu.h"))
-    return hs
+def _deps(src: str) -> list:
+    """The headers a source includes (quoted includes, followed through the
+    headers of this package and include/)."""
+    seen, todo = set(), [src]
+    dirs = [CSRC, os.path.join(HERE, "..", "include")]
+    while todo:
+        f = todo.pop()
+        try:
+            text = open(f).read()
+        except OSError:
+            continue
+        for line in text.splitlines():
+            line = line.strip()
+            if not line.startswith("#include \""):
+                continue
+            name = line.split('"')[1]
+            for d in [os.path.dirname(f)] + dirs:
+                h = os.path.normpath(os.path.join(d, name))
+                if os.path.exists(h):
+                    if h not in seen:
+                        seen.add(h)
+                        todo.append(h)
+                    break
+    return sorted(seen)
 
 
 def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    hdrs = _headers()
     cc = nvcc()
 
     def compile_one(src):
@@ -96,7 +118,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         cmd = [cc, *ARCH, *COMMON, *UNITS[src], "-c", srcp, "-o", obj]
         stamp = obj + ".cmd"  # the command that built obj: a flag change rebuilds it
         same_cmd = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
-        if not force and same_cmd and not _sources_newer(obj, [srcp] + hdrs):
+        if not force and same_cmd and not _sources_newer(obj, [srcp] + _deps(srcp)):
             return obj, None
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

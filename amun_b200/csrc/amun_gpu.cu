@@ -21,6 +21,7 @@
 #include "gp_weights.h"
 #include "launch.cuh"
 #include "regrid.h"
+#include "stage.cuh"
 #include "unit.h"
 
 using namespace amun;
@@ -68,8 +69,8 @@ struct Ctx {
   struct Mark { int kind; cudaEvent_t a, b; };
   std::vector<Mark> marks;
   std::vector<cudaEvent_t> event_pool;
-  double prof_ms[5] = {0, 0, 0, 0, 0};
-  long long prof_n[5] = {0, 0, 0, 0, 0};
+  double prof_ms[6] = {0, 0, 0, 0, 0, 0};
+  long long prof_n[6] = {0, 0, 0, 0, 0, 0};
   std::string err;
   // meshes with level jumps (set_blocks with blocks at several levels)
   bool amr = false;
@@ -98,6 +99,13 @@ struct Ctx {
   cudaStream_t cs_up = nullptr, cs_dn = nullptr;
   cudaEvent_t ev_tail = nullptr, ev_h2d = nullptr, ev_pack = nullptr, ev_d2h = nullptr;
   bool prefetched = false, posted = false;
+  // fused stage kernel (stage.cuh): tensor maps of the two primitive
+  // buffers (ring planes and y planes), whether they exist for this pool,
+  // whether the caller allows the kernel, and z planes per CTA
+  CUtensorMap tm_ring[2]{}, tm_y[2]{};
+  bool stage_maps = false;
+  int stage_mode = 0;
+  int stage_ks = 32;
 };
 
 Ctx C;
@@ -244,6 +252,7 @@ void free_pool() {
   C.prefetched = C.posted = false;
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
+  C.stage_maps = false;
   if (C.u0) cudaFree(C.u0);
   if (C.u1) cudaFree(C.u1);
   if (C.du) cudaFree(C.du);
@@ -363,6 +372,72 @@ int sweep_halo() {
   return v == REC_GEN ? 3 : (v == AMUN_REC_WENO5Z ? 2 : 1);
 }
 
+// The fused stage kernel covers WENO-Z on blocks of one level for the
+// adiabatic HD (HLL, HLLC) and MHD (HLL, HLLC, HLLD) systems, without the
+// passes of the generic sweep (mlp_limiting, source terms); its tiles need
+// ncells to be a multiple of 16 and nghosts a multiple of 4 (TMA boxes start
+// on 16-byte boundaries).  Everything else runs the per-direction sweeps.
+int effective_solver();
+bool stage_covers() {
+  const int eq = C.p.eqsys, rs = effective_solver();
+  if (eq != AMUN_EQ_HD && eq != AMUN_EQ_MHD) return false;
+  if (C.p.eos != AMUN_EOS_ADI) return false;
+  if (sweep_variant() != AMUN_REC_WENO5Z) return false;
+  if (!(rs == AMUN_RS_HLL || rs == AMUN_RS_HLLC || (eq == AMUN_EQ_MHD && rs == AMUN_RS_HLLD))) return false;
+  if (C.p.ncells % kStageTX || C.p.ncells % kStageTY || C.p.nghosts % 4 || C.p.nghosts < 4) return false;
+  return C.p.ndims == 2 || C.p.ndims == 3;
+}
+bool use_stage() { return C.stage_mode && C.stage_maps && !C.amr && stage_covers(); }
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda itself)
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// a tensor map over the padded primitive array [block][v][k][j][i] of one
+// q buffer with boxes of bx x by cells of one plane, all variables
+bool encode_q_map(CUtensorMap* m, void* base, unsigned bx, unsigned by) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const Geo& g = C.g;
+  const cuuint64_t es = rsize();
+  cuuint64_t dims[5] = {(cuuint64_t)g.IM, (cuuint64_t)g.JM, (cuuint64_t)g.KM, (cuuint64_t)C.nv,
+                        (cuuint64_t)C.nblocks};
+  cuuint64_t strides[4] = {g.IM * es, (cuuint64_t)g.IM * g.JM * es, (cuuint64_t)g.qvs * es,
+                           (cuuint64_t)g.qbs * es};
+  cuuint32_t box[5] = {bx, by, 1, (cuuint32_t)C.nv, 1};
+  cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  return fn(m, bulk() ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, base, dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the stage kernel's tensor maps for the current pool (when it covers the
+// configuration); without them the sweeps run
+void build_stage_maps() {
+  C.stage_maps = false;
+  if (C.amr || !stage_covers()) return;
+  bool ok = true;
+  for (int b = 0; b < 2 && ok; ++b) {
+    ok = encode_q_map(&C.tm_ring[b], C.q[b], kStageTX + 2 * kStageXH, kStageTY) &&
+         encode_q_map(&C.tm_y[b], C.q[b], kStageTX, kStageTY + 2 * kStageYH);
+  }
+  C.stage_maps = ok;
+}
+
 MethodConst method_const() {
   MethodConst m;
   m.gamma = C.gamma; m.gammam1 = C.gammam1; m.gammam1i = C.gammam1i; m.gammaxi = C.gammam1 / C.gamma;
@@ -431,7 +506,18 @@ int launch_stage(const StageDesc& st) {
   a.ugp = C.ugp;
   const int rs = effective_solver();
   const bool compact = rec_compact(C.p.reconstruction);
-  for (int d = 0; d < C.g.ndims; ++d) {
+  if (use_stage()) {
+    // every direction, the increment and the stage combination in one launch
+    StageArgs<R, R> sa;
+    sa.qout = a.qout; sa.qin = a.q; sa.u0 = C.u0; sa.u1 = a.u1; sa.sc = C.sc; sa.binv = C.binv;
+    sa.g = C.g; sa.m = a.m; sa.st = st;
+    sa.ks = C.g.ndims == 3 ? std::max(1, std::min(C.stage_ks, C.g.nc)) : 1;
+    sa.nseg = C.g.ndims == 3 ? (C.g.nc + sa.ks - 1) / sa.ks : 1;
+    ProfScope ps(5);
+    cudaError_t e = StageLaunch<R, R>::run(C.p.eqsys, rs, C.tm_ring[C.cur], C.tm_y[C.cur], sa, C.nblocks, C.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stage kernel");
+  }
+  for (int d = 0; d < C.g.ndims && !use_stage(); ++d) {
     a.first = d == 0;
     a.last = d == C.g.ndims - 1;
     ProfScope ps(d);
@@ -1153,6 +1239,7 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
     int r = build_level_tables(nblocks, blocks);
     if (r) { free_pool(); return r; }
   }
+  build_stage_maps();
   return 0;
 }
 
@@ -1581,6 +1668,7 @@ int amun_gpu_status(amun_status* s) {
   s->c2p_failures = (long long)h.c2p_failures;
   s->device_bytes = C.pool_bytes;
   s->unphysical_cells = (long long)h.unphysical;
+  s->stalls = (long long)h.stalls;
   if (h.fix_overflow)
     return fail(AMUN_E_UNSUPPORTED, "correct_unphysical_states: " + std::to_string(h.fix_overflow) +
                                         " cells beyond the replacement list were left uncorrected");
@@ -1710,17 +1798,30 @@ int amun_gpu_set_stream(void* stream) {
   return 0;
 }
 
+int amun_gpu_set_stage_kernel(int mode, int planes, int* active) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (mode != 0 && mode != 1) return fail(AMUN_E_BAD_ARGUMENT, "mode must be 0 (sweeps) or 1 (fused stage kernel)");
+  if (planes < 0) return fail(AMUN_E_BAD_ARGUMENT, "planes must be >= 0");
+  CK(cudaStreamSynchronize(C.stream));
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  C.stage_mode = mode;
+  if (planes > 0) C.stage_ks = planes;
+  if (active) *active = use_stage() ? 1 : 0;
+  return 0;
+}
+
 int amun_gpu_profile(int enable, int reset) {
   if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   prof_collect();
   if (reset)
-    for (int k = 0; k < 5; ++k) { C.prof_ms[k] = 0.0; C.prof_n[k] = 0; }
+    for (int k = 0; k < 6; ++k) { C.prof_ms[k] = 0.0; C.prof_n[k] = 0; }
   C.prof_on = enable != 0;
   return 0;
 }
 
 int amun_gpu_profile_read(int kind, double* total_ms, long long* launches) {
-  if (kind < 0 || kind > 4) return fail(AMUN_E_BAD_ARGUMENT, "kind must be 0..4");
+  if (kind < 0 || kind > 5) return fail(AMUN_E_BAD_ARGUMENT, "kind must be 0..5");
   prof_collect();
   if (total_ms) *total_ms = C.prof_ms[kind];
   if (launches) *launches = C.prof_n[kind];

@@ -47,6 +47,7 @@ struct DevScalars {
   unsigned long long unphysical;    // cells replaced by correct_unphysical_states
   unsigned long long fix_overflow;  // of those, cells beyond the fix list (not replaced)
   unsigned long long fix_count;     // entries of the current fix pass (reset per pass)
+  unsigned long long stalls;        // stage CTAs that gave up waiting for a copy
 };
 
 // One SSPRK stage combination.  ds = dscoef * dt.

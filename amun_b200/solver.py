@@ -193,7 +193,15 @@ class Simulation:
         N.check(self.L.amun_gpu_status(C.byref(s)))
         return dict(time=s.time, dt=s.dt, dtn=s.dtn, cmax=s.cmax, step=s.step,
                     nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes,
-                    unphysical_cells=s.unphysical_cells)
+                    unphysical_cells=s.unphysical_cells, stalls=s.stalls)
+
+    def set_stage_kernel(self, mode: int = 1, planes: int = 0) -> bool:
+        """1: one fused launch per stage where it covers the configuration,
+        0: one sweep per direction; planes > 0 sets the z planes per tile of
+        the fused kernel.  Returns whether the fused kernel runs."""
+        active = C.c_int()
+        N.check(self.L.amun_gpu_set_stage_kernel(int(mode), int(planes), C.byref(active)))
+        return bool(active.value)
 
     def _states(self, a: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float64)

@@ -145,6 +145,9 @@ typedef struct amun_status {
                              p <= 0 (src/equations.F90:4745-4777)           */
   long long device_bytes; /* bytes of device memory held by the block pool    */
   long long unphysical_cells; /* cells replaced by correct_unphysical_states  */
+  long long stalls;       /* fused stage kernel: tiles that gave up waiting for
+                             a tile copy (bounded wait; their cells are not
+                             updated, so a nonzero count is an error)       */
 } amun_status;
 
 /* Fill *p with the reference defaults (hd/adi, tvd/mm, hll, rk2, cfl 0.5 ...). */
@@ -299,10 +302,24 @@ int amun_gpu_set_stream(void* stream);
  * (src/timers.F90:154-299, e.g. src/evolution.F90:141-147).  While enabled,
  * every eagerly launched kernel is bracketed by CUDA events on the launching
  * stream (graph replays are not).  Kinds: 0/1/2 sweep along x/y/z, 3 ghost
- * fill, 4 time step and reductions.  enable=0 stops recording; reset != 0
- * clears the accumulated times. */
+ * fill, 4 time step and reductions, 5 fused stage kernel.  enable=0 stops
+ * recording; reset != 0 clears the accumulated times. */
 int amun_gpu_profile(int enable, int reset);
 int amun_gpu_profile_read(int kind, double* total_ms, long long* launches);
+
+/* How each SSPRK stage's fluxes are computed (no counterpart in the
+ * reference, whose update_fluxes loops over blocks and directions,
+ * src/evolution.F90:1807-1881): mode 1 runs one fused launch per stage
+ * (every direction, the increment, the stage combination and cons2prim)
+ * wherever it covers the configuration -- WENO-Z on blocks of one level,
+ * adiabatic HD (HLL, HLLC) or MHD (HLL, HLLC, HLLD), ncells a multiple of
+ * 16, nghosts a multiple of 4, no mlp_limiting or source terms; mode 0 (the
+ * default) runs one sweep per direction everywhere.  Both give the same
+ * FP64 results.  planes > 0 sets the z planes
+ * each tile of the fused kernel marches through (0 keeps the current value,
+ * initially 32).  *active (may be NULL) tells whether the fused kernel runs
+ * for the current configuration.  Invalidates captured graphs. */
+int amun_gpu_set_stage_kernel(int mode, int planes, int* active);
 
 /* Discrete adjoint of a run: no counterpart in the reference (AMUN has no
  * adjoint).  Supported: adiabatic HD and MHD, WENO-Z, HLL, any SSPRK
