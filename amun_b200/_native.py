@@ -107,6 +107,11 @@ def lib():
         "amun_gpu_profile": (i, [i, i]),
         "amun_gpu_profile_read": (i, [i, _D, C.POINTER(C.c_longlong)]),
         "amun_gpu_set_stage_kernel": (i, [i, i, C.POINTER(i)]),
+        "amun_gpu_context_create": (i, [C.POINTER(vp)]),
+        "amun_gpu_context_select": (i, [vp]),
+        "amun_gpu_context_destroy": (i, [vp]),
+        "amun_gpu_stage": (i, [i, d, d]),
+        "amun_gpu_stages": (i, [C.POINTER(i)]),
         "amun_gpu_forward_checkpointed": (i, [i, d, i]),
         "amun_gpu_replay": (i, [i]),
         "amun_gpu_adjoint": (i, [_D, _D, _D]),
@@ -136,3 +141,40 @@ def dptr(a):
         return None
     assert a.dtype.name == "float64" and a.flags["C_CONTIGUOUS"], "expected C-contiguous float64"
     return a.ctypes.data_as(_D)
+
+
+class ContextLib:
+    """The library bound to one context: every amun_gpu_* call first makes
+    that context current for the calling thread (amun_gpu_context_select),
+    so several Simulations in one process never share state."""
+
+    _UNBOUND = ("amun_gpu_context_create", "amun_gpu_context_select", "amun_gpu_context_destroy",
+                "amun_gpu_default_params", "amun_gpu_set_param")
+
+    def __init__(self):
+        self._lib = lib()
+        self._ctx = C.c_void_p()
+        check(self._lib.amun_gpu_context_create(C.byref(self._ctx)))
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    def __getattr__(self, name):
+        f = getattr(self._lib, name)
+        if not name.startswith("amun_gpu_") or name in self._UNBOUND:
+            return f
+        select, ctx = self._lib.amun_gpu_context_select, self._ctx
+
+        def call(*args):
+            select(ctx)
+            return f(*args)
+
+        call.__name__ = name
+        self.__dict__[name] = call
+        return call
+
+    def destroy(self):
+        if self._ctx:
+            self._lib.amun_gpu_context_destroy(self._ctx)
+            self._ctx = C.c_void_p()

@@ -5,6 +5,7 @@ Translation units:
   unit_fp64.cu           FP64 per-procedure stand-ins
   kernels_fp64*.cu       FP64 sweep and auxiliary kernels
   kernels_fp32*.cu       FP32-bulk sweep and auxiliary kernels
+  kernels_*_t.cu         TVD / WENO-Z sweeps with the tile shape fixed at compile time
   kernels_stage_fp*.cu   fused stage kernels (one launch per SSPRK stage)
 
 gp_weights.cpp is host C++ (quadruple precision through libquadmath).
@@ -63,6 +64,12 @@ UNITS = {
     "kernels_fp32_srhd.cu": FP32_SWEEP,
     "kernels_fp32_hd_iso.cu": FP32_SWEEP,
     "kernels_fp32_mhd_iso.cu": FP32_SWEEP,
+    "kernels_fp64_hd_t.cu": FP64_SWEEP,
+    "kernels_fp64_mhd_t.cu": FP64_SWEEP,
+    "kernels_fp64_srmhd_t.cu": FP64_SWEEP,
+    "kernels_fp32_hd_t.cu": FP32_SWEEP,
+    "kernels_fp32_mhd_t.cu": FP32_SWEEP,
+    "kernels_fp32_srmhd_t.cu": FP32_SWEEP,
     "kernels_stage_fp32.cu": FP32 + ["-DAMUN_STAGE_MIN_BLOCKS=3"],
     "kernels_stage_fp64.cu": FP64 + ["-DAMUN_STAGE_MIN_BLOCKS=2"],
 }

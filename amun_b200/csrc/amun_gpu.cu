@@ -15,6 +15,9 @@
 #include <unordered_map>
 #include <vector>
 #include <thread>
+#include <memory>
+#include <mutex>
+#include <set>
 
 #include "../../include/amun_gpu.h"
 #include "adjoint.h"
@@ -29,6 +32,25 @@ using namespace amun;
 namespace {
 
 enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
+
+// Recording of a forward run for the discrete adjoint: a copy of the state
+// (U0, the current primitives, the device scalars) every `interval` steps
+// plus after the last step, and each step's scalars after new_time_step.
+struct AdjCtx {
+  bool recorded = false;
+  int nsteps = 0, interval = 1, nseg = 0;
+  std::vector<double*> ck_u0;
+  std::vector<void*> ck_q;
+  DevScalars* ck_sc = nullptr;  // nseg + 1
+  DevScalars* rec = nullptr;    // nsteps
+  int ck_cap = 0, rec_cap = 0, seg_cap = 0;
+  double recompute_ms = 0.0, reverse_ms = 0.0;  // phases of the last adjoint
+  // reverse-pass work arrays (allocated by the first amun_gpu_adjoint)
+  void* seg_q = nullptr;        // interval x stages stage-input primitives
+  double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *G = nullptr, *P = nullptr;
+  double* stage = nullptr;      // host-layout staging
+  int* inv = nullptr;
+};
 
 struct Ctx {
   bool inited = false;
@@ -106,29 +128,31 @@ struct Ctx {
   bool stage_maps = false;
   int stage_mode = 0;
   int stage_ks = 32;
+  // the recorded forward run of the discrete adjoint
+  AdjCtx adj;
 };
 
-Ctx C;
+// Contexts: every host thread works on its current context, which is its
+// own default context unless amun_gpu_context_select picked another one
+// (amun_gpu_context_create).  The reference keeps this state in module
+// variables, one set per process (MPI rank); here several independent
+// contexts (meshes, schemes, devices) can live in one process.
+thread_local Ctx* t_current = nullptr;
+thread_local std::unique_ptr<Ctx> t_default;
+std::mutex g_ctx_mutex;
+std::set<Ctx*> g_contexts;  // contexts made by amun_gpu_context_create
 
-// Recording of a forward run for the discrete adjoint: a copy of the state
-// (U0, the current primitives, the device scalars) every `interval` steps
-// plus after the last step, and each step's scalars after new_time_step.
-struct AdjCtx {
-  bool recorded = false;
-  int nsteps = 0, interval = 1, nseg = 0;
-  std::vector<double*> ck_u0;
-  std::vector<void*> ck_q;
-  DevScalars* ck_sc = nullptr;  // nseg + 1
-  DevScalars* rec = nullptr;    // nsteps
-  int ck_cap = 0, rec_cap = 0, seg_cap = 0;
-  double recompute_ms = 0.0, reverse_ms = 0.0;  // phases of the last adjoint
-  // reverse-pass work arrays (allocated by the first amun_gpu_adjoint)
-  void* seg_q = nullptr;        // interval x stages stage-input primitives
-  double *lamU0 = nullptr, *lamU1 = nullptr, *lamdu = nullptr, *G = nullptr, *P = nullptr;
-  double* stage = nullptr;      // host-layout staging
-  int* inv = nullptr;
-};
-AdjCtx A;
+Ctx& current_ctx() {
+  if (!t_current) {
+    if (!t_default) t_default.reset(new Ctx());
+    t_current = t_default.get();
+  }
+  return *t_current;
+}
+// every function below works on the calling thread's current context
+#define C (current_ctx())
+#define A (current_ctx().adj)
+
 
 void adj_free() {
   for (auto p : A.ck_u0) cudaFree(p);
@@ -340,6 +364,14 @@ void tile_shape(int& LP, int& LW) {
     return;
   }
   int nc = C.g.nc;
+  // the shape compiled into the TVD and WENO-Z sweeps, where it fits
+  const int flp = bulk() ? FixedTile<float>::LP : FixedTile<double>::LP;
+  const int flw = bulk() ? FixedTile<float>::LW : FixedTile<double>::LW;
+  if (nc % flp == 0 && nc % flw == 0) {
+    LP = flp;
+    LW = flw;
+    return;
+  }
   LP = 1;
   for (int d = 32; d >= 1; --d)
     if (nc % d == 0) { LP = d; break; }
@@ -1421,6 +1453,43 @@ int amun_gpu_evolve(void) {
   return 0;
 }
 
+int amun_gpu_stages(int* nstages) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (!nstages) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  *nstages = (int)schedule().stages.size();
+  return 0;
+}
+
+int amun_gpu_stage(int s, double t, double dt) {
+  int r = check_ready();
+  if (r) return r;
+  const Schedule S = schedule();
+  if (s < 1 || s > (int)S.stages.size())
+    return fail(AMUN_E_BAD_ARGUMENT, "stage must be 1.." + std::to_string(S.stages.size()));
+  if (!(dt > 0.0)) return fail(AMUN_E_BAD_ARGUMENT, "dt must be positive");
+  // the step's dt (the module dt of the reference's evolve_*) and time
+  double v[2] = {dt, t};
+  CK(h2d(&C.sc->dt, &v[0], sizeof(double)));
+  CK(h2d(&C.sc->time, &v[1], sizeof(double)));
+  if (s == 1) {
+    // the final stage re-arms the max-speed accumulator of the new state
+    CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
+    C.ms_valid = false;
+    if (S.copy_first) {
+      const long long n = (long long)C.nblocks * C.g.ubs;
+      cudaError_t e = bulk() ? Launch<float, float>::copy_u0_u1(C.u0, (float*)C.u1, n, C.stream)
+                             : Launch<double, double>::copy_u0_u1(C.u0, (double*)C.u1, n, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "copy u0->u1");
+    }
+  }
+  const StageDesc& st = S.stages[s - 1];
+  r = bulk() ? launch_stage<float>(st) : launch_stage<double>(st);
+  if (r) return r;
+  if (st.final_stage) C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
 int amun_gpu_advance(double dtnext, double* time, double* dt) {
   int r = check_ready();
   if (r) return r;
@@ -1847,6 +1916,47 @@ void amun_gpu_finalize(void) {
 }
 
 const char* amun_gpu_last_error(void) { return C.err.c_str(); }
+
+int amun_gpu_context_create(void** handle) {
+  if (!handle) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  Ctx* c = new Ctx();
+  {
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    g_contexts.insert(c);
+  }
+  t_current = c;
+  *handle = c;
+  return 0;
+}
+
+int amun_gpu_context_select(void* handle) {
+  if (!handle) {
+    t_current = nullptr;  // the thread's default context
+    return 0;
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    if (!g_contexts.count(static_cast<Ctx*>(handle)))
+      return fail(AMUN_E_BAD_ARGUMENT, "not a context made by amun_gpu_context_create");
+  }
+  t_current = static_cast<Ctx*>(handle);
+  return 0;
+}
+
+int amun_gpu_context_destroy(void* handle) {
+  Ctx* c = static_cast<Ctx*>(handle);
+  {
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    if (!c || !g_contexts.count(c)) return fail(AMUN_E_BAD_ARGUMENT, "not a context made by amun_gpu_context_create");
+    g_contexts.erase(c);
+  }
+  Ctx* prev = t_current;
+  t_current = c;
+  amun_gpu_finalize();
+  t_current = prev == c ? nullptr : prev;
+  delete c;
+  return 0;
+}
 
 }  // extern "C"
 

@@ -1,0 +1,8 @@
+// Sweep kernels of the fp64 mode for the HD system, tile shape fixed at compile time.
+#define AMUN_SWEEP_IMPL
+#define AMUN_SWEEP_FIXED_IMPL
+#include "launch.cuh"
+namespace amun {
+template cudaError_t sweep_eq_fixed<double, double, EQ_HD>(int, int, int, const SweepArgs<double, double>&, dim3, int, size_t,
+                                                    cudaStream_t);
+}

@@ -48,10 +48,22 @@ template <typename R, typename U1T, int EQ>
 cudaError_t sweep_eq(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                      cudaStream_t s);
 
+// The tile shape compiled into the TVD and WENO-Z sweeps besides the
+// run-time one: 16 x 16 in FP32, 32 x 8 in FP64 (the autotuner's picks on
+// the 128^3 workload and the defaults of small blocks).
+template <typename R> struct FixedTile {
+  static constexpr int LP = sizeof(R) == 4 ? 16 : 32;
+  static constexpr int LW = sizeof(R) == 4 ? 16 : 8;
+};
+// the sweeps of the fixed tile shape; instantiated in kernels_<prec>_<eq>_t.cu
+template <typename R, typename U1T, int EQ>
+cudaError_t sweep_eq_fixed(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
+                           size_t smem, cudaStream_t s);
+
 #ifdef AMUN_SWEEP_IMPL
-template <typename R, typename U1T, int EQ, int REC, int RS, int DIR>
+template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP = 0, int TLW = 0>
 static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
-  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T>;
+  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -62,46 +74,46 @@ static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, 
   return cudaGetLastError();
 }
 
-template <typename R, typename U1T, int EQ, int REC, int RS>
+template <typename R, typename U1T, int EQ, int REC, int RS, int TLP = 0, int TLW = 0>
 static cudaError_t go_dir(int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
   switch (dir) {
-    case 0: return go_sweep<R, U1T, EQ, REC, RS, 0>(a, grid, threads, smem, s);
-    case 1: return go_sweep<R, U1T, EQ, REC, RS, 1>(a, grid, threads, smem, s);
-    default: return go_sweep<R, U1T, EQ, REC, RS, 2>(a, grid, threads, smem, s);
+    case 0: return go_sweep<R, U1T, EQ, REC, RS, 0, TLP, TLW>(a, grid, threads, smem, s);
+    case 1: return go_sweep<R, U1T, EQ, REC, RS, 1, TLP, TLW>(a, grid, threads, smem, s);
+    default: return go_sweep<R, U1T, EQ, REC, RS, 2, TLP, TLW>(a, grid, threads, smem, s);
   }
 }
 
 // the solvers each system offers (src/schemes.F90:159-503)
-template <typename R, typename U1T, int EQ, int REC>
+template <typename R, typename U1T, int EQ, int REC, int TLP = 0, int TLW = 0>
 static cudaError_t go_rs(int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem,
                          cudaStream_t s) {
   if constexpr (EQ == EQ_HD) {
     switch (rs) {
-      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
-      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC, TLP, TLW>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE, TLP, TLW>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL, TLP, TLW>(dir, a, grid, threads, smem, s);
     }
   } else if constexpr (EQ == EQ_MHD) {
     switch (rs) {
-      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
-      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
-      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC, TLP, TLW>(dir, a, grid, threads, smem, s);
+      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD, TLP, TLW>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE, TLP, TLW>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL, TLP, TLW>(dir, a, grid, threads, smem, s);
     }
   } else if constexpr (EQ == EQ_SRMHD || EQ == EQ_SRHD) {
     switch (rs) {
-      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLC: return go_dir<R, U1T, EQ, REC, RS_HLLC, TLP, TLW>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL, TLP, TLW>(dir, a, grid, threads, smem, s);
     }
   } else if constexpr (EQ == EQ_HD_ISO) {
-    if (rs == RS_ROE) return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-    return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+    if (rs == RS_ROE) return go_dir<R, U1T, EQ, REC, RS_ROE, TLP, TLW>(dir, a, grid, threads, smem, s);
+    return go_dir<R, U1T, EQ, REC, RS_HLL, TLP, TLW>(dir, a, grid, threads, smem, s);
   } else {
     switch (rs) {
-      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD>(dir, a, grid, threads, smem, s);
-      case RS_HLLDM: return go_dir<R, U1T, EQ, REC, RS_HLLDM>(dir, a, grid, threads, smem, s);
-      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE>(dir, a, grid, threads, smem, s);
-      default: return go_dir<R, U1T, EQ, REC, RS_HLL>(dir, a, grid, threads, smem, s);
+      case RS_HLLD: return go_dir<R, U1T, EQ, REC, RS_HLLD, TLP, TLW>(dir, a, grid, threads, smem, s);
+      case RS_HLLDM: return go_dir<R, U1T, EQ, REC, RS_HLLDM, TLP, TLW>(dir, a, grid, threads, smem, s);
+      case RS_ROE: return go_dir<R, U1T, EQ, REC, RS_ROE, TLP, TLW>(dir, a, grid, threads, smem, s);
+      default: return go_dir<R, U1T, EQ, REC, RS_HLL, TLP, TLW>(dir, a, grid, threads, smem, s);
     }
   }
 }
@@ -115,10 +127,26 @@ cudaError_t sweep_eq(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 
 }
 #endif  // AMUN_SWEEP_IMPL
 
+#ifdef AMUN_SWEEP_FIXED_IMPL
+template <typename R, typename U1T, int EQ>
+cudaError_t sweep_eq_fixed(int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
+                           size_t smem, cudaStream_t s) {
+  constexpr int LP = FixedTile<R>::LP, LW = FixedTile<R>::LW;
+  if (rec == REC_WENO5Z) return go_rs<R, U1T, EQ, REC_WENO5Z, LP, LW>(rs, dir, a, grid, threads, smem, s);
+  return go_rs<R, U1T, EQ, REC_TVD, LP, LW>(rs, dir, a, grid, threads, smem, s);
+}
+#endif  // AMUN_SWEEP_FIXED_IMPL
+
 #ifdef AMUN_LAUNCH_IMPL
 template <typename R, typename U1T>
 cudaError_t Launch<R, U1T>::sweep(int eq, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid,
                                   int threads, size_t smem, cudaStream_t s) {
+  if ((rec == REC_TVD || rec == REC_WENO5Z) && a.LP == FixedTile<R>::LP && a.LW == FixedTile<R>::LW &&
+      (eq == EQ_HD || eq == EQ_MHD || eq == EQ_SRMHD)) {
+    if (eq == EQ_HD) return sweep_eq_fixed<R, U1T, EQ_HD>(rec, rs, dir, a, grid, threads, smem, s);
+    if (eq == EQ_MHD) return sweep_eq_fixed<R, U1T, EQ_MHD>(rec, rs, dir, a, grid, threads, smem, s);
+    return sweep_eq_fixed<R, U1T, EQ_SRMHD>(rec, rs, dir, a, grid, threads, smem, s);
+  }
   if (eq == EQ_HD) return sweep_eq<R, U1T, EQ_HD>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_MHD) return sweep_eq<R, U1T, EQ_MHD>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_SRHD) return sweep_eq<R, U1T, EQ_SRHD>(rec, rs, dir, a, grid, threads, smem, s);

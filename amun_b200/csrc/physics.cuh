@@ -82,6 +82,24 @@ __device__ __forceinline__ float d_copysign(float a, float b) { return copysignf
 template <typename R> __device__ __forceinline__ R d_min(R a, R b) { return a < b ? a : b; }
 template <typename R> __device__ __forceinline__ R d_max(R a, R b) { return a > b ? a : b; }
 
+// Division by one denominator repeated over several numerators.  FP64
+// divides every time (the reference's arithmetic, operation by operation);
+// the FP32-bulk mode forms one approximate reciprocal (rcp.approx) and
+// multiplies.
+template <typename R> struct Div;
+template <> struct Div<double> {
+  double y;
+  __device__ __forceinline__ explicit Div(double d) : y(d) {}
+  __device__ __forceinline__ double operator()(double x) const { return x / y; }
+};
+template <> struct Div<float> {
+  float r;
+  __device__ __forceinline__ explicit Div(float d) {
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  }
+  __device__ __forceinline__ float operator()(float x) const { return x * r; }
+};
+
 // Fortran SIGN(x, a) = |x| with the sign of a.
 template <typename R> __device__ __forceinline__ R fsign(R x, R a) { return d_copysign(d_fabs(x), a); }
 
@@ -244,9 +262,10 @@ __device__ __forceinline__ void cons2prim(const R* u, R* q, const Phys<R>& P) {
     return;
   }
   q[V::DN] = u[V::DN];
-  q[V::VX] = u[V::VX] / u[V::DN];
-  q[V::VY] = u[V::VY] / u[V::DN];
-  q[V::VZ] = u[V::VZ] / u[V::DN];
+  const Div<R> by_dn(u[V::DN]);
+  q[V::VX] = by_dn(u[V::VX]);
+  q[V::VY] = by_dn(u[V::VY]);
+  q[V::VZ] = by_dn(u[V::VZ]);
   if constexpr (!V::MHD) {
     R ek = R(0.5) * (u[V::VX] * q[V::VX] + u[V::VY] * q[V::VY] + u[V::VZ] * q[V::VZ]);
     R ei = u[V::EN] - ek;
@@ -425,6 +444,82 @@ __device__ __forceinline__ void weno5z_faces(R fm2, R fm1, R f0, R fp1, R fp2, R
   qc = a21 * fp1 + a22 * f0 + a23 * fm1;
   qr = a31 * f0 + a32 * fm1 + a33 * fm2;
   fL = (wl * ql + wr * qr) + wc * qc;
+}
+
+// ---------------------------------------------------------------------------
+// WENO-Z faces for the FP32-bulk mode: the same scheme with fewer divisions
+// and two variables per instruction.  The weights need 1/(beta + eps) of the
+// three substencils; 1/(x_l x_c) gives the first two with one reciprocal
+// (x >= eps, so the product stays a normal float for eps = epsilon(1d0)),
+// and each face is normalised once: fR = (sum_k w_k q_k) / (sum_k w_k).
+// Four reciprocals per variable instead of seven divisions.  The lane type
+// is float (one variable) or float2 (two variables, packed f32x2
+// arithmetic); both give the same per-variable results.  FP64 keeps
+// weno5z_faces, which follows the reference operation by operation.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float lane_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float lane_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float lane_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float lane_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float lane_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float lane_abs(float a) { return fabsf(a); }
+__device__ __forceinline__ float lane_set(float a) { return a; }
+__device__ __forceinline__ float2 lane_rcp(float2 x) { return make_float2(lane_rcp(x.x), lane_rcp(x.y)); }
+__device__ __forceinline__ float2 lane_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 lane_sub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);  // a - b, rounded once
+}
+__device__ __forceinline__ float2 lane_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 lane_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 lane_abs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+template <typename T> __device__ __forceinline__ T lane_bcast(float a);
+template <> __device__ __forceinline__ float lane_bcast<float>(float a) { return a; }
+template <> __device__ __forceinline__ float2 lane_bcast<float2>(float a) { return make_float2(a, a); }
+
+template <typename T>
+__device__ __forceinline__ void weno5z_faces_fast(T fm2, T fm1, T f0, T fp1, T fp2, float eps, T& fR, T& fL) {
+  const T c1 = lane_bcast<T>(13.0f / 12.0f), c2 = lane_bcast<T>(0.25f), three = lane_bcast<T>(3.0f);
+  const T dl = lane_bcast<T>(0.1f), dc = lane_bcast<T>(0.6f), dr = lane_bcast<T>(0.3f);
+  const T one = lane_bcast<T>(1.0f), ep = lane_bcast<T>(eps);
+  const T a11 = lane_bcast<T>(2.0f / 6.0f), a12 = lane_bcast<T>(-7.0f / 6.0f), a13 = lane_bcast<T>(11.0f / 6.0f);
+  const T a21 = lane_bcast<T>(-1.0f / 6.0f), a22 = lane_bcast<T>(5.0f / 6.0f), a23 = lane_bcast<T>(2.0f / 6.0f);
+  const T dm1 = lane_sub(fm1, fm2), d0m = lane_sub(f0, fm1), d0p = lane_sub(fp1, f0), dp1 = lane_sub(fp2, fp1);
+  // smoothness indicators of the left, central and right substencils
+  T t = lane_sub(d0m, dm1), u = lane_sub(lane_mul(three, d0m), dm1);
+  const T bl = lane_fma(c1, lane_mul(t, t), lane_mul(c2, lane_mul(u, u)));
+  t = lane_sub(d0p, d0m); u = lane_add(d0p, d0m);
+  const T bc = lane_fma(c1, lane_mul(t, t), lane_mul(c2, lane_mul(u, u)));
+  t = lane_sub(dp1, d0p); u = lane_sub(lane_mul(three, d0p), dp1);
+  const T br = lane_fma(c1, lane_mul(t, t), lane_mul(c2, lane_mul(u, u)));
+  const T tau = lane_abs(lane_sub(br, bl));
+  const T xl = lane_add(bl, ep), xc = lane_add(bc, ep), xr = lane_add(br, ep);
+  const T rlc = lane_rcp(lane_mul(xl, xc));
+  const T al = lane_fma(tau, lane_mul(xc, rlc), one);
+  const T ac = lane_fma(tau, lane_mul(xl, rlc), one);
+  const T ar = lane_fma(tau, lane_rcp(xr), one);
+  const T wc = lane_mul(dc, ac);
+  // right face: weights 0.1 al, 0.6 ac, 0.3 ar on the candidate states
+  {
+    const T ql = lane_fma(a11, fm2, lane_fma(a12, fm1, lane_mul(a13, f0)));
+    const T qc = lane_fma(a21, fm1, lane_fma(a22, f0, lane_mul(a23, fp1)));
+    const T qr = lane_fma(a11, f0, lane_fma(a22, fp1, lane_mul(a21, fp2)));
+    const T wl = lane_mul(dl, al), wr = lane_mul(dr, ar);
+    const T num = lane_fma(wl, ql, lane_fma(wr, qr, lane_mul(wc, qc)));
+    fR = lane_mul(num, lane_rcp(lane_add(lane_add(wl, wr), wc)));
+  }
+  // left face: the mirrored stencils, weights 0.1 ar, 0.6 ac, 0.3 al
+  {
+    const T ql = lane_fma(a11, fp2, lane_fma(a12, fp1, lane_mul(a13, f0)));
+    const T qc = lane_fma(a21, fp1, lane_fma(a22, f0, lane_mul(a23, fm1)));
+    const T qr = lane_fma(a11, f0, lane_fma(a22, fm1, lane_mul(a21, fm2)));
+    const T wl = lane_mul(dl, ar), wr = lane_mul(dr, al);
+    const T num = lane_fma(wl, ql, lane_fma(wr, qr, lane_mul(wc, qc)));
+    fL = lane_mul(num, lane_rcp(lane_add(lane_add(wl, wr), wc)));
+  }
 }
 
 // clip_extrema src/interpolations.F90:5081-5175 restated per cell: the cell's
@@ -1069,12 +1164,13 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       return;
     }
     R srml = sr - sl;
+    const Div<R> by_srml(srml);
     R wl[NV], wr[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) { wl[v] = sl * ul[v] - fl[v]; wr[v] = sr * ur[v] - fr[v]; }
     if constexpr (RS == RS_HLL || V::SR) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+      for (int v = 0; v < NV; ++v) f[v] = by_srml(sl * wr[v] - sr * wl[v]);
       return;
     } else if constexpr (V::ISO) {
       static_assert(V::MHD && (RS == RS_HLLD || RS == RS_HLLDM), "isothermal: HLL, Roe, HLLD, HLLD-M");
@@ -1084,24 +1180,25 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       // HD HLLC
       R ui[NV];
       R dn = wr[Dn] - wl[Dn];
-      R sm = (wr[Mx] - wl[Mx]) / dn;
-      R pr = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn;
+      const Div<R> by_dn(dn);
+      R sm = by_dn(wr[Mx] - wl[Mx]);
+      R pr = by_dn(wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]);
       if (sm > R(0)) {
-        R slmm = sl - sm;
-        ui[Dn] = wl[Dn] / slmm;
+        const Div<R> by_slmm(sl - sm);
+        ui[Dn] = by_slmm(wl[Dn]);
         ui[Mx] = ui[Dn] * sm;
         ui[My] = ui[Dn] * ql[My];
         ui[Mz] = ui[Dn] * ql[Mz];
-        ui[En] = (wl[En] + sm * pr) / slmm;
+        ui[En] = by_slmm(wl[En] + sm * pr);
 #pragma unroll
         for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
       } else if (sm < R(0)) {
-        R srmm = sr - sm;
-        ui[Dn] = wr[Dn] / srmm;
+        const Div<R> by_srmm(sr - sm);
+        ui[Dn] = by_srmm(wr[Dn]);
         ui[Mx] = ui[Dn] * sm;
         ui[My] = ui[Dn] * qr[My];
         ui[Mz] = ui[Dn] * qr[Mz];
-        ui[En] = (wr[En] + sm * pr) / srmm;
+        ui[En] = by_srmm(wr[En] + sm * pr);
 #pragma unroll
         for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
       } else {
@@ -1112,16 +1209,17 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       constexpr int Bx = V::BX, By = V::BY, Bz = V::BZ, Bp = V::BP;
       R ui[NV];
       R dn = wr[Dn] - wl[Dn];
-      R sm = (wr[Mx] - wl[Mx]) / dn;
+      const Div<R> by_dn(dn);
+      R sm = by_dn(wr[Mx] - wl[Mx]);
       if constexpr (RS == RS_HLLC) {
         R bx = ql[Bx];
         R b2 = ql[Bx] * qr[Bx];
         if (b2 > R(0)) {
           R pt = R(0.5) * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx])) + b2;
-          R vy = (wr[My] - wl[My]) / dn;
-          R vz = (wr[Mz] - wl[Mz]) / dn;
-          R by = (wr[By] - wl[By]) / srml;
-          R bz = (wr[Bz] - wl[Bz]) / srml;
+          R vy = by_dn(wr[My] - wl[My]);
+          R vz = by_dn(wr[Mz] - wl[Mz]);
+          R by = by_srml(wr[By] - wl[By]);
+          R bz = by_srml(wr[Bz] - wl[Bz]);
           R vb = sm * bx + vy * by + vz * bz;
           if (sm > R(0)) {
             R slmm = sl - sm;
@@ -1139,7 +1237,7 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
             for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
           } else {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+            for (int v = 0; v < NV; ++v) f[v] = by_srml(sl * wr[v] - sr * wl[v]);
           }
         } else {
           R pt = R(0.5) * ((wl[Dn] * sm - wl[Mx]) + (wr[Dn] * sm - wr[Mx]));
@@ -1166,30 +1264,33 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
       } else {
         // MHD HLLD
         R slmm = sl - sm, srmm = sr - sm;
-        R dnl = wl[Dn] / slmm, dnr = wr[Dn] / srmm;
+        const Div<R> by_slmm(slmm), by_srmm(srmm);
+        R dnl = by_slmm(wl[Dn]), dnr = by_srmm(wr[Dn]);
         R bx = ql[Bx];
         R b2 = ql[Bx] * qr[Bx];
-        R pt = (wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) / dn + b2;
+        R pt = by_dn(wl[Dn] * wr[Mx] - wr[Dn] * wl[Mx]) + b2;
         R vy, vz, by, bz, vb, dvl = R(0), dvr = R(0);
         auto outer_left = [&]() {
-          vy = (slmm * wl[My] - bx * wl[By]) / dvl;
-          vz = (slmm * wl[Mz] - bx * wl[Bz]) / dvl;
-          by = (wl[Dn] * wl[By] - bx * wl[My]) / dvl;
-          bz = (wl[Dn] * wl[Bz] - bx * wl[Mz]) / dvl;
+          const Div<R> by_dvl(dvl);
+          vy = by_dvl(slmm * wl[My] - bx * wl[By]);
+          vz = by_dvl(slmm * wl[Mz] - bx * wl[Bz]);
+          by = by_dvl(wl[Dn] * wl[By] - bx * wl[My]);
+          bz = by_dvl(wl[Dn] * wl[Bz] - bx * wl[Mz]);
           vb = sm * bx + vy * by + vz * bz;
           ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
           ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
-          ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+          ui[En] = by_slmm(wl[En] + sm * pt - bx * vb);
         };
         auto outer_right = [&]() {
-          vy = (srmm * wr[My] - bx * wr[By]) / dvr;
-          vz = (srmm * wr[Mz] - bx * wr[Bz]) / dvr;
-          by = (wr[Dn] * wr[By] - bx * wr[My]) / dvr;
-          bz = (wr[Dn] * wr[Bz] - bx * wr[Mz]) / dvr;
+          const Div<R> by_dvr(dvr);
+          vy = by_dvr(srmm * wr[My] - bx * wr[By]);
+          vz = by_dvr(srmm * wr[Mz] - bx * wr[Bz]);
+          by = by_dvr(wr[Dn] * wr[By] - bx * wr[My]);
+          bz = by_dvr(wr[Dn] * wr[Bz] - bx * wr[Mz]);
           vb = sm * bx + vy * by + vz * bz;
           ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
           ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
-          ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+          ui[En] = by_srmm(wr[En] + sm * pt - bx * vb);
         };
         if (b2 > R(1.0e-08) * d_max(dnl * (sl * sl), dnr * (sr * sr))) {
           R cal = d_sqrt(b2 / dnl), car = d_sqrt(b2 / dnr);
@@ -1213,12 +1314,12 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
               outer_right();
 #pragma unroll
               for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
-              R dv = car * dnr + cal * dnl;
-              vy = (wcr[My] - wcl[My]) / dv;
-              vz = (wcr[Mz] - wcl[Mz]) / dv;
-              dv = car + cal;
-              by = (wcr[By] - wcl[By]) / dv;
-              bz = (wcr[Bz] - wcl[Bz]) / dv;
+              const Div<R> by_dv(car * dnr + cal * dnl);
+              vy = by_dv(wcr[My] - wcl[My]);
+              vz = by_dv(wcr[Mz] - wcl[Mz]);
+              const Div<R> by_dc(car + cal);
+              by = by_dc(wcr[By] - wcl[By]);
+              bz = by_dc(wcr[Bz] - wcl[Bz]);
               vb = sm * bx + vy * by + vz * bz;
               if (sm > R(0)) {
                 ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
@@ -1247,12 +1348,12 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
                 R wcl[NV];
 #pragma unroll
                 for (int v = 0; v < NV; ++v) wcl[v] = (sml - sl) * ui[v] + wl[v];
-                R dv = srmm * dnr + cal * dnl;
-                vy = (wr[My] - wcl[My]) / dv;
-                vz = (wr[Mz] - wcl[Mz]) / dv;
-                dv = sr - sml;
-                by = (wr[By] - wcl[By]) / dv;
-                bz = (wr[Bz] - wcl[Bz]) / dv;
+                const Div<R> by_dv(srmm * dnr + cal * dnl);
+                vy = by_dv(wr[My] - wcl[My]);
+                vz = by_dv(wr[Mz] - wcl[Mz]);
+                const Div<R> by_dc(sr - sml);
+                by = by_dc(wr[By] - wcl[By]);
+                bz = by_dc(wr[Bz] - wcl[Bz]);
                 vb = sm * bx + vy * by + vz * bz;
                 ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
                 ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
@@ -1264,7 +1365,7 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
 #pragma unroll
                   for (int v = 0; v < NV; ++v) {
                     R wcr = (sm - sml) * ui[v] + wcl[v];
-                    f[v] = (sm * wr[v] - sr * wcr) / srmm;
+                    f[v] = by_srmm(sm * wr[v] - sr * wcr);
                   }
                 }
               }
@@ -1277,12 +1378,12 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
                 R wcr[NV];
 #pragma unroll
                 for (int v = 0; v < NV; ++v) wcr[v] = (smr - sr) * ui[v] + wr[v];
-                R dv = slmm * dnl - car * dnr;
-                vy = (wl[My] - wcr[My]) / dv;
-                vz = (wl[Mz] - wcr[Mz]) / dv;
-                dv = sl - smr;
-                by = (wl[By] - wcr[By]) / dv;
-                bz = (wl[Bz] - wcr[Bz]) / dv;
+                const Div<R> by_dv(slmm * dnl - car * dnr);
+                vy = by_dv(wl[My] - wcr[My]);
+                vz = by_dv(wl[Mz] - wcr[Mz]);
+                const Div<R> by_dc(sl - smr);
+                by = by_dc(wl[By] - wcr[By]);
+                bz = by_dc(wl[Bz] - wcr[Bz]);
                 vb = sm * bx + vy * by + vz * bz;
                 ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
                 ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
@@ -1294,53 +1395,53 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
 #pragma unroll
                   for (int v = 0; v < NV; ++v) {
                     R wcl = (sm - smr) * ui[v] + wcr[v];
-                    f[v] = (sm * wl[v] - sl * wcl) / slmm;
+                    f[v] = by_slmm(sm * wl[v] - sl * wcl);
                   }
                 }
               }
             } else {
 #pragma unroll
-              for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+              for (int v = 0; v < NV; ++v) f[v] = by_srml(sl * wr[v] - sr * wl[v]);
             }
           }
         } else if (b2 > R(0)) {
-          vy = (wr[My] - wl[My]) / dn;
-          vz = (wr[Mz] - wl[Mz]) / dn;
-          by = (wr[By] - wl[By]) / srml;
-          bz = (wr[Bz] - wl[Bz]) / srml;
+          vy = by_dn(wr[My] - wl[My]);
+          vz = by_dn(wr[Mz] - wl[Mz]);
+          by = by_srml(wr[By] - wl[By]);
+          bz = by_srml(wr[Bz] - wl[Bz]);
           vb = sm * bx + vy * by + vz * bz;
           if (sm > R(0)) {
             ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = dnl * vy; ui[Mz] = dnl * vz;
             ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ul[Bp];
-            ui[En] = (wl[En] + sm * pt - bx * vb) / slmm;
+            ui[En] = by_slmm(wl[En] + sm * pt - bx * vb);
 #pragma unroll
             for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
           } else if (sm < R(0)) {
             ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = dnr * vy; ui[Mz] = dnr * vz;
             ui[Bx] = bx; ui[By] = by; ui[Bz] = bz; ui[Bp] = ur[Bp];
-            ui[En] = (wr[En] + sm * pt - bx * vb) / srmm;
+            ui[En] = by_srmm(wr[En] + sm * pt - bx * vb);
 #pragma unroll
             for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
           } else {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+            for (int v = 0; v < NV; ++v) f[v] = by_srml(sl * wr[v] - sr * wl[v]);
           }
         } else {
           if (sm > R(0)) {
-            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = wl[My] / slmm; ui[Mz] = wl[Mz] / slmm;
-            ui[Bx] = R(0); ui[By] = wl[By] / slmm; ui[Bz] = wl[Bz] / slmm; ui[Bp] = ul[Bp];
-            ui[En] = (wl[En] + sm * pt) / slmm;
+            ui[Dn] = dnl; ui[Mx] = dnl * sm; ui[My] = by_slmm(wl[My]); ui[Mz] = by_slmm(wl[Mz]);
+            ui[Bx] = R(0); ui[By] = by_slmm(wl[By]); ui[Bz] = by_slmm(wl[Bz]); ui[Bp] = ul[Bp];
+            ui[En] = by_slmm(wl[En] + sm * pt);
 #pragma unroll
             for (int v = 0; v < NV; ++v) f[v] = sl * ui[v] - wl[v];
           } else if (sm < R(0)) {
-            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = wr[My] / srmm; ui[Mz] = wr[Mz] / srmm;
-            ui[Bx] = R(0); ui[By] = wr[By] / srmm; ui[Bz] = wr[Bz] / srmm; ui[Bp] = ur[Bp];
-            ui[En] = (wr[En] + sm * pt) / srmm;
+            ui[Dn] = dnr; ui[Mx] = dnr * sm; ui[My] = by_srmm(wr[My]); ui[Mz] = by_srmm(wr[Mz]);
+            ui[Bx] = R(0); ui[By] = by_srmm(wr[By]); ui[Bz] = by_srmm(wr[Bz]); ui[Bp] = ur[Bp];
+            ui[En] = by_srmm(wr[En] + sm * pt);
 #pragma unroll
             for (int v = 0; v < NV; ++v) f[v] = sr * ui[v] - wr[v];
           } else {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) f[v] = (sl * wr[v] - sr * wl[v]) / srml;
+            for (int v = 0; v < NV; ++v) f[v] = by_srml(sl * wr[v] - sr * wl[v]);
           }
         }
         return;

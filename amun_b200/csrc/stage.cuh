@@ -245,12 +245,35 @@ __global__ void __launch_bounds__(StageShape<TY>::NT, AMUN_STAGE_MIN_BLOCKS)
   // WENO-Z faces (with clip_extrema / fix_positivity) of one cell from five
   // stencil values per variable: p[o] + v * vs is variable v at offset o-2
   auto faces = [&](const R* const* p, long long vs, R* fR, R* fL) {
+    constexpr bool fast = std::is_same<R, float>::value;
+    if constexpr (fast) {
+      // FP32 bulk: two variables per instruction (weno5z_faces_fast)
+#pragma unroll
+      for (int v = 0; v + 1 < NV; v += 2) {
+        const long long o = (long long)v * vs;
+        float2 st[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) st[q] = make_float2(p[q][o], p[q][o + vs]);
+        float2 r, l;
+        weno5z_faces_fast(st[0], st[1], st[2], st[3], st[4], (float)a.m.eps, r, l);
+        fR[v] = r.x; fR[v + 1] = r.y; fL[v] = l.x; fL[v + 1] = l.y;
+      }
+      if constexpr (NV & 1) {
+        const long long o = (long long)(NV - 1) * vs;
+        weno5z_faces_fast(p[0][o], p[1][o], p[2][o], p[3][o], p[4][o], (float)a.m.eps, fR[NV - 1], fL[NV - 1]);
+      }
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const long long o = (long long)v * vs;
       const R fm2 = p[0][o], fm1 = p[1][o], f0 = p[2][o], fp1 = p[3][o], fp2 = p[4][o];
       R r, l;
-      weno5z_faces(fm2, fm1, f0, fp1, fp2, eps, r, l);
+      if constexpr (fast) {
+        r = fR[v];
+        l = fL[v];
+      } else {
+        weno5z_faces(fm2, fm1, f0, fp1, fp2, eps, r, l);
+      }
       const bool positive = (v == V::DN || v == V::PR);
       if (a.m.clip) clip_cell(fm1, f0, fp1, a.m.clim, eps, r, l);
       if (positive && a.m.positivity && (r <= R(0) || l <= R(0))) { r = f0; l = f0; }

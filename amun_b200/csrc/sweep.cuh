@@ -20,6 +20,7 @@
 //   U1 [b][v][k][j][i]   interior only, stage state (FP64, or FP32 in bulk)
 //   du [b][v][k][j][i]   interior only, increment in the working precision
 #pragma once
+#include <type_traits>
 #include "physics.cuh"
 
 namespace amun {
@@ -325,7 +326,10 @@ __device__ __forceinline__ void mlp_faces(const R* qb, const Geo& g, bool four, 
   }
 }
 
-template <int EQ, int REC, int RS, int DIR, typename R, typename U1T>
+// TLP x TLW > 0: the tile shape fixed at compile time (a.LP, a.LW must equal
+// it), so every shared-memory index and task split folds to constants;
+// 0 x 0: the shape is read from the arguments
+template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0>
 #ifndef AMUN_SWEEP_MIN_BLOCKS
 #define AMUN_SWEEP_MIN_BLOCKS 1
 #endif
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   const bool four = V::SR && a.m.states_4vec;
   constexpr int RR = REC == REC_WENO5Z ? 2 : (REC == REC_GEN ? 3 : 1);
   const Geo& g = a.g;
-  const int LP = a.LP, LW = a.LW;
+  const int LP = TLP ? TLP : a.LP, LW = TLW ? TLW : a.LW;
   const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
   R* Qs = sm;
   R* FLs = Qs + (size_t)NV * NPQ * LW;
@@ -524,8 +528,34 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       int pp, ll; decode(t, NPF, pp, ll);
       const int cq = pp + RR;  // index of this cell in Qs
       R fRv[NV], fLv[NV];
+      constexpr bool fast = REC == REC_WENO5Z && std::is_same<R, float>::value;
+      if constexpr (fast) {
+        // FP32 bulk: two variables per instruction (weno5z_faces_fast)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
+        for (int v = 0; v + 1 < NV; v += 2) {
+          float2 st[5];
+#pragma unroll
+          for (int o = 0; o < 5; ++o)
+            st[o] = make_float2(Qs[sidx(v, cq - 2 + o, ll, NPQ)], Qs[sidx(v + 1, cq - 2 + o, ll, NPQ)]);
+          float2 r, l;
+          weno5z_faces_fast(st[0], st[1], st[2], st[3], st[4], (float)a.m.eps, r, l);
+          fRv[v] = r.x; fRv[v + 1] = r.y; fLv[v] = l.x; fLv[v + 1] = l.y;
+        }
+        if constexpr (NV & 1) {
+          float st[5];
+#pragma unroll
+          for (int o = 0; o < 5; ++o) st[o] = Qs[sidx(NV - 1, cq - 2 + o, ll, NPQ)];
+          weno5z_faces_fast(st[0], st[1], st[2], st[3], st[4], (float)a.m.eps, fRv[NV - 1], fLv[NV - 1]);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const bool positive = (v == V::DN || v == V::PR);
+          dir_fix(Qs[sidx(v, cq - 1, ll, NPQ)], Qs[sidx(v, cq, ll, NPQ)], Qs[sidx(v, cq + 1, ll, NPQ)], positive,
+                  fRv[v], fLv[v]);
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV && !fast; ++v) {
         R fR, fL;
         const R f0 = Qs[sidx(v, cq, ll, NPQ)];
         const R fm1 = Qs[sidx(v, cq - 1, ll, NPQ)], fp1 = Qs[sidx(v, cq + 1, ll, NPQ)];

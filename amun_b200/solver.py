@@ -27,7 +27,7 @@ class Simulation:
     def __init__(self, params: dict, precision: str = "fp64", mesh=None):
         self.params = dict(params)
         self.params["precision"] = precision
-        self.L = N.lib()
+        self.L = N.ContextLib()  # this Simulation's own library context
         self.native = to_native(self.params)
         self.geo = geometry(self.params)
         self.mesh = UniformMesh(self.geo) if mesh is None else mesh
@@ -195,6 +195,17 @@ class Simulation:
                     nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes,
                     unphysical_cells=s.unphysical_cells, stalls=s.stalls)
 
+    def stages(self) -> int:
+        """Number of stages of the selected integrator."""
+        n = C.c_int()
+        N.check(self.L.amun_gpu_stages(C.byref(n)))
+        return n.value
+
+    def stage(self, s: int, t: float, dt: float):
+        """Stage s (1-based) of the selected integrator with the step's time
+        and dt (the per-stage body of evolve_*)."""
+        N.check(self.L.amun_gpu_stage(int(s), float(t), float(dt)))
+
     def set_stage_kernel(self, mode: int = 1, planes: int = 0) -> bool:
         """1: one fused launch per stage where it covers the configuration,
         0: one sweep per direction; planes > 0 sets the z planes per tile of
@@ -297,3 +308,4 @@ class Simulation:
 
     def close(self):
         self.L.amun_gpu_finalize()
+        self.L.destroy()

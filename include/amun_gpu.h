@@ -245,6 +245,21 @@ int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt);
  * including ghost fill and primitive update after each stage. */
 int amun_gpu_evolve(void);
 
+/* One stage of the selected integrator, for a caller that does its own
+ * work between stages (the per-stage body of evolve_*, e.g. evolve_rk2
+ * src/evolution.F90:681-704 and 729-753: update_fluxes, update_increment,
+ * the stage combination, update_variables).  s counts from 1 to the number
+ * of stages (amun_gpu_stages); t and dt are the step's time and time step
+ * (dt becomes the module dt the stages use).  Stage 1 also copies U^n into
+ * the stage array where the integrator starts so (evolve_ssprk2); the final
+ * stage applies the GLM psi decay and leaves the new state's maximum speed
+ * for the next new_time_step.  Calling stages 1..n in order with the dt of
+ * new_time_step gives the results of amun_gpu_evolve bit for bit.  The time
+ * is not advanced (the driver does that, src/driver.F90:579-585). */
+int amun_gpu_stage(int s, double t, double dt);
+/* The number of stages of the selected integrator. */
+int amun_gpu_stages(int* nstages);
+
 /* advance (src/evolution.F90:292-372, single-level mesh) followed by the
  * driver's time/step update (src/driver.F90:579-585). */
 int amun_gpu_advance(double dtnext, double* time, double* dt);

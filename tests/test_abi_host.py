@@ -151,3 +151,43 @@ def test_mesh_descriptors_periodic():
         assert right == ((bx + 1) % 3) + 3 * by
         assert d[b].neighbor[0] == -1 or True
         assert all(d[b].neighbor[n] == -1 for n in range(27) if n // 9 != 1)
+
+
+def test_contexts_are_independent():
+    """Each library context keeps its own state and error text; selecting
+    a handle that amun_gpu_context_create did not make is refused, and the
+    default context comes back with NULL."""
+    L = N.lib()
+    a, b = C.c_void_p(), C.c_void_p()
+    assert L.amun_gpu_context_create(C.byref(a)) == 0
+    assert L.amun_gpu_context_create(C.byref(b)) == 0
+    try:
+        assert a.value != b.value
+        assert L.amun_gpu_context_select(a) == 0
+        assert L.amun_gpu_evolve() == N.AMUN_E_NOT_INITIALIZED
+        assert b"amun_gpu_init" in L.amun_gpu_last_error()
+        assert L.amun_gpu_context_select(b) == 0
+        assert L.amun_gpu_last_error() == b""
+        assert L.amun_gpu_context_select(a) == 0
+        assert b"amun_gpu_init" in L.amun_gpu_last_error()
+        bogus = C.c_void_p(12345)
+        assert L.amun_gpu_context_select(bogus) == N.AMUN_E_BAD_ARGUMENT
+        assert L.amun_gpu_context_select(None) == 0
+    finally:
+        assert L.amun_gpu_context_destroy(a) == 0
+        assert L.amun_gpu_context_destroy(b) == 0
+    assert L.amun_gpu_context_destroy(a) == N.AMUN_E_BAD_ARGUMENT
+
+
+def test_context_lib_selects_its_context():
+    """ContextLib (the binding each Simulation uses) makes its own context
+    current before every call."""
+    x, y = N.ContextLib(), N.ContextLib()
+    try:
+        assert x.amun_gpu_stage(1, 0.0, 1e-3) == N.AMUN_E_NOT_INITIALIZED
+        assert b"amun_gpu_init" in N.lib().amun_gpu_last_error()
+        y.amun_gpu_wait_posted  # binding only, no call
+        assert y.amun_gpu_stages(C.byref(C.c_int())) == N.AMUN_E_NOT_INITIALIZED
+    finally:
+        x.destroy()
+        y.destroy()

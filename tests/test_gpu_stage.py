@@ -129,8 +129,10 @@ def test_graph_replay_matches_eager(Sim):
 @pytest.mark.parametrize("eq,rs,nd", [("mhd", "hlld", 3), ("hd", "hllc", 3), ("mhd", "hll", 2)])
 def test_fp32_fused_matches_fp32_sweeps(Sim, eq, rs, nd):
     """FP32 bulk: the fused kernel and the per-direction sweeps compute the
-    same FP32 arithmetic; after 5 steps they agree to 1e-6 (L1 relative of
-    every conserved variable)."""
+    same scheme in FP32 (their roundings differ where the compiler contracts
+    differently); after 5 steps they agree to 1e-6, L1 relative per
+    conserved variable.  The GLM scalar psi starts at zero and stays near
+    round-off size, so it is measured against the magnetic field's scale."""
     p = unit_box(params(eq, "weno5z", rs, "rk3", ndims=nd, ncells=32))
     a, b = Sim(p, precision="fp32"), Sim(p, precision="fp32")
     try:
@@ -143,7 +145,8 @@ def test_fp32_fused_matches_fp32_sweeps(Sim, eq, rs, nd):
                 s.advance(1.0e30)
         ua, ub = a.conserved(), b.conserved()
         for v in range(ua.shape[-1]):
-            den = np.sum(np.abs(ub[..., v])) or 1.0
+            ref = 4 if (eq == "mhd" and v == 7) else v  # psi against Bx
+            den = np.sum(np.abs(ub[..., ref])) or 1.0
             assert np.sum(np.abs(ua[..., v] - ub[..., v])) / den <= 1e-6, v
         assert a.status()["stalls"] == 0
     finally:
@@ -169,3 +172,45 @@ def test_stage_kernel_coverage(Sim):
             assert not s.set_stage_kernel(1)
         finally:
             s.close()
+
+
+@pytest.mark.parametrize("ta", ["rk2", "rk3", "ssprk(m,2)", "ssprk(5,3)"])
+@pytest.mark.parametrize("fused", [0, 1])
+def test_stage_by_stage_equals_evolve(Sim, ta, fused):
+    """amun_gpu_stage called for stages 1..n with the dt of new_time_step
+    gives the state of amun_gpu_evolve bit for bit (the per-stage drop-in of
+    evolve_*), with the sweeps and with the fused kernel."""
+    p = unit_box(params("mhd", "weno5z", "hlld", ta, ndims=3, ncells=16, xblocks=2, yblocks=1, zblocks=1))
+    a, b = Sim(p), Sim(p)
+    try:
+        q0 = problems.turbulence(a.mesh, 5.0 / 3.0, seed=6)
+        for s in (a, b):
+            s.set_stage_kernel(fused, 8)
+            s.set_primitive(q0)
+        t = 0.0
+        for _ in range(3):
+            _, dta = a.new_time_step(1.0e30)
+            a.evolve()
+            _, dtb = b.new_time_step(1.0e30)
+            assert dta == dtb
+            for st in range(1, b.stages() + 1):
+                b.stage(st, t, dtb)
+            t += dta
+        assert_same(a.conserved(), b.conserved(), f"stages of {ta}")
+        assert_same(a.primitive(), b.primitive(), "primitives")
+    finally:
+        a.close()
+        b.close()
+
+
+def test_stage_rejects_bad_arguments(Sim):
+    from amun_b200 import _native as N
+    p = unit_box(params("hd", "weno5z", "hllc", "rk3", ndims=2, ncells=16))
+    s = Sim(p)
+    try:
+        assert s.stages() == 3
+        assert s.L.amun_gpu_stage(0, 0.0, 1e-3) == N.AMUN_E_BAD_ARGUMENT
+        assert s.L.amun_gpu_stage(4, 0.0, 1e-3) == N.AMUN_E_BAD_ARGUMENT
+        assert s.L.amun_gpu_stage(1, 0.0, 0.0) == N.AMUN_E_BAD_ARGUMENT
+    finally:
+        s.close()
