@@ -112,6 +112,7 @@ def lib():
         "amun_gpu_context_destroy": (i, [vp]),
         "amun_gpu_stage": (i, [i, d, d]),
         "amun_gpu_stages": (i, [C.POINTER(i)]),
+        "amun_gpu_integrals": (i, [_D]),
         "amun_gpu_forward_checkpointed": (i, [i, d, i]),
         "amun_gpu_replay": (i, [i]),
         "amun_gpu_adjoint": (i, [_D, _D, _D]),

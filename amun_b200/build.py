@@ -51,6 +51,7 @@ UNITS = {
     "adjoint.cu": FP64,
     "kernels_fp64.cu": FP64,
     "regrid.cu": FP64,
+    "integrals.cu": FP64,
     "kernels_fp64_hd.cu": FP64_SWEEP,
     "kernels_fp64_mhd.cu": FP64_SWEEP,
     "kernels_fp64_srmhd.cu": FP64_SWEEP,

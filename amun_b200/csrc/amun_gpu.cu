@@ -22,6 +22,7 @@
 #include "../../include/amun_gpu.h"
 #include "adjoint.h"
 #include "gp_weights.h"
+#include "integrals.h"
 #include "launch.cuh"
 #include "regrid.h"
 #include "stage.cuh"
@@ -130,6 +131,9 @@ struct Ctx {
   int stage_ks = 32;
   // the recorded forward run of the discrete adjoint
   AdjCtx adj;
+  // store_integrals: CTA partials and the 29 results
+  double* int_buf = nullptr;
+  int int_cap = 0;
 };
 
 // Contexts: every host thread works on its current context, which is its
@@ -277,6 +281,9 @@ void free_pool() {
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   C.stage_maps = false;
+  if (C.int_buf) cudaFree(C.int_buf);
+  C.int_buf = nullptr;
+  C.int_cap = 0;
   if (C.u0) cudaFree(C.u0);
   if (C.u1) cudaFree(C.u1);
   if (C.du) cudaFree(C.du);
@@ -1449,6 +1456,36 @@ int amun_gpu_evolve(void) {
   CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
   if ((r = evolve_launches())) return r;
   C.ms_valid = true;
+  CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_integrals(double* out) {
+  int r = check_ready();
+  if (r) return r;
+  if (!out) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  const int np = integrals_partials(C.g.uvs * C.nblocks);
+  if (C.int_cap < np) {
+    if (C.int_buf) cudaFree(C.int_buf);
+    C.int_buf = nullptr;
+    C.int_cap = 0;
+    CK(cudaMalloc(&C.int_buf, ((size_t)np * 42 + 32) * sizeof(double)));
+    C.int_cap = np;
+  }
+  // the domain volume: the leaves cover it (voli of src/coordinates.F90:290)
+  const int nd = C.g.ndims;
+  double vol = 0.0;
+  for (const auto& b : C.blocks) {
+    const double cells = nd == 3 ? (double)C.g.nc * C.g.nc * C.g.nc : (double)C.g.nc * C.g.nc;
+    vol += cells * b.dx[0] * b.dx[1] * (nd == 3 ? b.dx[2] : 1.0);
+  }
+  double* res = C.int_buf + (size_t)C.int_cap * 42;
+  cudaError_t e = bulk() ? run_integrals<float>(C.p.eqsys, C.u0, (const float*)C.q[C.cur], C.g, C.bdx, C.nblocks,
+                                                C.gamma, C.p.csnd, 1.0 / vol, C.int_buf, res, C.stream)
+                         : run_integrals<double>(C.p.eqsys, C.u0, (const double*)C.q[C.cur], C.g, C.bdx, C.nblocks,
+                                                 C.gamma, C.p.csnd, 1.0 / vol, C.int_buf, res, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "integrals");
+  CK(cudaMemcpyAsync(out, res, 29 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
   CK(cudaStreamSynchronize(C.stream));
   return 0;
 }

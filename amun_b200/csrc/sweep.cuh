@@ -374,6 +374,24 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     else { pp = t / LW; ll = t - pp * LW; }
   };
 
+  // ---- the last direction's stage operands (U^n and the stage state of the
+  // tile's cells) are requested into L2 now, so that the combination after
+  // the Riemann problems finds them there
+  if (a.last) {
+    for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
+      int pp, ll;
+      if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
+      const long long ci = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP + (long long)(l0 - ng + ll) * iL +
+                           (long long)(g.ndims == 3 ? th : 0) * iT;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const long long o = ci + v * g.uvs;
+        if (a.st.a_src == 0 || (a.st.form != 0 && a.st.b_src == 0)) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u0 + o));
+        if (a.st.a_src == 1 || (a.st.form != 0 && a.st.b_src == 1)) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u1 + o));
+      }
+    }
+  }
+
   // ---- load the tile and its halo --------------------------------------------
   // (the generic variant's three-cell halo is clamped to the block: methods
   // with shorter stencils run with fewer ghost layers and never read it)

@@ -195,6 +195,20 @@ class Simulation:
                     nonpositive=s.nonpositive, c2p_failures=s.c2p_failures, device_bytes=s.device_bytes,
                     unphysical_cells=s.unphysical_cells, stalls=s.stalls)
 
+    INTEGRAL_NAMES = ("mass", "momx", "momy", "momz", "energy", "ekin", "emag", "eint")
+    STAT_NAMES = ("dens", "pres", "vel", "mag", "psi", "mach_sonic", "mach_alfven")
+
+    def integrals(self) -> dict:
+        """store_integrals (src/integrals.F90:254-485) of the current state,
+        computed on the device: {"integrals": {name: value}, "mean"/"min"/"max":
+        {name: value}}."""
+        out = np.zeros(29)
+        N.check(self.L.amun_gpu_integrals(N.dptr(out)))
+        return {"integrals": dict(zip(self.INTEGRAL_NAMES, out[0:8].tolist())),
+                "mean": dict(zip(self.STAT_NAMES, out[8:15].tolist())),
+                "min": dict(zip(self.STAT_NAMES, out[15:22].tolist())),
+                "max": dict(zip(self.STAT_NAMES, out[22:29].tolist())), "raw": out}
+
     def stages(self) -> int:
         """Number of stages of the selected integrator."""
         n = C.c_int()

@@ -289,27 +289,139 @@ def amr_timing(torch, prec, steps=10, warmup=3):
     return out
 
 
-def cpu_baseline(threads: int, steps: int = 1):
-    """The oracle (FP64 C++ restatement of the reference) on the host cores:
-    a 64^3 sample of the same scheme (64 blocks of 16^3, block-parallel
-    threads like the reference's MPI block decomposition)."""
+def oracle_rate(p, q_of_mesh, threads, steps, warmup=1):
+    """zone-updates/s of the oracle (FP64 C++ restatement of the reference,
+    blocks spread over `threads` host threads as the reference spreads them
+    over MPI ranks) on the workload `p` from the state q_of_mesh(mesh)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from amun_b200.mesh import UniformMesh
     from amun_b200.params import geometry
-    p = dict(WORKLOAD, ncells=16, xblocks=4, yblocks=4, zblocks=4)
     o = oracle.Oracle(p, threads=threads)
     mesh = UniformMesh(geometry(p))
-    o.set_prim(initial_state(mesh))
-    o.advance(1.0)  # warm-up step
+    o.set_prim(q_of_mesh(mesh))
+    for _ in range(warmup):
+        o.advance(1.0e30)
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.advance(1.0)
+        o.advance(1.0e30)
     dt = time.perf_counter() - t0
-    zu = mesh.ncells_total * steps / dt
-    return {"value": zu, "unit": "zone-updates/s", "cores": threads, "kind": "port",
-            "sample": f"64^3 periodic box, 64 blocks of 16^3, {steps} SSPRK(3,3) step(s) of the same scheme, "
-                      f"{threads} threads"}
+    return mesh.ncells_total * steps / dt, dt
+
+
+# the 128^3 workload as the oracle runs it: 8^3 blocks of 16^3 (its results
+# do not depend on the block decomposition)
+ORACLE_WORKLOAD = dict(WORKLOAD, ncells=16, xblocks=8, yblocks=8, zblocks=8)
+
+
+def cpu_baseline(threads: int, steps: int = 3):
+    """The oracle on the host cores: all threads on the 128^3 workload itself
+    (3 steps after one warm-up), and one thread on a 64^3 sample (the same
+    scheme and state generator on a 64^3 box, 2 steps)."""
+    allcore, _ = oracle_rate(ORACLE_WORKLOAD, initial_state, threads, steps)
+    serial, _ = oracle_rate(dict(WORKLOAD, ncells=16, xblocks=4, yblocks=4, zblocks=4), initial_state, 1, 2,
+                            warmup=0)
+    return {"value": allcore, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": f"the 128^3 workload itself (8^3 blocks of 16^3), {steps} SSPRK(3,3) steps, {threads} threads",
+            "serial": {"value": serial, "cores": 1,
+                       "sample": "64^3 box of the same scheme and state generator, 2 steps, 1 thread"}}
+
+
+BLAST_WORKLOAD = dict(ndims=2, equation_system="hd", equation_of_state="adi", reconstruction="tvd", limiter="mc",
+                      riemann_solver="hllc", time_advance="rk2", cfl=0.4, gamma=GAMMA, nghosts=2, ncells=256,
+                      xblocks=1, yblocks=1, maxlev=1, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5)
+
+
+def blast_state(mesh):
+    from amun_b200 import problems
+    return problems.blast(mesh, 5, GAMMA, ratio=10.0, radius=0.1, csnd=math.sqrt(GAMMA))
+
+
+def blast_timing(torch, threads):
+    """The 2D HD blast (256^2 periodic, TVD-MC, HLLC, SSPRK(2,2), CFL 0.4)
+    run to t = 0.2 in FP64 and in FP32 bulk: steps, zone-updates/s over the
+    whole run (graph-replayed steps, CUDA events), the FP32 error against
+    FP64 at t = 0.2, and the oracle over the same run on the host cores."""
+    from amun_b200.solver import Simulation
+    out = {}
+    fields = {}
+    stream = torch.cuda.current_stream()
+    for prec in ("fp64", "fp32"):
+        sim = Simulation(BLAST_WORKLOAD, precision=prec)
+        sim.L.amun_gpu_set_stream(stream.cuda_stream)
+        q0 = blast_state(sim.mesh)
+        # the step count of the run to t = 0.2 (do while time < tmax)
+        sim.set_primitive(q0)
+        nsteps, t = 0, 0.0
+        while t < 0.2:
+            t, _ = sim.advance(1.0e30)
+            nsteps += 1
+        sim.set_primitive(q0)
+        sim.run(3, 1.0e30, graph=True)  # warm-up and capture
+        sim.set_primitive(q0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.run(nsteps, 1.0e30, graph=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        fields[prec] = sim.conserved()
+        out[prec] = {"value": sim.mesh.ncells_total * nsteps / (ms * 1e-3), "ms_total": ms, "steps": nsteps,
+                     "time": sim.status()["time"]}
+        sim.close()
+    u64, u32 = fields["fp64"], fields["fp32"]
+    out["fp32_l1_density_rel_vs_fp64"] = float(np.sum(np.abs(u32[..., 0] - u64[..., 0])) / np.sum(np.abs(u64[..., 0])))
+    steps_cpu = min(out["fp64"]["steps"], 100)
+    zu, _ = oracle_rate(dict(BLAST_WORKLOAD, ncells=16, xblocks=16, yblocks=16), blast_state, threads, steps_cpu)
+    out["cpu_baseline"] = {"value": zu, "cores": threads, "kind": "port",
+                           "sample": f"the first {steps_cpu} steps of the same run, 16^2 blocks of 16^2"}
+    return out
+
+
+SRMHD_WORKLOAD = dict(ndims=3, equation_system="srmhd", equation_of_state="adi", reconstruction="tvd", limiter="mc",
+                      riemann_solver="hll", time_advance="rk2", cfl=0.4, gamma=4.0 / 3.0, nghosts=2, ncells=128,
+                      xblocks=1, yblocks=1, zblocks=1, maxlev=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0,
+                      zmax=1.0, tolerance=1.0e-12, nr_maxit=50, state_variables="4vec")
+
+
+def srmhd_timing(torch, steps=20, warmup=3):
+    """The relativistic box (128^3 periodic, gamma 4/3, rho 1, p 1,
+    B = (0.5, 0, 0), random-phase velocity scaled to a largest Lorentz factor
+    of 10; TVD-MC, HLL, SSPRK(2,2); the Newton recovery in FP64 with
+    tolerance 1e-12 and at most 50 iterations), FP64 and FP32 bulk: 20 steps
+    timed, recovery failures, and the FP32 error against FP64 after them."""
+    from amun_b200 import problems
+    from amun_b200.solver import Simulation
+    out, fields = {}, {}
+    stream = torch.cuda.current_stream()
+    q0 = None
+    for prec in ("fp64", "fp32"):
+        sim = Simulation(SRMHD_WORKLOAD, precision=prec)
+        sim.L.amun_gpu_set_stream(stream.cuda_stream)
+        if q0 is None:
+            q0 = problems.srmhd_turbulence(sim.mesh, seed=0, lorentz_max=10.0)
+        sim.set_primitive(q0)
+        sim.run(warmup, 1.0e30, graph=True)
+        sim.set_primitive(q0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.run(steps, 1.0e30, graph=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        st = sim.status()
+        fields[prec] = sim.conserved()
+        out[prec] = {"value": sim.mesh.ncells_total * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "c2p_failures": st["c2p_failures"], "steps": steps}
+        sim.close()
+    u64, u32 = fields["fp64"], fields["fp32"]
+    out["fp32_l1_density_rel_vs_fp64"] = float(np.sum(np.abs(u32[..., 0] - u64[..., 0])) / np.sum(np.abs(u64[..., 0])))
+    out["fp32_linf_density_rel_vs_fp64"] = float(np.max(np.abs(u32[..., 0] - u64[..., 0])) / np.max(np.abs(u64[..., 0])))
+    out["finite"] = bool(np.isfinite(u64).all() and np.isfinite(u32).all())
+    out["speedup_fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def run_reference(args):
@@ -317,28 +429,18 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from amun_b200.mesh import UniformMesh
-    from amun_b200.params import geometry
-    p = dict(WORKLOAD, ncells=16, xblocks=4, yblocks=4, zblocks=4)
-    o = oracle.Oracle(p, threads=threads)
-    mesh = UniformMesh(geometry(p))
-    o.set_prim(initial_state(mesh))
-    for _ in range(args.warmup):
-        o.advance(1.0)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        o.advance(1.0)
-    dt = time.perf_counter() - t0
-    zu = mesh.ncells_total * args.steps / dt
-    sample = (f"64^3 periodic sample of the 128^3 workload (64 blocks of 16^3), block-parallel over {threads} "
-              f"host threads; FP64 C++ restatement of the reference (the Fortran reference cannot be built here)")
+    # the workload itself (8^3 blocks of 16^3 over the host threads); a step
+    # takes about 1.5 s on 16 cores, so the warm-up is capped at one step
+    zu, dt = oracle_rate(ORACLE_WORKLOAD, initial_state, threads, args.steps, warmup=min(args.warmup, 1))
+    sample = (f"the 128^3 workload itself (8^3 blocks of 16^3), block-parallel over {threads} host threads; "
+              f"FP64 C++ restatement of the reference (the Fortran reference cannot be built here or on the GPU "
+              f"box: no Fortran compiler)")
     line = {"impl": "reference", "metric": METRIC, "value": zu, "unit": "zone-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "mhd3d-128-wenoz-hlld-ssprk33", "sample": "64^3", "parallelism": "host threads"},
+            "config": {"workload": "mhd3d-128^3-periodic weno5z hlld ssprk(3,3) cfl0.4", "same_config": True,
+                       "parallelism": "host threads"},
             "cpu_baseline": {"value": zu, "unit": "zone-updates/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": zu, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -353,6 +455,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the blast and relativistic legs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -493,6 +596,17 @@ def main():
         except Exception as exc:  # pragma: no cover
             adjoint[prec] = {"error": str(exc)}
 
+    extra_cfg = {}
+    if not args.no_extra:
+        try:
+            extra_cfg["blast2d"] = blast_timing(torch, os.cpu_count() or 1)
+        except Exception as exc:  # pragma: no cover
+            extra_cfg["blast2d"] = {"error": str(exc)}
+        try:
+            extra_cfg["srmhd3d"] = srmhd_timing(torch)
+        except Exception as exc:  # pragma: no cover
+            extra_cfg["srmhd3d"] = {"error": str(exc)}
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         r32, r64 = results["fp32"], results["fp64"]
@@ -542,6 +656,11 @@ def main():
             "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
                                     "J = kinetic energy in [0,0.25]^2, dJ/drho0",
                         "fp64": adjoint["fp64"], "fp32": adjoint["fp32"]},
+            "blast2d": dict({"workload": "hd2d-256^2-periodic blast (p 10 inside r < 0.1) tvd-mc hllc ssprk(2,2) "
+                                         "cfl0.4, run to t = 0.2"}, **extra_cfg.get("blast2d", {})),
+            "srmhd3d": dict({"workload": "srmhd3d-128^3-periodic gamma 4/3, B=(0.5,0,0), max Lorentz factor 10, "
+                                         "tvd-mc hll ssprk(2,2), 4-velocity states, FP64 Newton recovery "
+                                         "(1e-12, 50 iterations)"}, **extra_cfg.get("srmhd3d", {})),
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": clocks,
         }

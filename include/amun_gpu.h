@@ -245,6 +245,19 @@ int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt);
  * including ghost fill and primitive update after each stage. */
 int amun_gpu_evolve(void);
 
+/* store_integrals (src/integrals.F90:254-485) of the current state on the
+ * device, returned instead of written to the integrals and statistics
+ * files.  out[0..7]: inarr(1:8) -- mass, x/y/z momentum, total, kinetic,
+ * magnetic and internal energy; out[8..14]: avarr(1:7) -- volume averages of
+ * density, pressure, |v|, |B|, psi, sonic and Alfvenic Mach number;
+ * out[15..21], out[22..28]: their minima and maxima.  The sums are
+ * compensated (double-double) and deterministic, within a few units in the
+ * last place of the exact sums; the reference sums each block in element
+ * order and the blocks in list order, so the two agree to that order's
+ * rounding (about 1e-13 relative for a 128^3 box).  Minima and maxima are
+ * exact.  Entries a system lacks are 0. */
+int amun_gpu_integrals(double* out);
+
 /* One stage of the selected integrator, for a caller that does its own
  * work between stages (the per-stage body of evolve_*, e.g. evolve_rk2
  * src/evolution.F90:681-704 and 729-753: update_fluxes, update_increment,

@@ -28,6 +28,7 @@
 #include <vector>
 #include <thread>
 #include <algorithm>
+#include <limits>
 #include <atomic>
 #include <quadmath.h>
 #include <stdexcept>
@@ -4667,6 +4668,91 @@ void or_advance(void* h, double dtnext, double* time, double* dt) {
   o->step += 1;
   *time = o->time; *dt = o->dt;
 }
+// store_integrals src/integrals.F90:254-485 on the current state: the
+// volume integrals inarr(1:8) (mass, momenta, total, kinetic, magnetic and
+// internal energy) and the volume averages, minima and maxima of density,
+// pressure, |v|, |B|, psi, sonic and Alfvenic Mach numbers, with the
+// reference's order of operations: each block's sum runs over its interior
+// cells in column-major order (Fortran SUM), is multiplied by the cell
+// volume of the block's level (advol, src/coordinates.F90:369) and added to
+// the total in block-list order.  out: inarr(1:8), avarr(1:7), mnarr(1:7),
+// mxarr(1:7).
+void or_integrals(void* h, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const double eps = std::numeric_limits<double>::epsilon(), big = std::numeric_limits<double>::max();
+  double inarr[16], avarr[16], mnarr[16], mxarr[16];
+  for (int n = 0; n < 16; ++n) { inarr[n] = 0.0; avarr[n] = 0.0; mnarr[n] = big; mxarr[n] = -big; }
+  if (o->ipr < 1) { mnarr[1] = 0.0; mxarr[1] = 0.0; }
+  if (o->ibx < 1) { mnarr[3] = mxarr[3] = 0.0; mnarr[4] = mxarr[4] = 0.0; mnarr[6] = mxarr[6] = 0.0; }
+  for (auto& B : o->blocks) {
+    const double dvol = B.dx * B.dy * (o->p.ndims == 3 ? B.dz : 1.0), dvolh = 0.5 * dvol;
+    // per-block sums in element order
+    auto bsum = [&](auto f) {
+      double s = 0.0;
+      for (int k = o->kb; k <= o->ke; ++k)
+        for (int j = o->jb; j <= o->je; ++j)
+          for (int i = o->ib; i <= o->ie; ++i) s = s + f(o->qi(1, i, j, k));
+      return s;
+    };
+    auto bstat = [&](int slot, auto f) {
+      double s = 0.0;
+      for (int k = o->kb; k <= o->ke; ++k)
+        for (int j = o->jb; j <= o->je; ++j)
+          for (int i = o->ib; i <= o->ie; ++i) {
+            const double v = f(o->qi(1, i, j, k));
+            s = s + v;
+            mnarr[slot] = std::min(mnarr[slot], v);
+            mxarr[slot] = std::max(mxarr[slot], v);
+          }
+      avarr[slot] = avarr[slot] + s * dvol;
+    };
+    const double* u = B.u;
+    const double* q = B.q.data();
+    const int idn = o->idn - 1, imx = o->imx - 1, imy = o->imy - 1, imz = o->imz - 1;
+    inarr[0] = inarr[0] + bsum([&](size_t c) { return u[c + idn]; }) * dvol;
+    inarr[1] = inarr[1] + bsum([&](size_t c) { return u[c + imx]; }) * dvol;
+    inarr[2] = inarr[2] + bsum([&](size_t c) { return u[c + imy]; }) * dvol;
+    inarr[3] = inarr[3] + bsum([&](size_t c) { return u[c + imz]; }) * dvol;
+    if (o->ien > 0) inarr[4] = inarr[4] + bsum([&](size_t c) { return u[c + o->ien - 1]; }) * dvol;
+    inarr[5] = inarr[5] + bsum([&](size_t c) {
+                 return (u[c + imx] * u[c + imx] + u[c + imy] * u[c + imy] + u[c + imz] * u[c + imz]) / u[c + idn];
+               }) * dvolh;
+    if (o->ibx > 0) {
+      const int bx = o->ibx - 1, by = o->iby - 1, bz = o->ibz - 1;
+      inarr[6] = inarr[6] + bsum([&](size_t c) {
+                   return u[c + bx] * u[c + bx] + u[c + by] * u[c + by] + u[c + bz] * u[c + bz];
+                 }) * dvolh;
+    }
+    const int ivx = o->ivx - 1, ivy = o->ivy - 1, ivz = o->ivz - 1;
+    auto vel = [&](size_t c) { return std::sqrt(q[c + ivx] * q[c + ivx] + q[c + ivy] * q[c + ivy] + q[c + ivz] * q[c + ivz]); };
+    auto mag = [&](size_t c) {
+      const int bx = o->ibx - 1, by = o->iby - 1, bz = o->ibz - 1;
+      return std::sqrt(q[c + bx] * q[c + bx] + q[c + by] * q[c + by] + q[c + bz] * q[c + bz]);
+    };
+    bstat(0, [&](size_t c) { return q[c + idn]; });
+    if (o->ipr > 0) bstat(1, [&](size_t c) { return q[c + o->ipr - 1]; });
+    bstat(2, vel);
+    if (o->ibx > 0) {
+      bstat(3, mag);
+      bstat(4, [&](size_t c) { return q[c + o->ibp - 1]; });
+    }
+    if (o->ipr > 0)
+      bstat(5, [&](size_t c) { return std::sqrt(q[c + idn]) * vel(c) / std::sqrt(o->gamma * q[c + o->ipr - 1]); });
+    else
+      bstat(5, [&](size_t c) { return vel(c) / o->csnd; });
+    if (o->ibx > 0) bstat(6, [&](size_t c) { return std::sqrt(q[c + idn]) * vel(c) / std::max(eps, mag(c)); });
+  }
+  if (o->ien > 0) inarr[7] = inarr[4] - inarr[5] - inarr[6];
+  const double zlen = o->p.ndims == 3 ? o->p.zmax - o->p.zmin : 1.0;
+  const double voli = 1.0 / ((o->p.xmax - o->p.xmin) * (o->p.ymax - o->p.ymin) * zlen);
+  for (int n = 0; n < 8; ++n) out[n] = inarr[n];
+  for (int n = 0; n < 7; ++n) {
+    out[8 + n] = avarr[n] * voli;
+    out[15 + n] = mnarr[n];
+    out[22 + n] = mxarr[n];
+  }
+}
+
 void or_scalars(void* h, double* out) {
   Oracle* o = static_cast<Oracle*>(h);
   out[0] = o->time; out[1] = o->dt; out[2] = o->cmax; out[3] = (double)o->step; out[4] = (double)o->nonpositive;

@@ -65,6 +65,7 @@ def lib():
         L.or_new_time_step.argtypes = [vp, C.c_double, d, d]
         L.or_advance.argtypes = [vp, C.c_double, d, d]
         L.or_scalars.argtypes = [vp, d]
+        L.or_integrals.argtypes = [vp, d]
         L.or_set_cmax.argtypes = [vp, C.c_double]
         L.or_prim2cons.argtypes = [vp, i, d, d]
         L.or_cons2prim.argtypes = [vp, i, d, d]
@@ -152,6 +153,13 @@ class Oracle:
                     c2p_failures=int(s[5]), unphysical_cells=int(s[6]))
 
     # ---- unit level --------------------------------------------------------
+    def integrals(self) -> np.ndarray:
+        """store_integrals (src/integrals.F90:254-485): inarr(1:8),
+        avarr(1:7), mnarr(1:7), mxarr(1:7) as one array of 29."""
+        out = np.zeros(29)
+        self.L.or_integrals(self.h, _p(out))
+        return out
+
     def set_cmax(self, cmax: float):
         self.L.or_set_cmax(self.h, cmax)
 

@@ -177,3 +177,31 @@ def test_unknown_keys_and_errors(oracle_mod):
         oracle_mod.Oracle(params(reconstruction="nope"))
     with pytest.raises(ValueError):
         oracle_mod.Oracle(params(equation_system="srhd_unknown"))
+
+
+def test_oracle_integrals_match_numpy(oracle_mod):
+    """The oracle's store_integrals against a direct numpy evaluation of the
+    same sums (src/integrals.F90:340-436) on a two-level-free block mesh."""
+    from helpers import params as mk, smooth_field as sf
+    p = mk("mhd", "tvd", "hll", "rk2", ndims=2, ncells=8, xblocks=2, yblocks=2, xmin=0.0, xmax=2.0, ymin=0.0,
+           ymax=1.0)
+    o = oracle_mod.Oracle(p)
+    nx, ny = 16, 16
+    q = sf((1, ny, nx), 9, seed=7, amp=0.3)
+    o.set_prim(q)
+    r = o.integrals()
+    u = o.cons()
+    dv = (2.0 / nx) * (1.0 / ny)
+    qq = o.prim()
+    assert np.isclose(r[0], u[..., 0].sum() * dv, rtol=1e-13)
+    assert np.isclose(r[4], u[..., 8].sum() * dv, rtol=1e-13)
+    ek = 0.5 * ((u[..., 1] ** 2 + u[..., 2] ** 2 + u[..., 3] ** 2) / u[..., 0]).sum() * dv
+    assert np.isclose(r[5], ek, rtol=1e-13)
+    em = 0.5 * (u[..., 4] ** 2 + u[..., 5] ** 2 + u[..., 6] ** 2).sum() * dv
+    assert np.isclose(r[6], em, rtol=1e-13)
+    assert np.isclose(r[7], r[4] - r[5] - r[6], rtol=1e-13)
+    vel = np.sqrt(qq[..., 1] ** 2 + qq[..., 2] ** 2 + qq[..., 3] ** 2)
+    assert np.isclose(r[8 + 2], vel.sum() * dv / 2.0, rtol=1e-13)
+    assert r[15] == qq[..., 0].min() and r[22] == qq[..., 0].max()
+    mach = np.sqrt(qq[..., 0]) * vel / np.sqrt(5.0 / 3.0 * qq[..., 8])
+    assert np.isclose(r[22 + 5], mach.max(), rtol=1e-15)
