@@ -136,6 +136,13 @@ def check(code: int):
         raise AmunError(code, msg.decode() if msg else "")
 
 
+def tptr(t):
+    """double* of a contiguous float64 torch tensor (host or device)."""
+    if t.dtype.itemsize != 8 or not t.is_contiguous():
+        raise ValueError("expected a contiguous float64 tensor")
+    return C.cast(C.c_void_p(t.data_ptr()), _D)
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (or None)."""
     if a is None:

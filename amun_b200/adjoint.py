@@ -15,15 +15,22 @@ import torch
 
 
 class Evolve(torch.autograd.Function):
+    """CUDA tensors stay on the device (the library reads and writes them
+    directly); CPU tensors go through host arrays."""
+
     @staticmethod
     def forward(ctx, q0, sim, nsteps, interval, dtnext):
-        sim.set_primitive(q0.detach().cpu().numpy().astype(np.float64))
+        ctx.device = q0.is_cuda
+        if q0.is_cuda:
+            sim.set_primitive_device(q0)
+        else:
+            sim.set_primitive(q0.detach().numpy().astype(np.float64))
         sim.forward_checkpointed(nsteps, dtnext, interval)
         ctx.sim = sim
         # the library keeps one recorded run per context: a later recording
         # on the same Simulation overwrites the checkpoints this backward needs
         ctx.recording = sim.recording
-        u = torch.from_numpy(sim.conserved())
+        u = sim.conserved_device() if q0.is_cuda else torch.from_numpy(sim.conserved())
         return u.to(device=q0.device, dtype=q0.dtype)
 
     @staticmethod
@@ -31,9 +38,11 @@ class Evolve(torch.autograd.Function):
         if ctx.sim.recording != ctx.recording:
             raise RuntimeError("the Simulation recorded another run after this forward; its checkpoints are gone "
                                "(use one Simulation per differentiated run, or call backward first)")
-        lam = grad_u.detach().cpu().numpy().astype(np.float64)
-        lam_q0, _ = ctx.sim.adjoint(lam)
-        return torch.from_numpy(lam_q0).to(device=grad_u.device, dtype=grad_u.dtype), None, None, None, None
+        if ctx.device:
+            lam_q0, _ = ctx.sim.adjoint_device(grad_u.contiguous())
+        else:
+            lam_q0 = torch.from_numpy(ctx.sim.adjoint(grad_u.detach().numpy().astype(np.float64))[0])
+        return lam_q0.to(device=grad_u.device, dtype=grad_u.dtype), None, None, None, None
 
 
 def evolve(q0: torch.Tensor, sim, nsteps: int, interval: int = 20, dtnext: float = 1.0e30) -> torch.Tensor:

@@ -226,12 +226,14 @@ int cuda_fail(cudaError_t e, const char* where) {
 // the call returns.  (Plain cudaMemcpy/cudaMemset run on the legacy default
 // stream, which does not order against a non-blocking stream: a kernel on
 // C.stream could read a buffer whose host-to-device DMA has not finished.)
+// The copy kind is inferred from the addresses (unified addressing), so the
+// block, per-procedure and adjoint entry points take host or device arrays.
 cudaError_t h2d(void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, C.stream);
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, C.stream);
   return e != cudaSuccess ? e : cudaStreamSynchronize(C.stream);
 }
 cudaError_t d2h(void* dst, const void* src, size_t bytes) {
-  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, C.stream);
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, C.stream);
   return e != cudaSuccess ? e : cudaStreamSynchronize(C.stream);
 }
 cudaError_t dset(void* dst, int value, size_t bytes) {
@@ -1291,18 +1293,18 @@ static int upload_range(int first, int count, const double* u0, const double* u1
   if ((r = ensure_staging(per * count))) return r;
   cudaError_t e;
   if (q) {
-    CK(cudaMemcpyAsync(C.staging, q, per * count, cudaMemcpyHostToDevice, C.stream));
+    CK(cudaMemcpyAsync(C.staging, q, per * count, cudaMemcpyDefault, C.stream));
     e = bulk() ? Launch<float, float>::upload_q(C.staging, (float*)C.q[C.cur], g, C.nv, first, count, C.stream)
                : Launch<double, double>::upload_q(C.staging, (double*)C.q[C.cur], g, C.nv, first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload q");
   }
   if (u0) {
-    CK(cudaMemcpyAsync(C.staging, u0, per * count, cudaMemcpyHostToDevice, C.stream));
+    CK(cudaMemcpyAsync(C.staging, u0, per * count, cudaMemcpyDefault, C.stream));
     e = Launch<double, double>::upload_u0(C.staging, C.u0, g, C.nv, first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload u0");
   }
   if (u1) {
-    CK(cudaMemcpyAsync(C.staging, u1, per * count, cudaMemcpyHostToDevice, C.stream));
+    CK(cudaMemcpyAsync(C.staging, u1, per * count, cudaMemcpyDefault, C.stream));
     e = bulk() ? Launch<float, float>::upload_u1(C.staging, (float*)C.u1, g, C.nv, first, count, C.stream)
                : Launch<double, double>::upload_u1(C.staging, (double*)C.u1, g, C.nv, first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload u1");
@@ -1389,7 +1391,7 @@ static int download_range(int first, int count, double* u0, double* u1, double* 
                : Launch<double, double>::download_q((const double*)C.q[C.cur], C.staging, g, C.nv, first, count,
                                                     C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "download q");
-    CK(cudaMemcpyAsync(q, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaMemcpyAsync(q, C.staging, per * count, cudaMemcpyDefault, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   if (u0) {
@@ -1398,7 +1400,7 @@ static int download_range(int first, int count, double* u0, double* u1, double* 
                : Launch<double, double>::download_u0(C.p.eqsys, C.u0, (const double*)C.q[C.cur], C.staging, g,
                                                      method_const(), first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "download u0");
-    CK(cudaMemcpyAsync(u0, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaMemcpyAsync(u0, C.staging, per * count, cudaMemcpyDefault, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   if (u1) {
@@ -1407,7 +1409,7 @@ static int download_range(int first, int count, double* u0, double* u1, double* 
                : Launch<double, double>::download_u1(C.p.eqsys, (const double*)C.u1, (const double*)C.q[C.cur],
                                                      C.staging, g, method_const(), first, count, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "download u1");
-    CK(cudaMemcpyAsync(u1, C.staging, per * count, cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaMemcpyAsync(u1, C.staging, per * count, cudaMemcpyDefault, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   return 0;
@@ -2312,7 +2314,7 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
   }
   if ((r = build_inverse_neighbours())) return r;
   AdjGeo ag{g, C.nv, C.p.eqsys, C.nblocks};
-  CK(cudaMemcpyAsync(A.stage, lam_u, qd * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+  CK(cudaMemcpyAsync(A.stage, lam_u, qd * sizeof(double), cudaMemcpyDefault, C.stream));
   cudaError_t e = adj_from_host_layout(ag, A.stage, A.lamU0, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "adjoint input");
   CK(cudaMemsetAsync(A.lamU1, 0, ud * sizeof(double), C.stream));
@@ -2321,7 +2323,7 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
   if (lam_u0) {
     e = adj_to_host_layout(ag, A.lamU0, A.stage, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint output");
-    CK(cudaMemcpyAsync(lam_u0, A.stage, qd * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaMemcpyAsync(lam_u0, A.stage, qd * sizeof(double), cudaMemcpyDefault, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   if (lam_q0) {
@@ -2331,7 +2333,7 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
     if (e != cudaSuccess) return cuda_fail(e, "adjoint prim2cons");
     e = adj_to_host_layout(ag, A.lamdu, A.stage, C.stream);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint output");
-    CK(cudaMemcpyAsync(lam_q0, A.stage, qd * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CK(cudaMemcpyAsync(lam_q0, A.stage, qd * sizeof(double), cudaMemcpyDefault, C.stream));
     CK(cudaStreamSynchronize(C.stream));
   }
   // leave the recorded final state on the device

@@ -97,6 +97,40 @@ class UniformMesh:
                 out[b] = padded[:, by * nc:by * nc + self.jm, bx * nc:bx * nc + self.im]
         return out
 
+    def to_blocks_torch(self, field):
+        """to_blocks for a torch tensor, on the tensor's device."""
+        import torch
+        ng, nc = self.ng, self.nc
+        if self.ndims == 3:
+            idx = [torch.arange(-ng, n + ng, device=field.device) % n for n in field.shape[:3]]
+            padded = field[idx[0]][:, idx[1]][:, :, idx[2]]
+        else:
+            iy = torch.arange(-ng, field.shape[1] + ng, device=field.device) % field.shape[1]
+            ix = torch.arange(-ng, field.shape[2] + ng, device=field.device) % field.shape[2]
+            padded = field[:, iy][:, :, ix]
+        blocks = []
+        for b in range(self.nblocks):
+            bx, by, bz = self.block_coords(b)
+            if self.ndims == 3:
+                blocks.append(padded[bz * nc:bz * nc + self.km, by * nc:by * nc + self.jm, bx * nc:bx * nc + self.im])
+            else:
+                blocks.append(padded[:, by * nc:by * nc + self.jm, bx * nc:bx * nc + self.im])
+        return torch.stack(blocks).contiguous()
+
+    def from_blocks_torch(self, blocks):
+        """from_blocks for a torch tensor, on the tensor's device."""
+        import torch
+        ng, nc = self.ng, self.nc
+        out = torch.empty(self.shape + (blocks.shape[-1],), dtype=blocks.dtype, device=blocks.device)
+        for b in range(self.nblocks):
+            bx, by, bz = self.block_coords(b)
+            if self.ndims == 3:
+                out[bz * nc:(bz + 1) * nc, by * nc:(by + 1) * nc, bx * nc:(bx + 1) * nc] = \
+                    blocks[b, ng:ng + nc, ng:ng + nc, ng:ng + nc]
+            else:
+                out[:, by * nc:(by + 1) * nc, bx * nc:(bx + 1) * nc] = blocks[b, :, ng:ng + nc, ng:ng + nc]
+        return out
+
     def from_blocks(self, blocks: np.ndarray) -> np.ndarray:
         """Block arrays -> global interior field."""
         nv = blocks.shape[-1]

@@ -48,6 +48,37 @@ class Simulation:
         N.check(self.L.amun_gpu_boundary_variables())
         N.check(self.L.amun_gpu_set_time(0.0, 0.0))
 
+    # ---- the same on device tensors (no host round trip) ---------------------
+    def set_primitive_device(self, q):
+        """set_primitive from a torch CUDA tensor (NZ, NY, NX, nv), float64,
+        on the current device: the block arrays are formed on the device and
+        passed to the library as device arrays."""
+        import torch
+        qb = self.mesh.to_blocks_torch(q.detach().to(torch.float64))
+        ub = torch.empty_like(qb)
+        N.check(self.L.amun_gpu_prim2cons(qb.numel() // self.nv, N.tptr(qb), N.tptr(ub)))
+        N.check(self.L.amun_gpu_upload_blocks(0, self.mesh.nblocks, N.tptr(ub), N.tptr(qb)))
+        N.check(self.L.amun_gpu_boundary_variables())
+        N.check(self.L.amun_gpu_set_time(0.0, 0.0))
+
+    def conserved_device(self):
+        """The conserved field as a torch CUDA tensor (NZ, NY, NX, nv)."""
+        import torch
+        shp = (self.mesh.nblocks, self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)
+        ub = torch.empty(shp, dtype=torch.float64, device="cuda")
+        qb = torch.empty_like(ub)
+        N.check(self.L.amun_gpu_download_blocks(0, self.mesh.nblocks, N.tptr(ub), N.tptr(qb)))
+        return self.mesh.from_blocks_torch(ub)
+
+    def adjoint_device(self, lam_u):
+        """adjoint with torch CUDA tensors: lam_u = dJ/dU of the recorded
+        final state (NZ, NY, NX, nv) -> (dJ/dq0, dJ/dU0) as CUDA tensors."""
+        import torch
+        lb = self.mesh.to_blocks_torch(lam_u.detach().to(torch.float64))
+        lq, lu = torch.empty_like(lb), torch.empty_like(lb)
+        N.check(self.L.amun_gpu_adjoint(N.tptr(lb), N.tptr(lq), N.tptr(lu)))
+        return self.mesh.from_blocks_torch(lq), self.mesh.from_blocks_torch(lu)
+
     def set_primitive_blocks(self, qb: np.ndarray):
         """Set the state from block arrays of primitives (nblocks, km, jm, im,
         nv), ghost entries ignored: u0 = prim2cons(q), upload, ghost fill."""

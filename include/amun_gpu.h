@@ -169,8 +169,11 @@ int amun_gpu_init(const amun_params* p);
  * block pool and invalidates captured CUDA graphs. */
 int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks);
 
-/* Copy one block's arrays host -> device (u1 may be NULL).  Device state
- * stays resident between calls. */
+/* Copy one block's arrays into the device pool (u1 may be NULL).  Device
+ * state stays resident between calls.  Here and in the download, the
+ * per-procedure and the adjoint entry points, arrays may be host memory or
+ * device memory of the current device (the copies follow unified
+ * addressing). */
 int amun_gpu_upload(int block, const double* u0, const double* u1, const double* q);
 /* Same for `count` consecutive blocks stored back to back. */
 int amun_gpu_upload_blocks(int first, int count, const double* u0, const double* q);

@@ -191,3 +191,18 @@ def test_context_lib_selects_its_context():
     finally:
         x.destroy()
         y.destroy()
+
+
+@pytest.mark.parametrize("nd,nb", [(2, 2), (3, 2)])
+def test_torch_block_conversion_matches_numpy(nd, nb):
+    """to_blocks_torch / from_blocks_torch (the device path of the autograd
+    binding) equal the numpy forms, periodic ghosts included."""
+    import torch
+    geo = dict(ndims=nd, ncells=4, nghosts=2, maxlev=1, xblocks=nb, yblocks=nb, zblocks=nb, xmin=0.0, xmax=1.0,
+               ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0)
+    m = UniformMesh(geo)
+    f = np.random.default_rng(0).normal(size=m.shape + (3,))
+    b_np = m.to_blocks(f)
+    b_t = m.to_blocks_torch(torch.from_numpy(f)).numpy()
+    assert np.array_equal(b_np, b_t)
+    assert np.array_equal(m.from_blocks_torch(torch.from_numpy(b_np)).numpy(), f)

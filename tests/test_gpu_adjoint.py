@@ -126,6 +126,65 @@ def test_adjoint_finite_differences():
         sim.close()
 
 
+def test_adjoint_finite_differences_full_size():
+    """The differentiation configuration at its stated size: 2D MHD 256^2,
+    WENO-Z, HLL, SSPRK(3,3), 200 steps, checkpoint every 20; dJ/drho0 along 8
+    seeded smooth directions agrees with central differences to 1e-6 (FD
+    step swept over 1e-5..1e-7; the runs replay the recorded dt and cmax)."""
+    from amun_b200.adjoint import kinetic_energy
+    from amun_b200.solver import Simulation
+    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=256, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    q0 = problems.smooth_mhd(mesh, seed=0)
+    sim = Simulation(p)
+    try:
+        g, _, _ = gpu_gradient(sim, mesh, q0, 200, 20)
+
+        def J(q):
+            sim.set_primitive(q)
+            sim.replay(200)
+            return float(kinetic_energy(torch.from_numpy(sim.conserved()), mesh))
+
+        for k in range(8):
+            d = problems.random_phase_field(mesh.shape[1:], 100 + k, ncomp=1)[None, ..., 0]
+            ad = float(np.sum(g[..., 0] * d))
+            errs = []
+            for eps in (1e-5, 1e-6, 1e-7):
+                qp, qm = q0.copy(), q0.copy()
+                qp[..., 0] += eps * d
+                qm[..., 0] -= eps * d
+                errs.append(abs((J(qp) - J(qm)) / (2 * eps) - ad) / abs(ad))
+            assert min(errs) <= 1e-6, (k, errs)
+    finally:
+        sim.close()
+
+
+def test_evolve_on_cuda_tensors_matches_host_path():
+    """torch.autograd through Evolve with CUDA tensors (the library reads and
+    writes device memory, no host copies) gives the forward state and the
+    gradient of the host path bit for bit."""
+    from amun_b200.adjoint import evolve, kinetic_energy
+    from amun_b200.solver import Simulation
+    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    q0 = problems.smooth_mhd(mesh, seed=2)
+    out = {}
+    for dev in ("cpu", "cuda"):
+        sim = Simulation(p)
+        try:
+            q = torch.from_numpy(q0).to(dev).requires_grad_(True)
+            u = evolve(q, sim, 12, interval=4)
+            assert u.device.type == dev
+            J = kinetic_energy(u, mesh)
+            J.backward()
+            out[dev] = (u.detach().cpu().numpy(), q.grad.detach().cpu().numpy(), float(J))
+        finally:
+            sim.close()
+    assert np.array_equal(out["cpu"][0], out["cuda"][0])
+    assert out["cpu"][2] == out["cuda"][2]
+    assert np.array_equal(out["cpu"][1], out["cuda"][1])
+
+
 def test_adjoint_fp32_bulk():
     """FP32-bulk forward and adjoint: dJ/drho0 within 1e-3 (relative to its
     largest entry) of the FP64 tape's (measured 2.8e-4).  The gradients with
