@@ -39,6 +39,7 @@ enum { TA_EULER = 0, TA_RK2, TA_SSPRK2, TA_RK3, TA_SSPRK34, TA_SSPRK35 };
 // plus after the last step, and each step's scalars after new_time_step.
 struct AdjCtx {
   bool recorded = false;
+  bool keep_all = false;  // every stage input kept while recording (interval 0)
   int nsteps = 0, interval = 1, nseg = 0;
   std::vector<double*> ck_u0;
   std::vector<void*> ck_q;
@@ -2183,6 +2184,7 @@ int reverse_step(int n, int slot, const AdjGeo& ag) {
 
 template <typename R>
 int forward_recorded(int nsteps, double dtnext) {
+  const size_t qb = qpool_bytes();
   for (int n = 0; n < nsteps; ++n) {
     if (n % A.interval == 0) {
       int r = save_state(n / A.interval);
@@ -2191,8 +2193,23 @@ int forward_recorded(int nsteps, double dtnext) {
     new_time_step_kernel<<<1, 32, 0, C.stream>>>(C.sc, C.cfl, C.dx_min, dtnext, visc_res());
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(A.rec + n, C.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, C.stream));
-    int r = launch_evolve<R>();
-    if (r) return r;
+    if (!A.keep_all) {
+      int r = launch_evolve<R>();
+      if (r) return r;
+    } else {
+      // every stage input stays on the device: the adjoint recomputes nothing
+      Schedule S = schedule();
+      if (S.copy_first) {
+        cudaError_t e = Launch<R, R>::copy_u0_u1(C.u0, (R*)C.u1, (long long)C.nblocks * C.g.ubs, C.stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copy u0->u1");
+      }
+      for (size_t st = 0; st < S.stages.size(); ++st) {
+        char* dst = (char*)A.seg_q + ((size_t)n * S.stages.size() + st) * qb;
+        CK(cudaMemcpyAsync(dst, C.q[C.cur], qb, cudaMemcpyDeviceToDevice, C.stream));
+        int r = launch_stage<R>(S.stages[st]);
+        if (r) return r;
+      }
+    }
     end_step_kernel<<<1, 32, 0, C.stream>>>(C.sc);
     CK(cudaGetLastError());
   }
@@ -2210,8 +2227,10 @@ int adjoint_pass(const AdjGeo& ag) {
     const int n0 = seg * A.interval;
     const int n1 = n0 + A.interval < A.nsteps ? n0 + A.interval : A.nsteps;
     cudaEventRecord(ev[3 * seg], C.stream);
-    r = restore_state(seg);
-    for (int n = n0; n < n1 && !r; ++n) r = replay_step<R>(n, n - n0);
+    if (!A.keep_all) {
+      r = restore_state(seg);
+      for (int n = n0; n < n1 && !r; ++n) r = replay_step<R>(n, n - n0);
+    }
     cudaEventRecord(ev[3 * seg + 1], C.stream);
     for (int n = n1 - 1; n >= n0 && !r; --n) r = reverse_step<R>(n, n - n0, ag);
     cudaEventRecord(ev[3 * seg + 2], C.stream);
@@ -2236,7 +2255,10 @@ int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval) {
   int r = check_ready();
   if (r) return r;
   if ((r = adj_supported())) return r;
-  if (nsteps <= 0 || interval <= 0) return fail(AMUN_E_BAD_ARGUMENT, "nsteps and interval must be positive");
+  if (nsteps <= 0 || interval < 0) return fail(AMUN_E_BAD_ARGUMENT, "nsteps must be positive, interval >= 0");
+  // interval 0: one segment whose stage inputs are kept while recording
+  A.keep_all = interval == 0;
+  if (interval == 0) interval = nsteps;
   // buffers of an earlier recording on the same mesh are reused (a free
   // would synchronise the device); they grow when this run needs more
   A.recorded = false;
@@ -2269,6 +2291,18 @@ int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval) {
   A.nsteps = nsteps;
   A.interval = interval;
   A.nseg = nseg;
+  if (A.keep_all && !A.seg_q) {
+    const size_t ns = schedule().stages.size();
+    const size_t need = (size_t)interval * ns * qpool_bytes();
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    if (need + ((size_t)1 << 30) > free_b)
+      return fail(AMUN_E_BAD_ARGUMENT, "interval 0 keeps " + std::to_string(need >> 20) +
+                                           " MiB of stage inputs; the device has " + std::to_string(free_b >> 20) +
+                                           " MiB free: record with checkpoints instead");
+    CK(cudaMalloc(&A.seg_q, need));
+    A.seg_cap = interval;
+  }
   if ((r = ensure_maxspeed())) return r;
   r = bulk() ? forward_recorded<float>(nsteps, dtnext) : forward_recorded<double>(nsteps, dtnext);
   if (r) return r;

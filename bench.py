@@ -180,12 +180,13 @@ ADJOINT_WORKLOAD = dict(ndims=2, equation_system="mhd", equation_of_state="adi",
 ADJOINT_STEPS, ADJOINT_INTERVAL = 200, 20
 
 
-def adjoint_timing(torch, prec):
+def adjoint_timing(torch, prec, interval=ADJOINT_INTERVAL):
     """2D MHD 256^2 (WENO-Z, HLL, SSPRK(3,3)), smooth seeded state, 200 steps:
     the plain forward run (graphs) against the recorded forward (checkpoint
-    every 20 steps) and the adjoint call (segment recomputation + reverse) for
-    J = kinetic energy in [0,0.25]^2 at the final step, all timed with CUDA
-    events on the library's stream."""
+    every `interval` steps; 0: every stage input kept, no recomputation) and
+    the adjoint call (segment recomputation + reverse) for J = kinetic energy
+    in [0,0.25]^2 at the final step, all timed with CUDA events on the
+    library's stream."""
     from amun_b200 import problems
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
@@ -210,13 +211,13 @@ def adjoint_timing(torch, prec):
     # warm-up: one full recording and one adjoint, so the checkpoints and the
     # adjoint's work arrays are allocated before the timed calls
     sim.set_primitive(q0)
-    sim.forward_checkpointed(ADJOINT_STEPS, 1.0e30, ADJOINT_INTERVAL)
+    sim.forward_checkpointed(ADJOINT_STEPS, 1.0e30, interval)
     u = torch.from_numpy(sim.conserved()).requires_grad_(True)
     kinetic_energy(u, sim.mesh).backward()
     lam = u.grad.numpy()
     sim.adjoint(lam)
     sim.set_primitive(q0)
-    rec = events(lambda: sim.forward_checkpointed(ADJOINT_STEPS, 1.0e30, ADJOINT_INTERVAL))
+    rec = events(lambda: sim.forward_checkpointed(ADJOINT_STEPS, 1.0e30, interval))
     out = {}
     adj = events(lambda: out.setdefault("g", sim.adjoint(lam)))
     gbytes = sim.adjoint_bytes()
@@ -228,7 +229,7 @@ def adjoint_timing(torch, prec):
             "adjoint_recompute_ms": recompute_ms, "adjoint_reverse_ms": reverse_ms,
             "reverse_stage_over_forward_stage": reverse_ms / fwd,
             "adjoint_over_forward": adj / fwd, "gradient_over_forward": (rec + adj) / fwd,
-            "steps": ADJOINT_STEPS, "checkpoint_interval": ADJOINT_INTERVAL, "device_bytes": gbytes,
+            "steps": ADJOINT_STEPS, "checkpoint_interval": interval, "device_bytes": gbytes,
             "grad_rho_l2": float(np.sqrt(np.sum(out["g"][0][..., 0] ** 2)))}
 
 
@@ -592,7 +593,10 @@ def main():
     adjoint = {}
     for prec in ("fp64", "fp32"):
         try:
-            adjoint[prec] = adjoint_timing(torch, prec)
+            # every stage input kept (fits: 200 x 3 x 5 MB), and checkpoints
+            # every 20 steps with recomputation
+            adjoint[prec] = adjoint_timing(torch, prec, 0)
+            adjoint[prec]["checkpointed"] = adjoint_timing(torch, prec, ADJOINT_INTERVAL)
         except Exception as exc:  # pragma: no cover
             adjoint[prec] = {"error": str(exc)}
 
@@ -654,7 +658,8 @@ def main():
                                         "tvd-mc hlld ssprk(2,2) cfl0.4, ratio 1000",
                             "fp64": amr["fp64"], "fp32": amr["fp32"]},
             "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
-                                    "J = kinetic energy in [0,0.25]^2, dJ/drho0",
+                                    "J = kinetic energy in [0,0.25]^2, dJ/drho0; every stage input kept "
+                                    "(\"checkpointed\": every 20 steps, with recomputation)",
                         "fp64": adjoint["fp64"], "fp32": adjoint["fp32"]},
             "blast2d": dict({"workload": "hd2d-256^2-periodic blast (p 10 inside r < 0.1) tvd-mc hllc ssprk(2,2) "
                                          "cfl0.4, run to t = 0.2"}, **extra_cfg.get("blast2d", {})),

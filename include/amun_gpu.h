@@ -361,7 +361,10 @@ int amun_gpu_set_stage_kernel(int mode, int planes, int* active);
  * amun_gpu_forward_checkpointed: nsteps steps from the current state (as
  * amun_gpu_run without graphs), keeping a device copy of the state every
  * `interval` steps and each step's dt and cmax.  Afterwards the device holds
- * the final state. */
+ * the final state.  interval 0 keeps instead every stage's input primitives
+ * of every step (nsteps x stages copies of the primitive pool), so that
+ * amun_gpu_adjoint recomputes nothing; it is refused when that does not fit
+ * in device memory with 1 GiB to spare. */
 int amun_gpu_forward_checkpointed(int nsteps, double dtnext, int interval);
 
 /* nsteps (<= the recorded count) steps from the current state with the dt

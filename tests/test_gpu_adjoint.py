@@ -159,6 +159,25 @@ def test_adjoint_finite_differences_full_size():
         sim.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_adjoint_without_recomputation_equals_checkpointed(prec):
+    """Recording with interval 0 (every stage input kept, no recomputation)
+    gives the gradient of checkpointed recording bit for bit."""
+    from amun_b200.solver import Simulation
+    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    q0 = problems.smooth_mhd(mesh, seed=4)
+    out = []
+    for interval in (5, 0):
+        sim = Simulation(p, prec)
+        try:
+            out.append(gpu_gradient(sim, mesh, q0, 12, interval))
+        finally:
+            sim.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_evolve_on_cuda_tensors_matches_host_path():
     """torch.autograd through Evolve with CUDA tensors (the library reads and
     writes device memory, no host copies) gives the forward state and the
