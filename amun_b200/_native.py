@@ -113,6 +113,15 @@ def lib():
         "amun_gpu_stage": (i, [i, d, d]),
         "amun_gpu_stages": (i, [C.POINTER(i)]),
         "amun_gpu_integrals": (i, [_D]),
+        "amun_gpu_set_blocks_sharded": (i, [i, C.POINTER(amun_block_desc), C.POINTER(i), i]),
+        "amun_gpu_halo_peers": (i, [i, C.POINTER(i), C.POINTER(i), C.POINTER(C.c_longlong),
+                                    C.POINTER(C.c_longlong), C.POINTER(i)]),
+        "amun_gpu_halo_pack": (i, [vp]),
+        "amun_gpu_halo_unpack": (i, [vp]),
+        "amun_gpu_get_maxspeed": (i, [_D]),
+        "amun_gpu_set_maxspeed": (i, [d]),
+        "amun_gpu_halo_plan": (i, [i, C.POINTER(amun_block_desc), C.POINTER(i), i, i, i, i, i, C.POINTER(i),
+                                   C.POINTER(i), C.POINTER(i), C.POINTER(i)]),
         "amun_gpu_forward_checkpointed": (i, [i, d, i]),
         "amun_gpu_replay": (i, [i]),
         "amun_gpu_adjoint": (i, [_D, _D, _D]),

@@ -135,6 +135,15 @@ struct Ctx {
   // store_integrals: CTA partials and the 29 results
   double* int_buf = nullptr;
   int int_cap = 0;
+  // blocks sharded over ranks (amun_gpu_set_blocks_sharded): this rank's
+  // ghost slabs to send and to receive, per peer in rank order
+  bool sharded = false, sharding_next = false;
+  std::vector<int> halo_peers;
+  std::vector<long long> halo_send_n, halo_recv_n;  // elements per peer
+  HaloSlab* halo_send = nullptr;
+  HaloSlab* halo_recv = nullptr;
+  int halo_nsend = 0, halo_nrecv = 0;
+  long long halo_max_cells = 0;
 };
 
 // Contexts: every host thread works on its current context, which is its
@@ -284,6 +293,12 @@ void free_pool() {
   C.tile_LP = C.tile_LW = 0;
   C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
   C.stage_maps = false;
+  if (C.halo_send) cudaFree(C.halo_send);
+  if (C.halo_recv) cudaFree(C.halo_recv);
+  C.halo_send = C.halo_recv = nullptr;
+  C.halo_nsend = C.halo_nrecv = 0;
+  C.halo_peers.clear(); C.halo_send_n.clear(); C.halo_recv_n.clear();
+  C.halo_max_cells = 0;
   if (C.int_buf) cudaFree(C.int_buf);
   C.int_buf = nullptr;
   C.int_cap = 0;
@@ -1187,6 +1202,53 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
 // pressure variable (last) of the adiabatic systems; none when isothermal
 int pressure_index() { return (C.p.eqsys == EQ_HD_ISO || C.p.eqsys == EQ_MHD_ISO) ? -1 : C.nv - 1; }
 
+// The exchange plan of one rank on a mesh of one level whose leaves are
+// spread over ranks (owner[b]): the ghost slabs it receives (its blocks'
+// directions whose neighbour lives elsewhere) and those it sends (its
+// blocks as the neighbour of another rank's block).  Both sides list the
+// slabs of a peer by (receiving block, direction), so a peer's segment of
+// the send buffer matches the receiver's segment slab for slab.  Each entry:
+// peer rank, this rank's block (global id), the other block, direction,
+// cells.
+struct PlanSlab {
+  int peer, block, other, dir;
+  long long cells;
+};
+long long slab_cells(int dir, int nd, int nc, int ng) {
+  const int o[3] = {dir % 3 - 1, (dir / 3) % 3 - 1, dir / 9 - 1};
+  long long c = 1;
+  for (int a = 0; a < nd; ++a) c *= o[a] == 0 ? nc : ng;
+  return c;
+}
+int build_halo_plan(int nblocks, const amun_block_desc* d, const int* owner, int rank, int nd, int nc, int ng,
+                    std::vector<PlanSlab>& send, std::vector<PlanSlab>& recv, std::string& err) {
+  send.clear();
+  recv.clear();
+  for (int b = 0; b < nblocks; ++b) {
+    for (int n = 0; n < 27; ++n) {
+      if (n == 13 || (nd == 2 && n / 9 != 1)) continue;
+      const int nb = d[b].neighbor[n];
+      if (nb < 0 || nb >= nblocks) {
+        err = "sharded blocks need a periodic neighbour in every direction";
+        return AMUN_E_UNSUPPORTED;
+      }
+      if (d[nb].level != d[b].level) {
+        err = "sharded blocks must all be at one level";
+        return AMUN_E_UNSUPPORTED;
+      }
+      const long long cells = slab_cells(n, nd, nc, ng);
+      if (owner[b] == rank && owner[nb] != rank) recv.push_back({owner[nb], b, nb, n, cells});
+      if (owner[b] != rank && owner[nb] == rank) send.push_back({owner[b], nb, b, n, cells});
+    }
+  }
+  // peers in rank order, each peer's slabs in (receiving block, direction)
+  // order; the loops above already visit (b, n) in that order
+  auto by_peer = [](const PlanSlab& x, const PlanSlab& y) { return x.peer < y.peer; };
+  std::stable_sort(send.begin(), send.end(), by_peer);
+  std::stable_sort(recv.begin(), recv.end(), by_peer);
+  return 0;
+}
+
 template <typename R>
 cudaError_t ghost_fill(R* q) {
   if (C.amr)
@@ -1202,6 +1264,10 @@ extern "C" {
 int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
   if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
   if (nblocks <= 0 || !blocks) return fail(AMUN_E_BAD_ARGUMENT, "empty block list");
+  // a block list of one rank among several (set by amun_gpu_set_blocks_sharded
+  // for this call only): neighbours on other ranks are -1
+  C.sharded = C.sharding_next;
+  C.sharding_next = false;
   bool levels_differ = false;
   for (int b = 1; b < nblocks; ++b) levels_differ |= blocks[b].level != blocks[0].level;
   if (!levels_differ) {
@@ -1212,7 +1278,8 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
         if (nb >= nblocks) return fail(AMUN_E_BAD_ARGUMENT, "neighbour index out of range");
         if (nb >= 0 && blocks[nb].level != blocks[b].level)
           return fail(AMUN_E_BAD_ARGUMENT, "a same-level neighbour at another level");
-        if (nb < 0 && n != 13) return fail(AMUN_E_UNSUPPORTED, "non-periodic domain boundaries are not supported");
+        if (nb < 0 && n != 13 && !C.sharded)
+          return fail(AMUN_E_UNSUPPORTED, "non-periodic domain boundaries are not supported");
       }
     }
   }
@@ -1460,6 +1527,154 @@ int amun_gpu_evolve(void) {
   if ((r = evolve_launches())) return r;
   C.ms_valid = true;
   CK(cudaStreamSynchronize(C.stream));
+  return 0;
+}
+
+int amun_gpu_halo_plan(int nblocks, const amun_block_desc* blocks, const int* owner, int rank, int ndims,
+                       int ncells, int nghosts, int cap, int* nsend, int* send, int* nrecv, int* recv) {
+  if (nblocks <= 0 || !blocks || !owner || !nsend || !nrecv || (ndims != 2 && ndims != 3) || ncells <= 0 ||
+      nghosts <= 0)
+    return fail(AMUN_E_BAD_ARGUMENT, "bad arguments");
+  std::vector<PlanSlab> ps, pr;
+  std::string err;
+  if (int r = build_halo_plan(nblocks, blocks, owner, rank, ndims, ncells, nghosts, ps, pr, err)) return fail(r, err);
+  *nsend = (int)ps.size();
+  *nrecv = (int)pr.size();
+  auto put = [&](const std::vector<PlanSlab>& v, int* out) {
+    for (size_t k = 0; k < v.size() && (int)k < cap; ++k) {
+      int* e = out + 5 * k;
+      e[0] = v[k].peer; e[1] = v[k].block; e[2] = v[k].other; e[3] = v[k].dir; e[4] = (int)v[k].cells;
+    }
+  };
+  if (send) put(ps, send);
+  if (recv) put(pr, recv);
+  return 0;
+}
+
+int amun_gpu_set_blocks_sharded(int nblocks, const amun_block_desc* blocks, const int* owner, int rank) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  if (nblocks <= 0 || !blocks || !owner) return fail(AMUN_E_BAD_ARGUMENT, "empty block list");
+  if (C.p.fix_unphysical) return fail(AMUN_E_UNSUPPORTED, "fix_unphysical_cells with sharded blocks");
+  const int nd = C.p.ndims, nc = C.p.ncells, ng = C.p.nghosts;
+  std::vector<PlanSlab> ps, pr;
+  std::string err;
+  if (int r = build_halo_plan(nblocks, blocks, owner, rank, nd, nc, ng, ps, pr, err)) return fail(r, err);
+  // this rank's blocks in global order, neighbours renumbered, remote -1
+  std::vector<int> local(nblocks, -1);
+  std::vector<amun_block_desc> mine;
+  for (int b = 0; b < nblocks; ++b)
+    if (owner[b] == rank) { local[b] = (int)mine.size(); mine.push_back(blocks[b]); }
+  if (mine.empty()) return fail(AMUN_E_BAD_ARGUMENT, "no block belongs to this rank");
+  for (size_t k = 0; k < mine.size(); ++k)
+    for (int n = 0; n < 27; ++n) {
+      int& nb = mine[k].neighbor[n];
+      nb = n == 13 ? (int)k : (nb < 0 ? nb : local[nb]);
+    }
+  C.sharding_next = true;
+  int r = amun_gpu_set_blocks((int)mine.size(), mine.data());
+  if (r) return r;
+  // dx_min over every rank's blocks (new_time_step reduces the level,
+  // src/evolution.F90:459-460)
+  for (int b = 0; b < nblocks; ++b) {
+    double m = std::min(blocks[b].dx[0], blocks[b].dx[1]);
+    if (nd == 3) m = std::min(m, blocks[b].dx[2]);
+    C.dx_min = std::min(C.dx_min, m);
+  }
+  // device slab tables with offsets into the send / receive buffers
+  auto tables = [&](const std::vector<PlanSlab>& v, HaloSlab*& dev, int& n) -> int {
+    std::vector<HaloSlab> h;
+    long long off = 0;
+    for (const auto& e : v) {
+      if (C.halo_peers.empty() || C.halo_peers.back() != e.peer) {
+        if (std::find(C.halo_peers.begin(), C.halo_peers.end(), e.peer) == C.halo_peers.end())
+          C.halo_peers.push_back(e.peer);
+      }
+      h.push_back({local[e.block], e.dir, e.cells, off});
+      off += e.cells * C.nv;
+      C.halo_max_cells = std::max(C.halo_max_cells, e.cells);
+    }
+    n = (int)h.size();
+    if (n > 65535) return fail(AMUN_E_UNSUPPORTED, "more than 65535 ghost slabs cross ranks");
+    if (n) {
+      CK(cudaMalloc(&dev, h.size() * sizeof(HaloSlab)));
+      CK(h2d(dev, h.data(), h.size() * sizeof(HaloSlab)));
+    }
+    return 0;
+  };
+  if ((r = tables(ps, C.halo_send, C.halo_nsend))) return r;
+  if ((r = tables(pr, C.halo_recv, C.halo_nrecv))) return r;
+  std::sort(C.halo_peers.begin(), C.halo_peers.end());
+  C.halo_send_n.assign(C.halo_peers.size(), 0);
+  C.halo_recv_n.assign(C.halo_peers.size(), 0);
+  for (size_t k = 0; k < C.halo_peers.size(); ++k) {
+    for (const auto& e : ps) if (e.peer == C.halo_peers[k]) C.halo_send_n[k] += e.cells * C.nv;
+    for (const auto& e : pr) if (e.peer == C.halo_peers[k]) C.halo_recv_n[k] += e.cells * C.nv;
+  }
+  return 0;
+}
+
+int amun_gpu_halo_peers(int cap, int* npeers, int* ranks, long long* send_elems, long long* recv_elems,
+                        int* elem_bytes) {
+  int r = check_ready();
+  if (r) return r;
+  if (!npeers) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  *npeers = (int)C.halo_peers.size();
+  for (int k = 0; k < *npeers && k < cap; ++k) {
+    if (ranks) ranks[k] = C.halo_peers[k];
+    if (send_elems) send_elems[k] = C.halo_send_n[k];
+    if (recv_elems) recv_elems[k] = C.halo_recv_n[k];
+  }
+  if (elem_bytes) *elem_bytes = (int)rsize();
+  return 0;
+}
+
+int amun_gpu_halo_pack(void* send) {
+  int r = check_ready();
+  if (r) return r;
+  if (!C.halo_nsend) return 0;
+  if (!send) return fail(AMUN_E_BAD_ARGUMENT, "null buffer");
+  cudaError_t e = bulk() ? Launch<float, float>::halo(true, (float*)C.q[C.cur], (float*)send, C.halo_send,
+                                                      C.halo_nsend, C.halo_max_cells, C.g, C.nv, C.stream)
+                         : Launch<double, double>::halo(true, (double*)C.q[C.cur], (double*)send, C.halo_send,
+                                                        C.halo_nsend, C.halo_max_cells, C.g, C.nv, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "halo pack");
+  return 0;
+}
+
+int amun_gpu_halo_unpack(const void* recv) {
+  int r = check_ready();
+  if (r) return r;
+  if (!C.halo_nrecv) return 0;
+  if (!recv) return fail(AMUN_E_BAD_ARGUMENT, "null buffer");
+  cudaError_t e = bulk() ? Launch<float, float>::halo(false, (float*)C.q[C.cur], (float*)recv, C.halo_recv,
+                                                      C.halo_nrecv, C.halo_max_cells, C.g, C.nv, C.stream)
+                         : Launch<double, double>::halo(false, (double*)C.q[C.cur], (double*)recv, C.halo_recv,
+                                                        C.halo_nrecv, C.halo_max_cells, C.g, C.nv, C.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "halo unpack");
+  // the maximum speed of the state is unaffected (ghost cells are not in it)
+  return 0;
+}
+
+int amun_gpu_get_maxspeed(double* ms) {
+  int r = check_ready();
+  if (r) return r;
+  if (!ms) return fail(AMUN_E_BAD_ARGUMENT, "null argument");
+  if ((r = ensure_maxspeed())) return r;
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, &C.sc->ms_bits, sizeof(bits), cudaMemcpyDeviceToHost, C.stream));
+  CK(cudaStreamSynchronize(C.stream));
+  memcpy(ms, &bits, sizeof(double));
+  return 0;
+}
+
+int amun_gpu_set_maxspeed(double ms) {
+  int r = check_ready();
+  if (r) return r;
+  if (!(ms >= 0.0)) return fail(AMUN_E_BAD_ARGUMENT, "the maximum speed must be >= 0");
+  unsigned long long bits;
+  memcpy(&bits, &ms, sizeof(bits));
+  CK(h2d(&C.sc->ms_bits, &bits, sizeof(bits)));
+  C.ms_valid = true;
   return 0;
 }
 

@@ -10,6 +10,9 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t sweep(int eq, int rec, int rs, int dir, const SweepArgs<R, U1T>& a, dim3 grid, int threads,
                            size_t smem, cudaStream_t s);
   static cudaError_t ghost(R* q, const int* nbr, const Geo& g, int nv, int nblocks, cudaStream_t s);
+  // ghost slabs exchanged with other ranks: pack from q into buf or unpack
+  static cudaError_t halo(bool pack, R* q, R* buf, const HaloSlab* tab, int nslabs, long long max_cells, const Geo& g,
+                          int nv, cudaStream_t s);
   // meshes with level jumps: copies and restrictions, then prolongations
   static cudaError_t amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
                                const Geo& g, int nv, int ipr, int plim, double eps, cudaStream_t s);
@@ -153,6 +156,17 @@ cudaError_t Launch<R, U1T>::sweep(int eq, int rec, int rs, int dir, const SweepA
   if (eq == EQ_HD_ISO) return sweep_eq<R, U1T, EQ_HD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
   if (eq == EQ_MHD_ISO) return sweep_eq<R, U1T, EQ_MHD_ISO>(rec, rs, dir, a, grid, threads, smem, s);
   return sweep_eq<R, U1T, EQ_SRMHD>(rec, rs, dir, a, grid, threads, smem, s);
+}
+
+template <typename R, typename U1T>
+cudaError_t Launch<R, U1T>::halo(bool pack, R* q, R* buf, const HaloSlab* tab, int nslabs, long long max_cells,
+                                 const Geo& g, int nv, cudaStream_t s) {
+  if (nslabs <= 0) return cudaSuccess;
+  const int threads = 256;
+  dim3 grid(grid_for(max_cells, threads, 512), nslabs);
+  if (pack) halo_slab_kernel<R, true><<<grid, threads, 0, s>>>(q, buf, tab, g, nv);
+  else halo_slab_kernel<R, false><<<grid, threads, 0, s>>>(q, buf, tab, g, nv);
+  return cudaGetLastError();
 }
 
 template <typename R, typename U1T>

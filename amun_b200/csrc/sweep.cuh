@@ -960,6 +960,43 @@ __global__ void ghost_copy_kernel(R* q, const int* nbr, Geo g, int nv, long long
 }
 
 // ---------------------------------------------------------------------------
+// Ghost slabs of blocks whose same-level neighbour lives on another rank.
+// Slab s covers the ghost cells of block `dst_block` (on the receiving rank)
+// in direction `dir` (n = (ox+1) + 3 (oy+1) + 9 (oz+1)); its values are the
+// neighbour's cells (i - ox nc, j - oy nc, k - oz nc), the source of the
+// same-level copy of boundaries_*_copy (src/boundaries.F90:1273-1635).  The
+// sender packs them from its block `block` into buf[off + v cells + t], the
+// receiver unpacks them into its block `block`'s ghost cells.
+// ---------------------------------------------------------------------------
+struct HaloSlab {
+  int block, dir;
+  long long cells, off;
+};
+
+template <typename R, bool PACK>
+__global__ void halo_slab_kernel(R* q, R* buf, const HaloSlab* __restrict__ tab, Geo g, int nv) {
+  const HaloSlab s = tab[blockIdx.y];
+  const int nc = g.nc, ng = g.ng;
+  const int ox = s.dir % 3 - 1, oy = (s.dir / 3) % 3 - 1, oz = s.dir / 9 - 1;
+  auto lo = [&](int o) { return o < 0 ? 0 : (o == 0 ? ng : ng + nc); };
+  auto len = [&](int o) { return o == 0 ? nc : ng; };
+  const int lx = len(ox), ly = len(oy);
+  const int x0 = lo(ox), y0 = lo(oy), z0 = g.ndims == 3 ? lo(oz) : 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < s.cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = x0 + (int)(t % lx), j = y0 + (int)((t / lx) % ly), k = z0 + (int)(t / ((long long)lx * ly));
+    const long long c = PACK ? ((long long)(k - oz * nc) * g.JM + (j - oy * nc)) * g.IM + (i - ox * nc)
+                             : ((long long)k * g.JM + j) * g.IM + i;
+    R* qb = q + (long long)s.block * g.qbs + c;
+    R* bb = buf + s.off + t;
+    for (int v = 0; v < nv; ++v) {
+      if (PACK) bb[(long long)v * s.cells] = qb[(long long)v * g.qvs];
+      else qb[(long long)v * g.qvs] = bb[(long long)v * s.cells];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Ghost fill on meshes with level jumps (boundary_variables,
 // src/boundaries.F90:372-479): one operation per ghost cell, built on the
 // host from the block positions.  dst/src are (block * qbs + padded cell);

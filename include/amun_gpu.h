@@ -248,6 +248,41 @@ int amun_gpu_new_time_step(double dtnext, double* cmax, double* dt);
  * including ghost fill and primitive update after each stage. */
 int amun_gpu_evolve(void);
 
+/* Blocks spread over ranks, one process (and GPU) per rank, as the
+ * reference spreads its leaves over MPI processes (src/mesh.F90:652-721) and
+ * exchanges ghost slabs between them every stage (boundaries_*_copy with
+ * exchange_real_arrays, src/boundaries.F90:1554, src/mpitools.F90:1472-1539).
+ * Every rank passes the whole leaf list (global neighbour ids) and the rank
+ * owning each leaf; the context keeps the leaves of `rank`.  Same-level
+ * meshes only (every leaf at one level, periodic).  A ghost cell whose
+ * source leaf lives on another rank is filled by amun_gpu_halo_unpack from
+ * the buffer the caller received: after every stage (amun_gpu_stage) the
+ * caller packs this rank's outgoing slabs (amun_gpu_halo_pack), exchanges
+ * each peer's segment (one send and one receive per peer, e.g. NCCL), and
+ * unpacks.  Buffers are device memory of elements of the stage precision
+ * (elem_bytes: 8 plain, 4 FP32 bulk), peers' segments back to back in
+ * ascending rank order; within a segment the slabs are ordered by
+ * (receiving leaf, direction) on both sides.  The time step needs the
+ * maximum speed over all ranks (reduce_maximum_real,
+ * src/evolution.F90:459-460): amun_gpu_get_maxspeed gives this rank's,
+ * amun_gpu_set_maxspeed installs the reduced one before
+ * amun_gpu_new_time_step.  pack/unpack are queued on the library stream and
+ * do not synchronise. */
+int amun_gpu_set_blocks_sharded(int nblocks, const amun_block_desc* blocks, const int* owner, int rank);
+int amun_gpu_halo_peers(int cap, int* npeers, int* ranks, long long* send_elems, long long* recv_elems,
+                        int* elem_bytes);
+int amun_gpu_halo_pack(void* send);
+int amun_gpu_halo_unpack(const void* recv);
+int amun_gpu_get_maxspeed(double* ms);
+int amun_gpu_set_maxspeed(double ms);
+/* The exchange plan alone (host only, no device or context needed): the
+ * slabs `rank` sends and receives, 5 ints each -- peer rank, this rank's
+ * leaf, the other leaf, direction (0..26, (dx+1) + 3 (dy+1) + 9 (dz+1)),
+ * cells -- in buffer order; *nsend / *nrecv are the counts (up to `cap`
+ * entries are written). */
+int amun_gpu_halo_plan(int nblocks, const amun_block_desc* blocks, const int* owner, int rank, int ndims,
+                       int ncells, int nghosts, int cap, int* nsend, int* send, int* nrecv, int* recv);
+
 /* store_integrals (src/integrals.F90:254-485) of the current state on the
  * device, returned instead of written to the integrals and statistics
  * files.  out[0..7]: inarr(1:8) -- mass, x/y/z momentum, total, kinetic,
