@@ -702,6 +702,14 @@ int unit_cell_sizes(const double* dx, UnitArgs& u) {
   return 0;
 }
 
+// the step's dt and time in the device scalars (amun_gpu_stage)
+__global__ void set_step_kernel(DevScalars* sc, double dt, double t) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    sc->dt = dt;
+    sc->time = t;
+  }
+}
+
 // adds a per-call event counter of a unit entry point to the context's
 // status counter (amun_status.nonpositive)
 __global__ void add_counter_kernel(unsigned long long* dst, const unsigned long long* src) {
@@ -1722,10 +1730,10 @@ int amun_gpu_stage(int s, double t, double dt) {
   if (s < 1 || s > (int)S.stages.size())
     return fail(AMUN_E_BAD_ARGUMENT, "stage must be 1.." + std::to_string(S.stages.size()));
   if (!(dt > 0.0)) return fail(AMUN_E_BAD_ARGUMENT, "dt must be positive");
-  // the step's dt (the module dt of the reference's evolve_*) and time
-  double v[2] = {dt, t};
-  CK(h2d(&C.sc->dt, &v[0], sizeof(double)));
-  CK(h2d(&C.sc->time, &v[1], sizeof(double)));
+  // the step's dt (the module dt of the reference's evolve_*) and time,
+  // written by a kernel so that nothing waits for the host
+  set_step_kernel<<<1, 1, 0, C.stream>>>(C.sc, dt, t);
+  CK(cudaGetLastError());
   if (s == 1) {
     // the final stage re-arms the max-speed accumulator of the new state
     CK(cudaMemsetAsync(&C.sc->ms_bits, 0, sizeof(unsigned long long), C.stream));
@@ -1741,7 +1749,6 @@ int amun_gpu_stage(int s, double t, double dt) {
   r = bulk() ? launch_stage<float>(st) : launch_stage<double>(st);
   if (r) return r;
   if (st.final_stage) C.ms_valid = true;
-  CK(cudaStreamSynchronize(C.stream));
   return 0;
 }
 

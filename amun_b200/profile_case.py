@@ -8,6 +8,9 @@ end of step).
 
     python -m amun_b200.profile_case --precision fp32 --n 128 --steps 2
 
+With --stage-kernel: one fused launch per stage (amun_gpu_set_stage_kernel)
+instead of the three sweeps.
+
 With --adjoint: the differentiation workload instead (2D GLM-MHD 256^2, smooth
 seeded state, WENO-Z, HLL, SSPRK(3,3)): `--steps` recorded steps with one
 checkpoint, then one adjoint of J = kinetic energy in [0,0.25]^2.
@@ -43,6 +46,7 @@ def main(argv=None):
     ap.add_argument("--adjoint", action="store_true")
     ap.add_argument("--regrid", action="store_true")
     ap.add_argument("--maxlev", type=int, default=3)
+    ap.add_argument("--stage-kernel", action="store_true", help="one fused launch per stage instead of the sweeps")
     a = ap.parse_args(argv)
     if a.adjoint:
         return adjoint_case(a)
@@ -55,6 +59,8 @@ def main(argv=None):
              nghosts=2 if a.reconstruction == "tvd" else 4, ncells=a.n, xmin=0, xmax=1, ymin=0, ymax=1,
              zmin=0, zmax=1)
     sim = Simulation(p, precision=a.precision)
+    if a.stage_kernel and not sim.set_stage_kernel(1):
+        raise SystemExit("the fused stage kernel does not cover this configuration")
     sim.set_primitive(problems.turbulence(sim.mesh, 5.0 / 3.0, seed=0))
     for _ in range(a.steps):
         t, dt = sim.advance(1.0e30)

@@ -112,6 +112,26 @@ class ShardedSimulation:
         N.check(self.L.amun_gpu_set_time(0.0, 0.0))
         self.time = 0.0
 
+    def set_primitive_blocks(self, qb: np.ndarray):
+        """This rank's block arrays of primitives (Fortran layout, ghost
+        entries ignored) as the state; the caller exchanges afterwards."""
+        qb = np.ascontiguousarray(qb, dtype=np.float64)
+        ub = np.empty_like(qb)
+        N.check(self.L.amun_gpu_prim2cons(qb.size // self.nv, N.dptr(qb), N.dptr(ub)))
+        N.check(self.L.amun_gpu_upload_blocks(0, len(self.mine), N.dptr(ub), N.dptr(qb)))
+        N.check(self.L.amun_gpu_boundary_variables())
+        N.check(self.L.amun_gpu_set_time(0.0, 0.0))
+        self.time = 0.0
+
+    def upload_conserved(self, ub: np.ndarray):
+        """This rank's conserved block arrays (Fortran layout, host or
+        device); primitives and local ghosts are rebuilt on the device, the
+        caller exchanges the remote ghosts afterwards."""
+        N.check(self.L.amun_gpu_upload_conserved(0, len(self.mine), N.dptr(ub)))
+
+    def download_conserved(self, ub: np.ndarray):
+        N.check(self.L.amun_gpu_download_blocks(0, len(self.mine), N.dptr(ub), None))
+
     def blocks(self):
         """(u0, q) block arrays of this rank's leaves (Fortran layout)."""
         shp = (len(self.mine), self.mesh.km, self.mesh.jm, self.mesh.im, self.nv)

@@ -449,6 +449,95 @@ def run_reference(args):
     return 0
 
 
+def sharded_main(args, torch, dist, ws, rank, local):
+    """N GPUs: the 128^3 box repeated N times along x, one 128^3 block per
+    rank (weak scaling), the leaves spread over the ranks as the reference
+    spreads them over MPI processes; every stage exchanges the ghost slabs
+    between neighbouring ranks (NCCL send/receive of the packed slabs) and
+    every step reduces the maximum speed over the ranks."""
+    from amun_b200.mesh import UniformMesh
+    from amun_b200.params import geometry
+    from amun_b200.shards import ShardedSimulation
+    p = dict(WORKLOAD, xblocks=ws, xmax=float(ws))
+    box = UniformMesh(geometry(WORKLOAD))
+    qb = box.to_blocks(initial_state(box))  # every rank's block: the periodic box
+    dtnext = 1.0e30
+    stream = torch.cuda.current_stream()
+    results = {}
+    for prec in ("fp64", "fp32"):
+        sim = ShardedSimulation(p, rank, ws, precision=prec)
+        sim.set_primitive_blocks(qb)
+        sim.exchange()
+        for _ in range(args.warmup):
+            sim.advance(dtnext)
+        dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            a.record(stream)
+            for _ in range(args.steps):
+                sim.advance(dtnext)
+            b.record(stream)
+            torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        results[prec] = {"ms": ms, "clocks": clk.summary(),
+                         "zu_per_s": ws * NCELL * args.steps / (ms * 1e-3)}
+        # e2e: each rank uploads its block's conserved state from pinned host
+        # memory, the ranks advance one step together and read it back
+        if prec == "fp32":
+            shp = qb.shape
+            uh = torch.empty(shp, dtype=torch.float64, pin_memory=True).numpy()
+            sim.download_conserved(uh)
+            e2e_steps = max(3, min(args.steps, 10))
+            dist.barrier()
+            torch.cuda.synchronize()
+            a.record(stream)
+            for _ in range(e2e_steps):
+                sim.upload_conserved(uh)
+                sim.exchange()
+                sim.advance(dtnext)
+                sim.download_conserved(uh)
+            b.record(stream)
+            torch.cuda.synchronize()
+            t = torch.tensor([a.elapsed_time(b) / e2e_steps], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+            nb = int(np.prod(shp)) * 8
+            results["e2e"] = {"value": ws * NCELL / (e2e_ms * 1e-3), "unit": "zone-updates/s",
+                              "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": e2e_ms,
+                              "per_rank": True}
+        sim.close()
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        r32, r64 = results["fp32"], results["fp64"]
+        achieved = (r32["zu_per_s"] / ws) * B_ZU["fp32"] / 1e9
+        line = {
+            "metric": METRIC, "value": r32["zu_per_s"], "unit": "zone-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r32["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-phase velocity, PCG64 seed 0)",
+            "config": {"workload": f"mhd3d-{ws}x128 x 128 x 128-periodic weno5z hlld ssprk(3,3) cfl0.4",
+                       "cells_per_gpu": NCELL, "blocks": f"{ws} blocks of 128^3, one per rank",
+                       "parallelism": f"blocks sharded over {ws} ranks: ghost slabs exchanged every stage "
+                                      f"(NCCL send/receive), max speed all-reduced every step",
+                       "l2": "state arrays larger than L2 (>= 0.5 GB resident per GPU)",
+                       "precision": "FP32 reconstruction/fluxes/increments, FP64 U^n and stage combination"},
+            "fp64": {"value": r64["zu_per_s"], "ms_per_step": r64["ms"] / args.steps},
+            "speedup_fp32_over_fp64": r32["zu_per_s"] / r64["zu_per_s"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "whole SSPRK step per GPU (432 B/zone-update)"},
+            "cpu_baseline": None, "e2e": results.get("e2e"),
+            "gpu_launches": (LAUNCHES_PER_STEP + 2 * 3) * args.steps,
+            "clocks": r32["clocks"] or {},
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,7 +558,10 @@ def main():
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+        try:
+            return sharded_main(args, torch, dist, ws, rank, local)
+        finally:
+            dist.destroy_process_group()
 
     def barrier():
         if pg:
@@ -617,15 +709,17 @@ def main():
         zu = r32["zu_per_s"]
         per_gpu = zu / ws
         achieved = per_gpu * B_ZU["fp32"] / 1e9
-        # DRAM bytes (read + write) of one FP32 step of this workload, from
-        # `ncu --set full -k regex:sweep_kernel -s 3 -c 3` on
-        # `python -m amun_b200.profile_case --precision fp32 --n 128 --steps 1`
-        # (the x, y, z sweeps of the middle stage: 120.7, 206.7 and 532.3 MB),
-        # times three stages; the ghost fills add under 1 %
-        traffic = 3 * (120.7e6 + 206.7e6 + 532.3e6) if WORKLOAD.get("ncells") == 128 else None
+        # DRAM bytes (read + write) of one FP32 step of this workload with the
+        # sweeps, from profiles/sweep_mhd3d_128_full.md (`ncu --set full -k
+        # regex:sweep_kernel -s 3 -c 3` on `python -m amun_b200.profile_case
+        # --precision fp32 --n 128 --steps 1`: the x, y, z sweeps of the middle
+        # stage, 123.5, 205.7 and 527.9 MB) times three stages; the ghost
+        # fills add under 1 %.  Only this workload was captured.
+        traffic = 3 * (123.5e6 + 205.7e6 + 527.9e6) if WORKLOAD.get("ncells") == 128 else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind,
                     "kernel": "stage sweeps x/y/z + ghost fill (whole SSPRK step, 432 B/zone-update)",
+                    "traffic_source": "profiles/sweep_mhd3d_128_full.md (ncu, same build, same workload)",
                     "traffic": traffic, "traffic_unit": "bytes per step and GPU",
                     "traffic_per_zone_update": traffic / NCELL if traffic else None,
                     "fp64": {"achieved": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9,

@@ -306,7 +306,8 @@ int amun_gpu_integrals(double* out);
  * stage applies the GLM psi decay and leaves the new state's maximum speed
  * for the next new_time_step.  Calling stages 1..n in order with the dt of
  * new_time_step gives the results of amun_gpu_evolve bit for bit.  The time
- * is not advanced (the driver does that, src/driver.F90:579-585). */
+ * is not advanced (the driver does that, src/driver.F90:579-585).  The
+ * stage is queued on the library stream; the call does not wait for it. */
 int amun_gpu_stage(int s, double t, double dt);
 /* The number of stages of the selected integrator. */
 int amun_gpu_stages(int* nstages);
