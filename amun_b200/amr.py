@@ -23,20 +23,22 @@ from . import _native as N
 
 
 class BlockView:
-    """One block seen as a small uniform mesh (for initial conditions)."""
+    """One block seen as a small uniform mesh (for initial conditions): its
+    interior cells, or with `ghosts` layers of ghost cells around them (the
+    cells setup_problem fills, at their own unwrapped coordinates)."""
 
-    def __init__(self, amr, level, cx, cy, cz):
+    def __init__(self, amr, level, cx, cy, cz, ghosts=0):
         self.ndims = amr.ndims
         self.nc = amr.nc
         self.dx, self.dy, self.dz = amr.level_dx(level)
-        self.x0 = amr.xmin + cx * self.nc * self.dx
-        self.y0 = amr.ymin + cy * self.nc * self.dy
-        self.z0 = amr.zmin + cz * self.nc * self.dz if self.ndims == 3 else 0.0
-        n = self.nc
+        self.x0 = amr.xmin + (cx * self.nc - ghosts) * self.dx
+        self.y0 = amr.ymin + (cy * self.nc - ghosts) * self.dy
+        self.z0 = amr.zmin + (cz * self.nc - ghosts) * self.dz if self.ndims == 3 else 0.0
+        n = self.n = self.nc + 2 * ghosts
         self.shape = (n if self.ndims == 3 else 1, n, n)
 
     def cell_centres(self):
-        n = self.nc
+        n = self.n
         x = self.x0 + (np.arange(n) + 0.5) * self.dx
         y = self.y0 + (np.arange(n) + 0.5) * self.dy
         z = self.z0 + (np.arange(n) + 0.5) * self.dz if self.ndims == 3 else np.zeros(1)
@@ -323,18 +325,24 @@ class AMRMesh:
         view["coord"] = t[:, 1:]
         return arr
 
-    def view(self, b):
+    def view(self, b, ghosts=False):
         l, cx, cy, cz = self.order[b]
-        return BlockView(self, l, cx, cy, cz)
+        return BlockView(self, l, cx, cy, cz, self.ng if ghosts else 0)
 
-    def blocks_from(self, fn, nv):
+    def blocks_from(self, fn, nv, ghosts=False, only=None):
         """Block arrays (nblocks, km, jm, im, nv) whose interiors are fn(view)
-        ((nz, ny, nx, nv) of each block); ghost entries are zero."""
+        ((nz, ny, nx, nv) of each block); ghost entries are zero, or with
+        `ghosts` fn of the whole padded block.  With `only` (one flag per
+        block) the other blocks stay zero."""
         out = np.zeros((self.nblocks, self.km, self.jm, self.im, nv))
         ng, nc = self.ng, self.nc
         for b in range(self.nblocks):
-            q = fn(self.view(b))
-            if self.ndims == 3:
+            if only is not None and not only[b]:
+                continue
+            q = fn(self.view(b, ghosts))
+            if ghosts:
+                out[b] = q
+            elif self.ndims == 3:
                 out[b, ng:ng + nc, ng:ng + nc, ng:ng + nc] = q
             else:
                 out[b, 0, ng:ng + nc, ng:ng + nc] = q[0]

@@ -104,6 +104,8 @@ struct Ctx {
   int* fquad = nullptr;      // [b][dir][side][4]
   int* blist = nullptr;      // blocks ordered finest level first
   void* ff = nullptr;        // stored face fluxes
+  int* fcount = nullptr;     // [b][dir][side] tiles that stored a face (one launch over all levels)
+  bool level_launches = false;  // one sweep launch per level instead of one over all levels
   std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
   // sweep tile chosen by amun_gpu_autotune (0: the default shape)
   int tile_LP = 0, tile_LW = 0;
@@ -273,10 +275,10 @@ void free_pool() {
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   for (auto& x : C.q)
     if (x) { cudaFree(x); x = nullptr; }
-  void* amrp[] = {C.gop, C.frole, C.fquad, C.blist, C.ff};
+  void* amrp[] = {C.gop, C.frole, C.fquad, C.blist, C.ff, C.fcount};
   for (void* x : amrp)
     if (x) cudaFree(x);
-  C.gop = nullptr; C.frole = C.fquad = C.blist = nullptr; C.ff = nullptr;
+  C.gop = nullptr; C.frole = C.fquad = C.blist = C.fcount = nullptr; C.ff = nullptr;
   if (C.fix_idx) cudaFree(C.fix_idx);
   if (C.fix_val) cudaFree(C.fix_val);
   C.fix_idx = nullptr; C.fix_val = nullptr; C.fix_cap = 0;
@@ -558,7 +560,7 @@ int launch_stage(const StageDesc& st) {
   a.m = method_const();
   a.st = st;
   a.LP = LP; a.LW = LW;
-  a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr;
+  a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr; a.fcount = nullptr; a.nfcount = 0;
   a.fcl = (const R*)C.fcl; a.fcr = (const R*)C.fcr;
   a.ugp = C.ugp;
   const int rs = effective_solver();
@@ -589,9 +591,21 @@ int launch_stage(const StageDesc& st) {
       if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
       continue;
     }
-    // level jumps: one launch per level, finest first, so the finer face
-    // fluxes a coarse block takes are stored before it runs
+    // level jumps: one launch over every level, blocks finest first, the
+    // coarse faces waiting in the kernel for the finer face fluxes they take
+    // (or one launch per level, finest first)
     a.frole = C.frole; a.fquad = C.fquad; a.ff = (R*)C.ff;
+    if (!C.level_launches) {
+      CK(cudaMemsetAsync(C.fcount, 0, ((size_t)C.nblocks * 6 + 1) * sizeof(int), C.stream));
+      a.blist = C.blist;
+      a.fcount = C.fcount;
+      a.nfcount = C.nblocks * 6;
+      dim3 gl(grid.x, C.nblocks);
+      cudaError_t e = Launch<R, R>::sweep(C.p.eqsys, sweep_variant(), rs, d, a, gl, threads, smem, C.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+      continue;
+    }
+    a.fcount = nullptr;
     for (const auto& grp : C.lgroups) {
       a.blist = C.blist + grp.first;
       dim3 gl(grid.x, grp.second);
@@ -700,6 +714,16 @@ int unit_cell_sizes(const double* dx, UnitArgs& u) {
   }
   for (int d = 0; d < C.p.ndims; ++d) u.h[d] = dx[d];
   return 0;
+}
+
+// waits (bounded) on a count nothing raises, as the sweeps wait on the face
+// counts of finer blocks: the wait must give up and record a stall
+__global__ void wait_selftest_kernel(DevScalars* sc, long long cycles) {
+  __shared__ int never;
+  if (threadIdx.x == 0) {
+    never = 0;
+    if (!wait_count_bounded(&never, 1, cycles)) atomicAdd(&sc->stalls, 1ull);
+  }
 }
 
 // the step's dt and time in the device scalars (amun_gpu_stage)
@@ -1195,6 +1219,7 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
   CK(cudaMalloc(&C.fquad, quad.size() * sizeof(int)));
   CK(cudaMalloc(&C.blist, order.size() * sizeof(int)));
   CK(cudaMalloc(&C.ff, (size_t)nblocks * 6 * C.nv * NT * rsize()));
+  CK(cudaMalloc(&C.fcount, ((size_t)nblocks * 6 + 1) * sizeof(int)));
   if (!all.empty()) CK(h2d(C.gop, all.data(), all.size() * sizeof(GhostOp)));
   CK(h2d(C.frole, role.data(), role.size() * sizeof(int)));
   CK(h2d(C.fquad, quad.data(), quad.size() * sizeof(int)));
@@ -1764,6 +1789,7 @@ int amun_gpu_advance(double dtnext, double* time, double* dt) {
     CK(cudaStreamSynchronize(C.stream));
     if (time) *time = h.time;
     if (dt) *dt = h.dt;
+    if (h.stalls) return fail(AMUN_E_CUDA, "a device wait gave up (amun_status.stalls)");
   } else {
     CK(cudaStreamSynchronize(C.stream));
   }
@@ -2126,6 +2152,33 @@ int amun_gpu_set_stream(void* stream) {
   for (auto& gx : C.graph)
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   C.stream = stream ? (cudaStream_t)stream : C.own_stream;
+  return 0;
+}
+
+int amun_gpu_set_level_launches(int per_level) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  CK(cudaStreamSynchronize(C.stream));
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  C.level_launches = per_level != 0;
+  return 0;
+}
+
+int amun_gpu_wait_selftest(long long cycles, int* gave_up) {
+  int r = check_ready();
+  if (r) return r;
+  if (!gave_up || cycles < 0) return fail(AMUN_E_BAD_ARGUMENT, "bad arguments");
+  DevScalars h{};
+  CK(cudaMemcpyAsync(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+  CK(cudaStreamSynchronize(C.stream));
+  const unsigned long long before = h.stalls;
+  wait_selftest_kernel<<<1, 32, 0, C.stream>>>(C.sc, cycles);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&h, C.sc, sizeof(h), cudaMemcpyDeviceToHost, C.stream));
+  CK(cudaStreamSynchronize(C.stream));
+  *gave_up = h.stalls > before ? 1 : 0;
+  // the count is the selftest's, not the state's
+  CK(h2d(&C.sc->stalls, &before, sizeof(before)));
   return 0;
 }
 

@@ -113,6 +113,14 @@ template <typename R, typename U1T> struct SweepArgs {
   const int* fquad;    // [b][dir][side][4]: finer block of each quarter of
                        // the face (transverse halves a + 2 b)
   R* ff;               // [b][dir][side][v][transverse] stored face fluxes
+  // one launch over every level (blist finest first): tiles that stored a
+  // face count themselves in fcount[b][dir][side] (cleared before the
+  // launch); a tile replacing its face fluxes waits for the count of each
+  // finer neighbour's face.  Null when each level has its own launch.
+  // fcount[nblocks * 6] is the launch's ticket: CTAs take their tile in the
+  // order they start, so every tile waited on belongs to a running CTA.
+  int* fcount;
+  int nfcount;
   // compact reconstructions: this direction's face values from the line
   // pass, in the layout of q (fcl the reference's fl, fcr its fr)
   const R* fcl;
@@ -122,6 +130,35 @@ template <typename R, typename U1T> struct SweepArgs {
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
+
+// a load through L2 that the compiler keeps after the preceding barrier
+// (the ld.global.cg intrinsic is a plain asm the compiler may hoist above the
+// wait that makes the data valid)
+__device__ __forceinline__ double ld_l2_ordered(const double* p) {
+  double r;
+  asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(r) : "l"(p) : "memory");
+  return r;
+}
+__device__ __forceinline__ float ld_l2_ordered(const float* p) {
+  float r;
+  asm volatile("ld.global.cg.f32 %0, [%1];" : "=f"(r) : "l"(p) : "memory");
+  return r;
+}
+
+// ~1 s at the B200's clocks: far beyond any dependency inside one launch
+constexpr long long kDeviceWaitCycles = 2000000000LL;
+
+// waits until *c >= expect (another CTA of the same launch raises it);
+// false after ~limit cycles (the caller records the failure)
+__device__ __forceinline__ bool wait_count_bounded(const int* c, int expect, long long limit) {
+  if (*(volatile const int*)c >= expect) return true;
+  const long long t0 = clock64();
+  while (*(volatile const int*)c < expect) {
+    if (clock64() - t0 > limit) return false;
+    __nanosleep(200);
+  }
+  return true;
+}
 
 // block-wide max of non-negative doubles, then one atomicMax per CTA on the
 // ordered bit image (non-negative IEEE doubles order like their bits)
@@ -349,8 +386,16 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
 
   const int nc = g.nc, ng = g.ng;
-  const int b = a.blist ? a.blist[blockIdx.y] : (int)blockIdx.y;
-  int tile = blockIdx.x;
+  int bx = blockIdx.x, by = blockIdx.y;
+  if (a.fcount) {
+    __shared__ int ticket;
+    if (threadIdx.x == 0) ticket = atomicAdd(a.fcount + a.nfcount, 1);
+    __syncthreads();
+    bx = ticket % gridDim.x;
+    by = ticket / gridDim.x;
+  }
+  const int b = a.blist ? a.blist[by] : by;
+  int tile = bx;
   const int ntp = nc / LP, ntl = nc / LW;
   const int tp = tile % ntp; tile /= ntp;
   const int tl = tile % ntl; tile /= ntl;
@@ -683,29 +728,61 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       const long long NT = (long long)nc * (g.ndims == 3 ? nc : 1);
       const int half = nc / 2;
       const int tb = g.ndims == 3 ? th : 0;
+      // the stores of this tile's coarser-side faces first, then their count
       for (int side = 0; side < 2; ++side) {
-        const int role = side ? rhi : rlo;
-        if (!role) continue;
+        if ((side ? rhi : rlo) != 1) continue;
         const int pf = side ? LP : 0;
         const int slab = (b * 3 + DIR) * 2 + side;
         for (int t = threadIdx.x; t < LW * NV; t += blockDim.x) {
           const int ll = t % LW, v = t / LW;
           const int ta = l0 - ng + ll;
-          if (role == 1) {
-            a.ff[((long long)slab * NV + v) * NT + ta + (long long)nc * tb] = Fs[sidx(v, pf, ll, NPI)];
-          } else {
-            const int fb = a.fquad[slab * 4 + ta / half + 2 * (tb / half)];
-            const int fa = 2 * (ta % half), fbb = 2 * (tb % half);
-            const R* F = a.ff + ((long long)((fb * 3 + DIR) * 2 + (1 - side)) * NV + v) * NT;
-            R val;
-            if (g.ndims == 2) {
-              val = (F[fa] + F[fa + 1]) / R(2);
-            } else {
-              val = ((F[fa + (long long)nc * fbb] + F[fa + 1 + (long long)nc * (fbb + 1)]) +
-                     (F[fa + (long long)nc * (fbb + 1)] + F[fa + 1 + (long long)nc * fbb])) / R(4);
+          a.ff[((long long)slab * NV + v) * NT + ta + (long long)nc * tb] = Fs[sidx(v, pf, ll, NPI)];
+        }
+      }
+      if (a.fcount) {
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          for (int side = 0; side < 2; ++side)
+            if ((side ? rhi : rlo) == 1) atomicAdd(&a.fcount[(b * 3 + DIR) * 2 + side], 1);
+          // every tile of a finer neighbour's face has stored it (finer
+          // levels come first in the launch and never wait on coarser ones)
+          const int expect = (nc / LW) * (g.ndims == 3 ? nc : 1);
+          bool ok = true;
+          for (int side = 0; side < 2 && ok; ++side) {
+            if ((side ? rhi : rlo) != 2) continue;
+            const int slab = (b * 3 + DIR) * 2 + side;
+            for (int q = 0; q < (g.ndims == 3 ? 4 : 2) && ok; ++q) {
+              const int fb = a.fquad[slab * 4 + q];
+              if (fb < 0) continue;
+              ok = wait_count_bounded(&a.fcount[(fb * 3 + DIR) * 2 + (1 - side)], expect, kDeviceWaitCycles);
             }
-            Fs[sidx(v, pf, ll, NPI)] = val;
           }
+          if (!ok) atomicAdd(&a.sc->stalls, 1ull);
+          __threadfence();
+        }
+        __syncthreads();
+      }
+      for (int side = 0; side < 2; ++side) {
+        if ((side ? rhi : rlo) != 2) continue;
+        const int pf = side ? LP : 0;
+        const int slab = (b * 3 + DIR) * 2 + side;
+        for (int t = threadIdx.x; t < LW * NV; t += blockDim.x) {
+          const int ll = t % LW, v = t / LW;
+          const int ta = l0 - ng + ll;
+          const int fb = a.fquad[slab * 4 + ta / half + 2 * (tb / half)];
+          const int fa = 2 * (ta % half), fbb = 2 * (tb % half);
+          const R* F = a.ff + ((long long)((fb * 3 + DIR) * 2 + (1 - side)) * NV + v) * NT;
+          // through L2, after the wait: written by other CTAs of this launch
+          auto ld = [&](long long o) -> R { return ld_l2_ordered(F + o); };
+          R val;
+          if (g.ndims == 2) {
+            val = (ld(fa) + ld(fa + 1)) / R(2);
+          } else {
+            val = ((ld(fa + (long long)nc * fbb) + ld(fa + 1 + (long long)nc * (fbb + 1))) +
+                   (ld(fa + (long long)nc * (fbb + 1)) + ld(fa + 1 + (long long)nc * fbb))) / R(4);
+          }
+          Fs[sidx(v, pf, ll, NPI)] = val;
         }
       }
       __syncthreads();

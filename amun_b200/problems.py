@@ -62,24 +62,30 @@ def blast(mesh, nv: int, gamma: float, dens=1.0, ratio=100.0, radius=0.1, csnd=0
     edge = ~(inside | outside)
     fc[inside] = 1.0
     idx = np.argwhere(edge)
-    for (kk, jj, ii) in idx:
-        a_xl, a_xu, a_yl, a_yu = xl[kk, jj, ii], xu[kk, jj, ii], yl[kk, jj, ii], yu[kk, jj, ii]
-        if mesh.ndims == 3:
-            # sub-cells fully inside count 1, cut ones 1/2 (src/problems.F90:
-            # 620-657); counted at once rather than accumulated one by one
-            a_zl = zl[kk, jj, ii]
-            n = max(1, int(nsubgrid))
-            fm = (np.arange(n) * 1.0) / n
-            fp = (np.arange(1, n + 1) * 1.0) / n
+    if mesh.ndims == 3:
+        # sub-cells fully inside count 1, cut ones 1/2 (src/problems.F90:
+        # 620-657); counted at once rather than accumulated one by one, for
+        # a batch of edge cells at a time
+        n = max(1, int(nsubgrid))
+        fm = (np.arange(n) * 1.0) / n
+        fp = (np.arange(1, n + 1) * 1.0) / n
+        for s0 in range(0, len(idx), 2048):
+            kk, jj, ii = idx[s0:s0 + 2048].T
+            a_xl, a_yl, a_zl = xl[kk, jj, ii][:, None], yl[kk, jj, ii][:, None], zl[kk, jj, ii][:, None]
             xb, xt = (a_xl + fm * dx) ** 2, (a_xl + fp * dx) ** 2
             yb, yt = (a_yl + fm * dy) ** 2, (a_yl + fp * dy) ** 2
             zb, zt = (a_zl + fm * dz) ** 2, (a_zl + fp * dz) ** 2
-            top = zt[:, None, None] + yt[None, :, None] + xt[None, None, :]
-            bot = zb[:, None, None] + yb[None, :, None] + xb[None, None, :]
+            top = zt[:, :, None, None] + yt[:, None, :, None] + xt[:, None, None, :]
+            bot = zb[:, :, None, None] + yb[:, None, :, None] + xb[:, None, None, :]
             full = top <= r2
             half = (~full) & (bot < r2)
-            f = (dvol / n ** 3) * (np.count_nonzero(full) + 0.5 * np.count_nonzero(half))
-        else:
+            nf = full.reshape(len(kk), -1).sum(axis=1)
+            nh = half.reshape(len(kk), -1).sum(axis=1)
+            f = (dvol / n ** 3) * (nf + 0.5 * nh)
+            fc[kk, jj, ii] = f / dvol
+    else:
+        for (kk, jj, ii) in idx:
+            a_xl, a_xu, a_yl, a_yu = xl[kk, jj, ii], xu[kk, jj, ii], yl[kk, jj, ii], yu[kk, jj, ii]
             rlu = a_xl * a_xl + a_yu * a_yu
             rul = a_xu * a_xu + a_yl * a_yl
             if min(rlu, rul) >= r2:
@@ -110,7 +116,7 @@ def blast(mesh, nv: int, gamma: float, dens=1.0, ratio=100.0, radius=0.1, csnd=0
                 ph = 2.0 * math.asin(sn)
                 sn = math.sin(ph)
                 f = dvol - 0.5 * (xt * yt - (ph - sn) * r2)
-        fc[kk, jj, ii] = f / dvol
+            fc[kk, jj, ii] = f / dvol
     q = np.zeros(mesh.shape + (nv,))
     fa = 1.0 - fc
     q[..., DN] = np.where(inside, dn_ovr, np.where(outside, dn_amb, fc * dn_ovr + fa * dn_amb))

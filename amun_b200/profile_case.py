@@ -88,7 +88,8 @@ def regrid_case(a):
                                                    csnd=math.sqrt(gamma * 0.1), buni=1.0, angle=45.0,
                                                    nsubgrid=10), 9)
     sim = Simulation(p, precision=a.precision, mesh=mesh)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # not the legacy default stream (handle 0)
+    torch.cuda.set_stream(stream)
     sim.L.amun_gpu_set_stream(stream.cuda_stream)
     sim.set_primitive_blocks(qb)
     sim.advance(1.0e30)

@@ -97,7 +97,13 @@ class ShardedSimulation:
         N.check(self.L.amun_gpu_stages(C.byref(n)))
         self.nstages = n.value
         self.time, self.dt = 0.0, 0.0
-        N.check(self.L.amun_gpu_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        # the library launches on the caller's current stream, so that the
+        # pack, the transfers and the unpack are ordered on one stream; the
+        # legacy default stream (handle 0) would mean the library's own
+        # stream, unordered with torch's work, so a new stream replaces it
+        cur = torch.cuda.current_stream()
+        self.stream = cur if cur.cuda_stream else torch.cuda.Stream()
+        N.check(self.L.amun_gpu_set_stream(C.c_void_p(self.stream.cuda_stream)))
 
     # ---- state -----------------------------------------------------------------
     def set_primitive(self, q: np.ndarray):
@@ -170,6 +176,7 @@ class ShardedSimulation:
         """Pack, one send and one receive per peer, unpack (NCCL orders the
         transfers after the pack on the current stream and the unpack after
         the transfers)."""
+        import torch
         import torch.distributed as dist
         self.pack()
         ops, so, ro = [], 0, 0
@@ -178,8 +185,9 @@ class ShardedSimulation:
             ops.append(dist.P2POp(dist.irecv, self.recvbuf[ro:ro + nr], peer, group))
             so, ro = so + ns, ro + nr
         if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+            with torch.cuda.stream(self.stream):
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()
         self.unpack()
 
     def allreduce_maxspeed(self, group=None) -> float:

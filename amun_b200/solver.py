@@ -127,6 +127,38 @@ class Simulation:
         self.mesh = mesh
         self._desc = desc
 
+    def generate_mesh(self, initial):
+        """generate_mesh (src/mesh.F90:436-741) from the current mesh (the
+        base level): for level = 1 .. maxlev - 1, the initial state
+        initial(view) (primitives of a block view, ghost cells included, as
+        setup_problem fills them) on every leaf, the refinement criterion on
+        the device, kept for the leaves of that level (clipped at 0; 1 below
+        minlev and for a single base block), and the flagged leaves refined
+        together with their coarser neighbours (2:1, set_neighbors_refine);
+        then the initial state on the final leaves, ghost cells filled by the
+        boundary update.  Returns the new mesh."""
+        mesh = self.mesh
+        if not hasattr(mesh, "update_plan"):
+            raise ValueError("generate_mesh needs a mesh with levels")
+        nbase = mesh.nblocks
+        for level in range(1, mesh.maxlev):
+            # only the leaves of this level are evaluated (the others stay
+            # zero: their criterion is not used)
+            lv = mesh.levels()
+            qb = mesh.blocks_from(initial, self.nv, ghosts=True, only=lv == level)
+            self.upload_blocks(self.prim2cons(qb), qb)
+            crit, _ = self.refinement_criterion()
+            flag = np.where(lv == level, np.maximum(crit, 0), 0).astype(np.int32)
+            if level < mesh.minlev or (nbase == 1 and level == 1):
+                flag[lv == level] = 1
+            if not flag.any():
+                continue
+            new, src = mesh.update_plan(flag)
+            self.regrid(new, src)
+            mesh = new
+        self.set_primitive_blocks(mesh.blocks_from(initial, self.nv))
+        return mesh
+
     def update_mesh(self):
         """One mesh update (src/mesh.F90:756-821 then update_variables): the
         criterion on the device, the new leaves on the host, the data moved

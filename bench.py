@@ -236,30 +236,46 @@ def adjoint_timing(torch, prec, interval=ADJOINT_INTERVAL):
 AMR_WORKLOAD = dict(ndims=3, equation_system="mhd", equation_of_state="adi", reconstruction="tvd", limiter="mc",
                     riemann_solver="hlld", time_advance="rk2", cfl=0.4, gamma=GAMMA, nghosts=4, ncells=16,
                     xblocks=4, yblocks=4, zblocks=4, minlev=1, maxlev=4, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5,
-                    zmin=-0.5, zmax=0.5)
+                    zmin=-0.5, zmax=0.5, refinement_variables="pres")
+
+
+def amr_blast(view):
+    """The AMR blast's initial primitives on a block view (ratio 1000 inside
+    r = 0.1, p_amb 0.1, B = (1,1,0)/sqrt(2), 10 sub-cells per edge cell)."""
+    from amun_b200 import problems
+    return problems.blast(view, NV, GAMMA, dens=1.0, ratio=1000.0, radius=0.1, csnd=math.sqrt(GAMMA * 0.1),
+                          buni=1.0, angle=45.0, nsubgrid=10)
+
+
+_AMR = {}
 
 
 def amr_mesh():
-    """The AMR blast mesh: 4^3 level-1 blocks of 16^3 cells, refined to level
-    4 wherever a block comes within 0.2 of the centre (2:1 balanced): 3424
-    leaves at levels 2-4, 14.0 M cells."""
-    from amun_b200.amr import AMRMesh
-    from amun_b200.params import geometry
-    m = AMRMesh(geometry(AMR_WORKLOAD))
-    m.refine_where(lambda lo, hi, level: float(np.linalg.norm(np.clip(0.0, lo, hi))) < 0.2)
-    return m
+    """The AMR blast mesh as generate_mesh builds it from 4^3 level-1 blocks
+    of 16^3 cells: level by level, the blast's pressure evaluated on the
+    leaves and the refinement criterion (second-derivative indicator of the
+    pressure, the reference's default thresholds) taken on the device, up to
+    level 4, 2:1 balanced.  Returns (mesh, block primitives), built once."""
+    if not _AMR:
+        from amun_b200.amr import AMRMesh
+        from amun_b200.params import geometry
+        from amun_b200.solver import Simulation
+        sim = Simulation(AMR_WORKLOAD, mesh=AMRMesh(geometry(AMR_WORKLOAD)))
+        try:
+            mesh = sim.generate_mesh(amr_blast)
+        finally:
+            sim.close()
+        _AMR["mesh"] = mesh
+        _AMR["q"] = mesh.blocks_from(amr_blast, NV)
+    return _AMR["mesh"], _AMR["q"]
 
 
 def amr_timing(torch, prec, steps=10, warmup=3):
     """3D MHD AMR blast (ratio 1000, p_amb 0.1, B = (1,1,0)/sqrt(2), 10
     sub-cells per edge cell), TVD-MC, HLLD, SSPRK(2,2): zone-updates/s over
     all leaf cells, graph-replayed steps timed with CUDA events."""
-    from amun_b200 import problems
     from amun_b200.solver import Simulation
-    mesh = amr_mesh()
-    qb = mesh.blocks_from(lambda v: problems.blast(v, NV, GAMMA, dens=1.0, ratio=1000.0, radius=0.1,
-                                                   csnd=math.sqrt(GAMMA * 0.1), buni=1.0, angle=45.0,
-                                                   nsubgrid=10), NV)
+    mesh, qb = amr_mesh()
     sim = Simulation(AMR_WORKLOAD, precision=prec, mesh=mesh)
     sim.L.amun_gpu_set_stream(torch.cuda.current_stream().cuda_stream)
     sim.set_primitive_blocks(qb)
@@ -271,7 +287,7 @@ def amr_timing(torch, prec, steps=10, warmup=3):
            "device_bytes": sim.status()["device_bytes"]}
     # one mesh update after the timed steps (not part of the step time): the
     # refinement indicators on the device, the new leaves on the host, the
-    # block data moved on the device (refinement_variables "dens pres")
+    # block data moved on the device (refinement_variables "pres")
     stream = torch.cuda.current_stream()
     sim.refinement_criterion()
     torch.cuda.synchronize()
@@ -553,6 +569,10 @@ def main():
     import torch
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    # a stream of our own: torch's legacy default stream has the handle 0,
+    # which the library reads as "launch on your own stream", and events or
+    # NCCL calls on it would not be ordered with the library's launches
+    torch.cuda.set_stream(torch.cuda.Stream())
     pg = None
     if ws > 1:
         import torch.distributed as dist
@@ -748,8 +768,10 @@ def main():
             "accuracy_vs_fp64": accuracy,
             "kernel_profile_fp32": r32["profile"], "kernel_profile_fp64": r64["profile"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "amr_blast3d": {"workload": "mhd3d AMR blast, 4^3 level-1 blocks of 16^3 cells, levels 1-4, "
-                                        "tvd-mc hlld ssprk(2,2) cfl0.4, ratio 1000",
+            "amr_blast3d": {"workload": "mhd3d AMR blast, 4^3 level-1 blocks of 16^3 cells, levels 1-4 refined "
+                                        "on the pressure's second-derivative indicator by generate_mesh on the "
+                                        "device, tvd-mc hlld ssprk(2,2) cfl0.4, ratio 1000, one sweep launch per "
+                                        "direction over all levels",
                             "fp64": amr["fp64"], "fp32": amr["fp32"]},
             "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
                                     "J = kinetic energy in [0,0.25]^2, dJ/drho0; every stage input kept "

@@ -145,9 +145,9 @@ typedef struct amun_status {
                              p <= 0 (src/equations.F90:4745-4777)           */
   long long device_bytes; /* bytes of device memory held by the block pool    */
   long long unphysical_cells; /* cells replaced by correct_unphysical_states  */
-  long long stalls;       /* fused stage kernel: tiles that gave up waiting for
-                             a tile copy (bounded wait; their cells are not
-                             updated, so a nonzero count is an error)       */
+  long long stalls;       /* device waits that gave up (fused stage kernel:
+                             a tile copy; one launch over all levels: finer
+                             face fluxes); a nonzero count is an error       */
 } amun_status;
 
 /* Fill *p with the reference defaults (hd/adi, tvd/mm, hll, rk2, cfl 0.5 ...). */
@@ -373,6 +373,23 @@ int amun_gpu_set_stream(void* stream);
  * recording; reset != 0 clears the accumulated times. */
 int amun_gpu_profile(int enable, int reset);
 int amun_gpu_profile_read(int kind, double* total_ms, long long* launches);
+
+/* Meshes with level jumps: by default each sweep direction is one launch
+ * over every block of every level (blocks finest first); a block face whose
+ * neighbours are finer takes their stored face fluxes (boundary_fluxes,
+ * src/boundaries.F90:494-1087) after waiting in the kernel, bounded, until
+ * every tile of those finer faces has stored them.  per_level != 0 launches
+ * each level separately instead, finest first (no waits).  Both give the
+ * same results.  A wait that gives up is counted in amun_status.stalls and
+ * amun_gpu_advance then fails; it does not happen when the tiles of a launch
+ * start in index order.  Invalidates captured graphs. */
+int amun_gpu_set_level_launches(int per_level);
+/* Runs one bounded device wait on a count that nothing raises (the wait of
+ * the flux correction above, given `cycles` clock cycles) and reports in
+ * *gave_up whether it gave up and recorded a stall, as it must; the stall
+ * count of the state is left unchanged.  A check that device waits end
+ * with an error status instead of hanging. */
+int amun_gpu_wait_selftest(long long cycles, int* gave_up);
 
 /* How each SSPRK stage's fluxes are computed (no counterpart in the
  * reference, whose update_fluxes loops over blocks and directions,

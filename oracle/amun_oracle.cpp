@@ -610,8 +610,12 @@ struct Oracle {
     dy = (p.ymax - p.ymin) / (p.yblocks * (jn * ff));
     dz = (p.ndims == 3) ? (p.zmax - p.zmin) / (p.zblocks * (kn * ff)) : 1.0;
     nbx = p.xblocks * ff; nby = p.yblocks * ff; nbz = (p.ndims == 3) ? p.zblocks * ff : 1;
-    blocks.assign((size_t)nbx * nby * nbz, Block());
     mlev = lev;
+    // the uniform mesh of the finest level; a mesh too large to hold here is
+    // left out (set_mesh then provides the leaves)
+    const double bytes = (double)nbx * nby * nbz * nv * cells() * (3 + p.ndims) * sizeof(double);
+    if (bytes > 4.0e9) { blocks.clear(); return 0; }
+    blocks.assign((size_t)nbx * nby * nbz, Block());
     for (size_t bi = 0; bi < blocks.size(); ++bi) {
       Block& b = blocks[bi];
       b.u0.assign(nv * cells(), 0.0); b.u1.assign(nv * cells(), 0.0);
@@ -4642,6 +4646,21 @@ void or_set_blocks_prim(void* h, const double* qb) {
     B.u = B.u0.data();
   }
   o->boundary_variables();
+  o->time = 0.0; o->step = 0;
+}
+
+// The state of every block as setup_problem leaves it inside generate_mesh
+// (src/mesh.F90:535, src/problems.F90): q over the whole block, ghost cells
+// included, u0 = prim2cons(q) there, no boundary update.
+void or_set_blocks_raw(void* h, const double* qb) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t per = (size_t)o->nv * o->cells();
+  for (size_t b = 0; b < o->blocks.size(); ++b) {
+    auto& B = o->blocks[b];
+    std::memcpy(B.q.data(), qb + b * per, per * sizeof(double));
+    o->prim2cons((int)o->cells(), B.q.data(), B.u0.data());
+    B.u = B.u0.data();
+  }
   o->time = 0.0; o->step = 0;
 }
 

@@ -54,6 +54,7 @@ def lib():
         L.or_set_mesh.argtypes = [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.or_set_mesh.restype = i
         L.or_set_blocks_prim.argtypes = [vp, d]
+        L.or_set_blocks_raw.argtypes = [vp, d]
         L.or_gp_weights.argtypes = [vp, d]
         L.or_gp_weights.restype = i
         L.or_mgp_weights.argtypes = [vp, d]
@@ -265,6 +266,12 @@ class Oracle:
         """Primitive state of every block, (nblocks, km, jm, im, nv) with
         ghosts (ignored); u0 = prim2cons(q) and the ghost cells are filled."""
         self.L.or_set_blocks_prim(self.h, _p(qb))
+
+    def set_blocks_raw(self, qb: np.ndarray):
+        """Primitive state of every block, ghost cells included, as
+        setup_problem sets it: u0 = prim2cons(q) everywhere, no ghost fill."""
+        qb = np.ascontiguousarray(qb, dtype=np.float64)
+        self.L.or_set_blocks_raw(self.h, _p(qb))
 
     def block(self, b: int, which: str = "q"):
         out = np.empty((self.km, self.jm, self.im, self.nv))

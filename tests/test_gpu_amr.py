@@ -96,3 +96,74 @@ def test_amr_graph_run_and_fp32_bulk():
         assert np.sum(np.abs(d - r)) / np.sum(np.abs(r)) <= 1e-5
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("prec,graph", [("fp64", False), ("fp32", True)])
+def test_one_launch_over_levels_equals_level_launches(prec, graph):
+    """One sweep launch per direction over every level (coarse faces wait in
+    the kernel for the finer face fluxes) gives the state of one launch per
+    level bit for bit, eager and from graphs, with no wait giving up."""
+    from amun_b200.solver import Simulation
+    p, mesh = amr_case(eq="mhd", rec="tvd", rs="hlld", ndims=3, ta="rk2", ncells=8, prolongation_limiter="mc")
+    qb = smooth_blocks(mesh, 9, seed=7)
+    out = []
+    for per_level in (1, 0):
+        s = Simulation(p, precision=prec, mesh=mesh)
+        try:
+            N = s.L
+            assert N.amun_gpu_set_level_launches(per_level) == 0
+            s.set_primitive_blocks(qb)
+            if graph:
+                s.run(4, 1.0e30, graph=True)
+            else:
+                for _ in range(4):
+                    s.advance(1.0e30)
+            out.append(s.download_blocks())
+            assert s.status()["stalls"] == 0
+        finally:
+            s.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_device_wait_gives_up_with_a_status():
+    """A bounded device wait on a count that nothing raises ends, records
+    the failure and leaves the context usable."""
+    import ctypes as C
+    from amun_b200.solver import Simulation
+    p, mesh = amr_case(eq="hd", rec="tvd", rs="hllc", ndims=2, ta="rk2", ncells=8, prolongation_limiter="mm")
+    s = Simulation(p, mesh=mesh)
+    try:
+        s.set_primitive_blocks(smooth_blocks(mesh, 5, seed=1))
+        gave_up = C.c_int(-1)
+        assert s.L.amun_gpu_wait_selftest(20_000_000, C.byref(gave_up)) == 0   # ~10 ms
+        assert gave_up.value == 1
+        assert s.status()["stalls"] == 0
+        s.advance(1.0e30)  # the context still steps
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("eq,nd,nc,nb,maxlev,refvars", [("hd", 2, 8, 4, 4, "pres"), ("mhd", 3, 8, 2, 3, "dens pres")])
+def test_generate_mesh_matches_oracle(oracle_mod, eq, nd, nc, nb, maxlev, refvars):
+    """generate_mesh driven by the device refinement criterion builds the
+    same leaves as the oracle's restatement, and leaves the initial state on
+    them with the ghost cells of the boundary update."""
+    from amun_b200.amr import AMRMesh
+    from amun_b200.params import geometry
+    from amun_b200.solver import Simulation
+    from test_oracle_amr import blast_case, oracle_generate_mesh, oracle_on
+    p, nv, initial = blast_case(eq, nd, nc, nb, maxlev, refvars)
+    ref = oracle_generate_mesh(oracle_mod, p, AMRMesh(geometry(p)), initial, nv)
+    s = Simulation(p, mesh=AMRMesh(geometry(p)))
+    try:
+        mesh = s.generate_mesh(initial)
+        assert mesh.leaves == ref.leaves
+        assert len(set(mesh.levels().tolist())) >= 2
+        o = oracle_on(oracle_mod, p, ref)
+        o.set_blocks_prim(ref.blocks_from(initial, nv))
+        u, q = s.download_blocks()
+        qo = np.stack([o.block(b, "q") for b in range(ref.nblocks)])
+        assert np.array_equal(q, qo)
+    finally:
+        s.close()

@@ -36,6 +36,73 @@ def oracle_on(oracle_mod, p, mesh):
     return o
 
 
+def oracle_generate_mesh(oracle_mod, p, mesh, initial, nv):
+    """generate_mesh (src/mesh.F90:436-741) with the oracle's refinement
+    criterion: for level = 1 .. maxlev - 1 the leaves of that level get the
+    initial state over the whole block (setup_problem, ghost cells
+    included), refine = max(0, check_refinement_criterion) (1 below minlev,
+    1 for a single base block, 540-549); then from that level down to 2 every
+    leaf flagged 1 flags its coarser neighbours across faces, edges and
+    corners (set_neighbors_refine, src/blocks.F90:3825-3851, 4297-4352), and
+    every flagged leaf is refined (587-603)."""
+    nbase = mesh.nblocks
+    for level in range(1, mesh.maxlev):
+        o = oracle_on(oracle_mod, p, mesh)
+        o.set_blocks_raw(mesh.blocks_from(initial, nv, ghosts=True, only=mesh.levels() == level))
+        crit, _ = o.refinement_criterion()
+        refine = {}
+        for t, c in zip(mesh.order, crit):
+            if t[0] == level:
+                refine[t] = 1 if (level < mesh.minlev or (nbase == 1 and level == 1)) else max(0, int(c))
+        for lev in range(level, 1, -1):
+            for t in mesh.order:
+                if t[0] == lev and refine.get(t) == 1:
+                    for n in mesh.neighbours(t):
+                        if n[0] < lev:
+                            refine[n] = 1
+        for t, r in refine.items():
+            if r == 1:
+                mesh.refine(t)
+    return mesh
+
+
+def blast_case(eq, ndims, ncells, nb, maxlev, refvars):
+    """A blast at the centre of [-0.5, 0.5]^d on a base of nb^d blocks."""
+    kw = dict(ndims=ndims, ncells=ncells, nghosts=2, xblocks=nb, yblocks=nb, maxlev=maxlev, xmin=-0.5, xmax=0.5,
+              ymin=-0.5, ymax=0.5, refinement_variables=refvars)
+    if ndims == 3:
+        kw.update(zblocks=nb, zmin=-0.5, zmax=0.5)
+    p = params(eq, "tvd", "hll", "rk2", **kw)
+    from amun_b200 import problems
+    nv = 9 if eq == "mhd" else 5
+    gamma = 5.0 / 3.0
+
+    def initial(view):
+        return problems.blast(view, nv, gamma, ratio=10.0, radius=0.15, csnd=np.sqrt(gamma), buni=1.0,
+                              angle=45.0, nsubgrid=4)
+
+    return p, nv, initial
+
+
+def test_generated_mesh_follows_the_blast(oracle_mod):
+    """The mesh the criterion builds is balanced, reaches maxlev only where
+    the blast's edge is, and is the same whether the leaves are visited in
+    one order or another (the flags depend on the state alone)."""
+    p, nv, initial = blast_case("hd", 2, 8, 4, 4, "pres")
+    mesh = oracle_generate_mesh(oracle_mod, p, AMRMesh(geometry(p)), initial, nv)
+    assert mesh.is_balanced()
+    lv = mesh.levels()
+    assert lv.max() == 4 and lv.min() <= 2
+    for t in mesh.leaves:
+        if t[0] == 4:
+            lo, hi = mesh.box(t)
+            # the nearest and farthest points of the block from the centre
+            # bracket the blast radius within a block of the level below
+            near = np.linalg.norm(np.clip(0.0, lo[:2], hi[:2]))
+            far = np.linalg.norm(np.maximum(np.abs(lo[:2]), np.abs(hi[:2])))
+            assert near - 0.07 <= 0.15 <= far + 0.07
+
+
 def test_mesh_is_balanced_and_covers_the_domain():
     for nd in (2, 3):
         p, mesh = amr_case(ndims=nd, ncells=4 if nd == 3 else 8, maxlev=3)
