@@ -280,11 +280,18 @@ def amr_timing(torch, prec, steps=10, warmup=3):
     sim.L.amun_gpu_set_stream(torch.cuda.current_stream().cuda_stream)
     sim.set_primitive_blocks(qb)
     ms = timed_run(sim, torch, steps, warmup, 1.0e30)
+    # the same steps with one sweep launch per level (finest first) instead
+    # of one launch over all levels
+    sim.L.amun_gpu_set_level_launches(1)
+    ms_lv = timed_run(sim, torch, steps, warmup, 1.0e30)
+    sim.L.amun_gpu_set_level_launches(0)
     lv = mesh.levels()
     out = {"value": mesh.ncells_total * steps / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms / steps,
            "steps": steps, "leaves": int(mesh.nblocks), "cells": int(mesh.ncells_total),
            "leaves_per_level": {int(l): int((lv == l).sum()) for l in np.unique(lv)},
-           "device_bytes": sim.status()["device_bytes"]}
+           "device_bytes": sim.status()["device_bytes"],
+           "launch_per_level": {"value": mesh.ncells_total * steps / (ms_lv * 1e-3), "ms_per_step": ms_lv / steps},
+           "stalls": sim.status()["stalls"]}
     # one mesh update after the timed steps (not part of the step time): the
     # refinement indicators on the device, the new leaves on the host, the
     # block data moved on the device (refinement_variables "pres")
@@ -744,6 +751,17 @@ def main():
                     "traffic_per_zone_update": traffic / NCELL if traffic else None,
                     "fp64": {"achieved": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9,
                              "frac": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9 / peak}}
+        # the sweeps are bound by instruction issue: warp instructions per
+        # zone-update (ncu, profiles/sweep_mhd3d_128_full.md: 1440 + 1382 +
+        # 1834 thread-instruction slots per cell and stage, three stages)
+        # against 4 issues per SM and cycle at the sampled SM clock
+        wi = 3 * (1440 + 1382 + 1834) / 32
+        mhz = (r32["clocks"] or {}).get("sm_mhz") or 1965.0
+        issue_peak = 148 * 4 * mhz * 1e6
+        roofline["issue"] = {"warp_instructions_per_zone_update": wi, "peak_warp_instructions_per_s": issue_peak,
+                             "achieved_warp_instructions_per_s": (zu / ws) * wi,
+                             "frac": (zu / ws) * wi / issue_peak,
+                             "source": "profiles/sweep_mhd3d_128_full.md, profiles/sweep_x_variants_mhd3d_128.md"}
         cpu = None
         if not args.no_cpu:
             try:
