@@ -175,6 +175,68 @@ class AMRMesh:
         out.discard(leaf)
         return out
 
+    def neighbour_lists(self):
+        """For every leaf in block-index order, the block indices of the
+        leaves touching it across faces, edges and corners, ascending (the
+        same sets as neighbours(), looked up for all leaves at once: the
+        same level, the coarser level, or the finer leaves next to it, as a
+        2:1 balanced mesh has them)."""
+        order = self.order
+        nb = len(order)
+        t = np.array(order, dtype=np.int64).reshape(nb, 4)
+        lev = t[:, 0]
+        maxl = int(lev.max())
+        ext = np.stack([np.array(self.extent(l)) for l in range(1, maxl + 2)])
+
+        def enc(l, x, y, z):
+            return ((l * 65536 + x) * 65536 + y) * 65536 + z
+
+        keys = enc(lev, t[:, 1], t[:, 2], t[:, 3])
+        srt = np.argsort(keys)
+        skeys = keys[srt]
+
+        def look(k):
+            pos = np.minimum(np.searchsorted(skeys, k), nb - 1)
+            return np.where(skeys[pos] == k, srt[pos], -1)
+
+        found = [[] for _ in range(nb)]
+        rows, cols = [], []
+        for o in self._offsets():
+            e = ext[lev - 1]
+            p = [(t[:, 1 + a] + o[a]) % e[:, a] for a in range(3)]
+            hit = look(enc(lev, p[0], p[1], p[2]))
+            miss = hit < 0
+            coarse = np.where(miss & (lev > 1), look(enc(lev - 1, p[0] // 2, p[1] // 2, p[2] // 2)), -1)
+            rows.append(np.nonzero(hit >= 0)[0]); cols.append(hit[hit >= 0])
+            rows.append(np.nonzero(coarse >= 0)[0]); cols.append(coarse[coarse >= 0])
+            fine = miss & (coarse < 0)
+            if fine.any():
+                subs = [(0,) if d == 1 else ((1,) if d == -1 else (0, 1)) for d in o]
+                if self.ndims == 2:
+                    subs[2] = (0,)
+                idx = np.nonzero(fine)[0]
+                for c in subs[2]:
+                    for b in subs[1]:
+                        for a in subs[0]:
+                            f = look(enc(lev[idx] + 1, 2 * p[0][idx] + a, 2 * p[1][idx] + b, 2 * p[2][idx] + c))
+                            for r in idx[f < 0]:  # deeper than one level: the general search
+                                found[r].extend(self.neighbours(order[r]))
+                            rows.append(idx[f >= 0]); cols.append(f[f >= 0])
+        index = {tt: b for b, tt in enumerate(order)}
+        for r in range(nb):
+            for x in found[r]:
+                rows.append(np.array([r]))
+                cols.append(np.array([index[x]]))
+        rows = np.concatenate(rows).astype(np.int64)
+        cols = np.concatenate(cols).astype(np.int64)
+        pair = np.unique(rows * nb + cols)  # sorted by leaf, then neighbour
+        r, c = pair // nb, pair % nb
+        keep = r != c
+        r, c = r[keep], c[keep]
+        cut = np.searchsorted(r, np.arange(nb + 1))
+        cl = c.tolist()
+        return [cl[cut[b]:cut[b + 1]] for b in range(nb)]
+
     def is_balanced(self) -> bool:
         """Neighbours across faces, edges and corners differ by at most one level."""
         return all(abs(n[0] - t[0]) <= 1 for t in self.leaves for n in self.neighbours(t))
@@ -209,11 +271,13 @@ class AMRMesh:
             if l > self.maxlev:
                 r = -1
             ref[t] = r
+        nbrs = self.neighbour_lists()
+        by_level = {}
+        for t in order:
+            by_level.setdefault(t[0], []).append(t)
         for l in range(self.maxlev, 0, -1):
-            for t in order:
-                if t[0] != l:
-                    continue
-                for n in sorted(self.neighbours(t), key=lambda x: index[x]):
+            for t in by_level.get(l, []):
+                for n in (order[k] for k in nbrs[index[t]]):
                     if ref[t] == 1:
                         ref[n] = max(0, ref[n])
                         if n[0] < l:

@@ -98,8 +98,10 @@ struct Ctx {
   std::string err;
   // meshes with level jumps (set_blocks with blocks at several levels)
   bool amr = false;
-  GhostOp* gop = nullptr;    // copies + restrictions, then prolongations
-  long long nop1 = 0, nop2 = 0;
+  GhostRegion* greg = nullptr;  // [b][27]: how each ghost region is filled
+  BlockPos* gpos = nullptr;      // level and position of every block
+  int* glist = nullptr;          // b * 27 + region: copies and restrictions, then prolongations
+  int gn0 = 0, gn1 = 0;
   int* frole = nullptr;      // [b][dir][side]
   int* fquad = nullptr;      // [b][dir][side][4]
   int* blist = nullptr;      // blocks ordered finest level first
@@ -275,10 +277,10 @@ void free_pool() {
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   for (auto& x : C.q)
     if (x) { cudaFree(x); x = nullptr; }
-  void* amrp[] = {C.gop, C.frole, C.fquad, C.blist, C.ff, C.fcount};
+  void* amrp[] = {C.greg, C.gpos, C.glist, C.frole, C.fquad, C.blist, C.ff, C.fcount};
   for (void* x : amrp)
     if (x) cudaFree(x);
-  C.gop = nullptr; C.frole = C.fquad = C.blist = C.fcount = nullptr; C.ff = nullptr;
+  C.greg = nullptr; C.gpos = nullptr; C.glist = nullptr; C.gn0 = C.gn1 = 0; C.frole = C.fquad = C.blist = C.fcount = nullptr; C.ff = nullptr;
   if (C.fix_idx) cudaFree(C.fix_idx);
   if (C.fix_val) cudaFree(C.fix_val);
   C.fix_idx = nullptr; C.fix_val = nullptr; C.fix_cap = 0;
@@ -293,7 +295,7 @@ void free_pool() {
   C.stg_bytes = 0;
   C.prefetched = C.posted = false;
   C.tile_LP = C.tile_LW = 0;
-  C.nop1 = C.nop2 = 0; C.lgroups.clear(); C.amr = false;
+  C.lgroups.clear(); C.amr = false;
   C.stage_maps = false;
   if (C.halo_send) cudaFree(C.halo_send);
   if (C.halo_recv) cudaFree(C.halo_recv);
@@ -1062,107 +1064,90 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
     return it == where.end() ? -1 : it->second;
   };
   auto wrap = [&](int v, int l, int a) { const int n = (base[a] << (l - 1)) * nc; v %= n; return v < 0 ? v + n : v; };
-  const Geo& g = C.g;
-  auto cell = [&](const int* c) {  // padded linear index of global cell c inside its block
-    const int i = c[0] % nc + ng, j = c[1] % nc + ng, k = nd == 3 ? c[2] % nc + ng : 0;
-    return ((long long)k * g.JM + j) * g.IM + i;
+  auto wrapb = [&](int v, int l, int a) { const int n = base[a] << (l - 1); v %= n; return v < 0 ? v + n : v; };
+  auto at = [&](int l, const int* s) -> int {  // the leaf at level l, position s (in blocks)
+    if (l < 1) return -1;
+    auto it = where.find(key(l, s[0], s[1], nd == 3 ? s[2] : 0));
+    return it == where.end() ? -1 : it->second;
   };
-  std::vector<signed char> kind((size_t)nblocks * g.qvs, -1);  // op kind of every ghost cell
-  // the ghost cells of each block are independent: blocks are split into
-  // contiguous ranges over host threads, each building its own op lists,
-  // which are joined in block order (the same lists as one thread builds)
-  const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  const int per = (nblocks + nth - 1) / nth;
-  std::vector<std::vector<GhostOp>> t1(nth), t2(nth);
-  std::vector<std::string> terr(nth);
-  auto work = [&](int t) {
-    // one remembered lookup per level offset: neighbouring ghost cells of a
-    // row mostly fall in the same block
-    long long mk[3] = {-1, -1, -1};
-    int mv[3] = {-1, -1, -1};
-    auto findm = [&](int slot, int l, const int* c) -> int {
-      if (l < 1) return -1;
-      const long long k = key(l, c[0] / nc, c[1] / nc, nd == 3 ? c[2] / nc : 0);
-      if (k != mk[slot]) {
-        auto it = where.find(k);
-        mk[slot] = k;
-        mv[slot] = it == where.end() ? -1 : it->second;
+  // how the block-sized slot of each block's level next to each of its
+  // faces, edges and corners is covered: a block of the same level, a
+  // coarser block, or 2^d finer ones
+  std::vector<GhostRegion> reg((size_t)nblocks * 27);
+  std::vector<BlockPos> bpos(nblocks);
+  std::string err;
+  for (int b = 0; b < nblocks && err.empty(); ++b) {
+    const int L = d[b].level;
+    bpos[b].level = L;
+    for (int a = 0; a < 3; ++a) bpos[b].c[a] = a < nd ? d[b].coord[a] : 0;
+    for (int dd = 0; dd < 27; ++dd) {
+      GhostRegion& R = reg[(size_t)b * 27 + dd];
+      R.kind = -1;
+      for (int m = 0; m < 8; ++m) R.src[m] = -1;
+      const int o[3] = {dd % 3 - 1, (dd / 3) % 3 - 1, dd / 9 - 1};
+      if (dd == 13 || (nd == 2 && o[2] != 0)) continue;
+      int sl[3] = {0, 0, 0};
+      for (int a = 0; a < nd; ++a) sl[a] = wrapb(d[b].coord[a] + o[a], L, a);
+      int S = at(L, sl);
+      if (S >= 0) { R.kind = 0; R.src[0] = S; continue; }
+      const int cs[3] = {sl[0] / 2, sl[1] / 2, sl[2] / 2};
+      S = at(L - 1, cs);
+      if (S >= 0) { R.kind = 2; R.src[0] = S; continue; }
+      // the finer blocks of the slot's half next to the block (the ghost
+      // cells reach ng <= nc / 2 cells into the slot); the far half may be
+      // refined further
+      R.kind = 1;
+      for (int sub = 0; sub < (1 << nd); ++sub) {
+        int fs[3] = {0, 0, 0};
+        bool near = true;
+        for (int a = 0; a < nd; ++a) {
+          const int h = (sub >> a) & 1;
+          if ((o[a] > 0 && h == 1) || (o[a] < 0 && h == 0)) near = false;
+          fs[a] = 2 * sl[a] + h;
+        }
+        if (!near) continue;
+        R.src[sub] = at(L + 1, fs);
+        if (R.src[sub] < 0) {
+          err = "a ghost region is covered by no block at its level or the next ones (mesh not 2:1 balanced, "
+                "or a gap)";
+          break;
+        }
       }
-      return mv[slot];
-    };
-    const int b0 = t * per, b1 = std::min(nblocks, b0 + per);
-    for (int b = b0; b < b1; ++b) {
-      const int L = d[b].level;
-      for (int k = 0; k < g.KM; ++k)
-        for (int j = 0; j < g.JM; ++j)
-          for (int i = 0; i < g.IM; ++i) {
-            const bool inside =
-                i >= ng && i < ng + nc && j >= ng && j < ng + nc && (nd == 2 || (k >= ng && k < ng + nc));
-            if (inside) continue;
-            int c[3] = {wrap(d[b].coord[0] * nc + i - ng, L, 0), wrap(d[b].coord[1] * nc + j - ng, L, 1),
-                        nd == 3 ? wrap(d[b].coord[2] * nc + k - ng, L, 2) : 0};
-            GhostOp op;
-            op.dst = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
-            int S = findm(0, L, c);
-            if (S >= 0) {
-              op.sk = op_pack((long long)S * g.qbs + cell(c), 0);
-              t1[t].push_back(op);
-            } else {
-              int cc[3] = {c[0] / 2, c[1] / 2, c[2] / 2};
-              int Cb = findm(1, L - 1, cc);
-              if (Cb >= 0) {
-                op.sk = op_pack((long long)Cb * g.qbs + cell(cc),
-                                2 | (((c[0] & 1) | ((c[1] & 1) << 1) | ((nd == 3 ? c[2] & 1 : 0) << 2)) << 2));
-                t2[t].push_back(op);
-              } else {
-                int fc[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
-                int F = findm(2, L + 1, fc);
-                if (F < 0) {
-                  terr[t] = "a ghost cell is covered by no block at its level or the next ones (mesh not 2:1 "
-                            "balanced, or a gap)";
-                  return;
-                }
-                op.sk = op_pack((long long)F * g.qbs + cell(fc), 1);
-                t1[t].push_back(op);
-              }
-            }
-            kind[(size_t)b * g.qvs + (size_t)(op.dst - (long long)b * g.qbs)] = (signed char)(op_kind(op) & 3);
-          }
     }
-  };
-  {
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nth; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
   }
-  // one list: the copies and restrictions, then the prolongations
-  size_t n1 = 0, n2 = 0;
-  for (int t = 0; t < nth; ++t) {
-    if (!terr[t].empty()) return fail(AMUN_E_UNSUPPORTED, terr[t]);
-    n1 += t1[t].size();
-    n2 += t2[t].size();
-  }
-  std::vector<GhostOp> all;
-  all.reserve(n1 + n2);
-  for (int t = 0; t < nth; ++t) {
-    all.insert(all.end(), t1[t].begin(), t1[t].end());
-    std::vector<GhostOp>().swap(t1[t]);
-  }
-  for (int t = 0; t < nth; ++t) {
-    all.insert(all.end(), t2[t].begin(), t2[t].end());
-    std::vector<GhostOp>().swap(t2[t]);
-  }
+  if (!err.empty()) return fail(AMUN_E_UNSUPPORTED, err);
   // a prolongation reads its coarse cell and the neighbours along each
-  // direction: none of them may be a prolonged ghost itself
-  const long long st[3] = {1, g.IM, (long long)g.IM * g.JM};
-  for (size_t o = n1; o < all.size(); ++o) {
-    const long long src = op_src(all[o]);
-    const long long sb = src / g.qbs, sc = src - sb * g.qbs;  // block, padded cell
-    for (int a = 0; a < nd; ++a)
-      for (int sgn = -1; sgn <= 1; sgn += 2)
-        if (kind[(size_t)sb * g.qvs + (size_t)(sc + sgn * st[a])] == 2)
-          return fail(AMUN_E_UNSUPPORTED, "a prolongation would read a prolonged ghost (mesh not 2:1 balanced)");
+  // direction: none of them may be a prolonged ghost of the coarser block
+  for (int b = 0; b < nblocks; ++b) {
+    const int L = d[b].level;
+    for (int dd = 0; dd < 27; ++dd) {
+      const GhostRegion& R = reg[(size_t)b * 27 + dd];
+      if (R.kind != 2) continue;
+      const int Cb = R.src[0];
+      const int o[3] = {dd % 3 - 1, (dd / 3) % 3 - 1, dd / 9 - 1};
+      int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // coarse cells read, padded, in Cb
+      for (int a = 0; a < nd; ++a) {
+        const int i0 = o[a] < 0 ? 0 : (o[a] == 0 ? ng : ng + nc), i1 = i0 + (o[a] == 0 ? nc : ng) - 1;
+        const int c0 = wrap(d[b].coord[a] * nc + i0 - ng, L, a) / 2, c1 = wrap(d[b].coord[a] * nc + i1 - ng, L, a) / 2;
+        lo[a] = c0 - d[Cb].coord[a] * nc + ng;
+        hi[a] = c1 - d[Cb].coord[a] * nc + ng;
+      }
+      for (int ax = 0; ax < nd; ++ax) {
+        int rl[3] = {1, 1, 1}, rh[3] = {1, 1, 1};
+        for (int a = 0; a < nd; ++a) {
+          const int x0 = lo[a] - (a == ax), x1 = hi[a] + (a == ax);
+          rl[a] = x0 < ng ? 0 : (x0 < ng + nc ? 1 : 2);
+          rh[a] = x1 < ng ? 0 : (x1 < ng + nc ? 1 : 2);
+        }
+        for (int rz = rl[2]; rz <= rh[2]; ++rz)
+          for (int ry = rl[1]; ry <= rh[1]; ++ry)
+            for (int rx = rl[0]; rx <= rh[0]; ++rx) {
+              const int dc = rx + 3 * ry + 9 * rz;
+              if (dc != 13 && reg[(size_t)Cb * 27 + dc].kind == 2)
+                return fail(AMUN_E_UNSUPPORTED, "a prolongation would read a prolonged ghost (mesh not 2:1 balanced)");
+            }
+      }
+    }
   }
   // face roles and the finer blocks of coarse faces
   std::vector<int> role((size_t)nblocks * 6, 0), quad((size_t)nblocks * 24, -1);
@@ -1211,20 +1196,29 @@ int build_level_tables(int nblocks, const amun_block_desc* d) {
     C.lgroups.push_back({s0, e - s0});
     s0 = e;
   }
-  C.nop1 = (long long)n1;
-  C.nop2 = (long long)n2;
   const size_t NT = (size_t)nc * (nd == 3 ? nc : 1);
-  CK(cudaMalloc(&C.gop, std::max<size_t>(all.size(), 1) * sizeof(GhostOp)));
+  std::vector<int> glist;
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t e = 0; e < reg.size(); ++e)
+      if (reg[e].kind >= 0 && (reg[e].kind == 2) == (pass == 1)) glist.push_back((int)e);
+  C.gn1 = (int)std::count_if(reg.begin(), reg.end(), [](const GhostRegion& r) { return r.kind == 2; });
+  C.gn0 = (int)glist.size() - C.gn1;
+  CK(cudaMalloc(&C.greg, reg.size() * sizeof(GhostRegion)));
+  CK(cudaMalloc(&C.gpos, bpos.size() * sizeof(BlockPos)));
+  CK(cudaMalloc(&C.glist, std::max<size_t>(glist.size(), 1) * sizeof(int)));
+  if (!glist.empty()) CK(h2d(C.glist, glist.data(), glist.size() * sizeof(int)));
   CK(cudaMalloc(&C.frole, role.size() * sizeof(int)));
   CK(cudaMalloc(&C.fquad, quad.size() * sizeof(int)));
   CK(cudaMalloc(&C.blist, order.size() * sizeof(int)));
   CK(cudaMalloc(&C.ff, (size_t)nblocks * 6 * C.nv * NT * rsize()));
   CK(cudaMalloc(&C.fcount, ((size_t)nblocks * 6 + 1) * sizeof(int)));
-  if (!all.empty()) CK(h2d(C.gop, all.data(), all.size() * sizeof(GhostOp)));
+  CK(h2d(C.greg, reg.data(), reg.size() * sizeof(GhostRegion)));
+  CK(h2d(C.gpos, bpos.data(), bpos.size() * sizeof(BlockPos)));
   CK(h2d(C.frole, role.data(), role.size() * sizeof(int)));
   CK(h2d(C.fquad, quad.data(), quad.size() * sizeof(int)));
   CK(h2d(C.blist, order.data(), order.size() * sizeof(int)));
-  C.pool_bytes += (long long)(all.size() * sizeof(GhostOp) + (role.size() + quad.size() + order.size()) * sizeof(int) +
+  C.pool_bytes += (long long)(reg.size() * sizeof(GhostRegion) + bpos.size() * sizeof(BlockPos) +
+                              (role.size() + quad.size() + order.size()) * sizeof(int) +
                               (size_t)nblocks * 6 * C.nv * NT * rsize());
   C.amr = true;
   return 0;
@@ -1285,8 +1279,9 @@ int build_halo_plan(int nblocks, const amun_block_desc* d, const int* owner, int
 template <typename R>
 cudaError_t ghost_fill(R* q) {
   if (C.amr)
-    return Launch<R, R>::amr_ghost(q, C.gop, C.nop1, C.gop + C.nop1, C.nop2, C.g, C.nv, pressure_index(),
-                                   C.p.prolongation_limiter, C.p.eps, C.stream);
+    return Launch<R, R>::amr_ghost(q, C.greg, C.gpos, C.glist, C.gn0, C.gn1, C.g,
+                                   BaseGrid{{C.p.xblocks, C.p.yblocks, C.g.ndims == 3 ? C.p.zblocks : 1}}, C.nv,
+                                   pressure_index(), C.p.prolongation_limiter, C.p.eps, C.stream);
   return Launch<R, R>::ghost(q, C.nbr, C.g, C.nv, C.nblocks, C.stream);
 }
 

@@ -14,8 +14,8 @@ template <typename R, typename U1T> struct Launch {
   static cudaError_t halo(bool pack, R* q, R* buf, const HaloSlab* tab, int nslabs, long long max_cells, const Geo& g,
                           int nv, cudaStream_t s);
   // meshes with level jumps: copies and restrictions, then prolongations
-  static cudaError_t amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
-                               const Geo& g, int nv, int ipr, int plim, double eps, cudaStream_t s);
+  static cudaError_t amr_ghost(R* q, const GhostRegion* reg, const BlockPos* pos, const int* list, int n0, int n1,
+                               const Geo& g, BaseGrid base, int nv, int ipr, int plim, double eps, cudaStream_t s);
   static cudaError_t maxspeed(int eq, const R* q, const Geo& g, double gamma, double csnd, DevScalars* sc,
                               int nblocks, cudaStream_t s);
   static cudaError_t copy_u0_u1(const double* u0, U1T* u1, long long n, cudaStream_t s);
@@ -195,11 +195,17 @@ cudaError_t Launch<R, U1T>::cons2prim_blocks(int eq, const double* u0, R* q, con
 }
 
 template <typename R, typename U1T>
-cudaError_t Launch<R, U1T>::amr_ghost(R* q, const GhostOp* ops1, long long n1, const GhostOp* ops2, long long n2,
-                                      const Geo& g, int nv, int ipr, int plim, double eps, cudaStream_t s) {
-  const int threads = 256;
-  if (n1 > 0) amr_copy_restrict_kernel<R><<<grid_for(n1, threads), threads, 0, s>>>(q, ops1, n1, g, nv);
-  if (n2 > 0) amr_prolong_kernel<R><<<grid_for(n2, threads), threads, 0, s>>>(q, ops2, n2, g, nv, ipr, plim, R(eps));
+cudaError_t Launch<R, U1T>::amr_ghost(R* q, const GhostRegion* reg, const BlockPos* pos, const int* list, int n0,
+                                      int n1, const Geo& g, BaseGrid base, int nv, int ipr, int plim, double eps,
+                                      cudaStream_t s) {
+  const int threads = 128;
+  // the copies and restrictions (list[0, n0)), then the prolongations
+  if (n0 > 0)
+    amr_ghost_kernel<R><<<n0 < 1048576 ? n0 : 1048576, threads, 0, s>>>(q, reg, pos, list, n0, g, base, nv, ipr,
+                                                                        plim, R(eps));
+  if (n1 > 0)
+    amr_ghost_kernel<R><<<n1 < 1048576 ? n1 : 1048576, threads, 0, s>>>(q, reg, pos, list + n0, n1, g, base, nv,
+                                                                        ipr, plim, R(eps));
   return cudaGetLastError();
 }
 

@@ -1075,96 +1075,159 @@ __global__ void halo_slab_kernel(R* q, R* buf, const HaloSlab* __restrict__ tab,
 
 // ---------------------------------------------------------------------------
 // Ghost fill on meshes with level jumps (boundary_variables,
-// src/boundaries.F90:372-479): one operation per ghost cell, built on the
-// host from the block positions.  dst/src are (block * qbs + padded cell);
-// kind & 3: 0 copy of a same-level cell (boundaries_*_copy), 1 mean of the
-// 2^d finer cells whose lower corner is src (block_*_restrict,
-// src/boundaries.F90:5637-6070, same pairing), 2 prolongation of the coarser
-// cell src (block_*_prolong, 6071-6450); kind >> 2: the child (bit d set for
-// the upper half along d).  Copies and restrictions run first; the
-// prolongations read the coarser blocks' cells and ghosts after them.
-// one ghost cell of a mesh with levels: the q offset it fills and, in one
-// word, the q offset it reads (low 58 bits) and its kind (the bits above:
-// 0 copy, 1 restriction, 2 | child << 2 prolongation) -- 16 bytes a ghost
-struct GhostOp {
-  long long dst, sk;
+// src/boundaries.F90:372-479).  The ghost cells of a block fall in 26
+// regions (faces, edges, corners: the positions below / inside / above the
+// interior along each axis).  Each region lies in one block-sized slot of the
+// block's level, and the host table says how that slot is covered:
+//   kind 0: by a block of the same level, src[0]: its cells are copied
+//           (boundaries_*_copy);
+//   kind 1: by 2^d finer blocks, src[x + 2 y + 4 z] the one at the upper
+//           (1) or lower (0) half along each axis: the mean of the 2^d finer
+//           cells (block_*_restrict, src/boundaries.F90:5637-6070, same
+//           pairing);
+//   kind 2: by a coarser block, src[0]: the prolongation of its cell
+//           (block_*_prolong, 6071-6450), the child given by the ghost cell's
+//           parity along each axis.
+// Each ghost cell computes its source from the table and the block's level
+// and position: a few hundred bytes of tables instead of 16 bytes per ghost
+// cell.  Copies and restrictions run first (pass 0); the prolongations read
+// the coarser blocks' cells and ghosts after them (pass 1).
+// ---------------------------------------------------------------------------
+struct GhostRegion {
+  int kind;
+  int src[8];
 };
-__host__ __device__ __forceinline__ long long op_src(const GhostOp& o) { return o.sk & ((1LL << 58) - 1); }
-__host__ __device__ __forceinline__ int op_kind(const GhostOp& o) { return (int)((unsigned long long)o.sk >> 58); }
-__host__ __device__ __forceinline__ long long op_pack(long long src, int kind) {
-  return src | ((long long)kind << 58);
-}
+struct BlockPos {
+  int level;
+  int c[3];  // position at its level, in blocks
+};
 
 template <typename R>
-__global__ void amr_copy_restrict_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv) {
+__device__ __forceinline__ void ghost_copy_restrict(R* q, long long dst, long long src, bool restrict_, const Geo& g,
+                                                    int nv) {
   const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const GhostOp op = ops[t];
-    const long long src = op_src(op);
-    const int kind = op_kind(op);
-    for (int v = 0; v < nv; ++v) {
-      const R* s = q + src + v * g.qvs;
-      R val;
-      if ((kind & 3) == 0) {
-        val = s[0];
-      } else if (g.ndims == 2) {
-        val = R(0.25) * ((s[0] + s[sX + sY]) + (s[sY] + s[sX]));
-      } else {
-        val = R(0.125) * (((s[0] + s[sX + sY + sZ]) + (s[sZ] + s[sX + sY])) +
-                          ((s[sY + sZ] + s[sX]) + (s[sY] + s[sX + sZ])));
-      }
-      q[op.dst + v * g.qvs] = val;
+  for (int v = 0; v < nv; ++v) {
+    const R* s = q + src + v * g.qvs;
+    R val;
+    if (!restrict_) {
+      val = s[0];
+    } else if (g.ndims == 2) {
+      val = R(0.25) * ((s[0] + s[sX + sY]) + (s[sY] + s[sX]));
+    } else {
+      val = R(0.125) * (((s[0] + s[sX + sY + sZ]) + (s[sZ] + s[sX + sY])) +
+                        ((s[sY + sZ] + s[sX]) + (s[sY] + s[sX + sZ])));
     }
+    q[dst + v * g.qvs] = val;
   }
 }
 
 template <typename R>
-__global__ void amr_prolong_kernel(R* q, const GhostOp* __restrict__ ops, long long n, Geo g, int nv, int ipr,
-                                   int plim, R eps) {
+__device__ __forceinline__ void ghost_prolong(R* q, long long dst, long long src, int sx, int sy, int sz,
+                                              const Geo& g, int nv, int ipr, int plim, R eps) {
   const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const GhostOp op = ops[t];
-    const long long src = op_src(op);
-    const int bits = op_kind(op) >> 2;
-    const int sx = bits & 1, sy = (bits >> 1) & 1, sz = (bits >> 2) & 1;
-    for (int v = 0; v < nv; ++v) {
-      const R* c = q + src + v * g.qvs;
-      const R q0 = c[0];
-      R d0 = limiter<R>(plim, R(0.5), q0 - c[-sX], c[sX] - q0, eps);
-      R d1 = limiter<R>(plim, R(0.5), q0 - c[-sY], c[sY] - q0, eps);
-      R d2 = g.ndims == 3 ? limiter<R>(plim, R(0.5), q0 - c[-sZ], c[sZ] - q0, eps) : R(0);
-      if (v == 0 || v == ipr) {  // density and pressure (ipr < 0: isothermal)
-        if (q0 > R(0)) {
-          for (int it = 0; it < 4096; ++it) {
-            R sa = d_fabs(d0) + d_fabs(d1);
-            if (g.ndims == 3) sa = sa + d_fabs(d2);
-            if (!(q0 <= sa)) break;
-            d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
-          }
-        } else {
-          d0 = d1 = d2 = R(0);
+  for (int v = 0; v < nv; ++v) {
+    const R* c = q + src + v * g.qvs;
+    const R q0 = c[0];
+    R d0 = limiter<R>(plim, R(0.5), q0 - c[-sX], c[sX] - q0, eps);
+    R d1 = limiter<R>(plim, R(0.5), q0 - c[-sY], c[sY] - q0, eps);
+    R d2 = g.ndims == 3 ? limiter<R>(plim, R(0.5), q0 - c[-sZ], c[sZ] - q0, eps) : R(0);
+    if (v == 0 || v == ipr) {  // density and pressure (ipr < 0: isothermal)
+      if (q0 > R(0)) {
+        for (int it = 0; it < 4096; ++it) {
+          R sa = d_fabs(d0) + d_fabs(d1);
+          if (g.ndims == 3) sa = sa + d_fabs(d2);
+          if (!(q0 <= sa)) break;
+          d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
         }
-      }
-      d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
-      R val;
-      if (g.ndims == 2) {
-        const R dq1 = d0 + d1, dq2 = d0 - d1;
-        const int ch = sx + 2 * sy;
-        val = ch == 0 ? q0 - dq1 : (ch == 1 ? q0 + dq2 : (ch == 2 ? q0 - dq2 : q0 + dq1));
       } else {
-        const R dq1 = d0 + d1 + d2, dq2 = d0 - d1 - d2, dq3 = d0 - d1 + d2, dq4 = d0 + d1 - d2;
-        switch (sx + 2 * sy + 4 * sz) {
-          case 0: val = q0 - dq1; break;
-          case 1: val = q0 + dq2; break;
-          case 2: val = q0 - dq3; break;
-          case 3: val = q0 + dq4; break;
-          case 4: val = q0 - dq4; break;
-          case 5: val = q0 + dq3; break;
-          case 6: val = q0 - dq2; break;
-          default: val = q0 + dq1; break;
-        }
+        d0 = d1 = d2 = R(0);
       }
-      q[op.dst + v * g.qvs] = val;
+    }
+    d0 = R(0.5) * d0; d1 = R(0.5) * d1; d2 = R(0.5) * d2;
+    R val;
+    if (g.ndims == 2) {
+      const R dq1 = d0 + d1, dq2 = d0 - d1;
+      const int ch = sx + 2 * sy;
+      val = ch == 0 ? q0 - dq1 : (ch == 1 ? q0 + dq2 : (ch == 2 ? q0 - dq2 : q0 + dq1));
+    } else {
+      const R dq1 = d0 + d1 + d2, dq2 = d0 - d1 - d2, dq3 = d0 - d1 + d2, dq4 = d0 + d1 - d2;
+      switch (sx + 2 * sy + 4 * sz) {
+        case 0: val = q0 - dq1; break;
+        case 1: val = q0 + dq2; break;
+        case 2: val = q0 - dq3; break;
+        case 3: val = q0 + dq4; break;
+        case 4: val = q0 - dq4; break;
+        case 5: val = q0 + dq3; break;
+        case 6: val = q0 - dq2; break;
+        default: val = q0 + dq1; break;
+      }
+    }
+    q[dst + v * g.qvs] = val;
+  }
+}
+
+// base: blocks per direction at level 1 (1 along z in 2D)
+struct BaseGrid {
+  int n[3];
+};
+
+// One CTA per ghost region of a list (entries b * 27 + region: the copies
+// and restrictions, or the prolongations); the region's kind, source blocks
+// and the offsets between its cells and theirs are set up once per CTA, so a
+// cell needs no divisions by the domain size.
+template <typename R>
+__global__ void amr_ghost_kernel(R* q, const GhostRegion* __restrict__ reg, const BlockPos* __restrict__ pos,
+                                 const int* __restrict__ list, int nlist, Geo g, BaseGrid base, int nv, int ipr,
+                                 int plim, R eps) {
+  const int nc = g.nc, ng = g.ng, nd = g.ndims;
+  for (int e = blockIdx.x; e < nlist; e += gridDim.x) {
+    const int b = list[e] / 27, d = list[e] - 27 * (list[e] / 27);
+    const int o[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+    const GhostRegion* rg = reg + (long long)b * 27 + d;
+    const int kind = rg->kind;
+    const BlockPos P = pos[b];
+    // first padded index, extent and global coordinate (periodic, at the
+    // block's level) of the region along each axis
+    int i0[3] = {0, 0, 0}, n[3] = {1, 1, 1}, cf[3] = {0, 0, 0};
+    for (int a = 0; a < nd; ++a) {
+      i0[a] = o[a] < 0 ? 0 : (o[a] == 0 ? ng : ng + nc);
+      n[a] = o[a] == 0 ? nc : ng;
+      const int ext = (base.n[a] << (P.level - 1)) * nc;
+      int v = (P.c[a] * nc + i0[a] - ng) % ext;
+      cf[a] = v < 0 ? v + ext : v;
+    }
+    // copies: the source block's padded index of the region's first cell
+    int lo[3] = {0, 0, 0};
+    if (kind == 0) {
+      const BlockPos S = pos[rg->src[0]];
+      for (int a = 0; a < nd; ++a) lo[a] = cf[a] - S.c[a] * nc + ng;
+    }
+    const int cnt = n[0] * n[1] * n[2];
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const int x = t % n[0], y = (t / n[0]) % n[1], z = t / (n[0] * n[1]);
+      const long long dst = (long long)b * g.qbs + ((long long)(i0[2] + z) * g.JM + (i0[1] + y)) * g.IM + (i0[0] + x);
+      const int c[3] = {cf[0] + x, cf[1] + y, nd == 3 ? cf[2] + z : 0};
+      if (kind == 0) {
+        const long long src = (long long)rg->src[0] * g.qbs +
+                              ((long long)(nd == 3 ? lo[2] + z : 0) * g.JM + (lo[1] + y)) * g.IM + (lo[0] + x);
+        ghost_copy_restrict<R>(q, dst, src, false, g, nv);
+      } else if (kind == 1) {
+        int sub = 0;
+        for (int a = 0; a < nd; ++a) sub |= (((2 * c[a]) / nc) & 1) << a;
+        const int F = rg->src[sub];
+        const BlockPos FP = pos[F];
+        const long long src = (long long)F * g.qbs +
+                              ((long long)(nd == 3 ? 2 * c[2] - FP.c[2] * nc + ng : 0) * g.JM +
+                               (2 * c[1] - FP.c[1] * nc + ng)) * g.IM + (2 * c[0] - FP.c[0] * nc + ng);
+        ghost_copy_restrict<R>(q, dst, src, true, g, nv);
+      } else {
+        const int Cb = rg->src[0];
+        const BlockPos CP = pos[Cb];
+        const long long src = (long long)Cb * g.qbs +
+                              ((long long)(nd == 3 ? (c[2] >> 1) - CP.c[2] * nc + ng : 0) * g.JM +
+                               ((c[1] >> 1) - CP.c[1] * nc + ng)) * g.IM + ((c[0] >> 1) - CP.c[0] * nc + ng);
+        ghost_prolong<R>(q, dst, src, c[0] & 1, c[1] & 1, nd == 3 ? c[2] & 1 : 0, g, nv, ipr, plim, eps);
+      }
     }
   }
 }
