@@ -108,6 +108,10 @@ struct Ctx {
   void* ff = nullptr;        // stored face fluxes
   int* fcount = nullptr;     // [b][dir][side] tiles that stored a face (one launch over all levels)
   bool level_launches = false;  // one sweep launch per level instead of one over all levels
+  // one-level meshes: the neighbour table is symmetric (nbr[nbr[b][n]][26-n]
+  // == b), so the last sweep can write the ghost cells itself
+  bool nbr_sym = false;
+  bool ghost_in_sweep = true;
   std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
   // sweep tile chosen by amun_gpu_autotune (0: the default shape)
   int tile_LP = 0, tile_LW = 0;
@@ -432,6 +436,11 @@ int sweep_halo() {
   const int v = sweep_variant();
   return v == REC_GEN ? 3 : (v == AMUN_REC_WENO5Z ? 2 : 1);
 }
+// staged variable planes of a sweep CTA: the FP32 WENO-Z and TVD sweeps keep
+// their variables in pairs, so an odd count takes one plane more
+int sweep_planes(size_t rsz) {
+  return (rsz == sizeof(float) && sweep_variant() != REC_GEN) ? (C.nv + 1) & ~1 : C.nv;
+}
 
 // The fused stage kernel covers WENO-Z on blocks of one level for the
 // adiabatic HD (HLL, HLLC) and MHD (HLL, HLLC, HLLD) systems, without the
@@ -540,13 +549,18 @@ int effective_solver() {
 template <typename R>
 cudaError_t ghost_fill(R* q);
 
+// the last sweep of a stage writes the same-level ghost cells (instead of
+// ghost_copy_kernel after it) on one-level meshes with a symmetric
+// neighbour table, when the sweeps run (not the fused stage kernel)
+bool ghost_in_sweep() { return C.ghost_in_sweep && !C.amr && C.nbr_sym && !use_stage(); }
+
 template <typename R>
 int launch_stage(const StageDesc& st) {
   int LP, LW;
   tile_shape(LP, LW);
   const int RR = sweep_halo();
   const int threads = (((LP + 2) * LW + 31) / 32) * 32;
-  const size_t smem = (size_t)C.nv * ((LP + 2 * RR + 2) + 2 * (LP + 2)) * LW * sizeof(R);
+  const size_t smem = (size_t)sweep_planes(sizeof(R)) * ((LP + 2 * RR + 2) + 2 * (LP + 2)) * LW * sizeof(R);
   const int nthird = C.g.ndims == 3 ? C.g.nc : 1;
   dim3 grid((C.g.nc / LP) * (C.g.nc / LW) * nthird, C.nblocks);
   SweepArgs<R, R> a;
@@ -565,6 +579,9 @@ int launch_stage(const StageDesc& st) {
   a.blist = nullptr; a.frole = nullptr; a.fquad = nullptr; a.ff = nullptr; a.fcount = nullptr; a.nfcount = 0;
   a.fcl = (const R*)C.fcl; a.fcr = (const R*)C.fcr;
   a.ugp = C.ugp;
+  // same-level ghost cells written by the last sweep (one-level meshes)
+  const bool ghost_fused = ghost_in_sweep();
+  a.gnbr = ghost_fused ? C.nbr : nullptr;
   const int rs = effective_solver();
   const bool compact = rec_compact(C.p.reconstruction);
   if (use_stage()) {
@@ -616,9 +633,12 @@ int launch_stage(const StageDesc& st) {
     }
   }
   C.cur = 1 - C.cur;
-  ProfScope ps(3);
-  cudaError_t e = ghost_fill<R>((R*)C.q[C.cur]);
-  if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  cudaError_t e = cudaSuccess;
+  if (!ghost_fused) {
+    ProfScope ps(3);
+    e = ghost_fill<R>((R*)C.q[C.cur]);
+    if (e != cudaSuccess) return cuda_fail(e, "ghost fill");
+  }
   if (C.p.fix_unphysical) {
     // correct_unphysical_states after the boundary update
     // (src/evolution.F90:2043-2068); the maximum speed of the final stage's
@@ -1349,6 +1369,12 @@ int amun_gpu_set_blocks(int nblocks, const amun_block_desc* blocks) {
     if (nd == 3) m = m < blocks[b].dx[2] ? m : blocks[b].dx[2];
     if (m < C.dx_min) C.dx_min = m;
   }
+  C.nbr_sym = true;
+  for (int b = 0; b < nblocks && C.nbr_sym; ++b)
+    for (int n = 0; n < 27; ++n) {
+      const int t = nbr[27 * b + n];
+      if (t >= nblocks || (t >= 0 && nbr[27 * (size_t)t + (26 - n)] != b)) { C.nbr_sym = false; break; }
+    }
   CK(cudaMalloc(&C.nbr, nbr.size() * sizeof(int)));
   CK(cudaMalloc(&C.binv, binv.size() * sizeof(double)));
   CK(h2d(C.nbr, nbr.data(), nbr.size() * sizeof(int)));
@@ -2159,6 +2185,15 @@ int amun_gpu_set_level_launches(int per_level) {
   return 0;
 }
 
+int amun_gpu_set_ghost_in_sweep(int on) {
+  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
+  CK(cudaStreamSynchronize(C.stream));
+  for (auto& gx : C.graph)
+    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  C.ghost_in_sweep = on != 0;
+  return 0;
+}
+
 int amun_gpu_wait_selftest(long long cycles, int* gave_up) {
   int r = check_ready();
   if (r) return r;
@@ -2664,7 +2699,7 @@ int amun_gpu_autotune(int reps, int* best_lp, int* best_lw, double* best_ms) {
     const int big = lws.back();
     for (int lw : lws) {
       if (lw != big && 2 * lw != big && 4 * lw != big) continue;
-      const size_t smem = (size_t)C.nv * ((lp + 2 * RR + 2) + 2 * (lp + 2)) * lw * rsize();
+      const size_t smem = (size_t)sweep_planes(rsize()) * ((lp + 2 * RR + 2) + 2 * (lp + 2)) * lw * rsize();
       if (smem <= 200 * 1024) cand.push_back({lp, lw});
     }
   }

@@ -127,6 +127,10 @@ template <typename R, typename U1T> struct SweepArgs {
   const R* fcr;
   // multidimensional GP: weights [dir][side][ngp^NDIMS points]
   const double* ugp;
+  // one-level meshes with a symmetric neighbour table [b][27] (null
+  // otherwise): the last direction also writes each new cell into the ghost
+  // cells that copy it, so the stage needs no separate ghost fill
+  const int* gnbr;
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
@@ -380,9 +384,15 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   const Geo& g = a.g;
   const int LP = TLP ? TLP : a.LP, LW = TLW ? TLW : a.LW;
   const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
+  // FP32 WENO-Z and TVD: the staged states, face states and fluxes of the
+  // variables 2m and 2m+1 sit side by side, so one 64-bit shared-memory
+  // access moves both operands of a packed f32x2 instruction (an odd last
+  // variable has a pair slot of its own); otherwise one plane per variable
+  constexpr bool PAIR = (REC == REC_WENO5Z || REC == REC_TVD) && std::is_same<R, float>::value;
+  constexpr int NVP = PAIR ? (NV + 1) & ~1 : NV;
   R* Qs = sm;
-  R* FLs = Qs + (size_t)NV * NPQ * LW;
-  R* FRs = FLs + (size_t)NV * NPF * LW;
+  R* FLs = Qs + (size_t)NVP * NPQ * LW;
+  R* FRs = FLs + (size_t)NVP * NPF * LW;
   R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
 
   const int nc = g.nc, ng = g.ng;
@@ -412,8 +422,43 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   const R* qb = a.q + (long long)b * g.qbs;
 
   auto sidx = [&](int v, int pp, int ll, int NP) -> int {
+    if constexpr (PAIR) {
+      const int c = DIR == 0 ? ((v >> 1) * LW + ll) * NP + pp : ((v >> 1) * NP + pp) * LW + ll;
+      return 2 * c + (v & 1);
+    }
     return DIR == 0 ? (v * LW + ll) * NP + pp : (v * NP + pp) * LW + ll;
   };
+  // the pair (v, v+1), v even, of a paired array
+  auto ld2 = [&](const R* s, int v, int pp, int ll, int NP) -> float2 {
+    return *reinterpret_cast<const float2*>(s + sidx(v, pp, ll, NP));
+  };
+  auto st2 = [&](R* s, int v, int pp, int ll, int NP, float x, float y) {
+    *reinterpret_cast<float2*>(s + sidx(v, pp, ll, NP)) = make_float2(x, y);
+  };
+  // every variable of one cell from / into a staged array
+  auto load_all = [&](const R* s, int pp, int ll, int NP, R* out) {
+    if constexpr (PAIR) {
+#pragma unroll
+      for (int v = 0; v < NV; v += 2) {
+        const float2 p = ld2(s, v, pp, ll, NP);
+        out[v] = p.x;
+        if (v + 1 < NV) out[v + 1] = p.y;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v] = s[sidx(v, pp, ll, NP)];
+    }
+  };
+  auto store_all = [&](R* s, int pp, int ll, int NP, const R* in) {
+    if constexpr (PAIR) {
+#pragma unroll
+      for (int v = 0; v < NV; v += 2) st2(s, v, pp, ll, NP, in[v], v + 1 < NV ? in[v + 1] : 0.0f);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[sidx(v, pp, ll, NP)] = in[v];
+    }
+  };
+  (void)ld2; (void)st2;
   auto decode = [&](int t, int NP, int& pp, int& ll) {
     if (DIR == 0) { ll = t / NP; pp = t - ll * NP; }
     else { pp = t / LW; ll = t - pp * LW; }
@@ -452,8 +497,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     if constexpr (V::SR) {
       if (four) to_four_velocity(qc);
     }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) Qs[sidx(v, pp, ll, NPQ)] = qc[v];
+    store_all(Qs, pp, ll, NPQ, qc);
   }
   (void)PM;
   __syncthreads();
@@ -593,32 +637,40 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       R fRv[NV], fLv[NV];
       constexpr bool fast = REC == REC_WENO5Z && std::is_same<R, float>::value;
       if constexpr (fast) {
-        // FP32 bulk: two variables per instruction (weno5z_faces_fast)
+        // FP32 bulk: two variables per instruction (weno5z_faces_fast), the
+        // stencil of a pair in five 64-bit loads; the per-variable fixes
+        // take the centre values from the same registers
 #pragma unroll
         for (int v = 0; v + 1 < NV; v += 2) {
           float2 st[5];
 #pragma unroll
-          for (int o = 0; o < 5; ++o)
-            st[o] = make_float2(Qs[sidx(v, cq - 2 + o, ll, NPQ)], Qs[sidx(v + 1, cq - 2 + o, ll, NPQ)]);
+          for (int o = 0; o < 5; ++o) st[o] = ld2(Qs, v, cq - 2 + o, ll, NPQ);
           float2 r, l;
           weno5z_faces_fast(st[0], st[1], st[2], st[3], st[4], (float)a.m.eps, r, l);
           fRv[v] = r.x; fRv[v + 1] = r.y; fLv[v] = l.x; fLv[v + 1] = l.y;
+          dir_fix(st[1].x, st[2].x, st[3].x, v == V::DN || v == V::PR, fRv[v], fLv[v]);
+          dir_fix(st[1].y, st[2].y, st[3].y, v + 1 == V::DN || v + 1 == V::PR, fRv[v + 1], fLv[v + 1]);
         }
         if constexpr (NV & 1) {
           float st[5];
 #pragma unroll
           for (int o = 0; o < 5; ++o) st[o] = Qs[sidx(NV - 1, cq - 2 + o, ll, NPQ)];
           weno5z_faces_fast(st[0], st[1], st[2], st[3], st[4], (float)a.m.eps, fRv[NV - 1], fLv[NV - 1]);
+          dir_fix(st[1], st[2], st[3], NV - 1 == V::DN || NV - 1 == V::PR, fRv[NV - 1], fLv[NV - 1]);
         }
+      }
+      // FP32 TVD: the three cells of a variable pair in three 64-bit loads
+      constexpr bool tvd_pair = PAIR && REC == REC_TVD;
+      if constexpr (tvd_pair) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const bool positive = (v == V::DN || v == V::PR);
-          dir_fix(Qs[sidx(v, cq - 1, ll, NPQ)], Qs[sidx(v, cq, ll, NPQ)], Qs[sidx(v, cq + 1, ll, NPQ)], positive,
-                  fRv[v], fLv[v]);
+        for (int v = 0; v < NV; v += 2) {
+          const float2 m = ld2(Qs, v, cq - 1, ll, NPQ), c = ld2(Qs, v, cq, ll, NPQ), p = ld2(Qs, v, cq + 1, ll, NPQ);
+          tvd(v, pp, ll, c.x, m.x, p.x, v == V::DN || v == V::PR, fRv[v], fLv[v]);
+          if (v + 1 < NV) tvd(v + 1, pp, ll, c.y, m.y, p.y, v + 1 == V::DN || v + 1 == V::PR, fRv[v + 1], fLv[v + 1]);
         }
       }
 #pragma unroll
-      for (int v = 0; v < NV && !fast; ++v) {
+      for (int v = 0; v < NV && !fast && !tvd_pair; ++v) {
         R fR, fL;
         const R f0 = Qs[sidx(v, cq, ll, NPQ)];
         const R fm1 = Qs[sidx(v, cq - 1, ll, NPQ)], fp1 = Qs[sidx(v, cq + 1, ll, NPQ)];
@@ -659,11 +711,8 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       if constexpr (V::SR) {
         if (four && !mlp) { from_four_velocity(fRv); from_four_velocity(fLv); }
       }
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        FLs[sidx(v, pp, ll, NPF)] = fRv[v];
-        FRs[sidx(v, pp, ll, NPF)] = fLv[v];
-      }
+      store_all(FLs, pp, ll, NPF, fRv);
+      store_all(FRs, pp, ll, NPF, fLv);
     }
   }
   __syncthreads();
@@ -704,14 +753,13 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     for (int t = threadIdx.x; t < NPI * LW; t += blockDim.x) {
       int pp, ll; decode(t, NPI, pp, ll);
       R ql[NV], qr[NV], tl[NV], tr[NV], f[NV], fo[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) { tl[v] = FLs[sidx(v, pp, ll, NPF)]; tr[v] = FRs[sidx(v, pp + 1, ll, NPF)]; }
+      load_all(FLs, pp, ll, NPF, tl);
+      load_all(FRs, pp + 1, ll, NPF, tr);
       rotate<EQ, DIR>(tl, ql);
       rotate<EQ, DIR>(tr, qr);
       riemann<EQ, RS>(ql, qr, f, P);
       unrotate<EQ, DIR>(f, fo);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) Fs[sidx(v, pp, ll, NPI)] = fo[v];
+      store_all(Fs, pp, ll, NPI, fo);
     }
   }
   __syncthreads();
@@ -799,10 +847,21 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
     const long long ci = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP + (long long)(l0 - ng + ll) * iL +
                          (long long)(g.ndims == 3 ? th : 0) * iT;
-    R dloc[NV];
+    R dloc[NV], dfl[NV];
+    if constexpr (PAIR) {
+#pragma unroll
+      for (int v = 0; v < NV; v += 2) {
+        const float2 hi = ld2(Fs, v, pp + 1, ll, NPI), lo = ld2(Fs, v, pp, ll, NPI);
+        dfl[v] = hi.x - lo.x;
+        if (v + 1 < NV) dfl[v + 1] = hi.y - lo.y;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) dfl[v] = Fs[sidx(v, pp + 1, ll, NPI)] - Fs[sidx(v, pp, ll, NPI)];
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      R d = Fs[sidx(v, pp + 1, ll, NPI)] - Fs[sidx(v, pp, ll, NPI)];
+      R d = dfl[v];
       if (a.first) dloc[v] = -(dsi * d);
       else dloc[v] = a.du[ci + v * g.uvs] - dsi * d;
     }
@@ -872,6 +931,31 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) a.qout[co + v * g.qvs] = qs[v];
+    if (a.gnbr) {
+      // the same-level ghost copy (boundaries_*_copy, src/boundaries.F90:
+      // 1273-1635) done by the source cell: a cell within nghosts of a block
+      // face is the source of the ghost cell s - e nc of the neighbour
+      // across e, for every direction e whose components are 0 or point to
+      // a face the cell is near
+      const int Pc = p0 + pp, Lc = l0 + ll;
+      const int sx = DIR == 0 ? Pc : Lc, sy = DIR == 1 ? Pc : (DIR == 0 ? Lc : t0), sz = DIR == 2 ? Pc : t0;
+      const int xlo = sx < 2 * ng ? -1 : 0, xhi = sx >= nc ? 1 : 0;
+      const int ylo = sy < 2 * ng ? -1 : 0, yhi = sy >= nc ? 1 : 0;
+      const int zlo = g.ndims == 3 && sz < 2 * ng ? -1 : 0, zhi = g.ndims == 3 && sz >= nc ? 1 : 0;
+      if ((xlo | xhi | ylo | yhi | zlo | zhi) != 0) {
+        for (int ez = zlo; ez <= zhi; ++ez)
+          for (int ey = ylo; ey <= yhi; ++ey)
+            for (int ex = xlo; ex <= xhi; ++ex) {
+              if ((ex | ey | ez) == 0) continue;
+              const int nb = a.gnbr[27 * b + (ex + 1) + 3 * (ey + 1) + 9 * (ez + 1)];
+              if (nb < 0) continue;
+              const long long dst = (long long)nb * g.qbs +
+                                    ((long long)(sz - ez * nc) * g.JM + (sy - ey * nc)) * g.IM + (sx - ex * nc);
+#pragma unroll
+              for (int v = 0; v < NV; ++v) a.qout[dst + v * g.qvs] = qs[v];
+            }
+      }
+    }
     if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma, a.m.csnd));
   }
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);

@@ -291,6 +291,11 @@ class Simulation:
         N.check(self.L.amun_gpu_set_stage_kernel(int(mode), int(planes), C.byref(active)))
         return bool(active.value)
 
+    def set_ghost_in_sweep(self, on: bool = True) -> None:
+        """True (the default): on one-level meshes the last sweep of a stage
+        writes the same-level ghost cells; False: a separate ghost fill."""
+        N.check(self.L.amun_gpu_set_ghost_in_sweep(int(bool(on))))
+
     def _states(self, a: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float64)
         if a.ndim == 0 or a.shape[-1] != self.nv:

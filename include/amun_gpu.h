@@ -384,6 +384,16 @@ int amun_gpu_profile_read(int kind, double* total_ms, long long* launches);
  * amun_gpu_advance then fails; it does not happen when the tiles of a launch
  * start in index order.  Invalidates captured graphs. */
 int amun_gpu_set_level_launches(int per_level);
+
+/* Same-level ghost cells (boundaries_*_copy, src/boundaries.F90:1273-1635,
+ * called from boundary_variables 372-479): on a mesh of one level whose
+ * neighbour table is symmetric, the last sweep of each stage writes every
+ * new interior cell near a block face into the ghost cells that copy it, so
+ * no separate ghost-fill launch follows (on == 1, the default).  on == 0
+ * restores the separate fill.  Both give the same ghost cells; meshes with
+ * level jumps and the fused stage kernel always fill separately.
+ * Invalidates captured graphs.  No reference counterpart (a launch choice). */
+int amun_gpu_set_ghost_in_sweep(int on);
 /* Runs one bounded device wait on a count that nothing raises (the wait of
  * the flux correction above, given `cycles` clock cycles) and reports in
  * *gave_up whether it gave up and recorded a stall, as it must; the stall
