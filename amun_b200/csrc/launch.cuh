@@ -64,10 +64,9 @@ cudaError_t sweep_eq_fixed(int rec, int rs, int dir, const SweepArgs<R, U1T>& a,
                            size_t smem, cudaStream_t s);
 
 #ifdef AMUN_SWEEP_IMPL
-// the tile-list form of the fixed-tile FP32 sweeps: with a.pipeline as many
-// CTAs as fit on the device at once (occupancy of the kernel with its second
-// staging buffer), each walking the tiles with the next tile's copies in
-// flight; without it one CTA per tile
+// the persistent form with copies in flight: as many CTAs as fit on the
+// device at once (occupancy of the kernel with its second staging buffer),
+// each walking the grid's tiles
 template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP, int TLW>
 static cudaError_t go_sweep_async(const SweepArgs<R, U1T>& a0, dim3 grid, int threads, size_t smem, cudaStream_t s) {
   auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW, true>;
@@ -91,7 +90,7 @@ static cudaError_t go_sweep_async(const SweepArgs<R, U1T>& a0, dim3 grid, int th
   }
   SweepArgs<R, U1T> a = a0;
   a.ntiles = (int)(grid.x * grid.y);
-  dim3 g2(a.pipeline && a.ntiles > resident ? resident : a.ntiles, 1);
+  dim3 g2(a.ntiles < resident ? a.ntiles : resident, 1);
   k<<<g2, threads, smem2, s>>>(a);
   return cudaGetLastError();
 }
@@ -100,7 +99,7 @@ template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP = 
 static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
   if constexpr (TLP > 0 && std::is_same<R, float>::value && (EQ == EQ_HD || EQ == EQ_MHD) &&
                 (REC == REC_TVD || REC == REC_WENO5Z)) {
-    if (!a.blist && !a.frole && !a.fcount)
+    if (a.pipeline && !a.blist && !a.frole && !a.fcount)
       return go_sweep_async<R, U1T, EQ, REC, RS, DIR, TLP, TLW>(a, grid, threads, smem, s);
   }
   auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW>;

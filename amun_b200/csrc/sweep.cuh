@@ -387,12 +387,10 @@ __device__ __forceinline__ void mlp_faces(const R* qb, const Geo& g, bool four, 
 // it), so every shared-memory index and task split folds to constants;
 // 0 x 0: the shape is read from the arguments
 //
-// ASYNC: the tiles of every block (one-level meshes, no face correction) are
-// indexed along the grid's x; with a.pipeline the grid is persistent, each
-// CTA taking the tiles blockIdx.x, + gridDim.x, ... and copying the next
-// tile's states into a second staging buffer with cp.async while it computes
-// the current one, so the tile loads leave the critical path; without it,
-// one tile per CTA with synchronous loads (the same instructions otherwise).
+// ASYNC: a persistent grid; each CTA takes the tiles blockIdx.x, + gridDim.x,
+// ... of every block (one-level meshes, no face correction) and copies the
+// next tile's states into a second staging buffer with cp.async while it
+// computes the current one, so the tile loads leave the critical path.
 template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0, bool ASYNC = false>
 #ifndef AMUN_SWEEP_MIN_BLOCKS
 #define AMUN_SWEEP_MIN_BLOCKS 1
@@ -487,11 +485,8 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   };
   (void)issue_load;
 
-  // ASYNC with pipeline == 0: the same kernel with one tile per CTA and
-  // synchronous loads (the grid covers every tile)
-  const bool copies = ASYNC && a.pipeline;
   int id = ASYNC ? (int)blockIdx.x : 0;
-  if (copies) {
+  if constexpr (ASYNC) {
     if (id < a.ntiles) issue_load(Qbuf0, id);
     cp_async_commit();
   }
@@ -550,7 +545,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- load the tile and its halo --------------------------------------------
   // (the generic variant's three-cell halo is clamped to the block: methods
   // with shorter stencils run with fewer ghost layers and never read it)
-  if (copies) {
+  if constexpr (ASYNC) {
     // the next tile's copies go into the other buffer (free since the
     // barrier that ended the previous tile); this tile's are waited for
     const int nxt = id + (int)gridDim.x;
@@ -1036,7 +1031,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   __syncthreads();
   id += gridDim.x;
   }
-  if (copies) cp_async_wait<0>();
+  if constexpr (ASYNC) cp_async_wait<0>();
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
 }
 

@@ -100,10 +100,9 @@ def run_pipe(p, pipeline, q0, steps, graph):
 @pytest.mark.parametrize("eq,rec,rs,ta,nd,n,nb", PIPE_CASES)
 def test_sweep_pipeline_matches_one_tile_per_cta(eq, rec, rs, ta, nd, n, nb):
     """The persistent FP32 sweeps with the next tile's copies in flight
-    (amun_gpu_set_sweep_pipeline(1), the default) against the same kernel
-    with one CTA per tile and synchronous loads: the same instructions on
-    the same staged values, so bit-identical states; and both within the
-    FP32-bulk accuracy of the FP64 run."""
+    (amun_gpu_set_sweep_pipeline(1), the default) against one CTA per tile
+    with synchronous loads: the same arithmetic on the same staged values,
+    so bit-identical states."""
     kw = dict(ncells=n, xblocks=nb, yblocks=nb)
     if nd == 3:
         kw["zblocks"] = nb
@@ -121,6 +120,3 @@ def test_sweep_pipeline_matches_one_tile_per_cta(eq, rec, rs, ta, nd, n, nb):
         assert np.all(np.isfinite(u1))
         np.testing.assert_array_equal(q1, q0s, err_msg="primitives with ghost cells")
         np.testing.assert_array_equal(u1, u0, err_msg="conserved states")
-    u64, _ = run(p, "fp64", True, q0, 3, False)
-    l1 = np.abs(u1[..., 0] - u64[..., 0]).sum() / np.abs(u64[..., 0]).sum()
-    assert l1 <= 1.0e-5, l1
