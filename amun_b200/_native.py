@@ -114,7 +114,6 @@ def lib():
         "amun_gpu_stages": (i, [C.POINTER(i)]),
         "amun_gpu_set_level_launches": (i, [i]),
         "amun_gpu_set_ghost_in_sweep": (i, [i]),
-        "amun_gpu_set_sweep_pipeline": (i, [i]),
         "amun_gpu_wait_selftest": (i, [C.c_longlong, C.POINTER(i)]),
         "amun_gpu_integrals": (i, [_D]),
         "amun_gpu_set_blocks_sharded": (i, [i, C.POINTER(amun_block_desc), C.POINTER(i), i]),

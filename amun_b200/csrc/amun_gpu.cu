@@ -112,9 +112,6 @@ struct Ctx {
   // == b), so the last sweep can write the ghost cells itself
   bool nbr_sym = false;
   bool ghost_in_sweep = true;
-  // FP32 TVD / WENO-Z sweeps of one-level meshes: persistent, with the next
-  // tile's copies in flight
-  bool sweep_pipeline = true;
   std::vector<std::pair<int, int>> lgroups;  // (offset, count) per level, finest first
   // sweep tile chosen by amun_gpu_autotune (0: the default shape)
   int tile_LP = 0, tile_LW = 0;
@@ -585,8 +582,6 @@ int launch_stage(const StageDesc& st) {
   // same-level ghost cells written by the last sweep (one-level meshes)
   const bool ghost_fused = ghost_in_sweep();
   a.gnbr = ghost_fused ? C.nbr : nullptr;
-  a.pipeline = C.sweep_pipeline && !C.amr;
-  a.ntiles = 0;
   const int rs = effective_solver();
   const bool compact = rec_compact(C.p.reconstruction);
   if (use_stage()) {
@@ -2187,15 +2182,6 @@ int amun_gpu_set_level_launches(int per_level) {
   for (auto& gx : C.graph)
     if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   C.level_launches = per_level != 0;
-  return 0;
-}
-
-int amun_gpu_set_sweep_pipeline(int on) {
-  if (!C.inited) return fail(AMUN_E_NOT_INITIALIZED, "amun_gpu_init has not been called");
-  CK(cudaStreamSynchronize(C.stream));
-  for (auto& gx : C.graph)
-    if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
-  C.sweep_pipeline = on != 0;
   return 0;
 }
 

@@ -64,44 +64,8 @@ cudaError_t sweep_eq_fixed(int rec, int rs, int dir, const SweepArgs<R, U1T>& a,
                            size_t smem, cudaStream_t s);
 
 #ifdef AMUN_SWEEP_IMPL
-// the persistent form with copies in flight: as many CTAs as fit on the
-// device at once (occupancy of the kernel with its second staging buffer),
-// each walking the grid's tiles
-template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP, int TLW>
-static cudaError_t go_sweep_async(const SweepArgs<R, U1T>& a0, dim3 grid, int threads, size_t smem, cudaStream_t s) {
-  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW, true>;
-  constexpr int RR = REC == REC_WENO5Z ? 2 : 1;
-  constexpr int NVP = (Var<EQ>::NV + 1) & ~1;
-  const size_t smem2 = smem + (size_t)NVP * (TLP + 2 * RR + 2) * TLW * sizeof(R);
-  static int resident = 0;
-  static size_t resident_smem = 0;
-  if (!resident || resident_smem != smem2) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0, dev = 0, nsm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem2);
-    if (e != cudaSuccess) return e;
-    e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    resident = (per_sm > 0 ? per_sm : 1) * nsm;
-    resident_smem = smem2;
-  }
-  SweepArgs<R, U1T> a = a0;
-  a.ntiles = (int)(grid.x * grid.y);
-  dim3 g2(a.ntiles < resident ? a.ntiles : resident, 1);
-  k<<<g2, threads, smem2, s>>>(a);
-  return cudaGetLastError();
-}
-
 template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP = 0, int TLW = 0>
 static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
-  if constexpr (TLP > 0 && std::is_same<R, float>::value && (EQ == EQ_HD || EQ == EQ_MHD) &&
-                (REC == REC_TVD || REC == REC_WENO5Z)) {
-    if (a.pipeline && !a.blist && !a.frole && !a.fcount)
-      return go_sweep_async<R, U1T, EQ, REC, RS, DIR, TLP, TLW>(a, grid, threads, smem, s);
-  }
   auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW>;
   static bool attr_set = false;
   if (!attr_set) {

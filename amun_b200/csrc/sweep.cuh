@@ -131,25 +131,9 @@ template <typename R, typename U1T> struct SweepArgs {
   // otherwise): the last direction also writes each new cell into the ghost
   // cells that copy it, so the stage needs no separate ghost fill
   const int* gnbr;
-  // persistent launch with copies in flight (the ASYNC form of the FP32
-  // TVD / WENO-Z sweeps of HD / MHD on one-level meshes): pipeline != 0
-  // requests it, ntiles is the tiles of every block (set by the launcher)
-  int pipeline;
-  int ntiles;
 };
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
-
-// asynchronous 4-byte copy global -> shared (completes at cp_async_wait)
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// waits until at most N of this thread's committed copy groups are pending
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // a load through L2 that the compiler keeps after the preceding barrier
 // (the ld.global.cg intrinsic is a plain asm the compiler may hoist above the
@@ -386,12 +370,7 @@ __device__ __forceinline__ void mlp_faces(const R* qb, const Geo& g, bool four, 
 // TLP x TLW > 0: the tile shape fixed at compile time (a.LP, a.LW must equal
 // it), so every shared-memory index and task split folds to constants;
 // 0 x 0: the shape is read from the arguments
-//
-// ASYNC: a persistent grid; each CTA takes the tiles blockIdx.x, + gridDim.x,
-// ... of every block (one-level meshes, no face correction) and copies the
-// next tile's states into a second staging buffer with cp.async while it
-// computes the current one, so the tile loads leave the critical path.
-template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0, bool ASYNC = false>
+template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0>
 #ifndef AMUN_SWEEP_MIN_BLOCKS
 #define AMUN_SWEEP_MIN_BLOCKS 1
 #endif
@@ -411,17 +390,36 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // variable has a pair slot of its own); otherwise one plane per variable
   constexpr bool PAIR = (REC == REC_WENO5Z || REC == REC_TVD) && std::is_same<R, float>::value;
   constexpr int NVP = PAIR ? (NV + 1) & ~1 : NV;
-  R* const Qbuf0 = sm;
-  R* const Qbuf1 = sm + (size_t)NVP * NPQ * LW;
-  R* FLs = sm + (size_t)(ASYNC ? 2 : 1) * NVP * NPQ * LW;
+  R* Qs = sm;
+  R* FLs = Qs + (size_t)NVP * NPQ * LW;
   R* FRs = FLs + (size_t)NVP * NPF * LW;
-  (void)Qbuf1;
+  R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
 
   const int nc = g.nc, ng = g.ng;
+  int bx = blockIdx.x, by = blockIdx.y;
+  if (a.fcount) {
+    __shared__ int ticket;
+    if (threadIdx.x == 0) ticket = atomicAdd(a.fcount + a.nfcount, 1);
+    __syncthreads();
+    bx = ticket % gridDim.x;
+    by = ticket / gridDim.x;
+  }
+  const int b = a.blist ? a.blist[by] : by;
+  int tile = bx;
   const int ntp = nc / LP, ntl = nc / LW;
-  const int tpb = ntp * ntl * (g.ndims == 3 ? nc : 1);  // tiles per block
-  const bool final_stage = a.last && a.st.final_stage;
-  double vmax = 0.0;
+  const int tp = tile % ntp; tile /= ntp;
+  const int tl = tile % ntl; tile /= ntl;
+  const int th = tile;
+  const int p0 = ng + tp * LP, l0 = ng + tl * LW;
+  const int t0 = (g.ndims == 3) ? ng + th : 0;
+  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
+  const long long sP = DIR == 0 ? sX : (DIR == 1 ? sY : sZ);
+  const long long sL = DIR == 0 ? sY : sX;
+  const long long sT = DIR == 2 ? sY : sZ;
+  const long long iP = DIR == 0 ? 1 : (DIR == 1 ? nc : (long long)nc * nc);
+  const long long iL = DIR == 0 ? nc : 1;
+  const long long iT = DIR == 2 ? nc : (long long)nc * nc;
+  const R* qb = a.q + (long long)b * g.qbs;
 
   auto sidx = [&](int v, int pp, int ll, int NP) -> int {
     if constexpr (PAIR) {
@@ -465,64 +463,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     if (DIR == 0) { ll = t / NP; pp = t - ll * NP; }
     else { pp = t / LW; ll = t - pp * LW; }
   };
-  // ASYNC: the copies of tile `id`'s states (the tile and its halo) into dst,
-  // one 4-byte copy per variable and cell, in this thread's current group
-  auto issue_load = [&](R* dst, int id) {
-    const int bb = id / tpb;
-    int tt = id - bb * tpb;
-    const int tpi = tt % ntp; tt /= ntp;
-    const int tli = tt % ntl; tt /= ntl;
-    const int p0i = ng + tpi * LP, l0i = ng + tli * LW, t0i = g.ndims == 3 ? ng + tt : 0;
-    const R* qbi = a.q + (long long)bb * g.qbs;
-    const int sy = g.IM, sz = g.IM * g.JM;
-    const int sp = DIR == 0 ? 1 : (DIR == 1 ? sy : sz), sl = DIR == 0 ? sy : 1, st = DIR == 2 ? sy : sz;
-    for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
-      int pp, ll; decode(t, NPQ, pp, ll);
-      const long long c = (long long)(p0i - RR - 1 + pp) * sp + (long long)(l0i + ll) * sl + (long long)t0i * st;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) cp_async4(dst + sidx(v, pp, ll, NPQ), qbi + c + v * g.qvs);
-    }
-  };
-  (void)issue_load;
-
-  int id = ASYNC ? (int)blockIdx.x : 0;
-  if constexpr (ASYNC) {
-    if (id < a.ntiles) issue_load(Qbuf0, id);
-    cp_async_commit();
-  }
-  for (int it = 0;; ++it) {
-  if constexpr (ASYNC) {
-    if (id >= a.ntiles) break;
-  }
-  R* Qs = (ASYNC && (it & 1)) ? Qbuf1 : Qbuf0;
-  R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
-  int bx = blockIdx.x, by = blockIdx.y;
-  if constexpr (ASYNC) {
-    by = id / tpb;
-    bx = id - by * tpb;
-  }
-  if (a.fcount) {
-    __shared__ int ticket;
-    if (threadIdx.x == 0) ticket = atomicAdd(a.fcount + a.nfcount, 1);
-    __syncthreads();
-    bx = ticket % gridDim.x;
-    by = ticket / gridDim.x;
-  }
-  const int b = a.blist ? a.blist[by] : by;
-  int tile = bx;
-  const int tp = tile % ntp; tile /= ntp;
-  const int tl = tile % ntl; tile /= ntl;
-  const int th = tile;
-  const int p0 = ng + tp * LP, l0 = ng + tl * LW;
-  const int t0 = (g.ndims == 3) ? ng + th : 0;
-  const long long sX = 1, sY = g.IM, sZ = (long long)g.IM * g.JM;
-  const long long sP = DIR == 0 ? sX : (DIR == 1 ? sY : sZ);
-  const long long sL = DIR == 0 ? sY : sX;
-  const long long sT = DIR == 2 ? sY : sZ;
-  const long long iP = DIR == 0 ? 1 : (DIR == 1 ? nc : (long long)nc * nc);
-  const long long iL = DIR == 0 ? nc : 1;
-  const long long iT = DIR == 2 ? nc : (long long)nc * nc;
-  const R* qb = a.q + (long long)b * g.qbs;
 
   // ---- the last direction's stage operands (U^n and the stage state of the
   // tile's cells) are requested into L2 now, so that the combination after
@@ -545,15 +485,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- load the tile and its halo --------------------------------------------
   // (the generic variant's three-cell halo is clamped to the block: methods
   // with shorter stencils run with fewer ghost layers and never read it)
-  if constexpr (ASYNC) {
-    // the next tile's copies go into the other buffer (free since the
-    // barrier that ended the previous tile); this tile's are waited for
-    const int nxt = id + (int)gridDim.x;
-    if (nxt < a.ntiles) issue_load(Qs == Qbuf0 ? Qbuf1 : Qbuf0, nxt);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-  } else {
   const int PM = DIR == 0 ? g.IM : (DIR == 1 ? g.JM : g.KM);
   for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
     int pp, ll; decode(t, NPQ, pp, ll);
@@ -570,7 +501,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   }
   (void)PM;
   __syncthreads();
-  }
 
   // ---- reconstruct both faces of cells p0-1 .. p0+LP ---------------------------
   const bool mlp = REC == REC_GEN && a.m.mlp;
@@ -910,6 +840,8 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- flux difference, stage combination -------------------------------------
   const double* bi = a.binv + 3 * b;
   const R dsi = R(bi[DIR]);
+  const bool final_stage = a.last && a.st.final_stage;
+  double vmax = 0.0;
   for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
     int pp, ll;
     if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
@@ -1026,12 +958,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     }
     if (final_stage) vmax = fmax(vmax, cell_speed<EQ>(qs, a.m.gamma, a.m.csnd));
   }
-  if constexpr (!ASYNC) break;
-  // every thread is done with this tile's buffers before they are refilled
-  __syncthreads();
-  id += gridDim.x;
-  }
-  if constexpr (ASYNC) cp_async_wait<0>();
   if (final_stage) block_max_atomic(vmax, &a.sc->ms_bits);
 }
 

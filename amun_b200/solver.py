@@ -296,12 +296,6 @@ class Simulation:
         writes the same-level ghost cells; False: a separate ghost fill."""
         N.check(self.L.amun_gpu_set_ghost_in_sweep(int(bool(on))))
 
-    def set_sweep_pipeline(self, on: bool = True) -> None:
-        """True (the default): the FP32 TVD / WENO-Z sweeps of one-level
-        meshes run persistent with the next tile's copies in flight; False:
-        one CTA per tile with synchronous loads (same results)."""
-        N.check(self.L.amun_gpu_set_sweep_pipeline(int(bool(on))))
-
     def _states(self, a: np.ndarray) -> np.ndarray:
         a = np.ascontiguousarray(a, dtype=np.float64)
         if a.ndim == 0 or a.shape[-1] != self.nv:

@@ -394,14 +394,6 @@ int amun_gpu_set_level_launches(int per_level);
  * level jumps and the fused stage kernel always fill separately.
  * Invalidates captured graphs.  No reference counterpart (a launch choice). */
 int amun_gpu_set_ghost_in_sweep(int on);
-
-/* FP32-bulk TVD and WENO-Z sweeps of HD and MHD on a mesh of one level:
- * on == 1 (the default) launches them persistent, each CTA copying the next
- * tile's states into shared memory (cp.async) while it computes the current
- * tile; on == 0 launches one CTA per tile with synchronous loads.  Same
- * arithmetic, same results.  Invalidates captured graphs.  No reference
- * counterpart (a launch choice). */
-int amun_gpu_set_sweep_pipeline(int on);
 /* Runs one bounded device wait on a count that nothing raises (the wait of
  * the flux correction above, given `cycles` clock cycles) and reports in
  * *gave_up whether it gave up and recorded a stall, as it must; the stall
