@@ -48,7 +48,9 @@ NCELL = 128 ** 3
 # U^{n+1} stay FP64, intermediate stage states are FP32: 48 x 9 = 432 B.
 B_ZU = {"fp64": 8 * NV * 8, "fp32": 48 * NV}
 METRIC = "zone-updates/s FP32 vs FP64 at stated L1 error vs FP64; adjoint/forward time"
-LAUNCHES_PER_STEP = 2 + 3 * (3 + 1)  # dt + end-of-step + 3 stages x (3 sweeps + ghost fill)
+# dt + end-of-step + 3 stages x 3 sweeps (the last sweep of a stage writes the
+# same-level ghost cells, so no ghost-fill launch follows)
+LAUNCHES_PER_STEP = 2 + 3 * 3
 
 
 def dist_env():
@@ -745,7 +747,7 @@ def main():
         traffic = 3 * (123.5e6 + 205.7e6 + 527.9e6) if WORKLOAD.get("ncells") == 128 else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind,
-                    "kernel": "stage sweeps x/y/z + ghost fill (whole SSPRK step, 432 B/zone-update)",
+                    "kernel": "stage sweeps x/y/z, ghost cells written by the last (whole SSPRK step, 432 B/zone-update)",
                     "traffic_source": "profiles/sweep_mhd3d_128_full.md (ncu, same build, same workload)",
                     "traffic": traffic, "traffic_unit": "bytes per step and GPU",
                     "traffic_per_zone_update": traffic / NCELL if traffic else None,
