@@ -464,25 +464,20 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     else { pp = t / LW; ll = t - pp * LW; }
   };
 
-  // ---- the operands the flux difference and the stage combination read
-  // from global memory (du after the first direction; U^n and the stage
-  // state in the last) are requested into L2 now, one run along x of the
-  // tile (a 128-byte line or half of one) per request, so that they are
-  // there after the Riemann problems
-  {
-    const bool pu0 = a.last && (a.st.a_src == 0 || (a.st.form != 0 && a.st.b_src == 0));
-    const bool pu1 = a.last && (a.st.a_src == 1 || (a.st.form != 0 && a.st.b_src == 1));
-    const bool pdu = !a.first;
-    if (pu0 || pu1 || pdu) {
-      const int nrow = DIR == 0 ? LW : LP;  // runs along x: LP cells (x sweep) or LW lanes
-      for (int t = threadIdx.x; t < nrow * NV; t += blockDim.x) {
-        const int v = t / nrow, r = t - v * nrow;
-        const int pp = DIR == 0 ? 0 : r, ll = DIR == 0 ? r : 0;
-        const long long o = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP + (long long)(l0 - ng + ll) * iL +
-                            (long long)(g.ndims == 3 ? th : 0) * iT + (long long)v * g.uvs;
-        if (pu0) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u0 + o));
-        if (pu1) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u1 + o));
-        if (pdu) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.du + o));
+  // ---- the last direction's stage operands (U^n and the stage state of the
+  // tile's cells) are requested into L2 now, so that the combination after
+  // the Riemann problems finds them there
+  if (a.last) {
+    for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
+      int pp, ll;
+      if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
+      const long long ci = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP + (long long)(l0 - ng + ll) * iL +
+                           (long long)(g.ndims == 3 ? th : 0) * iT;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const long long o = ci + v * g.uvs;
+        if (a.st.a_src == 0 || (a.st.form != 0 && a.st.b_src == 0)) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u0 + o));
+        if (a.st.a_src == 1 || (a.st.form != 0 && a.st.b_src == 1)) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.u1 + o));
       }
     }
   }
