@@ -64,9 +64,9 @@ cudaError_t sweep_eq_fixed(int rec, int rs, int dir, const SweepArgs<R, U1T>& a,
                            size_t smem, cudaStream_t s);
 
 #ifdef AMUN_SWEEP_IMPL
-template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP = 0, int TLW = 0>
-static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
-  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW>;
+template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP, int TLW, int LASTK>
+static cudaError_t go_sweep_k(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
+  auto k = sweep_kernel<EQ, REC, RS, DIR, R, U1T, TLP, TLW, LASTK>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -75,6 +75,26 @@ static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, 
   }
   k<<<grid, threads, smem, s>>>(a);
   return cudaGetLastError();
+}
+
+// the fixed-tile sweeps are compiled per role: x never ends a stage, z always
+// does, y ends it in 2D only; the run-time-tile sweeps read a.last
+template <typename R, typename U1T, int EQ, int REC, int RS, int DIR, int TLP = 0, int TLW = 0>
+static cudaError_t go_sweep(const SweepArgs<R, U1T>& a, dim3 grid, int threads, size_t smem, cudaStream_t s) {
+  if constexpr (TLP > 0) {
+    if constexpr (DIR == 0) {
+      if (a.last) return cudaErrorInvalidValue;
+      return go_sweep_k<R, U1T, EQ, REC, RS, DIR, TLP, TLW, 0>(a, grid, threads, smem, s);
+    } else if constexpr (DIR == 2) {
+      if (!a.last) return cudaErrorInvalidValue;
+      return go_sweep_k<R, U1T, EQ, REC, RS, DIR, TLP, TLW, 1>(a, grid, threads, smem, s);
+    } else {
+      if (a.last) return go_sweep_k<R, U1T, EQ, REC, RS, DIR, TLP, TLW, 1>(a, grid, threads, smem, s);
+      return go_sweep_k<R, U1T, EQ, REC, RS, DIR, TLP, TLW, 0>(a, grid, threads, smem, s);
+    }
+  } else {
+    return go_sweep_k<R, U1T, EQ, REC, RS, DIR, TLP, TLW, -1>(a, grid, threads, smem, s);
+  }
 }
 
 template <typename R, typename U1T, int EQ, int REC, int RS, int TLP = 0, int TLW = 0>

@@ -369,8 +369,11 @@ __device__ __forceinline__ void mlp_faces(const R* qb, const Geo& g, bool four, 
 
 // TLP x TLW > 0: the tile shape fixed at compile time (a.LP, a.LW must equal
 // it), so every shared-memory index and task split folds to constants;
-// 0 x 0: the shape is read from the arguments
-template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0>
+// 0 x 0: the shape is read from the arguments.
+// LASTK 0 / 1: the sweep is known at compile time not to be / to be the
+// stage's last direction (a.last must agree), so the other directions carry
+// no stage epilogue and keep its registers; -1: a.last decides at run time
+template <int EQ, int REC, int RS, int DIR, typename R, typename U1T, int TLP = 0, int TLW = 0, int LASTK = -1>
 #ifndef AMUN_SWEEP_MIN_BLOCKS
 #define AMUN_SWEEP_MIN_BLOCKS 1
 #endif
@@ -384,6 +387,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   const Geo& g = a.g;
   const int LP = TLP ? TLP : a.LP, LW = TLW ? TLW : a.LW;
   const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
+  const bool last = LASTK < 0 ? a.last != 0 : LASTK == 1;
   // FP32 WENO-Z and TVD: the staged states, face states and fluxes of the
   // variables 2m and 2m+1 sit side by side, so one 64-bit shared-memory
   // access moves both operands of a packed f32x2 instruction (an odd last
@@ -467,7 +471,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- the last direction's stage operands (U^n and the stage state of the
   // tile's cells) are requested into L2 now, so that the combination after
   // the Riemann problems finds them there
-  if (a.last) {
+  if (last) {
     for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
       int pp, ll;
       if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
@@ -840,7 +844,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- flux difference, stage combination -------------------------------------
   const double* bi = a.binv + 3 * b;
   const R dsi = R(bi[DIR]);
-  const bool final_stage = a.last && a.st.final_stage;
+  const bool final_stage = last && a.st.final_stage;
   double vmax = 0.0;
   for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
     int pp, ll;
@@ -865,7 +869,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
       if (a.first) dloc[v] = -(dsi * d);
       else dloc[v] = a.du[ci + v * g.uvs] - dsi * d;
     }
-    if (!a.last) {
+    if (!last) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) a.du[ci + v * g.uvs] = dloc[v];
       continue;
