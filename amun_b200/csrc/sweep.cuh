@@ -388,6 +388,8 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   const int LP = TLP ? TLP : a.LP, LW = TLW ? TLW : a.LW;
   const int NPQ = LP + 2 * RR + 2, NPF = LP + 2, NPI = LP + 1;
   const bool last = LASTK < 0 ? a.last != 0 : LASTK == 1;
+  // the fixed-tile roles also fix the first direction: x starts every stage
+  const bool first = LASTK < 0 ? a.first != 0 : DIR == 0;
   // FP32 WENO-Z and TVD: the staged states, face states and fluxes of the
   // variables 2m and 2m+1 sit side by side, so one 64-bit shared-memory
   // access moves both operands of a packed f32x2 instruction (an odd last
@@ -866,7 +868,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       R d = dfl[v];
-      if (a.first) dloc[v] = -(dsi * d);
+      if (first) dloc[v] = -(dsi * d);
       else dloc[v] = a.du[ci + v * g.uvs] - dsi * d;
     }
     if (!last) {
