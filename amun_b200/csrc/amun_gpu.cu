@@ -2490,6 +2490,7 @@ int reverse_step(int n, int slot, const AdjGeo& ag) {
 template <typename R>
 int forward_recorded(int nsteps, double dtnext) {
   const size_t qb = qpool_bytes();
+  void* const pool[2] = {C.q[0], C.q[1]};
   for (int n = 0; n < nsteps; ++n) {
     if (n % A.interval == 0) {
       int r = save_state(n / A.interval);
@@ -2501,8 +2502,35 @@ int forward_recorded(int nsteps, double dtnext) {
     if (!A.keep_all) {
       int r = launch_evolve<R>();
       if (r) return r;
+    } else if (!use_stage()) {
+      // every stage input stays on the device: the adjoint recomputes
+      // nothing.  Each stage writes its output primitives straight into the
+      // slot of the next stage input (the last one into a pool buffer), so
+      // only the first input is copied
+      Schedule S = schedule();
+      const size_t ns = S.stages.size();
+      if (S.copy_first) {
+        cudaError_t e = Launch<R, R>::copy_u0_u1(C.u0, (R*)C.u1, (long long)C.nblocks * C.g.ubs, C.stream);
+        if (e != cudaSuccess) return cuda_fail(e, "copy u0->u1");
+      }
+      if (n == 0) {
+        CK(cudaMemcpyAsync(A.seg_q, C.q[C.cur], qb, cudaMemcpyDeviceToDevice, C.stream));
+        C.q[C.cur] = A.seg_q;
+      }
+      for (size_t st = 0; st < ns; ++st) {
+        const size_t next = (size_t)n * ns + st + 1;  // slot of the next stage input
+        const bool to_slot = next < (size_t)nsteps * ns;
+        // the last output goes to the pool buffer of its parity, so that
+        // both pool buffers are back in place afterwards (captured step
+        // graphs hold their addresses)
+        C.q[1 - C.cur] = to_slot ? (void*)((char*)A.seg_q + next * qb) : pool[1 - C.cur];
+        int r = launch_stage<R>(S.stages[st]);
+        if (r) { C.q[0] = pool[0]; C.q[1] = pool[1]; return r; }
+      }
+      if (n == nsteps - 1) C.q[1 - C.cur] = pool[1 - C.cur];
     } else {
-      // every stage input stays on the device: the adjoint recomputes nothing
+      // the fused stage kernel's tensor maps are bound to the pool buffers:
+      // copy each stage input
       Schedule S = schedule();
       if (S.copy_first) {
         cudaError_t e = Launch<R, R>::copy_u0_u1(C.u0, (R*)C.u1, (long long)C.nblocks * C.g.ubs, C.stream);

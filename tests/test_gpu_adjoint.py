@@ -178,6 +178,35 @@ def test_adjoint_without_recomputation_equals_checkpointed(prec):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_recording_keeps_the_state_buffers(prec):
+    """Recording with every stage input kept writes each stage's output into
+    the slot of the next stage input; afterwards the state is in the
+    library's own buffers again: steps replayed from graphs captured before
+    the recording continue exactly as a run without it."""
+    from amun_b200.solver import Simulation
+    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    mesh = UniformMesh(geometry(p))
+    q0 = problems.smooth_mhd(mesh, seed=6)
+    out = []
+    for record in (True, False):
+        sim = Simulation(p, prec)
+        try:
+            sim.set_primitive(q0)
+            sim.run(2, 1.0e30, graph=True)
+            if record:
+                sim.forward_checkpointed(7, 1.0e30, 0)
+            else:
+                for _ in range(7):
+                    sim.advance(1.0e30)
+            sim.run(3, 1.0e30, graph=True)
+            out.append(sim.download_blocks())
+        finally:
+            sim.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_evolve_on_cuda_tensors_matches_host_path():
     """torch.autograd through Evolve with CUDA tensors (the library reads and
     writes device memory, no host copies) gives the forward state and the
