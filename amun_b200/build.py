@@ -49,6 +49,7 @@ UNITS = {
     "gp_weights.cpp": [],
     "unit_fp64.cu": FP64,
     "adjoint.cu": FP64,
+    "adjoint_fp32.cu": FP32,
     "kernels_fp64.cu": FP64,
     "regrid.cu": FP64,
     "integrals.cu": FP64,

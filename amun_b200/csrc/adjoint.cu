@@ -331,6 +331,11 @@ __global__ void to_aos_kernel(const double* __restrict__ soa, double* __restrict
 
 }  // namespace
 
+// The FP64 build of this file holds the launchers of both precisions' FP64
+// arrays and the FP64 instantiations; adjoint_fp32.cu builds it again with the
+// FP32-bulk compiler flags (contraction, approximate division) for the
+// instantiations on FP32 stage states.
+#ifndef AMUN_ADJ_FP32_UNIT
 cudaError_t adj_combination(const AdjGeo& a, const StageDesc& st, const DevScalars* rec, double decay, double* lamU0,
                             double* lamU1, double* lamdu, cudaStream_t s) {
   const long long n = (long long)a.nblocks * a.g.ubs;
@@ -344,6 +349,8 @@ cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStr
   fold_kernel<<<blocks_for(n), kThreads, 0, s>>>(lamU0, lamU1, n);
   return cudaGetLastError();
 }
+
+#endif  // AMUN_ADJ_FP32_UNIT
 
 template <typename R>
 cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* G, double* P, const double* binv,
@@ -377,6 +384,7 @@ cudaError_t adj_prim2cons(const AdjGeo& a, const R* Q, const double* lamU, doubl
   return cudaGetLastError();
 }
 
+#ifndef AMUN_ADJ_FP32_UNIT
 cudaError_t adj_from_host_layout(const AdjGeo& a, const double* aos, double* soa, cudaStream_t s) {
   dim3 grid(blocks_for(a.g.uvs), a.nblocks);
   from_aos_kernel<<<grid, kThreads, 0, s>>>(aos, soa, a.g, a.nv);
@@ -391,14 +399,16 @@ cudaError_t adj_to_host_layout(const AdjGeo& a, const double* soa, double* aos, 
 
 template cudaError_t adj_faces<double>(const AdjGeo&, const double*, const double*, double*, double*, const double*,
                                        const MethodConst&, const DevScalars*, cudaStream_t);
-template cudaError_t adj_faces<float>(const AdjGeo&, const float*, const double*, double*, double*, const double*,
-                                      const MethodConst&, const DevScalars*, cudaStream_t);
 template cudaError_t adj_cells<double>(const AdjGeo&, const double*, const double*, const int*, double, double*,
                                        cudaStream_t);
-template cudaError_t adj_cells<float>(const AdjGeo&, const float*, const double*, const int*, double, double*,
-                                      cudaStream_t);
 template cudaError_t adj_prim2cons<double>(const AdjGeo&, const double*, const double*, double, double*,
                                            cudaStream_t);
+#else
+template cudaError_t adj_faces<float>(const AdjGeo&, const float*, const double*, double*, double*, const double*,
+                                      const MethodConst&, const DevScalars*, cudaStream_t);
+template cudaError_t adj_cells<float>(const AdjGeo&, const float*, const double*, const int*, double, double*,
+                                      cudaStream_t);
 template cudaError_t adj_prim2cons<float>(const AdjGeo&, const float*, const double*, double, double*, cudaStream_t);
+#endif  // AMUN_ADJ_FP32_UNIT
 
 }  // namespace amun
