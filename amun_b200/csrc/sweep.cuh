@@ -491,19 +491,40 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   // ---- load the tile and its halo --------------------------------------------
   // (the generic variant's three-cell halo is clamped to the block: methods
   // with shorter stencils run with fewer ghost layers and never read it)
+  // The staged cells number at most twice the threads ((LP + 2 RR + 2) LW
+  // against (LP + 2) LW, LP >= 4): a thread loads its first and second cell
+  // before it stores either, so the threads with two cells wait for one
+  // round trip to memory, not two, before the barrier.
   const int PM = DIR == 0 ? g.IM : (DIR == 1 ? g.JM : g.KM);
-  for (int t = threadIdx.x; t < NPQ * LW; t += blockDim.x) {
-    int pp, ll; decode(t, NPQ, pp, ll);
+  auto cell_of = [&](int t, int& pp, int& ll) -> long long {
+    decode(t, NPQ, pp, ll);
     int pi = p0 - RR - 1 + pp;
     if constexpr (REC == REC_GEN) pi = pi < 0 ? 0 : (pi >= PM ? PM - 1 : pi);
-    long long c = (long long)pi * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
-    R qc[NV];
+    return (long long)pi * sP + (long long)(l0 + ll) * sL + (long long)t0 * sT;
+  };
+  for (int t = threadIdx.x; t < NPQ * LW; t += 2 * blockDim.x) {
+    const int t2 = t + blockDim.x;
+    const bool two = t2 < NPQ * LW;
+    int pp, ll, pp2 = 0, ll2 = 0;
+    const long long c = cell_of(t, pp, ll);
+    const long long c2 = two ? cell_of(t2, pp2, ll2) : c;
+    R qc[NV], qd[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = ld_ro(qb + c + v * g.qvs);
+    if (two) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qd[v] = ld_ro(qb + c2 + v * g.qvs);
+    }
     if constexpr (V::SR) {
       if (four) to_four_velocity(qc);
     }
     store_all(Qs, pp, ll, NPQ, qc);
+    if (two) {
+      if constexpr (V::SR) {
+        if (four) to_four_velocity(qd);
+      }
+      store_all(Qs, pp2, ll2, NPQ, qd);
+    }
   }
   (void)PM;
   __syncthreads();
