@@ -73,9 +73,6 @@ static cudaError_t go_sweep_k(const SweepArgs<R, U1T>& a, dim3 grid, int threads
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  // the FP32 fixed-tile last sweep also stages U^n of its cells (doubles)
-  if constexpr (LASTK == 1 && TLP > 0 && std::is_same<R, float>::value)
-    smem += (size_t)TLP * TLW * Var<EQ>::NV * sizeof(double);
   k<<<grid, threads, smem, s>>>(a);
   return cudaGetLastError();
 }

@@ -135,15 +135,6 @@ template <typename R, typename U1T> struct SweepArgs {
 
 template <typename T> __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
 
-// asynchronous 8-byte copy global -> shared; complete for the issuing thread
-// after cp_async_wait_all
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // a load through L2 that the compiler keeps after the preceding barrier
 // (the ld.global.cg intrinsic is a plain asm the compiler may hoist above the
 // wait that makes the data valid)
@@ -409,12 +400,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
   R* FLs = Qs + (size_t)NVP * NPQ * LW;
   R* FRs = FLs + (size_t)NVP * NPF * LW;
   R* Fs = Qs;  // fluxes overwrite the staged states after reconstruction
-  // FP32 fixed-tile last sweep: U^n of the tile's cells is copied into shared
-  // memory (cp.async) while the faces and fluxes are computed, each thread
-  // copying the cells it combines, so the combination reads it from there
-  constexpr bool U0S = LASTK == 1 && TLP > 0 && std::is_same<R, float>::value;
-  double* U0s = reinterpret_cast<double*>(FRs + (size_t)NVP * NPF * LW);
-  (void)U0s;
 
   const int nc = g.nc, ng = g.ng;
   int bx = blockIdx.x, by = blockIdx.y;
@@ -542,18 +527,6 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
     }
   }
   (void)PM;
-  if constexpr (U0S) {
-    if (a.st.a_src == 0) {
-      for (int t = threadIdx.x; t < LP * LW; t += blockDim.x) {
-        int pp, ll;
-        if (DIR == 0) { ll = t / LP; pp = t - ll * LP; } else { pp = t / LW; ll = t - pp * LW; }
-        const long long ci = (long long)b * g.ubs + (long long)(p0 - ng + pp) * iP +
-                             (long long)(l0 - ng + ll) * iL + (long long)(g.ndims == 3 ? th : 0) * iT;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) cp_async8(U0s + v * LP * LW + t, a.u0 + ci + v * g.uvs);
-      }
-    }
-  }
   __syncthreads();
 
   // ---- reconstruct both faces of cells p0-1 .. p0+LP ---------------------------
@@ -940,12 +913,7 @@ __global__ void __launch_bounds__(288, AMUN_SWEEP_MIN_BLOCKS) sweep_kernel(const
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const long long o = ci + v * g.uvs;
-      if constexpr (U0S) {
-        if (v == 0 && a.st.a_src == 0) cp_async_wait_all();
-        Av[v] = a.st.a_src == 0 ? U0s[v * LP * LW + t] : (double)a.u1[o];
-      } else {
-        Av[v] = a.st.a_src == 0 ? a.u0[o] : (double)a.u1[o];
-      }
+      Av[v] = a.st.a_src == 0 ? a.u0[o] : (double)a.u1[o];
       Bv[v] = a.st.form == 0 ? 0.0 : (a.st.b_src == 0 ? a.u0[o] : (double)a.u1[o]);
     }
 #pragma unroll
