@@ -744,7 +744,7 @@ def main():
         # --precision fp32 --n 128 --steps 1`: the x, y, z sweeps of the middle
         # stage, 123.5, 205.7 and 527.9 MB) times three stages; the ghost
         # fills add under 1 %.  Only this workload was captured.
-        traffic = 3 * (118.6e6 + 197.7e6 + 516.0e6) if WORKLOAD.get("ncells") == 128 else None
+        traffic = 3 * (118.6e6 + 197.1e6 + 516.1e6) if WORKLOAD.get("ncells") == 128 else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": peak_kind,
                     "kernel": "stage sweeps x/y/z, ghost cells written by the last (whole SSPRK step, 432 B/zone-update)",
@@ -754,10 +754,10 @@ def main():
                     "fp64": {"achieved": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9,
                              "frac": (r64["zu_per_s"] / ws) * B_ZU["fp64"] / 1e9 / peak}}
         # the sweeps are bound by instruction issue: warp instructions per
-        # zone-update (ncu, profiles/sweep_mhd3d_128_full.md: 39.7 + 37.6 +
-        # 57.1 warp instructions per cell and stage, three stages) against 4
+        # zone-update (ncu, profiles/sweep_mhd3d_128_full.md: 40.3 + 38.2 +
+        # 57.7 warp instructions per cell and stage, three stages) against 4
         # issues per SM and cycle at the sampled SM clock
-        wi = 3 * (39.7 + 37.6 + 57.1)
+        wi = 3 * (40.3 + 38.2 + 57.7)
         mhz = (r32["clocks"] or {}).get("sm_mhz") or 1965.0
         issue_peak = 148 * 4 * mhz * 1e6
         roofline["issue"] = {"warp_instructions_per_zone_update": wi, "peak_warp_instructions_per_s": issue_peak,
