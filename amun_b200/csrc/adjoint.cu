@@ -206,12 +206,12 @@ __global__ void weno_rev_kernel(const R* __restrict__ Q, const double* __restric
   }
 }
 
-// acc += the stencil partials of variable v aimed at padded cell (i,j,k) of
-// block pb, over the directions whose line through the cell is an interior
-// line (the only lines the WENO kernel covers) and sources s = a-2..a+2 in
-// ng-1..ng+nc.
-__device__ __forceinline__ void gather_at_one(const double* __restrict__ P, const Geo& g, long long qd, int pb, int i,
-                                              int j, int k, int v, double& acc) {
+// lq += the stencil partials aimed at padded cell (i,j,k) of block pb, over
+// the directions whose line through the cell is an interior line (the only
+// lines the WENO kernel covers) and sources s = a-2..a+2 in ng-1..ng+nc.
+template <int NV>
+__device__ __forceinline__ void gather_at(const double* __restrict__ P, const Geo& g, long long qd, int pb, int i,
+                                          int j, int k, double* lq) {
   const int nc = g.nc, ng = g.ng;
   const long long cell = ((long long)k * g.JM + j) * g.IM + i;
   const bool ti = i >= ng && i < ng + nc, tj = j >= ng && j < ng + nc;
@@ -221,44 +221,38 @@ __device__ __forceinline__ void gather_at_one(const double* __restrict__ P, cons
     if (!line) continue;
     const int a = d == 0 ? i : (d == 1 ? j : k);
     const long long sD = d == 0 ? 1LL : (d == 1 ? (long long)g.IM : (long long)g.IM * g.JM);
-    const double* Pd = P + (long long)d * 5 * qd + (long long)pb * 5 * g.qbs + (long long)v * g.qvs;
+    const double* Pd = P + (long long)d * 5 * qd + (long long)pb * 5 * g.qbs;
 #pragma unroll
     for (int mm = 0; mm < 5; ++mm) {
       const int s = a + 2 - mm;
       if (s < ng - 1 || s > ng + nc) continue;
-      acc += Pd[mm * g.qbs + cell + (long long)(s - a) * sD];
+      const double* ps = Pd + mm * g.qbs + cell + (long long)(s - a) * sD;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) lq[v] += ps[v * g.qvs];
     }
   }
 }
 
 // Per interior cell: lam of its primitive state = the partials aimed at it
 // and at its ghost copies (image at c + o nc in block inv[o], for each of the
-// 26 directions o); then lamIn += cons2prim^T lam.  A CTA takes kCellsPerCta
-// cells: one thread per cell and variable gathers (the memory-bound part,
-// nv times the parallelism of one thread per cell), then one thread per cell
-// applies cons2prim^T.
-constexpr int kCellsPerCta = 32;
+// 26 directions o); then lamIn += cons2prim^T lam.
 template <int EQ, typename R>
 __global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ P, const int* __restrict__ inv,
                             double gammam1, double* __restrict__ lamIn, Geo g) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
-  __shared__ double lqs[NV][kCellsPerCta];
   const int nc = g.nc, ng = g.ng, b = blockIdx.y;
   const long long qd = g.qbs * gridDim.y;
   const int nz = g.ndims == 3 ? 1 : 0;
-  const int v = threadIdx.x / kCellsPerCta, cl = threadIdx.x - v * kCellsPerCta;
-  const long long t = (long long)blockIdx.x * kCellsPerCta + cl;
-  auto cell_ijk = [&](long long tt, int& i, int& j, int& k) {
-    i = ng + (int)(tt % nc);
-    j = ng + (int)((tt / nc) % nc);
-    k = g.ndims == 3 ? ng + (int)(tt / ((long long)nc * nc)) : 0;
-  };
-  if (v < NV && t < g.uvs) {
-    int i, j, k;
-    cell_ijk(t, i, j, k);
-    double acc = 0.0;
-    gather_at_one(P, g, qd, b, i, j, k, v, acc);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < g.uvs; t += (long long)gridDim.x * blockDim.x) {
+    const int ii = (int)(t % nc);
+    const int jj = (int)((t / nc) % nc);
+    const int kk = g.ndims == 3 ? (int)(t / ((long long)nc * nc)) : 0;
+    const int i = ng + ii, j = ng + jj, k = g.ndims == 3 ? ng + kk : 0;
+    double lq[NV], q[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) lq[v] = 0.0;
+    gather_at<NV>(P, g, qd, b, i, j, k, lq);
     for (int oz = -nz; oz <= nz; ++oz)
       for (int oy = -1; oy <= 1; ++oy)
         for (int ox = -1; ox <= 1; ++ox) {
@@ -267,25 +261,17 @@ __global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ 
           if (gi < 0 || gi >= g.IM || gj < 0 || gj >= g.JM || gk < 0 || gk >= g.KM) continue;
           const int src = inv[27 * b + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
           if (src < 0) continue;
-          gather_at_one(P, g, qd, src, gi, gj, gk, v, acc);
+          gather_at<NV>(P, g, qd, src, gi, gj, gk, lq);
         }
-    lqs[v][cl] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x < kCellsPerCta && t < g.uvs) {
-    int i, j, k;
-    cell_ijk(t, i, j, k);
     const long long cell = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
-    double q[NV], lq[NV], lu[NV];
 #pragma unroll
-    for (int w = 0; w < NV; ++w) {
-      q[w] = (double)Q[cell + w * g.qvs];
-      lq[w] = lqs[w][cl];
-      lu[w] = 0.0;
-    }
+    for (int v = 0; v < NV; ++v) q[v] = (double)Q[cell + v * g.qvs];
+    double lu[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) lu[v] = 0.0;
     cons2prim_rev<EQ, double>(q, lq, lu, gammam1);
 #pragma unroll
-    for (int w = 0; w < NV; ++w) lamIn[(long long)b * g.ubs + w * g.uvs + t] += lu[w];
+    for (int v = 0; v < NV; ++v) lamIn[(long long)b * g.ubs + v * g.uvs + t] += lu[v];
   }
 }
 
@@ -383,9 +369,9 @@ cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* 
 template <typename R>
 cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* P, const int* inv, double gammam1, double* lamIn,
                       cudaStream_t s) {
-  dim3 grid((unsigned)((a.g.uvs + kCellsPerCta - 1) / kCellsPerCta), a.nblocks);
-  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, Var<EQ_HD>::NV * kCellsPerCta, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
-  else cell_kernel<EQ_MHD, R><<<grid, Var<EQ_MHD>::NV * kCellsPerCta, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
+  dim3 grid(blocks_for(a.g.uvs), a.nblocks);
+  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
+  else cell_kernel<EQ_MHD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
   return cudaGetLastError();
 }
 
