@@ -12,7 +12,6 @@
 // Conserved variables use the same slots (momenta, energy in the pres slot).
 #pragma once
 #include <cstdint>
-#include <type_traits>
 
 namespace amun {
 
@@ -537,71 +536,6 @@ __device__ __forceinline__ void clip_cell(R fm1, R f0, R fp1, int clim, R eps, R
   }
 }
 
-// FP32 adiabatic HD / MHD: prim2cons and fluxspeed (above) of a left and a
-// right state at once, every operation on a packed f32x2 pair (x: left, y:
-// right); the fast speed takes sqrt(fc) as 0 where fc <= 0, which is the
-// reference's other branch.
-template <int EQ>
-__device__ __forceinline__ void p2c_flux_lr(const float* ql, const float* qr, float* ul, float* ur, float* fl,
-                                            float* fr, float& clm, float& clp, float& crm, float& crp,
-                                            const Phys<float>& P) {
-  using V = Var<EQ>;
-  static_assert(!V::SR && !V::ISO, "adiabatic HD and MHD");
-  auto pk = [&](int v) { return make_float2(ql[v], qr[v]); };
-  auto put = [&](float* a, float* b, int v, float2 x) { a[v] = x.x; b[v] = x.y; };
-  const float2 half = lane_bcast<float2>(0.5f);
-  const float2 dn = pk(V::DN), vx = pk(V::VX), vy = pk(V::VY), vz = pk(V::VZ), pr = pk(V::PR);
-  const float2 mx = lane_mul(dn, vx), my = lane_mul(dn, vy), mz = lane_mul(dn, vz);
-  const float2 ei = lane_mul(lane_bcast<float2>(P.gammam1i), pr);
-  const float2 ek = lane_mul(half, lane_fma(mx, vx, lane_fma(my, vy, lane_mul(mz, vz))));
-  put(ul, ur, V::DN, dn);
-  put(ul, ur, V::VX, mx);
-  put(ul, ur, V::VY, my);
-  put(ul, ur, V::VZ, mz);
-  float2 c2;
-  if constexpr (!V::MHD) {
-    const float2 en = lane_add(ei, ek);
-    put(ul, ur, V::EN, en);
-    put(fl, fr, V::DN, mx);
-    put(fl, fr, V::VX, lane_fma(vx, mx, pr));
-    put(fl, fr, V::VY, lane_mul(vx, my));
-    put(fl, fr, V::VZ, lane_mul(vx, mz));
-    put(fl, fr, V::EN, lane_mul(vx, lane_add(en, pr)));
-    c2 = lane_mul(lane_mul(lane_bcast<float2>(P.gamma), pr), lane_rcp(dn));
-  } else {
-    const float2 bx = pk(V::BX), by = pk(V::BY), bz = pk(V::BZ), bp = pk(V::BP);
-    put(ul, ur, V::BX, bx);
-    put(ul, ur, V::BY, by);
-    put(ul, ur, V::BZ, bz);
-    put(ul, ur, V::BP, bp);
-    const float2 bx2 = lane_mul(bx, bx);
-    const float2 bb = lane_fma(bz, bz, lane_fma(by, by, bx2));
-    const float2 en = lane_fma(half, bb, lane_add(ei, ek));
-    put(ul, ur, V::EN, en);
-    const float2 vb = lane_fma(vz, bz, lane_fma(vy, by, lane_mul(vx, bx)));
-    const float2 pt = lane_fma(half, bb, pr);
-    put(fl, fr, V::DN, mx);
-    put(fl, fr, V::VX, lane_add(lane_sub(lane_mul(vx, mx), bx2), pt));
-    put(fl, fr, V::VY, lane_sub(lane_mul(vx, my), lane_mul(bx, by)));
-    put(fl, fr, V::VZ, lane_sub(lane_mul(vx, mz), lane_mul(bx, bz)));
-    put(fl, fr, V::BX, bp);
-    put(fl, fr, V::BY, lane_sub(lane_mul(vx, by), lane_mul(bx, vy)));
-    put(fl, fr, V::BZ, lane_sub(lane_mul(vx, bz), lane_mul(bx, vz)));
-    put(fl, fr, V::BP, lane_mul(lane_bcast<float2>(P.cmax2), bx));
-    put(fl, fr, V::EN, lane_sub(lane_mul(vx, lane_add(en, pt)), lane_mul(bx, vb)));
-    const float2 fa = lane_mul(lane_bcast<float2>(P.gamma), pr);
-    const float2 fb = lane_add(fa, bb);
-    const float2 fc = lane_sub(lane_mul(fb, fb), lane_mul(lane_mul(lane_bcast<float2>(4.0f), fa), bx2));
-    const float2 sq = make_float2(fc.x > 0.0f ? d_sqrt(fc.x) : 0.0f, fc.y > 0.0f ? d_sqrt(fc.y) : 0.0f);
-    c2 = lane_mul(lane_mul(half, lane_add(fb, sq)), lane_rcp(dn));
-  }
-  const float cl = d_sqrt(c2.x), cr = d_sqrt(c2.y);
-  clm = vx.x - cl;
-  clp = vx.x + cl;
-  crm = vx.y - cr;
-  crp = vx.y + cr;
-}
-
 // ---------------------------------------------------------------------------
 // Riemann solvers on rotated primitive states (normal component first).
 // ---------------------------------------------------------------------------
@@ -1122,13 +1056,8 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
   R ul[NV], ur[NV], fl[NV], fr[NV];
   R clm, clp, crm, crp;
   if constexpr (V::MHD) glm_average<EQ>(ql, qr, P);
-  // FP32 adiabatic HD / MHD, two-wave family: both states' conserved
-  // variables, fluxes and speeds on packed f32x2 pairs (left, right)
-  constexpr bool LR = std::is_same<R, float>::value && !V::SR && !V::ISO && RS != RS_ROE;
-  if constexpr (!LR) {
-    prim2cons<EQ>(ql, ul, P);
-    prim2cons<EQ>(qr, ur, P);
-  }
+  prim2cons<EQ>(ql, ul, P);
+  prim2cons<EQ>(qr, ur, P);
   if constexpr (RS == RS_ROE) {
     fluxspeed<EQ, false>(ql, ul, fl, clm, clp, P);
     fluxspeed<EQ, false>(qr, ur, fr, crm, crp, P);
@@ -1216,12 +1145,8 @@ __device__ __forceinline__ void riemann(R* ql, R* qr, R* f, const Phys<R>& P) {
     }
     return;
   } else {
-    if constexpr (LR) {
-      p2c_flux_lr<EQ>(ql, qr, ul, ur, fl, fr, clm, clp, crm, crp, P);
-    } else {
-      fluxspeed<EQ, true>(ql, ul, fl, clm, clp, P);
-      fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
-    }
+    fluxspeed<EQ, true>(ql, ul, fl, clm, clp, P);
+    fluxspeed<EQ, true>(qr, ur, fr, crm, crp, P);
     R sl = d_min(clm, crm), sr = d_max(clp, crp);
     if constexpr (V::SR && RS == RS_HLLC) {
       if constexpr (V::MHD) srmhd_hllc(ql, qr, ul, ur, fl, fr, sl, sr, f);
