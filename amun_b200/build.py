@@ -19,7 +19,8 @@ that that many 288-thread CTAs fit on an SM.  Measured on B200 (128^3 MHD,
 WENO-Z, HLLD, SSPRK3): FP64 with 1/2/3 CTAs 7.8/5.1/4.8 ms per step (results
 bit-identical, small spills at 3); FP32 bulk with 2/3/4/5 CTAs
 2.40/1.92/1.79/1.89 ms, and 1.69/1.83 ms at 4/5 CTAs once the last
-sweep's cons2prim ran in FP32.  The FP32 units also use the approximate
+sweep's cons2prim ran in FP32; with the sweeps compiled per role (x, y
+and z without spills at 4 CTAs) 3/4/5 CTAs give 1.203/1.095/1.287 ms.  The FP32 units also use the approximate
 single-precision divide and square root with denormals flushed; their
 conserved totals and the relativistic recovery stay in FP64.
 """
