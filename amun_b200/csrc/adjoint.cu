@@ -1,5 +1,6 @@
 // adjoint.cu -- kernels of the discrete adjoint of one SSPRK stage (HD and
-// GLM-MHD, WENO-Z reconstruction, HLL fluxes) on the uniform block mesh.
+// GLM-MHD, WENO-Z or TVD reconstruction, HLL fluxes) on the uniform block
+// mesh.
 //
 // Reverse of one stage, given lam of the stage output:
 //   adj_combination   out = comb(A, B, ds du): lamdu, lam[A], lam[B]
@@ -8,7 +9,8 @@
 //                     face states, lamF = (lamdu(i+1) - lamdu(i))/dx, reverse
 //                     HLL -> lam of the two face states (G);
 //                     WENO kernel, per cell and variable: reverse WENO-Z of
-//                     both faces -> five stencil partials (P)
+//                     both faces -> five stencil partials (P); with TVD
+//                     reconstruction the TVD kernel (three partials)
 //   adj_cells         per interior cell: sum the partials aimed at the cell
 //                     and at its ghost copies in the neighbour blocks (a
 //                     gather, no atomics, so the result does not depend on
@@ -92,10 +94,10 @@ __device__ __forceinline__ long long dir_stride(const Geo& g) {
 // Per interface i+1/2 along DIR (cells L = i, R = i+1 on interior lines):
 // WENO-Z face states, HLL flux reverse.  G[DIR][0] at L receives lam of L's
 // right face state, G[DIR][1] at R lam of R's left face state.
-template <int EQ, int DIR, typename R>
+template <int EQ, int DIR, int REC, typename R>
 __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const R* __restrict__ Q,
                                           const double* __restrict__ lamdu, double* __restrict__ G, double dxi,
-                                          const Geo& g, const Phys<R>& P, R eps) {
+                                          const Geo& g, const Phys<R>& P, R eps, int lim) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
   const int nc = g.nc, ng = g.ng;
@@ -116,9 +118,17 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     const R* q = Q + cL + v * g.qvs;
-    const R s0 = q[-2 * sD], s1 = q[-sD], s2 = q[0], s3 = q[sD], s4 = q[2 * sD], s5 = q[3 * sD];
-    ql[v] = weno5z_right_value<R>(s0, s1, s2, s3, s4, eps);  // right face of L
-    qr[v] = weno5z_right_value<R>(s5, s4, s3, s2, s1, eps);  // left face of R (mirror)
+    if constexpr (REC == REC_TVD) {
+      const long long sxyz[3] = {1LL, (long long)g.IM, (long long)g.IM * g.JM};
+      const bool pos = v == V::DN || v == V::PR;
+      R fac;
+      ql[v] = q[0] + tvd_slope<R>(q, DIR, sxyz, g.ndims, pos, lim, eps, fac);      // right face of L
+      qr[v] = q[sD] - tvd_slope<R>(q + sD, DIR, sxyz, g.ndims, pos, lim, eps, fac);  // left face of R
+    } else {
+      const R s0 = q[-2 * sD], s1 = q[-sD], s2 = q[0], s3 = q[sD], s4 = q[2 * sD], s5 = q[3 * sD];
+      ql[v] = weno5z_right_value<R>(s0, s1, s2, s3, s4, eps);  // right face of L
+      qr[v] = weno5z_right_value<R>(s5, s4, s3, s2, s1, eps);  // left face of R (mirror)
+    }
     const double lR = inR ? lamdu[iu + uD + v * g.uvs] : 0.0;
     const double lL = inL ? lamdu[iu + v * g.uvs] : 0.0;
     lF[v] = R(dxi * (lR - lL));
@@ -140,7 +150,7 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
 }
 
 // blockIdx.z = direction
-template <int EQ, typename R>
+template <int EQ, int REC, typename R>
 __global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_kernel(const R* __restrict__ Q,
                                                             const double* __restrict__ lamdu,
                                                             double* __restrict__ G, const double* __restrict__ binv,
@@ -152,9 +162,9 @@ __global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_k
   const R eps = R(m.eps);
   const double dxi = binv[3 * b + dir];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
-    if (dir == 0) face_body<EQ, 0, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
-    else if (dir == 1) face_body<EQ, 1, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
-    else face_body<EQ, 2, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps);
+    if (dir == 0) face_body<EQ, 0, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
+    else if (dir == 1) face_body<EQ, 1, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
+    else face_body<EQ, 2, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
   }
 }
 
@@ -203,6 +213,61 @@ __global__ void weno_rev_kernel(const R* __restrict__ Q, const double* __restric
     if (dir == 0) weno_body<0, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
     else if (dir == 1) weno_body<1, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
     else weno_body<2, R>(t, b, gridDim.y, Q, G, P, g, nv, eps);
+  }
+}
+
+// Per cell c along DIR (ng-1 .. ng+nc) on interior lines and variable: TVD
+// reverse of the cell's two faces q +- fac lim(0.5, a, b), a = q - q(-1),
+// b = q(+1) - q, with lam of the right face from G[DIR][0] and of the left
+// face from G[DIR][1]; the partials go to P[DIR][1..3] (cells c-1, c, c+1),
+// P[DIR][0] and P[DIR][4] are zero.  pr = index of the pressure.
+template <int DIR, typename R>
+__device__ __forceinline__ void tvd_body(long long t, int b, int nblocks, const R* __restrict__ Q,
+                                         const double* __restrict__ G, double* __restrict__ P, const Geo& g, int nv,
+                                         int pr, int lim, R eps) {
+  const int nc = g.nc, ng = g.ng;
+  const int nt2 = g.ndims == 3 ? nc : 1;
+  const long long per_v = (long long)(nc + 2) * nc * nt2;
+  const long long qd = g.qbs * nblocks;
+  const long long sxyz[3] = {1LL, (long long)g.IM, (long long)g.IM * g.JM};
+  const long long sD = sxyz[DIR];
+  const int v = (int)(t / per_v);
+  if (v >= nv) return;
+  int a, t1, t2;
+  line_index<DIR>(t - v * per_v, nc + 2, nc, nt2, a, t1, t2);
+  a += ng - 1;
+  int i, j, k;
+  line_cell<DIR>(g, a, t1, t2, i, j, k);
+  const long long cell = ((long long)k * g.JM + j) * g.IM + i;
+  const long long c = (long long)b * g.qbs + v * g.qvs + cell;
+  const double* G0 = G + (long long)(2 * DIR) * qd;
+  const R lR = R(a <= ng + nc - 1 ? G0[c] : 0.0);
+  const R lL = R(a >= ng ? G0[qd + c] : 0.0);
+  const R* q = Q + c;
+  R fac;
+  tvd_slope<R>(q, DIR, sxyz, g.ndims, v == 0 || v == pr, lim, eps, fac);
+  R la = R(0), lb = R(0);
+  const R ls = (lR - lL) * fac;
+  if (ls != R(0)) limiter_rev<R>(lim, R(0.5), q[0] - q[-sD], q[sD] - q[0], eps, ls, la, lb);
+  double* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
+  Pd[0] = 0.0;
+  Pd[g.qbs] = (double)(-la);
+  Pd[2 * g.qbs] = (double)((lR + lL) + (la - lb));
+  Pd[3 * g.qbs] = (double)lb;
+  Pd[4 * g.qbs] = 0.0;
+}
+
+template <typename R>
+__global__ void tvd_rev_kernel(const R* __restrict__ Q, const double* __restrict__ G, double* __restrict__ P, Geo g,
+                               int nv, int lim, double eps_d) {
+  const int b = blockIdx.y, dir = blockIdx.z;
+  const int nt2 = g.ndims == 3 ? g.nc : 1;
+  const long long per = (long long)(g.nc + 2) * g.nc * nt2 * nv;
+  const R eps = R(eps_d);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
+    if (dir == 0) tvd_body<0, R>(t, b, gridDim.y, Q, G, P, g, nv, nv - 1, lim, eps);
+    else if (dir == 1) tvd_body<1, R>(t, b, gridDim.y, Q, G, P, g, nv, nv - 1, lim, eps);
+    else tvd_body<2, R>(t, b, gridDim.y, Q, G, P, g, nv, nv - 1, lim, eps);
   }
 }
 
@@ -360,9 +425,15 @@ cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* 
   const long long nf = (long long)(g.nc + 1) * g.nc * nt2;
   const long long nw = (long long)(g.nc + 2) * g.nc * nt2 * a.nv;
   const dim3 gf(blocks_of(nf, kFaceThreads), a.nblocks, g.ndims), gw(blocks_for(nw), a.nblocks, g.ndims);
-  if (a.eq == EQ_HD) face_kernel<EQ_HD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
-  else face_kernel<EQ_MHD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
-  weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.eps);
+  if (m.rec == REC_TVD) {
+    if (a.eq == EQ_HD) face_kernel<EQ_HD, REC_TVD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else face_kernel<EQ_MHD, REC_TVD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    tvd_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.lim, m.eps);
+  } else {
+    if (a.eq == EQ_HD) face_kernel<EQ_HD, REC_WENO5Z, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else face_kernel<EQ_MHD, REC_WENO5Z, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.eps);
+  }
   return cudaGetLastError();
 }
 

@@ -16,6 +16,104 @@ namespace amun {
 
 template <typename R> __device__ __forceinline__ R rsign(R x) { return x > R(0) ? R(1) : (x < R(0) ? R(-1) : R(0)); }
 
+// Reverse of limiter(which, x, a, b, eps) (src/interpolations.F90:4684-4877):
+// la += d lim / d a * lam, lb += d lim / d b * lam.  The sign factors are
+// piecewise constant; min/max differentiate the operand they returned (the
+// second one on ties, as d_min/d_max do).
+template <typename R>
+__device__ __forceinline__ void limiter_rev(int which, R x, R a, R b, R eps, R lam, R& la, R& lb) {
+  switch (which) {
+    case LIM_MM: {
+      const R S = R(0.5) * (fsign(x, a) + fsign(x, b)) * lam;
+      if (d_fabs(a) < d_fabs(b)) la += S * rsign(a); else lb += S * rsign(b);
+      break;
+    }
+    case LIM_MC: {
+      const R S = (fsign(x, a) + fsign(x, b)) * lam;
+      const R fa = d_fabs(a), fb = d_fabs(b);
+      if (d_min(fa, fb) < R(0.25) * d_fabs(a + b)) {
+        if (fa < fb) la += S * rsign(a); else lb += S * rsign(b);
+      } else {
+        const R t = R(0.25) * S * rsign(a + b);
+        la += t;
+        lb += t;
+      }
+      break;
+    }
+    case LIM_SB: {
+      const R S = R(0.5) * (fsign(x, a) + fsign(x, b)) * lam;
+      const R fa = d_fabs(a), fb = d_fabs(b);
+      if (d_min(R(2) * fa, fb) > d_min(fa, R(2) * fb)) {
+        if (R(2) * fa < fb) la += R(2) * S * rsign(a); else lb += S * rsign(b);
+      } else {
+        if (fa < R(2) * fb) la += S * rsign(a); else lb += R(2) * S * rsign(b);
+      }
+      break;
+    }
+    case LIM_VL:
+      // 2 x a b / (a + b) where a b > 0
+      if (a * b > R(0)) {
+        const R s = a + b;
+        const R k = R(2) * x * lam / (s * s);
+        la += k * b * b;
+        lb += k * a * a;
+      }
+      break;
+    case LIM_VA: {
+      // x a b (a + b) / max(eps, a^2 + b^2)
+      const R s2 = a * a + b * b;
+      const R N = x * a * b * (a + b);
+      const R dNa = x * (R(2) * a * b + b * b), dNb = x * (a * a + R(2) * a * b);
+      if (eps > s2) {
+        la += lam * dNa / eps;
+        lb += lam * dNb / eps;
+      } else {
+        la += lam * (dNa * s2 - N * R(2) * a) / (s2 * s2);
+        lb += lam * (dNb * s2 - N * R(2) * b) / (s2 * s2);
+      }
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// The TVD half-slope of one variable at a padded cell along direction sD
+// (interfaces_tvd, src/interpolations.F90:729-848, as the forward sweep
+// computes it): limiter(0.5, q - q(-1), q(+1) - q); for a positive variable
+// the slopes of every direction are halved together while q <= their |sum|,
+// and all are zero where q <= 0.  fac receives the factor applied to this
+// direction's limited slope (0.5^k, or 0), which the derivative holds
+// constant.  s[] = the strides of x, y, z.
+template <typename R>
+__device__ __forceinline__ R tvd_slope(const R* q, int dir, const long long* s, int ndims, bool positive, int lim,
+                                       R eps, R& fac) {
+  const R f0 = q[0];
+  if (!positive) {
+    fac = R(1);
+    return limiter<R>(lim, R(0.5), f0 - q[-s[dir]], q[s[dir]] - f0, eps);
+  }
+  R dq[3];
+  dq[0] = limiter<R>(lim, R(0.5), f0 - q[-s[0]], q[s[0]] - f0, eps);
+  dq[1] = limiter<R>(lim, R(0.5), f0 - q[-s[1]], q[s[1]] - f0, eps);
+  dq[2] = R(0);
+  if (ndims == 3) dq[2] = limiter<R>(lim, R(0.5), f0 - q[-s[2]], q[s[2]] - f0, eps);
+  fac = R(1);
+  if (f0 > R(0)) {
+    for (int it = 0; it < 4096; ++it) {
+      R t = d_fabs(dq[0]) + d_fabs(dq[1]);
+      if (ndims == 3) t = t + d_fabs(dq[2]);
+      if (!(f0 <= t)) break;
+      dq[0] = R(0.5) * dq[0]; dq[1] = R(0.5) * dq[1]; dq[2] = R(0.5) * dq[2];
+      fac = R(0.5) * fac;
+    }
+  } else {
+    dq[0] = dq[1] = dq[2] = R(0);
+    fac = R(0);
+  }
+  return dq[dir];
+}
+
 // Reverse of the right-face state fR of weno5z_faces (the reference's fl(i),
 // src/interpolations.F90:1937-2083) for the stencil f[0..4] = f(i-2..i+2):
 // g[0..4] += d fR / d f * lam.

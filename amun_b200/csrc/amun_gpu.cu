@@ -2394,12 +2394,14 @@ __global__ void load_step_kernel(DevScalars* sc, const DevScalars* rec) {
 int adj_supported() {
   if (C.p.eqsys != AMUN_EQ_HD && C.p.eqsys != AMUN_EQ_MHD)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: adiabatic HD and MHD only");
-  if (C.p.reconstruction != AMUN_REC_WENO5Z) return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z reconstruction only");
+  if (C.p.reconstruction != AMUN_REC_WENO5Z && C.p.reconstruction != AMUN_REC_TVD)
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z or TVD reconstruction only");
   if (effective_solver() != AMUN_RS_HLL) return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL Riemann solver only");
   if (C.p.fix_positivity || C.p.clip_extrema || C.p.mlp)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity, clip_extrema and mlp_limiting must be off");
   if (sources_on()) return fail(AMUN_E_UNSUPPORTED, "adjoint: no source terms");
-  if (C.p.nghosts < 4) return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4");
+  if (C.p.nghosts < (C.p.reconstruction == AMUN_REC_TVD ? 2 : 4))
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: needs nghosts >= 4 (WENO-Z) or >= 2 (TVD)");
   if (C.amr) return fail(AMUN_E_UNSUPPORTED, "adjoint: meshes at one level only");
   return 0;
 }

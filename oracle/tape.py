@@ -2,7 +2,8 @@
 
 A differentiable restatement, in torch FP64 on the host, of the stage update
 whose discrete adjoint the GPU library implements: adiabatic HD or GLM-MHD,
-WENO-Z reconstruction (src/interpolations.F90:1937-2083), the HLL solver
+WENO-Z reconstruction (src/interpolations.F90:1937-2083) or TVD with the
+positivity halving (729-848) and the limiters of 4684-4877, the HLL solver
 (src/schemes.F90:1248-1341, 3163-3274 with the GLM averaging), the flux
 difference (src/evolution.F90:1898-1977), the SSPRK stage combinations of
 src/evolution.F90 (628-770 rk2, 1005-1208 rk3) and the psi decay
@@ -31,7 +32,8 @@ _ROT = {0: (0, 1, 2), 1: (1, 2, 0), 2: (2, 0, 1)}
 
 class Scheme:
     def __init__(self, nv: int, ndims: int, gamma: float, cfl: float, dx, alpha: float = 2.0,
-                 eps: float = 2.220446049250313e-16, time_advance: str = "rk3"):
+                 eps: float = 2.220446049250313e-16, time_advance: str = "rk3", reconstruction: str = "weno5z",
+                 limiter: str = "mc"):
         self.nv, self.ndims = nv, ndims
         self.mhd = nv == 9
         self.gamma = gamma
@@ -44,6 +46,8 @@ class Scheme:
         self.decay = math.exp(-alpha * cfl)
         self.ta = time_advance
         self.pr = nv - 1
+        self.rec = reconstruction
+        self.lim = limiter
 
     # ---- equations -------------------------------------------------------------
     def prim2cons(self, q):
@@ -140,12 +144,66 @@ class Scheme:
         qr = (2.0 / 6.0) * f0 + (5.0 / 6.0) * fp1 + (-1.0 / 6.0) * fp2
         return (wl * ql + wr * qr) + wc * qc
 
+    def limiter(self, x, a, b):
+        """limiter_{mm,mc,sb,vl,va} (src/interpolations.F90:4684-4877) with the
+        GPU kernels' branch choices (min/max return the second operand on ties;
+        SIGN(x, a) follows the sign bit of a)."""
+        def dmin(p, q):
+            return torch.where(p < q, p, q)
+
+        def dmax(p, q):
+            return torch.where(p > q, p, q)
+
+        sa = torch.copysign(torch.full_like(a, abs(x)), a)
+        sb = torch.copysign(torch.full_like(b, abs(x)), b)
+        if self.lim == "mm":
+            return 0.5 * (sa + sb) * dmin(torch.abs(a), torch.abs(b))
+        if self.lim == "mc":
+            return (sa + sb) * dmin(dmin(torch.abs(a), torch.abs(b)), 0.25 * torch.abs(a + b))
+        if self.lim == "sb":
+            return 0.5 * (sa + sb) * dmax(dmin(2.0 * torch.abs(a), torch.abs(b)), dmin(torch.abs(a), 2.0 * torch.abs(b)))
+        if self.lim == "vl":
+            c = a * b
+            pos = c > 0.0
+            den = torch.where(pos, a + b, torch.ones_like(a))
+            return torch.where(pos, 2.0 * x * c / den, torch.zeros_like(a))
+        if self.lim == "va":
+            return x * a * b * (a + b) / dmax(torch.full_like(a, self.eps), a * a + b * b)
+        raise ValueError(self.lim)
+
+    def tvd_slopes(self, q):
+        """interfaces_tvd (src/interpolations.F90:729-848) on the periodic
+        field: per variable and direction the half-slope limiter(0.5, q -
+        q(-1), q(+1) - q); density and pressure have the slopes of every
+        direction halved together while q <= the sum of their magnitudes, and
+        zeroed where q <= 0."""
+        nd = self.ndims
+        out = []
+        for v, c in enumerate(q):
+            sl = []
+            for d in range(nd):
+                axis = c.dim() - 1 - d
+                sl.append(self.limiter(0.5, c - torch.roll(c, 1, axis), torch.roll(c, -1, axis) - c))
+            if v == DN or v == self.pr:
+                for _ in range(4096):
+                    t = torch.abs(sl[0]) + torch.abs(sl[1])
+                    if nd == 3:
+                        t = t + torch.abs(sl[2])
+                    m = (c > 0.0) & (c <= t)
+                    if not bool(m.any()):
+                        break
+                    sl = [torch.where(m, 0.5 * x, x) for x in sl]
+                sl = [torch.where(c > 0.0, x, torch.zeros_like(x)) for x in sl]
+            out.append(sl)
+        return out
+
     # ---- one stage operator L(q) ---------------------------------------------------
     def increment(self, q, cmax, cmax2):
         """du for interior cells from the primitive field q (list of nv
         tensors, spatial shape (NZ,)NY,NX, periodic)."""
         du = [torch.zeros_like(q[0]) for _ in range(self.nv)]
         nd = self.ndims
+        slopes = self.tvd_slopes(q) if self.rec == "tvd" else None
         for d in range(nd):
             axis = q[0].dim() - 1 - d  # x is the last axis
             n = q[0].shape[axis]
@@ -155,7 +213,16 @@ class Scheme:
             # interfaces i+1/2 for i = -1..n-1: left state = right face of cell i,
             # right state = left face of cell i+1 (mirror stencil)
             ql, qr = [], []
-            for c in pads:
+            if slopes is not None:
+                # faces of the TVD cells: q_i + dq_i and q_{i+1} - dq_{i+1}
+                for v, c in enumerate(q):
+                    fr = c + slopes[v][d]
+                    fl = c - slopes[v][d]
+                    fr = torch.cat([fr.narrow(axis, n - 1, 1), fr], dim=axis).movedim(axis, -1)
+                    fl = torch.cat([fl, fl.narrow(axis, 0, 1)], dim=axis).movedim(axis, -1)
+                    ql.append(fr)
+                    qr.append(fl)
+            for c in pads if slopes is None else ():
                 s = [c[..., k:k + n + 1] for k in range(6)]  # cells i-2 .. i+3
                 ql.append(self.weno_right(s[0], s[1], s[2], s[3], s[4]))
                 qr.append(self.weno_right(s[5], s[4], s[3], s[2], s[1]))

@@ -34,10 +34,32 @@ def field(mesh, nv, seed):
     return q
 
 
+def field_all(mesh, nv, seed):
+    """Every primitive variable a smooth seeded field, none constant along a
+    direction and none zero.  The TVD limiters have a kink where both
+    one-sided differences vanish; a variable that is constant along a line
+    (or zero, as psi starts) sits on it, where round-off in the forward state
+    decides which side's derivative a gradient takes, so the TVD gradients
+    are compared on states away from it."""
+    shp = mesh.shape if mesh.ndims == 3 else mesh.shape[1:]
+    f = np.concatenate([problems.random_phase_field(shp, seed + 97 * i, ncomp=4) for i in range(3)], axis=-1)
+    if mesh.ndims == 2:
+        f = f[None]
+    f /= np.max(np.abs(f).reshape(-1, f.shape[-1]), axis=0)
+    q = problems.uniform(mesh, nv)
+    q[..., 0] = 1.0 + 0.05 * f[..., 0]
+    q[..., 1:4] = 0.1 * f[..., 1:4]
+    if nv == 9:
+        q[..., 4:7] = 0.2 + 0.05 * f[..., 4:7]
+        q[..., 7] = 0.01 * f[..., 7]
+    q[..., nv - 1] = 1.0 + 0.05 * f[..., 8]
+    return q
+
+
 def tape_gradient(tape, p, mesh, nv, q0, nsteps):
     from amun_b200.adjoint import kinetic_energy
     s = tape.Scheme(nv, mesh.ndims, p.get("gamma", 5.0 / 3.0), p.get("cfl", 0.4), [mesh.dx, mesh.dy, mesh.dz],
-                    time_advance=p["time_advance"])
+                    time_advance=p["time_advance"], reconstruction=p["reconstruction"], limiter=p["limiter"])
     qt = torch.from_numpy(q0[0] if mesh.ndims == 2 else q0).clone().requires_grad_(True)
     u = tape.evolve(s, qt, nsteps)
     uf = u[None] if mesh.ndims == 2 else u
@@ -57,25 +79,32 @@ def gpu_gradient(sim, mesh, q0, nsteps, interval):
 
 
 CASES = [
-    # eq, integrator, ndims, ncells, blocks per direction, steps, checkpoint interval
-    ("mhd", "rk3", 2, 32, 1, 10, 4),
-    ("hd", "rk2", 2, 8, 2, 6, 3),
-    ("mhd", "rk2", 3, 8, 1, 4, 2),
-    ("mhd", "rk3", 3, 4, 2, 3, 1),
+    # eq, integrator, ndims, ncells, blocks per direction, steps, checkpoint
+    # interval, reconstruction, limiter
+    ("mhd", "rk3", 2, 32, 1, 10, 4, "weno5z", "mc"),
+    ("hd", "rk2", 2, 8, 2, 6, 3, "weno5z", "mc"),
+    ("mhd", "rk2", 3, 8, 1, 4, 2, "weno5z", "mc"),
+    ("mhd", "rk3", 3, 4, 2, 3, 1, "weno5z", "mc"),
+    # TVD with nghosts = 2, one case per limiter
+    ("mhd", "rk2", 2, 32, 1, 10, 4, "tvd", "mc"),
+    ("hd", "rk3", 2, 8, 2, 6, 3, "tvd", "mm"),
+    ("mhd", "rk2", 3, 8, 1, 4, 2, "tvd", "sb"),
+    ("hd", "rk2", 3, 4, 2, 3, 1, "tvd", "vl"),
+    ("mhd", "rk3", 2, 16, 2, 5, 2, "tvd", "va"),
 ]
 
 
-@pytest.mark.parametrize("eq,ta,nd,n,nb,nsteps,interval", CASES)
-def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval):
+@pytest.mark.parametrize("eq,ta,nd,n,nb,nsteps,interval,rec,lim", CASES)
+def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval, rec, lim):
     import tape
     from amun_b200.solver import Simulation
-    kw = dict(UNIT, ndims=nd, ncells=n, xblocks=nb, yblocks=nb)
+    kw = dict(UNIT, ndims=nd, ncells=n, xblocks=nb, yblocks=nb, limiter=lim)
     if nd == 3:
         kw["zblocks"] = nb
-    p = params(eq, "weno5z", "hll", ta, **kw)
+    p = params(eq, rec, "hll", ta, **kw)
     mesh = UniformMesh(geometry(p))
     nv = 9 if eq == "mhd" else 5
-    q0 = field(mesh, nv, seed=3)
+    q0 = field(mesh, nv, seed=3) if rec == "weno5z" else field_all(mesh, nv, seed=3)
     sim = Simulation(p)
     try:
         gg, ug, Jg = gpu_gradient(sim, mesh, q0, nsteps, interval)
@@ -93,16 +122,19 @@ def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval):
     assert np.all(err <= 1e-9), err
 
 
-def test_adjoint_finite_differences():
+@pytest.mark.parametrize("rec", ["weno5z", "tvd"])
+def test_adjoint_finite_differences(rec):
     """The configuration's scheme (2D MHD, WENO-Z, HLL, SSPRK(3,3)) on 32^2,
-    20 steps with checkpoints every 5: dJ/drho0 along 8 seeded smooth
-    directions agrees with central differences to 1e-6 (FD step swept over
-    1e-6..1e-8, runs replaying the recorded dt and cmax)."""
+    20 steps with checkpoints every 5, and the same with TVD-MC (on a state
+    with every variable varying in every direction, field_all): dJ/drho0
+    along 8 seeded smooth directions agrees with central differences to 1e-6
+    (FD step swept over 1e-6..1e-8, runs replaying the recorded dt and
+    cmax)."""
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
-    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    p = params("mhd", rec, "hll", "rk3", ndims=2, ncells=32, **UNIT)
     mesh = UniformMesh(geometry(p))
-    q0 = problems.smooth_mhd(mesh, seed=0)
+    q0 = problems.smooth_mhd(mesh, seed=0) if rec == "weno5z" else field_all(mesh, 9, seed=0)
     sim = Simulation(p)
     try:
         g, _, _ = gpu_gradient(sim, mesh, q0, 20, 5)
@@ -116,7 +148,9 @@ def test_adjoint_finite_differences():
             d = problems.random_phase_field(mesh.shape[1:], 100 + k, ncomp=1)[None, ..., 0]
             ad = float(np.sum(g[..., 0] * d))
             errs = []
-            for eps in (1e-6, 1e-7, 1e-8):
+            # the TVD update is only piecewise smooth (limiter branches), so
+            # larger steps cross kinks: its sweep goes one step further down
+            for eps in (1e-6, 1e-7, 1e-8) + ((1e-9,) if rec == "tvd" else ()):
                 qp, qm = q0.copy(), q0.copy()
                 qp[..., 0] += eps * d
                 qm[..., 0] -= eps * d
@@ -233,18 +267,20 @@ def test_evolve_on_cuda_tensors_matches_host_path():
     assert np.array_equal(out["cpu"][1], out["cuda"][1])
 
 
-def test_adjoint_fp32_bulk():
+@pytest.mark.parametrize("rec", ["weno5z", "tvd"])
+def test_adjoint_fp32_bulk(rec):
     """FP32-bulk forward and adjoint: dJ/drho0 within 1e-3 (relative to its
-    largest entry) of the FP64 tape's (measured 2.8e-4).  The gradients with
-    respect to the initial pressure and psi are not compared: both fields
-    start uniform, so their WENO-Z smoothness indicators are built from
-    differences near the FP32 resolution of the stored state and the weight
-    derivatives carry percent-level quantisation noise."""
+    largest entry) of the FP64 tape's (measured 2.8e-4 for WENO-Z).  The
+    gradients with respect to the initial pressure and psi are not compared:
+    both fields start uniform, so their WENO-Z smoothness indicators are
+    built from differences near the FP32 resolution of the stored state and
+    the weight derivatives carry percent-level quantisation noise.  TVD-MC
+    runs on a state with every variable varying (field_all)."""
     import tape
     from amun_b200.solver import Simulation
-    p = params("mhd", "weno5z", "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    p = params("mhd", rec, "hll", "rk3", ndims=2, ncells=32, **UNIT)
     mesh = UniformMesh(geometry(p))
-    q0 = problems.smooth_mhd(mesh, seed=1)
+    q0 = problems.smooth_mhd(mesh, seed=1) if rec == "weno5z" else field_all(mesh, 9, seed=1)
     sim = Simulation(p, "fp32")
     try:
         gg, _, _ = gpu_gradient(sim, mesh, q0, 10, 5)
