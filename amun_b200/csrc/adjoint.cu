@@ -7,7 +7,8 @@
 //   adj_faces         all directions in one launch each:
 //                     face kernel, per interface i+1/2: recompute the WENO-Z
 //                     face states, lamF = (lamdu(i+1) - lamdu(i))/dx, reverse
-//                     HLL -> lam of the two face states (G);
+//                     HLL (HLLC, HLLD: dual numbers, dual.cuh) -> lam of
+//                     the two face states (G);
 //                     WENO kernel, per cell and variable: reverse WENO-Z of
 //                     both faces -> five stencil partials (P); with TVD
 //                     reconstruction the TVD kernel (three partials)
@@ -17,6 +18,7 @@
 //                     thread order), then cons2prim^T into lam of the stage
 //                     input
 #include "adjoint.cuh"
+#include "dual.cuh"
 #include "adjoint.h"
 
 namespace amun {
@@ -94,7 +96,7 @@ __device__ __forceinline__ long long dir_stride(const Geo& g) {
 // Per interface i+1/2 along DIR (cells L = i, R = i+1 on interior lines):
 // WENO-Z face states, HLL flux reverse.  G[DIR][0] at L receives lam of L's
 // right face state, G[DIR][1] at R lam of R's left face state.
-template <int EQ, int DIR, int REC, typename R>
+template <int EQ, int DIR, int REC, int RS, typename R>
 __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const R* __restrict__ Q,
                                           const double* __restrict__ lamdu, double* __restrict__ G, double dxi,
                                           const Geo& g, const Phys<R>& P, R eps, int lim) {
@@ -137,7 +139,8 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
   rotate<EQ, DIR>(ql, a);
   rotate<EQ, DIR>(qr, c);
   rotate<EQ, DIR>(lF, ql);  // ql reused: rotated lF
-  hll_rev<EQ>(a, c, ql, lql, lqr, P);
+  if constexpr (RS == RS_HLL) hll_rev<EQ>(a, c, ql, lql, lqr, P);
+  else riemann_rev_dual<EQ, RS, R>(a, c, ql, lql, lqr, P);
   unrotate<EQ, DIR>(lql, a);
   unrotate<EQ, DIR>(lqr, c);
   double* G0 = G + (long long)(2 * DIR) * qd;
@@ -150,7 +153,7 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
 }
 
 // blockIdx.z = direction
-template <int EQ, int REC, typename R>
+template <int EQ, int REC, int RS, typename R>
 __global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_kernel(const R* __restrict__ Q,
                                                             const double* __restrict__ lamdu,
                                                             double* __restrict__ G, const double* __restrict__ binv,
@@ -162,9 +165,9 @@ __global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_k
   const R eps = R(m.eps);
   const double dxi = binv[3 * b + dir];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < per; t += (long long)gridDim.x * blockDim.x) {
-    if (dir == 0) face_body<EQ, 0, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
-    else if (dir == 1) face_body<EQ, 1, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
-    else face_body<EQ, 2, REC, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
+    if (dir == 0) face_body<EQ, 0, REC, RS, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
+    else if (dir == 1) face_body<EQ, 1, REC, RS, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
+    else face_body<EQ, 2, REC, RS, R>(t, b, gridDim.y, Q, lamdu, G, dxi, g, P, eps, m.lim);
   }
 }
 
@@ -417,6 +420,23 @@ cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStr
 
 #endif  // AMUN_ADJ_FP32_UNIT
 
+// face kernel of the configured system and solver: HLL has the hand-written
+// reverse, HLLC and HLLD (MHD) the dual-number one
+template <int REC, typename R>
+static void launch_faces(const AdjGeo& a, dim3 gf, const R* Q, const double* lamdu, double* G, const double* binv,
+                  const MethodConst& m, const DevScalars* rec, cudaStream_t s) {
+  const Geo& g = a.g;
+  if (a.eq == EQ_HD) {
+    if (a.rs == RS_HLLC) face_kernel<EQ_HD, REC, RS_HLLC, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else face_kernel<EQ_HD, REC, RS_HLL, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+  } else {
+    if (a.rs == RS_HLLC) face_kernel<EQ_MHD, REC, RS_HLLC, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else if (a.rs == RS_HLLD)
+      face_kernel<EQ_MHD, REC, RS_HLLD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else face_kernel<EQ_MHD, REC, RS_HLL, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+  }
+}
+
 template <typename R>
 cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* G, double* P, const double* binv,
                       const MethodConst& m, const DevScalars* rec, cudaStream_t s) {
@@ -426,12 +446,10 @@ cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* 
   const long long nw = (long long)(g.nc + 2) * g.nc * nt2 * a.nv;
   const dim3 gf(blocks_of(nf, kFaceThreads), a.nblocks, g.ndims), gw(blocks_for(nw), a.nblocks, g.ndims);
   if (m.rec == REC_TVD) {
-    if (a.eq == EQ_HD) face_kernel<EQ_HD, REC_TVD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
-    else face_kernel<EQ_MHD, REC_TVD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    launch_faces<REC_TVD, R>(a, gf, Q, lamdu, G, binv, m, rec, s);
     tvd_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.lim, m.eps);
   } else {
-    if (a.eq == EQ_HD) face_kernel<EQ_HD, REC_WENO5Z, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
-    else face_kernel<EQ_MHD, REC_WENO5Z, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    launch_faces<REC_WENO5Z, R>(a, gf, Q, lamdu, G, binv, m, rec, s);
     weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.eps);
   }
   return cudaGetLastError();

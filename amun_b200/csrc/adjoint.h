@@ -19,6 +19,7 @@ namespace amun {
 struct AdjGeo {
   Geo g;
   int nv, eq, nblocks;
+  int rs;  // Riemann solver (RS_HLL, RS_HLLC, RS_HLLD)
 };
 
 // lam[out] -> lamdu and lam[A], lam[B] for one stage combination

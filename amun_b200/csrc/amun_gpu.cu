@@ -2396,7 +2396,9 @@ int adj_supported() {
     return fail(AMUN_E_UNSUPPORTED, "adjoint: adiabatic HD and MHD only");
   if (C.p.reconstruction != AMUN_REC_WENO5Z && C.p.reconstruction != AMUN_REC_TVD)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z or TVD reconstruction only");
-  if (effective_solver() != AMUN_RS_HLL) return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL Riemann solver only");
+  if (effective_solver() != AMUN_RS_HLL && effective_solver() != AMUN_RS_HLLC &&
+      !(C.p.eqsys == AMUN_EQ_MHD && effective_solver() == AMUN_RS_HLLD))
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL, HLLC or HLLD Riemann solver only");
   if (C.p.fix_positivity || C.p.clip_extrema || C.p.mlp)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity, clip_extrema and mlp_limiting must be off");
   if (sources_on()) return fail(AMUN_E_UNSUPPORTED, "adjoint: no source terms");
@@ -2682,7 +2684,7 @@ int amun_gpu_adjoint(const double* lam_u, double* lam_q0, double* lam_u0) {
     CK(cudaMalloc(&A.stage, qd * sizeof(double)));
   }
   if ((r = build_inverse_neighbours())) return r;
-  AdjGeo ag{g, C.nv, C.p.eqsys, C.nblocks};
+  AdjGeo ag{g, C.nv, C.p.eqsys, C.nblocks, effective_solver()};
   CK(cudaMemcpyAsync(A.stage, lam_u, qd * sizeof(double), cudaMemcpyDefault, C.stream));
   cudaError_t e = adj_from_host_layout(ag, A.stage, A.lamU0, C.stream);
   if (e != cudaSuccess) return cuda_fail(e, "adjoint input");

@@ -4,6 +4,7 @@ A differentiable restatement, in torch FP64 on the host, of the stage update
 whose discrete adjoint the GPU library implements: adiabatic HD or GLM-MHD,
 WENO-Z reconstruction (src/interpolations.F90:1937-2083) or TVD with the
 positivity halving (729-848) and the limiters of 4684-4877, the HLL solver
+(and for HD the HLLC solver, src/schemes.F90:1366-1513)
 (src/schemes.F90:1248-1341, 3163-3274 with the GLM averaging), the flux
 difference (src/evolution.F90:1898-1977), the SSPRK stage combinations of
 src/evolution.F90 (628-770 rk2, 1005-1208 rk3) and the psi decay
@@ -33,7 +34,7 @@ _ROT = {0: (0, 1, 2), 1: (1, 2, 0), 2: (2, 0, 1)}
 class Scheme:
     def __init__(self, nv: int, ndims: int, gamma: float, cfl: float, dx, alpha: float = 2.0,
                  eps: float = 2.220446049250313e-16, time_advance: str = "rk3", reconstruction: str = "weno5z",
-                 limiter: str = "mc"):
+                 limiter: str = "mc", riemann: str = "hll"):
         self.nv, self.ndims = nv, ndims
         self.mhd = nv == 9
         self.gamma = gamma
@@ -48,6 +49,9 @@ class Scheme:
         self.pr = nv - 1
         self.rec = reconstruction
         self.lim = limiter
+        if riemann == "hllc" and self.mhd:
+            raise ValueError("the tape has HLLC for HD only")
+        self.rs = riemann
 
     # ---- equations -------------------------------------------------------------
     def prim2cons(self, q):
@@ -122,6 +126,41 @@ class Scheme:
             wr = sr * ur[v] - fr[v]
             fm = (sl * wr - sr * wl) / srml
             out.append(torch.where(left, fl[v], torch.where(right, fr[v], fm)))
+        return out
+
+    def hllc(self, ql, qr, cmax, cmax2):
+        """HD HLLC (src/schemes.F90:1366-1513) in the GPU solver's operation
+        order: the HLL speeds, the contact speed sm and pressure from the
+        HLL fluxes w = s u - f, the star state of the side sm points away
+        from (the flux -w_x of the momentum only when sm = 0).  Unused
+        branches divide by 1 so their zero gradients stay finite."""
+        ul, ur = self.prim2cons(ql), self.prim2cons(qr)
+        fl, clm, clp = self.fluxspeed(ql, ul, cmax2)
+        fr, crm, crp = self.fluxspeed(qr, ur, cmax2)
+        sl = torch.where(clm < crm, clm, crm)
+        sr = torch.where(clp > crp, clp, crp)
+        left, right = sl >= 0, sr <= 0
+        mid = ~(left | right)
+        one = torch.ones_like(sl)
+        wl = [sl * ul[v] - fl[v] for v in range(self.nv)]
+        wr = [sr * ur[v] - fr[v] for v in range(self.nv)]
+        dn = torch.where(mid, wr[DN] - wl[DN], one)
+        sm = (wr[VX] - wl[VX]) / dn
+        pr = (wl[DN] * wr[VX] - wr[DN] * wl[VX]) / dn
+        pos, neg = mid & (sm > 0), mid & (sm < 0)
+        slmm = torch.where(pos, sl - sm, one)
+        srmm = torch.where(neg, sr - sm, one)
+        en = self.pr
+        dl = wl[DN] / slmm
+        uil = [dl, dl * sm, dl * ql[VY], dl * ql[VZ], (wl[en] + sm * pr) / slmm]
+        dr = wr[DN] / srmm
+        uir = [dr, dr * sm, dr * qr[VY], dr * qr[VZ], (wr[en] + sm * pr) / srmm]
+        zero = torch.zeros_like(sl)
+        out = []
+        for v in range(self.nv):
+            f0 = -wl[VX] if v == VX else zero
+            fs = torch.where(pos, sl * uil[v] - wl[v], torch.where(neg, sr * uir[v] - wr[v], f0))
+            out.append(torch.where(left, fl[v], torch.where(right, fr[v], fs)))
         return out
 
     # ---- reconstruction ----------------------------------------------------------
@@ -237,7 +276,7 @@ class Scheme:
                     st[BX:BZ + 1] = mag
                 return st
 
-            F = self.hll(rotate(ql), rotate(qr), cmax, cmax2)
+            F = (self.hllc if self.rs == "hllc" else self.hll)(rotate(ql), rotate(qr), cmax, cmax2)
             Fu = list(F)
             for m, r in enumerate(rot):
                 Fu[VX + r] = F[VX + m]

@@ -59,7 +59,8 @@ def field_all(mesh, nv, seed):
 def tape_gradient(tape, p, mesh, nv, q0, nsteps):
     from amun_b200.adjoint import kinetic_energy
     s = tape.Scheme(nv, mesh.ndims, p.get("gamma", 5.0 / 3.0), p.get("cfl", 0.4), [mesh.dx, mesh.dy, mesh.dz],
-                    time_advance=p["time_advance"], reconstruction=p["reconstruction"], limiter=p["limiter"])
+                    time_advance=p["time_advance"], reconstruction=p["reconstruction"], limiter=p["limiter"],
+                    riemann=p["riemann_solver"])
     qt = torch.from_numpy(q0[0] if mesh.ndims == 2 else q0).clone().requires_grad_(True)
     u = tape.evolve(s, qt, nsteps)
     uf = u[None] if mesh.ndims == 2 else u
@@ -80,28 +81,31 @@ def gpu_gradient(sim, mesh, q0, nsteps, interval):
 
 CASES = [
     # eq, integrator, ndims, ncells, blocks per direction, steps, checkpoint
-    # interval, reconstruction, limiter
-    ("mhd", "rk3", 2, 32, 1, 10, 4, "weno5z", "mc"),
-    ("hd", "rk2", 2, 8, 2, 6, 3, "weno5z", "mc"),
-    ("mhd", "rk2", 3, 8, 1, 4, 2, "weno5z", "mc"),
-    ("mhd", "rk3", 3, 4, 2, 3, 1, "weno5z", "mc"),
+    # interval, reconstruction, limiter, Riemann solver
+    ("mhd", "rk3", 2, 32, 1, 10, 4, "weno5z", "mc", "hll"),
+    ("hd", "rk2", 2, 8, 2, 6, 3, "weno5z", "mc", "hll"),
+    ("mhd", "rk2", 3, 8, 1, 4, 2, "weno5z", "mc", "hll"),
+    ("mhd", "rk3", 3, 4, 2, 3, 1, "weno5z", "mc", "hll"),
     # TVD with nghosts = 2, one case per limiter
-    ("mhd", "rk2", 2, 32, 1, 10, 4, "tvd", "mc"),
-    ("hd", "rk3", 2, 8, 2, 6, 3, "tvd", "mm"),
-    ("mhd", "rk2", 3, 8, 1, 4, 2, "tvd", "sb"),
-    ("hd", "rk2", 3, 4, 2, 3, 1, "tvd", "vl"),
-    ("mhd", "rk3", 2, 16, 2, 5, 2, "tvd", "va"),
+    ("mhd", "rk2", 2, 32, 1, 10, 4, "tvd", "mc", "hll"),
+    ("hd", "rk3", 2, 8, 2, 6, 3, "tvd", "mm", "hll"),
+    ("mhd", "rk2", 3, 8, 1, 4, 2, "tvd", "sb", "hll"),
+    ("hd", "rk2", 3, 4, 2, 3, 1, "tvd", "vl", "hll"),
+    ("mhd", "rk3", 2, 16, 2, 5, 2, "tvd", "va", "hll"),
+    # HLLC (dual-number reverse), the blast configuration's TVD-MC/HLLC/SSPRK(2,2)
+    ("hd", "rk2", 2, 16, 2, 8, 4, "tvd", "mc", "hllc"),
+    ("hd", "rk3", 3, 8, 1, 4, 2, "weno5z", "mc", "hllc"),
 ]
 
 
-@pytest.mark.parametrize("eq,ta,nd,n,nb,nsteps,interval,rec,lim", CASES)
-def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval, rec, lim):
+@pytest.mark.parametrize("eq,ta,nd,n,nb,nsteps,interval,rec,lim,rs", CASES)
+def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval, rec, lim, rs):
     import tape
     from amun_b200.solver import Simulation
     kw = dict(UNIT, ndims=nd, ncells=n, xblocks=nb, yblocks=nb, limiter=lim)
     if nd == 3:
         kw["zblocks"] = nb
-    p = params(eq, rec, "hll", ta, **kw)
+    p = params(eq, rec, rs, ta, **kw)
     mesh = UniformMesh(geometry(p))
     nv = 9 if eq == "mhd" else 5
     q0 = field(mesh, nv, seed=3) if rec == "weno5z" else field_all(mesh, nv, seed=3)
@@ -122,17 +126,18 @@ def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval, rec, lim):
     assert np.all(err <= 1e-9), err
 
 
-@pytest.mark.parametrize("rec", ["weno5z", "tvd"])
-def test_adjoint_finite_differences(rec):
+@pytest.mark.parametrize("rec,rs", [("weno5z", "hll"), ("tvd", "hll"), ("weno5z", "hllc"), ("weno5z", "hlld"),
+                                    ("tvd", "hlld")])
+def test_adjoint_finite_differences(rec, rs):
     """The configuration's scheme (2D MHD, WENO-Z, HLL, SSPRK(3,3)) on 32^2,
     20 steps with checkpoints every 5, and the same with TVD-MC (on a state
-    with every variable varying in every direction, field_all): dJ/drho0
-    along 8 seeded smooth directions agrees with central differences to 1e-6
-    (FD step swept over 1e-6..1e-8, runs replaying the recorded dt and
-    cmax)."""
+    with every variable varying in every direction, field_all) and with the
+    MHD HLLC and HLLD solvers (dual-number reverse): dJ/drho0 along 8 seeded
+    smooth directions agrees with central differences to 1e-6 (FD step
+    swept over 1e-6..1e-8, runs replaying the recorded dt and cmax)."""
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
-    p = params("mhd", rec, "hll", "rk3", ndims=2, ncells=32, **UNIT)
+    p = params("mhd", rec, rs, "rk3", ndims=2, ncells=32, **UNIT)
     mesh = UniformMesh(geometry(p))
     q0 = problems.smooth_mhd(mesh, seed=0) if rec == "weno5z" else field_all(mesh, 9, seed=0)
     sim = Simulation(p)
@@ -294,7 +299,7 @@ def test_adjoint_fp32_bulk(rec):
 def test_adjoint_rejects_unsupported():
     from amun_b200 import _native as N
     from amun_b200.solver import Simulation
-    sim = Simulation(params("mhd", "tvd", "hlld", "rk2", ndims=2, ncells=16))
+    sim = Simulation(params("mhd", "tvd", "roe", "rk2", ndims=2, ncells=16))
     try:
         with pytest.raises(N.AmunError) as e:
             sim.forward_checkpointed(2, 1.0e30, 1)

@@ -12,17 +12,19 @@ from amun_b200.params import geometry
 
 def tape_scheme(tape, p, mesh, nv):
     return tape.Scheme(nv, mesh.ndims, p.get("gamma", 5.0 / 3.0), p.get("cfl", 0.4), [mesh.dx, mesh.dy, mesh.dz],
-                       time_advance=p["time_advance"], reconstruction=p["reconstruction"], limiter=p["limiter"])
+                       time_advance=p["time_advance"], reconstruction=p["reconstruction"], limiter=p["limiter"],
+                       riemann=p["riemann_solver"])
 
 
-@pytest.mark.parametrize("eq,ta,nd,rec,lim", [
-    ("mhd", "rk3", 2, "weno5z", "mc"), ("hd", "rk2", 2, "weno5z", "mc"), ("mhd", "rk2", 3, "weno5z", "mc"),
-    ("mhd", "rk3", 2, "tvd", "mc"), ("hd", "rk2", 2, "tvd", "mm"), ("mhd", "rk2", 3, "tvd", "sb"),
-    ("hd", "rk3", 3, "tvd", "vl"), ("mhd", "rk2", 2, "tvd", "va")])
-def test_tape_matches_oracle(oracle_mod, eq, ta, nd, rec, lim):
+@pytest.mark.parametrize("eq,ta,nd,rec,lim,rs", [
+    ("mhd", "rk3", 2, "weno5z", "mc", "hll"), ("hd", "rk2", 2, "weno5z", "mc", "hll"),
+    ("mhd", "rk2", 3, "weno5z", "mc", "hll"), ("mhd", "rk3", 2, "tvd", "mc", "hll"), ("hd", "rk2", 2, "tvd", "mm", "hll"),
+    ("mhd", "rk2", 3, "tvd", "sb", "hll"), ("hd", "rk3", 3, "tvd", "vl", "hll"), ("mhd", "rk2", 2, "tvd", "va", "hll"),
+    ("hd", "rk2", 2, "tvd", "mc", "hllc"), ("hd", "rk3", 3, "weno5z", "mc", "hllc")])
+def test_tape_matches_oracle(oracle_mod, eq, ta, nd, rec, lim, rs):
     import tape
     n = 16 if nd == 2 else 8
-    p = params(eq, rec, "hll", ta, ndims=nd, ncells=n, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, limiter=lim)
+    p = params(eq, rec, rs, ta, ndims=nd, ncells=n, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, limiter=lim)
     mesh = UniformMesh(geometry(p))
     o = oracle_mod.Oracle(p)
     nv = 9 if eq == "mhd" else 5
