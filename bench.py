@@ -180,22 +180,34 @@ ADJOINT_WORKLOAD = dict(ndims=2, equation_system="mhd", equation_of_state="adi",
                         limiter="mc", riemann_solver="hll", time_advance="rk3", cfl=0.4, gamma=GAMMA, nghosts=4,
                         ncells=256, xblocks=1, yblocks=1, maxlev=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0)
 ADJOINT_STEPS, ADJOINT_INTERVAL = 200, 20
+# the other schemes' reverses on the same 256^2 smooth state (FP64, every
+# stage input kept): the blast configuration's TVD-MC/HLLC/SSPRK(2,2) on HD and
+# the MHD configurations' TVD-MC and WENO-Z with HLLD (dual-number reverse)
+ADJOINT_SCHEMES = {
+    "hd2d-256^2 tvd-mc hllc ssprk(2,2)": dict(ADJOINT_WORKLOAD, equation_system="hd", reconstruction="tvd",
+                                               riemann_solver="hllc", time_advance="rk2", nghosts=2),
+    "mhd2d-256^2 tvd-mc hlld ssprk(2,2)": dict(ADJOINT_WORKLOAD, reconstruction="tvd", riemann_solver="hlld",
+                                                time_advance="rk2", nghosts=2),
+    "mhd2d-256^2 weno5z hlld ssprk(3,3)": dict(ADJOINT_WORKLOAD, riemann_solver="hlld"),
+}
 
 
-def adjoint_timing(torch, prec, interval=ADJOINT_INTERVAL):
-    """2D MHD 256^2 (WENO-Z, HLL, SSPRK(3,3)), smooth seeded state, 200 steps:
-    the plain forward run (graphs) against the recorded forward (checkpoint
-    every `interval` steps; 0: every stage input kept, no recomputation) and
-    the adjoint call (segment recomputation + reverse) for J = kinetic energy
-    in [0,0.25]^2 at the final step, all timed with CUDA events on the
-    library's stream."""
+def adjoint_timing(torch, prec, interval=ADJOINT_INTERVAL, workload=ADJOINT_WORKLOAD):
+    """2D MHD 256^2 (WENO-Z, HLL, SSPRK(3,3); or `workload`), smooth seeded
+    state, 200 steps: the plain forward run (graphs) against the recorded
+    forward (checkpoint every `interval` steps; 0: every stage input kept, no
+    recomputation) and the adjoint call (segment recomputation + reverse) for
+    J = kinetic energy in [0,0.25]^2 at the final step, all timed with CUDA
+    events on the library's stream."""
     from amun_b200 import problems
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
-    sim = Simulation(ADJOINT_WORKLOAD, precision=prec)
+    sim = Simulation(workload, precision=prec)
     stream = torch.cuda.current_stream()
     sim.L.amun_gpu_set_stream(stream.cuda_stream)
     q0 = problems.smooth_mhd(sim.mesh, seed=0)
+    if workload["equation_system"] == "hd":
+        q0 = np.ascontiguousarray(q0[..., [0, 1, 2, 3, 8]])
 
     def events(fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -720,6 +732,14 @@ def main():
             adjoint[prec]["checkpointed"] = adjoint_timing(torch, prec, ADJOINT_INTERVAL)
         except Exception as exc:  # pragma: no cover
             adjoint[prec] = {"error": str(exc)}
+    adjoint_schemes = {}
+    for name, wl in ADJOINT_SCHEMES.items():
+        try:
+            r = adjoint_timing(torch, "fp64", 0, wl)
+            adjoint_schemes[name] = {k: r[k] for k in ("forward_ms", "recorded_forward_ms", "adjoint_ms",
+                                                         "adjoint_over_forward", "gradient_over_forward")}
+        except Exception as exc:  # pragma: no cover
+            adjoint_schemes[name] = {"error": str(exc)}
 
     extra_cfg = {}
     if not args.no_extra:
@@ -796,7 +816,8 @@ def main():
             "adjoint": {"workload": "mhd2d-256^2-periodic smooth weno5z hll ssprk(3,3), 200 steps, "
                                     "J = kinetic energy in [0,0.25]^2, dJ/drho0; every stage input kept "
                                     "(\"checkpointed\": every 20 steps, with recomputation)",
-                        "fp64": adjoint["fp64"], "fp32": adjoint["fp32"]},
+                        "fp64": adjoint["fp64"], "fp32": adjoint["fp32"],
+                        "other_schemes_fp64": adjoint_schemes},
             "blast2d": dict({"workload": "hd2d-256^2-periodic blast (p 10 inside r < 0.1) tvd-mc hllc ssprk(2,2) "
                                          "cfl0.4, run to t = 0.2"}, **extra_cfg.get("blast2d", {})),
             "srmhd3d": dict({"workload": "srmhd3d-128^3-periodic gamma 4/3, B=(0.5,0,0), max Lorentz factor 10, "
