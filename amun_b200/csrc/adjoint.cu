@@ -34,6 +34,15 @@ constexpr int kFaceThreads = 128;
 #define AMUN_ADJ_FACE_MIN_BLOCKS 4
 #endif
 
+// the same for the MHD face kernels of HLLC / HLLD, whose dual-number passes
+// (dual.cuh) spill at 4 CTAs (measured on B200, 2D MHD 256^2 FP64, 200
+// steps: the HLLD adjoint 405 -> 377 ms with TVD, 608 -> 575 ms with WENO-Z;
+// the HD HLLC kernel spills nothing at 4 CTAs and was slower at 2, 46.7 ->
+// 59.5 ms, so it keeps AMUN_ADJ_FACE_MIN_BLOCKS)
+#ifndef AMUN_ADJ_DUAL_MIN_BLOCKS
+#define AMUN_ADJ_DUAL_MIN_BLOCKS 2
+#endif
+
 int blocks_of(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   return (int)(b < 1 ? 1 : (b > 65535LL * 32 ? 65535LL * 32 : b));
@@ -154,7 +163,9 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
 
 // blockIdx.z = direction
 template <int EQ, int REC, int RS, typename R>
-__global__ void __launch_bounds__(kFaceThreads, AMUN_ADJ_FACE_MIN_BLOCKS) face_kernel(const R* __restrict__ Q,
+__global__ void __launch_bounds__(kFaceThreads, RS == RS_HLL || EQ == EQ_HD ? AMUN_ADJ_FACE_MIN_BLOCKS
+                                                                            : AMUN_ADJ_DUAL_MIN_BLOCKS)
+    face_kernel(const R* __restrict__ Q,
                                                             const double* __restrict__ lamdu,
                                                             double* __restrict__ G, const double* __restrict__ binv,
                                                             Geo g, MethodConst m, const DevScalars* rec) {
