@@ -13,9 +13,11 @@ instead of the three sweeps.
 
 With --adjoint: the differentiation workload instead (2D GLM-MHD 256^2, smooth
 seeded state, WENO-Z, HLL, SSPRK(3,3)): `--steps` recorded steps with one
-checkpoint, then one adjoint of J = kinetic energy in [0,0.25]^2.
+checkpoint, then one adjoint of J = kinetic energy in [0,0.25]^2;
+--adj-reconstruction / --adj-riemann choose another scheme (tvd, hllc, hlld).
 
     python -m amun_b200.profile_case --adjoint --precision fp64 --steps 20
+    python -m amun_b200.profile_case --adjoint --precision fp64 --steps 20 --adj-reconstruction tvd --adj-riemann hlld
 
 With --regrid: a mesh update of the 3D MHD blast on a block mesh (4^3
 level-1 blocks of 16^3 cells, refined to --maxlev within 0.2 of the centre),
@@ -44,6 +46,8 @@ def main(argv=None):
     ap.add_argument("--reconstruction", default="weno5z")
     ap.add_argument("--riemann", default="hlld")
     ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--adj-reconstruction", default="weno5z", help="scheme of the --adjoint case")
+    ap.add_argument("--adj-riemann", default="hll", help="solver of the --adjoint case")
     ap.add_argument("--regrid", action="store_true")
     ap.add_argument("--maxlev", type=int, default=3)
     ap.add_argument("--stage-kernel", action="store_true", help="one fused launch per stage instead of the sweeps")
@@ -119,8 +123,9 @@ def adjoint_case(a):
     from amun_b200 import problems
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
-    p = dict(ndims=2, equation_system="mhd", reconstruction="weno5z", limiter="mc", riemann_solver="hll",
-             time_advance="rk3", cfl=0.4, gamma=5.0 / 3.0, nghosts=4, ncells=256, xmin=0, xmax=1, ymin=0, ymax=1)
+    p = dict(ndims=2, equation_system="mhd", reconstruction=a.adj_reconstruction, limiter="mc",
+             riemann_solver=a.adj_riemann, time_advance="rk3", cfl=0.4, gamma=5.0 / 3.0,
+             nghosts=2 if a.adj_reconstruction == "tvd" else 4, ncells=256, xmin=0, xmax=1, ymin=0, ymax=1)
     sim = Simulation(p, precision=a.precision)
     sim.set_primitive(problems.smooth_mhd(sim.mesh, seed=0))
     sim.forward_checkpointed(a.steps, 1.0e30, a.steps)
