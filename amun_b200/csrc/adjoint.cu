@@ -107,7 +107,7 @@ __device__ __forceinline__ long long dir_stride(const Geo& g) {
 // right face state, G[DIR][1] at R lam of R's left face state.
 template <int EQ, int DIR, int REC, int RS, typename R>
 __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const R* __restrict__ Q,
-                                          const double* __restrict__ lamdu, double* __restrict__ G, double dxi,
+                                          const double* __restrict__ lamdu, R* __restrict__ G, double dxi,
                                           const Geo& g, const Phys<R>& P, R eps, int lim) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
@@ -152,12 +152,12 @@ __device__ __forceinline__ void face_body(long long t, int b, int nblocks, const
   else riemann_rev_dual<EQ, RS, R>(a, c, ql, lql, lqr, P);
   unrotate<EQ, DIR>(lql, a);
   unrotate<EQ, DIR>(lqr, c);
-  double* G0 = G + (long long)(2 * DIR) * qd;
-  double* G1 = G0 + qd;
+  R* G0 = G + (long long)(2 * DIR) * qd;
+  R* G1 = G0 + qd;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    G0[cL + v * g.qvs] = (double)a[v];
-    G1[cL + sD + v * g.qvs] = (double)c[v];
+    G0[cL + v * g.qvs] = a[v];
+    G1[cL + sD + v * g.qvs] = c[v];
   }
 }
 
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kFaceThreads, RS == RS_HLL || EQ == EQ_HD ? AM
                                                                             : AMUN_ADJ_DUAL_MIN_BLOCKS)
     face_kernel(const R* __restrict__ Q,
                                                             const double* __restrict__ lamdu,
-                                                            double* __restrict__ G, const double* __restrict__ binv,
+                                                            R* __restrict__ G, const double* __restrict__ binv,
                                                             Geo g, MethodConst m, const DevScalars* rec) {
   const int b = blockIdx.y, dir = blockIdx.z;
   const int nt2 = g.ndims == 3 ? g.nc : 1;
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kFaceThreads, RS == RS_HLL || EQ == EQ_HD ? AM
 // P[DIR][m] at c = the partial for cell c-2+m.
 template <int DIR, typename R>
 __device__ __forceinline__ void weno_body(long long t, int b, int nblocks, const R* __restrict__ Q,
-                                          const double* __restrict__ G, double* __restrict__ P, const Geo& g,
+                                          const R* __restrict__ G, R* __restrict__ P, const Geo& g,
                                           int nv, R eps) {
   const int nc = g.nc, ng = g.ng;
   const int nt2 = g.ndims == 3 ? nc : 1;
@@ -204,20 +204,20 @@ __device__ __forceinline__ void weno_body(long long t, int b, int nblocks, const
   line_cell<DIR>(g, a, t1, t2, i, j, k);
   const long long cell = ((long long)k * g.JM + j) * g.IM + i;
   const long long c = (long long)b * g.qbs + v * g.qvs + cell;
-  const double* G0 = G + (long long)(2 * DIR) * qd;
-  const double lR = a <= ng + nc - 1 ? G0[c] : 0.0;
-  const double lL = a >= ng ? G0[qd + c] : 0.0;
+  const R* G0 = G + (long long)(2 * DIR) * qd;
+  const R lR = a <= ng + nc - 1 ? G0[c] : R(0);
+  const R lL = a >= ng ? G0[qd + c] : R(0);
   const R* q = Q + c;
   const R st[5] = {q[-2 * sD], q[-sD], q[0], q[sD], q[2 * sD]};
   R gg[5] = {R(0), R(0), R(0), R(0), R(0)};
   weno5z_pair_rev(st, R(lR), R(lL), gg, eps);
-  double* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
+  R* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
 #pragma unroll
-  for (int mm = 0; mm < 5; ++mm) Pd[mm * g.qbs] = (double)gg[mm];
+  for (int mm = 0; mm < 5; ++mm) Pd[mm * g.qbs] = gg[mm];
 }
 
 template <typename R>
-__global__ void weno_rev_kernel(const R* __restrict__ Q, const double* __restrict__ G, double* __restrict__ P, Geo g,
+__global__ void weno_rev_kernel(const R* __restrict__ Q, const R* __restrict__ G, R* __restrict__ P, Geo g,
                                 int nv, double eps_d) {
   const int b = blockIdx.y, dir = blockIdx.z;
   const int nt2 = g.ndims == 3 ? g.nc : 1;
@@ -237,7 +237,7 @@ __global__ void weno_rev_kernel(const R* __restrict__ Q, const double* __restric
 // P[DIR][0] and P[DIR][4] are zero.  pr = index of the pressure.
 template <int DIR, typename R>
 __device__ __forceinline__ void tvd_body(long long t, int b, int nblocks, const R* __restrict__ Q,
-                                         const double* __restrict__ G, double* __restrict__ P, const Geo& g, int nv,
+                                         const R* __restrict__ G, R* __restrict__ P, const Geo& g, int nv,
                                          int pr, int lim, R eps) {
   const int nc = g.nc, ng = g.ng;
   const int nt2 = g.ndims == 3 ? nc : 1;
@@ -254,25 +254,25 @@ __device__ __forceinline__ void tvd_body(long long t, int b, int nblocks, const 
   line_cell<DIR>(g, a, t1, t2, i, j, k);
   const long long cell = ((long long)k * g.JM + j) * g.IM + i;
   const long long c = (long long)b * g.qbs + v * g.qvs + cell;
-  const double* G0 = G + (long long)(2 * DIR) * qd;
-  const R lR = R(a <= ng + nc - 1 ? G0[c] : 0.0);
-  const R lL = R(a >= ng ? G0[qd + c] : 0.0);
+  const R* G0 = G + (long long)(2 * DIR) * qd;
+  const R lR = a <= ng + nc - 1 ? G0[c] : R(0);
+  const R lL = a >= ng ? G0[qd + c] : R(0);
   const R* q = Q + c;
   R fac;
   tvd_slope<R>(q, DIR, sxyz, g.ndims, v == 0 || v == pr, lim, eps, fac);
   R la = R(0), lb = R(0);
   const R ls = (lR - lL) * fac;
   if (ls != R(0)) limiter_rev<R>(lim, R(0.5), q[0] - q[-sD], q[sD] - q[0], eps, ls, la, lb);
-  double* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
-  Pd[0] = 0.0;
-  Pd[g.qbs] = (double)(-la);
-  Pd[2 * g.qbs] = (double)((lR + lL) + (la - lb));
-  Pd[3 * g.qbs] = (double)lb;
-  Pd[4 * g.qbs] = 0.0;
+  R* Pd = P + (long long)DIR * 5 * qd + (long long)b * 5 * g.qbs + v * g.qvs + cell;
+  Pd[0] = R(0);
+  Pd[g.qbs] = -la;
+  Pd[2 * g.qbs] = (lR + lL) + (la - lb);
+  Pd[3 * g.qbs] = lb;
+  Pd[4 * g.qbs] = R(0);
 }
 
 template <typename R>
-__global__ void tvd_rev_kernel(const R* __restrict__ Q, const double* __restrict__ G, double* __restrict__ P, Geo g,
+__global__ void tvd_rev_kernel(const R* __restrict__ Q, const R* __restrict__ G, R* __restrict__ P, Geo g,
                                int nv, int lim, double eps_d) {
   const int b = blockIdx.y, dir = blockIdx.z;
   const int nt2 = g.ndims == 3 ? g.nc : 1;
@@ -288,8 +288,8 @@ __global__ void tvd_rev_kernel(const R* __restrict__ Q, const double* __restrict
 // lq += the stencil partials aimed at padded cell (i,j,k) of block pb, over
 // the directions whose line through the cell is an interior line (the only
 // lines the WENO kernel covers) and sources s = a-2..a+2 in ng-1..ng+nc.
-template <int NV>
-__device__ __forceinline__ void gather_at(const double* __restrict__ P, const Geo& g, long long qd, int pb, int i,
+template <int NV, typename R>
+__device__ __forceinline__ void gather_at(const R* __restrict__ P, const Geo& g, long long qd, int pb, int i,
                                           int j, int k, double* lq) {
   const int nc = g.nc, ng = g.ng;
   const long long cell = ((long long)k * g.JM + j) * g.IM + i;
@@ -300,14 +300,14 @@ __device__ __forceinline__ void gather_at(const double* __restrict__ P, const Ge
     if (!line) continue;
     const int a = d == 0 ? i : (d == 1 ? j : k);
     const long long sD = d == 0 ? 1LL : (d == 1 ? (long long)g.IM : (long long)g.IM * g.JM);
-    const double* Pd = P + (long long)d * 5 * qd + (long long)pb * 5 * g.qbs;
+    const R* Pd = P + (long long)d * 5 * qd + (long long)pb * 5 * g.qbs;
 #pragma unroll
     for (int mm = 0; mm < 5; ++mm) {
       const int s = a + 2 - mm;
       if (s < ng - 1 || s > ng + nc) continue;
-      const double* ps = Pd + mm * g.qbs + cell + (long long)(s - a) * sD;
+      const R* ps = Pd + mm * g.qbs + cell + (long long)(s - a) * sD;
 #pragma unroll
-      for (int v = 0; v < NV; ++v) lq[v] += ps[v * g.qvs];
+      for (int v = 0; v < NV; ++v) lq[v] += (double)ps[v * g.qvs];
     }
   }
 }
@@ -316,7 +316,7 @@ __device__ __forceinline__ void gather_at(const double* __restrict__ P, const Ge
 // and at its ghost copies (image at c + o nc in block inv[o], for each of the
 // 26 directions o); then lamIn += cons2prim^T lam.
 template <int EQ, typename R>
-__global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ P, const int* __restrict__ inv,
+__global__ void cell_kernel(const R* __restrict__ Q, const R* __restrict__ P, const int* __restrict__ inv,
                             double gammam1, double* __restrict__ lamIn, Geo g) {
   using V = Var<EQ>;
   constexpr int NV = V::NV;
@@ -331,7 +331,7 @@ __global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ 
     double lq[NV], q[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) lq[v] = 0.0;
-    gather_at<NV>(P, g, qd, b, i, j, k, lq);
+    gather_at<NV, R>(P, g, qd, b, i, j, k, lq);
     for (int oz = -nz; oz <= nz; ++oz)
       for (int oy = -1; oy <= 1; ++oy)
         for (int ox = -1; ox <= 1; ++ox) {
@@ -340,7 +340,7 @@ __global__ void cell_kernel(const R* __restrict__ Q, const double* __restrict__ 
           if (gi < 0 || gi >= g.IM || gj < 0 || gj >= g.JM || gk < 0 || gk >= g.KM) continue;
           const int src = inv[27 * b + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
           if (src < 0) continue;
-          gather_at<NV>(P, g, qd, src, gi, gj, gk, lq);
+          gather_at<NV, R>(P, g, qd, src, gi, gj, gk, lq);
         }
     const long long cell = (long long)b * g.qbs + ((long long)k * g.JM + j) * g.IM + i;
 #pragma unroll
@@ -434,7 +434,7 @@ cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStr
 // face kernel of the configured system and solver: HLL has the hand-written
 // reverse, HLLC and HLLD (MHD) the dual-number one
 template <int REC, typename R>
-static void launch_faces(const AdjGeo& a, dim3 gf, const R* Q, const double* lamdu, double* G, const double* binv,
+static void launch_faces(const AdjGeo& a, dim3 gf, const R* Q, const double* lamdu, R* G, const double* binv,
                   const MethodConst& m, const DevScalars* rec, cudaStream_t s) {
   const Geo& g = a.g;
   if (a.eq == EQ_HD) {
@@ -456,12 +456,16 @@ cudaError_t adj_faces(const AdjGeo& a, const R* Q, const double* lamdu, double* 
   const long long nf = (long long)(g.nc + 1) * g.nc * nt2;
   const long long nw = (long long)(g.nc + 2) * g.nc * nt2 * a.nv;
   const dim3 gf(blocks_of(nf, kFaceThreads), a.nblocks, g.ndims), gw(blocks_for(nw), a.nblocks, g.ndims);
+  // G and P hold values computed in the working precision R: stored in R
+  // (the FP64-sized arrays are half used in FP32 bulk), read back exactly
+  R* Gr = reinterpret_cast<R*>(G);
+  R* Pr = reinterpret_cast<R*>(P);
   if (m.rec == REC_TVD) {
-    launch_faces<REC_TVD, R>(a, gf, Q, lamdu, G, binv, m, rec, s);
-    tvd_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.lim, m.eps);
+    launch_faces<REC_TVD, R>(a, gf, Q, lamdu, Gr, binv, m, rec, s);
+    tvd_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, Gr, Pr, g, a.nv, m.lim, m.eps);
   } else {
-    launch_faces<REC_WENO5Z, R>(a, gf, Q, lamdu, G, binv, m, rec, s);
-    weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, G, P, g, a.nv, m.eps);
+    launch_faces<REC_WENO5Z, R>(a, gf, Q, lamdu, Gr, binv, m, rec, s);
+    weno_rev_kernel<R><<<gw, kThreads, 0, s>>>(Q, Gr, Pr, g, a.nv, m.eps);
   }
   return cudaGetLastError();
 }
@@ -470,8 +474,9 @@ template <typename R>
 cudaError_t adj_cells(const AdjGeo& a, const R* Q, const double* P, const int* inv, double gammam1, double* lamIn,
                       cudaStream_t s) {
   dim3 grid(blocks_for(a.g.uvs), a.nblocks);
-  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
-  else cell_kernel<EQ_MHD, R><<<grid, kThreads, 0, s>>>(Q, P, inv, gammam1, lamIn, a.g);
+  const R* Pr = reinterpret_cast<const R*>(P);
+  if (a.eq == EQ_HD) cell_kernel<EQ_HD, R><<<grid, kThreads, 0, s>>>(Q, Pr, inv, gammam1, lamIn, a.g);
+  else cell_kernel<EQ_MHD, R><<<grid, kThreads, 0, s>>>(Q, Pr, inv, gammam1, lamIn, a.g);
   return cudaGetLastError();
 }
 

@@ -3,11 +3,13 @@
 // Device arrays (per block b; the layouts of sweep.cuh):
 //   Q      [b][v][k][j][i]     stage-input primitives, padded, working precision
 //   lamU0, lamU1, lamdu        [b][v][k][j][i] interior, FP64
-//   G      [d][side][b][v][k][j][i] padded, FP64: lam of a cell's right
-//                              (side 0) / left (side 1) face state along d
-//   P      [d][b][m][v][k][j][i] padded, FP64, m = 0..4: the WENO-Z stencil
+//   G      [d][side][b][v][k][j][i] padded, working precision (allocated
+//                              as FP64): lam of a cell's right (side 0) /
+//                              left (side 1) face state along d
+//   P      [d][b][m][v][k][j][i] padded, working precision (allocated as
+//                              FP64), m = 0..4: the WENO-Z (TVD) stencil
 //                              partials of a cell's two face states along d
-//                              with respect to cells c-2..c+2
+//                              with respect to cells c-2..c+2 (c-1..c+1)
 //   inv    [27 b + o]          the block whose neighbour in direction o is b
 #pragma once
 #include <cuda_runtime.h>
