@@ -7,7 +7,7 @@
 //   adj_faces         all directions in one launch each:
 //                     face kernel, per interface i+1/2: recompute the WENO-Z
 //                     face states, lamF = (lamdu(i+1) - lamdu(i))/dx, reverse
-//                     HLL (HLLC, HLLD: dual numbers, dual.cuh) -> lam of
+//                     HLL (HLLC, HLLD, Roe: dual numbers, dual.cuh) -> lam of
 //                     the two face states (G);
 //                     WENO kernel, per cell and variable: reverse WENO-Z of
 //                     both faces -> five stencil partials (P); with TVD
@@ -432,18 +432,22 @@ cudaError_t adj_fold_copy(const AdjGeo& a, double* lamU0, double* lamU1, cudaStr
 #endif  // AMUN_ADJ_FP32_UNIT
 
 // face kernel of the configured system and solver: HLL has the hand-written
-// reverse, HLLC and HLLD (MHD) the dual-number one
+// reverse, HLLC, HLLD (MHD) and Roe the dual-number one
 template <int REC, typename R>
 static void launch_faces(const AdjGeo& a, dim3 gf, const R* Q, const double* lamdu, R* G, const double* binv,
                   const MethodConst& m, const DevScalars* rec, cudaStream_t s) {
   const Geo& g = a.g;
   if (a.eq == EQ_HD) {
     if (a.rs == RS_HLLC) face_kernel<EQ_HD, REC, RS_HLLC, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else if (a.rs == RS_ROE)
+      face_kernel<EQ_HD, REC, RS_ROE, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
     else face_kernel<EQ_HD, REC, RS_HLL, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
   } else {
     if (a.rs == RS_HLLC) face_kernel<EQ_MHD, REC, RS_HLLC, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
     else if (a.rs == RS_HLLD)
       face_kernel<EQ_MHD, REC, RS_HLLD, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
+    else if (a.rs == RS_ROE)
+      face_kernel<EQ_MHD, REC, RS_ROE, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
     else face_kernel<EQ_MHD, REC, RS_HLL, R><<<gf, kFaceThreads, 0, s>>>(Q, lamdu, G, binv, g, m, rec);
   }
 }

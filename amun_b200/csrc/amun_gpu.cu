@@ -2396,9 +2396,9 @@ int adj_supported() {
     return fail(AMUN_E_UNSUPPORTED, "adjoint: adiabatic HD and MHD only");
   if (C.p.reconstruction != AMUN_REC_WENO5Z && C.p.reconstruction != AMUN_REC_TVD)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: WENO-Z or TVD reconstruction only");
-  if (effective_solver() != AMUN_RS_HLL && effective_solver() != AMUN_RS_HLLC &&
+  if (effective_solver() != AMUN_RS_HLL && effective_solver() != AMUN_RS_HLLC && effective_solver() != AMUN_RS_ROE &&
       !(C.p.eqsys == AMUN_EQ_MHD && effective_solver() == AMUN_RS_HLLD))
-    return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL, HLLC or HLLD Riemann solver only");
+    return fail(AMUN_E_UNSUPPORTED, "adjoint: HLL, HLLC, HLLD or Roe Riemann solver only");
   if (C.p.fix_positivity || C.p.clip_extrema || C.p.mlp)
     return fail(AMUN_E_UNSUPPORTED, "adjoint: fix_positivity, clip_extrema and mlp_limiting must be off");
   if (sources_on()) return fail(AMUN_E_UNSUPPORTED, "adjoint: no source terms");

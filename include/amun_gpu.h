@@ -418,8 +418,8 @@ int amun_gpu_set_stage_kernel(int mode, int planes, int* active);
 /* Discrete adjoint of a run: no counterpart in the reference (AMUN has no
  * adjoint).  Supported: adiabatic HD and MHD, WENO-Z (nghosts >= 4) or TVD
  * with any limiter (with the multi-dimensional positivity halving, whose
- * factor the derivative holds constant; nghosts >= 2), HLL, HLLC or (MHD)
- * HLLD, any SSPRK
+ * factor the derivative holds constant; nghosts >= 2), HLL, HLLC, (MHD)
+ * HLLD or Roe, any SSPRK
  * integrator, fix_positivity, clip_extrema and mlp_limiting off, FP64 or
  * FP32 bulk.  Each step's dt and GLM speed cmax are those of the forward run
  * and are held constant in the derivative.

@@ -126,20 +126,22 @@ def test_adjoint_matches_tape(eq, ta, nd, n, nb, nsteps, interval, rec, lim, rs)
     assert np.all(err <= 1e-9), err
 
 
-@pytest.mark.parametrize("rec,rs", [("weno5z", "hll"), ("tvd", "hll"), ("weno5z", "hllc"), ("weno5z", "hlld"),
-                                    ("tvd", "hlld")])
-def test_adjoint_finite_differences(rec, rs):
+@pytest.mark.parametrize("eq,rec,rs", [("mhd", "weno5z", "hll"), ("mhd", "tvd", "hll"), ("mhd", "weno5z", "hllc"),
+                                       ("mhd", "weno5z", "hlld"), ("mhd", "tvd", "hlld"), ("mhd", "weno5z", "roe"),
+                                       ("hd", "tvd", "roe")])
+def test_adjoint_finite_differences(eq, rec, rs):
     """The configuration's scheme (2D MHD, WENO-Z, HLL, SSPRK(3,3)) on 32^2,
     20 steps with checkpoints every 5, and the same with TVD-MC (on a state
     with every variable varying in every direction, field_all) and with the
-    MHD HLLC and HLLD solvers (dual-number reverse): dJ/drho0 along 8 seeded
-    smooth directions agrees with central differences to 1e-6 (FD step
-    swept over 1e-6..1e-8, runs replaying the recorded dt and cmax)."""
+    HLLC, HLLD and Roe solvers (dual-number reverse): dJ/drho0 along 8
+    seeded smooth directions agrees with central differences to 1e-6 (FD
+    step swept over 1e-6..1e-8, runs replaying the recorded dt and cmax)."""
     from amun_b200.adjoint import kinetic_energy
     from amun_b200.solver import Simulation
-    p = params("mhd", rec, rs, "rk3", ndims=2, ncells=32, **UNIT)
+    p = params(eq, rec, rs, "rk3", ndims=2, ncells=32, **UNIT)
     mesh = UniformMesh(geometry(p))
-    q0 = problems.smooth_mhd(mesh, seed=0) if rec == "weno5z" else field_all(mesh, 9, seed=0)
+    nv = 9 if eq == "mhd" else 5
+    q0 = problems.smooth_mhd(mesh, seed=0) if rec == "weno5z" else field_all(mesh, nv, seed=0)
     sim = Simulation(p)
     try:
         g, _, _ = gpu_gradient(sim, mesh, q0, 20, 5)
@@ -299,7 +301,7 @@ def test_adjoint_fp32_bulk(rec):
 def test_adjoint_rejects_unsupported():
     from amun_b200 import _native as N
     from amun_b200.solver import Simulation
-    sim = Simulation(params("mhd", "tvd", "roe", "rk2", ndims=2, ncells=16))
+    sim = Simulation(params("mhd", "weno3", "hll", "rk2", ndims=2, ncells=16))
     try:
         with pytest.raises(N.AmunError) as e:
             sim.forward_checkpointed(2, 1.0e30, 1)
